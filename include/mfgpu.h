@@ -1,0 +1,159 @@
+/* mfgpu.h -- C ABI of libmfgpu.so, a B200 (sm_100a) multifrontal sparse LU.
+ *
+ * libmfgpu replaces the numeric multifrontal factorization and the triangular
+ * solves of PureUMFPACK.jl behind the reference's own entry points:
+ *
+ *   splu(A; method=:multifrontal, scale, check)   src/interface.jl:93-120
+ *   multifrontal_lu(A; q, tol, check)            src/multifrontal.jl:146-358
+ *   PureUMFPACK.solve(F::PureLU, b; refine)       src/interface.jl:170-177
+ *   F \ b                                         src/interface.jl:179, src/solve.jl:66-79
+ *
+ * and keeps UMFPACK's convention  (F.Rs .* A)[F.p, F.q] == F.L * F.U.
+ *
+ * Conventions
+ *   - Every index array is int64 and 1-based, exactly the buffers of a Julia
+ *     SparseMatrixCSC{Float64,Int64} / Vector{Int64}; values are double.
+ *   - Functions return MFGPU_OK (0) on success, a positive column number k for
+ *     a zero pivot at factor column k when `check` is set (the reference's
+ *     SingularException(k)), or a negative MFGPU_ERR_* code.
+ *   - The caller allocates every output buffer; sizes come from the *_sizes
+ *     queries.  The library owns its device memory, one context per handle;
+ *     handles are independent and may be used from different host threads
+ *     (one thread per handle at a time).  No torch types cross this ABI.
+ */
+#ifndef MFGPU_H
+#define MFGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  MFGPU_OK = 0,
+  MFGPU_ERR_ARGUMENT = -1,      /* bad pointer, size or permutation (ArgumentError) */
+  MFGPU_ERR_CUDA = -2,          /* CUDA runtime error; see mfgpu_last_error */
+  MFGPU_ERR_NOMEM = -3,         /* device allocation failed */
+  MFGPU_ERR_STATE = -4,         /* call order: factor before analyze, solve before factor */
+  MFGPU_ERR_TIMEOUT = -5,       /* a bounded device wait ran out */
+  MFGPU_ERR_DIMENSION = -6,     /* non-square matrix (DimensionMismatch) */
+  MFGPU_ERR_INTERNAL = -7,
+  MFGPU_ERR_NO_DEVICE = -8      /* no CUDA device / wrong architecture */
+};
+
+enum { MFGPU_SCALE_NONE = 0, MFGPU_SCALE_SUM = 1, MFGPU_SCALE_MAX = 2 }; /* src/scaling.jl:11 */
+
+enum {
+  MFGPU_PRECISION_FP64 = 0,  /* all-FP64 fronts: the plain form */
+  MFGPU_PRECISION_MIXED = 1  /* FP32 fronts, FP64 refinement */
+};
+
+/* ------------------------------------------------------------------------
+ * Host-side ordering and symbolic analysis (no GPU needed).  The Julia host
+ * keeps its own code for these; they are here for hosts without it and give
+ * identical output.
+ * ---------------------------------------------------------------------- */
+
+/* row_scaling(A, kind) -> Rs (src/scaling.jl:92-115). */
+int mfgpu_row_scaling(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval, int32_t kind,
+                      double* rs);
+
+/* amd_order_sym(A; dense) (src/amd.jl:141-148): perm of 1:n. */
+int mfgpu_amd_order(int64_t n, const int64_t* colptr, const int64_t* rowval, double dense, int64_t* perm);
+
+/* colamd_order(A; dense) (src/amd.jl:183-188): AMD on the A'A column graph. */
+int mfgpu_colamd_order(int64_t m, int64_t n, const int64_t* colptr, const int64_t* rowval, double dense,
+                       int64_t* perm);
+
+typedef struct mfgpu_symbolic mfgpu_symbolic;
+
+/* symbolic_mf(A; q) (src/symbolic.jl:211-226); q may be NULL (AMD). */
+int mfgpu_symbolic_create(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* q,
+                          mfgpu_symbolic** out);
+void mfgpu_symbolic_destroy(mfgpu_symbolic* sym);
+/* out4 = {n, nsuper, length(upd_idx), length(child_idx)} */
+int mfgpu_symbolic_sizes(const mfgpu_symbolic* sym, int64_t* out4);
+/* SymbolicMF fields (src/symbolic.jl:203-209), flattened, any pointer may be
+ * NULL.  qf(n), parent(n; 0 = root), colcount(n) = length(colstruct[j]),
+ * sstart(nsuper+1), upd_ptr/upd_idx = colstruct[last column of each
+ * supernode], child_ptr/child_idx = childsupers. */
+int mfgpu_symbolic_get(const mfgpu_symbolic* sym, int64_t* qf, int64_t* parent, int64_t* colcount, int64_t* sstart,
+                       int64_t* upd_ptr, int64_t* upd_idx, int64_t* child_ptr, int64_t* child_idx);
+/* predicted_fill(S) (src/symbolic.jl:230-237). */
+int64_t mfgpu_symbolic_predicted_fill(const mfgpu_symbolic* sym);
+/* _factor_colptrs (src/multifrontal.jl:73-104): Lcolptr, Ucolptr (n+1 each). */
+int mfgpu_factor_colptrs(const mfgpu_symbolic* sym, int64_t* lcolptr, int64_t* ucolptr);
+const char* mfgpu_host_last_error(void);
+
+/* ------------------------------------------------------------------------
+ * GPU numeric factorization and solves.
+ * ---------------------------------------------------------------------- */
+
+typedef struct mfgpu_ctx mfgpu_ctx;
+
+typedef struct {
+  int32_t device;     /* CUDA device ordinal */
+  int32_t precision;  /* MFGPU_PRECISION_* */
+  int32_t flags;      /* reserved, 0 */
+  int32_t reserved;
+} mfgpu_options;
+
+int mfgpu_create(const mfgpu_options* opts, mfgpu_ctx** out);
+void mfgpu_destroy(mfgpu_ctx* h);
+const char* mfgpu_last_error(const mfgpu_ctx* h);
+/* Work is issued on this stream (a cudaStream_t; NULL = the handle's own). */
+int mfgpu_set_stream(mfgpu_ctx* h, void* cuda_stream);
+int mfgpu_set_precision(mfgpu_ctx* h, int32_t precision);
+
+/* Pattern analysis for the numeric phase, from the reference's own symbolic
+ * result: A's pattern (colptr, rowval, n x n), SymbolicMF.qf, .parent,
+ * .sstart, and the update set of every supernode, i.e. colstruct[sstart[s+1]-1]
+ * flattened into upd_ptr (nsuper+1) / upd_idx.  Replaces the pattern-only part
+ * of multifrontal_lu (src/multifrontal.jl:152-196). */
+int mfgpu_analyze(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf,
+                  const int64_t* parent, int64_t nsuper, const int64_t* sstart, const int64_t* upd_ptr,
+                  const int64_t* upd_idx);
+/* Same, from a libmfgpu symbolic object. */
+int mfgpu_analyze_symbolic(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const int64_t* rowval,
+                           const mfgpu_symbolic* sym);
+
+/* Numeric factorization of Diagonal(Rs) * A with A's values nzval (host
+ * memory, pattern as analyzed); Rs may be NULL (no scaling, as
+ * multifrontal_lu).  Replaces the hot loop of src/multifrontal.jl:198-357.
+ * Returns 0, the singular column (check != 0), or an error. */
+int mfgpu_factor(mfgpu_ctx* h, const double* nzval, const double* rs, int32_t check);
+/* Same with device pointers (inputs already resident in HBM). */
+int mfgpu_factor_device(mfgpu_ctx* h, const double* d_nzval, const double* d_rs, int32_t check);
+
+/* out3 = {n, nnz(L), nnz(U)} of the last factorization. */
+int mfgpu_factor_sizes(mfgpu_ctx* h, int64_t* out3);
+/* Copy the factors to host CSC buffers (GPLUFactorization fields,
+ * src/gplu.jl:45-51): L unit lower with its diagonal first, U upper with its
+ * diagonal last, p, q, pinv; any pointer may be NULL. */
+int mfgpu_get_factors(mfgpu_ctx* h, int64_t* lcolptr, int64_t* lrowval, double* lnzval, int64_t* ucolptr,
+                      int64_t* urowval, double* unzval, int64_t* p, int64_t* q, int64_t* pinv);
+
+/* solve(F, b; refine) for nrhs right-hand sides B (n x nrhs, column-major,
+ * leading dimension ldb) into X (ldx), host memory.  The factors are those of
+ * the last mfgpu_factor; Rs is the scaling given there; the refinement
+ * residual r = b - A x uses the unscaled A values given there
+ * (src/interface.jl:123-138, 170-177; src/solve.jl:10-39). */
+int mfgpu_solve(mfgpu_ctx* h, int64_t nrhs, const double* b, int64_t ldb, double* x, int64_t ldx, int32_t refine);
+/* Same with device pointers. */
+int mfgpu_solve_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ldb, double* d_x, int64_t ldx,
+                       int32_t refine);
+
+/* Normwise backward error max_k ||b_k - A x_k||_inf / (||A||_inf ||x_k||_inf + ||b_k||_inf)
+ * of device arrays, computed in FP64 on the GPU with the analyzed pattern. */
+int mfgpu_backward_error_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ldb, const double* d_x,
+                                int64_t ldx, double* out);
+
+/* JSON object with the last call's phase times, sizes and counters. */
+int mfgpu_stats_json(mfgpu_ctx* h, char* buf, int64_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MFGPU_H */

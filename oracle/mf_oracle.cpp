@@ -1,0 +1,1089 @@
+// mf_oracle.cpp -- CPU oracle for the multifrontal LU path of PureUMFPACK.jl.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the checker: tests, the smoke check
+// and the CPU-baseline leg of the benchmark call it to produce the reference
+// answer.  The shipped library (libmfgpu.so) never links, loads or calls it.
+//
+// It restates, step for step, the reference's Julia algorithm:
+//   row scaling            src/scaling.jl:92-126
+//   AMD / COLAMD ordering  src/amd.jl:13-539   (CSparse cs_amd, order=1)
+//   symbolic analysis      src/symbolic.jl:15-237
+//   numeric multifrontal   src/multifrontal.jl:45-375
+//   CSC triangular solves  src/solve.jl:10-39
+//   solve + refinement     src/interface.jl:123-177
+// The dense front kernels (getrf / trsm / gemm) are the same LAPACK/BLAS calls
+// the reference makes through Julia's LinearAlgebra (multifrontal.jl:248,265,
+// 266,268).  They are taken from numpy's bundled ILP64 OpenBLAS, loaded with
+// dlopen at run time (orc_set_blas), so pivot choices follow LAPACK's partial
+// pivoting exactly as Julia's OpenBLAS does.
+//
+// Index convention on the C ABI: 1-based int64, as SparseMatrixCSC{Float64,Int64}.
+// Internally everything is 0-based.
+
+#include <dlfcn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+typedef int64_t i64;
+using std::vector;
+
+// ---------------------------------------------------------------------------
+// BLAS / LAPACK (ILP64 Fortran interface of numpy's OpenBLAS)
+// ---------------------------------------------------------------------------
+typedef void (*dgetrf_fn)(const i64*, const i64*, double*, const i64*, i64*, i64*);
+typedef void (*dtrsm_fn)(const char*, const char*, const char*, const char*, const i64*,
+                         const i64*, const double*, const double*, const i64*, double*,
+                         const i64*, size_t, size_t, size_t, size_t);
+typedef void (*dgemm_fn)(const char*, const char*, const i64*, const i64*, const i64*,
+                         const double*, const double*, const i64*, const double*, const i64*,
+                         const double*, double*, const i64*, size_t, size_t);
+typedef void (*setthreads_fn)(int);
+typedef int (*getthreads_fn)(void);
+
+static dgetrf_fn g_dgetrf = nullptr;
+static dtrsm_fn g_dtrsm = nullptr;
+static dgemm_fn g_dgemm = nullptr;
+static setthreads_fn g_setthreads = nullptr;
+static getthreads_fn g_getthreads = nullptr;
+static std::string g_err;
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// CSC helpers (0-based)
+// ---------------------------------------------------------------------------
+struct Pattern {           // CSC pattern with sorted rows
+  i64 n = 0;
+  vector<i64> cp;          // n+1
+  vector<i64> ri;
+};
+
+// Transpose of a CSC pattern (m rows, n cols) -> (n rows, m cols); rows come
+// out sorted because columns are visited in order (counting sort).
+Pattern transpose_pattern(i64 m, i64 n, const i64* cp, const i64* ri) {
+  Pattern t;
+  t.n = m;
+  t.cp.assign(m + 1, 0);
+  i64 nz = cp[n];
+  t.ri.resize(nz);
+  for (i64 p = 0; p < nz; ++p) t.cp[ri[p] + 1]++;
+  for (i64 i = 0; i < m; ++i) t.cp[i + 1] += t.cp[i];
+  vector<i64> cur(t.cp.begin(), t.cp.end() - 1);
+  for (i64 j = 0; j < n; ++j)
+    for (i64 p = cp[j]; p < cp[j + 1]; ++p) t.ri[cur[ri[p]]++] = j;
+  return t;
+}
+
+// Pattern of A + A^T with sorted rows (sparse add of two sorted CSC), diagonal
+// kept or dropped.  Mirrors `Pat + copy(transpose(Pat))` (amd.jl:84-87,
+// symbolic.jl:16-17) followed by the diagonal drop.
+Pattern sym_pattern(i64 n, const i64* cp, const i64* ri, bool drop_diag) {
+  Pattern t = transpose_pattern(n, n, cp, ri);
+  Pattern s;
+  s.n = n;
+  s.cp.assign(n + 1, 0);
+  s.ri.reserve(2 * cp[n]);
+  for (i64 j = 0; j < n; ++j) {
+    i64 a = cp[j], ae = cp[j + 1], b = t.cp[j], be = t.cp[j + 1];
+    while (a < ae || b < be) {
+      i64 r;
+      if (b >= be || (a < ae && ri[a] < t.ri[b])) {
+        r = ri[a++];
+      } else if (a >= ae || t.ri[b] < ri[a]) {
+        r = t.ri[b++];
+      } else {
+        r = ri[a];
+        ++a;
+        ++b;
+      }
+      if (!(drop_diag && r == j)) s.ri.push_back(r);
+    }
+    s.cp[j + 1] = (i64)s.ri.size();
+  }
+  return s;
+}
+
+// Symmetric permutation of a symmetric pattern: new column j = old column
+// perm[j], rows relabelled through inv(perm) and re-sorted.
+// Restates _permute_sym_csc1 (symbolic.jl:40-63).
+Pattern permute_sym(const Pattern& a, const vector<i64>& perm) {
+  i64 n = a.n;
+  vector<i64> pinv(n);
+  for (i64 k = 0; k < n; ++k) pinv[perm[k]] = k;
+  Pattern b;
+  b.n = n;
+  b.cp.assign(n + 1, 0);
+  for (i64 j = 0; j < n; ++j) b.cp[j + 1] = b.cp[j] + (a.cp[perm[j] + 1] - a.cp[perm[j]]);
+  b.ri.resize(b.cp[n]);
+  for (i64 j = 0; j < n; ++j) {
+    i64 oj = perm[j], dst = b.cp[j];
+    for (i64 p = a.cp[oj]; p < a.cp[oj + 1]; ++p) b.ri[dst++] = pinv[a.ri[p]];
+    std::sort(b.ri.begin() + b.cp[j], b.ri.begin() + b.cp[j + 1]);
+  }
+  return b;
+}
+
+// ---------------------------------------------------------------------------
+// AMD  (amd.jl:191-539; CSparse cs_amd with order = 1)
+// ---------------------------------------------------------------------------
+inline i64 flip(i64 x) { return -x - 2; }
+
+i64 wclear(i64 mark, i64 lemax, i64* w, i64 n) {   // amd.jl:17-25
+  if (mark < 2 || mark + lemax < 0) {
+    for (i64 k = 0; k < n; ++k)
+      if (w[k] != 0) w[k] = 1;
+    mark = 2;
+  }
+  return mark;
+}
+
+i64 tdfs(i64 j, i64 k, i64* head, const i64* next, i64* post, i64* stack) {  // amd.jl:28-48
+  i64 top = 0;
+  stack[0] = j;
+  while (top >= 0) {
+    i64 p = stack[top];
+    i64 i = head[p];
+    if (i == -1) {
+      --top;
+      post[k++] = p;
+    } else {
+      head[p] = next[i];
+      stack[++top] = i;
+    }
+  }
+  return k;
+}
+
+// cp: n+1 column pointers (0-based), ci: row indices (diagonal dropped,
+// sorted).  Returns the 0-based permutation.
+vector<i64> amd_core(i64 n, const vector<i64>& cp, const vector<i64>& ci0, double dense) {
+  i64 cnz = cp[n];
+  i64 t = cnz + cnz / 5 + 2 * n;
+  vector<i64> Ci(std::max<i64>(t, 1));
+  std::copy(ci0.begin(), ci0.begin() + cnz, Ci.begin());
+  double dthresh = std::max(16.0, dense * std::sqrt((double)n));
+  i64 densethr = std::min<i64>(n - 2, (i64)std::floor(dthresh));
+
+  vector<i64> len(n + 1), nv(n + 1), next(n + 1), head(n + 1), elen(n + 1), degree(n + 1),
+      w(n + 1), hhead(n + 1), last(n + 1), P(n + 1), Cp(n + 1);
+  for (i64 k = 0; k < n; ++k) {
+    len[k] = cp[k + 1] - cp[k];
+    Cp[k] = cp[k];
+  }
+  Cp[n] = cp[n];
+  len[n] = 0;
+  i64 nzmax = (i64)Ci.size();
+  for (i64 i = 0; i <= n; ++i) {
+    head[i] = -1;
+    last[i] = -1;
+    next[i] = -1;
+    hhead[i] = -1;
+    nv[i] = 1;
+    w[i] = 1;
+    elen[i] = 0;
+    degree[i] = len[i];
+  }
+  i64 mark = wclear(0, 0, w.data(), n);
+  elen[n] = -2;
+  Cp[n] = -1;
+  w[n] = 0;
+
+  i64 nel = 0;
+  for (i64 i = 0; i < n; ++i) {     // initialize degree lists (amd.jl:240-260)
+    i64 d = degree[i];
+    if (d == 0) {
+      elen[i] = -2;
+      ++nel;
+      Cp[i] = -1;
+      w[i] = 0;
+    } else if (d > densethr) {
+      nv[i] = 0;
+      elen[i] = -1;
+      ++nel;
+      Cp[i] = flip(n);
+      nv[n]++;
+    } else {
+      if (head[d] != -1) last[head[d]] = i;
+      next[i] = head[d];
+      head[d] = i;
+    }
+  }
+
+  i64 mindeg = 0, lemax = 0;
+  while (nel < n) {
+    // select node of minimum approximate degree (amd.jl:267-281)
+    i64 k = -1;
+    for (; mindeg < n; ++mindeg) {
+      k = head[mindeg];
+      if (k != -1) break;
+    }
+    if (next[k] != -1) last[next[k]] = -1;
+    head[mindeg] = next[k];
+    i64 elenk = elen[k], nvk = nv[k];
+    nel += nvk;
+
+    // garbage collection (amd.jl:283-308)
+    if (elenk > 0 && cnz + mindeg >= nzmax) {
+      for (i64 j = 0; j < n; ++j) {
+        i64 p = Cp[j];
+        if (p >= 0) {
+          Cp[j] = Ci[p];
+          Ci[p] = flip(j);
+        }
+      }
+      i64 q = 0, p = 0;
+      while (p < cnz) {
+        i64 j = flip(Ci[p++]);
+        if (j >= 0) {
+          Ci[q] = Cp[j];
+          Cp[j] = q++;
+          for (i64 k3 = 0; k3 < len[j] - 1; ++k3) Ci[q++] = Ci[p++];
+        }
+      }
+      cnz = q;
+    }
+
+    // construct new element (amd.jl:311-356)
+    i64 dk = 0;
+    nv[k] = -nvk;
+    i64 p = Cp[k];
+    i64 pk1 = (elenk == 0) ? p : cnz;
+    i64 pk2 = pk1;
+    for (i64 k1 = 1; k1 <= elenk + 1; ++k1) {
+      i64 e, pj, ln;
+      if (k1 > elenk) {
+        e = k;
+        pj = p;
+        ln = len[k] - elenk;
+      } else {
+        e = Ci[p++];
+        pj = Cp[e];
+        ln = len[e];
+      }
+      for (i64 k2 = 1; k2 <= ln; ++k2) {
+        i64 i = Ci[pj++];
+        i64 nvi = nv[i];
+        if (nvi <= 0) continue;
+        dk += nvi;
+        nv[i] = -nvi;
+        Ci[pk2++] = i;
+        if (next[i] != -1) last[next[i]] = last[i];
+        if (last[i] != -1)
+          next[last[i]] = next[i];
+        else
+          head[degree[i]] = next[i];
+      }
+      if (e != k) {
+        Cp[e] = flip(k);
+        w[e] = 0;
+      }
+    }
+    if (elenk != 0) cnz = pk2;
+    degree[k] = dk;
+    Cp[k] = pk1;
+    len[k] = pk2 - pk1;
+    elen[k] = -2;
+
+    // set differences (amd.jl:359-374)
+    mark = wclear(mark, lemax, w.data(), n);
+    for (i64 pk = pk1; pk < pk2; ++pk) {
+      i64 i = Ci[pk];
+      i64 eln = elen[i];
+      if (eln <= 0) continue;
+      i64 nvi = -nv[i];
+      i64 wnvi = mark - nvi;
+      for (i64 p2 = Cp[i]; p2 <= Cp[i] + eln - 1; ++p2) {
+        i64 e = Ci[p2];
+        if (w[e] >= mark)
+          w[e] -= nvi;
+        else if (w[e] != 0)
+          w[e] = degree[e] + wnvi;
+      }
+    }
+
+    // degree update (amd.jl:377-432)
+    for (i64 pk = pk1; pk < pk2; ++pk) {
+      i64 i = Ci[pk];
+      i64 p1 = Cp[i];
+      i64 p2 = p1 + elen[i] - 1;
+      i64 pn = p1;
+      i64 h = 0, d = 0;
+      for (i64 p3 = p1; p3 <= p2; ++p3) {
+        i64 e = Ci[p3];
+        if (w[e] != 0) {
+          i64 dext = w[e] - mark;
+          if (dext > 0) {
+            d += dext;
+            Ci[pn++] = e;
+            h += e;
+          } else {
+            Cp[e] = flip(k);
+            w[e] = 0;
+          }
+        }
+      }
+      elen[i] = pn - p1 + 1;
+      i64 p3 = pn;
+      i64 p4 = p1 + len[i];
+      for (i64 p5 = p2 + 1; p5 < p4; ++p5) {
+        i64 j = Ci[p5];
+        i64 nvj = nv[j];
+        if (nvj <= 0) continue;
+        d += nvj;
+        Ci[pn++] = j;
+        h += j;
+      }
+      if (d == 0) {
+        Cp[i] = flip(k);
+        i64 nvi = -nv[i];
+        dk -= nvi;
+        nvk += nvi;
+        nel += nvi;
+        nv[i] = 0;
+        elen[i] = -1;
+      } else {
+        degree[i] = std::min(degree[i], d);
+        Ci[pn] = Ci[p3];
+        Ci[p3] = Ci[p1];
+        Ci[p1] = k;
+        len[i] = pn - p1 + 1;
+        h = h % n;
+        next[i] = hhead[h];
+        hhead[h] = i;
+        last[i] = h;
+      }
+    }
+    degree[k] = dk;
+    lemax = std::max(lemax, dk);
+    mark = wclear(mark + lemax, lemax, w.data(), n);
+
+    // supervariable detection (amd.jl:438-474)
+    for (i64 pk = pk1; pk < pk2; ++pk) {
+      i64 i = Ci[pk];
+      if (nv[i] >= 0) continue;
+      i64 h = last[i];
+      i = hhead[h];
+      hhead[h] = -1;
+      while (i != -1 && next[i] != -1) {
+        i64 ln = len[i], eln = elen[i];
+        for (i64 pp = Cp[i] + 1; pp <= Cp[i] + ln - 1; ++pp) w[Ci[pp]] = mark;
+        i64 jlast = i;
+        i64 j = next[i];
+        while (j != -1) {
+          bool ok = (len[j] == ln) && (elen[j] == eln);
+          for (i64 pp = Cp[j] + 1; ok && pp <= Cp[j] + ln - 1; ++pp)
+            if (w[Ci[pp]] != mark) ok = false;
+          if (ok) {
+            Cp[j] = flip(i);
+            nv[i] += nv[j];
+            nv[j] = 0;
+            elen[j] = -1;
+            j = next[j];
+            next[jlast] = j;
+          } else {
+            jlast = j;
+            j = next[j];
+          }
+        }
+        i = next[i];
+        ++mark;
+      }
+    }
+
+    // finalize new element (amd.jl:477-504)
+    p = pk1;
+    for (i64 pk = pk1; pk < pk2; ++pk) {
+      i64 i = Ci[pk];
+      i64 nvi = -nv[i];
+      if (nvi <= 0) continue;
+      nv[i] = nvi;
+      i64 d = degree[i] + dk - nvi;
+      d = std::min(d, n - nel - nvi);
+      if (head[d] != -1) last[head[d]] = i;
+      next[i] = head[d];
+      last[i] = -1;
+      head[d] = i;
+      mindeg = std::min(mindeg, d);
+      degree[i] = d;
+      Ci[p++] = i;
+    }
+    nv[k] = nvk;
+    len[k] = p - pk1;
+    if (len[k] == 0) {
+      Cp[k] = -1;
+      w[k] = 0;
+    }
+    if (elenk != 0) cnz = p;
+  }
+
+  // postorder the assembly tree (amd.jl:508-531)
+  for (i64 i = 0; i < n; ++i) Cp[i] = flip(Cp[i]);
+  for (i64 j = 0; j <= n; ++j) head[j] = -1;
+  for (i64 j = n; j >= 0; --j) {
+    if (nv[j] > 0) continue;
+    next[j] = head[Cp[j]];
+    head[Cp[j]] = j;
+  }
+  for (i64 e = n; e >= 0; --e) {
+    if (nv[e] <= 0) continue;
+    if (Cp[e] != -1) {
+      next[e] = head[Cp[e]];
+      head[Cp[e]] = e;
+    }
+  }
+  i64 k = 0;
+  for (i64 i = 0; i <= n; ++i)
+    if (Cp[i] == -1) k = tdfs(i, k, head.data(), next.data(), P.data(), w.data());
+  return vector<i64>(P.begin(), P.begin() + n);
+}
+
+vector<i64> amd_order_sym0(i64 n, const i64* cp, const i64* ri, double dense) {  // amd.jl:141-148
+  if (n == 0) return {};
+  if (n == 1) return {0};
+  Pattern s = sym_pattern(n, cp, ri, true);
+  return amd_core(n, s.cp, s.ri, dense);
+}
+
+// COLAMD = AMD on the pattern of A^T A with dense rows of A dropped
+// (amd.jl:91-104, 183-188).  m = number of rows of A.
+vector<i64> colamd_order0(i64 m, i64 n, const i64* cp, const i64* ri, double dense) {
+  vector<i64> id(n);
+  if (n <= 1) {
+    for (i64 j = 0; j < n; ++j) id[j] = j;
+    return id;
+  }
+  Pattern at = transpose_pattern(m, n, cp, ri);   // column i of AT = row i of A
+  i64 densethr = (i64)std::floor(std::min((double)(n - 2), std::max(16.0, dense * std::sqrt((double)n))));
+  // C = AT2 * AT2^T restricted to kept rows: C(:,j) = union over rows r of A in
+  // column j (kept) of the columns of row r.
+  vector<char> keep(m);
+  for (i64 r = 0; r < m; ++r) keep[r] = (at.cp[r + 1] - at.cp[r]) <= densethr;
+  Pattern c;
+  c.n = n;
+  c.cp.assign(n + 1, 0);
+  vector<i64> mark(n, -1), buf;
+  for (i64 j = 0; j < n; ++j) {
+    buf.clear();
+    for (i64 p = cp[j]; p < cp[j + 1]; ++p) {
+      i64 r = ri[p];
+      if (!keep[r]) continue;
+      for (i64 q = at.cp[r]; q < at.cp[r + 1]; ++q) {
+        i64 i = at.ri[q];
+        if (mark[i] != j) {
+          mark[i] = j;
+          if (i != j) buf.push_back(i);
+        }
+      }
+    }
+    std::sort(buf.begin(), buf.end());
+    c.ri.insert(c.ri.end(), buf.begin(), buf.end());
+    c.cp[j + 1] = (i64)c.ri.size();
+  }
+  return amd_core(n, c.cp, c.ri, dense);
+}
+
+// ---------------------------------------------------------------------------
+// Symbolic analysis (symbolic.jl:15-237)
+// ---------------------------------------------------------------------------
+vector<i64> etree0(const Pattern& s) {   // symbolic.jl:67-82 (nil = -1)
+  i64 n = s.n;
+  vector<i64> parent(n, -1), anc(n, -1);
+  for (i64 k = 0; k < n; ++k) {
+    for (i64 p = s.cp[k]; p < s.cp[k + 1]; ++p) {
+      i64 i = s.ri[p];
+      while (i != -1 && i < k) {
+        i64 inext = anc[i];
+        anc[i] = k;
+        if (inext == -1) parent[i] = k;
+        i = inext;
+      }
+    }
+  }
+  return parent;
+}
+
+vector<i64> postorder0(const vector<i64>& parent) {   // symbolic.jl:86-116
+  i64 n = (i64)parent.size();
+  vector<i64> head(n, -1), nextc(n, -1), post(n), stack(n);
+  for (i64 j = n - 1; j >= 0; --j) {
+    i64 p = parent[j];
+    if (p != -1) {
+      nextc[j] = head[p];
+      head[p] = j;
+    }
+  }
+  i64 k = 0;
+  for (i64 j = 0; j < n; ++j) {
+    if (parent[j] != -1) continue;
+    i64 top = 0;
+    stack[0] = j;
+    while (top >= 0) {
+      i64 p = stack[top];
+      i64 i = head[p];
+      if (i == -1) {
+        --top;
+        post[k++] = p;
+      } else {
+        head[p] = nextc[i];
+        stack[++top] = i;
+      }
+    }
+  }
+  return post;
+}
+
+struct Symbolic {
+  i64 n = 0;
+  vector<i64> qf;                       // 0-based
+  vector<i64> parent;                   // -1 = root
+  vector<i64> cs_ptr, cs_idx;           // colstruct, flattened (0-based rows)
+  vector<i64> sstart;                   // nsuper+1, 0-based
+  vector<i64> super_of;
+  vector<i64> ch_ptr, ch_idx;           // childsupers, flattened, 0-based
+};
+
+// symbolic.jl:122-160 (union rule), 167-194 (fundamental supernodes), 211-226.
+Symbolic symbolic_mf0(i64 n, const i64* cp, const i64* ri, const vector<i64>* q) {
+  Symbolic S;
+  S.n = n;
+  vector<i64> qamd = q ? *q : amd_order_sym0(n, cp, ri, 10.0);
+  Pattern sym = sym_pattern(n, cp, ri, true);
+  Pattern p1 = permute_sym(sym, qamd);       // == _sym_csc1(A[qamd,qamd])
+  vector<i64> parent1 = etree0(p1);
+  vector<i64> post = postorder0(parent1);
+  S.qf.resize(n);
+  for (i64 k = 0; k < n; ++k) S.qf[k] = qamd[post[k]];
+  Pattern pf = permute_sym(p1, post);
+  S.parent = etree0(pf);
+
+  // column structure of L
+  vector<i64> head(n, -1), nextc(n, -1), marker(n, -1), scratch(n);
+  for (i64 j = n - 1; j >= 0; --j) {
+    i64 p = S.parent[j];
+    if (p != -1) {
+      nextc[j] = head[p];
+      head[p] = j;
+    }
+  }
+  S.cs_ptr.assign(n + 1, 0);
+  vector<vector<i64>> cols(n);
+  for (i64 j = 0; j < n; ++j) {
+    i64 cnt = 0;
+    marker[j] = j;
+    for (i64 p = pf.cp[j]; p < pf.cp[j + 1]; ++p) {
+      i64 i = pf.ri[p];
+      if (i > j && marker[i] != j) {
+        marker[i] = j;
+        scratch[cnt++] = i;
+      }
+    }
+    for (i64 c = head[j]; c != -1; c = nextc[c]) {
+      for (i64 i : cols[c]) {
+        if (i > j && marker[i] != j) {
+          marker[i] = j;
+          scratch[cnt++] = i;
+        }
+      }
+    }
+    cols[j].assign(scratch.begin(), scratch.begin() + cnt);
+    std::sort(cols[j].begin(), cols[j].end());
+  }
+  for (i64 j = 0; j < n; ++j) S.cs_ptr[j + 1] = S.cs_ptr[j] + (i64)cols[j].size();
+  S.cs_idx.reserve(S.cs_ptr[n]);
+  for (i64 j = 0; j < n; ++j) S.cs_idx.insert(S.cs_idx.end(), cols[j].begin(), cols[j].end());
+
+  // fundamental supernodes
+  vector<i64> nchild(n, 0);
+  for (i64 j = 0; j < n; ++j)
+    if (S.parent[j] != -1) nchild[S.parent[j]]++;
+  S.super_of.assign(n, 0);
+  i64 nsuper = 0;
+  for (i64 j = 0; j < n; ++j) {
+    bool cont = j > 0 && S.parent[j - 1] == j && nchild[j] == 1 &&
+                (i64)cols[j - 1].size() == (i64)cols[j].size() + 1;
+    if (!cont) {
+      ++nsuper;
+      S.sstart.push_back(j);
+    }
+    S.super_of[j] = nsuper - 1;
+  }
+  S.sstart.push_back(n);
+  vector<vector<i64>> kids(nsuper);
+  for (i64 sk = 0; sk < nsuper; ++sk) {
+    i64 lastcol = S.sstart[sk + 1] - 1;
+    i64 p = S.parent[lastcol];
+    if (p != -1) kids[S.super_of[p]].push_back(sk);
+  }
+  S.ch_ptr.assign(nsuper + 1, 0);
+  for (i64 sk = 0; sk < nsuper; ++sk) {
+    S.ch_ptr[sk + 1] = S.ch_ptr[sk] + (i64)kids[sk].size();
+    S.ch_idx.insert(S.ch_idx.end(), kids[sk].begin(), kids[sk].end());
+  }
+  return S;
+}
+
+// ---------------------------------------------------------------------------
+// Numeric multifrontal (multifrontal.jl:45-375)
+// ---------------------------------------------------------------------------
+struct Factor {
+  i64 n = 0;
+  vector<i64> Lp, Li, Up, Ui;           // 0-based
+  vector<double> Lx, Ux;
+  vector<i64> p, q, pinv;               // 0-based
+  i64 status = 0;                       // 0 ok, k>0: singular at column k (1-based)
+};
+
+// A[qf,qf] as CSC (sorted rows) plus its transpose.
+struct Csc {
+  i64 n = 0;
+  vector<i64> cp, ri;
+  vector<double> x;
+};
+
+Csc permute_csc(i64 n, const i64* cp, const i64* ri, const double* x, const vector<i64>& q) {
+  vector<i64> pinv(n);
+  for (i64 k = 0; k < n; ++k) pinv[q[k]] = k;
+  Csc v;
+  v.n = n;
+  v.cp.assign(n + 1, 0);
+  for (i64 j = 0; j < n; ++j) v.cp[j + 1] = v.cp[j] + (cp[q[j] + 1] - cp[q[j]]);
+  v.ri.resize(v.cp[n]);
+  v.x.resize(v.cp[n]);
+  vector<std::pair<i64, double>> tmp;
+  for (i64 j = 0; j < n; ++j) {
+    tmp.clear();
+    for (i64 p = cp[q[j]]; p < cp[q[j] + 1]; ++p) tmp.push_back({pinv[ri[p]], x[p]});
+    std::sort(tmp.begin(), tmp.end(),
+              [](const std::pair<i64, double>& a, const std::pair<i64, double>& b) { return a.first < b.first; });
+    for (size_t t = 0; t < tmp.size(); ++t) {
+      v.ri[v.cp[j] + t] = tmp[t].first;
+      v.x[v.cp[j] + t] = tmp[t].second;
+    }
+  }
+  return v;
+}
+
+Csc transpose_csc(const Csc& a) {
+  Csc t;
+  i64 n = a.n;
+  t.n = n;
+  t.cp.assign(n + 1, 0);
+  i64 nz = a.cp[n];
+  t.ri.resize(nz);
+  t.x.resize(nz);
+  for (i64 p = 0; p < nz; ++p) t.cp[a.ri[p] + 1]++;
+  for (i64 i = 0; i < n; ++i) t.cp[i + 1] += t.cp[i];
+  vector<i64> cur(t.cp.begin(), t.cp.end() - 1);
+  for (i64 j = 0; j < n; ++j)
+    for (i64 p = a.cp[j]; p < a.cp[j + 1]; ++p) {
+      i64 d = cur[a.ri[p]]++;
+      t.ri[d] = j;
+      t.x[d] = a.x[p];
+    }
+  return t;
+}
+
+// _factor_colptrs (multifrontal.jl:73-104), 0-based pointers.
+void factor_colptrs(const Symbolic& S, vector<i64>& Lp, vector<i64>& Up) {
+  i64 n = S.n, nsuper = (i64)S.sstart.size() - 1;
+  Lp.assign(n + 1, 0);
+  Up.assign(n + 1, 0);
+  vector<i64> ucount(n, 0);
+  for (i64 sk = 0; sk < nsuper; ++sk) {
+    i64 c1 = S.sstart[sk], c2 = S.sstart[sk + 1] - 1, np = c2 - c1 + 1;
+    i64 nu = S.cs_ptr[c2 + 1] - S.cs_ptr[c2];
+    for (i64 j = c1; j <= c2; ++j) {
+      Lp[j + 1] = 1 + (c2 - j) + nu;
+      ucount[j] += j - c1 + 1;
+    }
+    for (i64 t = 0; t < nu; ++t) ucount[S.cs_idx[S.cs_ptr[c2] + t]] += np;
+  }
+  for (i64 j = 0; j < n; ++j) Lp[j + 1] += Lp[j];
+  for (i64 j = 0; j < n; ++j) Up[j + 1] = Up[j] + ucount[j];
+}
+
+int numeric_mf(i64 n, const i64* cp, const i64* ri, const double* x, const Symbolic& S, bool check,
+               Factor& F) {
+  if (!g_dgetrf || !g_dtrsm || !g_dgemm) {
+    g_err = "BLAS not loaded (call orc_set_blas first)";
+    return -1;
+  }
+  F.n = n;
+  Csc V = permute_csc(n, cp, ri, x, S.qf);
+  Csc Vt = transpose_csc(V);
+  i64 nsuper = (i64)S.sstart.size() - 1;
+  vector<i64> loc(n, -1), prow(n);
+  for (i64 k = 0; k < n; ++k) prow[k] = k;
+  i64 maxnf = 0;
+  for (i64 sk = 0; sk < nsuper; ++sk) {
+    i64 c2 = S.sstart[sk + 1] - 1;
+    i64 nfk = (c2 + 1 - S.sstart[sk]) + (S.cs_ptr[c2 + 1] - S.cs_ptr[c2]);
+    maxnf = std::max(maxnf, nfk);
+  }
+  vector<double> Fbuf((size_t)std::max<i64>(maxnf * maxnf, 1));
+  vector<double> cbval((size_t)std::max<i64>(64, maxnf * maxnf));
+  i64 cbtop = 0;
+  vector<i64> cboff(nsuper, 0);
+  factor_colptrs(S, F.Lp, F.Up);
+  F.Li.resize(F.Lp[n]);
+  F.Lx.resize(F.Lp[n]);
+  F.Ui.resize(F.Up[n]);
+  F.Ux.resize(F.Up[n]);
+  vector<i64> Lcur(F.Lp.begin(), F.Lp.end() - 1), Ucur(F.Up.begin(), F.Up.end() - 1);
+  vector<i64> ipiv;
+  vector<i64> orig;
+  F.status = 0;
+
+  for (i64 sk = 0; sk < nsuper; ++sk) {
+    i64 c1 = S.sstart[sk], c2 = S.sstart[sk + 1] - 1, np = c2 - c1 + 1;
+    const i64* upd = S.cs_idx.data() + S.cs_ptr[c2];
+    i64 nu = S.cs_ptr[c2 + 1] - S.cs_ptr[c2];
+    i64 nf = np + nu;
+    i64 ld = nf;
+    for (i64 a = 0; a < np; ++a) loc[c1 + a] = a;
+    for (i64 t = 0; t < nu; ++t) loc[upd[t]] = np + t;
+    double* Fm = Fbuf.data();
+    std::fill(Fm, Fm + nf * nf, 0.0);
+#define FE(r, c) Fm[(r) + (c) * ld]
+    // assemble original entries (multifrontal.jl:217-231)
+    for (i64 a = 0; a < np; ++a) {
+      i64 j = c1 + a;
+      for (i64 p = V.cp[j]; p < V.cp[j + 1]; ++p) {
+        i64 i = V.ri[p];
+        if (i >= j && loc[i] != -1) FE(loc[i], a) += V.x[p];
+      }
+      for (i64 p = Vt.cp[j]; p < Vt.cp[j + 1]; ++p) {
+        i64 k = Vt.ri[p];
+        if (k > j && loc[k] != -1) FE(a, loc[k]) += Vt.x[p];
+      }
+    }
+    // extend-add children, last child first (multifrontal.jl:235-243)
+    for (i64 ci = S.ch_ptr[sk + 1] - 1; ci >= S.ch_ptr[sk]; --ci) {
+      i64 ck = S.ch_idx[ci];
+      i64 cl = S.sstart[ck + 1] - 1;
+      const i64* crows = S.cs_idx.data() + S.cs_ptr[cl];
+      i64 m = S.cs_ptr[cl + 1] - S.cs_ptr[cl];
+      if (m == 0) continue;
+      const double* cb = cbval.data() + cboff[ck];
+      for (i64 s = 0; s < m; ++s) {
+        i64 cs = loc[crows[s]];
+        for (i64 r = 0; r < m; ++r) FE(loc[crows[r]], cs) += cb[r + s * m];
+      }
+      cbtop = cboff[ck];
+    }
+    // getrf on the pivot block (multifrontal.jl:247-252)
+    ipiv.assign(std::max<i64>(np, 1), 0);
+    i64 info = 0;
+    g_dgetrf(&np, &np, Fm, &ld, ipiv.data(), &info);
+    if (check && info != 0) {
+      F.status = c1 + info;   // 1-based column, = c1 + info - 1 in 1-based c1
+      return 1;
+    }
+    if (nu > 0) {
+      for (i64 k = 0; k < np; ++k) {    // swap R12 rows (multifrontal.jl:256-263)
+        i64 pk = ipiv[k] - 1;
+        if (pk != k)
+          for (i64 col = 0; col < nu; ++col) std::swap(FE(k, np + col), FE(pk, np + col));
+      }
+      const double one = 1.0, mone = -1.0;
+      // L21 = A21 * U11^{-1}; U12 = L11^{-1} * A12; F22 -= L21 * U12
+      g_dtrsm("R", "U", "N", "N", &nu, &np, &one, Fm, &ld, &FE(np, 0), &ld, 1, 1, 1, 1);
+      g_dtrsm("L", "L", "N", "U", &np, &nu, &one, Fm, &ld, &FE(0, np), &ld, 1, 1, 1, 1);
+      g_dgemm("N", "N", &nu, &nu, &np, &mone, &FE(np, 0), &ld, &FE(0, np), &ld, &one, &FE(np, np), &ld,
+              1, 1);
+    }
+    // _pivot_rows (multifrontal.jl:363-375)
+    orig.resize(np);
+    for (i64 a = 0; a < np; ++a) orig[a] = c1 + a;
+    for (i64 k = 0; k < np; ++k) {
+      i64 pk = ipiv[k] - 1;
+      if (pk != k) std::swap(orig[k], orig[pk]);
+    }
+    for (i64 a = 0; a < np; ++a) prow[c1 + a] = orig[a];
+    // scatter L and U (multifrontal.jl:278-317)
+    for (i64 a = 0; a < np; ++a) {
+      i64 g = c1 + a;
+      i64 lp = Lcur[g];
+      F.Li[lp] = orig[a];
+      F.Lx[lp++] = 1.0;
+      for (i64 b = a + 1; b < np; ++b) {
+        F.Li[lp] = orig[b];
+        F.Lx[lp++] = FE(b, a);
+      }
+      for (i64 t = 0; t < nu; ++t) {
+        F.Li[lp] = upd[t];
+        F.Lx[lp++] = FE(np + t, a);
+      }
+      Lcur[g] = lp;
+      i64 up = Ucur[g];
+      for (i64 b = 0; b <= a; ++b) {
+        F.Ui[up] = c1 + b;
+        F.Ux[up++] = FE(b, a);
+      }
+      Ucur[g] = up;
+    }
+    for (i64 t = 0; t < nu; ++t) {
+      i64 J = upd[t];
+      i64 up = Ucur[J];
+      for (i64 a = 0; a < np; ++a) {
+        F.Ui[up] = c1 + a;
+        F.Ux[up++] = FE(a, np + t);
+      }
+      Ucur[J] = up;
+    }
+    // push the Schur block (multifrontal.jl:321-332)
+    if (nu > 0) {
+      if ((i64)cbval.size() < cbtop + nu * nu) cbval.resize(std::max(cbtop + nu * nu, 2 * (i64)cbval.size()));
+      cboff[sk] = cbtop;
+      for (i64 s = 0; s < nu; ++s)
+        for (i64 r = 0; r < nu; ++r) cbval[cbtop + s * nu + r] = FE(np + r, np + s);
+      cbtop += nu * nu;
+    }
+#undef FE
+    for (i64 a = 0; a < np; ++a) loc[c1 + a] = -1;
+    for (i64 t = 0; t < nu; ++t) loc[upd[t]] = -1;
+  }
+  // relabel L rows, permutations (multifrontal.jl:347-357)
+  vector<i64> rowfac(n);
+  for (i64 k = 0; k < n; ++k) rowfac[prow[k]] = k;
+  for (auto& r : F.Li) r = rowfac[r];
+  F.q = S.qf;
+  F.p.resize(n);
+  F.pinv.resize(n);
+  for (i64 k = 0; k < n; ++k) F.p[k] = S.qf[prow[k]];
+  for (i64 k = 0; k < n; ++k) F.pinv[F.p[k]] = k;
+  return 0;
+}
+
+// solve.jl:10-22 and 25-39
+void lsolve(const Factor& F, double* y) {
+  for (i64 j = 0; j < F.n; ++j) {
+    double yj = y[j];
+    for (i64 p = F.Lp[j] + 1; p < F.Lp[j + 1]; ++p) y[F.Li[p]] -= F.Lx[p] * yj;
+  }
+}
+void usolve(const Factor& F, double* y) {
+  for (i64 j = F.n - 1; j >= 0; --j) {
+    i64 pd = F.Up[j + 1] - 1;
+    double yj = y[j] / F.Ux[pd];
+    y[j] = yj;
+    for (i64 p = F.Up[j]; p < pd; ++p) y[F.Ui[p]] -= F.Ux[p] * yj;
+  }
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI (ctypes).  All index arrays are 1-based int64.
+// ===========================================================================
+extern "C" {
+
+const char* orc_last_error() { return g_err.c_str(); }
+
+int orc_set_blas(const char* path) {
+  void* h = dlopen(path, RTLD_NOW | RTLD_LOCAL);
+  if (!h) {
+    g_err = dlerror();
+    return -1;
+  }
+  g_dgetrf = (dgetrf_fn)dlsym(h, "scipy_dgetrf_64_");
+  g_dtrsm = (dtrsm_fn)dlsym(h, "scipy_dtrsm_64_");
+  g_dgemm = (dgemm_fn)dlsym(h, "scipy_dgemm_64_");
+  g_setthreads = (setthreads_fn)dlsym(h, "scipy_openblas_set_num_threads64_");
+  g_getthreads = (getthreads_fn)dlsym(h, "scipy_openblas_get_num_threads64_");
+  if (!g_dgetrf || !g_dtrsm || !g_dgemm) {
+    g_err = "missing BLAS symbols";
+    return -2;
+  }
+  return 0;
+}
+
+int orc_blas_threads(int k) {
+  if (k > 0 && g_setthreads) g_setthreads(k);
+  return g_getthreads ? g_getthreads() : -1;
+}
+
+// scaling.jl:92-115.  kind: 0 NONE, 1 SUM, 2 MAX.
+void orc_row_scaling(i64 n, const i64* colptr, const i64* rowval, const double* nzval, int kind, double* Rs) {
+  for (i64 i = 0; i < n; ++i) Rs[i] = 1.0;
+  if (kind == 0) return;
+  vector<double> acc(n, 0.0);
+  i64 nz = colptr[n] - 1;
+  if (kind == 1) {
+    for (i64 p = 0; p < nz; ++p) acc[rowval[p] - 1] += std::fabs(nzval[p]);
+  } else {
+    for (i64 p = 0; p < nz; ++p) {
+      i64 i = rowval[p] - 1;
+      double v = std::fabs(nzval[p]);
+      acc[i] = v > acc[i] ? v : acc[i];
+    }
+  }
+  for (i64 i = 0; i < n; ++i) Rs[i] = acc[i] > 0 ? 1.0 / acc[i] : 1.0;
+}
+
+static void to0(i64 n, const i64* cp1, const i64* ri1, vector<i64>& cp, vector<i64>& ri) {
+  cp.resize(n + 1);
+  for (i64 j = 0; j <= n; ++j) cp[j] = cp1[j] - 1;
+  ri.resize(cp[n]);
+  for (i64 p = 0; p < cp[n]; ++p) ri[p] = ri1[p] - 1;
+}
+
+int orc_amd_order_sym(i64 n, const i64* colptr, const i64* rowval, double dense, i64* perm) {
+  vector<i64> cp, ri;
+  to0(n, colptr, rowval, cp, ri);
+  vector<i64> p = amd_order_sym0(n, cp.data(), ri.data(), dense);
+  for (i64 k = 0; k < n; ++k) perm[k] = p[k] + 1;
+  return 0;
+}
+
+int orc_colamd_order(i64 m, i64 n, const i64* colptr, const i64* rowval, double dense, i64* perm) {
+  vector<i64> cp, ri;
+  to0(n, colptr, rowval, cp, ri);
+  vector<i64> p = colamd_order0(m, n, cp.data(), ri.data(), dense);
+  for (i64 k = 0; k < n; ++k) perm[k] = p[k] + 1;
+  return 0;
+}
+
+// ---- symbolic object ------------------------------------------------------
+void* orc_symbolic(i64 n, const i64* colptr, const i64* rowval, const i64* q1) {
+  vector<i64> cp, ri;
+  to0(n, colptr, rowval, cp, ri);
+  vector<i64> q;
+  if (q1) {
+    q.resize(n);
+    for (i64 k = 0; k < n; ++k) q[k] = q1[k] - 1;
+  }
+  return new Symbolic(symbolic_mf0(n, cp.data(), ri.data(), q1 ? &q : nullptr));
+}
+void orc_symbolic_free(void* h) { delete (Symbolic*)h; }
+// sizes: [n, nsuper, nnz(colstruct), nnz(childsupers)]
+void orc_symbolic_sizes(void* h, i64* out) {
+  Symbolic* S = (Symbolic*)h;
+  out[0] = S->n;
+  out[1] = (i64)S->sstart.size() - 1;
+  out[2] = S->cs_ptr.empty() ? 0 : S->cs_ptr[S->n];
+  out[3] = (i64)S->ch_idx.size();
+}
+// 1-based copies: qf(n), parent(n; 0 = root), cs_ptr(n+1), cs_idx, sstart(nsuper+1),
+// ch_ptr(nsuper+1), ch_idx.
+void orc_symbolic_get(void* h, i64* qf, i64* parent, i64* cs_ptr, i64* cs_idx, i64* sstart, i64* ch_ptr,
+                      i64* ch_idx) {
+  Symbolic* S = (Symbolic*)h;
+  i64 n = S->n, ns = (i64)S->sstart.size() - 1;
+  for (i64 k = 0; k < n; ++k) {
+    qf[k] = S->qf[k] + 1;
+    parent[k] = S->parent[k] + 1;
+  }
+  for (i64 k = 0; k <= n; ++k) cs_ptr[k] = S->cs_ptr[k] + 1;
+  for (size_t k = 0; k < S->cs_idx.size(); ++k) cs_idx[k] = S->cs_idx[k] + 1;
+  for (i64 k = 0; k <= ns; ++k) {
+    sstart[k] = S->sstart[k] + 1;
+    ch_ptr[k] = S->ch_ptr[k] + 1;
+  }
+  for (size_t k = 0; k < S->ch_idx.size(); ++k) ch_idx[k] = S->ch_idx[k] + 1;
+}
+
+// ---- numeric factor object --------------------------------------------------
+// Factor V = A (already scaled by the caller, as splu does) with optional
+// caller order q1 (1-based, may be NULL).  Returns a handle; *status = 0 on
+// success, k > 0 when check is set and the pivot at column k is zero, < 0 on
+// error.
+void* orc_multifrontal_lu(i64 n, const i64* colptr, const i64* rowval, const double* nzval, const i64* q1,
+                          int check, i64* status) {
+  vector<i64> cp, ri;
+  to0(n, colptr, rowval, cp, ri);
+  vector<i64> q;
+  if (q1) {
+    q.resize(n);
+    for (i64 k = 0; k < n; ++k) q[k] = q1[k] - 1;
+  }
+  Symbolic S = symbolic_mf0(n, cp.data(), ri.data(), q1 ? &q : nullptr);
+  Factor* F = new Factor();
+  int rc = numeric_mf(n, cp.data(), ri.data(), nzval, S, check != 0, *F);
+  *status = rc < 0 ? rc : F->status;
+  return F;
+}
+// Numeric only, with a precomputed symbolic object (for timing the numeric
+// phase separately from the symbolic one).
+void* orc_numeric(void* sym, const double* nzval, const i64* colptr, const i64* rowval, int check, i64* status) {
+  Symbolic* S = (Symbolic*)sym;
+  vector<i64> cp, ri;
+  to0(S->n, colptr, rowval, cp, ri);
+  Factor* F = new Factor();
+  int rc = numeric_mf(S->n, cp.data(), ri.data(), nzval, *S, check != 0, *F);
+  *status = rc < 0 ? rc : F->status;
+  return F;
+}
+void orc_factor_free(void* h) { delete (Factor*)h; }
+void orc_factor_sizes(void* h, i64* out) {
+  Factor* F = (Factor*)h;
+  out[0] = F->n;
+  out[1] = F->Lp.empty() ? 0 : F->Lp[F->n];
+  out[2] = F->Up.empty() ? 0 : F->Up[F->n];
+}
+void orc_factor_get(void* h, i64* Lp, i64* Li, double* Lx, i64* Up, i64* Ui, double* Ux, i64* p, i64* q,
+                    i64* pinv) {
+  Factor* F = (Factor*)h;
+  i64 n = F->n;
+  for (i64 k = 0; k <= n; ++k) {
+    Lp[k] = F->Lp[k] + 1;
+    Up[k] = F->Up[k] + 1;
+  }
+  for (size_t k = 0; k < F->Li.size(); ++k) {
+    Li[k] = F->Li[k] + 1;
+    Lx[k] = F->Lx[k];
+  }
+  for (size_t k = 0; k < F->Ui.size(); ++k) {
+    Ui[k] = F->Ui[k] + 1;
+    Ux[k] = F->Ux[k];
+  }
+  for (i64 k = 0; k < n; ++k) {
+    p[k] = F->p[k] + 1;
+    q[k] = F->q[k] + 1;
+    pinv[k] = F->pinv[k] + 1;
+  }
+}
+
+// _solve_factor (interface.jl:123-138) with Rs (NULL = no scaling, as the raw
+// GPLUFactorization solve at solve.jl:66-77).
+void orc_solve_factor(void* h, const double* Rs, const double* b, double* x) {
+  Factor* F = (Factor*)h;
+  i64 n = F->n;
+  vector<double> c(n);
+  for (i64 k = 0; k < n; ++k) c[k] = Rs ? Rs[F->p[k]] * b[F->p[k]] : b[F->p[k]];
+  lsolve(*F, c.data());
+  usolve(*F, c.data());
+  for (i64 k = 0; k < n; ++k) x[F->q[k]] = c[k];
+}
+
+// solve(F::PureLU, b; refine) (interface.jl:170-177).  A is the UNSCALED
+// original matrix (1-based CSC), nrhs columns of b / x stored with leading
+// dimension n.
+void orc_solve(void* h, const double* Rs, i64 n, const i64* colptr, const i64* rowval, const double* nzval,
+               i64 nrhs, const double* B, double* X, int refine) {
+  vector<double> r(n), d(n);
+  for (i64 c = 0; c < nrhs; ++c) {
+    const double* b = B + c * n;
+    double* x = X + c * n;
+    orc_solve_factor(h, Rs, b, x);
+    for (int it = 0; it < refine; ++it) {
+      // r = b - A*x (column-oriented SpMV as SparseArrays does)
+      std::vector<double> ax(n, 0.0);
+      for (i64 j = 0; j < n; ++j) {
+        double xj = x[j];
+        for (i64 p = colptr[j] - 1; p < colptr[j + 1] - 1; ++p) ax[rowval[p] - 1] += nzval[p] * xj;
+      }
+      for (i64 i = 0; i < n; ++i) r[i] = b[i] - ax[i];
+      orc_solve_factor(h, Rs, r.data(), d.data());
+      for (i64 i = 0; i < n; ++i) x[i] = x[i] + d[i];
+    }
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,303 @@
+"""ctypes front end of the CPU oracle (``oracle/mf_oracle.cpp``).
+
+TEST INFRASTRUCTURE ONLY.  Tests, ``__graft_entry__.smoke()`` and the CPU
+baseline leg of ``bench.py`` use this module as the checker / reference
+timing.  The shipped package never imports it.
+
+Every function mirrors one piece of the reference (PureUMFPACK.jl) and keeps
+its 1-based Int64 index convention:
+
+* ``row_scaling``        src/scaling.jl:92-115
+* ``amd_order_sym``      src/amd.jl:141-148
+* ``colamd_order``       src/amd.jl:183-188
+* ``symbolic_mf``        src/symbolic.jl:211-226
+* ``multifrontal_lu``    src/multifrontal.jl:146-358
+* ``solve``              src/interface.jl:170-177 (with ``_solve_factor`` :123-138)
+"""
+
+from __future__ import annotations
+
+import ctypes
+import glob
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libmforacle.so")
+_lib = None
+
+SCALE_NONE, SCALE_SUM, SCALE_MAX = 0, 1, 2
+
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_f64p = ctypes.POINTER(ctypes.c_double)
+
+
+def openblas_path() -> str:
+    """Path of numpy's bundled ILP64 OpenBLAS (exports scipy_dgetrf_64_ etc.)."""
+    import numpy
+
+    libs = os.path.join(os.path.dirname(os.path.dirname(numpy.__file__)), "numpy.libs")
+    hits = sorted(glob.glob(os.path.join(libs, "libscipy_openblas64_*.so")))
+    if not hits:
+        raise RuntimeError("numpy's bundled OpenBLAS (libscipy_openblas64_) not found")
+    return hits[0]
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(
+            os.path.join(_HERE, "mf_oracle.cpp")
+        ):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.orc_last_error.restype = ctypes.c_char_p
+        L.orc_set_blas.argtypes = [ctypes.c_char_p]
+        L.orc_blas_threads.argtypes = [ctypes.c_int]
+        L.orc_symbolic.restype = ctypes.c_void_p
+        L.orc_symbolic.argtypes = [ctypes.c_int64, _i64p, _i64p, _i64p]
+        L.orc_symbolic_free.argtypes = [ctypes.c_void_p]
+        L.orc_symbolic_sizes.argtypes = [ctypes.c_void_p, _i64p]
+        L.orc_symbolic_get.argtypes = [ctypes.c_void_p] + [_i64p] * 7
+        L.orc_multifrontal_lu.restype = ctypes.c_void_p
+        L.orc_multifrontal_lu.argtypes = [ctypes.c_int64, _i64p, _i64p, _f64p, _i64p, ctypes.c_int, _i64p]
+        L.orc_numeric.restype = ctypes.c_void_p
+        L.orc_numeric.argtypes = [ctypes.c_void_p, _f64p, _i64p, _i64p, ctypes.c_int, _i64p]
+        L.orc_factor_free.argtypes = [ctypes.c_void_p]
+        L.orc_factor_sizes.argtypes = [ctypes.c_void_p, _i64p]
+        L.orc_factor_get.argtypes = [ctypes.c_void_p, _i64p, _i64p, _f64p, _i64p, _i64p, _f64p, _i64p, _i64p, _i64p]
+        L.orc_solve_factor.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p]
+        L.orc_solve.argtypes = [ctypes.c_void_p, _f64p, ctypes.c_int64, _i64p, _i64p, _f64p, ctypes.c_int64,
+                                _f64p, _f64p, ctypes.c_int]
+        L.orc_row_scaling.argtypes = [ctypes.c_int64, _i64p, _i64p, _f64p, ctypes.c_int, _f64p]
+        L.orc_amd_order_sym.argtypes = [ctypes.c_int64, _i64p, _i64p, ctypes.c_double, _i64p]
+        L.orc_colamd_order.argtypes = [ctypes.c_int64, ctypes.c_int64, _i64p, _i64p, ctypes.c_double, _i64p]
+        rc = L.orc_set_blas(openblas_path().encode())
+        if rc != 0:
+            raise RuntimeError("oracle: cannot load OpenBLAS: " + L.orc_last_error().decode())
+        _lib = L
+    return _lib
+
+
+def _p(a, ty=_i64p):
+    return a.ctypes.data_as(ty) if a is not None else None
+
+
+def _i(a):
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+def _f(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def blas_threads(k: int = 0) -> int:
+    """Set (k > 0) and return OpenBLAS's thread count."""
+    return int(lib().orc_blas_threads(int(k)))
+
+
+def row_scaling(A, kind: int) -> np.ndarray:
+    n = A.m
+    Rs = np.empty(n)
+    lib().orc_row_scaling(n, _p(_i(A.colptr)), _p(_i(A.rowval)), _p(_f(A.nzval), _f64p), int(kind), _p(Rs, _f64p))
+    return Rs
+
+
+def apply_row_scaling(A, Rs):
+    """Diagonal(Rs) * A with the same pattern (scaling.jl:118-126)."""
+    B = A.copy()
+    B.nzval = B.nzval * Rs[B.rowval - 1]
+    return B
+
+
+def amd_order_sym(A, dense: float = 10.0) -> np.ndarray:
+    n = A.n
+    perm = np.empty(n, dtype=np.int64)
+    lib().orc_amd_order_sym(n, _p(_i(A.colptr)), _p(_i(A.rowval)), float(dense), _p(perm))
+    return perm
+
+
+def colamd_order(A, dense: float = 10.0) -> np.ndarray:
+    n = A.n
+    perm = np.empty(n, dtype=np.int64)
+    lib().orc_colamd_order(A.m, n, _p(_i(A.colptr)), _p(_i(A.rowval)), float(dense), _p(perm))
+    return perm
+
+
+@dataclass
+class Symbolic:
+    """SymbolicMF (symbolic.jl:203-209), flattened; all indices 1-based."""
+
+    qf: np.ndarray
+    parent: np.ndarray          # 0 = root
+    cs_ptr: np.ndarray          # colstruct[j] = cs_idx[cs_ptr[j]-1 : cs_ptr[j+1]-1]
+    cs_idx: np.ndarray
+    sstart: np.ndarray
+    ch_ptr: np.ndarray
+    ch_idx: np.ndarray
+    handle: int = 0
+
+    def colstruct(self, j: int) -> np.ndarray:   # j 1-based
+        return self.cs_idx[self.cs_ptr[j - 1] - 1 : self.cs_ptr[j] - 1]
+
+    def childsupers(self, s: int) -> np.ndarray:  # s 1-based
+        return self.ch_idx[self.ch_ptr[s - 1] - 1 : self.ch_ptr[s] - 1]
+
+    @property
+    def nsuper(self) -> int:
+        return len(self.sstart) - 1
+
+    def __del__(self):
+        if self.handle and _lib is not None:
+            _lib.orc_symbolic_free(ctypes.c_void_p(self.handle))
+            self.handle = 0
+
+
+def predicted_fill(S: Symbolic) -> int:
+    """symbolic.jl:230-237."""
+    n = len(S.qf)
+    return 2 * (n + int(S.cs_ptr[-1] - 1))
+
+
+def symbolic_mf(A, q=None) -> Symbolic:
+    n = A.n
+    qa = _i(q) if q is not None else None
+    h = lib().orc_symbolic(n, _p(_i(A.colptr)), _p(_i(A.rowval)), _p(qa))
+    sz = np.empty(4, dtype=np.int64)
+    lib().orc_symbolic_sizes(ctypes.c_void_p(h), _p(sz))
+    ns, ncs, nch = int(sz[1]), int(sz[2]), int(sz[3])
+    qf = np.empty(n, np.int64)
+    parent = np.empty(n, np.int64)
+    cs_ptr = np.empty(n + 1, np.int64)
+    cs_idx = np.empty(ncs, np.int64)
+    sstart = np.empty(ns + 1, np.int64)
+    ch_ptr = np.empty(ns + 1, np.int64)
+    ch_idx = np.empty(nch, np.int64)
+    lib().orc_symbolic_get(ctypes.c_void_p(h), _p(qf), _p(parent), _p(cs_ptr), _p(cs_idx), _p(sstart), _p(ch_ptr),
+                           _p(ch_idx))
+    return Symbolic(qf, parent, cs_ptr, cs_idx, sstart, ch_ptr, ch_idx, handle=h)
+
+
+class SingularException(Exception):
+    """Julia's LinearAlgebra.SingularException(info)."""
+
+    def __init__(self, info: int):
+        super().__init__(f"SingularException({info})")
+        self.info = info
+
+
+@dataclass
+class Factor:
+    """GPLUFactorization (gplu.jl:45-51) from the oracle; 1-based."""
+
+    Lcolptr: np.ndarray
+    Lrowval: np.ndarray
+    Lnzval: np.ndarray
+    Ucolptr: np.ndarray
+    Urowval: np.ndarray
+    Unzval: np.ndarray
+    p: np.ndarray
+    q: np.ndarray
+    pinv: np.ndarray
+    handle: int = 0
+
+    def __del__(self):
+        if self.handle and _lib is not None:
+            _lib.orc_factor_free(ctypes.c_void_p(self.handle))
+            self.handle = 0
+
+
+def _extract(h) -> Factor:
+    sz = np.empty(3, dtype=np.int64)
+    lib().orc_factor_sizes(ctypes.c_void_p(h), _p(sz))
+    n, nl, nu = (int(v) for v in sz)
+    Lp = np.empty(n + 1, np.int64)
+    Up = np.empty(n + 1, np.int64)
+    Li = np.empty(nl, np.int64)
+    Ui = np.empty(nu, np.int64)
+    Lx = np.empty(nl)
+    Ux = np.empty(nu)
+    p = np.empty(n, np.int64)
+    q = np.empty(n, np.int64)
+    pinv = np.empty(n, np.int64)
+    lib().orc_factor_get(ctypes.c_void_p(h), _p(Lp), _p(Li), _p(Lx, _f64p), _p(Up), _p(Ui), _p(Ux, _f64p), _p(p),
+                         _p(q), _p(pinv))
+    return Factor(Lp, Li, Lx, Up, Ui, Ux, p, q, pinv, handle=h)
+
+
+def multifrontal_lu(A, q=None, check: bool = True) -> Factor:
+    """multifrontal.jl:146-358 on the matrix as given (no scaling)."""
+    n = A.n
+    st = np.zeros(1, np.int64)
+    qa = _i(q) if q is not None else None
+    h = lib().orc_multifrontal_lu(n, _p(_i(A.colptr)), _p(_i(A.rowval)), _p(_f(A.nzval), _f64p), _p(qa),
+                                  int(check), _p(st))
+    if st[0] < 0:
+        lib().orc_factor_free(ctypes.c_void_p(h))
+        raise RuntimeError("oracle: " + lib().orc_last_error().decode())
+    if st[0] > 0:
+        lib().orc_factor_free(ctypes.c_void_p(h))
+        raise SingularException(int(st[0]))
+    return _extract(h)
+
+
+def numeric(S: Symbolic, A, check: bool = True) -> Factor:
+    """Numeric phase only, on a precomputed symbolic object."""
+    st = np.zeros(1, np.int64)
+    h = lib().orc_numeric(ctypes.c_void_p(S.handle), _p(_f(A.nzval), _f64p), _p(_i(A.colptr)), _p(_i(A.rowval)),
+                          int(check), _p(st))
+    if st[0] != 0:
+        lib().orc_factor_free(ctypes.c_void_p(h))
+        raise SingularException(int(st[0])) if st[0] > 0 else RuntimeError("oracle numeric failed")
+    return _extract(h)
+
+
+@dataclass
+class PureLU:
+    """interface.jl:38-48: (Rs .* A)[p, q] == L * U."""
+
+    F: Factor
+    Rs: np.ndarray
+    A: object
+
+
+def splu(A, scale: int = SCALE_SUM, check: bool = True, q=None) -> PureLU:
+    """splu(A; method=:multifrontal, scale) (interface.jl:93-105).
+
+    ``q`` (not part of ``splu``) routes a caller order through
+    ``multifrontal_lu(As; q)`` as ``multifrontal.jl:152`` allows.
+    """
+    if A.m != A.n:
+        raise ValueError("DimensionMismatch: splu requires a square matrix")
+    Rs = row_scaling(A, scale)
+    As = A if scale == SCALE_NONE else apply_row_scaling(A, Rs)
+    F = multifrontal_lu(As, q=q, check=check)
+    return PureLU(F, Rs, A)
+
+
+def solve(F: PureLU, b: np.ndarray, refine: int = 0) -> np.ndarray:
+    """solve(F::PureLU, b; refine) (interface.jl:170-177); b may be n x k."""
+    A = F.A
+    B = np.asfortranarray(b, dtype=np.float64)
+    nrhs = 1 if B.ndim == 1 else B.shape[1]
+    X = np.empty_like(B)
+    lib().orc_solve(ctypes.c_void_p(F.F.handle), _p(_f(F.Rs), _f64p), A.n, _p(_i(A.colptr)), _p(_i(A.rowval)),
+                    _p(_f(A.nzval), _f64p), nrhs, _p(B, _f64p), _p(X, _f64p), int(refine))
+    return X
+
+
+def solve_raw(F: Factor, b: np.ndarray) -> np.ndarray:
+    """solve(F::GPLUFactorization, b) (solve.jl:66-77)."""
+    x = np.empty(len(b))
+    bb = _f(b)
+    lib().orc_solve_factor(ctypes.c_void_p(F.handle), None, _p(bb, _f64p), _p(x, _f64p))
+    return x
