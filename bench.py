@@ -1,0 +1,425 @@
+"""Benchmark: 64^3 Poisson multifrontal factor + solve on B200 (libmfgpu).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload poisson3d-64|poisson3d-48|poisson2d-100] [--forms fp64,mixed]
+
+One step = numeric multifrontal factorization of A = poisson3d(64) (SCALE_SUM
+row scaling, AMD order) followed by solve(F, B; refine) for 256 N(0,1)
+right-hand sides (seed 4), with the refinement count each form needs to bring
+the normwise backward error of every right-hand side to <= 1e-14.  The
+pattern analysis (ordering + symbolic, done once per sparsity pattern) is
+timed separately and reported as `analyze_s`.
+
+`value` is the step time (seconds, lower is better) of the mixed form when it
+reaches the accuracy target, else of the FP64 form; both forms are reported
+under `forms`.  Inputs (A's values, Rs, B) are resident in HBM when the timed
+region starts; `e2e` repeats the step through the C ABI with pinned host
+buffers, host<->device copies included.  `--impl reference` times the CPU
+oracle (the reference's algorithm restated in C++ over OpenBLAS) on the same
+workload, on the host cores.
+
+With N > 1 (torchrun), every rank factors and solves its own copy of the
+system (replicas: one sparse system does not shard), the step time is the max
+over ranks, and value = that time / N (seconds per system, whole job).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "pureumfpack.jl_b200")]
+
+TARGET_ETA = 1e-14
+MAX_REFINE = 8
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="poisson3d-64")
+    ap.add_argument("--nrhs", type=int, default=256)
+    ap.add_argument("--forms", default="fp64,mixed")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def make_workload(name: str, nrhs: int):
+    from pureumfpack import matrices as M
+
+    kind, k = name.rsplit("-", 1)
+    k = int(k)
+    if kind == "poisson3d":
+        A = M.poisson3d(k)
+        seed = 4
+    elif kind == "poisson3d_shift":
+        A = M.poisson3d(k).add_diagonal(1e-3)
+        seed = 1
+    elif kind == "poisson2d":
+        A = M.poisson2d(k)
+        seed = 0
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    B = M.rhs(A.n, seed=seed, nrhs=nrhs)
+    if B.ndim == 1:
+        B = B.reshape(-1, 1)
+    return A, np.asfortranarray(B)
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def fp_peak_tflops(torch, dtype, device) -> float:
+    """In-run cuBLAS GEMM throughput (TFLOP/s) as the roofline denominator for
+    a precision MEASURED_PEAKS.json does not cover (FP64, FP32 SIMT)."""
+    n = 8192 if dtype == torch.float64 else 8192
+    a = torch.randn(n, n, dtype=dtype, device=device)
+    b = torch.randn(n, n, dtype=dtype, device=device)
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline(A, B, refine: int, sample_rhs: int = 4):
+    """The oracle (C++ restatement of the reference over OpenBLAS, all host
+    threads): symbolic + numeric multifrontal_lu of the full matrix, then
+    solve(F, b; refine) for `sample_rhs` right-hand sides, scaled to the full
+    RHS count.  Returns (seconds per step, details)."""
+    from oracle import oracle as O
+
+    cores = os.cpu_count() or 1
+    O.blas_threads(cores)
+    t0 = time.perf_counter()
+    S = O.symbolic_mf(A)
+    t1 = time.perf_counter()
+    Rs = O.row_scaling(A, O.SCALE_SUM)
+    As = O.apply_row_scaling(A, Rs)
+    Fo = O.numeric(S, As, check=False)
+    t2 = time.perf_counter()
+    F = O.PureLU(Fo, Rs, A)
+    nrhs = B.shape[1]
+    k = min(sample_rhs, nrhs)
+    t3 = time.perf_counter()
+    O.solve(F, np.asfortranarray(B[:, :k]), refine=refine)
+    t4 = time.perf_counter()
+    numeric = t2 - t1
+    solve_full = (t4 - t3) * nrhs / k
+    return numeric + solve_full, {
+        "symbolic_s": t1 - t0, "numeric_s": numeric, "solve_s_per_rhs": (t4 - t3) / k, "cores": cores,
+        "sample": f"full {A.n}-unknown numeric factorization (OpenBLAS, {cores} threads) + solve(refine={refine}) "
+                  f"of {k} of {nrhs} right-hand sides, scaled x{nrhs / k:g}; symbolic phase reported separately",
+    }
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    A, B = make_workload(args.workload, args.nrhs)
+    times, det = [], None
+    for i in range(max(1, min(args.warmup, 1)) + args.steps):
+        t, det = cpu_baseline(A, B, refine=1)
+        if i >= max(1, min(args.warmup, 1)):
+            times.append(t)
+    v = float(np.mean(times))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args, A),
+        "cpu_baseline": {"value": v, "unit": "s", "cores": det["cores"], "kind": "port", "sample": det["sample"],
+                         "symbolic_s": det["symbolic_s"]},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+METRIC = "64^3 Poisson factor+solve s at bwd err <=1e-14: mixed vs FP64 on 1 B200; %roofline"
+
+
+def workload_config(args, A):
+    return {"workload": f"{args.workload} n={A.n} nnz={A.nnz()} nrhs={args.nrhs} AMD SCALE_SUM, numeric factor + "
+                        f"solve(refine) to normwise backward error <= 1e-14",
+            "nrhs": args.nrhs, "l2": "working set (fronts) larger than L2; no explicit flush",
+            "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "1 GPU"}
+
+
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+
+    from pureumfpack import GpuContext, row_scaling, symbolic_mf, PRECISION_FP64, PRECISION_MIXED
+
+    A, B = make_workload(args.workload, args.nrhs)
+    n, R = A.n, B.shape[1]
+    t0 = time.perf_counter()
+    S = symbolic_mf(A)
+    Rs = row_scaling(A, 1)
+    t_sym = time.perf_counter() - t0
+
+    stream = torch.cuda.current_stream(dev)
+    d_ax = torch.from_numpy(A.nzval).to(dev)
+    d_rs = torch.from_numpy(Rs).to(dev)
+    d_b = torch.from_numpy(np.asfortranarray(B).ravel(order="F")).to(dev)
+    d_x = torch.empty(n * R, dtype=torch.float64, device=dev)
+
+    forms = {}
+    peaks = measured_peaks()
+    for form in [f for f in args.forms.split(",") if f]:
+        prec = PRECISION_MIXED if form == "mixed" else PRECISION_FP64
+        ctx = GpuContext(device=local, precision=prec)
+        ctx.set_stream(stream.cuda_stream)
+        t0 = time.perf_counter()
+        ctx.analyze(A, S)
+        t_an = time.perf_counter() - t0
+
+        def step(refine):
+            st = ctx.factor_device(d_ax.data_ptr(), d_rs.data_ptr(), True)
+            if st != 0:
+                raise RuntimeError(f"singular pivot at column {st}")
+            ctx.solve_device(R, d_b.data_ptr(), n, d_x.data_ptr(), n, refine)
+
+        # refinement count that reaches the accuracy target on every rhs
+        refine, eta = 0, None
+        for refine in range(0, MAX_REFINE + 1):
+            step(refine)
+            eta = ctx.backward_error_device(R, d_b.data_ptr(), n, d_x.data_ptr(), n)
+            if eta <= TARGET_ETA:
+                break
+        for _ in range(args.warmup):
+            step(refine)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local)
+        clocks.start()
+        ctx.set_profiling(False)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step(refine)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        ms = e0.elapsed_time(e1) / args.steps
+        launches = ctx.stats()["launches"]
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+        eta = ctx.backward_error_device(R, d_b.data_ptr(), n, d_x.data_ptr(), n)
+        # profiled pass (not timed): per-kernel-class device times
+        ctx.set_profiling(True)
+        step(refine)
+        torch.cuda.synchronize()
+        st = ctx.stats()
+        ctx.set_profiling(False)
+        # end to end through the C ABI with pinned host buffers
+        e2e = None
+        if not args.no_e2e:
+            h_ax = torch.from_numpy(A.nzval).pin_memory()
+            h_rs = torch.from_numpy(Rs).pin_memory()
+            h_b = torch.from_numpy(np.asfortranarray(B).ravel(order="F")).pin_memory()
+            h_x = torch.empty(n * R, dtype=torch.float64).pin_memory()
+            lib = ctx._lib
+            import ctypes
+
+            def e2e_step():
+                rc = lib.mfgpu_factor(ctx._h, ctypes.cast(h_ax.data_ptr(), ctypes.POINTER(ctypes.c_double)),
+                                      ctypes.cast(h_rs.data_ptr(), ctypes.POINTER(ctypes.c_double)), 1)
+                if rc != 0:
+                    raise RuntimeError(f"mfgpu_factor -> {rc}")
+                rc = lib.mfgpu_solve(ctx._h, R, ctypes.cast(h_b.data_ptr(), ctypes.POINTER(ctypes.c_double)), n,
+                                     ctypes.cast(h_x.data_ptr(), ctypes.POINTER(ctypes.c_double)), n, refine)
+                if rc != 0:
+                    raise RuntimeError(f"mfgpu_solve -> {rc}")
+
+            e2e_step()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                e2e_step()
+            torch.cuda.synchronize()
+            e2e_s = (time.perf_counter() - t0) / args.steps
+            if world > 1:
+                t = torch.tensor([e2e_s], device=dev)
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                e2e_s = float(t.item())
+            e2e = {"value": e2e_s / world, "unit": "s", "h2d_bytes_per_step": 8 * (A.nnz() + n + n * R),
+                   "d2h_bytes_per_step": 8 * n * R}
+        forms[form] = {"ms_per_step": ms, "refine": refine, "eta": eta, "analyze_s": t_an + t_sym,
+                       "stats": st, "clocks": clk, "launches_timed": launches, "e2e": e2e}
+        del ctx
+        torch.cuda.empty_cache()
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+
+    primary = "mixed" if ("mixed" in forms and forms["mixed"]["eta"] <= TARGET_ETA) else "fp64"
+    if primary not in forms:
+        primary = next(iter(forms))
+    P = forms[primary]
+    kern = P["stats"]["kernels"]
+    dom = max(kern, key=lambda k: kern[k]["ms"])
+    kd = kern[dom]
+    per_launch_ms = kd["ms"] / max(kd["launches"], 1)
+    if dom.startswith("gemm"):
+        if primary == "fp64":
+            peak = fp_peak_tflops(torch, torch.float64, dev)
+            peak_src = "in-run cuBLAS DGEMM 8192^3 (FP64 peak is not in MEASURED_PEAKS.json)"
+        else:
+            peak = fp_peak_tflops(torch, torch.float32, dev)
+            peak_src = "in-run cuBLAS SGEMM 8192^3, TF32 off (FP32 SIMT peak)"
+        achieved = kd["flops"] / (kd["ms"] * 1e-3) / 1e12
+        roof = {"bound": "tensor" if primary == "fp64" else "compute", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": peak_src}
+    else:
+        peak = peaks.get("hbm_gbs", 6650.0)
+        achieved = kd["bytes"] / (kd["ms"] * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback"}
+    roof.update({"kernel": dom, "launches": kd["launches"], "avg_launch_ms": per_launch_ms,
+                 "traffic": None, "note": "achieved = algorithmic work of the kernel class / its CUDA-event time "
+                                          "over one profiled step"})
+
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            v, det = cpu_baseline(A, B, refine=forms.get("fp64", P)["refine"])
+            cpu = {"value": v, "unit": "s", "cores": det["cores"], "kind": "port", "sample": det["sample"],
+                   "symbolic_s": det["symbolic_s"], "numeric_s": det["numeric_s"]}
+        except Exception as e:  # the baseline must not kill the GPU number
+            cpu = {"value": None, "error": str(e)}
+
+    value = P["ms_per_step"] / 1e3 / world
+    line = {
+        "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": P["ms_per_step"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if primary == "fp64" else "f32+f64", "data": "synthetic", "form": primary,
+        "config": workload_config(args, A),
+        "forms": {k: {"s_per_step": f["ms_per_step"] / 1e3, "refine": f["refine"], "bwd_err": f["eta"],
+                      "factor_ms": f["stats"]["factor_ms"], "solve_ms": f["stats"]["solve_ms"],
+                      "analyze_s": f["analyze_s"], "e2e_s": f["e2e"]["value"] if f["e2e"] else None,
+                      "kernels_ms": {kk: round(vv["ms"], 3) for kk, vv in f["stats"]["kernels"].items()}}
+                  for k, f in forms.items()},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": P["e2e"],
+        "gpu_launches": P["launches_timed"],
+        "clocks": P["clocks"],
+        "stats": {k: P["stats"][k] for k in ("n", "nsuper", "levels", "nnz_l", "nnz_u", "max_front", "flops",
+                                             "front_elems")},
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

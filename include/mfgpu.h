@@ -149,8 +149,13 @@ int mfgpu_solve_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ld
 int mfgpu_backward_error_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ldb, const double* d_x,
                                 int64_t ldx, double* out);
 
-/* JSON object with the last call's phase times, sizes and counters. */
+/* JSON object with the last call's phase times, sizes and counters, and the
+ * per-kernel-class profile gathered since the last mfgpu_set_profiling. */
 int mfgpu_stats_json(mfgpu_ctx* h, char* buf, int64_t cap);
+/* Reset the launch counter and the kernel profile; on != 0 brackets every
+ * kernel launch with CUDA events on the launching stream (device times per
+ * kernel class, with their algorithmic flops and bytes). */
+int mfgpu_set_profiling(mfgpu_ctx* h, int32_t on);
 
 #ifdef __cplusplus
 }

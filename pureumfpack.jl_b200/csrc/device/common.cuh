@@ -1,0 +1,121 @@
+// common.cuh -- device helpers shared by libmfgpu's kernels (sm_100a).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../plan.h"
+
+namespace mfgpu {
+
+// Device copies of the pattern-only plan arrays (see plan.h for meaning).
+struct DevPlan {
+  int64_t n, ns;
+  const int32_t* c1;
+  const int32_t* np;
+  const int32_t* nu;
+  const int32_t* nf;
+  const int64_t* upd_off;
+  const int64_t* front_off;
+  const int64_t* colbase;
+  const int32_t* child_ptr;
+  const int32_t* child_idx;
+  const int32_t* upd;
+  const int32_t* rel;
+  const int64_t* uoff;
+  const int32_t* v_src;
+  const int32_t* v_srow;
+  const int32_t* v_frow;
+  const int32_t* fc_super;
+  const int32_t* fc_vbeg;
+  const int32_t* fc_vend;
+  const int32_t* fc_ch_ptr;
+  const int32_t* fc_ch;
+  const int64_t* lcolptr;
+  const int64_t* ucolptr;
+  const int32_t* qf;
+  const int32_t* csr_ptr;
+  const int32_t* csr_col;
+  const int32_t* csr_src;
+};
+
+// Per-factorization numeric state.
+struct DevState {
+  int32_t* ipiv;        // n: local pivot row (0-based within the supernode) of each elimination step
+  int32_t* info;        // ns: first zero pivot (local), INT32_MAX if none
+  int32_t* prow;        // n: V-row of each factor row
+  int32_t* rowfac;      // n: factor row of each V-row
+  int32_t* flags;       // [0]: speculative pivot order violated
+};
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ int warp_id() { return threadIdx.x >> 5; }
+
+// (|value|, index) argmax with LAPACK idamax tie-breaking: the first (lowest)
+// index among equal magnitudes wins.
+struct ArgMax {
+  double v;
+  int i;
+};
+__device__ __forceinline__ ArgMax better(ArgMax a, ArgMax b) {
+  if (b.v > a.v || (b.v == a.v && b.i < a.i)) return b;
+  return a;
+}
+__device__ __forceinline__ ArgMax warp_argmax(ArgMax a) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ArgMax b;
+    b.v = __shfl_xor_sync(0xffffffffu, a.v, o);
+    b.i = __shfl_xor_sync(0xffffffffu, a.i, o);
+    a = better(a, b);
+  }
+  return a;
+}
+
+// Block-wide argmax; `red` needs blockDim/32 entries.  All threads get the result.
+__device__ __forceinline__ ArgMax block_argmax(ArgMax a, ArgMax* red) {
+  a = warp_argmax(a);
+  const int nw = blockDim.x >> 5;
+  if (lane_id() == 0) red[warp_id()] = a;
+  __syncthreads();
+  if (warp_id() == 0) {
+    ArgMax b = lane_id() < nw ? red[lane_id()] : ArgMax{-1.0, 0x7fffffff};
+    b = warp_argmax(b);
+    if (lane_id() == 0) red[0] = b;
+  }
+  __syncthreads();
+  ArgMax r = red[0];
+  __syncthreads();
+  return r;
+}
+
+template <typename T>
+__device__ __forceinline__ double absd(T x) {
+  return fabs((double)x);
+}
+
+// 8-byte asynchronous global->shared copy with zero fill when !pred.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int bytes = pred ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool pred) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int bytes = pred ? 4 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// D += A * B on one 8x8x4 FP64 tensor-core tile (A row-major 8x4, B col-major 4x8).
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+}  // namespace mfgpu

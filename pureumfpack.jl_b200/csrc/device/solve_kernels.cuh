@@ -1,0 +1,287 @@
+// solve_kernels.cuh -- supernodal forward/backward solves on the resident fronts.
+//
+// Restates _solve_factor (src/interface.jl:123-138) with lsolve!/usolve!
+// (src/solve.jl:10-39) over the same factors, organised by supernode instead
+// of by CSC column: the unit-lower L panel [L11; L21] and the upper panel
+// [U11 U12] of every supernode are read straight from its front.
+//
+// Forward (leaves to root, one launch group per tree level): each supernode
+// gathers its right-hand-side block -- the scaled, permuted b on its pivot
+// rows (c = Rs[p] .* b[p]) plus the update vectors of its children, added in
+// the children's LIFO order exactly like the matrix extend-add -- solves with
+// L11 and forms its own update vector w = f[np:] - L21 * y.  No atomics, so
+// the result is deterministic.  Backward (root to leaves): x_piv =
+// U11 \ (y - U12 * x[upd]), gathering x of the ancestors' columns.  Finally
+// x[q] = x_factor (interface.jl:134-136).  Work arrays are column-major with
+// one column per right-hand side.
+#pragma once
+
+#include "common.cuh"
+
+namespace mfgpu {
+
+constexpr int kSolveCols = 32;      // right-hand sides per CTA in the small-supernode kernels
+constexpr int kSolveThreads = 128;
+
+struct SolveArgs {
+  int64_t nrhs;
+  const double* b;      // right-hand sides (col-major, ldb), original row order
+  int64_t ldb;
+  const double* rs;     // row scaling or nullptr
+  int64_t ldx;          // leading dimension of x (factor order), = n
+};
+
+// Pivot-row value of block position a: the scaled rhs at V-row prow[c1+a].
+__device__ __forceinline__ double rhs_value(const DevPlan& P, const DevState& S, const SolveArgs& A, int c1, int a,
+                                            int64_t col) {
+  const int g = S.prow[c1 + a];
+  const int orow = P.qf[g];
+  const double v = A.b[orow + col * A.ldb];
+  return A.rs ? A.rs[orow] * v : v;
+}
+
+// Block position of V-row position r (0..nf) of a child contribution: pivot
+// rows are reordered by the supernode's interchanges, update rows are not.
+__device__ __forceinline__ int front_pos(const DevState& S, int c1, int np, int rel) {
+  return rel < np ? S.rowfac[c1 + rel] - c1 : rel;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSolveThreads) k_fwd_small(DevPlan P, DevState S, SolveArgs A,
+                                                             const int32_t* __restrict__ tasks,
+                                                             const T* __restrict__ pool, T* __restrict__ fsol) {
+  __shared__ T f[kSmallFront * kSolveCols];
+  const int s = tasks[blockIdx.x];
+  const int c0 = blockIdx.y * kSolveCols;
+  const int rc = min(kSolveCols, (int)(A.nrhs - c0));
+  const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
+  const int tid = threadIdx.x;
+  const int64_t R = A.nrhs;
+  for (int e = tid; e < nf * rc; e += blockDim.x) {
+    const int r = e % nf, c = e / nf;
+    f[e] = r < np ? (T)rhs_value(P, S, A, c1, r, c0 + c) : T(0);
+  }
+  __syncthreads();
+  for (int ci = P.child_ptr[s + 1] - 1; ci >= P.child_ptr[s]; --ci) {
+    const int k = P.child_idx[ci];
+    const int m = P.nu[k], nfk = P.nf[k], npk = P.np[k];
+    const T* w = fsol + P.colbase[k] * R + npk;
+    const int32_t* rl = P.rel + P.upd_off[k];
+    for (int e = tid; e < m * rc; e += blockDim.x) {
+      const int r = e % m, c = e / m;
+      f[front_pos(S, c1, np, rl[r]) + c * nf] += w[r + (int64_t)(c0 + c) * nfk];
+    }
+    __syncthreads();
+  }
+  const T* L = pool + P.front_off[s];
+  for (int a = 0; a < np; ++a) {
+    const int rows = nf - a - 1;
+    for (int e = tid; e < rows * rc; e += blockDim.x) {
+      const int i = a + 1 + e % rows, c = e / rows;
+      f[i + c * nf] -= L[i + (int64_t)a * nf] * f[a + c * nf];
+    }
+    __syncthreads();
+  }
+  T* out = fsol + P.colbase[s] * R;
+  for (int e = tid; e < nf * rc; e += blockDim.x) {
+    const int r = e % nf, c = e / nf;
+    out[r + (int64_t)(c0 + c) * nf] = f[e];
+  }
+}
+
+// Large supernodes: gather the rhs block (one warp per right-hand side).
+template <typename T>
+__global__ void __launch_bounds__(256) k_fwd_assemble(DevPlan P, DevState S, SolveArgs A,
+                                                      const int32_t* __restrict__ tasks, T* __restrict__ fsol) {
+  const int s = tasks[blockIdx.x];
+  const int64_t col = (int64_t)blockIdx.y * 8 + warp_id();
+  if (col >= A.nrhs) return;
+  const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
+  const int lane = lane_id();
+  const int64_t R = A.nrhs;
+  T* f = fsol + P.colbase[s] * R + col * nf;
+  for (int r = lane; r < nf; r += 32) f[r] = r < np ? (T)rhs_value(P, S, A, c1, r, col) : T(0);
+  __syncwarp();
+  for (int ci = P.child_ptr[s + 1] - 1; ci >= P.child_ptr[s]; --ci) {
+    const int k = P.child_idx[ci];
+    const int m = P.nu[k], nfk = P.nf[k], npk = P.np[k];
+    const T* w = fsol + P.colbase[k] * R + npk + col * nfk;
+    const int32_t* rl = P.rel + P.upd_off[k];
+    for (int r = lane; r < m; r += 32) f[front_pos(S, c1, np, rl[r])] += w[r];
+    __syncwarp();
+  }
+}
+
+struct SolveBlockTask {
+  int32_t s, k0;
+};
+
+// Unit-lower diagonal block solve of rows k0..k1-1 (forward), one thread per rhs.
+template <typename T>
+__global__ void __launch_bounds__(64) k_fwd_diag(DevPlan P, const SolveBlockTask* __restrict__ tasks, int64_t nrhs,
+                                                 const T* __restrict__ pool, T* __restrict__ fsol) {
+  __shared__ T Ld[64 * 65];
+  const SolveBlockTask tk = tasks[blockIdx.x];
+  const int s = tk.s, k0 = tk.k0;
+  const int np = P.np[s], nf = P.nf[s];
+  const int kb = min(kPanel, np - k0);
+  const T* F = pool + P.front_off[s];
+  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) Ld[e % kb + (e / kb) * 65] = F[(k0 + e % kb) + (int64_t)(k0 + e / kb) * nf];
+  __syncthreads();
+  const int64_t col = (int64_t)blockIdx.y * blockDim.x + threadIdx.x;
+  if (col >= nrhs) return;
+  T* y = fsol + P.colbase[s] * nrhs + col * nf + k0;
+  T v[kPanel];
+#pragma unroll 8
+  for (int i = 0; i < kPanel; ++i)
+    if (i < kb) v[i] = y[i];
+  for (int i = 0; i < kb; ++i) {
+    T t = v[i];
+    for (int j = 0; j < i; ++j) t -= Ld[i + j * 65] * v[j];
+    v[i] = t;
+  }
+#pragma unroll 8
+  for (int i = 0; i < kPanel; ++i)
+    if (i < kb) y[i] = v[i];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSolveThreads) k_bwd_small(DevPlan P, SolveArgs A, const int32_t* __restrict__ tasks,
+                                                             const T* __restrict__ pool, T* __restrict__ fsol,
+                                                             T* __restrict__ xw) {
+  __shared__ T y[kSmallFront * kSolveCols];
+  __shared__ T g[kSmallFront * kSolveCols];
+  const int s = tasks[blockIdx.x];
+  const int c0 = blockIdx.y * kSolveCols;
+  const int rc = min(kSolveCols, (int)(A.nrhs - c0));
+  const int np = P.np[s], nu = P.nu[s], nf = P.nf[s], c1 = P.c1[s];
+  const int tid = threadIdx.x;
+  const int64_t R = A.nrhs;
+  const T* f = fsol + P.colbase[s] * R;
+  const int32_t* us = P.upd + P.upd_off[s];
+  for (int e = tid; e < np * rc; e += blockDim.x) {
+    const int r = e % np, c = e / np;
+    y[r + c * np] = f[r + (int64_t)(c0 + c) * nf];
+  }
+  for (int e = tid; e < nu * rc; e += blockDim.x) {
+    const int t = e % nu, c = e / nu;
+    g[t + c * nu] = xw[us[t] + (int64_t)(c0 + c) * A.ldx];
+  }
+  __syncthreads();
+  const T* U = pool + P.front_off[s];
+  for (int e = tid; e < np * rc; e += blockDim.x) {
+    const int a = e % np, c = e / np;
+    T acc = y[a + c * np];
+    for (int t = 0; t < nu; ++t) acc -= U[a + (int64_t)(np + t) * nf] * g[t + c * nu];
+    y[a + c * np] = acc;
+  }
+  __syncthreads();
+  for (int a = np - 1; a >= 0; --a) {
+    for (int c = tid; c < rc; c += blockDim.x) y[a + c * np] /= U[a + (int64_t)a * nf];
+    __syncthreads();
+    for (int e = tid; e < a * rc; e += blockDim.x) {
+      const int i = e % a, c = e / a;
+      y[i + c * np] -= U[i + (int64_t)a * nf] * y[a + c * np];
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < np * rc; e += blockDim.x) {
+    const int r = e % np, c = e / np;
+    xw[c1 + r + (int64_t)(c0 + c) * A.ldx] = y[r + c * np];
+  }
+}
+
+// Large supernodes: gather x of the update columns into the w rows.
+template <typename T>
+__global__ void __launch_bounds__(256) k_bwd_gather(DevPlan P, SolveArgs A, const int32_t* __restrict__ tasks,
+                                                    T* __restrict__ fsol, const T* __restrict__ xw) {
+  const int s = tasks[blockIdx.x];
+  const int64_t col = (int64_t)blockIdx.y * 8 + warp_id();
+  if (col >= A.nrhs) return;
+  const int np = P.np[s], nu = P.nu[s], nf = P.nf[s];
+  T* f = fsol + P.colbase[s] * A.nrhs + col * nf + np;
+  const int32_t* us = P.upd + P.upd_off[s];
+  for (int t = lane_id(); t < nu; t += 32) f[t] = xw[us[t] + col * A.ldx];
+}
+
+// Upper diagonal block solve of rows k0..k1-1 (backward); writes x.
+template <typename T>
+__global__ void __launch_bounds__(64) k_bwd_diag(DevPlan P, const SolveBlockTask* __restrict__ tasks, int64_t nrhs,
+                                                 int64_t ldx, const T* __restrict__ pool, T* __restrict__ fsol,
+                                                 T* __restrict__ xw) {
+  __shared__ T Ud[64 * 65];
+  const SolveBlockTask tk = tasks[blockIdx.x];
+  const int s = tk.s, k0 = tk.k0;
+  const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
+  const int kb = min(kPanel, np - k0);
+  const T* F = pool + P.front_off[s];
+  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) Ud[e % kb + (e / kb) * 65] = F[(k0 + e % kb) + (int64_t)(k0 + e / kb) * nf];
+  __syncthreads();
+  const int64_t col = (int64_t)blockIdx.y * blockDim.x + threadIdx.x;
+  if (col >= nrhs) return;
+  T* y = fsol + P.colbase[s] * nrhs + col * nf + k0;
+  T v[kPanel];
+#pragma unroll 8
+  for (int i = 0; i < kPanel; ++i)
+    if (i < kb) v[i] = y[i];
+  for (int i = kb - 1; i >= 0; --i) {
+    T t = v[i];
+    for (int j = i + 1; j < kb; ++j) t -= Ud[i + j * 65] * v[j];
+    v[i] = t / Ud[i + i * 65];
+  }
+#pragma unroll 8
+  for (int i = 0; i < kPanel; ++i)
+    if (i < kb) {
+      y[i] = v[i];
+      xw[c1 + k0 + i + col * ldx] = v[i];
+    }
+}
+
+// x[q[k]] = x_factor[k] (interface.jl:134-136); optionally accumulate (x += d).
+template <typename T>
+__global__ void k_solve_finish(int64_t n, int64_t nrhs, const int32_t* __restrict__ qf, const T* __restrict__ xw,
+                               int64_t ldw, double* __restrict__ x, int64_t ldx, int accumulate) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n * nrhs) return;
+  const int64_t k = e % n, c = e / n;
+  const double v = (double)xw[k + c * ldw];
+  double* dst = x + qf[k] + c * ldx;
+  *dst = accumulate ? *dst + v : v;
+}
+
+// r = b - A * x with the unscaled A in CSR (interface.jl:173), FP64.
+__global__ void k_residual(int64_t n, int64_t nrhs, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                           const int32_t* __restrict__ src, const double* __restrict__ ax,
+                           const double* __restrict__ b, int64_t ldb, const double* __restrict__ x, int64_t ldx,
+                           double* __restrict__ r, int64_t ldr) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n * nrhs) return;
+  const int64_t i = e % n, c = e / n;
+  double acc = 0.0;
+  for (int p = rp[i]; p < rp[i + 1]; ++p) acc += ax[src[p]] * x[ci[p] + c * ldx];
+  r[i + c * ldr] = b[i + c * ldb] - acc;
+}
+
+// Per-column maxima of |r|, |x|, |b| for the normwise backward error.
+__global__ void k_bwd_error_parts(int64_t n, int64_t nrhs, const double* __restrict__ r, int64_t ldr,
+                                  const double* __restrict__ x, int64_t ldx, const double* __restrict__ b, int64_t ldb,
+                                  unsigned long long* __restrict__ out) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n * nrhs) return;
+  const int64_t i = e % n, c = e / n;
+  atomicMax(out + 3 * c + 0, (unsigned long long)__double_as_longlong(fabs(r[i + c * ldr])));
+  atomicMax(out + 3 * c + 1, (unsigned long long)__double_as_longlong(fabs(x[i + c * ldx])));
+  atomicMax(out + 3 * c + 2, (unsigned long long)__double_as_longlong(fabs(b[i + c * ldb])));
+}
+
+// ||A||_inf = max row sum of |a_ij|.
+__global__ void k_norm_inf(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ src,
+                           const double* __restrict__ ax, unsigned long long* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double acc = 0.0;
+  for (int p = rp[i]; p < rp[i + 1]; ++p) acc += fabs(ax[src[p]]);
+  atomicMax(out, (unsigned long long)__double_as_longlong(acc));
+}
+
+}  // namespace mfgpu

@@ -1,0 +1,1030 @@
+// mfgpu.cu -- C ABI of libmfgpu's GPU numeric factorization and solves.
+//
+// One context per handle: a plan (pattern analysis), its device copy, the
+// front pool and the factors resident in HBM, one CUDA stream.  The numeric
+// factorization replaces the hot loop of src/multifrontal.jl:198-357 and the
+// solves replace src/interface.jl:123-177 / src/solve.jl:10-79; see the
+// kernel headers for the step-by-step correspondence.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/mfgpu.h"
+#include "device/factor_kernels.cuh"
+#include "device/gemm_kernels.cuh"
+#include "device/solve_kernels.cuh"
+#include "host/symbolic.h"
+#include "plan.h"
+
+using namespace mfgpu;
+
+struct mfgpu_symbolic {
+  mfgpu::SymbolicMF s;
+};
+
+namespace {
+
+struct CudaError : std::runtime_error {
+  cudaError_t code;
+  CudaError(cudaError_t c, const char* what) : std::runtime_error(what), code(c) {}
+};
+
+#define CK(x)                                                                                     \
+  do {                                                                                            \
+    cudaError_t e_ = (x);                                                                         \
+    if (e_ != cudaSuccess)                                                                        \
+      throw CudaError(e_, (std::string(#x) + ": " + cudaGetErrorString(e_)).c_str());            \
+  } while (0)
+
+// Grow-only device buffer.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void ensure(size_t need) {
+    if (need <= bytes) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    if (need == 0) return;
+    cudaError_t e = cudaMalloc(&p, need);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw CudaError(e, ("device allocation of " + std::to_string(need) + " bytes failed").c_str());
+    }
+    bytes = need;
+  }
+  template <typename T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+};
+
+template <typename T>
+void upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
+  b.ensure(std::max<size_t>(v.size() * sizeof(T), 16));
+  if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
+inline unsigned grid1(int64_t work, int per) { return (unsigned)((work + per - 1) / per); }
+
+enum KernelClass {
+  KC_BUILD_VALUES, KC_SMALL, KC_ASSEMBLE, KC_PANEL, KC_TRSM, KC_GEMM_FACTOR, KC_PIVOTS, KC_SCATTER,
+  KC_FWD_SMALL, KC_FWD_ASSEMBLE, KC_FWD_DIAG, KC_GEMM_SOLVE, KC_BWD_SMALL, KC_BWD_GATHER, KC_BWD_DIAG,
+  KC_SOLVE_FINISH, KC_RESIDUAL, KC_COUNT
+};
+const char* const kKernelClassName[KC_COUNT] = {
+    "build_values", "small_fronts", "assemble_columns", "panel", "panel_trsm", "gemm_factor", "finalize_pivots",
+    "scatter_csc", "fwd_small", "fwd_assemble", "fwd_diag", "gemm_solve", "bwd_small", "bwd_gather", "bwd_diag",
+    "solve_finish", "residual"};
+
+struct KStat {
+  double ms = 0, flops = 0, bytes = 0;
+  int64_t launches = 0;
+};
+
+struct SolveSchedule {
+  int64_t nrhs = -1;
+  struct Step {
+    int kind;        // 0 fwd_small, 1 fwd_assemble, 2 fwd_diag, 3 gemm(front,fsol,fsol), 4 bwd_small,
+                     // 5 bwd_gather, 6 bwd_diag
+    int64_t first, count, tiles;
+    double flops = 0, elems = 0;
+  };
+  std::vector<Step> steps;
+  std::vector<int32_t> ids;
+  std::vector<SolveBlockTask> blocks;
+  std::vector<GemmTask> gemms;
+  DevBuf d_ids, d_blocks, d_gemms;
+};
+
+}  // namespace
+
+struct mfgpu_ctx {
+  int device = 0;
+  int precision = MFGPU_PRECISION_FP64;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  bool analyzed = false, factored = false, csc_ready = false;
+  Plan plan;
+  DevPlan dp{};
+  // plan arrays
+  DevBuf b_c1, b_np, b_nu, b_nf, b_upd_off, b_front_off, b_colbase, b_child_ptr, b_child_idx, b_upd, b_rel, b_uoff,
+      b_v_src, b_v_srow, b_v_frow, b_fc_super, b_fc_vbeg, b_fc_vend, b_fc_ch_ptr, b_fc_ch, b_lcolptr, b_ucolptr, b_qf,
+      b_csr_ptr, b_csr_col, b_csr_src;
+  DevBuf b_small, b_panel, b_trsm, b_gemm;
+  bool launches_safe = false;
+  // numeric state
+  DevBuf b_pool, b_vx, b_ax, b_rs, b_ipiv, b_info, b_prow, b_rowfac, b_flags;
+  bool have_rs = false;
+  int factor_precision = MFGPU_PRECISION_FP64;
+  DevBuf b_li, b_lx, b_ui, b_ux;
+  // solve state
+  SolveSchedule sched;
+  DevBuf b_fsol, b_xw, b_b, b_x, b_r, b_d, b_err, b_norm;
+  // stats
+  double t_analyze_ms = 0, t_factor_ms = 0, t_solve_ms = 0, t_csc_ms = 0;
+  int factor_reruns = 0;
+  int32_t last_status = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // per-kernel-class profile (CUDA events around each launch when enabled)
+  bool profiling = false;
+  int64_t launch_count = 0;
+  KStat kstat[KC_COUNT];
+  struct Pending {
+    int kc;
+    cudaEvent_t a, b;
+    double flops, bytes;
+  };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> evpool;
+  size_t evnext = 0;
+};
+
+namespace {
+
+int fail(mfgpu_ctx* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+template <typename F>
+int guarded(mfgpu_ctx* h, F&& body) {
+  try {
+    return body();
+  } catch (const CudaError& e) {
+    return fail(h, e.code == cudaErrorMemoryAllocation ? MFGPU_ERR_NOMEM : MFGPU_ERR_CUDA, e.what());
+  } catch (const std::invalid_argument& e) {
+    return fail(h, MFGPU_ERR_ARGUMENT, e.what());
+  } catch (const std::exception& e) {
+    return fail(h, MFGPU_ERR_INTERNAL, e.what());
+  }
+}
+
+void upload_plan(mfgpu_ctx* h) {
+  const Plan& P = h->plan;
+  cudaStream_t st = h->stream;
+  upload(h->b_c1, P.c1, st);
+  upload(h->b_np, P.np, st);
+  upload(h->b_nu, P.nu, st);
+  upload(h->b_nf, P.nf, st);
+  upload(h->b_upd_off, P.upd_off, st);
+  upload(h->b_front_off, P.front_off, st);
+  upload(h->b_colbase, P.colbase, st);
+  upload(h->b_child_ptr, P.child_ptr, st);
+  upload(h->b_child_idx, P.child_idx, st);
+  upload(h->b_upd, P.upd, st);
+  upload(h->b_rel, P.rel, st);
+  upload(h->b_uoff, P.uoff, st);
+  upload(h->b_v_src, P.v_src, st);
+  upload(h->b_v_srow, P.v_srow, st);
+  upload(h->b_v_frow, P.v_frow, st);
+  upload(h->b_fc_super, P.fc_super, st);
+  upload(h->b_fc_vbeg, P.fc_vbeg, st);
+  upload(h->b_fc_vend, P.fc_vend, st);
+  upload(h->b_fc_ch_ptr, P.fc_ch_ptr, st);
+  upload(h->b_fc_ch, P.fc_ch, st);
+  upload(h->b_lcolptr, P.lcolptr, st);
+  upload(h->b_ucolptr, P.ucolptr, st);
+  upload(h->b_qf, P.qf, st);
+  upload(h->b_csr_ptr, P.csr_ptr, st);
+  upload(h->b_csr_col, P.csr_col, st);
+  upload(h->b_csr_src, P.csr_src, st);
+  DevPlan& d = h->dp;
+  d.n = P.n;
+  d.ns = P.ns;
+  d.c1 = h->b_c1.as<int32_t>();
+  d.np = h->b_np.as<int32_t>();
+  d.nu = h->b_nu.as<int32_t>();
+  d.nf = h->b_nf.as<int32_t>();
+  d.upd_off = h->b_upd_off.as<int64_t>();
+  d.front_off = h->b_front_off.as<int64_t>();
+  d.colbase = h->b_colbase.as<int64_t>();
+  d.child_ptr = h->b_child_ptr.as<int32_t>();
+  d.child_idx = h->b_child_idx.as<int32_t>();
+  d.upd = h->b_upd.as<int32_t>();
+  d.rel = h->b_rel.as<int32_t>();
+  d.uoff = h->b_uoff.as<int64_t>();
+  d.v_src = h->b_v_src.as<int32_t>();
+  d.v_srow = h->b_v_srow.as<int32_t>();
+  d.v_frow = h->b_v_frow.as<int32_t>();
+  d.fc_super = h->b_fc_super.as<int32_t>();
+  d.fc_vbeg = h->b_fc_vbeg.as<int32_t>();
+  d.fc_vend = h->b_fc_vend.as<int32_t>();
+  d.fc_ch_ptr = h->b_fc_ch_ptr.as<int32_t>();
+  d.fc_ch = h->b_fc_ch.as<int32_t>();
+  d.lcolptr = h->b_lcolptr.as<int64_t>();
+  d.ucolptr = h->b_ucolptr.as<int64_t>();
+  d.qf = h->b_qf.as<int32_t>();
+  d.csr_ptr = h->b_csr_ptr.as<int32_t>();
+  d.csr_col = h->b_csr_col.as<int32_t>();
+  d.csr_src = h->b_csr_src.as<int32_t>();
+}
+
+void upload_launches(mfgpu_ctx* h) {
+  const Plan& P = h->plan;
+  upload(h->b_small, P.small_tasks, h->stream);
+  upload(h->b_panel, P.panel_tasks, h->stream);
+  upload(h->b_trsm, P.trsm_tasks, h->stream);
+  upload(h->b_gemm, P.gemm_tasks, h->stream);
+}
+
+DevState dev_state(mfgpu_ctx* h) {
+  DevState s;
+  s.ipiv = h->b_ipiv.as<int32_t>();
+  s.info = h->b_info.as<int32_t>();
+  s.prow = h->b_prow.as<int32_t>();
+  s.rowfac = h->b_rowfac.as<int32_t>();
+  s.flags = h->b_flags.as<int32_t>();
+  return s;
+}
+
+cudaEvent_t next_event(mfgpu_ctx* h) {
+  if (h->evnext == h->evpool.size()) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    h->evpool.push_back(e);
+  }
+  return h->evpool[h->evnext++];
+}
+
+// Every kernel launch of the library goes through here: it counts launches
+// and, when profiling is on, brackets the launch with CUDA events on the
+// launching stream and books its algorithmic work to its kernel class.
+template <typename F>
+void klaunch(mfgpu_ctx* h, int kc, double flops, double bytes, F&& f) {
+  ++h->launch_count;
+  if (!h->profiling) {
+    f();
+    return;
+  }
+  cudaEvent_t a = next_event(h), b = next_event(h);
+  CK(cudaEventRecord(a, h->stream));
+  f();
+  CK(cudaEventRecord(b, h->stream));
+  h->pending.push_back({kc, a, b, flops, bytes});
+}
+
+void prof_flush(mfgpu_ctx* h) {
+  for (auto& p : h->pending) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, p.a, p.b));
+    KStat& k = h->kstat[p.kc];
+    k.ms += ms;
+    k.flops += p.flops;
+    k.bytes += p.bytes;
+    ++k.launches;
+  }
+  h->pending.clear();
+  h->evnext = 0;
+}
+
+template <typename T>
+size_t panel_smem_bytes() {
+  return (size_t)kPivRowsSmem * kPanel * sizeof(T);
+}
+
+template <typename T>
+size_t trsm_smem_bytes() {
+  return (size_t)2 * 64 * 65 * sizeof(T);
+}
+
+template <typename T>
+void configure_kernels() {
+  static bool done = false;
+  if (done) return;
+  CK(cudaFuncSetAttribute(k_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_smem_bytes<T>()));
+  CK(cudaFuncSetAttribute(k_panel_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem_bytes<T>()));
+  done = true;
+}
+
+__global__ void k_fill_i32(int32_t* p, int64_t n, int32_t v) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+template <typename T>
+void launch_gemm(const GemmTask* tasks, int64_t count, int64_t tiles, const T* pa, const T* pb, T* pc,
+                 cudaStream_t st);
+template <>
+void launch_gemm<double>(const GemmTask* tasks, int64_t count, int64_t tiles, const double* pa, const double* pb,
+                         double* pc, cudaStream_t st) {
+  k_gemm_f64<<<(unsigned)tiles, kGemmThreads, 0, st>>>(tasks, (int)count, pa, pb, pc);
+}
+template <>
+void launch_gemm<float>(const GemmTask* tasks, int64_t count, int64_t tiles, const float* pa, const float* pb,
+                        float* pc, cudaStream_t st) {
+  k_gemm_f32<<<(unsigned)tiles, 256, 0, st>>>(tasks, (int)count, pa, pb, pc);
+}
+
+template <typename T>
+void run_factor_launches(mfgpu_ctx* h) {
+  const Plan& P = h->plan;
+  cudaStream_t st = h->stream;
+  T* pool = h->b_pool.as<T>();
+  const double* vx = h->b_vx.as<double>();
+  DevState S = dev_state(h);
+  for (const Launch& L : P.launches) {
+    const double bytes = L.elems * sizeof(T) + L.extra_bytes;
+    switch (L.kind) {
+      case kLaunchSmall:
+        klaunch(h, KC_SMALL, L.flops, bytes, [&] {
+          k_small_fronts<T><<<(unsigned)L.count, kSmallThreads, kSmallFront * kSmallFront * sizeof(T), st>>>(
+              h->dp, S, h->b_small.as<int32_t>() + L.first, pool, vx);
+        });
+        break;
+      case kLaunchAssemble:
+        klaunch(h, KC_ASSEMBLE, 0, bytes, [&] {
+          k_assemble_columns<T><<<grid1(L.count, 8), 256, 0, st>>>(h->dp, L.first, L.count, pool, vx);
+        });
+        break;
+      case kLaunchPanel:
+        klaunch(h, KC_PANEL, L.flops, bytes, [&] {
+          k_panel<T><<<(unsigned)L.count, kPanelThreads, panel_smem_bytes<T>(), st>>>(
+              h->dp, S, h->b_panel.as<PanelTask>() + L.first, pool);
+        });
+        break;
+      case kLaunchTrsm:
+        klaunch(h, KC_TRSM, L.flops, bytes, [&] {
+          k_panel_trsm<T><<<(unsigned)L.tiles, kTrsmThreads, trsm_smem_bytes<T>(), st>>>(
+              h->dp, S, h->b_trsm.as<TrsmTask>() + L.first, (int)L.count, pool);
+        });
+        break;
+      case kLaunchGemm:
+        klaunch(h, KC_GEMM_FACTOR, L.flops, bytes, [&] {
+          launch_gemm<T>(h->b_gemm.as<GemmTask>() + L.first, L.count, L.tiles, pool, pool, pool, st);
+        });
+        break;
+    }
+  }
+  CK(cudaGetLastError());
+}
+
+template <typename T>
+int factor_impl(mfgpu_ctx* h, int32_t check) {
+  Plan& P = h->plan;
+  cudaStream_t st = h->stream;
+  configure_kernels<T>();
+  h->b_pool.ensure(std::max<size_t>(P.front_elems * sizeof(T), 16));
+  h->b_ipiv.ensure(std::max<int64_t>(P.n, 1) * 4);
+  h->b_prow.ensure(std::max<int64_t>(P.n, 1) * 4);
+  h->b_rowfac.ensure(std::max<int64_t>(P.n, 1) * 4);
+  h->b_info.ensure(std::max<int64_t>(P.ns, 1) * 4);
+  h->b_flags.ensure(16);
+  h->b_vx.ensure(std::max<int64_t>(P.nnz_a, 1) * 8);
+  CK(cudaEventRecord(h->ev0, st));
+  klaunch(h, KC_BUILD_VALUES, P.nnz_a, 32.0 * P.nnz_a, [&] {
+    k_build_values<<<grid1(P.nnz_a, 256), 256, 0, st>>>(P.nnz_a, h->b_v_src.as<int32_t>(), h->b_v_srow.as<int32_t>(),
+                                                          h->b_ax.as<double>(),
+                                                          h->have_rs ? h->b_rs.as<double>() : nullptr,
+                                                          h->b_vx.as<double>());
+  });
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    if (P.ns) k_fill_i32<<<grid1(P.ns, 256), 256, 0, st>>>(h->b_info.as<int32_t>(), P.ns, INT32_MAX);
+    CK(cudaMemsetAsync(h->b_flags.p, 0, 16, st));
+    run_factor_launches<T>(h);
+    if (!P.has_speculative) break;
+    int32_t flag = 0;
+    CK(cudaMemcpyAsync(&flag, h->b_flags.p, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (!flag) break;
+    // a speculative panel met a row that partial pivoting would have chosen:
+    // redo the factorization with pivoting panels everywhere.
+    build_launches(P, true);
+    upload_launches(h);
+    h->launches_safe = true;
+    ++h->factor_reruns;
+  }
+  if (P.ns)
+    klaunch(h, KC_PIVOTS, 0, 16.0 * P.n, [&] { k_finalize_pivots<<<grid1(P.ns, 128), 128, 0, st>>>(h->dp, dev_state(h)); });
+  // direct CSC scatter of L and U
+  h->b_li.ensure(std::max<int64_t>(P.nnz_l, 1) * 8);
+  h->b_lx.ensure(std::max<int64_t>(P.nnz_l, 1) * 8);
+  h->b_ui.ensure(std::max<int64_t>(P.nnz_u, 1) * 8);
+  h->b_ux.ensure(std::max<int64_t>(P.nnz_u, 1) * 8);
+  if (P.fc_total)
+    klaunch(h, KC_SCATTER, 0, (double)(P.nnz_l + P.nnz_u) * (16.0 + sizeof(T)), [&] {
+      k_scatter_csc<T><<<grid1(P.fc_total, 8), 256, 0, st>>>(h->dp, dev_state(h), h->b_pool.as<T>(), P.fc_total,
+                                                             h->b_li.as<int64_t>(), h->b_lx.as<double>(),
+                                                             h->b_ui.as<int64_t>(), h->b_ux.as<double>());
+    });
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(h->ev1, st));
+  // status: first supernode (postorder) with a zero pivot
+  std::vector<int32_t> info(P.ns);
+  if (P.ns) CK(cudaMemcpyAsync(info.data(), h->b_info.p, P.ns * 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->t_factor_ms = ms;
+  prof_flush(h);
+  h->factored = true;
+  h->csc_ready = true;
+  h->factor_precision = (sizeof(T) == 8) ? MFGPU_PRECISION_FP64 : MFGPU_PRECISION_MIXED;
+  int32_t status = 0;
+  if (check)
+    for (int64_t s = 0; s < P.ns; ++s)
+      if (info[s] != INT32_MAX) {
+        status = P.c1[s] + info[s] + 1;
+        break;
+      }
+  h->last_status = status;
+  return status;
+}
+
+int factor_dispatch(mfgpu_ctx* h, int32_t check) {
+  if (h->precision == MFGPU_PRECISION_MIXED) return factor_impl<float>(h, check);
+  return factor_impl<double>(h, check);
+}
+
+// ---- solves ---------------------------------------------------------------
+void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
+  SolveSchedule& S = h->sched;
+  if (S.nrhs == R) return;
+  const Plan& P = h->plan;
+  S = SolveSchedule{};
+  S.nrhs = R;
+  auto ceil_div = [](int64_t a, int64_t b) { return (a + b - 1) / b; };
+  double work_flops = 0, work_elems = 0;
+  auto add_gemm = [&](std::vector<GemmTask>& v, int64_t& tiles, int64_t a, int64_t b, int64_t c, int m, int n, int k,
+                      int lda, int ldb, int ldc) {
+    if (m <= 0 || n <= 0 || k <= 0) return;
+    GemmTask g{};
+    g.a = a; g.b = b; g.c = c;
+    g.m = m; g.n = n; g.k = k;
+    g.lda = lda; g.ldb = ldb; g.ldc = ldc;
+    g.tiles_m = (int)ceil_div(m, 64);
+    g.tiles_n = (int)ceil_div(n, 64);
+    g.tile_base = tiles;
+    tiles += (int64_t)g.tiles_m * g.tiles_n;
+    v.push_back(g);
+    work_flops += 2.0 * m * n * k;
+    work_elems += 2.0 * m * n + (double)m * k + (double)k * n;
+  };
+  // small-supernode kernels: L or U panel read once, the rhs block read and written
+  auto small_work = [&](SolveSchedule::Step& st, int32_t s) {
+    const double a = P.np[s], u = P.nu[s];
+    st.flops += (a * a + 2.0 * a * u) * R;
+    st.elems += (a * a / 2 + a * u) + 2.0 * (a + u) * R;
+  };
+  // forward, leaves to root
+  for (int32_t L = 0; L < P.nlevels; ++L) {
+    const int32_t a = P.level_slot[L], m = P.level_large[L], e = P.level_slot[L + 1];
+    if (m > a) {
+      SolveSchedule::Step st{0, (int64_t)S.ids.size(), m - a, 0};
+      for (int32_t i = a; i < m; ++i) {
+        S.ids.push_back(P.slot_super[i]);
+        small_work(st, P.slot_super[i]);
+      }
+      S.steps.push_back(st);
+    }
+    if (e > m) {
+      const int64_t first = (int64_t)S.ids.size();
+      int32_t maxnp = 0;
+      for (int32_t i = m; i < e; ++i) {
+        S.ids.push_back(P.slot_super[i]);
+        maxnp = std::max(maxnp, P.np[P.slot_super[i]]);
+      }
+      S.steps.push_back({1, first, e - m, 0});
+      for (int32_t k0 = 0; k0 < maxnp; k0 += kPanel) {
+        SolveSchedule::Step d{2, (int64_t)S.blocks.size(), 0, 0};
+        SolveSchedule::Step g{3, (int64_t)S.gemms.size(), 0, 0};
+        work_flops = work_elems = 0;
+        for (int32_t i = m; i < e; ++i) {
+          const int32_t s = P.slot_super[i];
+          if (P.np[s] <= k0) continue;
+          const int k1 = std::min(k0 + kPanel, P.np[s]);
+          S.blocks.push_back({s, k0});
+          ++d.count;
+          d.flops += (double)(k1 - k0) * (k1 - k0) * R;
+          d.elems += (double)(k1 - k0) * (k1 - k0) + 2.0 * (k1 - k0) * R;
+          const int64_t fb = P.colbase[s] * R;
+          const int nf = P.nf[s];
+          add_gemm(S.gemms, g.tiles, P.front_off[s] + k1 + (int64_t)k0 * nf, fb + k0, fb + k1, nf - k1, (int)R,
+                   k1 - k0, nf, nf, nf);
+        }
+        g.count = (int64_t)S.gemms.size() - g.first;
+        g.flops = work_flops;
+        g.elems = work_elems;
+        if (d.count) S.steps.push_back(d);
+        if (g.count) S.steps.push_back(g);
+      }
+    }
+  }
+  // backward, root to leaves
+  for (int32_t L = P.nlevels - 1; L >= 0; --L) {
+    const int32_t a = P.level_slot[L], m = P.level_large[L], e = P.level_slot[L + 1];
+    if (e > m) {
+      const int64_t first = (int64_t)S.ids.size();
+      int32_t maxblocks = 0;
+      for (int32_t i = m; i < e; ++i) {
+        S.ids.push_back(P.slot_super[i]);
+        maxblocks = std::max<int32_t>(maxblocks, (int32_t)ceil_div(P.np[P.slot_super[i]], kPanel));
+      }
+      S.steps.push_back({5, first, e - m, 0});
+      SolveSchedule::Step g{3, (int64_t)S.gemms.size(), 0, 0};
+      work_flops = work_elems = 0;
+      for (int32_t i = m; i < e; ++i) {
+        const int32_t s = P.slot_super[i];
+        const int nf = P.nf[s], np = P.np[s];
+        const int64_t fb = P.colbase[s] * R;
+        add_gemm(S.gemms, g.tiles, P.front_off[s] + (int64_t)np * nf, fb + np, fb, np, (int)R, P.nu[s], nf, nf, nf);
+      }
+      g.count = (int64_t)S.gemms.size() - g.first;
+      g.flops = work_flops;
+      g.elems = work_elems;
+      if (g.count) S.steps.push_back(g);
+      for (int32_t bi = maxblocks - 1; bi >= 0; --bi) {
+        SolveSchedule::Step d{6, (int64_t)S.blocks.size(), 0, 0};
+        SolveSchedule::Step gg{3, (int64_t)S.gemms.size(), 0, 0};
+        work_flops = work_elems = 0;
+        for (int32_t i = m; i < e; ++i) {
+          const int32_t s = P.slot_super[i];
+          if (ceil_div(P.np[s], kPanel) <= bi) continue;
+          const int k0 = bi * kPanel, k1 = std::min(k0 + kPanel, P.np[s]);
+          S.blocks.push_back({s, k0});
+          ++d.count;
+          d.flops += (double)(k1 - k0) * (k1 - k0) * R;
+          d.elems += (double)(k1 - k0) * (k1 - k0) + 2.0 * (k1 - k0) * R;
+          const int64_t fb = P.colbase[s] * R;
+          const int nf = P.nf[s];
+          add_gemm(S.gemms, gg.tiles, P.front_off[s] + (int64_t)k0 * nf, fb + k0, fb, k0, (int)R, k1 - k0, nf, nf,
+                   nf);
+        }
+        gg.count = (int64_t)S.gemms.size() - gg.first;
+        gg.flops = work_flops;
+        gg.elems = work_elems;
+        if (d.count) S.steps.push_back(d);
+        if (gg.count) S.steps.push_back(gg);
+      }
+    }
+    if (m > a) {
+      SolveSchedule::Step st{4, (int64_t)S.ids.size(), m - a, 0};
+      for (int32_t i = a; i < m; ++i) {
+        S.ids.push_back(P.slot_super[i]);
+        small_work(st, P.slot_super[i]);
+      }
+      S.steps.push_back(st);
+    }
+  }
+  upload(S.d_ids, S.ids, h->stream);
+  upload(S.d_blocks, S.blocks, h->stream);
+  upload(S.d_gemms, S.gemms, h->stream);
+}
+
+// One solve A x = b for device b (ldb) into device x (ldx) (x overwritten, or
+// accumulated when `accumulate`).
+template <typename T>
+void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double* d_x, int64_t ldx, bool use_rs,
+                int accumulate) {
+  const Plan& P = h->plan;
+  cudaStream_t st = h->stream;
+  build_solve_schedule(h, R);
+  SolveSchedule& S = h->sched;
+  h->b_fsol.ensure(std::max<size_t>((size_t)P.fc_total * R * sizeof(T), 16));
+  h->b_xw.ensure(std::max<size_t>((size_t)P.n * R * sizeof(T), 16));
+  T* pool = h->b_pool.as<T>();
+  T* fsol = h->b_fsol.as<T>();
+  T* xw = h->b_xw.as<T>();
+  DevState DS = dev_state(h);
+  SolveArgs A{R, d_b, ldb, (use_rs && h->have_rs) ? h->b_rs.as<double>() : nullptr, P.n};
+  const unsigned ychunks = (unsigned)((R + kSolveCols - 1) / kSolveCols);
+  const unsigned wchunks = (unsigned)((R + 7) / 8);
+  const unsigned tchunks = (unsigned)((R + 63) / 64);
+  const int32_t* ids = S.d_ids.as<int32_t>();
+  const SolveBlockTask* blocks = S.d_blocks.as<SolveBlockTask>();
+  const GemmTask* gemms = S.d_gemms.as<GemmTask>();
+  for (const auto& s : S.steps) {
+    const double bytes = s.elems * sizeof(T);
+    switch (s.kind) {
+      case 0:
+        klaunch(h, KC_FWD_SMALL, s.flops, bytes, [&] {
+          k_fwd_small<T><<<dim3((unsigned)s.count, ychunks), kSolveThreads, 0, st>>>(h->dp, DS, A, ids + s.first,
+                                                                                     pool, fsol);
+        });
+        break;
+      case 1:
+        klaunch(h, KC_FWD_ASSEMBLE, 0, 0, [&] {
+          k_fwd_assemble<T><<<dim3((unsigned)s.count, wchunks), 256, 0, st>>>(h->dp, DS, A, ids + s.first, fsol);
+        });
+        break;
+      case 2:
+        klaunch(h, KC_FWD_DIAG, s.flops, bytes, [&] {
+          k_fwd_diag<T><<<dim3((unsigned)s.count, tchunks), 64, 0, st>>>(h->dp, blocks + s.first, R, pool, fsol);
+        });
+        break;
+      case 3:
+        klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
+          launch_gemm<T>(gemms + s.first, s.count, s.tiles, pool, fsol, fsol, st);
+        });
+        break;
+      case 4:
+        klaunch(h, KC_BWD_SMALL, s.flops, bytes, [&] {
+          k_bwd_small<T><<<dim3((unsigned)s.count, ychunks), kSolveThreads, 0, st>>>(h->dp, A, ids + s.first, pool,
+                                                                                     fsol, xw);
+        });
+        break;
+      case 5:
+        klaunch(h, KC_BWD_GATHER, 0, 0, [&] {
+          k_bwd_gather<T><<<dim3((unsigned)s.count, wchunks), 256, 0, st>>>(h->dp, A, ids + s.first, fsol, xw);
+        });
+        break;
+      case 6:
+        klaunch(h, KC_BWD_DIAG, s.flops, bytes, [&] {
+          k_bwd_diag<T><<<dim3((unsigned)s.count, tchunks), 64, 0, st>>>(h->dp, blocks + s.first, R, P.n, pool,
+                                                                         fsol, xw);
+        });
+        break;
+    }
+  }
+  klaunch(h, KC_SOLVE_FINISH, 0, (double)P.n * R * (sizeof(T) + 8.0 * (1 + accumulate)), [&] {
+    k_solve_finish<T><<<grid1(P.n * R, 256), 256, 0, st>>>(P.n, R, h->b_qf.as<int32_t>(), xw, P.n, d_x, ldx,
+                                                           accumulate);
+  });
+  CK(cudaGetLastError());
+}
+
+template <typename T>
+void solve_refine(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double* d_x, int64_t ldx, int refine,
+                  bool use_rs) {
+  const Plan& P = h->plan;
+  cudaStream_t st = h->stream;
+  solve_once<T>(h, R, d_b, ldb, d_x, ldx, use_rs, 0);
+  if (refine > 0) {
+    h->b_r.ensure(std::max<size_t>((size_t)P.n * R * 8, 16));
+    double* r = h->b_r.as<double>();
+    for (int it = 0; it < refine; ++it) {
+      klaunch(h, KC_RESIDUAL, 2.0 * P.nnz_a * R, 16.0 * P.nnz_a + 24.0 * P.n * R, [&] {
+        k_residual<<<grid1(P.n * R, 256), 256, 0, st>>>(P.n, R, h->b_csr_ptr.as<int32_t>(),
+                                                        h->b_csr_col.as<int32_t>(), h->b_csr_src.as<int32_t>(),
+                                                        h->b_ax.as<double>(), d_b, ldb, d_x, ldx, r, P.n);
+      });
+      solve_once<T>(h, R, r, P.n, d_x, ldx, use_rs, 1);
+    }
+  }
+  CK(cudaGetLastError());
+}
+
+void solve_dispatch(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double* d_x, int64_t ldx, int refine) {
+  if (h->factor_precision == MFGPU_PRECISION_MIXED) solve_refine<float>(h, R, d_b, ldb, d_x, ldx, refine, true);
+  else solve_refine<double>(h, R, d_b, ldb, d_x, ldx, refine, true);
+}
+
+int analyze_common(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf,
+                   const int64_t* parent, int64_t ns, const int64_t* sstart, const int64_t* upd_ptr,
+                   const int64_t* upd_idx) {
+  auto t0 = std::chrono::steady_clock::now();
+  build_plan(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, h->plan);
+  upload_plan(h);
+  upload_launches(h);
+  h->launches_safe = false;
+  h->analyzed = true;
+  h->factored = false;
+  h->csc_ready = false;
+  h->sched = SolveSchedule{};
+  CK(cudaStreamSynchronize(h->stream));
+  h->t_analyze_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return MFGPU_OK;
+}
+
+bool valid_csc(int64_t n, const int64_t* colptr, const int64_t* rowval) {
+  if (n < 0 || !colptr || colptr[0] != 1) return false;
+  for (int64_t j = 0; j < n; ++j)
+    if (colptr[j + 1] < colptr[j]) return false;
+  if (colptr[n] > 1 && !rowval) return false;
+  for (int64_t p = 0; p < colptr[n] - 1; ++p)
+    if (rowval[p] < 1 || rowval[p] > n) return false;
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mfgpu_create(const mfgpu_options* opts, mfgpu_ctx** out) {
+  if (!out) return MFGPU_ERR_ARGUMENT;
+  *out = nullptr;
+  auto* h = new mfgpu_ctx();
+  if (opts) {
+    h->device = opts->device;
+    h->precision = opts->precision;
+  }
+  int rc = guarded(h, [&]() -> int {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= h->device) {
+      cudaGetLastError();
+      return fail(h, MFGPU_ERR_NO_DEVICE, "no CUDA device");
+    }
+    CK(cudaSetDevice(h->device));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, h->device));
+    if (prop.major != 10) return fail(h, MFGPU_ERR_NO_DEVICE, "libmfgpu is built for sm_100a (B200)");
+    CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    h->stream = h->own_stream;
+    CK(cudaEventCreate(&h->ev0));
+    CK(cudaEventCreate(&h->ev1));
+    return MFGPU_OK;
+  });
+  if (rc != MFGPU_OK) {
+    mfgpu_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return MFGPU_OK;
+}
+
+void mfgpu_destroy(mfgpu_ctx* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  DevBuf* bufs[] = {&h->b_c1, &h->b_np, &h->b_nu, &h->b_nf, &h->b_upd_off, &h->b_front_off, &h->b_colbase,
+                    &h->b_child_ptr, &h->b_child_idx, &h->b_upd, &h->b_rel, &h->b_uoff, &h->b_v_src, &h->b_v_srow,
+                    &h->b_v_frow, &h->b_fc_super, &h->b_fc_vbeg, &h->b_fc_vend, &h->b_fc_ch_ptr, &h->b_fc_ch,
+                    &h->b_lcolptr, &h->b_ucolptr, &h->b_qf, &h->b_csr_ptr, &h->b_csr_col, &h->b_csr_src,
+                    &h->b_small, &h->b_panel, &h->b_trsm, &h->b_gemm, &h->b_pool, &h->b_vx, &h->b_ax, &h->b_rs,
+                    &h->b_ipiv, &h->b_info, &h->b_prow, &h->b_rowfac, &h->b_flags, &h->b_li, &h->b_lx, &h->b_ui,
+                    &h->b_ux, &h->b_fsol, &h->b_xw, &h->b_b, &h->b_x, &h->b_r, &h->b_d, &h->b_err, &h->b_norm,
+                    &h->sched.d_ids, &h->sched.d_blocks, &h->sched.d_gemms};
+  for (DevBuf* b : bufs) b->release();
+  for (cudaEvent_t e : h->evpool) cudaEventDestroy(e);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+}
+
+const char* mfgpu_last_error(const mfgpu_ctx* h) { return h ? h->err.c_str() : "null handle"; }
+
+int mfgpu_set_stream(mfgpu_ctx* h, void* s) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  h->stream = s ? (cudaStream_t)s : h->own_stream;
+  return MFGPU_OK;
+}
+
+int mfgpu_set_precision(mfgpu_ctx* h, int32_t p) {
+  if (!h || (p != MFGPU_PRECISION_FP64 && p != MFGPU_PRECISION_MIXED)) return MFGPU_ERR_ARGUMENT;
+  h->precision = p;
+  return MFGPU_OK;
+}
+
+int mfgpu_analyze(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf,
+                  const int64_t* parent, int64_t nsuper, const int64_t* sstart, const int64_t* upd_ptr,
+                  const int64_t* upd_idx) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->device));
+    if (!valid_csc(n, colptr, rowval) || !qf || !parent || !sstart || !upd_ptr || nsuper < 0 ||
+        (upd_ptr[nsuper] > 1 && !upd_idx))
+      return fail(h, MFGPU_ERR_ARGUMENT, "invalid analyze arguments");
+    std::vector<int64_t> cp(n + 1), ri(colptr[n] - 1), q(n), par(n), ss(nsuper + 1), up(nsuper + 1),
+        ui(upd_ptr[nsuper] - 1);
+    for (int64_t j = 0; j <= n; ++j) cp[j] = colptr[j] - 1;
+    for (size_t p = 0; p < ri.size(); ++p) ri[p] = rowval[p] - 1;
+    for (int64_t k = 0; k < n; ++k) {
+      q[k] = qf[k] - 1;
+      par[k] = parent[k] - 1;
+    }
+    for (int64_t s = 0; s <= nsuper; ++s) {
+      ss[s] = sstart[s] - 1;
+      up[s] = upd_ptr[s] - 1;
+    }
+    for (size_t p = 0; p < ui.size(); ++p) ui[p] = upd_idx[p] - 1;
+    return analyze_common(h, n, cp.data(), ri.data(), q.data(), par.data(), nsuper, ss.data(), up.data(), ui.data());
+  });
+}
+
+int mfgpu_analyze_symbolic(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const int64_t* rowval,
+                           const mfgpu_symbolic* sym) {
+  if (!h || !sym || sym->s.n != n) return MFGPU_ERR_ARGUMENT;
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->device));
+    if (!valid_csc(n, colptr, rowval)) return fail(h, MFGPU_ERR_ARGUMENT, "invalid CSC");
+    std::vector<int64_t> cp(n + 1), ri(colptr[n] - 1);
+    for (int64_t j = 0; j <= n; ++j) cp[j] = colptr[j] - 1;
+    for (size_t p = 0; p < ri.size(); ++p) ri[p] = rowval[p] - 1;
+    const auto& s = sym->s;
+    return analyze_common(h, n, cp.data(), ri.data(), s.qf.data(), s.parent.data(), s.nsuper(), s.sstart.data(),
+                          s.upd_ptr.data(), s.upd_idx.data());
+  });
+}
+
+int mfgpu_factor_device(mfgpu_ctx* h, const double* d_nzval, const double* d_rs, int32_t check) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  if (!h->analyzed) return fail(h, MFGPU_ERR_STATE, "factor before analyze");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->device));
+    const Plan& P = h->plan;
+    h->b_ax.ensure(std::max<int64_t>(P.nnz_a, 1) * 8);
+    if (P.nnz_a) CK(cudaMemcpyAsync(h->b_ax.p, d_nzval, P.nnz_a * 8, cudaMemcpyDeviceToDevice, h->stream));
+    h->have_rs = d_rs != nullptr;
+    if (d_rs) {
+      h->b_rs.ensure(std::max<int64_t>(P.n, 1) * 8);
+      CK(cudaMemcpyAsync(h->b_rs.p, d_rs, P.n * 8, cudaMemcpyDeviceToDevice, h->stream));
+    }
+    return factor_dispatch(h, check);
+  });
+}
+
+int mfgpu_factor(mfgpu_ctx* h, const double* nzval, const double* rs, int32_t check) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  if (!h->analyzed) return fail(h, MFGPU_ERR_STATE, "factor before analyze");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->device));
+    const Plan& P = h->plan;
+    h->b_ax.ensure(std::max<int64_t>(P.nnz_a, 1) * 8);
+    if (P.nnz_a) CK(cudaMemcpyAsync(h->b_ax.p, nzval, P.nnz_a * 8, cudaMemcpyHostToDevice, h->stream));
+    h->have_rs = rs != nullptr;
+    if (rs) {
+      h->b_rs.ensure(std::max<int64_t>(P.n, 1) * 8);
+      CK(cudaMemcpyAsync(h->b_rs.p, rs, P.n * 8, cudaMemcpyHostToDevice, h->stream));
+    }
+    return factor_dispatch(h, check);
+  });
+}
+
+int mfgpu_factor_sizes(mfgpu_ctx* h, int64_t* out3) {
+  if (!h || !out3) return MFGPU_ERR_ARGUMENT;
+  if (!h->analyzed) return fail(h, MFGPU_ERR_STATE, "not analyzed");
+  out3[0] = h->plan.n;
+  out3[1] = h->plan.nnz_l;
+  out3[2] = h->plan.nnz_u;
+  return MFGPU_OK;
+}
+
+int mfgpu_get_factors(mfgpu_ctx* h, int64_t* lcolptr, int64_t* lrowval, double* lnzval, int64_t* ucolptr,
+                      int64_t* urowval, double* unzval, int64_t* p, int64_t* q, int64_t* pinv) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  if (!h->factored) return fail(h, MFGPU_ERR_STATE, "no factorization");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->device));
+    const Plan& P = h->plan;
+    cudaStream_t st = h->stream;
+    if (lrowval && P.nnz_l) CK(cudaMemcpyAsync(lrowval, h->b_li.p, P.nnz_l * 8, cudaMemcpyDeviceToHost, st));
+    if (lnzval && P.nnz_l) CK(cudaMemcpyAsync(lnzval, h->b_lx.p, P.nnz_l * 8, cudaMemcpyDeviceToHost, st));
+    if (urowval && P.nnz_u) CK(cudaMemcpyAsync(urowval, h->b_ui.p, P.nnz_u * 8, cudaMemcpyDeviceToHost, st));
+    if (unzval && P.nnz_u) CK(cudaMemcpyAsync(unzval, h->b_ux.p, P.nnz_u * 8, cudaMemcpyDeviceToHost, st));
+    std::vector<int32_t> prow(P.n);
+    if (P.n) CK(cudaMemcpyAsync(prow.data(), h->b_prow.p, P.n * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int64_t j = 0; j <= P.n; ++j) {
+      if (lcolptr) lcolptr[j] = P.lcolptr[j] + 1;
+      if (ucolptr) ucolptr[j] = P.ucolptr[j] + 1;
+    }
+    // p = qf[prow] (src/multifrontal.jl:355-356)
+    for (int64_t k = 0; k < P.n; ++k) {
+      const int64_t pk = P.qf[prow[k]];
+      if (p) p[k] = pk + 1;
+      if (q) q[k] = (int64_t)P.qf[k] + 1;
+      if (pinv) pinv[pk] = k + 1;
+    }
+    return MFGPU_OK;
+  });
+}
+
+int mfgpu_solve_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ldb, double* d_x, int64_t ldx,
+                       int32_t refine) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  if (!h->factored) return fail(h, MFGPU_ERR_STATE, "solve before factor");
+  if (nrhs < 0 || ldb < h->plan.n || ldx < h->plan.n || refine < 0) return fail(h, MFGPU_ERR_ARGUMENT, "bad solve sizes");
+  if (nrhs == 0 || h->plan.n == 0) return MFGPU_OK;
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->device));
+    CK(cudaEventRecord(h->ev0, h->stream));
+    solve_dispatch(h, nrhs, d_b, ldb, d_x, ldx, refine);
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaEventSynchronize(h->ev1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->t_solve_ms = ms;
+    prof_flush(h);
+    return MFGPU_OK;
+  });
+}
+
+int mfgpu_solve(mfgpu_ctx* h, int64_t nrhs, const double* b, int64_t ldb, double* x, int64_t ldx, int32_t refine) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  if (!h->factored) return fail(h, MFGPU_ERR_STATE, "solve before factor");
+  const int64_t n = h->plan.n;
+  if (nrhs < 0 || ldb < n || ldx < n || refine < 0 || (nrhs && (!b || !x)))
+    return fail(h, MFGPU_ERR_ARGUMENT, "bad solve sizes");
+  if (nrhs == 0 || n == 0) return MFGPU_OK;
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    h->b_b.ensure((size_t)n * nrhs * 8);
+    h->b_x.ensure((size_t)n * nrhs * 8);
+    CK(cudaMemcpy2DAsync(h->b_b.p, n * 8, b, ldb * 8, n * 8, nrhs, cudaMemcpyHostToDevice, st));
+    solve_dispatch(h, nrhs, h->b_b.as<double>(), n, h->b_x.as<double>(), n, refine);
+    CK(cudaMemcpy2DAsync(x, ldx * 8, h->b_x.p, n * 8, n * 8, nrhs, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    prof_flush(h);
+    return MFGPU_OK;
+  });
+}
+
+int mfgpu_backward_error_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ldb, const double* d_x,
+                                int64_t ldx, double* out) {
+  if (!h || !out) return MFGPU_ERR_ARGUMENT;
+  if (!h->factored) return fail(h, MFGPU_ERR_STATE, "no matrix values");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->device));
+    const Plan& P = h->plan;
+    cudaStream_t st = h->stream;
+    const int64_t n = P.n;
+    h->b_r.ensure(std::max<size_t>((size_t)n * nrhs * 8, 16));
+    h->b_err.ensure(std::max<size_t>((size_t)nrhs * 3 * 8, 16));
+    h->b_norm.ensure(16);
+    CK(cudaMemsetAsync(h->b_err.p, 0, nrhs * 3 * 8, st));
+    CK(cudaMemsetAsync(h->b_norm.p, 0, 8, st));
+    k_residual<<<grid1(n * nrhs, 256), 256, 0, st>>>(n, nrhs, h->b_csr_ptr.as<int32_t>(), h->b_csr_col.as<int32_t>(),
+                                                     h->b_csr_src.as<int32_t>(), h->b_ax.as<double>(), d_b, ldb, d_x,
+                                                     ldx, h->b_r.as<double>(), n);
+    k_bwd_error_parts<<<grid1(n * nrhs, 256), 256, 0, st>>>(n, nrhs, h->b_r.as<double>(), n, d_x, ldx, d_b, ldb,
+                                                            h->b_err.as<unsigned long long>());
+    k_norm_inf<<<grid1(n, 256), 256, 0, st>>>(n, h->b_csr_ptr.as<int32_t>(), h->b_csr_src.as<int32_t>(),
+                                              h->b_ax.as<double>(), h->b_norm.as<unsigned long long>());
+    CK(cudaGetLastError());
+    std::vector<double> parts(3 * nrhs);
+    double anorm = 0;
+    CK(cudaMemcpyAsync(parts.data(), h->b_err.p, nrhs * 3 * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&anorm, h->b_norm.p, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double worst = 0;
+    for (int64_t c = 0; c < nrhs; ++c) {
+      const double den = anorm * parts[3 * c + 1] + parts[3 * c + 2];
+      const double eta = den > 0 ? parts[3 * c] / den : 0.0;
+      worst = std::max(worst, eta);
+    }
+    *out = worst;
+    return MFGPU_OK;
+  });
+}
+
+int mfgpu_stats_json(mfgpu_ctx* h, char* buf, int64_t cap) {
+  if (!h || !buf || cap <= 0) return MFGPU_ERR_ARGUMENT;
+  const Plan& P = h->plan;
+  int64_t nl = 0, nsmall = 0;
+  for (const auto& l : P.launches) {
+    ++nl;
+    if (l.kind == kLaunchSmall) nsmall += l.count;
+  }
+  char tmp[2048];
+  std::snprintf(tmp, sizeof tmp,
+                "{\"n\": %lld, \"nsuper\": %lld, \"levels\": %d, \"nnz_l\": %lld, \"nnz_u\": %lld, "
+                "\"max_front\": %d, \"max_pivots\": %d, \"front_elems\": %lld, \"flops\": %.6e, "
+                "\"flops_getrf\": %.6e, \"flops_trsm\": %.6e, \"flops_gemm\": %.6e, \"assembly_elem_moves\": %.6e, "
+                "\"factor_launches\": %lld, \"small_fronts\": %lld, \"speculative\": %s, \"safe_rerun\": %d, "
+                "\"analyze_ms\": %.3f, \"factor_ms\": %.3f, \"solve_ms\": %.3f, \"precision\": \"%s\", "
+                "\"status\": %d}",
+                (long long)P.n, (long long)P.ns, P.nlevels, (long long)P.nnz_l, (long long)P.nnz_u, P.max_nf,
+                P.max_np, (long long)P.front_elems, P.flops, P.flops_getrf, P.flops_trsm, P.flops_gemm,
+                P.assembly_bytes_per_elem, (long long)nl, (long long)nsmall, P.has_speculative ? "true" : "false",
+                h->factor_reruns, h->t_analyze_ms, h->t_factor_ms, h->t_solve_ms,
+                h->factor_precision == MFGPU_PRECISION_MIXED ? "mixed" : "fp64", h->last_status);
+  std::string js(tmp);
+  js.pop_back();   // reopen the object
+  char item[512];
+  std::snprintf(item, sizeof item, ", \"launches\": %lld, \"profiling\": %s, \"kernels\": {", (long long)h->launch_count,
+                h->profiling ? "true" : "false");
+  js += item;
+  bool first = true;
+  for (int k = 0; k < KC_COUNT; ++k) {
+    const KStat& ks = h->kstat[k];
+    if (!ks.launches) continue;
+    std::snprintf(item, sizeof item, "%s\"%s\": {\"ms\": %.6f, \"launches\": %lld, \"flops\": %.6e, \"bytes\": %.6e}",
+                  first ? "" : ", ", kKernelClassName[k], ks.ms, (long long)ks.launches, ks.flops, ks.bytes);
+    js += item;
+    first = false;
+  }
+  js += "}}";
+  if ((int64_t)js.size() >= cap) return MFGPU_ERR_ARGUMENT;
+  std::memcpy(buf, js.c_str(), js.size() + 1);
+  return MFGPU_OK;
+}
+
+int mfgpu_set_profiling(mfgpu_ctx* h, int32_t on) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  h->profiling = on != 0;
+  h->launch_count = 0;
+  for (auto& k : h->kstat) k = KStat{};
+  h->pending.clear();
+  h->evnext = 0;
+  return MFGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,419 @@
+// plan.cpp -- pattern analysis for the device factorization (see plan.h).
+
+#include "plan.h"
+
+#include <algorithm>
+#include <numeric>
+#include <stdexcept>
+
+namespace mfgpu {
+
+namespace {
+inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+}  // namespace
+
+void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf, const int64_t* parent,
+                int64_t ns, const int64_t* sstart, const int64_t* upd_ptr, const int64_t* upd_idx, Plan& P) {
+  P = Plan();
+  P.n = n;
+  P.ns = ns;
+  P.nnz_a = colptr[n];
+  if (P.nnz_a >= (int64_t(1) << 31)) throw std::invalid_argument("nnz(A) exceeds the 32-bit entry maps");
+  if (ns < 0 || (n > 0 && ns == 0) || sstart[0] != 0 || sstart[ns] != n)
+    throw std::invalid_argument("supernode partition does not cover 1:n");
+
+  // ---- supernodes -----------------------------------------------------------
+  std::vector<int32_t> super_of(n);
+  P.c1.resize(ns); P.np.resize(ns); P.nu.resize(ns); P.nf.resize(ns);
+  P.upd_off.resize(ns + 1);
+  for (int64_t s = 0; s < ns; ++s) {
+    if (sstart[s + 1] <= sstart[s]) throw std::invalid_argument("empty supernode");
+    P.c1[s] = (int32_t)sstart[s];
+    P.np[s] = (int32_t)(sstart[s + 1] - sstart[s]);
+    P.nu[s] = (int32_t)(upd_ptr[s + 1] - upd_ptr[s]);
+    P.nf[s] = P.np[s] + P.nu[s];
+    P.upd_off[s] = upd_ptr[s];
+    for (int64_t j = sstart[s]; j < sstart[s + 1]; ++j) super_of[j] = (int32_t)s;
+    P.max_nf = std::max(P.max_nf, P.nf[s]);
+    P.max_np = std::max(P.max_np, P.np[s]);
+  }
+  P.upd_off[ns] = upd_ptr[ns];
+  P.upd.resize(upd_ptr[ns]);
+  for (int64_t s = 0; s < ns; ++s) {
+    const int64_t c2 = sstart[s + 1] - 1;
+    for (int64_t p = upd_ptr[s]; p < upd_ptr[s + 1]; ++p) {
+      if (upd_idx[p] <= c2 || upd_idx[p] >= n || (p > upd_ptr[s] && upd_idx[p] <= upd_idx[p - 1]))
+        throw std::invalid_argument("update set must be sorted rows below the supernode");
+      P.upd[p] = (int32_t)upd_idx[p];
+    }
+  }
+
+  // children (ascending) and tree heights
+  P.parent_super.assign(ns, -1);
+  std::vector<int32_t> nkid(ns + 1, 0);
+  for (int64_t s = 0; s < ns; ++s) {
+    const int64_t pc = parent[sstart[s + 1] - 1];
+    if (pc >= 0) {
+      const int32_t ps = super_of[pc];
+      if (ps <= s) throw std::invalid_argument("supernodes are not in postorder");
+      if (P.nu[s] == 0 || P.upd[P.upd_off[s]] != pc) throw std::invalid_argument("parent is not the first update row");
+      P.parent_super[s] = ps;
+      ++nkid[ps + 1];
+    } else if (P.nu[s] != 0) {
+      throw std::invalid_argument("root supernode with a nonempty update set");
+    }
+  }
+  P.child_ptr.assign(ns + 1, 0);
+  for (int64_t s = 0; s < ns; ++s) P.child_ptr[s + 1] = P.child_ptr[s] + nkid[s + 1];
+  P.child_idx.resize(P.child_ptr[ns]);
+  {
+    std::vector<int32_t> cur(P.child_ptr.begin(), P.child_ptr.end() - 1);
+    for (int64_t s = 0; s < ns; ++s)
+      if (P.parent_super[s] >= 0) P.child_idx[cur[P.parent_super[s]]++] = (int32_t)s;
+  }
+  P.height.assign(ns, 0);
+  for (int64_t s = 0; s < ns; ++s)
+    if (P.parent_super[s] >= 0) P.height[P.parent_super[s]] = std::max(P.height[P.parent_super[s]], P.height[s] + 1);
+  P.nlevels = ns ? 1 + *std::max_element(P.height.begin(), P.height.end()) : 0;
+
+  // relative maps: position of each child update row in the parent front
+  P.rel.assign(P.upd.size(), -1);
+  for (int64_t k = 0; k < ns; ++k) {
+    const int32_t ps = P.parent_super[k];
+    if (ps < 0) continue;
+    const int32_t pc1 = P.c1[ps], pc2 = P.c1[ps] + P.np[ps] - 1;
+    const int32_t* pu = P.upd.data() + P.upd_off[ps];
+    for (int64_t p = P.upd_off[k]; p < P.upd_off[k + 1]; ++p) {
+      const int32_t g = P.upd[p];
+      if (g < pc1) throw std::invalid_argument("child update row below its parent");
+      if (g <= pc2) {
+        P.rel[p] = g - pc1;
+      } else {
+        const int32_t* it = std::lower_bound(pu, pu + P.nu[ps], g);
+        if (it == pu + P.nu[ps] || *it != g) throw std::invalid_argument("child update row missing from parent front");
+        P.rel[p] = P.np[ps] + (int32_t)(it - pu);
+      }
+    }
+  }
+
+  // ---- slots: supernodes ordered by (height, small before large, id) -------
+  P.slot_super.resize(ns);
+  std::iota(P.slot_super.begin(), P.slot_super.end(), 0);
+  std::stable_sort(P.slot_super.begin(), P.slot_super.end(), [&](int32_t a, int32_t b) {
+    if (P.height[a] != P.height[b]) return P.height[a] < P.height[b];
+    const bool la = P.nf[a] > kSmallFront, lb = P.nf[b] > kSmallFront;
+    return la < lb;
+  });
+  P.slot.resize(ns);
+  P.level_slot.assign(P.nlevels + 1, 0);
+  P.level_large.assign(P.nlevels, 0);
+  for (int64_t i = 0; i < ns; ++i) P.slot[P.slot_super[i]] = (int32_t)i;
+  for (int64_t i = 0; i < ns; ++i) P.level_slot[P.height[P.slot_super[i]] + 1] = (int32_t)(i + 1);
+  for (int32_t L = 0; L < P.nlevels; ++L) {
+    P.level_slot[L + 1] = std::max(P.level_slot[L + 1], P.level_slot[L]);
+    int32_t i = P.level_slot[L];
+    while (i < P.level_slot[L + 1] && P.nf[P.slot_super[i]] <= kSmallFront) ++i;
+    P.level_large[L] = i;
+  }
+  P.front_off.resize(ns);
+  P.colbase.resize(ns + 1);
+  int64_t fo = 0, cb = 0;
+  for (int64_t i = 0; i < ns; ++i) {
+    const int32_t s = P.slot_super[i];
+    P.front_off[s] = fo;
+    P.colbase[s] = cb;
+    fo += (int64_t)P.nf[s] * P.nf[s];
+    cb += P.nf[s];
+  }
+  P.colbase[ns] = cb;   // sentinel: total front columns (not indexed by supernode)
+  P.front_elems = fo;
+  P.fc_total = cb;
+  P.fc_super.resize(cb);
+  for (int64_t s = 0; s < ns; ++s)
+    for (int32_t c = 0; c < P.nf[s]; ++c) P.fc_super[P.colbase[s] + c] = (int32_t)s;
+
+  // ---- V = A[qf, qf] and the assembly map of its entries --------------------
+  P.qf.resize(n);
+  std::vector<int64_t> pinv(n, -1);
+  for (int64_t k = 0; k < n; ++k) {
+    if (qf[k] < 0 || qf[k] >= n || pinv[qf[k]] != -1) throw std::invalid_argument("qf is not a permutation");
+    pinv[qf[k]] = k;
+    P.qf[k] = (int32_t)qf[k];
+  }
+  const int64_t nz = P.nnz_a;
+  std::vector<int64_t> vcol(n + 1, 0);
+  for (int64_t g = 0; g < n; ++g) vcol[g + 1] = vcol[g] + (colptr[qf[g] + 1] - colptr[qf[g]]);
+  P.v_src.resize(nz);
+  P.v_srow.resize(nz);
+  P.v_frow.assign(nz, -1);
+  std::vector<int32_t> vrow(nz);
+  {
+    std::vector<std::pair<int64_t, int64_t>> tmp;
+    for (int64_t g = 0; g < n; ++g) {
+      tmp.clear();
+      for (int64_t p = colptr[qf[g]]; p < colptr[qf[g] + 1]; ++p) tmp.push_back({pinv[rowval[p]], p});
+      std::sort(tmp.begin(), tmp.end());
+      for (size_t t = 0; t < tmp.size(); ++t) {
+        if (t && tmp[t].first == tmp[t - 1].first) throw std::invalid_argument("duplicate entries in A");
+        const int64_t q = vcol[g] + (int64_t)t;
+        vrow[q] = (int32_t)tmp[t].first;
+        P.v_src[q] = (int32_t)tmp[t].second;
+        P.v_srow[q] = (int32_t)rowval[tmp[t].second];
+      }
+    }
+  }
+  P.fc_vbeg.assign(cb, 0);
+  P.fc_vend.assign(cb, 0);
+  int64_t assigned = 0;
+  for (int64_t s = 0; s < ns; ++s) {
+    const int32_t c1 = P.c1[s], c2 = c1 + P.np[s] - 1, npv = P.np[s];
+    const int32_t* us = P.upd.data() + P.upd_off[s];
+    auto front_row = [&](int32_t i) -> int32_t {
+      if (i <= c2) return i - c1;
+      const int32_t* it = std::lower_bound(us, us + P.nu[s], i);
+      if (it == us + P.nu[s] || *it != i) throw std::invalid_argument("entry of A outside the symbolic structure");
+      return npv + (int32_t)(it - us);
+    };
+    for (int32_t c = 0; c < P.nf[s]; ++c) {
+      const int32_t g = c < npv ? c1 + c : us[c - npv];
+      const int32_t* rb = vrow.data() + vcol[g];
+      const int32_t* re = vrow.data() + vcol[g + 1];
+      const int32_t* lo = std::lower_bound(rb, re, c1);
+      const int32_t* hi = c < npv ? re : std::upper_bound(lo, re, c2);
+      const int64_t fc = P.colbase[s] + c;
+      P.fc_vbeg[fc] = (int32_t)(vcol[g] + (lo - rb));
+      P.fc_vend[fc] = (int32_t)(vcol[g] + (hi - rb));
+      for (const int32_t* r = lo; r < hi; ++r) {
+        const int64_t q = vcol[g] + (r - rb);
+        if (P.v_frow[q] != -1) throw std::logic_error("V entry assembled twice");
+        P.v_frow[q] = front_row(*r);
+        ++assigned;
+      }
+    }
+  }
+  if (assigned != nz) throw std::invalid_argument("pattern of A is not covered by the symbolic structure");
+
+  // ---- children contributions per parent front column ------------------------
+  P.fc_ch_ptr.assign(cb + 1, 0);
+  for (int64_t k = 0; k < ns; ++k) {
+    const int32_t ps = P.parent_super[k];
+    if (ps < 0) continue;
+    for (int64_t p = P.upd_off[k]; p < P.upd_off[k + 1]; ++p) ++P.fc_ch_ptr[P.colbase[ps] + P.rel[p] + 1];
+  }
+  for (int64_t f = 0; f < cb; ++f) P.fc_ch_ptr[f + 1] += P.fc_ch_ptr[f];
+  P.fc_ch.resize(2 * (size_t)P.fc_ch_ptr[cb]);
+  {
+    std::vector<int32_t> cur(P.fc_ch_ptr.begin(), P.fc_ch_ptr.end() - 1);
+    for (int64_t ps = 0; ps < ns; ++ps) {
+      for (int32_t ci = P.child_ptr[ps + 1] - 1; ci >= P.child_ptr[ps]; --ci) {   // last child first
+        const int32_t k = P.child_idx[ci];
+        for (int32_t t = 0; t < P.nu[k]; ++t) {
+          const int64_t f = P.colbase[ps] + P.rel[P.upd_off[k] + t];
+          const int32_t at = cur[f]++;
+          P.fc_ch[2 * (size_t)at] = k;
+          P.fc_ch[2 * (size_t)at + 1] = t;
+        }
+      }
+    }
+  }
+
+  // ---- factor CSC layout -------------------------------------------------
+  P.lcolptr.assign(n + 1, 0);
+  P.ucolptr.assign(n + 1, 0);
+  for (int64_t s = 0; s < ns; ++s) {
+    const int32_t c1 = P.c1[s], c2 = c1 + P.np[s] - 1;
+    for (int32_t j = c1; j <= c2; ++j) {
+      P.lcolptr[j + 1] = 1 + (c2 - j) + P.nu[s];
+      P.ucolptr[j + 1] += j - c1 + 1;
+    }
+    for (int64_t p = P.upd_off[s]; p < P.upd_off[s + 1]; ++p) P.ucolptr[P.upd[p] + 1] += P.np[s];
+  }
+  for (int64_t j = 0; j < n; ++j) {
+    P.lcolptr[j + 1] += P.lcolptr[j];
+    P.ucolptr[j + 1] += P.ucolptr[j];
+  }
+  P.nnz_l = P.lcolptr[n];
+  P.nnz_u = P.ucolptr[n];
+  P.uoff.resize(P.upd.size());
+  {
+    std::vector<int64_t> cur(P.ucolptr.begin(), P.ucolptr.end() - 1);
+    for (int64_t s = 0; s < ns; ++s)
+      for (int64_t p = P.upd_off[s]; p < P.upd_off[s + 1]; ++p) {
+        P.uoff[p] = cur[P.upd[p]];
+        cur[P.upd[p]] += P.np[s];
+      }
+  }
+
+  // ---- A in CSR (residual r = b - A x) ------------------------------------
+  P.csr_ptr.assign(n + 1, 0);
+  for (int64_t p = 0; p < nz; ++p) ++P.csr_ptr[rowval[p] + 1];
+  for (int64_t i = 0; i < n; ++i) P.csr_ptr[i + 1] += P.csr_ptr[i];
+  P.csr_col.resize(nz);
+  P.csr_src.resize(nz);
+  {
+    std::vector<int32_t> cur(P.csr_ptr.begin(), P.csr_ptr.end() - 1);
+    for (int64_t j = 0; j < n; ++j)
+      for (int64_t p = colptr[j]; p < colptr[j + 1]; ++p) {
+        const int32_t at = cur[rowval[p]]++;
+        P.csr_col[at] = (int32_t)j;
+        P.csr_src[at] = (int32_t)p;
+      }
+  }
+
+  // ---- statistics ------------------------------------------------------------
+  for (int64_t s = 0; s < ns; ++s) {
+    const double a = P.np[s], u = P.nu[s];
+    P.flops_getrf += 2.0 / 3.0 * a * a * a;
+    P.flops_trsm += 2.0 * a * a * u;
+    P.flops_gemm += 2.0 * a * u * u;
+    double moves = (double)P.nf[s] * P.nf[s] + u * u;   // front write + CB handed on
+    for (int32_t ci = P.child_ptr[s]; ci < P.child_ptr[s + 1]; ++ci) {
+      const double m = P.nu[P.child_idx[ci]];
+      moves += 3.0 * m * m;                             // CB read + parent read-modify-write
+    }
+    P.assembly_bytes_per_elem += moves;
+  }
+  P.flops = P.flops_getrf + P.flops_trsm + P.flops_gemm;
+  build_launches(P, false);
+}
+
+namespace {
+// Algorithmic traffic of assembling front s: the zero-filled front written
+// once, each child's contribution block read once and added into the parent
+// (read-modify-write), and the original entries (value + 4-byte row).
+void assembly_work(const Plan& P, int32_t s, Launch& l) {
+  double e = (double)P.nf[s] * P.nf[s];
+  for (int32_t ci = P.child_ptr[s]; ci < P.child_ptr[s + 1]; ++ci) {
+    const double m = P.nu[P.child_idx[ci]];
+    e += 3.0 * m * m;
+  }
+  l.elems += e;
+  int64_t nv = 0;
+  for (int32_t c = 0; c < P.nf[s]; ++c) nv += P.fc_vend[P.colbase[s] + c] - P.fc_vbeg[P.colbase[s] + c];
+  l.extra_bytes += 12.0 * nv;
+}
+// Small fronts: assembly plus the dense factorization in shared memory.
+void front_work(const Plan& P, int32_t s, Launch& l) {
+  assembly_work(P, s, l);
+  const double a = P.np[s], u = P.nu[s];
+  l.flops += 2.0 / 3.0 * a * a * a + 2.0 * a * a * u + 2.0 * a * u * u;
+}
+}  // namespace
+
+void build_launches(Plan& P, bool safe) {
+  P.small_tasks.clear();
+  P.panel_tasks.clear();
+  P.trsm_tasks.clear();
+  P.gemm_tasks.clear();
+  P.launches.clear();
+  P.has_speculative = false;
+  std::vector<int32_t> large;
+  for (int32_t L = 0; L < P.nlevels; ++L) {
+    // fused small fronts
+    if (P.level_large[L] > P.level_slot[L]) {
+      Launch l{kLaunchSmall, L, (int64_t)P.small_tasks.size(), P.level_large[L] - P.level_slot[L], 0};
+      for (int32_t i = P.level_slot[L]; i < P.level_large[L]; ++i) {
+        const int32_t s = P.slot_super[i];
+        P.small_tasks.push_back(s);
+        front_work(P, s, l);
+      }
+      l.tiles = l.count;
+      P.launches.push_back(l);
+    }
+    if (P.level_slot[L + 1] == P.level_large[L]) continue;
+    large.assign(P.slot_super.begin() + P.level_large[L], P.slot_super.begin() + P.level_slot[L + 1]);
+    const int64_t fc0 = P.colbase[large.front()];
+    const int64_t fc1 = P.colbase[large.back()] + P.nf[large.back()];
+    {
+      Launch la{kLaunchAssemble, L, fc0, fc1 - fc0, fc1 - fc0};
+      for (int32_t s : large) assembly_work(P, s, la);
+      P.launches.push_back(la);
+    }
+    int32_t maxnp = 0;
+    for (int32_t s : large) maxnp = std::max(maxnp, P.np[s]);
+    for (int32_t k0 = 0; k0 < maxnp; k0 += kPanel) {
+      Launch lp{kLaunchPanel, L, (int64_t)P.panel_tasks.size(), 0, 0};
+      Launch lt{kLaunchTrsm, L, (int64_t)P.trsm_tasks.size(), 0, 0};
+      Launch lg{kLaunchGemm, L, (int64_t)P.gemm_tasks.size(), 0, 0};
+      for (int32_t s : large) {
+        const int32_t npv = P.np[s], nf = P.nf[s];
+        if (npv <= k0) continue;
+        const int32_t kb = std::min(kPanel, npv - k0), k1 = k0 + kb;
+        int32_t mode = (npv - k0 <= kPivRowsSmem) ? kPanelSmemPivot : (safe ? kPanelGlobalPivot : kPanelSpeculative);
+        if (mode == kPanelSpeculative) P.has_speculative = true;
+        P.panel_tasks.push_back(PanelTask{s, k0, mode, 0});
+        ++lp.count;
+        {
+          const double R = (mode == kPanelSpeculative) ? kb : (npv - k0);
+          lp.flops += R * kb * kb - kb * kb * kb / 3.0;
+          lp.elems += 2.0 * R * kb;
+        }
+        TrsmTask tt{};
+        tt.s = s;
+        tt.k0 = k0;
+        tt.r0 = (mode == kPanelSpeculative) ? k1 : npv;
+        tt.lrow_tiles = (int32_t)ceil_div(nf - tt.r0, 64);
+        tt.ucol_tiles = (int32_t)ceil_div(nf - k1, 64);
+        tt.check = (mode == kPanelSpeculative) ? 1 : 0;
+        if (tt.lrow_tiles + tt.ucol_tiles > 0) {
+          lt.flops += (double)(nf - tt.r0) * kb * kb + (double)(nf - k1) * kb * kb;
+          lt.elems += 2.0 * ((double)(nf - tt.r0) * kb + (double)(nf - k1) * kb);
+          tt.tile_base = lt.tiles;
+          lt.tiles += tt.lrow_tiles + tt.ucol_tiles;
+          P.trsm_tasks.push_back(tt);
+          ++lt.count;
+        }
+        const int64_t base = P.front_off[s];
+        auto add_gemm = [&](int64_t a, int64_t b, int64_t c, int32_t m, int32_t n, int32_t k) {
+          if (m <= 0 || n <= 0 || k <= 0) return;
+          GemmTask g{};
+          g.a = a; g.b = b; g.c = c;
+          g.m = m; g.n = n; g.k = k;
+          g.lda = g.ldb = g.ldc = nf;
+          g.tiles_m = (int32_t)ceil_div(m, 64);
+          g.tiles_n = (int32_t)ceil_div(n, 64);
+          g.tile_base = lg.tiles;
+          lg.tiles += (int64_t)g.tiles_m * g.tiles_n;
+          lg.flops += 2.0 * m * n * k;
+          lg.elems += 2.0 * m * n + (double)m * k + (double)k * n;
+          P.gemm_tasks.push_back(g);
+          ++lg.count;
+        };
+        if (npv > k1) {
+          add_gemm(base + k1 + (int64_t)k0 * nf, base + k0 + (int64_t)k1 * nf, base + k1 + (int64_t)k1 * nf, nf - k1,
+                   npv - k1, kb);
+          add_gemm(base + k1 + (int64_t)k0 * nf, base + k0 + (int64_t)npv * nf, base + k1 + (int64_t)npv * nf,
+                   npv - k1, nf - npv, kb);
+        }
+      }
+      lp.tiles = lp.count;
+      if (lp.count) P.launches.push_back(lp);
+      if (lt.count) P.launches.push_back(lt);
+      if (lg.count) P.launches.push_back(lg);
+    }
+    // deferred Schur update of every large front: F22 -= L21 * U12
+    Launch lg{kLaunchGemm, L, (int64_t)P.gemm_tasks.size(), 0, 0};
+    for (int32_t s : large) {
+      const int32_t npv = P.np[s], nu = P.nu[s], nf = P.nf[s];
+      if (nu == 0) continue;
+      const int64_t base = P.front_off[s];
+      GemmTask g{};
+      g.a = base + npv;
+      g.b = base + (int64_t)npv * nf;
+      g.c = base + npv + (int64_t)npv * nf;
+      g.m = nu; g.n = nu; g.k = npv;
+      g.lda = g.ldb = g.ldc = nf;
+      g.tiles_m = (int32_t)ceil_div(nu, 64);
+      g.tiles_n = (int32_t)ceil_div(nu, 64);
+      g.tile_base = lg.tiles;
+      lg.tiles += (int64_t)g.tiles_m * g.tiles_n;
+      lg.flops += 2.0 * nu * nu * npv;
+      lg.elems += 2.0 * nu * nu + 2.0 * nu * npv;
+      P.gemm_tasks.push_back(g);
+      ++lg.count;
+    }
+    if (lg.count) P.launches.push_back(lg);
+  }
+}
+
+}  // namespace mfgpu

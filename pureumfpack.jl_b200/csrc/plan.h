@@ -1,0 +1,128 @@
+// plan.h -- pattern-only analysis that turns a symbolic factorization into
+// the device schedule of libmfgpu's numeric factorization and solves.
+//
+// Everything here depends on the sparsity pattern only (the part of
+// src/multifrontal.jl:152-196 that does not touch values): front sizes and
+// pool offsets, the map of every entry of V = A[qf,qf] to its front position
+// (src/multifrontal.jl:217-231), the extend-add maps of every child
+// contribution block (src/multifrontal.jl:45-57, 235-243), the CSC offsets
+// of the factors (src/multifrontal.jl:73-104, 278-317), and the level-batched
+// launch sequence.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace mfgpu {
+
+// Front size limits of the kernel classes.
+constexpr int kSmallFront = 64;      // fronts with nf <= this are factored in one CTA, in shared memory
+constexpr int kPanel = 64;           // panel width of the blocked large-front factorization
+constexpr int kPivRowsSmem = 256;    // pivot rows a partial-pivoting panel keeps in shared memory
+
+enum PanelMode : int32_t {
+  kPanelSmemPivot = 0,   // rows k0..np-1 in shared memory, LAPACK partial pivoting
+  kPanelSpeculative = 1, // diagonal block only, no interchanges, exact pivot-order check
+  kPanelGlobalPivot = 2  // rows k0..np-1 in global memory, LAPACK partial pivoting
+};
+
+struct PanelTask {       // one panel step of one large front
+  int32_t s;             // supernode
+  int32_t k0;            // first panel column
+  int32_t mode;          // PanelMode
+  int32_t pad;
+};
+
+struct TrsmTask {        // triangular solves of one panel step
+  int32_t s, k0;
+  int32_t r0;            // first row of the L-part solve (k0+kb or np)
+  int32_t lrow_tiles;    // 64-row tiles of the L part
+  int32_t ucol_tiles;    // 64-column tiles of the U part
+  int32_t check;         // speculative: check pivot order on rows < np
+  int64_t tile_base;     // prefix over tasks
+};
+
+struct GemmTask {        // C -= A * B, column-major, offsets in elements of the front pool
+  int64_t a, b, c;
+  int32_t m, n, k;
+  int32_t lda, ldb, ldc;
+  int32_t tiles_m, tiles_n;
+  int32_t pad;
+  int64_t tile_base;
+};
+
+enum LaunchKind : int32_t {
+  kLaunchSmall = 0,      // fused assemble + factor of small fronts (tasks: supernode ids)
+  kLaunchAssemble = 1,   // column-wise assembly of large fronts (front-column range)
+  kLaunchPanel = 2,
+  kLaunchTrsm = 3,
+  kLaunchGemm = 4
+};
+
+struct Launch {
+  int32_t kind;
+  int32_t level;
+  int64_t first;         // offset into the task array of this kind (or fc begin)
+  int64_t count;         // tasks (or fc count)
+  int64_t tiles;         // grid size in tiles for TRSM / GEMM
+  double flops = 0;      // algorithmic flops of the launch
+  double elems = 0;      // algorithmic element moves (x sizeof(front type) = bytes)
+  double extra_bytes = 0;// index / FP64 input bytes
+};
+
+struct Plan {
+  int64_t n = 0, ns = 0, nnz_a = 0;
+  // per supernode (postorder id)
+  std::vector<int32_t> c1, np, nu, nf, height, slot;
+  std::vector<int64_t> upd_off, front_off, colbase;
+  std::vector<int32_t> child_ptr, child_idx, parent_super;
+  // per update-set entry (parallel arrays, sum of nu entries)
+  std::vector<int32_t> upd;           // V index of the update row/column
+  std::vector<int32_t> rel;           // its position in the parent's front
+  std::vector<int64_t> uoff;          // 0-based offset of this (supernode, column) block in U's CSC
+  // V = A[qf, qf] built from A's values
+  std::vector<int32_t> v_src;         // A.nzval index of each V entry
+  std::vector<int32_t> v_srow;        // original row (for Rs)
+  std::vector<int32_t> v_frow;        // front row of each V entry
+  // per front column, in slot order
+  std::vector<int32_t> fc_super;      // owning supernode
+  std::vector<int32_t> fc_vbeg, fc_vend;  // V entries assembled into this column
+  std::vector<int32_t> fc_ch_ptr;     // children contributions (child, child column)
+  std::vector<int32_t> fc_ch;         // pairs, flattened
+  int64_t fc_total = 0;
+  int64_t front_elems = 0;
+  // levels / slots
+  int32_t nlevels = 0;
+  std::vector<int32_t> slot_super;
+  std::vector<int32_t> level_slot;    // nlevels+1
+  std::vector<int32_t> level_large;   // first large slot of each level
+  // factor CSC (0-based pointers)
+  std::vector<int64_t> lcolptr, ucolptr;
+  int64_t nnz_l = 0, nnz_u = 0;
+  // qf (0-based) and original A in CSR for the residual
+  std::vector<int32_t> qf;
+  std::vector<int32_t> csr_ptr, csr_col, csr_src;
+  // launch sequences
+  std::vector<int32_t> small_tasks;
+  std::vector<PanelTask> panel_tasks;
+  std::vector<TrsmTask> trsm_tasks;
+  std::vector<GemmTask> gemm_tasks;
+  std::vector<Launch> launches;
+  bool has_speculative = false;
+  // statistics
+  double flops = 0, flops_getrf = 0, flops_trsm = 0, flops_gemm = 0;
+  double assembly_bytes_per_elem = 0;  // sum of nf^2 + 3 m^2 + nu^2 element moves (x sizeof(T) for bytes)
+  int32_t max_nf = 0, max_np = 0;
+};
+
+// Build the plan.  All inputs 0-based: A pattern (n x n CSC), qf, parent
+// (-1 = root), sstart (ns+1), upd_ptr (ns+1), upd_idx.
+// `safe` replaces speculative panels by global-memory partial pivoting.
+void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf, const int64_t* parent,
+                int64_t ns, const int64_t* sstart, const int64_t* upd_ptr, const int64_t* upd_idx, Plan& plan);
+
+// (Re)build the launch sequence: speculative panels, or only pivoting ones.
+void build_launches(Plan& plan, bool safe);
+
+}  // namespace mfgpu

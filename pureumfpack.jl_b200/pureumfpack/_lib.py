@@ -1,0 +1,86 @@
+"""ctypes binding of libmfgpu.so (declarations in include/mfgpu.h).
+
+The library is required: there is no CPU fallback for the numeric phase, so
+importing a GPU entry point without the built library raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmfgpu.so")
+
+i64 = ctypes.c_int64
+i32 = ctypes.c_int32
+f64 = ctypes.c_double
+vp = ctypes.c_void_p
+i64p = ctypes.POINTER(ctypes.c_int64)
+f64p = ctypes.POINTER(ctypes.c_double)
+cp = ctypes.c_char_p
+
+# (name, restype, argtypes) for every symbol of include/mfgpu.h
+SIGNATURES = [
+    ("mfgpu_row_scaling", ctypes.c_int, [i64, i64p, i64p, f64p, i32, f64p]),
+    ("mfgpu_amd_order", ctypes.c_int, [i64, i64p, i64p, f64, i64p]),
+    ("mfgpu_colamd_order", ctypes.c_int, [i64, i64, i64p, i64p, f64, i64p]),
+    ("mfgpu_symbolic_create", ctypes.c_int, [i64, i64p, i64p, i64p, ctypes.POINTER(vp)]),
+    ("mfgpu_symbolic_destroy", None, [vp]),
+    ("mfgpu_symbolic_sizes", ctypes.c_int, [vp, i64p]),
+    ("mfgpu_symbolic_get", ctypes.c_int, [vp, i64p, i64p, i64p, i64p, i64p, i64p, i64p, i64p]),
+    ("mfgpu_symbolic_predicted_fill", i64, [vp]),
+    ("mfgpu_factor_colptrs", ctypes.c_int, [vp, i64p, i64p]),
+    ("mfgpu_host_last_error", cp, []),
+    ("mfgpu_create", ctypes.c_int, [vp, ctypes.POINTER(vp)]),
+    ("mfgpu_destroy", None, [vp]),
+    ("mfgpu_last_error", cp, [vp]),
+    ("mfgpu_set_stream", ctypes.c_int, [vp, vp]),
+    ("mfgpu_set_precision", ctypes.c_int, [vp, i32]),
+    ("mfgpu_analyze", ctypes.c_int, [vp, i64, i64p, i64p, i64p, i64p, i64, i64p, i64p, i64p]),
+    ("mfgpu_analyze_symbolic", ctypes.c_int, [vp, i64, i64p, i64p, vp]),
+    ("mfgpu_factor", ctypes.c_int, [vp, f64p, f64p, i32]),
+    ("mfgpu_factor_device", ctypes.c_int, [vp, vp, vp, i32]),
+    ("mfgpu_factor_sizes", ctypes.c_int, [vp, i64p]),
+    ("mfgpu_get_factors", ctypes.c_int, [vp, i64p, i64p, f64p, i64p, i64p, f64p, i64p, i64p, i64p]),
+    ("mfgpu_solve", ctypes.c_int, [vp, i64, f64p, i64, f64p, i64, i32]),
+    ("mfgpu_solve_device", ctypes.c_int, [vp, i64, vp, i64, vp, i64, i32]),
+    ("mfgpu_backward_error_device", ctypes.c_int, [vp, i64, vp, i64, vp, i64, f64p]),
+    ("mfgpu_stats_json", ctypes.c_int, [vp, ctypes.c_char_p, i64]),
+    ("mfgpu_set_profiling", ctypes.c_int, [vp, i32]),
+]
+
+_lib = None
+
+
+class LibraryMissing(RuntimeError):
+    pass
+
+
+def lib():
+    """Load libmfgpu.so (built by pureumfpack.jl_b200/build.py)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise LibraryMissing(
+                f"{LIB_PATH} is not built; run `python pureumfpack.jl_b200/build.py` "
+                "(there is no CPU fallback for the numeric factorization)"
+            )
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class MfOptions(ctypes.Structure):
+    _fields_ = [("device", i32), ("precision", i32), ("flags", i32), ("reserved", i32)]
+
+
+def ptr(a, ty=i64p):
+    """ctypes pointer to a contiguous numpy array (None passes NULL)."""
+    if a is None:
+        return None
+    return a.ctypes.data_as(ty)

@@ -1,0 +1,442 @@
+"""The reference's public API for the multifrontal path, over libmfgpu.
+
+Mirrors PureUMFPACK.jl (names, argument meaning, errors):
+
+* ``splu(A; method=:multifrontal, ordering, tol, scale, check)`` -> ``PureLU``
+  (src/interface.jl:93-120)
+* ``multifrontal_lu(A; q, tol, check)`` -> ``GPLUFactorization``
+  (src/multifrontal.jl:146-358)
+* ``solve(F, b; refine)`` (src/interface.jl:170-177), ``F \\ b`` as
+  ``F.ldiv(b)`` / ``solve(F, b)`` (src/interface.jl:179, src/solve.jl:66-79)
+* ``row_scaling`` / ``apply_row_scaling`` / ``SCALE_*`` (src/scaling.jl)
+* ``amd_order_sym`` / ``colamd_order`` (src/amd.jl:141-188)
+* ``symbolic_mf`` / ``predicted_fill`` (src/symbolic.jl:203-237)
+
+Indices are 1-based Int64 as in Julia.  Every numeric step (scaling applied
+to the values, assembly, factorization, solves, refinement) runs on the GPU
+through libmfgpu; ordering and symbolic analysis are the library's host code,
+whose output is identical to the reference's.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import json
+from enum import IntEnum
+
+import numpy as np
+
+from . import _lib as L
+from .sparse import SparseCSC
+
+
+class ScaleKind(IntEnum):
+    """@enum ScaleKind (src/scaling.jl:11)."""
+
+    SCALE_NONE = 0
+    SCALE_SUM = 1
+    SCALE_MAX = 2
+
+
+SCALE_NONE = ScaleKind.SCALE_NONE
+SCALE_SUM = ScaleKind.SCALE_SUM
+SCALE_MAX = ScaleKind.SCALE_MAX
+
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+
+class ArgumentError(ValueError):
+    """Julia's ArgumentError."""
+
+
+class DimensionMismatch(ValueError):
+    """Julia's DimensionMismatch."""
+
+
+class SingularException(Exception):
+    """LinearAlgebra.SingularException(info): zero pivot at factor column info."""
+
+    def __init__(self, info: int):
+        super().__init__(f"SingularException({info})")
+        self.info = int(info)
+
+
+class MfgpuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"libmfgpu error {code}: {msg}")
+        self.code = code
+
+
+def _i(a):
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+def _f(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _check_host(rc: int):
+    if rc != 0:
+        msg = L.lib().mfgpu_host_last_error().decode()
+        if rc == -1:
+            raise ArgumentError(msg or "invalid argument")
+        raise MfgpuError(rc, msg)
+
+
+# ---------------------------------------------------------------------------
+# scaling, ordering, symbolic (host code of libmfgpu)
+# ---------------------------------------------------------------------------
+def row_scaling(A: SparseCSC, kind: ScaleKind) -> np.ndarray:
+    """Rs with row i of A multiplied by Rs[i]; empty rows get 1."""
+    if A.m != A.n:
+        # the reference computes Rs for any m x n; libmfgpu's square-only ABI
+        acc = np.zeros(A.m)
+        if kind == SCALE_SUM:
+            np.add.at(acc, A.rowval - 1, np.abs(A.nzval))
+        elif kind == SCALE_MAX:
+            np.maximum.at(acc, A.rowval - 1, np.abs(A.nzval))
+        return np.where(acc > 0, 1.0 / np.where(acc > 0, acc, 1.0), 1.0) if kind != SCALE_NONE else np.ones(A.m)
+    rs = np.empty(A.n)
+    _check_host(L.lib().mfgpu_row_scaling(A.n, L.ptr(_i(A.colptr)), L.ptr(_i(A.rowval)),
+                                          L.ptr(_f(A.nzval), L.f64p), int(kind), L.ptr(rs, L.f64p)))
+    return rs
+
+
+def apply_row_scaling(A: SparseCSC, Rs) -> SparseCSC:
+    """Diagonal(Rs) * A with the same pattern (src/scaling.jl:118-126)."""
+    B = A.copy()
+    B.nzval = B.nzval * np.asarray(Rs, dtype=np.float64)[B.rowval - 1]
+    return B
+
+
+def amd_order_sym(A: SparseCSC, dense: float = 10.0) -> np.ndarray:
+    if A.m != A.n:
+        raise DimensionMismatch("amd requires a square matrix")
+    perm = np.empty(A.n, dtype=np.int64)
+    _check_host(L.lib().mfgpu_amd_order(A.n, L.ptr(_i(A.colptr)), L.ptr(_i(A.rowval)), float(dense), L.ptr(perm)))
+    return perm
+
+
+def colamd_order(A: SparseCSC, dense: float = 10.0) -> np.ndarray:
+    perm = np.empty(A.n, dtype=np.int64)
+    _check_host(L.lib().mfgpu_colamd_order(A.m, A.n, L.ptr(_i(A.colptr)), L.ptr(_i(A.rowval)), float(dense),
+                                           L.ptr(perm)))
+    return perm
+
+
+class SymbolicMF:
+    """SymbolicMF (src/symbolic.jl:203-209); 1-based.
+
+    ``colstruct[j]`` (L's below-diagonal rows of column j) is derived on
+    demand from the supernode partition and the update sets: within a
+    fundamental supernode the structures nest, so column j of supernode s
+    holds rows j+1..last(s) followed by upd(s).
+    """
+
+    def __init__(self, handle, n, qf, parent, colcount, sstart, upd_ptr, upd_idx, child_ptr, child_idx):
+        self._h = handle
+        self.n = n
+        self.qf = qf
+        self.parent = parent
+        self.colcount = colcount
+        self.sstart = sstart
+        self.upd_ptr = upd_ptr
+        self.upd_idx = upd_idx
+        self.child_ptr = child_ptr
+        self.child_idx = child_idx
+        self._super_of = None
+
+    @property
+    def nsuper(self) -> int:
+        return len(self.sstart) - 1
+
+    def update_set(self, s: int) -> np.ndarray:
+        """colstruct[last column of supernode s] (s 1-based)."""
+        return self.upd_idx[self.upd_ptr[s - 1] - 1: self.upd_ptr[s] - 1]
+
+    @property
+    def childsupers(self):
+        return [self.child_idx[self.child_ptr[s] - 1: self.child_ptr[s + 1] - 1] for s in range(self.nsuper)]
+
+    def colstruct(self, j: int) -> np.ndarray:
+        if self._super_of is None:
+            self._super_of = np.repeat(np.arange(1, self.nsuper + 1), np.diff(self.sstart))
+        s = int(self._super_of[j - 1])
+        last = int(self.sstart[s]) - 1
+        return np.concatenate([np.arange(j + 1, last + 1, dtype=np.int64), self.update_set(s)])
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            try:
+                L.lib().mfgpu_symbolic_destroy(self._h)
+            except Exception:
+                pass
+            self._h = None
+
+
+def symbolic_mf(A: SparseCSC, q=None) -> SymbolicMF:
+    if A.m != A.n:
+        raise DimensionMismatch("symbolic analysis requires a square matrix")
+    lib = L.lib()
+    h = ctypes.c_void_p()
+    qa = _i(q) if q is not None else None
+    _check_host(lib.mfgpu_symbolic_create(A.n, L.ptr(_i(A.colptr)), L.ptr(_i(A.rowval)), L.ptr(qa), ctypes.byref(h)))
+    sz = np.empty(4, np.int64)
+    lib.mfgpu_symbolic_sizes(h, L.ptr(sz))
+    n, ns, nupd, nch = (int(v) for v in sz)
+    qf = np.empty(n, np.int64)
+    parent = np.empty(n, np.int64)
+    colcount = np.empty(n, np.int64)
+    sstart = np.empty(ns + 1, np.int64)
+    upd_ptr = np.empty(ns + 1, np.int64)
+    upd_idx = np.empty(nupd, np.int64)
+    child_ptr = np.empty(ns + 1, np.int64)
+    child_idx = np.empty(nch, np.int64)
+    lib.mfgpu_symbolic_get(h, L.ptr(qf), L.ptr(parent), L.ptr(colcount), L.ptr(sstart), L.ptr(upd_ptr),
+                           L.ptr(upd_idx), L.ptr(child_ptr), L.ptr(child_idx))
+    return SymbolicMF(h, n, qf, parent, colcount, sstart, upd_ptr, upd_idx, child_ptr, child_idx)
+
+
+def predicted_fill(S: SymbolicMF) -> int:
+    """nnz(L) + nnz(U) with both diagonals (src/symbolic.jl:230-237)."""
+    return 2 * (S.n + int(np.sum(S.colcount)))
+
+
+# ---------------------------------------------------------------------------
+# GPU context
+# ---------------------------------------------------------------------------
+class GpuContext:
+    """One libmfgpu handle: analysis, resident factors, solves."""
+
+    def __init__(self, device: int = 0, precision: int = PRECISION_FP64):
+        self._lib = L.lib()
+        opts = L.MfOptions(device, precision, 0, 0)
+        h = ctypes.c_void_p()
+        rc = self._lib.mfgpu_create(ctypes.byref(opts), ctypes.byref(h))
+        if rc != 0:
+            raise MfgpuError(rc, "mfgpu_create failed (needs a B200 / sm_100 device)")
+        self._h = h
+        self.n = 0
+        self.precision = precision
+
+    def _check(self, rc: int):
+        if rc < 0:
+            msg = self._lib.mfgpu_last_error(self._h).decode()
+            if rc == -1:
+                raise ArgumentError(msg)
+            if rc == -6:
+                raise DimensionMismatch(msg)
+            raise MfgpuError(rc, msg)
+        return rc
+
+    def set_precision(self, precision: int):
+        self._check(self._lib.mfgpu_set_precision(self._h, int(precision)))
+        self.precision = precision
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self._lib.mfgpu_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    def analyze(self, A: SparseCSC, S: SymbolicMF):
+        self._check(self._lib.mfgpu_analyze_symbolic(self._h, A.n, L.ptr(_i(A.colptr)), L.ptr(_i(A.rowval)), S._h))
+        self.n = A.n
+
+    def analyze_arrays(self, A: SparseCSC, qf, parent, sstart, upd_ptr, upd_idx):
+        """mfgpu_analyze with the reference's own symbolic arrays (1-based)."""
+        ns = len(sstart) - 1
+        self._check(self._lib.mfgpu_analyze(self._h, A.n, L.ptr(_i(A.colptr)), L.ptr(_i(A.rowval)), L.ptr(_i(qf)),
+                                            L.ptr(_i(parent)), ns, L.ptr(_i(sstart)), L.ptr(_i(upd_ptr)),
+                                            L.ptr(_i(upd_idx))))
+        self.n = A.n
+
+    def factor(self, nzval, Rs=None, check: bool = True) -> int:
+        rs = _f(Rs) if Rs is not None else None
+        return self._check(self._lib.mfgpu_factor(self._h, L.ptr(_f(nzval), L.f64p), L.ptr(rs, L.f64p), int(check)))
+
+    def factor_device(self, nzval_ptr: int, rs_ptr: int | None, check: bool = True) -> int:
+        return self._check(self._lib.mfgpu_factor_device(self._h, ctypes.c_void_p(nzval_ptr),
+                                                         ctypes.c_void_p(rs_ptr) if rs_ptr else None, int(check)))
+
+    def sizes(self):
+        out = np.empty(3, np.int64)
+        self._check(self._lib.mfgpu_factor_sizes(self._h, L.ptr(out)))
+        return int(out[0]), int(out[1]), int(out[2])
+
+    def factors(self):
+        n, nl, nu = self.sizes()
+        Lp = np.empty(n + 1, np.int64)
+        Li = np.empty(nl, np.int64)
+        Lx = np.empty(nl)
+        Up = np.empty(n + 1, np.int64)
+        Ui = np.empty(nu, np.int64)
+        Ux = np.empty(nu)
+        p = np.empty(n, np.int64)
+        q = np.empty(n, np.int64)
+        pinv = np.empty(n, np.int64)
+        self._check(self._lib.mfgpu_get_factors(self._h, L.ptr(Lp), L.ptr(Li), L.ptr(Lx, L.f64p), L.ptr(Up),
+                                                L.ptr(Ui), L.ptr(Ux, L.f64p), L.ptr(p), L.ptr(q), L.ptr(pinv)))
+        return SparseCSC(n, n, Lp, Li, Lx), SparseCSC(n, n, Up, Ui, Ux), p, q, pinv
+
+    def solve(self, b, refine: int = 0) -> np.ndarray:
+        B = np.asfortranarray(b, dtype=np.float64)
+        nrhs = 1 if B.ndim == 1 else B.shape[1]
+        X = np.empty_like(B)
+        n = B.shape[0]
+        self._check(self._lib.mfgpu_solve(self._h, nrhs, L.ptr(B, L.f64p), n, L.ptr(X, L.f64p), n, int(refine)))
+        return X
+
+    def solve_device(self, nrhs: int, b_ptr: int, ldb: int, x_ptr: int, ldx: int, refine: int = 0):
+        self._check(self._lib.mfgpu_solve_device(self._h, nrhs, ctypes.c_void_p(b_ptr), ldb, ctypes.c_void_p(x_ptr),
+                                                 ldx, int(refine)))
+
+    def backward_error_device(self, nrhs: int, b_ptr: int, ldb: int, x_ptr: int, ldx: int) -> float:
+        out = ctypes.c_double()
+        self._check(self._lib.mfgpu_backward_error_device(self._h, nrhs, ctypes.c_void_p(b_ptr), ldb,
+                                                          ctypes.c_void_p(x_ptr), ldx, ctypes.byref(out)))
+        return out.value
+
+    def stats(self) -> dict:
+        buf = ctypes.create_string_buffer(16384)
+        self._check(self._lib.mfgpu_stats_json(self._h, buf, 16384))
+        return json.loads(buf.value.decode())
+
+    def set_profiling(self, on: bool):
+        self._check(self._lib.mfgpu_set_profiling(self._h, int(bool(on))))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            try:
+                self._lib.mfgpu_destroy(self._h)
+            except Exception:
+                pass
+            self._h = None
+
+
+# ---------------------------------------------------------------------------
+# factorization objects
+# ---------------------------------------------------------------------------
+class _Factors:
+    """Lazily copied CSC factors of a GPU factorization."""
+
+    def __init__(self, ctx: GpuContext):
+        self._ctx = ctx
+        self._cache = None
+
+    def _get(self):
+        if self._cache is None:
+            self._cache = self._ctx.factors()
+        return self._cache
+
+
+class GPLUFactorization:
+    """src/gplu.jl:45-51: A[p, q] == L * U (factors resident on the GPU)."""
+
+    def __init__(self, ctx: GpuContext, symbolic: SymbolicMF | None = None):
+        self.ctx = ctx
+        self.symbolic = symbolic
+        self._f = _Factors(ctx)
+
+    L = property(lambda self: self._f._get()[0])
+    U = property(lambda self: self._f._get()[1])
+    p = property(lambda self: self._f._get()[2])
+    q = property(lambda self: self._f._get()[3])
+    pinv = property(lambda self: self._f._get()[4])
+
+    def size(self, i: int | None = None):
+        s = (self.ctx.n, self.ctx.n)
+        return s if i is None else s[i - 1]
+
+    def ldiv(self, b):
+        """F \\ b (src/solve.jl:66-79): no scaling, no refinement."""
+        return self.ctx.solve(b, 0)
+
+
+class PureLU:
+    """src/interface.jl:38-48: (Rs .* A)[p, q] == L * U."""
+
+    def __init__(self, ctx: GpuContext, Rs: np.ndarray, A: SparseCSC, symbolic: SymbolicMF | None = None):
+        self.ctx = ctx
+        self.Rs = Rs
+        self.A = A
+        self.symbolic = symbolic
+        self._f = _Factors(ctx)
+
+    L = property(lambda self: self._f._get()[0])
+    U = property(lambda self: self._f._get()[1])
+    p = property(lambda self: self._f._get()[2])
+    q = property(lambda self: self._f._get()[3])
+
+    def size(self, i: int | None = None):
+        s = (self.A.n, self.A.n)
+        return s if i is None else s[i - 1]
+
+    def ldiv(self, b):
+        """F \\ b = solve(F, b) with refine = 0 (src/interface.jl:179)."""
+        return solve(self, b)
+
+
+def _factor(A: SparseCSC, q, check: bool, Rs, device: int, precision: int):
+    S = symbolic_mf(A, q=q)
+    ctx = GpuContext(device=device, precision=precision)
+    ctx.analyze(A, S)
+    status = ctx.factor(A.nzval, Rs, check)
+    if status > 0:
+        raise SingularException(status)
+    return ctx, S
+
+
+def multifrontal_lu(A: SparseCSC, q=None, tol=None, check: bool = True, device: int = 0,
+                    precision: int = PRECISION_FP64) -> GPLUFactorization:
+    """Supernodal multifrontal LU of A as given (no scaling); ``tol`` is
+    accepted and ignored, as in the reference (src/multifrontal.jl:121,147)."""
+    if A.m != A.n:
+        raise DimensionMismatch("multifrontal_lu requires a square matrix")
+    ctx, S = _factor(A, q, check, None, device, precision)
+    return GPLUFactorization(ctx, S)
+
+
+def splu(A: SparseCSC, method: str = "gplu", ordering: str = "amd", tol: float = 0.1, scale=SCALE_SUM,
+         check: bool = True, device: int = 0, precision: int = PRECISION_FP64) -> PureLU:
+    """splu(A; method, ordering, tol, scale, check) (src/interface.jl:93-120).
+
+    ``method="multifrontal"`` is the path this library implements; as in the
+    reference it ignores ``ordering`` and ``tol`` (AMD + postorder).  The
+    Gilbert-Peierls method (the reference's default ``method=:gplu``) is not
+    part of this library.
+    """
+    method = method.lstrip(":") if isinstance(method, str) else method
+    if A.m != A.n:
+        raise DimensionMismatch("splu requires a square matrix")
+    scale = ScaleKind(int(scale))
+    if method == "multifrontal":
+        Rs = row_scaling(A, scale)
+        ctx, S = _factor(A, None, check, None if scale == SCALE_NONE else Rs, device, precision)
+        return PureLU(ctx, Rs, A, S)
+    if method == "gplu":
+        raise NotImplementedError("method=:gplu (Gilbert-Peierls) is outside libmfgpu; use method='multifrontal'")
+    raise ArgumentError(f"unknown method {method}")
+
+
+def splu_q(A: SparseCSC, q, scale=SCALE_SUM, check: bool = True, device: int = 0,
+           precision: int = PRECISION_FP64) -> PureLU:
+    """``PureLU`` of ``multifrontal_lu(apply_row_scaling(A, Rs); q)`` -- the
+    route by which a COLAMD (or any caller) order reaches the multifrontal
+    kernel in the reference (src/multifrontal.jl:152)."""
+    scale = ScaleKind(int(scale))
+    Rs = row_scaling(A, scale)
+    ctx, S = _factor(A, q, check, None if scale == SCALE_NONE else Rs, device, precision)
+    return PureLU(ctx, Rs, A, S)
+
+
+def solve(F, b, refine: int = 0) -> np.ndarray:
+    """solve(F::PureLU, b; refine) (src/interface.jl:170-177): x = F \\ b, then
+    ``refine`` steps of x += F \\ (b - A x) with the unscaled A, all on the GPU.
+    ``b`` may be a vector or an n x k matrix (k right-hand sides)."""
+    if isinstance(F, GPLUFactorization):
+        if refine:
+            raise ArgumentError("refinement needs a PureLU (it keeps A and Rs)")
+        return F.ldiv(b)
+    b = np.asarray(b, dtype=np.float64)
+    if b.shape[0] != F.A.n:
+        raise DimensionMismatch("length(b) must equal size(F, 1)")
+    return F.ctx.solve(b, refine)

@@ -114,6 +114,19 @@ def convdiff3d(k: int, velocity=(1.0, 0.5, 0.25), peclet: float = 10.0) -> Spars
     return SparseCSC.from_coo(np.concatenate(I), np.concatenate(J), np.concatenate(V), n, n)
 
 
+def grid3d_random(k: int, offdiag: float = 0.5, seed: int = 1) -> SparseCSC:
+    """7-point grid pattern (poisson3d's) with random values: diagonal
+    U[1, 2], off-diagonals N(0, offdiag^2), unsymmetric in value.  Partial
+    pivoting inside the pivot blocks then makes row interchanges with clear
+    margins and modest element growth."""
+    A = poisson3d(k)
+    rng = np.random.default_rng(seed)
+    v = rng.standard_normal(A.nnz()) * offdiag
+    diag = (A.rowval - 1) == A.colind()
+    v[diag] = 1.0 + rng.random(int(diag.sum()))
+    return SparseCSC(A.m, A.n, A.colptr, A.rowval, v)
+
+
 def random_unsym(n: int = 20000, per_col: int = 5, shift: float = 10.0, seed: int = 0) -> SparseCSC:
     """n x n, ``per_col`` entries per column at uniform random rows, N(0,1)
     values, plus ``shift`` * I."""

@@ -1,0 +1,44 @@
+"""Shared test setup: import paths, the `gpu` marker, and in-tree builds.
+
+Tests marked ``gpu`` need a B200 and call libmfgpu through its C ABI; the
+rest run on the CPU (oracle against its golden vectors, host symbolic code,
+ABI exports, multi-process host logic).
+"""
+
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "pureumfpack.jl_b200")
+for p in (ROOT, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+
+
+def _ensure_built():
+    lib = os.path.join(PKG, "pureumfpack", "libmfgpu.so")
+    if not os.path.exists(lib):
+        subprocess.run([sys.executable, os.path.join(PKG, "build.py")], check=True)
+    orc = os.path.join(ROOT, "oracle", "_build", "libmforacle.so")
+    if not os.path.exists(orc):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+
+
+_ensure_built()
+
+
+@pytest.fixture(scope="session")
+def has_gpu():
+    try:
+        import torch
+
+        return torch.cuda.is_available()
+    except Exception:
+        return False

@@ -1,0 +1,47 @@
+"""The C ABI library loads on a host without a GPU and exports every symbol
+declared in include/mfgpu.h; GPU entry points fail cleanly without a device."""
+
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "mfgpu.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(mfgpu_\w+)\s*\(", text)))
+
+
+def test_header_declares_the_api():
+    names = declared_functions()
+    for must in ("mfgpu_create", "mfgpu_analyze", "mfgpu_factor", "mfgpu_get_factors", "mfgpu_solve",
+                 "mfgpu_destroy", "mfgpu_amd_order", "mfgpu_symbolic_create"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    from pureumfpack import _lib
+
+    L = _lib.lib()
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+    bound = {s[0] for s in _lib.SIGNATURES}
+    assert set(declared_functions()) == bound
+
+
+def test_gpu_entry_points_fail_cleanly_without_device(has_gpu):
+    if has_gpu:
+        pytest.skip("a GPU is present")
+    from pureumfpack import _lib
+
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    rc = L.mfgpu_create(None, ctypes.byref(h))
+    assert rc == -8 and not h.value
+    assert L.mfgpu_factor(None, None, None, 1) == -1
+    assert L.mfgpu_solve(None, 1, None, 1, None, 1, 0) == -1
