@@ -258,7 +258,10 @@ def main():
     Rs = row_scaling(A, 1)
     t_sym = time.perf_counter() - t0
 
-    stream = torch.cuda.current_stream(dev)
+    # a dedicated stream shared with the library: CUDA events recorded on it
+    # bracket exactly the library's kernels (and it can be graph-captured)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
     d_ax = torch.from_numpy(A.nzval).to(dev)
     d_rs = torch.from_numpy(Rs).to(dev)
     d_b = torch.from_numpy(np.asfortranarray(B).ravel(order="F")).to(dev)
@@ -301,6 +304,7 @@ def main():
         for _ in range(args.steps):
             step(refine)
         e1.record(stream)
+        e1.synchronize()
         torch.cuda.synchronize()
         clk = clocks.stop()
         ms = e0.elapsed_time(e1) / args.steps

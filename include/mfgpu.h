@@ -156,6 +156,10 @@ int mfgpu_stats_json(mfgpu_ctx* h, char* buf, int64_t cap);
  * kernel launch with CUDA events on the launching stream (device times per
  * kernel class, with their algorithmic flops and bytes). */
 int mfgpu_set_profiling(mfgpu_ctx* h, int32_t on);
+/* JSON array of the profiled launches since mfgpu_set_profiling:
+ * [kernel class, tree level, tasks or tiles, device ms, flops, bytes] each.
+ * Returns MFGPU_OK, or the buffer size needed when cap is too small. */
+int mfgpu_launch_records(mfgpu_ctx* h, char* buf, int64_t cap);
 
 #ifdef __cplusplus
 }

@@ -37,6 +37,7 @@ struct DevPlan {
   const int32_t* csr_ptr;
   const int32_t* csr_col;
   const int32_t* csr_src;
+  const int64_t* dinv_off;   // per supernode: first 64-block of its inverted diagonal blocks (-1: small front)
 };
 
 // Per-factorization numeric state.
@@ -116,6 +117,77 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                : "+d"(d0), "+d"(d1)
                : "d"(a), "d"(b));
+}
+
+}  // namespace mfgpu
+
+namespace mfgpu {
+
+// Shared-memory leading dimensions of the 64x64 tile product operands,
+// chosen so DMMA fragment loads take the minimum two shared-memory wavefronts.
+constexpr int kLdP = 72;   // left operand, column-major
+constexpr int kLdQ = 68;   // right operand, column-major
+
+// D = P * Q for 64x64 tiles in shared memory (P col-major ld kLdP, Q col-major
+// ld kLdQ), 128 threads; D (col-major, ldd) may alias P or Q.
+template <typename T>
+__device__ void mm64(const T* P, const T* Q, T* D, int ldd);
+
+template <>
+__device__ __forceinline__ void mm64<double>(const double* P, const double* Q, double* D, int ldd) {
+  const int lane = lane_id(), warp = warp_id();
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+  double acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+#pragma unroll 4
+  for (int kk = 0; kk < 64; kk += 4) {
+    double af[4], bf[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) af[i] = P[(wm + i * 8 + (lane >> 2)) + (kk + (lane & 3)) * kLdP];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) bf[j] = Q[(kk + (lane & 3)) + (wn + j * 8 + (lane >> 2)) * kLdQ];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e)
+        D[(wm + i * 8 + (lane >> 2)) + (wn + j * 8 + 2 * (lane & 3) + e) * ldd] = acc[i][j][e];
+  __syncthreads();
+}
+
+template <>
+__device__ __forceinline__ void mm64<float>(const float* P, const float* Q, float* D, int ldd) {
+  const int t = threadIdx.x;
+  const int tm = (t & 15) * 4, tn = (t >> 4) * 8;
+  float acc[4][8] = {};
+#pragma unroll 8
+  for (int k = 0; k < 64; ++k) {
+    float a[4], b[8];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = P[tm + i + k * kLdP];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) b[j] = Q[k + (tn + j) * kLdQ];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) D[tm + i + (tn + j) * ldd] = acc[i][j];
+  __syncthreads();
 }
 
 }  // namespace mfgpu

@@ -158,93 +158,390 @@ __device__ void panel_lu_pivot(T* A, int lda, int R, int kb, int* piv, ArgMax* r
 }
 
 constexpr int kPanelThreads = 256;
+constexpr int kDinvElems = 2 * 64 * 64;   // inv(L_kk) then inv(U_kk), 64x64 col-major, zero padded
 
+// Inverses of the unit-lower and the upper triangle of the factored kb x kb
+// diagonal block D (shared, col-major, leading dimension ldd) into the 64x64
+// zero-padded Linv / Uinv (shared, col-major ld 64).  Column c of each
+// inverse is one thread's forward / backward substitution.
 template <typename T>
-__global__ void __launch_bounds__(kPanelThreads) k_panel(DevPlan P, DevState S, const PanelTask* __restrict__ tasks,
-                                                         T* __restrict__ pool) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sm = reinterpret_cast<T*>(smem_raw);
-  __shared__ ArgMax red[kPanelThreads / 32];
-  __shared__ int piv[kPanel];
-  __shared__ int first_zero;
-  const PanelTask tk = tasks[blockIdx.x];
-  const int s = tk.s, k0 = tk.k0;
-  const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
-  const int kb = min(kPanel, np - k0), k1 = k0 + kb;
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  T* F = pool + P.front_off[s];
-  if (tid == 0) first_zero = INT32_MAX;
-
-  if (tk.mode == kPanelSpeculative) {
-    // diagonal block only, no interchanges; flag any row that partial
-    // pivoting would have chosen instead of the diagonal.
-    for (int e = tid; e < kb * kb; e += nthr) sm[e] = F[(k0 + e % kb) + (int64_t)(k0 + e / kb) * nf];
-    __syncthreads();
-    for (int j = 0; j < kb; ++j) {
-      const T d = sm[j + j * kb];
-      const double ad = absd(d);
-      for (int i = j + 1 + tid; i < kb; i += nthr)
-        if (absd(sm[i + j * kb]) > ad) atomicOr(S.flags, 1);
-      if (d == T(0)) {
-        if (tid == 0) atomicOr(S.flags, 1);
-      } else {
-        const T rcp = T(1) / d;
-        for (int i = j + 1 + tid; i < kb; i += nthr) sm[i + j * kb] *= rcp;
+__device__ void diag_block_inverses(const T* D, int ldd, int kb, T* Linv, T* Uinv) {
+  for (int e = threadIdx.x; e < 2 * 64 * 64; e += blockDim.x) (e < 4096 ? Linv[e] : Uinv[e - 4096]) = T(0);
+  __syncthreads();
+  // one column per task; four partial sums break the FMA dependency chain
+  for (int task = threadIdx.x; task < 2 * kb; task += blockDim.x) {
+    if (task < kb) {
+      const int c = task;
+      T* x = Linv + c * 64;
+      x[c] = T(1);
+      for (int i = c + 1; i < kb; ++i) {
+        T v0 = T(0), v1 = T(0), v2 = T(0), v3 = T(0);
+        int k = c;
+        for (; k + 3 < i; k += 4) {
+          v0 += D[i + k * ldd] * x[k];
+          v1 += D[i + (k + 1) * ldd] * x[k + 1];
+          v2 += D[i + (k + 2) * ldd] * x[k + 2];
+          v3 += D[i + (k + 3) * ldd] * x[k + 3];
+        }
+        for (; k < i; ++k) v0 += D[i + k * ldd] * x[k];
+        x[i] = -((v0 + v1) + (v2 + v3));
       }
-      __syncthreads();
-      const int r = kb - j - 1;
-      for (int e = tid; e < r * r; e += nthr) {
-        const int i = j + 1 + e % r, c = j + 1 + e / r;
-        sm[i + c * kb] -= sm[i + j * kb] * sm[j + c * kb];
+    } else {
+      const int c = task - kb;
+      T* x = Uinv + c * 64;
+      x[c] = T(1) / D[c + c * ldd];
+      for (int i = c - 1; i >= 0; --i) {
+        T v0 = T(0), v1 = T(0), v2 = T(0), v3 = T(0);
+        int k = i + 1;
+        for (; k + 3 <= c; k += 4) {
+          v0 += D[i + k * ldd] * x[k];
+          v1 += D[i + (k + 1) * ldd] * x[k + 1];
+          v2 += D[i + (k + 2) * ldd] * x[k + 2];
+          v3 += D[i + (k + 3) * ldd] * x[k + 3];
+        }
+        for (; k <= c; ++k) v0 += D[i + k * ldd] * x[k];
+        x[i] = -((v0 + v1) + (v2 + v3)) / D[i + i * ldd];
       }
-      __syncthreads();
     }
-    for (int e = tid; e < kb * kb; e += nthr) F[(k0 + e % kb) + (int64_t)(k0 + e / kb) * nf] = sm[e];
-    for (int j = tid; j < kb; j += nthr) S.ipiv[c1 + k0 + j] = k0 + j;
-    return;
-  }
-
-  const int R = np - k0;
-  if (tk.mode == kPanelSmemPivot) {
-    for (int e = tid; e < R * kb; e += nthr) sm[e] = F[(k0 + e % R) + (int64_t)(k0 + e / R) * nf];
-    __syncthreads();
-    panel_lu_pivot(sm, R, R, kb, piv, red, &first_zero);
-    for (int e = tid; e < R * kb; e += nthr) F[(k0 + e % R) + (int64_t)(k0 + e / R) * nf] = sm[e];
-  } else {
-    __syncthreads();
-    panel_lu_pivot(F + k0 + (int64_t)k0 * nf, nf, R, kb, piv, red, &first_zero);
   }
   __syncthreads();
-  for (int j = tid; j < kb; j += nthr) S.ipiv[c1 + k0 + j] = k0 + piv[j];
-  if (tid == 0 && first_zero != INT32_MAX) atomicMin(S.info + s, k0 + first_zero);
-  // interchanges on the columns outside the panel, in LAPACK order
-  for (int cc = tid; cc < nf - kb; cc += nthr) {
-    const int c = cc < k0 ? cc : cc + kb;
-    T* col = F + (int64_t)c * nf;
-    for (int j = 0; j < kb; ++j) {
-      const int p = piv[j];
-      if (p != j) {
-        const T t = col[k0 + j];
-        col[k0 + j] = col[k0 + p];
-        col[k0 + p] = t;
-      }
-    }
-  }
-  (void)k1;
 }
 
-// Triangular solves of one panel step.  L part: rows r0..nf-1 of the panel
-// columns, X * U_kk = A (rdiv! with UpperTriangular, multifrontal.jl:265);
-// U part: rows k0..k1-1 of the columns right of the panel,
-// L_kk * X = A (ldiv! with UnitLowerTriangular, multifrontal.jl:266).
-constexpr int kTrsmThreads = 64;
+// ---------------------------------------------------------------------------
+// Register-tiled dense kernels for the panel.  A CTA of ROWS threads holds
+// an (R <= ROWS) x (kb <= 64) panel in registers: thread t owns rows
+// rb, rb+G, ..., rb+7G (rb = t % G, G = ROWS/8) of the 8 columns
+// c0..c0+7 (c0 = 8 (t / G)).  The G owners of one 8-column block are
+// consecutive lanes of one warp, and consecutive lanes own consecutive rows,
+// so global and shared accesses are coalesced and conflict-free.  Every
+// elimination step broadcasts one multiplier column and one pivot row through
+// shared memory; a thread's 64 updates are then independent FMAs on
+// registers (compile-time indices, predicated on the trailing region).
+// ---------------------------------------------------------------------------
+template <int G>
+__device__ __forceinline__ ArgMax group_argmax(ArgMax a) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) {
+    ArgMax b;
+    b.v = __shfl_xor_sync(0xffffffffu, a.v, o);
+    b.i = __shfl_xor_sync(0xffffffffu, a.i, o);
+    a = better(a, b);
+  }
+  return a;
+}
+
+// Value of row slot `slot` (runtime) of column q of a register tile.
+template <typename T>
+__device__ __forceinline__ T row_pick(const T (&a)[8][8], int slot, int q) {
+  T v = a[0][q];
+#pragma unroll
+  for (int ii = 1; ii < 8; ++ii)
+    if (ii == slot) v = a[ii][q];
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T col_pick(const T (&a)[8][8], int ii, int slot) {
+  T v = a[ii][0];
+#pragma unroll
+  for (int q = 1; q < 8; ++q)
+    if (q == slot) v = a[ii][q];
+  return v;
+}
+
+__device__ __forceinline__ void named_barrier(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// LU of the register panel with the pivot search restricted to rows
+// j..R-1 (PIVOT, LAPACK's first-maximum rule) or without interchanges and
+// with the partial-pivoting order check (!PIVOT).  sm_urow, sm_buf: 64 each;
+// sm_lcol: ROWS.
+template <typename T, int ROWS, bool PIVOT>
+__device__ void tile_lu(T (&a)[8][8], int R, int kb, T* sm_urow, T* sm_buf, T* sm_lcol, int* sm_p, int* piv,
+                        int* first_zero, bool* violated) {
+  constexpr int G = ROWS / 8;
+  const int t = threadIdx.x;
+  const int rb = t % G, cb = t / G, c0 = cb * 8;
+#pragma unroll 1
+  for (int j = 0; j < kb; ++j) {
+    const int jb = j >> 3, jo = j & 7;
+    const int jr = j % G, js = j / G;         // owner lane and slot of row j
+    int p = j;
+    if (PIVOT) {
+      // Every lane takes part in the shuffles (a warp holds 32/G column
+      // groups); only the owner group of column j has real candidates.
+      ArgMax m{-1.0, 0x7fffffff};
+      if (cb == jb) {
+#pragma unroll
+        for (int ii = 0; ii < 8; ++ii) {
+          const int i = rb + ii * G;
+          if (i >= j && i < R) m = better(m, ArgMax{absd(col_pick(a, ii, jo)), i});
+        }
+      }
+      m = group_argmax<G>(m);
+      if (cb == jb && rb == 0) *sm_p = m.i;
+      __syncthreads();
+      p = *sm_p;
+      if (p != j) {                           // uniform: swap rows j and p
+        const int pr = p % G, ps = p / G;
+        if (rb == jr) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) sm_urow[c0 + q] = row_pick(a, js, q);
+        }
+        if (rb == pr) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) sm_buf[c0 + q] = row_pick(a, ps, q);
+        }
+        __syncthreads();
+        if (rb == jr) {
+#pragma unroll
+          for (int ii = 0; ii < 8; ++ii)
+            if (ii == js)
+#pragma unroll
+              for (int q = 0; q < 8; ++q) a[ii][q] = sm_buf[c0 + q];
+        }
+        if (rb == pr) {
+#pragma unroll
+          for (int ii = 0; ii < 8; ++ii)
+            if (ii == ps)
+#pragma unroll
+              for (int q = 0; q < 8; ++q) a[ii][q] = sm_urow[c0 + q];
+        }
+        __syncthreads();
+      }
+    }
+    if (rb == jr) {                           // broadcast the pivot row
+#pragma unroll
+      for (int q = 0; q < 8; ++q) sm_urow[c0 + q] = row_pick(a, js, q);
+    }
+    __syncthreads();
+    const T d = sm_urow[j];
+    if (t == 0) {
+      piv[j] = p;
+      if (d == T(0) && *first_zero == INT32_MAX) *first_zero = j;
+    }
+    if (cb == jb) {                           // multipliers of column j
+      const T rcp = (d != T(0)) ? T(1) / d : T(1);
+#pragma unroll
+      for (int ii = 0; ii < 8; ++ii) {
+        const int i = rb + ii * G;
+        if (i > j && i < R) {
+          const T aj = col_pick(a, ii, jo);
+          if (!PIVOT && absd(aj) > absd(d)) *violated = true;
+          const T l = (d != T(0)) ? aj * rcp : aj;
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            if (q == jo) a[ii][q] = l;
+          sm_lcol[i] = l;
+        }
+      }
+    }
+    __syncthreads();
+    T u[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) u[q] = sm_urow[c0 + q];
+#pragma unroll
+    for (int ii = 0; ii < 8; ++ii) {
+      const int i = rb + ii * G;
+      if (i > j && i < R) {
+        const T l = sm_lcol[i];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (c0 + q > j) a[ii][q] -= l * u[q];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// inv(L_kk) (unit lower, !UPPER) or inv(U_kk) (UPPER) of the factored kb x kb
+// block D (shared, col-major ld ldd) into dst (global 64 x 64 col-major, zero
+// padded), by the 64 threads lane64 = 0..63 of one group synchronised on
+// named barrier `bar`: X = I, then one broadcast row of X per step.
+template <typename T, bool UPPER>
+__device__ void tile_inverse(const T* D, int ldd, int kb, T* dst, T* sm_xrow, int lane64, int bar) {
+  const int rb = lane64 % 8, c0 = (lane64 / 8) * 8;
+  T x[8][8];
+#pragma unroll
+  for (int ii = 0; ii < 8; ++ii)
+#pragma unroll
+    for (int q = 0; q < 8; ++q) x[ii][q] = (rb + ii * 8 == c0 + q && c0 + q < kb) ? T(1) : T(0);
+  for (int step = 0; step < kb; ++step) {
+    const int k = UPPER ? kb - 1 - step : step;
+    const int kr = k % 8, ks = k / 8;
+    if (UPPER && rb == kr) {                  // row k is final once divided by U_kk
+      const T rd = T(1) / D[k + k * ldd];
+#pragma unroll
+      for (int ii = 0; ii < 8; ++ii)
+        if (ii == ks)
+#pragma unroll
+          for (int q = 0; q < 8; ++q) x[ii][q] *= rd;
+    }
+    if (rb == kr) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) sm_xrow[c0 + q] = row_pick(x, ks, q);
+    }
+    named_barrier(bar, 64);
+    T xr[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) xr[q] = sm_xrow[c0 + q];
+#pragma unroll
+    for (int ii = 0; ii < 8; ++ii) {
+      const int i = rb + ii * 8;
+      if (UPPER ? (i < k) : (i > k && i < kb)) {
+        const T f = D[i + k * ldd];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) x[ii][q] -= f * xr[q];
+      }
+    }
+    named_barrier(bar, 64);
+  }
+#pragma unroll
+  for (int q = 0; q < 8; ++q)
+#pragma unroll
+    for (int ii = 0; ii < 8; ++ii) dst[(rb + ii * 8) + (c0 + q) * 64] = x[ii][q];
+}
+
+// Both inverses of the factored diagonal block into the 2 x 64 x 64 dinv slot.
+template <typename T, int ROWS>
+__device__ void block_inverses(const T* D, int ldd, int kb, T* dst, T* sm_xrow2) {
+  const int t = threadIdx.x;
+  if (ROWS >= 128) {
+    if (t < 64) tile_inverse<T, false>(D, ldd, kb, dst, sm_xrow2, t, 1);
+    else if (t < 128) tile_inverse<T, true>(D, ldd, kb, dst + 4096, sm_xrow2 + 64, t - 64, 2);
+  } else {
+    tile_inverse<T, false>(D, ldd, kb, dst, sm_xrow2, t, 1);
+    tile_inverse<T, true>(D, ldd, kb, dst + 4096, sm_xrow2 + 64, t, 1);
+  }
+}
+
+// Panel factorization of one panel step (k0..k1-1) of one large front.
+//  * kPanelSmemPivot: the R = np-k0 <= 256 candidate rows are held one row
+//    per thread in registers; the pivot of each column is a block-wide
+//    argmax (warp shuffles, LAPACK's first-maximum rule), the pivot row is
+//    broadcast through shared memory, and the interchanges are applied to
+//    the whole rows of the front (LAPACK getrf + the R12 swap of
+//    src/multifrontal.jl:247-263).
+//  * kPanelSpeculative: only the kb x kb diagonal block, without
+//    interchanges; any row that partial pivoting would have preferred raises
+//    flags[0] and the factorization is redone with pivoting panels.
+//  * kPanelGlobalPivot: R > 256 rows, partial pivoting on global memory.
+// Every mode ends by inverting the diagonal block's two triangles into dinv,
+// which turns the panel's triangular solves (and the solves' diagonal blocks)
+// into tensor-core tile products.
+// ROWS (= threads per CTA, 64 / 128 / 256) bounds the rows a launch holds in
+// registers, so small pivot blocks do not pay for the largest panel's
+// registers and shared memory.
+template <typename T, int ROWS>
+__global__ void __launch_bounds__(ROWS) k_panel(DevPlan P, DevState S, const PanelTask* __restrict__ tasks,
+                                                T* __restrict__ pool, T* __restrict__ dinv) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* stage = reinterpret_cast<T*>(smem_raw);            // panel copy, col-major ld ROWS (ROWS x 64)
+  T* sm_urow = stage + ROWS * kPanel;                   // 64
+  T* sm_buf = sm_urow + 64;                             // 64
+  T* sm_xrow = sm_buf + 64;                             // 2 x 64
+  T* sm_lcol = sm_xrow + 128;                           // ROWS
+  __shared__ ArgMax red[ROWS / 32];
+  __shared__ int piv[kPanel];
+  __shared__ int first_zero;
+  __shared__ int sm_p;
+  __shared__ int any_violation;
+  const PanelTask tk = tasks[blockIdx.x];
+  const int s = tk.s, k0 = tk.k0, mode = tk.mode;
+  const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
+  const int kb = min(kPanel, np - k0);
+  const int t = threadIdx.x, nthr = blockDim.x;
+  T* F = pool + P.front_off[s];
+  T* dst = dinv + (P.dinv_off[s] + k0 / kPanel) * (int64_t)kDinvElems;
+  if (t == 0) {
+    first_zero = INT32_MAX;
+    any_violation = 0;
+  }
+  __syncthreads();
+
+  if (mode != kPanelGlobalPivot) {
+    constexpr int G = ROWS / 8;
+    const int R = (mode == kPanelSpeculative) ? kb : np - k0;
+    const int rb = t % G, c0 = (t / G) * 8;
+    T a[8][8];
+#pragma unroll
+    for (int ii = 0; ii < 8; ++ii)
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int i = rb + ii * G, c = c0 + q;
+        a[ii][q] = (i < R && c < kb) ? F[(k0 + i) + (int64_t)(k0 + c) * nf] : T(0);
+      }
+    bool violated = false;
+    if (mode == kPanelSmemPivot)
+      tile_lu<T, ROWS, true>(a, R, kb, sm_urow, sm_buf, sm_lcol, &sm_p, piv, &first_zero, &violated);
+    else
+      tile_lu<T, ROWS, false>(a, R, kb, sm_urow, sm_buf, sm_lcol, &sm_p, piv, &first_zero, &violated);
+    if (violated) any_violation = 1;
+#pragma unroll
+    for (int ii = 0; ii < 8; ++ii)
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int i = rb + ii * G, c = c0 + q;
+        if (i < R && c < kb) {
+          F[(k0 + i) + (int64_t)(k0 + c) * nf] = a[ii][q];
+          stage[i + c * ROWS] = a[ii][q];
+        }
+      }
+    __syncthreads();
+    if (t == 0 && (any_violation || (mode == kPanelSpeculative && first_zero != INT32_MAX))) atomicOr(S.flags, 1);
+    block_inverses<T, ROWS>(stage, ROWS, kb, dst, sm_xrow);
+  } else {
+    panel_lu_pivot(F + k0 + (int64_t)k0 * nf, nf, np - k0, kb, piv, red, &first_zero);
+    for (int e = t; e < kb * kb; e += nthr) stage[(e % kb) + (e / kb) * ROWS] = F[(k0 + e % kb) + (int64_t)(k0 + e / kb) * nf];
+    __syncthreads();
+    block_inverses<T, ROWS>(stage, ROWS, kb, dst, sm_xrow);
+  }
+  __syncthreads();
+  for (int j = t; j < kb; j += nthr) S.ipiv[c1 + k0 + j] = k0 + piv[j];
+  if (t == 0 && first_zero != INT32_MAX) atomicMin(S.info + s, k0 + first_zero);
+  if (mode == kPanelSpeculative) return;
+  // interchanges on the columns outside the panel, in LAPACK order; only the
+  // steps that actually swapped are replayed
+  __shared__ int nswap;
+  __shared__ int swaps[kPanel];
+  if (t == 0) {
+    int c = 0;
+    for (int j = 0; j < kb; ++j)
+      if (piv[j] != j) swaps[c++] = j;
+    nswap = c;
+  }
+  __syncthreads();
+  const int ns = nswap;
+  if (ns == 0) return;
+  for (int cc = t; cc < nf - kb; cc += nthr) {
+    const int c = cc < k0 ? cc : cc + kb;
+    T* col = F + (int64_t)c * nf;
+    for (int q = 0; q < ns; ++q) {
+      const int j = swaps[q], p = piv[j];
+      const T tmp = col[k0 + j];
+      col[k0 + j] = col[k0 + p];
+      col[k0 + p] = tmp;
+    }
+  }
+}
+
+// Triangular solves of one panel step as tile products with the inverted
+// diagonal block: L part (rows r0..nf-1 of the panel columns)
+// X = A * inv(U_kk) (rdiv! with UpperTriangular, src/multifrontal.jl:265);
+// U part (rows k0..k1-1 right of the panel) X = inv(L_kk) * A (ldiv! with
+// UnitLowerTriangular, :266).  Each CTA owns one 64-row or 64-column tile,
+// reads it whole before writing it back, so the update is in place.  In
+// speculative panels an L entry with |l| > 1 on a pivot row (a row partial
+// pivoting would have chosen) raises flags[0].
+constexpr int kApplyThreads = 128;
 
 template <typename T>
-__global__ void __launch_bounds__(kTrsmThreads) k_panel_trsm(DevPlan P, DevState S, const TrsmTask* __restrict__ tasks,
-                                                             int ntasks, T* __restrict__ pool) {
+__global__ void __launch_bounds__(kApplyThreads) k_panel_apply(DevPlan P, DevState S, const TrsmTask* __restrict__ tasks,
+                                                               int ntasks, T* __restrict__ pool,
+                                                               const T* __restrict__ dinv) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sD = reinterpret_cast<T*>(smem_raw);
-  T* sX = sD + 64 * 65;
+  T* sP = reinterpret_cast<T*>(smem_raw);   // 64 x kLdP
+  T* sQ = sP + 64 * kLdP;                    // kLdQ x 64
   const int64_t tile = blockIdx.x;
   int lo = 0, hi = ntasks - 1;
   while (lo < hi) {
@@ -257,45 +554,44 @@ __global__ void __launch_bounds__(kTrsmThreads) k_panel_trsm(DevPlan P, DevState
   const int s = tk.s, k0 = tk.k0;
   const int np = P.np[s], nf = P.nf[s];
   const int kb = min(kPanel, np - k0), k1 = k0 + kb;
-  const int tid = threadIdx.x;
+  const int t = threadIdx.x;
   T* F = pool + P.front_off[s];
-  for (int e = tid; e < kb * kb; e += blockDim.x) sD[e % kb + (e / kb) * 65] = F[(k0 + e % kb) + (int64_t)(k0 + e / kb) * nf];
+  const T* W = dinv + (P.dinv_off[s] + k0 / kPanel) * (int64_t)kDinvElems;
+  const int r = t & 63, cg = t >> 6;   // row of the tile, column parity
   if (local < tk.lrow_tiles) {
     const int i0 = tk.r0 + 64 * local;
     const int rows = min(64, nf - i0);
-    for (int e = tid; e < rows * kb; e += blockDim.x)
-      sX[e % rows + (e / rows) * 65] = F[(i0 + e % rows) + (int64_t)(k0 + e / rows) * nf];
-    __syncthreads();
-    if (tid < rows) {
-      const bool chk = tk.check && (i0 + tid) < np;
-      for (int j = 0; j < kb; ++j) {
-        T num = sX[tid + j * 65];
-        for (int i = 0; i < j; ++i) num -= sX[tid + i * 65] * sD[i + j * 65];
-        const T d = sD[j + j * 65];
-        if (chk && absd(num) > absd(d)) atomicOr(S.flags, 1);
-        sX[tid + j * 65] = num * (T(1) / d);
-      }
+    const T* src = F + (i0 + r) + (int64_t)k0 * nf;
+#pragma unroll 8
+    for (int c = cg; c < 64; c += 2) {
+      sP[r + c * kLdP] = (r < rows && c < kb) ? src[(int64_t)c * nf] : T(0);
+      sQ[r + c * kLdQ] = W[4096 + r + c * 64];   // inv(U_kk)(r, c)
     }
     __syncthreads();
-    for (int e = tid; e < rows * kb; e += blockDim.x)
-      F[(i0 + e % rows) + (int64_t)(k0 + e / rows) * nf] = sX[e % rows + (e / rows) * 65];
+    mm64<T>(sP, sQ, sP, kLdP);
+    bool violated = false;
+    for (int e = t; e < rows * kb; e += blockDim.x) {
+      const int r = e % rows, c = e / rows;
+      const T v = sP[r + c * kLdP];
+      if (tk.check && i0 + r < np && absd(v) > 1.0) violated = true;
+      F[(i0 + r) + (int64_t)(k0 + c) * nf] = v;
+    }
+    if (violated) atomicOr(S.flags, 1);
   } else {
     const int j0 = k1 + 64 * (local - tk.lrow_tiles);
     const int cols = min(64, nf - j0);
-    for (int e = tid; e < kb * cols; e += blockDim.x)
-      sX[e % kb + (e / kb) * 65] = F[(k0 + e % kb) + (int64_t)(j0 + e / kb) * nf];
-    __syncthreads();
-    if (tid < cols) {
-      T* x = sX + tid * 65;
-      for (int i = 0; i < kb; ++i) {
-        T v = x[i];
-        for (int j = 0; j < i; ++j) v -= sD[i + j * 65] * x[j];
-        x[i] = v;
-      }
+    const T* src = F + (k0 + r) + (int64_t)j0 * nf;
+#pragma unroll 8
+    for (int c = cg; c < 64; c += 2) {
+      sP[r + c * kLdP] = W[r + c * 64];           // inv(L_kk)(r, c)
+      sQ[r + c * kLdQ] = (r < kb && c < cols) ? src[(int64_t)c * nf] : T(0);
     }
     __syncthreads();
-    for (int e = tid; e < kb * cols; e += blockDim.x)
-      F[(k0 + e % kb) + (int64_t)(j0 + e / kb) * nf] = sX[e % kb + (e / kb) * 65];
+    mm64<T>(sP, sQ, sQ, kLdQ);
+    for (int e = t; e < kb * cols; e += blockDim.x) {
+      const int r = e % kb, c = e / kb;
+      F[(k0 + r) + (int64_t)(j0 + c) * nf] = sQ[r + c * kLdQ];
+    }
   }
 }
 

@@ -17,6 +17,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "factor_kernels.cuh"
 
 namespace mfgpu {
 
@@ -116,33 +117,35 @@ struct SolveBlockTask {
   int32_t s, k0;
 };
 
-// Unit-lower diagonal block solve of rows k0..k1-1 (forward), one thread per rhs.
+// Forward diagonal block of rows k0..k1-1: y = inv(L_kk) * f on a 64-column
+// tile of right-hand sides, as a tensor-core tile product (the inverse was
+// formed by the panel factorization).
 template <typename T>
-__global__ void __launch_bounds__(64) k_fwd_diag(DevPlan P, const SolveBlockTask* __restrict__ tasks, int64_t nrhs,
-                                                 const T* __restrict__ pool, T* __restrict__ fsol) {
-  __shared__ T Ld[64 * 65];
+__global__ void __launch_bounds__(kApplyThreads) k_fwd_diag(DevPlan P, const SolveBlockTask* __restrict__ tasks,
+                                                            int64_t nrhs, const T* __restrict__ dinv,
+                                                            T* __restrict__ fsol) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sP = reinterpret_cast<T*>(smem_raw);
+  T* sQ = sP + 64 * kLdP;
   const SolveBlockTask tk = tasks[blockIdx.x];
   const int s = tk.s, k0 = tk.k0;
   const int np = P.np[s], nf = P.nf[s];
   const int kb = min(kPanel, np - k0);
-  const T* F = pool + P.front_off[s];
-  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) Ld[e % kb + (e / kb) * 65] = F[(k0 + e % kb) + (int64_t)(k0 + e / kb) * nf];
-  __syncthreads();
-  const int64_t col = (int64_t)blockIdx.y * blockDim.x + threadIdx.x;
-  if (col >= nrhs) return;
-  T* y = fsol + P.colbase[s] * nrhs + col * nf + k0;
-  T v[kPanel];
-#pragma unroll 8
-  for (int i = 0; i < kPanel; ++i)
-    if (i < kb) v[i] = y[i];
-  for (int i = 0; i < kb; ++i) {
-    T t = v[i];
-    for (int j = 0; j < i; ++j) t -= Ld[i + j * 65] * v[j];
-    v[i] = t;
+  const int64_t c0 = (int64_t)blockIdx.y * 64;
+  const int rc = (int)(nrhs - c0 < 64 ? nrhs - c0 : 64);
+  const T* W = dinv + (P.dinv_off[s] + k0 / kPanel) * (int64_t)kDinvElems;
+  T* y = fsol + P.colbase[s] * nrhs + k0;
+  for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
+    const int r = e & 63, c = e >> 6;
+    sP[r + c * kLdP] = W[e];
+    sQ[r + c * kLdQ] = (r < kb && c < rc) ? y[r + (c0 + c) * nf] : T(0);
   }
-#pragma unroll 8
-  for (int i = 0; i < kPanel; ++i)
-    if (i < kb) y[i] = v[i];
+  __syncthreads();
+  mm64<T>(sP, sQ, sQ, kLdQ);
+  for (int e = threadIdx.x; e < kb * rc; e += blockDim.x) {
+    const int r = e % kb, c = e / kb;
+    y[r + (c0 + c) * nf] = sQ[r + c * kLdQ];
+  }
 }
 
 template <typename T>
@@ -204,37 +207,35 @@ __global__ void __launch_bounds__(256) k_bwd_gather(DevPlan P, SolveArgs A, cons
   for (int t = lane_id(); t < nu; t += 32) f[t] = xw[us[t] + col * A.ldx];
 }
 
-// Upper diagonal block solve of rows k0..k1-1 (backward); writes x.
+// Backward diagonal block: x = inv(U_kk) * f, written to the block rows and to x.
 template <typename T>
-__global__ void __launch_bounds__(64) k_bwd_diag(DevPlan P, const SolveBlockTask* __restrict__ tasks, int64_t nrhs,
-                                                 int64_t ldx, const T* __restrict__ pool, T* __restrict__ fsol,
-                                                 T* __restrict__ xw) {
-  __shared__ T Ud[64 * 65];
+__global__ void __launch_bounds__(kApplyThreads) k_bwd_diag(DevPlan P, const SolveBlockTask* __restrict__ tasks,
+                                                            int64_t nrhs, int64_t ldx, const T* __restrict__ dinv,
+                                                            T* __restrict__ fsol, T* __restrict__ xw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sP = reinterpret_cast<T*>(smem_raw);
+  T* sQ = sP + 64 * kLdP;
   const SolveBlockTask tk = tasks[blockIdx.x];
   const int s = tk.s, k0 = tk.k0;
   const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
   const int kb = min(kPanel, np - k0);
-  const T* F = pool + P.front_off[s];
-  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) Ud[e % kb + (e / kb) * 65] = F[(k0 + e % kb) + (int64_t)(k0 + e / kb) * nf];
-  __syncthreads();
-  const int64_t col = (int64_t)blockIdx.y * blockDim.x + threadIdx.x;
-  if (col >= nrhs) return;
-  T* y = fsol + P.colbase[s] * nrhs + col * nf + k0;
-  T v[kPanel];
-#pragma unroll 8
-  for (int i = 0; i < kPanel; ++i)
-    if (i < kb) v[i] = y[i];
-  for (int i = kb - 1; i >= 0; --i) {
-    T t = v[i];
-    for (int j = i + 1; j < kb; ++j) t -= Ud[i + j * 65] * v[j];
-    v[i] = t / Ud[i + i * 65];
+  const int64_t c0 = (int64_t)blockIdx.y * 64;
+  const int rc = (int)(nrhs - c0 < 64 ? nrhs - c0 : 64);
+  const T* W = dinv + (P.dinv_off[s] + k0 / kPanel) * (int64_t)kDinvElems + 4096;
+  T* y = fsol + P.colbase[s] * nrhs + k0;
+  for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
+    const int r = e & 63, c = e >> 6;
+    sP[r + c * kLdP] = W[e];
+    sQ[r + c * kLdQ] = (r < kb && c < rc) ? y[r + (c0 + c) * nf] : T(0);
   }
-#pragma unroll 8
-  for (int i = 0; i < kPanel; ++i)
-    if (i < kb) {
-      y[i] = v[i];
-      xw[c1 + k0 + i + col * ldx] = v[i];
-    }
+  __syncthreads();
+  mm64<T>(sP, sQ, sQ, kLdQ);
+  for (int e = threadIdx.x; e < kb * rc; e += blockDim.x) {
+    const int r = e % kb, c = e / kb;
+    const T v = sQ[r + c * kLdQ];
+    y[r + (c0 + c) * nf] = v;
+    xw[c1 + k0 + r + (c0 + c) * ldx] = v;
+  }
 }
 
 // x[q[k]] = x_factor[k] (interface.jl:134-136); optionally accumulate (x += d).

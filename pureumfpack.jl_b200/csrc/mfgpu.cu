@@ -130,7 +130,7 @@ struct mfgpu_ctx {
   DevBuf b_small, b_panel, b_trsm, b_gemm;
   bool launches_safe = false;
   // numeric state
-  DevBuf b_pool, b_vx, b_ax, b_rs, b_ipiv, b_info, b_prow, b_rowfac, b_flags;
+  DevBuf b_pool, b_vx, b_ax, b_rs, b_ipiv, b_info, b_prow, b_rowfac, b_flags, b_dinv, b_dinv_off;
   bool have_rs = false;
   int factor_precision = MFGPU_PRECISION_FP64;
   DevBuf b_li, b_lx, b_ui, b_ux;
@@ -150,10 +150,27 @@ struct mfgpu_ctx {
     int kc;
     cudaEvent_t a, b;
     double flops, bytes;
+    int32_t level;
+    int64_t tasks;
   };
   std::vector<Pending> pending;
+  struct Record {   // one profiled launch
+    int kc;
+    int32_t level;
+    int64_t tasks;
+    float ms;
+    double flops, bytes;
+  };
+  std::vector<Record> records;
   std::vector<cudaEvent_t> evpool;
   size_t evnext = 0;
+  // CUDA graphs of the static launch sequences (keyed by everything a replay
+  // bakes in: sizes, flags and buffer addresses)
+  bool use_graphs = true;
+  std::vector<uintptr_t> factor_key, solve_key;
+  cudaGraphExec_t factor_exec = nullptr, solve_exec = nullptr;
+  int64_t factor_nodes = 0, solve_nodes = 0;   // kernel launches inside each graph
+  int64_t graph_replays = 0, graph_captures = 0;
 };
 
 namespace {
@@ -205,6 +222,7 @@ void upload_plan(mfgpu_ctx* h) {
   upload(h->b_csr_ptr, P.csr_ptr, st);
   upload(h->b_csr_col, P.csr_col, st);
   upload(h->b_csr_src, P.csr_src, st);
+  upload(h->b_dinv_off, P.dinv_off, st);
   DevPlan& d = h->dp;
   d.n = P.n;
   d.ns = P.ns;
@@ -234,6 +252,7 @@ void upload_plan(mfgpu_ctx* h) {
   d.csr_ptr = h->b_csr_ptr.as<int32_t>();
   d.csr_col = h->b_csr_col.as<int32_t>();
   d.csr_src = h->b_csr_src.as<int32_t>();
+  d.dinv_off = h->b_dinv_off.as<int64_t>();
 }
 
 void upload_launches(mfgpu_ctx* h) {
@@ -267,7 +286,7 @@ cudaEvent_t next_event(mfgpu_ctx* h) {
 // and, when profiling is on, brackets the launch with CUDA events on the
 // launching stream and books its algorithmic work to its kernel class.
 template <typename F>
-void klaunch(mfgpu_ctx* h, int kc, double flops, double bytes, F&& f) {
+void klaunch(mfgpu_ctx* h, int kc, double flops, double bytes, F&& f, int32_t level = -1, int64_t tasks = 0) {
   ++h->launch_count;
   if (!h->profiling) {
     f();
@@ -277,7 +296,7 @@ void klaunch(mfgpu_ctx* h, int kc, double flops, double bytes, F&& f) {
   CK(cudaEventRecord(a, h->stream));
   f();
   CK(cudaEventRecord(b, h->stream));
-  h->pending.push_back({kc, a, b, flops, bytes});
+  h->pending.push_back({kc, a, b, flops, bytes, level, tasks});
 }
 
 void prof_flush(mfgpu_ctx* h) {
@@ -289,27 +308,32 @@ void prof_flush(mfgpu_ctx* h) {
     k.flops += p.flops;
     k.bytes += p.bytes;
     ++k.launches;
+    if (h->records.size() < 200000) h->records.push_back({p.kc, p.level, p.tasks, ms, p.flops, p.bytes});
   }
   h->pending.clear();
   h->evnext = 0;
 }
 
 template <typename T>
-size_t panel_smem_bytes() {
-  return (size_t)kPivRowsSmem * kPanel * sizeof(T);
+size_t panel_smem_bytes(int rows) {
+  return ((size_t)rows * kPanel + 4 * 64 + rows) * sizeof(T);
 }
 
 template <typename T>
-size_t trsm_smem_bytes() {
-  return (size_t)2 * 64 * 65 * sizeof(T);
+size_t apply_smem_bytes() {
+  return (size_t)64 * (kLdP + kLdQ) * sizeof(T);
 }
 
 template <typename T>
 void configure_kernels() {
   static bool done = false;
   if (done) return;
-  CK(cudaFuncSetAttribute(k_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_smem_bytes<T>()));
-  CK(cudaFuncSetAttribute(k_panel_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem_bytes<T>()));
+  CK(cudaFuncSetAttribute(k_panel<T, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_smem_bytes<T>(64)));
+  CK(cudaFuncSetAttribute(k_panel<T, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_smem_bytes<T>(128)));
+  CK(cudaFuncSetAttribute(k_panel<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_smem_bytes<T>(256)));
+  CK(cudaFuncSetAttribute(k_panel_apply<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem_bytes<T>()));
+  CK(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem_bytes<T>()));
+  CK(cudaFuncSetAttribute(k_bwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem_bytes<T>()));
   done = true;
 }
 
@@ -346,32 +370,101 @@ void run_factor_launches(mfgpu_ctx* h) {
         klaunch(h, KC_SMALL, L.flops, bytes, [&] {
           k_small_fronts<T><<<(unsigned)L.count, kSmallThreads, kSmallFront * kSmallFront * sizeof(T), st>>>(
               h->dp, S, h->b_small.as<int32_t>() + L.first, pool, vx);
-        });
+        }, L.level, L.count);
         break;
       case kLaunchAssemble:
         klaunch(h, KC_ASSEMBLE, 0, bytes, [&] {
           k_assemble_columns<T><<<grid1(L.count, 8), 256, 0, st>>>(h->dp, L.first, L.count, pool, vx);
-        });
+        }, L.level, L.count);
         break;
       case kLaunchPanel:
         klaunch(h, KC_PANEL, L.flops, bytes, [&] {
-          k_panel<T><<<(unsigned)L.count, kPanelThreads, panel_smem_bytes<T>(), st>>>(
-              h->dp, S, h->b_panel.as<PanelTask>() + L.first, pool);
-        });
+          const PanelTask* pt = h->b_panel.as<PanelTask>() + L.first;
+          T* dinv = h->b_dinv.as<T>();
+          if (L.rows <= 64)
+            k_panel<T, 64><<<(unsigned)L.count, 64, panel_smem_bytes<T>(64), st>>>(h->dp, S, pt, pool, dinv);
+          else if (L.rows <= 128)
+            k_panel<T, 128><<<(unsigned)L.count, 128, panel_smem_bytes<T>(128), st>>>(h->dp, S, pt, pool, dinv);
+          else
+            k_panel<T, 256><<<(unsigned)L.count, 256, panel_smem_bytes<T>(256), st>>>(h->dp, S, pt, pool, dinv);
+        }, L.level * 1000 + L.rows, L.count);
         break;
       case kLaunchTrsm:
         klaunch(h, KC_TRSM, L.flops, bytes, [&] {
-          k_panel_trsm<T><<<(unsigned)L.tiles, kTrsmThreads, trsm_smem_bytes<T>(), st>>>(
-              h->dp, S, h->b_trsm.as<TrsmTask>() + L.first, (int)L.count, pool);
-        });
+          k_panel_apply<T><<<(unsigned)L.tiles, kApplyThreads, apply_smem_bytes<T>(), st>>>(
+              h->dp, S, h->b_trsm.as<TrsmTask>() + L.first, (int)L.count, pool, h->b_dinv.as<T>());
+        }, L.level, L.tiles);
         break;
       case kLaunchGemm:
         klaunch(h, KC_GEMM_FACTOR, L.flops, bytes, [&] {
           launch_gemm<T>(h->b_gemm.as<GemmTask>() + L.first, L.count, L.tiles, pool, pool, pool, st);
-        });
+        }, L.level, L.tiles);
         break;
     }
   }
+  CK(cudaGetLastError());
+}
+
+// Run `issue` on the handle's stream: replayed from a CUDA graph when the
+// key matches the cached one, captured first otherwise; eager when profiling
+// (per-launch events) or when graphs are disabled.
+template <typename F>
+void run_sequence(mfgpu_ctx* h, std::vector<uintptr_t>& cached_key, cudaGraphExec_t& exec, int64_t& nodes,
+                  const std::vector<uintptr_t>& key, F&& issue) {
+  if (h->profiling || !h->use_graphs) {
+    issue();
+    return;
+  }
+  if (!exec || cached_key != key) {
+    const int64_t before = h->launch_count;
+    if (exec) {
+      cudaGraphExecDestroy(exec);
+      exec = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      issue();
+    } catch (...) {
+      cudaStreamEndCapture(h->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    CK(cudaStreamEndCapture(h->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    cached_key = key;
+    nodes = h->launch_count - before;
+    h->launch_count = before;
+    ++h->graph_captures;
+  }
+  CK(cudaGraphLaunch(exec, h->stream));
+  h->launch_count += nodes;   // the kernels of the replayed graph
+  ++h->graph_replays;
+}
+
+template <typename T>
+void issue_factor(mfgpu_ctx* h) {
+  const Plan& P = h->plan;
+  cudaStream_t st = h->stream;
+  klaunch(h, KC_BUILD_VALUES, P.nnz_a, 32.0 * P.nnz_a, [&] {
+    k_build_values<<<grid1(P.nnz_a, 256), 256, 0, st>>>(P.nnz_a, h->b_v_src.as<int32_t>(), h->b_v_srow.as<int32_t>(),
+                                                          h->b_ax.as<double>(),
+                                                          h->have_rs ? h->b_rs.as<double>() : nullptr,
+                                                          h->b_vx.as<double>());
+  });
+  if (P.ns) k_fill_i32<<<grid1(P.ns, 256), 256, 0, st>>>(h->b_info.as<int32_t>(), P.ns, INT32_MAX);
+  CK(cudaMemsetAsync(h->b_flags.p, 0, 16, st));
+  run_factor_launches<T>(h);
+  if (P.ns)
+    klaunch(h, KC_PIVOTS, 0, 16.0 * P.n, [&] { k_finalize_pivots<<<grid1(P.ns, 128), 128, 0, st>>>(h->dp, dev_state(h)); });
+  if (P.fc_total)
+    klaunch(h, KC_SCATTER, 0, (double)(P.nnz_l + P.nnz_u) * (16.0 + sizeof(T)), [&] {
+      k_scatter_csc<T><<<grid1(P.fc_total, 8), 256, 0, st>>>(h->dp, dev_state(h), h->b_pool.as<T>(), P.fc_total,
+                                                             h->b_li.as<int64_t>(), h->b_lx.as<double>(),
+                                                             h->b_ui.as<int64_t>(), h->b_ux.as<double>());
+    });
   CK(cudaGetLastError());
 }
 
@@ -387,17 +480,20 @@ int factor_impl(mfgpu_ctx* h, int32_t check) {
   h->b_info.ensure(std::max<int64_t>(P.ns, 1) * 4);
   h->b_flags.ensure(16);
   h->b_vx.ensure(std::max<int64_t>(P.nnz_a, 1) * 8);
+  h->b_dinv.ensure(std::max<size_t>((size_t)P.dinv_blocks * kDinvElems * sizeof(T), 16));
+  h->b_li.ensure(std::max<int64_t>(P.nnz_l, 1) * 8);
+  h->b_lx.ensure(std::max<int64_t>(P.nnz_l, 1) * 8);
+  h->b_ui.ensure(std::max<int64_t>(P.nnz_u, 1) * 8);
+  h->b_ux.ensure(std::max<int64_t>(P.nnz_u, 1) * 8);
   CK(cudaEventRecord(h->ev0, st));
-  klaunch(h, KC_BUILD_VALUES, P.nnz_a, 32.0 * P.nnz_a, [&] {
-    k_build_values<<<grid1(P.nnz_a, 256), 256, 0, st>>>(P.nnz_a, h->b_v_src.as<int32_t>(), h->b_v_srow.as<int32_t>(),
-                                                          h->b_ax.as<double>(),
-                                                          h->have_rs ? h->b_rs.as<double>() : nullptr,
-                                                          h->b_vx.as<double>());
-  });
   for (int attempt = 0; attempt < 2; ++attempt) {
-    if (P.ns) k_fill_i32<<<grid1(P.ns, 256), 256, 0, st>>>(h->b_info.as<int32_t>(), P.ns, INT32_MAX);
-    CK(cudaMemsetAsync(h->b_flags.p, 0, 16, st));
-    run_factor_launches<T>(h);
+    const std::vector<uintptr_t> key = {
+        sizeof(T), (uintptr_t)h->launches_safe, (uintptr_t)h->have_rs, (uintptr_t)h->b_pool.p, (uintptr_t)h->b_vx.p,
+        (uintptr_t)h->b_ax.p, (uintptr_t)h->b_rs.p, (uintptr_t)h->b_dinv.p, (uintptr_t)h->b_li.p,
+        (uintptr_t)h->b_lx.p, (uintptr_t)h->b_ui.p, (uintptr_t)h->b_ux.p, (uintptr_t)h->b_small.p,
+        (uintptr_t)h->b_panel.p, (uintptr_t)h->b_trsm.p, (uintptr_t)h->b_gemm.p, (uintptr_t)h->b_ipiv.p,
+        (uintptr_t)h->b_info.p, (uintptr_t)h->b_flags.p, (uintptr_t)st};
+    run_sequence(h, h->factor_key, h->factor_exec, h->factor_nodes, key, [&] { issue_factor<T>(h); });
     if (!P.has_speculative) break;
     int32_t flag = 0;
     CK(cudaMemcpyAsync(&flag, h->b_flags.p, 4, cudaMemcpyDeviceToHost, st));
@@ -405,25 +501,12 @@ int factor_impl(mfgpu_ctx* h, int32_t check) {
     if (!flag) break;
     // a speculative panel met a row that partial pivoting would have chosen:
     // redo the factorization with pivoting panels everywhere.
+    prof_flush(h);
     build_launches(P, true);
     upload_launches(h);
     h->launches_safe = true;
     ++h->factor_reruns;
   }
-  if (P.ns)
-    klaunch(h, KC_PIVOTS, 0, 16.0 * P.n, [&] { k_finalize_pivots<<<grid1(P.ns, 128), 128, 0, st>>>(h->dp, dev_state(h)); });
-  // direct CSC scatter of L and U
-  h->b_li.ensure(std::max<int64_t>(P.nnz_l, 1) * 8);
-  h->b_lx.ensure(std::max<int64_t>(P.nnz_l, 1) * 8);
-  h->b_ui.ensure(std::max<int64_t>(P.nnz_u, 1) * 8);
-  h->b_ux.ensure(std::max<int64_t>(P.nnz_u, 1) * 8);
-  if (P.fc_total)
-    klaunch(h, KC_SCATTER, 0, (double)(P.nnz_l + P.nnz_u) * (16.0 + sizeof(T)), [&] {
-      k_scatter_csc<T><<<grid1(P.fc_total, 8), 256, 0, st>>>(h->dp, dev_state(h), h->b_pool.as<T>(), P.fc_total,
-                                                             h->b_li.as<int64_t>(), h->b_lx.as<double>(),
-                                                             h->b_ui.as<int64_t>(), h->b_ux.as<double>());
-    });
-  CK(cudaGetLastError());
   CK(cudaEventRecord(h->ev1, st));
   // status: first supernode (postorder) with a zero pivot
   std::vector<int32_t> info(P.ns);
@@ -515,8 +598,10 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
           d.elems += (double)(k1 - k0) * (k1 - k0) + 2.0 * (k1 - k0) * R;
           const int64_t fb = P.colbase[s] * R;
           const int nf = P.nf[s];
-          add_gemm(S.gemms, g.tiles, P.front_off[s] + k1 + (int64_t)k0 * nf, fb + k0, fb + k1, nf - k1, (int)R,
-                   k1 - k0, nf, nf, nf);
+          // rows of the pivot block below this block; the update rows are
+          // done once, after the whole pivot block (K = np)
+          add_gemm(S.gemms, g.tiles, P.front_off[s] + k1 + (int64_t)k0 * nf, fb + k0, fb + k1, P.np[s] - k1,
+                   (int)R, k1 - k0, nf, nf, nf);
         }
         g.count = (int64_t)S.gemms.size() - g.first;
         g.flops = work_flops;
@@ -524,6 +609,19 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
         if (d.count) S.steps.push_back(d);
         if (g.count) S.steps.push_back(g);
       }
+      // w = f[np:] - L21 * y for every large supernode of the level
+      SolveSchedule::Step g{3, (int64_t)S.gemms.size(), 0, 0};
+      work_flops = work_elems = 0;
+      for (int32_t i = m; i < e; ++i) {
+        const int32_t s = P.slot_super[i];
+        const int nf = P.nf[s], np = P.np[s];
+        const int64_t fb = P.colbase[s] * R;
+        add_gemm(S.gemms, g.tiles, P.front_off[s] + np, fb, fb + np, P.nu[s], (int)R, np, nf, nf, nf);
+      }
+      g.count = (int64_t)S.gemms.size() - g.first;
+      g.flops = work_flops;
+      g.elems = work_elems;
+      if (g.count) S.steps.push_back(g);
     }
   }
   // backward, root to leaves
@@ -590,14 +688,21 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
 // One solve A x = b for device b (ldb) into device x (ldx) (x overwritten, or
 // accumulated when `accumulate`).
 template <typename T>
+void prepare_solve(mfgpu_ctx* h, int64_t R, int refine) {
+  const Plan& P = h->plan;
+  build_solve_schedule(h, R);
+  h->b_fsol.ensure(std::max<size_t>((size_t)P.fc_total * R * sizeof(T), 16));
+  h->b_xw.ensure(std::max<size_t>((size_t)P.n * R * sizeof(T), 16));
+  if (refine > 0) h->b_r.ensure(std::max<size_t>((size_t)P.n * R * 8, 16));
+  configure_kernels<T>();
+}
+
+template <typename T>
 void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double* d_x, int64_t ldx, bool use_rs,
                 int accumulate) {
   const Plan& P = h->plan;
   cudaStream_t st = h->stream;
-  build_solve_schedule(h, R);
   SolveSchedule& S = h->sched;
-  h->b_fsol.ensure(std::max<size_t>((size_t)P.fc_total * R * sizeof(T), 16));
-  h->b_xw.ensure(std::max<size_t>((size_t)P.n * R * sizeof(T), 16));
   T* pool = h->b_pool.as<T>();
   T* fsol = h->b_fsol.as<T>();
   T* xw = h->b_xw.as<T>();
@@ -625,7 +730,8 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
         break;
       case 2:
         klaunch(h, KC_FWD_DIAG, s.flops, bytes, [&] {
-          k_fwd_diag<T><<<dim3((unsigned)s.count, tchunks), 64, 0, st>>>(h->dp, blocks + s.first, R, pool, fsol);
+          k_fwd_diag<T><<<dim3((unsigned)s.count, tchunks), kApplyThreads, apply_smem_bytes<T>(), st>>>(
+              h->dp, blocks + s.first, R, h->b_dinv.as<T>(), fsol);
         });
         break;
       case 3:
@@ -646,8 +752,8 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
         break;
       case 6:
         klaunch(h, KC_BWD_DIAG, s.flops, bytes, [&] {
-          k_bwd_diag<T><<<dim3((unsigned)s.count, tchunks), 64, 0, st>>>(h->dp, blocks + s.first, R, P.n, pool,
-                                                                         fsol, xw);
+          k_bwd_diag<T><<<dim3((unsigned)s.count, tchunks), kApplyThreads, apply_smem_bytes<T>(), st>>>(
+              h->dp, blocks + s.first, R, P.n, h->b_dinv.as<T>(), fsol, xw);
         });
         break;
     }
@@ -666,7 +772,6 @@ void solve_refine(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, doubl
   cudaStream_t st = h->stream;
   solve_once<T>(h, R, d_b, ldb, d_x, ldx, use_rs, 0);
   if (refine > 0) {
-    h->b_r.ensure(std::max<size_t>((size_t)P.n * R * 8, 16));
     double* r = h->b_r.as<double>();
     for (int it = 0; it < refine; ++it) {
       klaunch(h, KC_RESIDUAL, 2.0 * P.nnz_a * R, 16.0 * P.nnz_a + 24.0 * P.n * R, [&] {
@@ -680,9 +785,23 @@ void solve_refine(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, doubl
   CK(cudaGetLastError());
 }
 
+template <typename T>
+void solve_graph(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double* d_x, int64_t ldx, int refine) {
+  prepare_solve<T>(h, R, refine);
+  const SolveSchedule& S = h->sched;
+  const std::vector<uintptr_t> key = {
+      sizeof(T), (uintptr_t)R, (uintptr_t)d_b, (uintptr_t)ldb, (uintptr_t)d_x, (uintptr_t)ldx, (uintptr_t)refine,
+      (uintptr_t)h->have_rs, (uintptr_t)h->b_rs.p, (uintptr_t)h->b_pool.p, (uintptr_t)h->b_dinv.p,
+      (uintptr_t)h->b_fsol.p, (uintptr_t)h->b_xw.p, (uintptr_t)h->b_r.p, (uintptr_t)h->b_ax.p,
+      (uintptr_t)S.d_ids.p, (uintptr_t)S.d_blocks.p, (uintptr_t)S.d_gemms.p, (uintptr_t)h->b_prow.p,
+      (uintptr_t)h->b_rowfac.p, (uintptr_t)h->stream};
+  run_sequence(h, h->solve_key, h->solve_exec, h->solve_nodes, key,
+               [&] { solve_refine<T>(h, R, d_b, ldb, d_x, ldx, refine, true); });
+}
+
 void solve_dispatch(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double* d_x, int64_t ldx, int refine) {
-  if (h->factor_precision == MFGPU_PRECISION_MIXED) solve_refine<float>(h, R, d_b, ldb, d_x, ldx, refine, true);
-  else solve_refine<double>(h, R, d_b, ldb, d_x, ldx, refine, true);
+  if (h->factor_precision == MFGPU_PRECISION_MIXED) solve_graph<float>(h, R, d_b, ldb, d_x, ldx, refine);
+  else solve_graph<double>(h, R, d_b, ldb, d_x, ldx, refine);
 }
 
 int analyze_common(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf,
@@ -693,6 +812,11 @@ int analyze_common(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const int64_t
   upload_plan(h);
   upload_launches(h);
   h->launches_safe = false;
+  if (h->factor_exec) cudaGraphExecDestroy(h->factor_exec);
+  if (h->solve_exec) cudaGraphExecDestroy(h->solve_exec);
+  h->factor_exec = h->solve_exec = nullptr;
+  h->factor_key.clear();
+  h->solve_key.clear();
   h->analyzed = true;
   h->factored = false;
   h->csc_ready = false;
@@ -757,10 +881,13 @@ void mfgpu_destroy(mfgpu_ctx* h) {
                     &h->b_v_frow, &h->b_fc_super, &h->b_fc_vbeg, &h->b_fc_vend, &h->b_fc_ch_ptr, &h->b_fc_ch,
                     &h->b_lcolptr, &h->b_ucolptr, &h->b_qf, &h->b_csr_ptr, &h->b_csr_col, &h->b_csr_src,
                     &h->b_small, &h->b_panel, &h->b_trsm, &h->b_gemm, &h->b_pool, &h->b_vx, &h->b_ax, &h->b_rs,
-                    &h->b_ipiv, &h->b_info, &h->b_prow, &h->b_rowfac, &h->b_flags, &h->b_li, &h->b_lx, &h->b_ui,
+                    &h->b_ipiv, &h->b_info, &h->b_prow, &h->b_rowfac, &h->b_flags, &h->b_dinv, &h->b_dinv_off,
+                    &h->b_li, &h->b_lx, &h->b_ui,
                     &h->b_ux, &h->b_fsol, &h->b_xw, &h->b_b, &h->b_x, &h->b_r, &h->b_d, &h->b_err, &h->b_norm,
                     &h->sched.d_ids, &h->sched.d_blocks, &h->sched.d_gemms};
   for (DevBuf* b : bufs) b->release();
+  if (h->factor_exec) cudaGraphExecDestroy(h->factor_exec);
+  if (h->solve_exec) cudaGraphExecDestroy(h->solve_exec);
   for (cudaEvent_t e : h->evpool) cudaEventDestroy(e);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
@@ -999,7 +1126,10 @@ int mfgpu_stats_json(mfgpu_ctx* h, char* buf, int64_t cap) {
   std::string js(tmp);
   js.pop_back();   // reopen the object
   char item[512];
-  std::snprintf(item, sizeof item, ", \"launches\": %lld, \"profiling\": %s, \"kernels\": {", (long long)h->launch_count,
+  std::snprintf(item, sizeof item,
+                ", \"launches\": %lld, \"graph_replays\": %lld, \"graph_captures\": %lld, \"profiling\": %s, "
+                "\"kernels\": {",
+                (long long)h->launch_count, (long long)h->graph_replays, (long long)h->graph_captures,
                 h->profiling ? "true" : "false");
   js += item;
   bool first = true;
@@ -1017,8 +1147,25 @@ int mfgpu_stats_json(mfgpu_ctx* h, char* buf, int64_t cap) {
   return MFGPU_OK;
 }
 
+int mfgpu_launch_records(mfgpu_ctx* h, char* buf, int64_t cap) {
+  if (!h || !buf || cap <= 0) return MFGPU_ERR_ARGUMENT;
+  std::string js = "[";
+  char item[256];
+  for (size_t i = 0; i < h->records.size(); ++i) {
+    const auto& r = h->records[i];
+    std::snprintf(item, sizeof item, "%s[\"%s\", %d, %lld, %.6f, %.6e, %.6e]", i ? ", " : "",
+                  kKernelClassName[r.kc], r.level, (long long)r.tasks, r.ms, r.flops, r.bytes);
+    js += item;
+  }
+  js += "]";
+  if ((int64_t)js.size() >= cap) return (int)std::min<int64_t>(js.size() + 1, INT32_MAX);
+  std::memcpy(buf, js.c_str(), js.size() + 1);
+  return MFGPU_OK;
+}
+
 int mfgpu_set_profiling(mfgpu_ctx* h, int32_t on) {
   if (!h) return MFGPU_ERR_ARGUMENT;
+  h->records.clear();
   h->profiling = on != 0;
   h->launch_count = 0;
   for (auto& k : h->kstat) k = KStat{};

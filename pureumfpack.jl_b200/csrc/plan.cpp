@@ -260,6 +260,14 @@ void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const i
       }
   }
 
+  // ---- inverted diagonal blocks of large fronts ------------------------------
+  P.dinv_off.assign(ns, -1);
+  for (int64_t s = 0; s < ns; ++s)
+    if (P.nf[s] > kSmallFront) {
+      P.dinv_off[s] = P.dinv_blocks;
+      P.dinv_blocks += ceil_div(P.np[s], kPanel);
+    }
+
   // ---- statistics ------------------------------------------------------------
   for (int64_t s = 0; s < ns; ++s) {
     const double a = P.np[s], u = P.nu[s];
@@ -332,22 +340,19 @@ void build_launches(Plan& P, bool safe) {
     int32_t maxnp = 0;
     for (int32_t s : large) maxnp = std::max(maxnp, P.np[s]);
     for (int32_t k0 = 0; k0 < maxnp; k0 += kPanel) {
-      Launch lp{kLaunchPanel, L, (int64_t)P.panel_tasks.size(), 0, 0};
       Launch lt{kLaunchTrsm, L, (int64_t)P.trsm_tasks.size(), 0, 0};
       Launch lg{kLaunchGemm, L, (int64_t)P.gemm_tasks.size(), 0, 0};
+      // panel tasks of this step, one launch per row class (64 / 128 / 256)
+      std::vector<PanelTask> cls[3];
       for (int32_t s : large) {
         const int32_t npv = P.np[s], nf = P.nf[s];
         if (npv <= k0) continue;
         const int32_t kb = std::min(kPanel, npv - k0), k1 = k0 + kb;
         int32_t mode = (npv - k0 <= kPivRowsSmem) ? kPanelSmemPivot : (safe ? kPanelGlobalPivot : kPanelSpeculative);
         if (mode == kPanelSpeculative) P.has_speculative = true;
-        P.panel_tasks.push_back(PanelTask{s, k0, mode, 0});
-        ++lp.count;
-        {
-          const double R = (mode == kPanelSpeculative) ? kb : (npv - k0);
-          lp.flops += R * kb * kb - kb * kb * kb / 3.0;
-          lp.elems += 2.0 * R * kb;
-        }
+        const int32_t R = (mode == kPanelSpeculative) ? kb : npv - k0;
+        const int c = (mode == kPanelGlobalPivot || R > 128) ? 2 : (R > 64 ? 1 : 0);
+        cls[c].push_back(PanelTask{s, k0, mode, 0});
         TrsmTask tt{};
         tt.s = s;
         tt.k0 = k0;
@@ -356,8 +361,8 @@ void build_launches(Plan& P, bool safe) {
         tt.ucol_tiles = (int32_t)ceil_div(nf - k1, 64);
         tt.check = (mode == kPanelSpeculative) ? 1 : 0;
         if (tt.lrow_tiles + tt.ucol_tiles > 0) {
-          lt.flops += (double)(nf - tt.r0) * kb * kb + (double)(nf - k1) * kb * kb;
-          lt.elems += 2.0 * ((double)(nf - tt.r0) * kb + (double)(nf - k1) * kb);
+          lt.flops += 2.0 * ((double)(nf - tt.r0) * kb * kb + (double)(nf - k1) * kb * kb);
+          lt.elems += 2.0 * ((double)(nf - tt.r0) * kb + (double)(nf - k1) * kb) + 2.0 * 64 * 64;
           tt.tile_base = lt.tiles;
           lt.tiles += tt.lrow_tiles + tt.ucol_tiles;
           P.trsm_tasks.push_back(tt);
@@ -386,8 +391,19 @@ void build_launches(Plan& P, bool safe) {
                    npv - k1, nf - npv, kb);
         }
       }
-      lp.tiles = lp.count;
-      if (lp.count) P.launches.push_back(lp);
+      for (int c = 0; c < 3; ++c) {
+        if (cls[c].empty()) continue;
+        Launch lp{kLaunchPanel, L, (int64_t)P.panel_tasks.size(), (int64_t)cls[c].size(), (int64_t)cls[c].size()};
+        lp.rows = 64 << c;
+        for (const PanelTask& pt : cls[c]) {
+          const int32_t kb = std::min(kPanel, P.np[pt.s] - pt.k0);
+          const double R = (pt.mode == kPanelSpeculative) ? kb : (P.np[pt.s] - pt.k0);
+          lp.flops += 2.0 * (R * kb * kb - (double)kb * kb * kb / 3.0) + 4.0 / 3.0 * kb * kb * kb;
+          lp.elems += 2.0 * R * kb + 2.0 * 64 * 64;
+          P.panel_tasks.push_back(pt);
+        }
+        P.launches.push_back(lp);
+      }
       if (lt.count) P.launches.push_back(lt);
       if (lg.count) P.launches.push_back(lg);
     }

@@ -66,6 +66,7 @@ struct Launch {
   int64_t first;         // offset into the task array of this kind (or fc begin)
   int64_t count;         // tasks (or fc count)
   int64_t tiles;         // grid size in tiles for TRSM / GEMM
+  int32_t rows = 0;      // panel launches: row capacity (threads) of the kernel variant
   double flops = 0;      // algorithmic flops of the launch
   double elems = 0;      // algorithmic element moves (x sizeof(front type) = bytes)
   double extra_bytes = 0;// index / FP64 input bytes
@@ -103,6 +104,9 @@ struct Plan {
   // qf (0-based) and original A in CSR for the residual
   std::vector<int32_t> qf;
   std::vector<int32_t> csr_ptr, csr_col, csr_src;
+  // inverted 64x64 diagonal blocks of the large fronts' pivot blocks
+  std::vector<int64_t> dinv_off;      // per supernode, -1 for small fronts
+  int64_t dinv_blocks = 0;
   // launch sequences
   std::vector<int32_t> small_tasks;
   std::vector<PanelTask> panel_tasks;

@@ -48,6 +48,7 @@ SIGNATURES = [
     ("mfgpu_backward_error_device", ctypes.c_int, [vp, i64, vp, i64, vp, i64, f64p]),
     ("mfgpu_stats_json", ctypes.c_int, [vp, ctypes.c_char_p, i64]),
     ("mfgpu_set_profiling", ctypes.c_int, [vp, i32]),
+    ("mfgpu_launch_records", ctypes.c_int, [vp, ctypes.c_char_p, i64]),
 ]
 
 _lib = None

@@ -303,6 +303,18 @@ class GpuContext:
     def set_profiling(self, on: bool):
         self._check(self._lib.mfgpu_set_profiling(self._h, int(bool(on))))
 
+    def launch_records(self) -> list:
+        """Profiled launches: [kernel class, level, tasks, ms, flops, bytes]."""
+        cap = 1 << 20
+        while True:
+            buf = ctypes.create_string_buffer(cap)
+            rc = self._lib.mfgpu_launch_records(self._h, buf, cap)
+            if rc == 0:
+                return json.loads(buf.value.decode())
+            if rc < 0:
+                self._check(rc)
+            cap = rc + 16
+
     def __del__(self):
         if getattr(self, "_h", None):
             try:

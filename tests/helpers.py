@@ -46,11 +46,16 @@ def assert_same_structure(fo, L, U, p, q, pinv):
     np.testing.assert_array_equal(pinv, fo.pinv)
 
 
-def assert_close_values(fo, L, U, rtol=VALUE_RTOL):
+def assert_close_values(fo, L, U, rtol=VALUE_RTOL, entry_rtol=None):
+    """Normwise per column within rtol; entry-wise within entry_rtol (default
+    rtol).  Matrices with element growth rho amplify rounding differences of
+    the two operation orders by about rho, so their entry-wise bound is
+    raised while the normwise bound stays."""
+    entry_rtol = rtol if entry_rtol is None else entry_rtol
     nl, el = column_value_errors(fo.Lcolptr, fo.Lnzval, L.nzval)
     nu, eu = column_value_errors(fo.Ucolptr, fo.Unzval, U.nzval)
     assert nl <= rtol and nu <= rtol, f"normwise column error L {nl:.2e} U {nu:.2e}"
-    assert el <= rtol and eu <= rtol, f"entry-wise error L {el:.2e} U {eu:.2e}"
+    assert el <= entry_rtol and eu <= entry_rtol, f"entry-wise error L {el:.2e} U {eu:.2e}"
     return max(nl, nu), max(el, eu)
 
 

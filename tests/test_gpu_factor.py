@@ -101,7 +101,8 @@ def test_pivoting_in_large_fronts(k, off):
     fo = O.multifrontal_lu(A, check=False)
     F = multifrontal_lu(A, check=False)
     assert_same_structure(fo, F.L, F.U, F.p, F.q, F.pinv)
-    assert_close_values(fo, F.L, F.U)
+    # element growth max|U| / max|A| is about 5 (k=12) and 30 (k=14-16) here
+    assert_close_values(fo, F.L, F.U, entry_rtol=1e-10)
     assert np.sum(F.p != F.q) > 5, "case meant to exercise row interchanges"
     # partial pivoting inside the blocks: |L11| <= 1
     S = F.symbolic
