@@ -1,0 +1,114 @@
+# MFGPU.jl -- ccall shim that routes PureUMFPACK.jl's multifrontal path to
+# libmfgpu.so (include/mfgpu.h).  Drop this file into the reference package
+# (e.g. src/mfgpu.jl, `include("mfgpu.jl")` after "multifrontal.jl") and set
+# ENV["PUREUMFPACK_MFGPU"] to the library path.  The host keeps the
+# reference's own ordering, scaling and symbolic analysis (symbolic_mf); the
+# numeric factorization and the solves run on the GPU.
+#
+# Not executed in the build image (no Julia toolchain there); the Python
+# binding pureumfpack/_lib.py drives the same symbols and is what the tests run.
+
+module MFGPU
+
+using SparseArrays: SparseMatrixCSC, nonzeros, rowvals
+
+const libmfgpu = get(ENV, "PUREUMFPACK_MFGPU", joinpath(@__DIR__, "..", "pureumfpack", "libmfgpu.so"))
+
+mutable struct Handle
+    ptr::Ptr{Cvoid}
+    n::Int
+end
+
+function _check(h::Handle, rc::Cint)
+    rc >= 0 && return Int(rc)
+    msg = unsafe_string(ccall((:mfgpu_last_error, libmfgpu), Cstring, (Ptr{Cvoid},), h.ptr))
+    rc == -1 && throw(ArgumentError(msg))
+    rc == -6 && throw(DimensionMismatch(msg))
+    error("libmfgpu error $rc: $msg")
+end
+
+function create(; device::Integer = 0, precision::Integer = 0)
+    opts = Ref((Int32(device), Int32(precision), Int32(0), Int32(0)))
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    rc = ccall((:mfgpu_create, libmfgpu), Cint, (Ref{NTuple{4, Int32}}, Ref{Ptr{Cvoid}}), opts, out)
+    rc == 0 || error("mfgpu_create failed ($rc)")
+    h = Handle(out[], 0)
+    finalizer(x -> ccall((:mfgpu_destroy, libmfgpu), Cvoid, (Ptr{Cvoid},), x.ptr), h)
+    return h
+end
+
+# mfgpu_analyze from the reference's SymbolicMF (src/symbolic.jl:203-209):
+# update set of supernode s = colstruct[sstart[s+1]-1].
+function analyze!(h::Handle, A::SparseMatrixCSC{Float64, Int64}, S)
+    n = size(A, 2)
+    nsuper = length(S.sstart) - 1
+    upd_ptr = Vector{Int64}(undef, nsuper + 1)
+    upd_ptr[1] = 1
+    for s in 1:nsuper
+        upd_ptr[s + 1] = upd_ptr[s] + length(S.colstruct[S.sstart[s + 1] - 1])
+    end
+    upd_idx = Vector{Int64}(undef, upd_ptr[end] - 1)
+    for s in 1:nsuper
+        copyto!(upd_idx, upd_ptr[s], S.colstruct[S.sstart[s + 1] - 1], 1, upd_ptr[s + 1] - upd_ptr[s])
+    end
+    rc = ccall((:mfgpu_analyze, libmfgpu), Cint,
+        (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}),
+        h.ptr, n, A.colptr, rowvals(A), collect(Int64, S.qf), collect(Int64, S.parent), nsuper,
+        collect(Int64, S.sstart), upd_ptr, upd_idx)
+    _check(h, rc)
+    h.n = n
+    return h
+end
+
+# Numeric factorization of Diagonal(Rs) * A (Rs === nothing: no scaling).
+function factor!(h::Handle, A::SparseMatrixCSC{Float64, Int64}, Rs, check::Bool)
+    rs = Rs === nothing ? C_NULL : pointer(Rs)
+    rc = GC.@preserve Rs ccall((:mfgpu_factor, libmfgpu), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int32),
+        h.ptr, nonzeros(A), rs, Int32(check))
+    st = _check(h, rc)
+    st > 0 && throw(Main.LinearAlgebra.SingularException(st))
+    return h
+end
+
+# GPLUFactorization fields (src/gplu.jl:45-51) copied back from the GPU.
+function factors(h::Handle)
+    sz = Vector{Int64}(undef, 3)
+    _check(h, ccall((:mfgpu_factor_sizes, libmfgpu), Cint, (Ptr{Cvoid}, Ptr{Int64}), h.ptr, sz))
+    n, nl, nu = sz
+    Lp = Vector{Int64}(undef, n + 1); Li = Vector{Int64}(undef, nl); Lx = Vector{Float64}(undef, nl)
+    Up = Vector{Int64}(undef, n + 1); Ui = Vector{Int64}(undef, nu); Ux = Vector{Float64}(undef, nu)
+    p = Vector{Int64}(undef, n); q = Vector{Int64}(undef, n); pinv = Vector{Int64}(undef, n)
+    _check(h, ccall((:mfgpu_get_factors, libmfgpu), Cint,
+        (Ptr{Cvoid}, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}, Ptr{Int64},
+         Ptr{Int64}, Ptr{Int64}), h.ptr, Lp, Li, Lx, Up, Ui, Ux, p, q, pinv))
+    return SparseMatrixCSC(n, n, Lp, Li, Lx), SparseMatrixCSC(n, n, Up, Ui, Ux), p, q, pinv
+end
+
+# solve(F, b; refine) for a vector or an n x k matrix of right-hand sides.
+function solve(h::Handle, B::AbstractVecOrMat{Float64}; refine::Integer = 0)
+    Bc = Matrix{Float64}(reshape(B, size(B, 1), :))
+    X = similar(Bc)
+    n = size(Bc, 1)
+    _check(h, ccall((:mfgpu_solve, libmfgpu), Cint, (Ptr{Cvoid}, Int64, Ptr{Float64}, Int64, Ptr{Float64}, Int64, Int32),
+        h.ptr, size(Bc, 2), Bc, n, X, n, Int32(refine)))
+    return B isa AbstractVector ? vec(X) : X
+end
+
+end # module
+
+# --- the reference-side change (in src/interface.jl / src/multifrontal.jl) ---
+#
+#   struct GPUPureLU{Tv,Ti,Tr}  # PureLU plus the device handle
+#       F::PureLU{Tv,Ti,Tr}
+#       h::MFGPU.Handle
+#   end
+#
+#   # splu(A; method=:multifrontal) branch (src/interface.jl:103-105):
+#   S = symbolic_mf(A)                       # the reference's own host code
+#   h = MFGPU.analyze!(MFGPU.create(), A, S)
+#   MFGPU.factor!(h, A, scale == SCALE_NONE ? nothing : Rs, check)
+#   L, U, p, q, _ = MFGPU.factors(h)
+#   return GPUPureLU(PureLU(L, U, p, q, Rs, A), h)
+#
+#   solve(F::GPUPureLU, b; refine=0) = MFGPU.solve(F.h, b; refine = refine)
+#   Base.:\(F::GPUPureLU, b::AbstractVector) = solve(F, b)
