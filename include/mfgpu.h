@@ -149,6 +149,24 @@ int mfgpu_solve_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ld
 int mfgpu_backward_error_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ldb, const double* d_x,
                                 int64_t ldx, double* out);
 
+/* The same backward error, computed without allocating device memory, for
+ * callers that cannot allocate when they check accuracy (services that
+ * reserve all device memory at start-up, loops that must not take
+ * cudaMalloc's device-wide synchronisation).  No counterpart in the
+ * reference (PureUMFPACK.jl has no device code).  The residual is never
+ * stored: per right-hand side the maxima go to one fixed device array inside
+ * libmfgpu (98 KB, held on every GPU that loads the library until the
+ * process exits), shared by all calls and all handles of a device.
+ *   - nrhs must be 1..4096; larger counts return MFGPU_ERR_ARGUMENT.
+ *   - The first call on a device looks up that array's device address; make
+ *     that first call before any stream capture.
+ *   - The array keeps the last call's contents; each call clears it first.
+ *     Calls whose GPU work overlaps (other streams, other handles on the same
+ *     device, other host threads) race on it: serialise them.
+ * Requires a factorization (the values of A given to mfgpu_factor*). */
+int mfgpu_backward_error_noalloc(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ldb, const double* d_x,
+                                 int64_t ldx, double* out);
+
 /* JSON object with the last call's phase times, sizes and counters, and the
  * per-kernel-class profile gathered since the last mfgpu_set_profiling. */
 int mfgpu_stats_json(mfgpu_ctx* h, char* buf, int64_t cap);

@@ -15,6 +15,7 @@
 #include <exception>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -1175,3 +1176,108 @@ int mfgpu_set_profiling(mfgpu_ctx* h, int32_t on) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Backward error without device allocation.
+//
+// mfgpu_backward_error_device allocates a residual buffer the first time it
+// sees a size.  Some callers cannot allocate device memory when they check
+// accuracy: services that reserve all device memory when they start (behind a
+// caching allocator or a fixed budget), and latency-sensitive loops that must
+// not take cudaMalloc's device-wide synchronisation.  This variant never
+// stores the residual; per right-hand side it reduces max|b - A x|, max|x|,
+// max|b| and ||A||_inf into one file-scope __device__ array of fixed size,
+// then forms the error on the device and copies one double to the host.
+// ===========================================================================
+namespace {
+
+constexpr int64_t kNoAllocMaxRhs = 4096;          // right-hand sides per call
+constexpr int kNoAllocMaxDevices = 64;
+// [3c]: max|r_c|, [3c+1]: max|x_c|, [3c+2]: max|b_c| (as ordered bits of
+// non-negative doubles), [3*max]: ||A||_inf, [3*max+1]: result.
+// Every GPU that loads the library holds these 98 KB until the process exits.
+__device__ __align__(256) unsigned long long g_noalloc_scratch[3 * kNoAllocMaxRhs + 2];
+
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on `device` (the current device); the
+// symbol's name in host code is only a stand-in, so kernels get this address.
+void* noalloc_scratch(int device) {
+  if (device < 0 || device >= kNoAllocMaxDevices) throw std::invalid_argument("device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_ptr[device] = p;
+  }
+  return g_noalloc_ptr[device];
+}
+
+__global__ void k_noalloc_residual_max(int64_t n, int64_t nrhs, const int32_t* __restrict__ rp,
+                                       const int32_t* __restrict__ ci, const int32_t* __restrict__ src,
+                                       const double* __restrict__ ax, const double* __restrict__ b, int64_t ldb,
+                                       const double* __restrict__ x, int64_t ldx,
+                                       unsigned long long* __restrict__ scratch) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n * nrhs) return;
+  const int64_t i = e % n, c = e / n;
+  double acc = 0.0;
+  for (int p = rp[i]; p < rp[i + 1]; ++p) acc += ax[src[p]] * x[ci[p] + c * ldx];
+  const double bi = b[i + c * ldb];
+  atomicMax(scratch + 3 * c + 0, (unsigned long long)__double_as_longlong(fabs(bi - acc)));
+  atomicMax(scratch + 3 * c + 1, (unsigned long long)__double_as_longlong(fabs(x[i + c * ldx])));
+  atomicMax(scratch + 3 * c + 2, (unsigned long long)__double_as_longlong(fabs(bi)));
+}
+
+__global__ void k_noalloc_finish(int64_t nrhs, unsigned long long* __restrict__ scratch) {
+  __shared__ double red[256];
+  const double anorm = __longlong_as_double((long long)scratch[3 * kNoAllocMaxRhs]);
+  double worst = 0.0;
+  for (int64_t c = threadIdx.x; c < nrhs; c += blockDim.x) {
+    const double r = __longlong_as_double((long long)scratch[3 * c]);
+    const double xn = __longlong_as_double((long long)scratch[3 * c + 1]);
+    const double bn = __longlong_as_double((long long)scratch[3 * c + 2]);
+    const double den = anorm * xn + bn;
+    worst = fmax(worst, den > 0 ? r / den : 0.0);
+  }
+  red[threadIdx.x] = worst;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) scratch[3 * kNoAllocMaxRhs + 1] = (unsigned long long)__double_as_longlong(red[0]);
+}
+
+}  // namespace
+
+extern "C" int mfgpu_backward_error_noalloc(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ldb,
+                                            const double* d_x, int64_t ldx, double* out) {
+  if (!h || !out || !d_b || !d_x) return MFGPU_ERR_ARGUMENT;
+  if (!h->factored) return fail(h, MFGPU_ERR_STATE, "no matrix values (factor first)");
+  if (nrhs < 1 || nrhs > kNoAllocMaxRhs)
+    return fail(h, MFGPU_ERR_ARGUMENT, "mfgpu_backward_error_noalloc: nrhs must be in 1.." +
+                                           std::to_string(kNoAllocMaxRhs));
+  if (ldb < h->plan.n || ldx < h->plan.n) return fail(h, MFGPU_ERR_ARGUMENT, "leading dimension below n");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->device));
+    unsigned long long* scratch = static_cast<unsigned long long*>(noalloc_scratch(h->device));
+    const Plan& P = h->plan;
+    cudaStream_t st = h->stream;
+    const int64_t n = P.n;
+    CK(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long) * (3 * kNoAllocMaxRhs + 2), st));
+    k_noalloc_residual_max<<<grid1(n * nrhs, 256), 256, 0, st>>>(
+        n, nrhs, h->b_csr_ptr.as<int32_t>(), h->b_csr_col.as<int32_t>(), h->b_csr_src.as<int32_t>(),
+        h->b_ax.as<double>(), d_b, ldb, d_x, ldx, scratch);
+    k_norm_inf<<<grid1(n, 256), 256, 0, st>>>(n, h->b_csr_ptr.as<int32_t>(), h->b_csr_src.as<int32_t>(),
+                                              h->b_ax.as<double>(), scratch + 3 * kNoAllocMaxRhs);
+    k_noalloc_finish<<<1, 256, 0, st>>>(nrhs, scratch);
+    CK(cudaGetLastError());
+    unsigned long long bits = 0;
+    CK(cudaMemcpyAsync(&bits, scratch + 3 * kNoAllocMaxRhs + 1, sizeof bits, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::memcpy(out, &bits, sizeof bits);
+    return MFGPU_OK;
+  });
+}

@@ -46,6 +46,7 @@ SIGNATURES = [
     ("mfgpu_solve", ctypes.c_int, [vp, i64, f64p, i64, f64p, i64, i32]),
     ("mfgpu_solve_device", ctypes.c_int, [vp, i64, vp, i64, vp, i64, i32]),
     ("mfgpu_backward_error_device", ctypes.c_int, [vp, i64, vp, i64, vp, i64, f64p]),
+    ("mfgpu_backward_error_noalloc", ctypes.c_int, [vp, i64, vp, i64, vp, i64, f64p]),
     ("mfgpu_stats_json", ctypes.c_int, [vp, ctypes.c_char_p, i64]),
     ("mfgpu_set_profiling", ctypes.c_int, [vp, i32]),
     ("mfgpu_launch_records", ctypes.c_int, [vp, ctypes.c_char_p, i64]),
