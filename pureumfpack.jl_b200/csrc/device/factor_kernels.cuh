@@ -415,6 +415,200 @@ __device__ void block_inverses(const T* D, int ldd, int kb, T* dst, T* sm_xrow2)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Speculative panel: LU without interchanges of the 64 x 64 diagonal block of
+// a panel step, and the inverses of its two triangles, by 8 x 8 blocks.  The
+// block is padded to 64 x 64 with the identity (so L, U and both inverses are
+// block diagonal with identity beyond kb).  Step s of 8: one warp factors the
+// 8 x 8 diagonal block with shuffles and inverts its triangles; then the
+// block column below (L_rs = A_rs inv(U_ss)) and the block row to the right
+// (U_sc = inv(L_ss) A_sc) are formed, and the trailing blocks updated.  The
+// off-diagonal blocks of inv(L) and inv(U) are built by block substitution.
+// Every multiplier is checked against the partial-pivoting order (|l| <= 1);
+// a violation or a zero pivot raises flags[0] and the factorization is redone
+// with pivoting panels.
+// ---------------------------------------------------------------------------
+constexpr int kSpecThreads = 256;
+constexpr int kLdS = 65;   // shared leading dimension of the 64 x 64 blocks
+
+template <typename T>
+__global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState S, const PanelTask* __restrict__ tasks,
+                                                             T* __restrict__ pool, T* __restrict__ dinv) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* A = reinterpret_cast<T*>(smem_raw);     // 64 x 64, ld kLdS: L\U
+  T* Li = A + 64 * kLdS;                     // inv(L)
+  T* Ui = Li + 64 * kLdS;                    // inv(U)
+  T* Tb = Ui + 64 * kLdS;                    // 2 x 7 x 64 scratch of the inverse assembly
+  __shared__ int bad;
+  const PanelTask tk = tasks[blockIdx.x];
+  const int s_ = tk.s, k0 = tk.k0;
+  const int np = P.np[s_], nf = P.nf[s_], c1 = P.c1[s_];
+  const int kb = min(kPanel, np - k0);
+  const int t = threadIdx.x, lane = lane_id(), warp = warp_id();
+  T* F = pool + P.front_off[s_];
+  if (t == 0) bad = 0;
+  for (int e = t; e < 64 * 64; e += kSpecThreads) {
+    const int r = e & 63, c = e >> 6;
+    A[r + c * kLdS] = (r < kb && c < kb) ? F[(k0 + r) + (int64_t)(k0 + c) * nf] : (r == c ? T(1) : T(0));
+    Li[r + c * kLdS] = T(0);
+    Ui[r + c * kLdS] = T(0);
+  }
+  __syncthreads();
+  bool violated = false;
+  for (int sb = 0; sb < 8; ++sb) {
+    const int s8 = sb * 8;
+    if (warp == 0) {   // 8 x 8 diagonal block: lanes 0..7 hold its rows
+      T a[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) a[q] = lane < 8 ? A[(s8 + lane) + (s8 + q) * kLdS] : T(0);
+#pragma unroll
+      for (int jj = 0; jj < 8; ++jj) {
+        T u[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) u[q] = __shfl_sync(0xffffffffu, a[q], jj);
+        const T d = u[jj];
+        if (lane > jj && lane < 8) {
+          if (d == T(0) || absd(a[jj]) > absd(d)) violated = true;
+          const T l = d != T(0) ? a[jj] * (T(1) / d) : a[jj];
+          a[jj] = l;
+#pragma unroll
+          for (int q = jj + 1; q < 8; ++q) a[q] -= l * u[q];
+        }
+        if (lane == 0 && d == T(0)) violated = true;
+      }
+      if (lane < 8) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) A[(s8 + lane) + (s8 + q) * kLdS] = a[q];
+      }
+      __syncwarp();
+      if (lane < 8) {          // column `lane` of inv(L_ss)
+        const int c = lane;
+        T x[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x[i] = (i == c) ? T(1) : T(0);
+#pragma unroll
+        for (int i = 1; i < 8; ++i) {
+          T v = x[i];
+#pragma unroll
+          for (int k = 0; k < i; ++k) v -= A[(s8 + i) + (s8 + k) * kLdS] * x[k];
+          x[i] = (i > c) ? v : x[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) Li[(s8 + i) + (s8 + c) * kLdS] = x[i];
+      } else if (lane < 16) {  // column `lane-8` of inv(U_ss)
+        const int c = lane - 8;
+        T x[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x[i] = T(0);
+#pragma unroll
+        for (int i = 7; i >= 0; --i) {
+          T v = (i == c) ? T(1) : T(0);
+#pragma unroll
+          for (int k = i + 1; k < 8; ++k) v -= A[(s8 + i) + (s8 + k) * kLdS] * x[k];
+          x[i] = (i <= c) ? v / A[(s8 + i) + (s8 + i) * kLdS] : T(0);
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) Ui[(s8 + i) + (s8 + c) * kLdS] = x[i];
+      }
+    }
+    __syncthreads();
+    const int rest = 56 - s8;   // rows / columns after this block
+    if (t < rest) {             // L block column: row s8+8+t times inv(U_ss)
+      const int r = s8 + 8 + t;
+      T a[8], o[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) a[k] = A[r + (s8 + k) * kLdS];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        T v = T(0);
+#pragma unroll
+        for (int k = 0; k <= q; ++k) v += a[k] * Ui[(s8 + k) + (s8 + q) * kLdS];
+        o[q] = v;
+        if (absd(v) > 1.0) violated = true;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) A[r + (s8 + q) * kLdS] = o[q];
+    } else if (t >= 64 && t < 64 + rest) {   // U block row: inv(L_ss) times column s8+8+(t-64)
+      const int c = s8 + 8 + (t - 64);
+      T a[8], o[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) a[k] = A[(s8 + k) + c * kLdS];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        T v = a[i];
+#pragma unroll
+        for (int k = 0; k < i; ++k) v += Li[(s8 + i) + (s8 + k) * kLdS] * a[k];
+        o[i] = v;
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) A[(s8 + i) + c * kLdS] = o[i];
+    }
+    __syncthreads();
+    for (int e = t; e < rest * rest; e += kSpecThreads) {   // trailing update
+      const int r = s8 + 8 + e % rest, c = s8 + 8 + e / rest;
+      T v = A[r + c * kLdS];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v -= A[r + (s8 + k) * kLdS] * A[(s8 + k) + c * kLdS];
+      A[r + c * kLdS] = v;
+    }
+    __syncthreads();
+  }
+  // off-diagonal blocks of the inverses, one block row of each per iteration
+  T* Tl = Tb;
+  T* Tu = Tb + 7 * 64;
+  for (int i = 1; i < 8; ++i) {
+    const int ur = 7 - i;       // block row of inv(U) done this iteration
+    if (t < 128) {              // T_l(i, s) = sum_{s<=k<i} L_ik Li_ks, s < i
+      for (int e = t; e < i * 64; e += 128) {
+        const int sb = e >> 6, a = (e >> 3) & 7, b = e & 7;
+        T v = T(0);
+        for (int k = 8 * sb; k < 8 * i; ++k) v += A[(8 * i + a) + k * kLdS] * Li[k + (8 * sb + b) * kLdS];
+        Tl[e] = v;
+      }
+    } else {                    // T_u(ur, c) = sum_{ur<k<=c} U_{ur,k} Ui_kc, c > ur
+      for (int e = t - 128; e < i * 64; e += 128) {
+        const int cb = ur + 1 + (e >> 6), a = (e >> 3) & 7, b = e & 7;
+        T v = T(0);
+        for (int k = 8 * (ur + 1); k < 8 * (cb + 1); ++k) v += A[(8 * ur + a) + k * kLdS] * Ui[k + (8 * cb + b) * kLdS];
+        Tu[e] = v;
+      }
+    }
+    __syncthreads();
+    if (t < 128) {              // Li(i, s) = -Li_ii T_l(i, s)
+      for (int e = t; e < i * 64; e += 128) {
+        const int sb = e >> 6, a = (e >> 3) & 7, b = e & 7;
+        T v = T(0);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v -= Li[(8 * i + a) + (8 * i + k) * kLdS] * Tl[(sb << 6) + (k << 3) + b];
+        Li[(8 * i + a) + (8 * sb + b) * kLdS] = v;
+      }
+    } else {                    // Ui(ur, c) = -Ui_{ur,ur} T_u(ur, c)
+      for (int e = t - 128; e < i * 64; e += 128) {
+        const int cb = ur + 1 + (e >> 6), a = (e >> 3) & 7, b = e & 7;
+        T v = T(0);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v -= Ui[(8 * ur + a) + (8 * ur + k) * kLdS] * Tu[((e >> 6) << 6) + (k << 3) + b];
+        Ui[(8 * ur + a) + (8 * cb + b) * kLdS] = v;
+      }
+    }
+    __syncthreads();
+  }
+  if (violated) bad = 1;
+  __syncthreads();
+  if (t == 0 && bad) atomicOr(S.flags, 1);
+  for (int e = t; e < kb * kb; e += kSpecThreads) {
+    const int r = e % kb, c = e / kb;
+    F[(k0 + r) + (int64_t)(k0 + c) * nf] = A[r + c * kLdS];
+  }
+  T* dst = dinv + (P.dinv_off[s_] + k0 / kPanel) * (int64_t)kDinvElems;
+  for (int e = t; e < 64 * 64; e += kSpecThreads) {
+    const int r = e & 63, c = e >> 6;
+    dst[e] = Li[r + c * kLdS];
+    dst[4096 + e] = Ui[r + c * kLdS];
+  }
+  for (int j = t; j < kb; j += kSpecThreads) S.ipiv[c1 + k0 + j] = k0 + j;
+}
+
 // Panel factorization of one panel step (k0..k1-1) of one large front.
 //  * kPanelSmemPivot: the R = np-k0 <= 256 candidate rows are held one row
 //    per thread in registers; the pivot of each column is a block-wide

@@ -199,3 +199,116 @@ __global__ void __launch_bounds__(256) k_gemm_f32(const GemmTask* __restrict__ t
 }
 
 }  // namespace mfgpu
+
+namespace mfgpu {
+
+// FP64 batched GEMM, C -= A * B, templated on the CTA tile (BM x BN), the warp
+// tile (WM x WN, multiples of 8) and the cp.async pipeline depth.  Same task
+// format as k_gemm_f64; the tasks' tiles_m / tiles_n must use BM / BN.
+template <int BM, int BN, int WM, int WN, int STAGES>
+struct GemmCfg {
+  static constexpr int kWarps = (BM / WM) * (BN / WN);
+  static constexpr int kThreads = kWarps * 32;
+  static constexpr int BK = 16;
+  static constexpr int kLdA = BM + 8;     // A stage: k-major [BK][BM + 8]
+  static constexpr int kLdB = BK + 4;     // B stage: n-major [BN][BK + 4]
+  static constexpr int kStageA = BK * kLdA;
+  static constexpr int kStageB = BN * kLdB;
+  static constexpr int kLdC = BM + 1;
+  static constexpr size_t kSmemOps = (size_t)STAGES * (kStageA + kStageB);
+  static constexpr size_t kSmemC = (size_t)BN * kLdC;
+  static constexpr size_t kSmem = (kSmemOps > kSmemC ? kSmemOps : kSmemC) * sizeof(double);
+};
+
+template <int BM, int BN, int WM, int WN, int STAGES>
+__global__ void __launch_bounds__(GemmCfg<BM, BN, WM, WN, STAGES>::kThreads)
+    k_gemm_f64_t(const GemmTask* __restrict__ tasks, int ntasks, const double* __restrict__ pa,
+                 const double* __restrict__ pb, double* __restrict__ pc) {
+  using C = GemmCfg<BM, BN, WM, WN, STAGES>;
+  constexpr int BK = C::BK, NT = C::kThreads;
+  constexpr int FM = WM / 8, FN = WN / 8;           // 8x8 fragments per warp
+  extern __shared__ __align__(16) double gsm[];
+  double* As = gsm;
+  double* Bs = gsm + STAGES * C::kStageA;
+
+  const GemmTask tk = tasks[find_task(tasks, ntasks, blockIdx.x)];
+  const int64_t local = blockIdx.x - tk.tile_base;
+  const int m0 = (int)(local % tk.tiles_m) * BM;
+  const int n0 = (int)(local / tk.tiles_m) * BN;
+  const double* A = pa + tk.a;
+  const double* B = pb + tk.b;
+  double* Cg = pc + tk.c;
+  const int M = tk.m, N = tk.n, K = tk.k, lda = tk.lda, ldb = tk.ldb, ldc = tk.ldc;
+  const int tid = threadIdx.x, lane = lane_id(), warp = warp_id();
+  const int wm = (warp % (BM / WM)) * WM, wn = (warp / (BM / WM)) * WN;
+
+  auto load_stage = [&](int stage, int k0) {
+    double* as = As + stage * C::kStageA;
+    double* bs = Bs + stage * C::kStageB;
+#pragma unroll
+    for (int i = 0; i < (BM * BK) / NT; ++i) {
+      const int idx = tid + i * NT;
+      const int m = idx % BM, k = idx / BM;
+      const bool ok = (m0 + m < M) && (k0 + k < K);
+      cp_async8(as + k * C::kLdA + m, ok ? A + (int64_t)(m0 + m) + (int64_t)(k0 + k) * lda : A, ok);
+    }
+#pragma unroll
+    for (int i = 0; i < (BN * BK) / NT; ++i) {
+      const int idx = tid + i * NT;
+      const int k = idx % BK, n = idx / BK;
+      const bool ok = (n0 + n < N) && (k0 + k < K);
+      cp_async8(bs + n * C::kLdB + k, ok ? B + (int64_t)(k0 + k) + (int64_t)(n0 + n) * ldb : B, ok);
+    }
+  };
+
+  double acc[FM][FN][2];
+#pragma unroll
+  for (int i = 0; i < FM; ++i)
+#pragma unroll
+    for (int j = 0; j < FN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  const int ktiles = (K + BK - 1) / BK;
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < ktiles) load_stage(s, s * BK);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < ktiles; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    const int pre = kt + STAGES - 1;
+    if (pre < ktiles) load_stage(pre % STAGES, pre * BK);
+    cp_async_commit();
+    const double* as = As + (kt % STAGES) * C::kStageA;
+    const double* bs = Bs + (kt % STAGES) * C::kStageB;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      double af[FM], bf[FN];
+#pragma unroll
+      for (int i = 0; i < FM; ++i) af[i] = as[(kk + (lane & 3)) * C::kLdA + wm + i * 8 + (lane >> 2)];
+#pragma unroll
+      for (int j = 0; j < FN; ++j) bf[j] = bs[(wn + j * 8 + (lane >> 2)) * C::kLdB + kk + (lane & 3)];
+#pragma unroll
+      for (int i = 0; i < FM; ++i)
+#pragma unroll
+        for (int j = 0; j < FN; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  double* Cs = gsm;
+#pragma unroll
+  for (int i = 0; i < FM; ++i)
+#pragma unroll
+    for (int j = 0; j < FN; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e)
+        Cs[(wn + j * 8 + 2 * (lane & 3) + e) * C::kLdC + wm + i * 8 + (lane >> 2)] = acc[i][j][e];
+  __syncthreads();
+  for (int idx = tid; idx < BM * BN; idx += NT) {
+    const int m = idx % BM, n = idx / BM;
+    if (m0 + m < M && n0 + n < N) Cg[(int64_t)(m0 + m) + (int64_t)(n0 + n) * ldc] -= Cs[n * C::kLdC + m];
+  }
+}
+
+}  // namespace mfgpu

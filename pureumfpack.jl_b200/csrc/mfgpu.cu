@@ -321,6 +321,11 @@ size_t panel_smem_bytes(int rows) {
 }
 
 template <typename T>
+size_t spec_smem_bytes() {
+  return ((size_t)3 * 64 * kLdS + 2 * 7 * 64) * sizeof(T);
+}
+
+template <typename T>
 size_t apply_smem_bytes() {
   return (size_t)64 * (kLdP + kLdQ) * sizeof(T);
 }
@@ -329,6 +334,7 @@ template <typename T>
 void configure_kernels() {
   static bool done = false;
   if (done) return;
+  CK(cudaFuncSetAttribute(k_panel_spec<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)spec_smem_bytes<T>()));
   CK(cudaFuncSetAttribute(k_panel<T, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_smem_bytes<T>(64)));
   CK(cudaFuncSetAttribute(k_panel<T, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_smem_bytes<T>(128)));
   CK(cudaFuncSetAttribute(k_panel<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_smem_bytes<T>(256)));
@@ -382,7 +388,9 @@ void run_factor_launches(mfgpu_ctx* h) {
         klaunch(h, KC_PANEL, L.flops, bytes, [&] {
           const PanelTask* pt = h->b_panel.as<PanelTask>() + L.first;
           T* dinv = h->b_dinv.as<T>();
-          if (L.rows <= 64)
+          if (L.rows == 0)
+            k_panel_spec<T><<<(unsigned)L.count, kSpecThreads, spec_smem_bytes<T>(), st>>>(h->dp, S, pt, pool, dinv);
+          else if (L.rows <= 64)
             k_panel<T, 64><<<(unsigned)L.count, 64, panel_smem_bytes<T>(64), st>>>(h->dp, S, pt, pool, dinv);
           else if (L.rows <= 128)
             k_panel<T, 128><<<(unsigned)L.count, 128, panel_smem_bytes<T>(128), st>>>(h->dp, S, pt, pool, dinv);

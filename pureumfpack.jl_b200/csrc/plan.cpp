@@ -343,15 +343,17 @@ void build_launches(Plan& P, bool safe) {
       Launch lt{kLaunchTrsm, L, (int64_t)P.trsm_tasks.size(), 0, 0};
       Launch lg{kLaunchGemm, L, (int64_t)P.gemm_tasks.size(), 0, 0};
       // panel tasks of this step, one launch per row class (64 / 128 / 256)
-      std::vector<PanelTask> cls[3];
+      std::vector<PanelTask> cls[4];   // pivoting panels by row class, then speculative
       for (int32_t s : large) {
         const int32_t npv = P.np[s], nf = P.nf[s];
         if (npv <= k0) continue;
         const int32_t kb = std::min(kPanel, npv - k0), k1 = k0 + kb;
-        int32_t mode = (npv - k0 <= kPivRowsSmem) ? kPanelSmemPivot : (safe ? kPanelGlobalPivot : kPanelSpeculative);
+        // Speculative panels everywhere; the pivoting variants only run in
+        // the safe rerun after a speculative panel met a larger candidate.
+        int32_t mode = !safe ? kPanelSpeculative : (npv - k0 <= kPivRowsSmem ? kPanelSmemPivot : kPanelGlobalPivot);
         if (mode == kPanelSpeculative) P.has_speculative = true;
         const int32_t R = (mode == kPanelSpeculative) ? kb : npv - k0;
-        const int c = (mode == kPanelGlobalPivot || R > 128) ? 2 : (R > 64 ? 1 : 0);
+        const int c = mode == kPanelSpeculative ? 3 : ((mode == kPanelGlobalPivot || R > 128) ? 2 : (R > 64 ? 1 : 0));
         cls[c].push_back(PanelTask{s, k0, mode, 0});
         TrsmTask tt{};
         tt.s = s;
@@ -391,10 +393,10 @@ void build_launches(Plan& P, bool safe) {
                    npv - k1, nf - npv, kb);
         }
       }
-      for (int c = 0; c < 3; ++c) {
+      for (int c = 0; c < 4; ++c) {
         if (cls[c].empty()) continue;
         Launch lp{kLaunchPanel, L, (int64_t)P.panel_tasks.size(), (int64_t)cls[c].size(), (int64_t)cls[c].size()};
-        lp.rows = 64 << c;
+        lp.rows = c < 3 ? 64 << c : 0;   // 0: speculative kernel
         for (const PanelTask& pt : cls[c]) {
           const int32_t kb = std::min(kPanel, P.np[pt.s] - pt.k0);
           const double R = (pt.mode == kPanelSpeculative) ? kb : (P.np[pt.s] - pt.k0);
