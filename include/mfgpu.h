@@ -92,10 +92,15 @@ const char* mfgpu_host_last_error(void);
 
 typedef struct mfgpu_ctx mfgpu_ctx;
 
+/* mfgpu_options.flags */
+enum {
+  MFGPU_FLAG_NO_TENSOR_CORES = 1   /* FP32 fronts: SIMT FP32 Schur updates instead of tcgen05 3xTF32 */
+};
+
 typedef struct {
   int32_t device;     /* CUDA device ordinal */
   int32_t precision;  /* MFGPU_PRECISION_* */
-  int32_t flags;      /* reserved, 0 */
+  int32_t flags;      /* MFGPU_FLAG_* bits, 0 = defaults */
   int32_t reserved;
 } mfgpu_options;
 
@@ -166,6 +171,44 @@ int mfgpu_backward_error_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, i
  * Requires a factorization (the values of A given to mfgpu_factor*). */
 int mfgpu_backward_error_noalloc(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ldb, const double* d_x,
                                  int64_t ldx, double* out);
+
+/* ------------------------------------------------------------------------
+ * Batched systems: many independent square systems of uneven size through
+ * one handle, one factor launch sequence and one solve launch sequence.  No
+ * single counterpart in the reference: each system's result is that of
+ * splu(A_i; method=:multifrontal, scale) (src/interface.jl:93-120) or, with
+ * MFGPU_ORDER_COLAMD, of multifrontal_lu(Rs_i .* A_i; q=colamd_order(A_i))
+ * (src/multifrontal.jl:152), and solve(F_i, b_i; refine)
+ * (src/interface.jl:170-177) for every system.
+ * ---------------------------------------------------------------------- */
+enum { MFGPU_ORDER_AMD = 0, MFGPU_ORDER_COLAMD = 1 };
+
+/* Analyze nsys systems; system i is n[i] x n[i] with pattern colptr[i] /
+ * rowval[i].  Each system is ordered by itself, and the batch is analyzed as
+ * one block-diagonal matrix whose elimination forest holds every system's
+ * own tree: the fronts of all systems at one tree level share a launch.
+ * Replaces any previous analysis of the handle. */
+int mfgpu_batch_analyze(mfgpu_ctx* h, int64_t nsys, const int64_t* n, const int64_t* const* colptr,
+                        const int64_t* const* rowval, int32_t ordering);
+/* nsys, and the column (nsys+1) and value (nsys+1) offsets of every system
+ * in the concatenated arrays that mfgpu_factor_device / mfgpu_solve_device
+ * take for a batch (values of system i at nz_off[i].., its rows at
+ * col_off[i].. of every right-hand-side column).  Any pointer may be NULL. */
+int mfgpu_batch_layout(mfgpu_ctx* h, int64_t* nsys, int64_t* col_off, int64_t* nz_off);
+/* Factor every system with its values nzval[i] and its own row scaling of
+ * kind `scale`.  status[i] (nsys entries, may be NULL) receives 0 or the
+ * system's first singular factor column (1-based, as SingularException).
+ * Returns the number of singular systems when check != 0, else 0; or an error. */
+int mfgpu_batch_factor(mfgpu_ctx* h, const double* const* nzval, int32_t scale, int32_t check, int64_t* status);
+/* Solve every system for nrhs right-hand sides b[i] (n[i] x nrhs,
+ * column-major) into x[i], with `refine` refinement steps. */
+int mfgpu_batch_solve(mfgpu_ctx* h, int64_t nrhs, const double* const* b, double* const* x, int32_t refine);
+/* out3 = {n[i], nnz(L_i), nnz(U_i)} of system i (0-based index). */
+int mfgpu_batch_factor_sizes(mfgpu_ctx* h, int64_t sys, int64_t* out3);
+/* System i's own factors, as mfgpu_get_factors gives them for one system. */
+int mfgpu_batch_get_factors(mfgpu_ctx* h, int64_t sys, int64_t* lcolptr, int64_t* lrowval, double* lnzval,
+                            int64_t* ucolptr, int64_t* urowval, double* unzval, int64_t* p, int64_t* q,
+                            int64_t* pinv);
 
 /* JSON object with the last call's phase times, sizes and counters, and the
  * per-kernel-class profile gathered since the last mfgpu_set_profiling. */

@@ -28,6 +28,7 @@ DEPENDS = SOURCES + [
     "csrc/device/factor_kernels.cuh",
     "csrc/device/gemm_kernels.cuh",
     "csrc/device/solve_kernels.cuh",
+    "csrc/device/tc_gemm.cuh",
     "../include/mfgpu.h",
 ]
 NVCC_FLAGS = [

@@ -263,16 +263,36 @@ __global__ void k_residual(int64_t n, int64_t nrhs, const int32_t* __restrict__ 
   r[i + c * ldr] = b[i + c * ldb] - acc;
 }
 
-// Per-column maxima of |r|, |x|, |b| for the normwise backward error.
-__global__ void k_bwd_error_parts(int64_t n, int64_t nrhs, const double* __restrict__ r, int64_t ldr,
-                                  const double* __restrict__ x, int64_t ldx, const double* __restrict__ b, int64_t ldb,
-                                  unsigned long long* __restrict__ out) {
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n * nrhs) return;
-  const int64_t i = e % n, c = e / n;
-  atomicMax(out + 3 * c + 0, (unsigned long long)__double_as_longlong(fabs(r[i + c * ldr])));
-  atomicMax(out + 3 * c + 1, (unsigned long long)__double_as_longlong(fabs(x[i + c * ldx])));
-  atomicMax(out + 3 * c + 2, (unsigned long long)__double_as_longlong(fabs(b[i + c * ldb])));
+// Per-column maxima of |r|, |x|, |b| for the normwise backward error: a
+// 256-row slice of one column per CTA (grid: row slices x columns), reduced
+// in the CTA, then one atomic per quantity and CTA.  Non-negative doubles
+// order like their bit patterns, so the maxima are atomicMax on the bits.
+__global__ void __launch_bounds__(256) k_bwd_error_parts(int64_t n, int64_t nrhs, const double* __restrict__ r,
+                                                         int64_t ldr, const double* __restrict__ x, int64_t ldx,
+                                                         const double* __restrict__ b, int64_t ldb,
+                                                         unsigned long long* __restrict__ out) {
+  __shared__ double red[3][8];
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t c = blockIdx.y; c < nrhs; c += gridDim.y) {
+    double v[3] = {0.0, 0.0, 0.0};
+    if (i < n) {
+      v[0] = fabs(r[i + c * ldr]);
+      v[1] = fabs(x[i + c * ldx]);
+      v[2] = fabs(b[i + c * ldb]);
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+      for (int o = 16; o > 0; o >>= 1) v[q] = fmax(v[q], __shfl_xor_sync(0xffffffffu, v[q], o));
+    if (lane_id() == 0)
+      for (int q = 0; q < 3; ++q) red[q][warp_id()] = v[q];
+    __syncthreads();
+    if (threadIdx.x < 3) {
+      double m = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[threadIdx.x][w]);
+      atomicMax(out + 3 * c + threadIdx.x, (unsigned long long)__double_as_longlong(m));
+    }
+    __syncthreads();
+  }
 }
 
 // ||A||_inf = max row sum of |a_ij|.

@@ -23,6 +23,7 @@
 #include "../../include/mfgpu.h"
 #include "device/factor_kernels.cuh"
 #include "device/gemm_kernels.cuh"
+#include "device/tc_gemm.cuh"
 #include "device/solve_kernels.cuh"
 #include "host/symbolic.h"
 #include "plan.h"
@@ -128,7 +129,8 @@ struct mfgpu_ctx {
   DevBuf b_c1, b_np, b_nu, b_nf, b_upd_off, b_front_off, b_colbase, b_child_ptr, b_child_idx, b_upd, b_rel, b_uoff,
       b_v_src, b_v_srow, b_v_frow, b_fc_super, b_fc_vbeg, b_fc_vend, b_fc_ch_ptr, b_fc_ch, b_lcolptr, b_ucolptr, b_qf,
       b_csr_ptr, b_csr_col, b_csr_src;
-  DevBuf b_small, b_panel, b_trsm, b_gemm;
+  DevBuf b_small, b_panel, b_trsm, b_gemm, b_gemm_tc;
+  bool use_tc = true;   // FP32 fronts: Schur updates on tensor cores (3xTF32)
   bool launches_safe = false;
   // numeric state
   DevBuf b_pool, b_vx, b_ax, b_rs, b_ipiv, b_info, b_prow, b_rowfac, b_flags, b_dinv, b_dinv_off;
@@ -142,6 +144,18 @@ struct mfgpu_ctx {
   double t_analyze_ms = 0, t_factor_ms = 0, t_solve_ms = 0, t_csc_ms = 0;
   int factor_reruns = 0;
   int32_t last_status = 0;
+  std::vector<int32_t> last_info;   // per supernode: first zero pivot (block position) or INT32_MAX
+  // batched systems analyzed as one block-diagonal matrix
+  struct Batch {
+    int64_t nsys = 0;
+    std::vector<int64_t> off, nz_off;      // column and value offsets of every system (nsys + 1)
+    std::vector<int64_t> colptr, rowval;   // the block-diagonal pattern, 1-based
+    std::vector<int32_t> super_sys;        // system of every supernode
+    std::vector<double> nz, rs, b, x;      // host staging of the concatenated arrays
+    bool have_factors = false;             // global factors fetched for per-system slicing
+    std::vector<int64_t> lcolptr, lrowval, ucolptr, urowval, p, q;
+    std::vector<double> lnzval, unzval;
+  } batch;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // per-kernel-class profile (CUDA events around each launch when enabled)
   bool profiling = false;
@@ -262,6 +276,7 @@ void upload_launches(mfgpu_ctx* h) {
   upload(h->b_panel, P.panel_tasks, h->stream);
   upload(h->b_trsm, P.trsm_tasks, h->stream);
   upload(h->b_gemm, P.gemm_tasks, h->stream);
+  upload(h->b_gemm_tc, P.gemm_tasks_tc, h->stream);
 }
 
 DevState dev_state(mfgpu_ctx* h) {
@@ -341,6 +356,8 @@ void configure_kernels() {
   CK(cudaFuncSetAttribute(k_panel_apply<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem_bytes<T>()));
   CK(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem_bytes<T>()));
   CK(cudaFuncSetAttribute(k_bwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem_bytes<T>()));
+  CK(cudaFuncSetAttribute(k_gemm_tc<128, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)TcCfg<128, 3>::kSmem));
   done = true;
 }
 
@@ -405,9 +422,16 @@ void run_factor_launches(mfgpu_ctx* h) {
         }, L.level, L.tiles);
         break;
       case kLaunchGemm:
-        klaunch(h, KC_GEMM_FACTOR, L.flops, bytes, [&] {
-          launch_gemm<T>(h->b_gemm.as<GemmTask>() + L.first, L.count, L.tiles, pool, pool, pool, st);
-        }, L.level, L.tiles);
+        if (sizeof(T) == 4 && h->use_tc)
+          klaunch(h, KC_GEMM_FACTOR, L.flops, bytes, [&] {
+            k_gemm_tc<128, 3><<<(unsigned)L.tiles_tc, kTcThreads, TcCfg<128, 3>::kSmem, st>>>(
+                h->b_gemm_tc.as<GemmTask>() + L.first, (int)L.count, (const float*)pool, (const float*)pool,
+                (float*)pool, h->b_flags.as<int>());
+          }, L.level, L.tiles_tc);
+        else
+          klaunch(h, KC_GEMM_FACTOR, L.flops, bytes, [&] {
+            launch_gemm<T>(h->b_gemm.as<GemmTask>() + L.first, L.count, L.tiles, pool, pool, pool, st);
+          }, L.level, L.tiles);
         break;
     }
   }
@@ -501,6 +525,7 @@ int factor_impl(mfgpu_ctx* h, int32_t check) {
         (uintptr_t)h->b_ax.p, (uintptr_t)h->b_rs.p, (uintptr_t)h->b_dinv.p, (uintptr_t)h->b_li.p,
         (uintptr_t)h->b_lx.p, (uintptr_t)h->b_ui.p, (uintptr_t)h->b_ux.p, (uintptr_t)h->b_small.p,
         (uintptr_t)h->b_panel.p, (uintptr_t)h->b_trsm.p, (uintptr_t)h->b_gemm.p, (uintptr_t)h->b_ipiv.p,
+        (uintptr_t)h->b_gemm_tc.p, (uintptr_t)h->use_tc,
         (uintptr_t)h->b_info.p, (uintptr_t)h->b_flags.p, (uintptr_t)st};
     run_sequence(h, h->factor_key, h->factor_exec, h->factor_nodes, key, [&] { issue_factor<T>(h); });
     if (!P.has_speculative) break;
@@ -519,8 +544,15 @@ int factor_impl(mfgpu_ctx* h, int32_t check) {
   CK(cudaEventRecord(h->ev1, st));
   // status: first supernode (postorder) with a zero pivot
   std::vector<int32_t> info(P.ns);
+  int32_t flags[2] = {0, 0};
   if (P.ns) CK(cudaMemcpyAsync(info.data(), h->b_info.p, P.ns * 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(flags, h->b_flags.p, 8, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  if (flags[1]) {
+    prof_flush(h);
+    h->factored = false;
+    return fail(h, MFGPU_ERR_TIMEOUT, "a tensor-core GEMM gave up a bounded wait; the factorization is incomplete");
+  }
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
   h->t_factor_ms = ms;
@@ -536,6 +568,8 @@ int factor_impl(mfgpu_ctx* h, int32_t check) {
         break;
       }
   h->last_status = status;
+  h->last_info = std::move(info);
+  h->batch.have_factors = false;
   return status;
 }
 
@@ -856,6 +890,7 @@ int mfgpu_create(const mfgpu_options* opts, mfgpu_ctx** out) {
   if (opts) {
     h->device = opts->device;
     h->precision = opts->precision;
+    h->use_tc = !(opts->flags & MFGPU_FLAG_NO_TENSOR_CORES);
   }
   int rc = guarded(h, [&]() -> int {
     int ndev = 0;
@@ -889,7 +924,7 @@ void mfgpu_destroy(mfgpu_ctx* h) {
                     &h->b_child_ptr, &h->b_child_idx, &h->b_upd, &h->b_rel, &h->b_uoff, &h->b_v_src, &h->b_v_srow,
                     &h->b_v_frow, &h->b_fc_super, &h->b_fc_vbeg, &h->b_fc_vend, &h->b_fc_ch_ptr, &h->b_fc_ch,
                     &h->b_lcolptr, &h->b_ucolptr, &h->b_qf, &h->b_csr_ptr, &h->b_csr_col, &h->b_csr_src,
-                    &h->b_small, &h->b_panel, &h->b_trsm, &h->b_gemm, &h->b_pool, &h->b_vx, &h->b_ax, &h->b_rs,
+                    &h->b_small, &h->b_panel, &h->b_trsm, &h->b_gemm, &h->b_gemm_tc, &h->b_pool, &h->b_vx, &h->b_ax, &h->b_rs,
                     &h->b_ipiv, &h->b_info, &h->b_prow, &h->b_rowfac, &h->b_flags, &h->b_dinv, &h->b_dinv_off,
                     &h->b_li, &h->b_lx, &h->b_ui,
                     &h->b_ux, &h->b_fsol, &h->b_xw, &h->b_b, &h->b_x, &h->b_r, &h->b_d, &h->b_err, &h->b_norm,
@@ -1077,6 +1112,10 @@ int mfgpu_backward_error_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, i
                                 int64_t ldx, double* out) {
   if (!h || !out) return MFGPU_ERR_ARGUMENT;
   if (!h->factored) return fail(h, MFGPU_ERR_STATE, "no matrix values");
+  if (nrhs < 1 || h->plan.n == 0) {
+    *out = 0.0;
+    return MFGPU_OK;
+  }
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->device));
     const Plan& P = h->plan;
@@ -1090,8 +1129,8 @@ int mfgpu_backward_error_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, i
     k_residual<<<grid1(n * nrhs, 256), 256, 0, st>>>(n, nrhs, h->b_csr_ptr.as<int32_t>(), h->b_csr_col.as<int32_t>(),
                                                      h->b_csr_src.as<int32_t>(), h->b_ax.as<double>(), d_b, ldb, d_x,
                                                      ldx, h->b_r.as<double>(), n);
-    k_bwd_error_parts<<<grid1(n * nrhs, 256), 256, 0, st>>>(n, nrhs, h->b_r.as<double>(), n, d_x, ldx, d_b, ldb,
-                                                            h->b_err.as<unsigned long long>());
+    k_bwd_error_parts<<<dim3((unsigned)((n + 255) / 256), (unsigned)std::min<int64_t>(nrhs, 65535)), 256, 0, st>>>(
+        n, nrhs, h->b_r.as<double>(), n, d_x, ldx, d_b, ldb, h->b_err.as<unsigned long long>());
     k_norm_inf<<<grid1(n, 256), 256, 0, st>>>(n, h->b_csr_ptr.as<int32_t>(), h->b_csr_src.as<int32_t>(),
                                               h->b_ax.as<double>(), h->b_norm.as<unsigned long long>());
     CK(cudaGetLastError());
@@ -1286,6 +1325,224 @@ extern "C" int mfgpu_backward_error_noalloc(mfgpu_ctx* h, int64_t nrhs, const do
     CK(cudaMemcpyAsync(&bits, scratch + 3 * kNoAllocMaxRhs + 1, sizeof bits, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     std::memcpy(out, &bits, sizeof bits);
+    return MFGPU_OK;
+  });
+}
+
+// ---- batched systems ------------------------------------------------------
+// Many independent systems go through one handle as one block-diagonal
+// matrix: each system is ordered by itself and the symbolic pass of the
+// block-diagonal pattern under the concatenated orders is a forest holding
+// every system's own elimination tree, supernodes and update sets (column
+// offsets aside).  Each level-batched launch then factors the fronts of all
+// systems at that tree level together, and the per-level sequence is
+// replayed from one CUDA graph.  Every system's factors are exactly those of
+// splu(A_i; method=:multifrontal) (src/interface.jl:93-120) or of
+// multifrontal_lu(A_i; q=colamd_order(A_i)) (src/multifrontal.jl:152).
+namespace {
+
+int batch_fetch_factors(mfgpu_ctx* h) {
+  auto& B = h->batch;
+  if (B.have_factors) return MFGPU_OK;
+  const Plan& P = h->plan;
+  B.lcolptr.resize(P.n + 1);
+  B.ucolptr.resize(P.n + 1);
+  B.lrowval.resize(P.nnz_l);
+  B.lnzval.resize(P.nnz_l);
+  B.urowval.resize(P.nnz_u);
+  B.unzval.resize(P.nnz_u);
+  B.p.resize(P.n);
+  B.q.resize(P.n);
+  const int rc = mfgpu_get_factors(h, B.lcolptr.data(), B.lrowval.data(), B.lnzval.data(), B.ucolptr.data(),
+                                   B.urowval.data(), B.unzval.data(), B.p.data(), B.q.data(), nullptr);
+  if (rc == MFGPU_OK) B.have_factors = true;
+  return rc;
+}
+
+}  // namespace
+
+extern "C" int mfgpu_batch_analyze(mfgpu_ctx* h, int64_t nsys, const int64_t* n, const int64_t* const* colptr,
+                                   const int64_t* const* rowval, int32_t ordering) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  if (nsys < 1 || !n || !colptr || !rowval) return fail(h, MFGPU_ERR_ARGUMENT, "batch: no systems");
+  if (ordering != MFGPU_ORDER_AMD && ordering != MFGPU_ORDER_COLAMD)
+    return fail(h, MFGPU_ERR_ARGUMENT, "batch: ordering must be MFGPU_ORDER_AMD or MFGPU_ORDER_COLAMD");
+  return guarded(h, [&]() -> int {
+    auto& B = h->batch;
+    B = mfgpu_ctx::Batch{};
+    B.off.assign(nsys + 1, 0);
+    B.nz_off.assign(nsys + 1, 0);
+    for (int64_t i = 0; i < nsys; ++i) {
+      if (n[i] < 1 || !valid_csc(n[i], colptr[i], rowval[i]))
+        return fail(h, MFGPU_ERR_ARGUMENT, "batch: system " + std::to_string(i + 1) + " is not a valid square CSC");
+      B.off[i + 1] = B.off[i] + n[i];
+      B.nz_off[i + 1] = B.nz_off[i] + colptr[i][n[i]] - 1;
+    }
+    const int64_t N = B.off[nsys];
+    B.colptr.resize(N + 1);
+    B.rowval.resize(B.nz_off[nsys]);
+    std::vector<int64_t> q(N);
+    B.colptr[0] = 1;
+    for (int64_t i = 0; i < nsys; ++i) {
+      const int64_t o = B.off[i], z = B.nz_off[i], ni = n[i];
+      for (int64_t j = 1; j <= ni; ++j) B.colptr[o + j] = z + colptr[i][j];
+      for (int64_t k = 0; k < colptr[i][ni] - 1; ++k) B.rowval[z + k] = rowval[i][k] + o;
+      const int rc = ordering == MFGPU_ORDER_AMD ? mfgpu_amd_order(ni, colptr[i], rowval[i], 10.0, q.data() + o)
+                                                 : mfgpu_colamd_order(ni, ni, colptr[i], rowval[i], 10.0, q.data() + o);
+      if (rc != MFGPU_OK) return fail(h, rc, "batch: ordering of system " + std::to_string(i + 1) + " failed");
+      for (int64_t k = 0; k < ni; ++k) q[o + k] += o;
+    }
+    mfgpu_symbolic* sym = nullptr;
+    int rc = mfgpu_symbolic_create(N, B.colptr.data(), B.rowval.data(), q.data(), &sym);
+    if (rc != MFGPU_OK) return fail(h, rc, "batch: symbolic analysis failed");
+    std::unique_ptr<mfgpu_symbolic, void (*)(mfgpu_symbolic*)> guard(sym, mfgpu_symbolic_destroy);
+    // the forest keeps every system's columns together and in system order
+    const auto& S = sym->s;
+    const int64_t ns = S.nsuper();
+    B.super_sys.resize(ns);
+    int64_t sys = 0;
+    for (int64_t s = 0; s < ns; ++s) {
+      while (S.sstart[s] >= B.off[sys + 1]) ++sys;
+      if (S.sstart[s + 1] > B.off[sys + 1]) return fail(h, MFGPU_ERR_INTERNAL, "batch: supernode spans two systems");
+      B.super_sys[s] = (int32_t)sys;
+    }
+    for (int64_t i = 0; i < nsys; ++i)
+      for (int64_t k = B.off[i]; k < B.off[i + 1]; ++k)
+        if (S.qf[k] < B.off[i] || S.qf[k] >= B.off[i + 1])
+          return fail(h, MFGPU_ERR_INTERNAL, "batch: postorder mixes systems");
+    rc = mfgpu_analyze_symbolic(h, N, B.colptr.data(), B.rowval.data(), sym);
+    if (rc != MFGPU_OK) {
+      h->batch.nsys = 0;
+      return rc;
+    }
+    B.nsys = nsys;
+    return MFGPU_OK;
+  });
+}
+
+extern "C" int mfgpu_batch_layout(mfgpu_ctx* h, int64_t* nsys, int64_t* col_off, int64_t* nz_off) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  const auto& B = h->batch;
+  if (!B.nsys) return fail(h, MFGPU_ERR_STATE, "no batch analyzed");
+  if (nsys) *nsys = B.nsys;
+  for (int64_t i = 0; i <= B.nsys; ++i) {
+    if (col_off) col_off[i] = B.off[i];
+    if (nz_off) nz_off[i] = B.nz_off[i];
+  }
+  return MFGPU_OK;
+}
+
+extern "C" int mfgpu_batch_factor(mfgpu_ctx* h, const double* const* nzval, int32_t scale, int32_t check,
+                                  int64_t* status) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  auto& B = h->batch;
+  if (!B.nsys) return fail(h, MFGPU_ERR_STATE, "batch factor before batch analyze");
+  if (!nzval || scale < MFGPU_SCALE_NONE || scale > MFGPU_SCALE_MAX)
+    return fail(h, MFGPU_ERR_ARGUMENT, "batch: bad values or scale kind");
+  return guarded(h, [&]() -> int {
+    const int64_t N = B.off[B.nsys];
+    B.nz.resize(std::max<int64_t>(B.nz_off[B.nsys], 1));
+    for (int64_t i = 0; i < B.nsys; ++i) {
+      const int64_t cnt = B.nz_off[i + 1] - B.nz_off[i];
+      if (cnt && !nzval[i]) return fail(h, MFGPU_ERR_ARGUMENT, "batch: null values for system " + std::to_string(i + 1));
+      if (cnt) std::memcpy(B.nz.data() + B.nz_off[i], nzval[i], cnt * sizeof(double));
+    }
+    const double* rs = nullptr;
+    if (scale != MFGPU_SCALE_NONE) {
+      B.rs.resize(N);
+      const int rc = mfgpu_row_scaling(N, B.colptr.data(), B.rowval.data(), B.nz.data(), scale, B.rs.data());
+      if (rc != MFGPU_OK) return fail(h, rc, "batch: row scaling failed");
+      rs = B.rs.data();
+    }
+    const int rc = mfgpu_factor(h, B.nz.data(), rs, 0);
+    if (rc < 0) return rc;
+    // per system: the first supernode (postorder) with a zero pivot
+    std::vector<int64_t> st(B.nsys, 0);
+    int64_t singular = 0;
+    const Plan& P = h->plan;
+    for (int64_t s = 0; s < (int64_t)h->last_info.size(); ++s) {
+      if (h->last_info[s] == INT32_MAX) continue;
+      const int32_t sys = B.super_sys[s];
+      if (st[sys] == 0) {
+        st[sys] = (int64_t)P.c1[s] + h->last_info[s] + 1 - B.off[sys];
+        ++singular;
+      }
+    }
+    if (status) std::copy(st.begin(), st.end(), status);
+    return check ? (int)singular : MFGPU_OK;
+  });
+}
+
+extern "C" int mfgpu_batch_solve(mfgpu_ctx* h, int64_t nrhs, const double* const* b, double* const* x,
+                                 int32_t refine) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  auto& B = h->batch;
+  if (!B.nsys) return fail(h, MFGPU_ERR_STATE, "batch solve before batch analyze");
+  if (nrhs < 0 || refine < 0 || (nrhs && (!b || !x))) return fail(h, MFGPU_ERR_ARGUMENT, "batch: bad solve sizes");
+  if (nrhs == 0) return MFGPU_OK;
+  return guarded(h, [&]() -> int {
+    const int64_t N = B.off[B.nsys];
+    B.b.resize(N * nrhs);
+    B.x.resize(N * nrhs);
+    for (int64_t i = 0; i < B.nsys; ++i) {
+      const int64_t o = B.off[i], ni = B.off[i + 1] - o;
+      if (!b[i] || !x[i]) return fail(h, MFGPU_ERR_ARGUMENT, "batch: null rhs or solution for system " + std::to_string(i + 1));
+      for (int64_t k = 0; k < nrhs; ++k) std::memcpy(B.b.data() + k * N + o, b[i] + k * ni, ni * sizeof(double));
+    }
+    const int rc = mfgpu_solve(h, nrhs, B.b.data(), N, B.x.data(), N, refine);
+    if (rc != MFGPU_OK) return rc;
+    for (int64_t i = 0; i < B.nsys; ++i) {
+      const int64_t o = B.off[i], ni = B.off[i + 1] - o;
+      for (int64_t k = 0; k < nrhs; ++k) std::memcpy(x[i] + k * ni, B.x.data() + k * N + o, ni * sizeof(double));
+    }
+    return MFGPU_OK;
+  });
+}
+
+extern "C" int mfgpu_batch_factor_sizes(mfgpu_ctx* h, int64_t sys, int64_t* out3) {
+  if (!h || !out3) return MFGPU_ERR_ARGUMENT;
+  auto& B = h->batch;
+  if (!B.nsys || !h->factored) return fail(h, MFGPU_ERR_STATE, "no batch factorization");
+  if (sys < 0 || sys >= B.nsys) return fail(h, MFGPU_ERR_ARGUMENT, "batch: system index out of range");
+  const Plan& P = h->plan;
+  const int64_t a = B.off[sys], e = B.off[sys + 1];
+  out3[0] = e - a;
+  out3[1] = (int64_t)P.lcolptr[e] - P.lcolptr[a];
+  out3[2] = (int64_t)P.ucolptr[e] - P.ucolptr[a];
+  return MFGPU_OK;
+}
+
+extern "C" int mfgpu_batch_get_factors(mfgpu_ctx* h, int64_t sys, int64_t* lcolptr, int64_t* lrowval,
+                                       double* lnzval, int64_t* ucolptr, int64_t* urowval, double* unzval,
+                                       int64_t* p, int64_t* q, int64_t* pinv) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  auto& B = h->batch;
+  if (!B.nsys || !h->factored) return fail(h, MFGPU_ERR_STATE, "no batch factorization");
+  if (sys < 0 || sys >= B.nsys) return fail(h, MFGPU_ERR_ARGUMENT, "batch: system index out of range");
+  return guarded(h, [&]() -> int {
+    const int rc = batch_fetch_factors(h);
+    if (rc != MFGPU_OK) return rc;
+    const int64_t a = B.off[sys], ni = B.off[sys + 1] - a;
+    const int64_t l0 = B.lcolptr[a] - 1, u0 = B.ucolptr[a] - 1;
+    for (int64_t j = 0; j <= ni; ++j) {
+      if (lcolptr) lcolptr[j] = B.lcolptr[a + j] - l0;
+      if (ucolptr) ucolptr[j] = B.ucolptr[a + j] - u0;
+    }
+    const int64_t nl = B.lcolptr[a + ni] - 1 - l0, nu = B.ucolptr[a + ni] - 1 - u0;
+    for (int64_t k = 0; k < nl; ++k) {
+      if (lrowval) lrowval[k] = B.lrowval[l0 + k] - a;
+      if (lnzval) lnzval[k] = B.lnzval[l0 + k];
+    }
+    for (int64_t k = 0; k < nu; ++k) {
+      if (urowval) urowval[k] = B.urowval[u0 + k] - a;
+      if (unzval) unzval[k] = B.unzval[u0 + k];
+    }
+    for (int64_t k = 0; k < ni; ++k) {
+      const int64_t pk = B.p[a + k] - a;
+      if (p) p[k] = pk;
+      if (q) q[k] = B.q[a + k] - a;
+      if (pinv) pinv[pk - 1] = k + 1;
+    }
     return MFGPU_OK;
   });
 }

@@ -308,11 +308,29 @@ void front_work(const Plan& P, int32_t s, Launch& l) {
 }
 }  // namespace
 
+// Record C -= A * B in both tilings: 64 x 64 (FP64 and SIMT FP32 kernels)
+// and 128 x 128 (tensor-core FP32 kernel).
+void push_gemm(Plan& P, Launch& lg, const GemmTask& g0) {
+  GemmTask g = g0;
+  g.tiles_m = (int32_t)ceil_div(g.m, 64);
+  g.tiles_n = (int32_t)ceil_div(g.n, 64);
+  g.tile_base = lg.tiles;
+  lg.tiles += (int64_t)g.tiles_m * g.tiles_n;
+  P.gemm_tasks.push_back(g);
+  g.tiles_m = (int32_t)ceil_div(g.m, kTcTile);
+  g.tiles_n = (int32_t)ceil_div(g.n, kTcTile);
+  g.tile_base = lg.tiles_tc;
+  lg.tiles_tc += (int64_t)g.tiles_m * g.tiles_n;
+  P.gemm_tasks_tc.push_back(g);
+  ++lg.count;
+}
+
 void build_launches(Plan& P, bool safe) {
   P.small_tasks.clear();
   P.panel_tasks.clear();
   P.trsm_tasks.clear();
   P.gemm_tasks.clear();
+  P.gemm_tasks_tc.clear();
   P.launches.clear();
   P.has_speculative = false;
   std::vector<int32_t> large;
@@ -377,14 +395,9 @@ void build_launches(Plan& P, bool safe) {
           g.a = a; g.b = b; g.c = c;
           g.m = m; g.n = n; g.k = k;
           g.lda = g.ldb = g.ldc = nf;
-          g.tiles_m = (int32_t)ceil_div(m, 64);
-          g.tiles_n = (int32_t)ceil_div(n, 64);
-          g.tile_base = lg.tiles;
-          lg.tiles += (int64_t)g.tiles_m * g.tiles_n;
           lg.flops += 2.0 * m * n * k;
           lg.elems += 2.0 * m * n + (double)m * k + (double)k * n;
-          P.gemm_tasks.push_back(g);
-          ++lg.count;
+          push_gemm(P, lg, g);
         };
         if (npv > k1) {
           add_gemm(base + k1 + (int64_t)k0 * nf, base + k0 + (int64_t)k1 * nf, base + k1 + (int64_t)k1 * nf, nf - k1,
@@ -421,14 +434,9 @@ void build_launches(Plan& P, bool safe) {
       g.c = base + npv + (int64_t)npv * nf;
       g.m = nu; g.n = nu; g.k = npv;
       g.lda = g.ldb = g.ldc = nf;
-      g.tiles_m = (int32_t)ceil_div(nu, 64);
-      g.tiles_n = (int32_t)ceil_div(nu, 64);
-      g.tile_base = lg.tiles;
-      lg.tiles += (int64_t)g.tiles_m * g.tiles_n;
       lg.flops += 2.0 * nu * nu * npv;
       lg.elems += 2.0 * nu * nu + 2.0 * nu * npv;
-      P.gemm_tasks.push_back(g);
-      ++lg.count;
+      push_gemm(P, lg, g);
     }
     if (lg.count) P.launches.push_back(lg);
   }

@@ -20,6 +20,7 @@ namespace mfgpu {
 constexpr int kSmallFront = 64;      // fronts with nf <= this are factored in one CTA, in shared memory
 constexpr int kPanel = 64;           // panel width of the blocked large-front factorization
 constexpr int kPivRowsSmem = 256;    // pivot rows a partial-pivoting panel keeps in shared memory
+constexpr int kTcTile = 128;         // tile edge of the tensor-core GEMM of the FP32 fronts
 
 enum PanelMode : int32_t {
   kPanelSmemPivot = 0,   // rows k0..np-1 in shared memory, LAPACK partial pivoting
@@ -66,6 +67,7 @@ struct Launch {
   int64_t first;         // offset into the task array of this kind (or fc begin)
   int64_t count;         // tasks (or fc count)
   int64_t tiles;         // grid size in tiles for TRSM / GEMM
+  int64_t tiles_tc = 0;  // GEMM launches: grid size in 128 x 128 tensor-core tiles
   int32_t rows = 0;      // panel launches: row capacity (threads) of the kernel variant
   double flops = 0;      // algorithmic flops of the launch
   double elems = 0;      // algorithmic element moves (x sizeof(front type) = bytes)
@@ -112,6 +114,7 @@ struct Plan {
   std::vector<PanelTask> panel_tasks;
   std::vector<TrsmTask> trsm_tasks;
   std::vector<GemmTask> gemm_tasks;
+  std::vector<GemmTask> gemm_tasks_tc;   // the same updates tiled 128 x 128 (FP32 fronts, tensor cores)
   std::vector<Launch> launches;
   bool has_speculative = false;
   // statistics

@@ -13,6 +13,7 @@ from .api import (
     SCALE_NONE,
     SCALE_SUM,
     ArgumentError,
+    BatchLU,
     DimensionMismatch,
     GPLUFactorization,
     GpuContext,
@@ -22,6 +23,7 @@ from .api import (
     SingularException,
     SymbolicMF,
     amd_order_sym,
+    analyze_batch,
     apply_row_scaling,
     colamd_order,
     multifrontal_lu,
@@ -29,14 +31,15 @@ from .api import (
     row_scaling,
     solve,
     splu,
+    splu_batch,
     splu_q,
     symbolic_mf,
 )
 from .sparse import SparseCSC
 
 __all__ = [
-    "PRECISION_FP64", "PRECISION_MIXED", "SCALE_MAX", "SCALE_NONE", "SCALE_SUM", "ArgumentError",
+    "PRECISION_FP64", "PRECISION_MIXED", "SCALE_MAX", "SCALE_NONE", "SCALE_SUM", "ArgumentError", "BatchLU",
     "DimensionMismatch", "GPLUFactorization", "GpuContext", "MfgpuError", "PureLU", "ScaleKind",
-    "SingularException", "SymbolicMF", "SparseCSC", "amd_order_sym", "apply_row_scaling", "colamd_order",
-    "multifrontal_lu", "predicted_fill", "row_scaling", "solve", "splu", "splu_q", "symbolic_mf",
+    "SingularException", "SymbolicMF", "SparseCSC", "amd_order_sym", "analyze_batch", "apply_row_scaling", "colamd_order",
+    "multifrontal_lu", "predicted_fill", "row_scaling", "solve", "splu", "splu_batch", "splu_q", "symbolic_mf",
 ]

@@ -50,6 +50,12 @@ SIGNATURES = [
     ("mfgpu_stats_json", ctypes.c_int, [vp, ctypes.c_char_p, i64]),
     ("mfgpu_set_profiling", ctypes.c_int, [vp, i32]),
     ("mfgpu_launch_records", ctypes.c_int, [vp, ctypes.c_char_p, i64]),
+    ("mfgpu_batch_analyze", ctypes.c_int, [vp, i64, i64p, ctypes.POINTER(vp), ctypes.POINTER(vp), i32]),
+    ("mfgpu_batch_layout", ctypes.c_int, [vp, i64p, i64p, i64p]),
+    ("mfgpu_batch_factor", ctypes.c_int, [vp, ctypes.POINTER(vp), i32, i32, i64p]),
+    ("mfgpu_batch_solve", ctypes.c_int, [vp, i64, ctypes.POINTER(vp), ctypes.POINTER(vp), i32]),
+    ("mfgpu_batch_factor_sizes", ctypes.c_int, [vp, i64, i64p]),
+    ("mfgpu_batch_get_factors", ctypes.c_int, [vp, i64, i64p, i64p, f64p, i64p, i64p, f64p, i64p, i64p, i64p]),
 ]
 
 _lib = None
@@ -79,6 +85,11 @@ def lib():
 
 class MfOptions(ctypes.Structure):
     _fields_ = [("device", i32), ("precision", i32), ("flags", i32), ("reserved", i32)]
+
+
+def ptr_array(arrays):
+    """ctypes array of the data pointers of contiguous numpy arrays."""
+    return (vp * len(arrays))(*[a.ctypes.data for a in arrays])
 
 
 def ptr(a, ty=i64p):

@@ -44,6 +44,7 @@ SCALE_MAX = ScaleKind.SCALE_MAX
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
+FLAG_NO_TENSOR_CORES = 1   # mfgpu_options.flags: SIMT FP32 Schur updates in the mixed form
 
 
 class ArgumentError(ValueError):
@@ -209,9 +210,9 @@ def predicted_fill(S: SymbolicMF) -> int:
 class GpuContext:
     """One libmfgpu handle: analysis, resident factors, solves."""
 
-    def __init__(self, device: int = 0, precision: int = PRECISION_FP64):
+    def __init__(self, device: int = 0, precision: int = PRECISION_FP64, tensor_cores: bool = True):
         self._lib = L.lib()
-        opts = L.MfOptions(device, precision, 0, 0)
+        opts = L.MfOptions(device, precision, 0 if tensor_cores else FLAG_NO_TENSOR_CORES, 0)
         h = ctypes.c_void_p()
         rc = self._lib.mfgpu_create(ctypes.byref(opts), ctypes.byref(h))
         if rc != 0:
@@ -438,6 +439,105 @@ def splu_q(A: SparseCSC, q, scale=SCALE_SUM, check: bool = True, device: int = 0
     Rs = row_scaling(A, scale)
     ctx, S = _factor(A, q, check, None if scale == SCALE_NONE else Rs, device, precision)
     return PureLU(ctx, Rs, A, S)
+
+
+# ---------------------------------------------------------------------------
+# batched systems
+# ---------------------------------------------------------------------------
+ORDER_AMD = 0
+ORDER_COLAMD = 1
+
+
+class BatchLU:
+    """Factors of many independent systems held by one GPU handle.
+
+    System ``i`` behaves as ``splu(As[i]; method=:multifrontal, scale)``
+    (src/interface.jl:93-120), or with ``ordering="colamd"`` as
+    ``multifrontal_lu(Rs .* As[i]; q=colamd_order(As[i]))``
+    (src/multifrontal.jl:152); all systems are factored by one launch
+    sequence whose level-batched kernels take the fronts of every system at a
+    tree level together."""
+
+    def __init__(self, ctx: GpuContext, As, Rs, status):
+        self.ctx = ctx
+        self.As = list(As)
+        self.Rs = Rs
+        self.status = status
+        nsys = ctypes.c_int64()
+        col_off = np.empty(len(self.As) + 1, np.int64)
+        nz_off = np.empty(len(self.As) + 1, np.int64)
+        ctx._check(ctx._lib.mfgpu_batch_layout(ctx._h, ctypes.byref(nsys), L.ptr(col_off), L.ptr(nz_off)))
+        self.col_off, self.nz_off = col_off, nz_off
+
+    def __len__(self):
+        return len(self.As)
+
+    def solve(self, Bs, refine: int = 0):
+        """solve(F_i, b_i; refine) for every system; each b_i is a vector or
+        an n_i x k matrix with the same k for all systems."""
+        Bs = [np.asfortranarray(b, dtype=np.float64) for b in Bs]
+        if len(Bs) != len(self.As):
+            raise DimensionMismatch("one right-hand side block per system")
+        k = 1 if Bs[0].ndim == 1 else Bs[0].shape[1]
+        for A, b in zip(self.As, Bs):
+            if b.shape[0] != A.n or (1 if b.ndim == 1 else b.shape[1]) != k:
+                raise DimensionMismatch("right-hand side block does not match its system")
+        Xs = [np.empty_like(b) for b in Bs]
+        self.ctx._check(self.ctx._lib.mfgpu_batch_solve(self.ctx._h, k, L.ptr_array(Bs), L.ptr_array(Xs),
+                                                        int(refine)))
+        return Xs
+
+    def factors(self, i: int):
+        """(L, U, p, q, pinv) of system i: (Rs_i .* A_i)[p, q] == L * U."""
+        ctx = self.ctx
+        sz = np.empty(3, np.int64)
+        ctx._check(ctx._lib.mfgpu_batch_factor_sizes(ctx._h, int(i), L.ptr(sz)))
+        n, nl, nu = (int(v) for v in sz)
+        Lp, Li, Lx = np.empty(n + 1, np.int64), np.empty(nl, np.int64), np.empty(nl)
+        Up, Ui, Ux = np.empty(n + 1, np.int64), np.empty(nu, np.int64), np.empty(nu)
+        p, q, pinv = np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.int64)
+        ctx._check(ctx._lib.mfgpu_batch_get_factors(ctx._h, int(i), L.ptr(Lp), L.ptr(Li), L.ptr(Lx, L.f64p),
+                                                    L.ptr(Up), L.ptr(Ui), L.ptr(Ux, L.f64p), L.ptr(p), L.ptr(q),
+                                                    L.ptr(pinv)))
+        return SparseCSC(n, n, Lp, Li, Lx), SparseCSC(n, n, Up, Ui, Ux), p, q, pinv
+
+
+def analyze_batch(As, ordering: str = "amd", device: int = 0, precision: int = PRECISION_FP64) -> GpuContext:
+    """A GPU handle analyzed for the systems ``As`` (patterns only)."""
+    As = list(As)
+    if not As:
+        raise ArgumentError("empty batch")
+    for A in As:
+        if A.m != A.n:
+            raise DimensionMismatch("every system of a batch must be square")
+    order = {"amd": ORDER_AMD, "colamd": ORDER_COLAMD}.get(str(ordering).lstrip(":"))
+    if order is None:
+        raise ArgumentError(f"unknown ordering {ordering}")
+    ctx = GpuContext(device=device, precision=precision)
+    ns = np.array([A.n for A in As], np.int64)
+    cps = [_i(A.colptr) for A in As]
+    rvs = [_i(A.rowval) if A.nnz() else np.ones(1, np.int64) for A in As]
+    ctx._check(ctx._lib.mfgpu_batch_analyze(ctx._h, len(As), L.ptr(ns), L.ptr_array(cps), L.ptr_array(rvs), order))
+    ctx.n = int(ns.sum())
+    return ctx
+
+
+def splu_batch(As, scale=SCALE_SUM, ordering: str = "amd", check: bool = True, device: int = 0,
+               precision: int = PRECISION_FP64, ctx: GpuContext | None = None) -> BatchLU:
+    """Factor many independent systems in one batched call.  With ``check``
+    a singular system raises SingularException for the first such system
+    (``BatchLU.status`` lists every system's first singular column)."""
+    As = list(As)
+    scale = ScaleKind(int(scale))
+    if ctx is None:
+        ctx = analyze_batch(As, ordering, device, precision)
+    status = np.zeros(len(As), np.int64)
+    vals = [_f(A.nzval) if A.nnz() else np.zeros(1) for A in As]
+    ctx._check(ctx._lib.mfgpu_batch_factor(ctx._h, L.ptr_array(vals), int(scale), 0, L.ptr(status)))
+    if check and np.any(status):
+        raise SingularException(int(status[np.flatnonzero(status)[0]]))
+    Rs = [row_scaling(A, scale) for A in As]
+    return BatchLU(ctx, As, Rs, status)
 
 
 def solve(F, b, refine: int = 0) -> np.ndarray:
