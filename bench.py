@@ -320,10 +320,11 @@ def main():
             ctx.solve_device(R, d_b.data_ptr(), n, d_x.data_ptr(), n, refine)
 
         # refinement count that reaches the accuracy target on every rhs
-        refine, eta = 0, None
+        refine, eta, etas = 0, None, []
         for refine in range(0, MAX_REFINE + 1):
             step(refine)
             eta = ctx.backward_error_device(R, d_b.data_ptr(), n, d_x.data_ptr(), n)
+            etas.append(eta)
             if eta <= TARGET_ETA:
                 break
         for _ in range(args.warmup):
@@ -391,7 +392,7 @@ def main():
             e2e = {"value": e2e_s / world, "unit": "s", "h2d_bytes_per_step": 8 * (A.nnz() + n + n * R),
                    "d2h_bytes_per_step": 8 * n * R}
         forms[form] = {"ms_per_step": ms, "refine": refine, "eta": eta, "analyze_s": t_an + t_sym,
-                       "stats": st, "clocks": clk, "launches_timed": launches, "e2e": e2e}
+                       "stats": st, "clocks": clk, "launches_timed": launches, "e2e": e2e, "etas": etas}
         del ctx
         torch.cuda.empty_cache()
 
@@ -422,6 +423,7 @@ def main():
         "dtype": "f64" if primary == "fp64" else "f32+f64", "data": "synthetic", "form": primary,
         "config": workload_config(args, A),
         "forms": {k: {"s_per_step": f["ms_per_step"] / 1e3, "refine": f["refine"], "bwd_err": f["eta"],
+                      "bwd_err_by_refine": f.get("etas"),
                       "factor_ms": f["stats"]["factor_ms"], "solve_ms": f["stats"]["solve_ms"],
                       "analyze_s": f["analyze_s"], "e2e_s": f["e2e"]["value"] if f["e2e"] else None,
                       "kernels_ms": {kk: round(vv["ms"], 3) for kk, vv in f["stats"]["kernels"].items()}}

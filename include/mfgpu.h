@@ -94,7 +94,9 @@ typedef struct mfgpu_ctx mfgpu_ctx;
 
 /* mfgpu_options.flags */
 enum {
-  MFGPU_FLAG_NO_TENSOR_CORES = 1   /* FP32 fronts: SIMT FP32 Schur updates instead of tcgen05 3xTF32 */
+  MFGPU_FLAG_NO_TENSOR_CORES = 1,  /* FP32 fronts: SIMT FP32 Schur updates instead of tcgen05 3xTF32 */
+  MFGPU_FLAG_PERSISTENT_SOLVE = 2  /* solves: one cooperative persistent launch per pass instead of one launch
+                                      per step (fewer launches, lower occupancy; slower on the measured cases) */
 };
 
 typedef struct {
@@ -110,6 +112,12 @@ const char* mfgpu_last_error(const mfgpu_ctx* h);
 /* Work is issued on this stream (a cudaStream_t; NULL = the handle's own). */
 int mfgpu_set_stream(mfgpu_ctx* h, void* cuda_stream);
 int mfgpu_set_precision(mfgpu_ctx* h, int32_t precision);
+/* Mixed form: after the FP32 factorization the element growth
+ * max|U| / max|Rs .* A| is measured; above `limit` (default 1e4) the matrix
+ * is refactored in FP64 and solved with the FP64 factors (stats_json reports
+ * "growth" and "refactored_fp64").  No counterpart in the reference, which
+ * factors in the input precision only. */
+int mfgpu_set_growth_limit(mfgpu_ctx* h, double limit);
 
 /* Pattern analysis for the numeric phase, from the reference's own symbolic
  * result: A's pattern (colptr, rowval, n x n), SymbolicMF.qf, .parent,

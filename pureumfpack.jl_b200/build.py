@@ -29,6 +29,7 @@ DEPENDS = SOURCES + [
     "csrc/device/gemm_kernels.cuh",
     "csrc/device/solve_kernels.cuh",
     "csrc/device/tc_gemm.cuh",
+    "csrc/device/solve_persistent.cuh",
     "../include/mfgpu.h",
 ]
 NVCC_FLAGS = [

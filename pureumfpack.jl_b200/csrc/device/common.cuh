@@ -38,6 +38,7 @@ struct DevPlan {
   const int32_t* csr_col;
   const int32_t* csr_src;
   const int64_t* dinv_off;   // per supernode: first 64-block of its inverted diagonal blocks (-1: small front)
+  const int64_t* inv_off;    // per supernode: pool offset of inv(L11); inv(U11) follows (-1: small front)
 };
 
 // Per-factorization numeric state.

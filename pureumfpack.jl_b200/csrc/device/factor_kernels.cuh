@@ -115,7 +115,23 @@ __global__ void __launch_bounds__(256) k_assemble_columns(DevPlan P, int64_t fc0
     const int m = P.nu[k], nfk = P.nf[k], npk = P.np[k];
     const T* cb = pool + P.front_off[k] + npk + (int64_t)(npk + t) * nfk;
     const int32_t* rl = P.rel + P.upd_off[k];
-    for (int r = lane; r < m; r += 32) col[rl[r]] += cb[r];
+    // four rows per lane in flight (a child's rows map to distinct rows of
+    // this column, so all loads may precede the stores)
+    int r = lane;
+    for (; r + 96 < m; r += 128) {
+      int pos[4];
+      T v[4], o[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        pos[q] = rl[r + 32 * q];
+        v[q] = cb[r + 32 * q];
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) o[q] = col[pos[q]];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) col[pos[q]] = o[q] + v[q];
+    }
+    for (; r < m; r += 32) col[rl[r]] += cb[r];
     __syncwarp();
   }
 }
@@ -852,6 +868,29 @@ __global__ void k_build_values(int64_t nnz, const int32_t* __restrict__ src, con
   if (p >= nnz) return;
   const double v = ax[src[p]];
   vx[p] = rs ? rs[srow[p]] * v : v;
+}
+
+}  // namespace mfgpu
+
+namespace mfgpu {
+
+// Diagonal 64 x 64 blocks of the explicit pivot-block inverses, from the
+// panel factorization's inverted diagonal blocks: inv(L11) gets the unit
+// lower triangle, inv(U11) the upper one (the other triangles stay zero from
+// the clear that precedes this kernel).  One CTA per (supernode, block) pair.
+template <typename T>
+__global__ void __launch_bounds__(256) k_inv_init(DevPlan P, const int32_t* __restrict__ pairs,
+                                                  const T* __restrict__ dinv, T* __restrict__ pool) {
+  const int s = pairs[2 * blockIdx.x], j = pairs[2 * blockIdx.x + 1];
+  const int np = P.np[s], k0 = j * kPanel, kb = min(kPanel, np - k0);
+  const T* W = dinv + (P.dinv_off[s] + j) * (int64_t)kDinvElems;
+  T* li = pool + P.inv_off[s] + k0 + (int64_t)k0 * np;
+  T* ui = li + (int64_t)np * np;
+  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
+    const int r = e % kb, c = e / kb;
+    li[r + (int64_t)c * np] = r > c ? W[r + c * 64] : (r == c ? T(1) : T(0));
+    ui[r + (int64_t)c * np] = r <= c ? W[4096 + r + c * 64] : T(0);
+  }
 }
 
 }  // namespace mfgpu

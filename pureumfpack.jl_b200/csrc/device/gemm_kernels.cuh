@@ -1,11 +1,13 @@
-// gemm_kernels.cuh -- batched C -= A * B over heterogeneous problems.
+// gemm_kernels.cuh -- batched C = f(C, A * B) over heterogeneous problems.
 //
 // The dense updates of the large fronts (the trailing updates of the blocked
 // pivot-block LU and the Schur update F22 -= L21 * U12 of
 // src/multifrontal.jl:267-268) and the block updates of the supernodal solves
-// are all column-major C -= A * B on sub-blocks of resident buffers.  One
-// launch covers every problem of a level/step: a CTA owns one 64x64 tile of
-// one problem, located by binary search over the tile prefix.
+// are all column-major C -= A * B on sub-blocks of resident buffers; the
+// inversion of the pivot blocks and the inverse-based solves also need
+// C = A * B, C = -(A * B) and C = D - A * B (GemmTask::mode).  One launch
+// covers every problem of a level/step: a CTA owns one 64x64 tile of one
+// problem, located by binary search over the tile prefix.
 //
 // FP64: 8x8x4 DMMA tensor-core tiles (tcgen05 has no FP64 kind); operands are
 // staged through shared memory with cp.async double buffering.
@@ -28,19 +30,23 @@ __device__ __forceinline__ int find_task(const GemmTask* __restrict__ tasks, int
   return lo;
 }
 
-// pa / pb / pc: base pointers the task offsets refer to.
-__global__ void __launch_bounds__(kGemmThreads) k_gemm_f64(const GemmTask* __restrict__ tasks, int ntasks,
-                                                           const double* __restrict__ pa, const double* __restrict__ pb,
-                                                           double* __restrict__ pc) {
+constexpr int kGemmSmemF64 = 2 * kGemmBK * (kGemmBM + 8) + 2 * kGemmBN * (kGemmBK + 4);   // doubles
+
+// One 64 x 64 tile (index `tile` of the launch) of C -= A * B, 128 threads.
+// pa / pb / pc: base pointers the task offsets refer to; smem: kGemmSmemF64
+// doubles, 16-byte aligned.  C and B may be written by other steps of the
+// same persistent launch, so neither is read through the non-coherent path.
+__device__ __forceinline__ void gemm_tile_f64(const GemmTask* __restrict__ tasks, int ntasks,
+                                              const double* pa, const double* pb, double* pc, int64_t tile,
+                                              double* smem) {
   constexpr int BM = kGemmBM, BN = kGemmBN, BK = kGemmBK;
   constexpr int LDA_S = BM + 8;   // A tile stored k-major: As[k][m]
   constexpr int LDB_S = BK + 4;   // B tile stored n-major: Bs[n][k]
-  __shared__ __align__(16) double smem[2 * BK * LDA_S + 2 * BN * LDB_S];
   double* As = smem;
   double* Bs = smem + 2 * BK * LDA_S;
 
-  const GemmTask tk = tasks[find_task(tasks, ntasks, blockIdx.x)];
-  const int64_t local = blockIdx.x - tk.tile_base;
+  const GemmTask tk = tasks[find_task(tasks, ntasks, tile)];
+  const int64_t local = tile - tk.tile_base;
   const int m0 = (int)(local % tk.tiles_m) * BM;
   const int n0 = (int)(local / tk.tiles_m) * BN;
   const double* A = pa + tk.a;
@@ -119,13 +125,116 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_f64(const GemmTask* __res
         Cs[n * LDC_S + m] = acc[i][j][e];
       }
   __syncthreads();
-  for (int idx = tid; idx < BM * BN; idx += kGemmThreads) {
-    const int m = idx % BM, n = idx / BM;
-    if (m0 + m < M && n0 + n < N) {
-      double* cp = C + (int64_t)(m0 + m) + (int64_t)(n0 + n) * ldc;
-      *cp -= Cs[n * LDC_S + m];
-    }
+  // all loads of C before any store: the stores could alias later loads as
+  // far as the compiler knows, which would serialise one round trip each
+  constexpr int kPer = BM * BN / kGemmThreads;
+  const double* D = tk.mode == kGemmFrom ? pc + tk.d : C;
+  const int ldD = tk.mode == kGemmFrom ? tk.ldd : ldc;
+  const bool load = tk.mode == kGemmSub || tk.mode == kGemmFrom;
+  const double sgn = tk.mode == kGemmSet ? -1.0 : 1.0;   // Set: C = +AB; Neg: C = -AB = 0 - AB
+  double cv[kPer];
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    const int idx = tid + i * kGemmThreads, m = idx % BM, n = idx / BM;
+    cv[i] = (load && m0 + m < M && n0 + n < N) ? D[(int64_t)(m0 + m) + (int64_t)(n0 + n) * ldD] : 0.0;
   }
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    const int idx = tid + i * kGemmThreads, m = idx % BM, n = idx / BM;
+    if (m0 + m < M && n0 + n < N)
+      C[(int64_t)(m0 + m) + (int64_t)(n0 + n) * ldc] = cv[i] - sgn * Cs[n * LDC_S + m];
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kGemmThreads) k_gemm_f64(const GemmTask* __restrict__ tasks, int ntasks,
+                                                           const double* __restrict__ pa, const double* __restrict__ pb,
+                                                           double* __restrict__ pc) {
+  __shared__ __align__(16) double smem[kGemmSmemF64];
+  gemm_tile_f64(tasks, ntasks, pa, pb, pc, blockIdx.x, smem);
+}
+
+// FP32 64 x 64 tile for 128 threads (4 x 8 register micro-tiles), the same
+// task format; smem: kGemmSmemF32 floats.
+constexpr int kGemmSmemF32 = 2 * 16 * (64 + 4) * 2;
+__device__ __forceinline__ void gemm_tile_f32(const GemmTask* __restrict__ tasks, int ntasks, const float* pa,
+                                              const float* pb, float* pc, int64_t tile, float* smem) {
+  constexpr int BM = 64, BN = 64, BK = 16, LD = 64 + 4;
+  float* As = smem;                  // [2][BK][LD]
+  float* Bs = smem + 2 * BK * LD;    // [2][BK][LD]
+  const GemmTask tk = tasks[find_task(tasks, ntasks, tile)];
+  const int64_t local = tile - tk.tile_base;
+  const int m0 = (int)(local % tk.tiles_m) * BM;
+  const int n0 = (int)(local / tk.tiles_m) * BN;
+  const float* A = pa + tk.a;
+  const float* B = pb + tk.b;
+  float* C = pc + tk.c;
+  const int M = tk.m, N = tk.n, K = tk.k, lda = tk.lda, ldb = tk.ldb, ldc = tk.ldc;
+  const int tid = threadIdx.x;
+  const int tm = (tid & 15) * 4, tn = (tid >> 4) * 8;
+  float acc[4][8] = {};
+  auto load = [&](int st, int k0) {
+#pragma unroll
+    for (int i = 0; i < (BM * BK) / 128; ++i) {
+      const int idx = tid + i * 128;
+      const int m = idx % BM, k = idx / BM;
+      const bool ok = (m0 + m < M) && (k0 + k < K);
+      cp_async4(As + (st * BK + k) * LD + m, ok ? A + (int64_t)(m0 + m) + (int64_t)(k0 + k) * lda : A, ok);
+    }
+#pragma unroll
+    for (int i = 0; i < (BN * BK) / 128; ++i) {
+      const int idx = tid + i * 128;
+      const int k = idx % BK, n = idx / BK;
+      const bool ok = (n0 + n < N) && (k0 + k < K);
+      cp_async4(Bs + (st * BK + k) * LD + n, ok ? B + (int64_t)(k0 + k) + (int64_t)(n0 + n) * ldb : B, ok);
+    }
+    cp_async_commit();
+  };
+  const int ktiles = (K + BK - 1) / BK;
+  load(0, 0);
+  for (int kt = 0; kt < ktiles; ++kt) {
+    if (kt + 1 < ktiles) {
+      load((kt + 1) & 1, (kt + 1) * BK);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const float* as = As + (kt & 1) * BK * LD;
+    const float* bs = Bs + (kt & 1) * BK * LD;
+#pragma unroll
+    for (int k = 0; k < BK; ++k) {
+      float a[4], b[8];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = as[k * LD + tm + i];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) b[j] = bs[k * LD + tn + j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+  const float* D = tk.mode == kGemmFrom ? pc + tk.d : C;
+  const int ldD = tk.mode == kGemmFrom ? tk.ldd : ldc;
+  const bool ld = tk.mode == kGemmSub || tk.mode == kGemmFrom;
+  const float sgn = tk.mode == kGemmSet ? -1.0f : 1.0f;
+  float cv[4][8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int m = m0 + tm + i, n = n0 + tn + j;
+      cv[i][j] = (ld && m < M && n < N) ? D[(int64_t)m + (int64_t)n * ldD] : 0.0f;
+    }
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int m = m0 + tm + i, n = n0 + tn + j;
+      if (m < M && n < N) C[(int64_t)m + (int64_t)n * ldc] = cv[i][j] - sgn * acc[i][j];
+    }
 }
 
 // FP32 variant (mixed-precision fronts), CUDA-core FFMA with 4x4 register
@@ -189,126 +298,25 @@ __global__ void __launch_bounds__(256) k_gemm_f32(const GemmTask* __restrict__ t
     }
     __syncthreads();
   }
+  const float* D = tk.mode == kGemmFrom ? pc + tk.d : C;
+  const int ldD = tk.mode == kGemmFrom ? tk.ldd : ldc;
+  const bool ld = tk.mode == kGemmSub || tk.mode == kGemmFrom;
+  const float sgn = tk.mode == kGemmSet ? -1.0f : 1.0f;
+  float cv[4][4];
 #pragma unroll
   for (int j = 0; j < 4; ++j)
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int m = m0 + tm + i, n = n0 + tn + j;
-      if (m < M && n < N) C[(int64_t)m + (int64_t)n * ldc] -= acc[i][j];
-    }
-}
-
-}  // namespace mfgpu
-
-namespace mfgpu {
-
-// FP64 batched GEMM, C -= A * B, templated on the CTA tile (BM x BN), the warp
-// tile (WM x WN, multiples of 8) and the cp.async pipeline depth.  Same task
-// format as k_gemm_f64; the tasks' tiles_m / tiles_n must use BM / BN.
-template <int BM, int BN, int WM, int WN, int STAGES>
-struct GemmCfg {
-  static constexpr int kWarps = (BM / WM) * (BN / WN);
-  static constexpr int kThreads = kWarps * 32;
-  static constexpr int BK = 16;
-  static constexpr int kLdA = BM + 8;     // A stage: k-major [BK][BM + 8]
-  static constexpr int kLdB = BK + 4;     // B stage: n-major [BN][BK + 4]
-  static constexpr int kStageA = BK * kLdA;
-  static constexpr int kStageB = BN * kLdB;
-  static constexpr int kLdC = BM + 1;
-  static constexpr size_t kSmemOps = (size_t)STAGES * (kStageA + kStageB);
-  static constexpr size_t kSmemC = (size_t)BN * kLdC;
-  static constexpr size_t kSmem = (kSmemOps > kSmemC ? kSmemOps : kSmemC) * sizeof(double);
-};
-
-template <int BM, int BN, int WM, int WN, int STAGES>
-__global__ void __launch_bounds__(GemmCfg<BM, BN, WM, WN, STAGES>::kThreads)
-    k_gemm_f64_t(const GemmTask* __restrict__ tasks, int ntasks, const double* __restrict__ pa,
-                 const double* __restrict__ pb, double* __restrict__ pc) {
-  using C = GemmCfg<BM, BN, WM, WN, STAGES>;
-  constexpr int BK = C::BK, NT = C::kThreads;
-  constexpr int FM = WM / 8, FN = WN / 8;           // 8x8 fragments per warp
-  extern __shared__ __align__(16) double gsm[];
-  double* As = gsm;
-  double* Bs = gsm + STAGES * C::kStageA;
-
-  const GemmTask tk = tasks[find_task(tasks, ntasks, blockIdx.x)];
-  const int64_t local = blockIdx.x - tk.tile_base;
-  const int m0 = (int)(local % tk.tiles_m) * BM;
-  const int n0 = (int)(local / tk.tiles_m) * BN;
-  const double* A = pa + tk.a;
-  const double* B = pb + tk.b;
-  double* Cg = pc + tk.c;
-  const int M = tk.m, N = tk.n, K = tk.k, lda = tk.lda, ldb = tk.ldb, ldc = tk.ldc;
-  const int tid = threadIdx.x, lane = lane_id(), warp = warp_id();
-  const int wm = (warp % (BM / WM)) * WM, wn = (warp / (BM / WM)) * WN;
-
-  auto load_stage = [&](int stage, int k0) {
-    double* as = As + stage * C::kStageA;
-    double* bs = Bs + stage * C::kStageB;
-#pragma unroll
-    for (int i = 0; i < (BM * BK) / NT; ++i) {
-      const int idx = tid + i * NT;
-      const int m = idx % BM, k = idx / BM;
-      const bool ok = (m0 + m < M) && (k0 + k < K);
-      cp_async8(as + k * C::kLdA + m, ok ? A + (int64_t)(m0 + m) + (int64_t)(k0 + k) * lda : A, ok);
+      cv[i][j] = (ld && m < M && n < N) ? D[(int64_t)m + (int64_t)n * ldD] : 0.0f;
     }
 #pragma unroll
-    for (int i = 0; i < (BN * BK) / NT; ++i) {
-      const int idx = tid + i * NT;
-      const int k = idx % BK, n = idx / BK;
-      const bool ok = (n0 + n < N) && (k0 + k < K);
-      cp_async8(bs + n * C::kLdB + k, ok ? B + (int64_t)(k0 + k) + (int64_t)(n0 + n) * ldb : B, ok);
+  for (int j = 0; j < 4; ++j)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int m = m0 + tm + i, n = n0 + tn + j;
+      if (m < M && n < N) C[(int64_t)m + (int64_t)n * ldc] = cv[i][j] - sgn * acc[i][j];
     }
-  };
-
-  double acc[FM][FN][2];
-#pragma unroll
-  for (int i = 0; i < FM; ++i)
-#pragma unroll
-    for (int j = 0; j < FN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-
-  const int ktiles = (K + BK - 1) / BK;
-#pragma unroll
-  for (int s = 0; s < STAGES - 1; ++s) {
-    if (s < ktiles) load_stage(s, s * BK);
-    cp_async_commit();
-  }
-  for (int kt = 0; kt < ktiles; ++kt) {
-    cp_async_wait<STAGES - 2>();
-    __syncthreads();
-    const int pre = kt + STAGES - 1;
-    if (pre < ktiles) load_stage(pre % STAGES, pre * BK);
-    cp_async_commit();
-    const double* as = As + (kt % STAGES) * C::kStageA;
-    const double* bs = Bs + (kt % STAGES) * C::kStageB;
-#pragma unroll
-    for (int kk = 0; kk < BK; kk += 4) {
-      double af[FM], bf[FN];
-#pragma unroll
-      for (int i = 0; i < FM; ++i) af[i] = as[(kk + (lane & 3)) * C::kLdA + wm + i * 8 + (lane >> 2)];
-#pragma unroll
-      for (int j = 0; j < FN; ++j) bf[j] = bs[(wn + j * 8 + (lane >> 2)) * C::kLdB + kk + (lane & 3)];
-#pragma unroll
-      for (int i = 0; i < FM; ++i)
-#pragma unroll
-        for (int j = 0; j < FN; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
-    }
-  }
-  cp_async_wait<0>();
-  __syncthreads();
-  double* Cs = gsm;
-#pragma unroll
-  for (int i = 0; i < FM; ++i)
-#pragma unroll
-    for (int j = 0; j < FN; ++j)
-#pragma unroll
-      for (int e = 0; e < 2; ++e)
-        Cs[(wn + j * 8 + 2 * (lane & 3) + e) * C::kLdC + wm + i * 8 + (lane >> 2)] = acc[i][j][e];
-  __syncthreads();
-  for (int idx = tid; idx < BM * BN; idx += NT) {
-    const int m = idx % BM, n = idx / BM;
-    if (m0 + m < M && n0 + n < N) Cg[(int64_t)(m0 + m) + (int64_t)(n0 + n) * ldc] -= Cs[n * C::kLdC + m];
-  }
 }
 
 }  // namespace mfgpu

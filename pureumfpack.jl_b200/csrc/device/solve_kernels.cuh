@@ -13,7 +13,10 @@
 // the result is deterministic.  Backward (root to leaves): x_piv =
 // U11 \ (y - U12 * x[upd]), gathering x of the ancestors' columns.  Finally
 // x[q] = x_factor (interface.jl:134-136).  Work arrays are column-major with
-// one column per right-hand side.
+// one column per right-hand side.  Small supernodes (nf <= 64) substitute
+// column by column in one CTA; large ones multiply by the explicit inverses
+// of L11 and U11 formed after the factorization, so their solves are batched
+// GEMMs (the launch sequence is built in mfgpu.cu: build_solve_schedule).
 #pragma once
 
 #include "common.cuh"
@@ -47,13 +50,21 @@ __device__ __forceinline__ int front_pos(const DevState& S, int c1, int np, int 
   return rel < np ? S.rowfac[c1 + rel] - c1 : rel;
 }
 
+// Every solve kernel is a loop-free "item" function -- one (supernode or
+// block, right-hand-side chunk) per CTA -- so that the same code runs as a
+// one-launch-per-step kernel (the __global__ wrappers below) and inside the
+// persistent solve kernel, which walks all steps with grid barriers between
+// them.  fsol and xw are written and read by different steps of one
+// persistent launch, so they are never read through the non-coherent path.
+
+// Small supernodes, forward: one CTA per (supernode bx, 32-column chunk by).
+// smem: kSmallFront * kSolveCols elements.
 template <typename T>
-__global__ void __launch_bounds__(kSolveThreads) k_fwd_small(DevPlan P, DevState S, SolveArgs A,
-                                                             const int32_t* __restrict__ tasks,
-                                                             const T* __restrict__ pool, T* __restrict__ fsol) {
-  __shared__ T f[kSmallFront * kSolveCols];
-  const int s = tasks[blockIdx.x];
-  const int c0 = blockIdx.y * kSolveCols;
+__device__ __forceinline__ void fwd_small_item(const DevPlan& P, const DevState& S, const SolveArgs& A,
+                                               const int32_t* __restrict__ tasks, const T* __restrict__ pool,
+                                               T* fsol, int bx, int by, T* f) {
+  const int s = tasks[bx];
+  const int c0 = by * kSolveCols;
   const int rc = min(kSolveCols, (int)(A.nrhs - c0));
   const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
   const int tid = threadIdx.x;
@@ -88,14 +99,24 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd_small(DevPlan P, DevState
     const int r = e % nf, c = e / nf;
     out[r + (int64_t)(c0 + c) * nf] = f[e];
   }
+  __syncthreads();
 }
 
-// Large supernodes: gather the rhs block (one warp per right-hand side).
 template <typename T>
-__global__ void __launch_bounds__(256) k_fwd_assemble(DevPlan P, DevState S, SolveArgs A,
-                                                      const int32_t* __restrict__ tasks, T* __restrict__ fsol) {
-  const int s = tasks[blockIdx.x];
-  const int64_t col = (int64_t)blockIdx.y * 8 + warp_id();
+__global__ void __launch_bounds__(kSolveThreads) k_fwd_small(DevPlan P, DevState S, SolveArgs A,
+                                                             const int32_t* __restrict__ tasks,
+                                                             const T* __restrict__ pool, T* fsol) {
+  __shared__ T f[kSmallFront * kSolveCols];
+  fwd_small_item<T>(P, S, A, tasks, pool, fsol, blockIdx.x, blockIdx.y, f);
+}
+
+// Large supernodes: gather the rhs block, one warp per right-hand side;
+// item (bx, by) covers columns by * warps .. of supernode tasks[bx].
+template <typename T>
+__device__ __forceinline__ void fwd_assemble_item(const DevPlan& P, const DevState& S, const SolveArgs& A,
+                                                  const int32_t* __restrict__ tasks, T* fsol, int bx, int by) {
+  const int s = tasks[bx];
+  const int64_t col = (int64_t)by * (blockDim.x >> 5) + warp_id();
   if (col >= A.nrhs) return;
   const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
   const int lane = lane_id();
@@ -108,54 +129,41 @@ __global__ void __launch_bounds__(256) k_fwd_assemble(DevPlan P, DevState S, Sol
     const int m = P.nu[k], nfk = P.nf[k], npk = P.np[k];
     const T* w = fsol + P.colbase[k] * R + npk + col * nfk;
     const int32_t* rl = P.rel + P.upd_off[k];
-    for (int r = lane; r < m; r += 32) f[front_pos(S, c1, np, rl[r])] += w[r];
+    // four rows per lane in flight: a child's rows map to distinct front
+    // rows, so the loads may all precede the stores
+    int r = lane;
+    for (; r + 96 < m; r += 128) {
+      int pos[4];
+      T v[4], o[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        pos[q] = front_pos(S, c1, np, rl[r + 32 * q]);
+        v[q] = w[r + 32 * q];
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) o[q] = f[pos[q]];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) f[pos[q]] = o[q] + v[q];
+    }
+    for (; r < m; r += 32) f[front_pos(S, c1, np, rl[r])] += w[r];
     __syncwarp();
   }
 }
 
-struct SolveBlockTask {
-  int32_t s, k0;
-};
-
-// Forward diagonal block of rows k0..k1-1: y = inv(L_kk) * f on a 64-column
-// tile of right-hand sides, as a tensor-core tile product (the inverse was
-// formed by the panel factorization).
 template <typename T>
-__global__ void __launch_bounds__(kApplyThreads) k_fwd_diag(DevPlan P, const SolveBlockTask* __restrict__ tasks,
-                                                            int64_t nrhs, const T* __restrict__ dinv,
-                                                            T* __restrict__ fsol) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sP = reinterpret_cast<T*>(smem_raw);
-  T* sQ = sP + 64 * kLdP;
-  const SolveBlockTask tk = tasks[blockIdx.x];
-  const int s = tk.s, k0 = tk.k0;
-  const int np = P.np[s], nf = P.nf[s];
-  const int kb = min(kPanel, np - k0);
-  const int64_t c0 = (int64_t)blockIdx.y * 64;
-  const int rc = (int)(nrhs - c0 < 64 ? nrhs - c0 : 64);
-  const T* W = dinv + (P.dinv_off[s] + k0 / kPanel) * (int64_t)kDinvElems;
-  T* y = fsol + P.colbase[s] * nrhs + k0;
-  for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
-    const int r = e & 63, c = e >> 6;
-    sP[r + c * kLdP] = W[e];
-    sQ[r + c * kLdQ] = (r < kb && c < rc) ? y[r + (c0 + c) * nf] : T(0);
-  }
-  __syncthreads();
-  mm64<T>(sP, sQ, sQ, kLdQ);
-  for (int e = threadIdx.x; e < kb * rc; e += blockDim.x) {
-    const int r = e % kb, c = e / kb;
-    y[r + (c0 + c) * nf] = sQ[r + c * kLdQ];
-  }
+__global__ void __launch_bounds__(256) k_fwd_assemble(DevPlan P, DevState S, SolveArgs A,
+                                                      const int32_t* __restrict__ tasks, T* fsol) {
+  fwd_assemble_item<T>(P, S, A, tasks, fsol, blockIdx.x, blockIdx.y);
 }
 
+// Small supernodes, backward.  smem: 2 * kSmallFront * kSolveCols elements.
 template <typename T>
-__global__ void __launch_bounds__(kSolveThreads) k_bwd_small(DevPlan P, SolveArgs A, const int32_t* __restrict__ tasks,
-                                                             const T* __restrict__ pool, T* __restrict__ fsol,
-                                                             T* __restrict__ xw) {
-  __shared__ T y[kSmallFront * kSolveCols];
-  __shared__ T g[kSmallFront * kSolveCols];
-  const int s = tasks[blockIdx.x];
-  const int c0 = blockIdx.y * kSolveCols;
+__device__ __forceinline__ void bwd_small_item(const DevPlan& P, const SolveArgs& A,
+                                               const int32_t* __restrict__ tasks, const T* __restrict__ pool,
+                                               const T* fsol, T* xw, int bx, int by, T* y) {
+  T* g = y + kSmallFront * kSolveCols;
+  const int s = tasks[bx];
+  const int c0 = by * kSolveCols;
   const int rc = min(kSolveCols, (int)(A.nrhs - c0));
   const int np = P.np[s], nu = P.nu[s], nf = P.nf[s], c1 = P.c1[s];
   const int tid = threadIdx.x;
@@ -192,14 +200,23 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_small(DevPlan P, SolveArg
     const int r = e % np, c = e / np;
     xw[c1 + r + (int64_t)(c0 + c) * A.ldx] = y[r + c * np];
   }
+  __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSolveThreads) k_bwd_small(DevPlan P, SolveArgs A, const int32_t* __restrict__ tasks,
+                                                             const T* __restrict__ pool, const T* fsol, T* xw) {
+  __shared__ T y[2 * kSmallFront * kSolveCols];
+  bwd_small_item<T>(P, A, tasks, pool, fsol, xw, blockIdx.x, blockIdx.y, y);
 }
 
 // Large supernodes: gather x of the update columns into the w rows.
 template <typename T>
-__global__ void __launch_bounds__(256) k_bwd_gather(DevPlan P, SolveArgs A, const int32_t* __restrict__ tasks,
-                                                    T* __restrict__ fsol, const T* __restrict__ xw) {
-  const int s = tasks[blockIdx.x];
-  const int64_t col = (int64_t)blockIdx.y * 8 + warp_id();
+__device__ __forceinline__ void bwd_gather_item(const DevPlan& P, const SolveArgs& A,
+                                                const int32_t* __restrict__ tasks, T* fsol, const T* xw, int bx,
+                                                int by) {
+  const int s = tasks[bx];
+  const int64_t col = (int64_t)by * (blockDim.x >> 5) + warp_id();
   if (col >= A.nrhs) return;
   const int np = P.np[s], nu = P.nu[s], nf = P.nf[s];
   T* f = fsol + P.colbase[s] * A.nrhs + col * nf + np;
@@ -207,35 +224,10 @@ __global__ void __launch_bounds__(256) k_bwd_gather(DevPlan P, SolveArgs A, cons
   for (int t = lane_id(); t < nu; t += 32) f[t] = xw[us[t] + col * A.ldx];
 }
 
-// Backward diagonal block: x = inv(U_kk) * f, written to the block rows and to x.
 template <typename T>
-__global__ void __launch_bounds__(kApplyThreads) k_bwd_diag(DevPlan P, const SolveBlockTask* __restrict__ tasks,
-                                                            int64_t nrhs, int64_t ldx, const T* __restrict__ dinv,
-                                                            T* __restrict__ fsol, T* __restrict__ xw) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sP = reinterpret_cast<T*>(smem_raw);
-  T* sQ = sP + 64 * kLdP;
-  const SolveBlockTask tk = tasks[blockIdx.x];
-  const int s = tk.s, k0 = tk.k0;
-  const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
-  const int kb = min(kPanel, np - k0);
-  const int64_t c0 = (int64_t)blockIdx.y * 64;
-  const int rc = (int)(nrhs - c0 < 64 ? nrhs - c0 : 64);
-  const T* W = dinv + (P.dinv_off[s] + k0 / kPanel) * (int64_t)kDinvElems + 4096;
-  T* y = fsol + P.colbase[s] * nrhs + k0;
-  for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
-    const int r = e & 63, c = e >> 6;
-    sP[r + c * kLdP] = W[e];
-    sQ[r + c * kLdQ] = (r < kb && c < rc) ? y[r + (c0 + c) * nf] : T(0);
-  }
-  __syncthreads();
-  mm64<T>(sP, sQ, sQ, kLdQ);
-  for (int e = threadIdx.x; e < kb * rc; e += blockDim.x) {
-    const int r = e % kb, c = e / kb;
-    const T v = sQ[r + c * kLdQ];
-    y[r + (c0 + c) * nf] = v;
-    xw[c1 + k0 + r + (c0 + c) * ldx] = v;
-  }
+__global__ void __launch_bounds__(256) k_bwd_gather(DevPlan P, SolveArgs A, const int32_t* __restrict__ tasks,
+                                                    T* fsol, const T* xw) {
+  bwd_gather_item<T>(P, A, tasks, fsol, xw, blockIdx.x, blockIdx.y);
 }
 
 // x[q[k]] = x_factor[k] (interface.jl:134-136); optionally accumulate (x += d).
@@ -292,6 +284,23 @@ __global__ void __launch_bounds__(256) k_bwd_error_parts(int64_t n, int64_t nrhs
       atomicMax(out + 3 * c + threadIdx.x, (unsigned long long)__double_as_longlong(m));
     }
     __syncthreads();
+  }
+}
+
+// max |x_i| over n doubles into out (as bits; non-negative doubles order like
+// their bit patterns): grid-stride, reduced per CTA, one atomic per CTA.
+__global__ void __launch_bounds__(256) k_abs_max(const double* __restrict__ x, int64_t n,
+                                                 unsigned long long* __restrict__ out) {
+  __shared__ double red[8];
+  double m = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    m = fmax(m, fabs(x[i]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane_id() == 0) red[warp_id()] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+    atomicMax(out, (unsigned long long)__double_as_longlong(m));
   }
 }
 

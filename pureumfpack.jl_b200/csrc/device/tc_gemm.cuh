@@ -143,7 +143,7 @@ __device__ __forceinline__ void tc_put4(uint32_t hi_base, uint32_t lo_base, int 
 // Batched C -= A * B over GemmTasks whose tiles_m / tiles_n count
 // 128 x BN tiles.  flags[1] is set when a bounded wait expired.
 template <int BN, int STAGES>
-__global__ void __launch_bounds__(kTcThreads) k_gemm_tc(const GemmTask* __restrict__ tasks, int ntasks,
+__global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(const GemmTask* __restrict__ tasks, int ntasks,
                                                         const float* __restrict__ pa, const float* __restrict__ pb,
                                                         float* pc, int* __restrict__ flags) {
   using Cfg = TcCfg<BN, STAGES>;
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(kTcThreads) k_gemm_tc(const GemmTask* __restri
 
   if (warp < 4) {
     // ---- epilogue: warp w reads accumulator lanes 32w..32w+31 (rows of the tile)
-    const bool ok = mbar_wait(&done, 0u) && !failed && nk > 0;
+    const bool ok = mbar_wait(&done, 0u) && !failed;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok) {
       float* C = pc + tk.c;
@@ -264,6 +264,10 @@ __global__ void __launch_bounds__(kTcThreads) k_gemm_tc(const GemmTask* __restri
       for (int c0 = 0; c0 < BN; c0 += 32) {
         uint32_t v[32];
         const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+        if (nk == 0) {   // K = 0: the product is zero (C = D or C = 0)
+#pragma unroll
+          for (int j = 0; j < 32; ++j) v[j] = 0u;
+        } else {
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
             "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -275,17 +279,22 @@ __global__ void __launch_bounds__(kTcThreads) k_gemm_tc(const GemmTask* __restri
               "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
             : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        }
         if (row < M) {
+          const float* D = tk.mode == kGemmFrom ? pc + tk.d : C;
+          const int ldD = tk.mode == kGemmFrom ? tk.ldd : tk.ldc;
+          const bool ld = tk.mode == kGemmSub || tk.mode == kGemmFrom;
+          const float sgn = tk.mode == kGemmSet ? -1.0f : 1.0f;
           float cv[32];
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const int col = n0 + c0 + j;
-            cv[j] = col < N ? C[(int64_t)row + (int64_t)col * tk.ldc] : 0.0f;
+            cv[j] = (ld && col < N) ? D[(int64_t)row + (int64_t)col * ldD] : 0.0f;
           }
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const int col = n0 + c0 + j;
-            if (col < N) C[(int64_t)row + (int64_t)col * tk.ldc] = cv[j] - __uint_as_float(v[j]);
+            if (col < N) C[(int64_t)row + (int64_t)col * tk.ldc] = cv[j] - sgn * __uint_as_float(v[j]);
           }
         }
       }

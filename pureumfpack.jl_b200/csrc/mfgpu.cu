@@ -25,6 +25,7 @@
 #include "device/gemm_kernels.cuh"
 #include "device/tc_gemm.cuh"
 #include "device/solve_kernels.cuh"
+#include "device/solve_persistent.cuh"
 #include "host/symbolic.h"
 #include "plan.h"
 
@@ -86,13 +87,13 @@ inline unsigned grid1(int64_t work, int per) { return (unsigned)((work + per - 1
 
 enum KernelClass {
   KC_BUILD_VALUES, KC_SMALL, KC_ASSEMBLE, KC_PANEL, KC_TRSM, KC_GEMM_FACTOR, KC_PIVOTS, KC_SCATTER,
-  KC_FWD_SMALL, KC_FWD_ASSEMBLE, KC_FWD_DIAG, KC_GEMM_SOLVE, KC_BWD_SMALL, KC_BWD_GATHER, KC_BWD_DIAG,
-  KC_SOLVE_FINISH, KC_RESIDUAL, KC_COUNT
+  KC_FWD_SMALL, KC_FWD_ASSEMBLE, KC_GEMM_SOLVE, KC_BWD_SMALL, KC_BWD_GATHER,
+  KC_SOLVE_FINISH, KC_RESIDUAL, KC_INVERSE, KC_COUNT
 };
 const char* const kKernelClassName[KC_COUNT] = {
     "build_values", "small_fronts", "assemble_columns", "panel", "panel_trsm", "gemm_factor", "finalize_pivots",
-    "scatter_csc", "fwd_small", "fwd_assemble", "fwd_diag", "gemm_solve", "bwd_small", "bwd_gather", "bwd_diag",
-    "solve_finish", "residual"};
+    "scatter_csc", "fwd_small", "fwd_assemble", "gemm_solve", "bwd_small", "bwd_gather",
+    "solve_finish", "residual", "gemm_inverse"};
 
 struct KStat {
   double ms = 0, flops = 0, bytes = 0;
@@ -102,16 +103,17 @@ struct KStat {
 struct SolveSchedule {
   int64_t nrhs = -1;
   struct Step {
-    int kind;        // 0 fwd_small, 1 fwd_assemble, 2 fwd_diag, 3 gemm(front,fsol,fsol), 4 bwd_small,
-                     // 5 bwd_gather, 6 bwd_diag
+    int kind;        // 0 fwd_small, 1 fwd_assemble, 3 gemm (A: pool; B, C, D: solve arena), 4 bwd_small,
+                     // 5 bwd_gather
     int64_t first, count, tiles;
     double flops = 0, elems = 0;
+    int64_t tiles_tc = 0;   // GEMM steps: grid in 128 x 128 tensor-core tiles (gemms_tc)
   };
   std::vector<Step> steps;
   std::vector<int32_t> ids;
-  std::vector<SolveBlockTask> blocks;
-  std::vector<GemmTask> gemms;
-  DevBuf d_ids, d_blocks, d_gemms;
+  std::vector<GemmTask> gemms, gemms_tc;   // 64 x 64 tiles; 128 x 128 tiles (FP32 on tensor cores)
+  std::vector<SolvePhase> phases;   // the steps as work-item phases of the persistent solve
+  DevBuf d_ids, d_gemms, d_gemms_tc, d_phases;
 };
 
 }  // namespace
@@ -134,15 +136,29 @@ struct mfgpu_ctx {
   bool launches_safe = false;
   // numeric state
   DevBuf b_pool, b_vx, b_ax, b_rs, b_ipiv, b_info, b_prow, b_rowfac, b_flags, b_dinv, b_dinv_off;
+  DevBuf b_inv_off, b_inv_blocks, b_inv_tasks, b_inv_tasks_tc;   // pivot-block inversion
   bool have_rs = false;
   int factor_precision = MFGPU_PRECISION_FP64;
   DevBuf b_li, b_lx, b_ui, b_ux;
   // solve state
   SolveSchedule sched;
-  DevBuf b_fsol, b_xw, b_b, b_x, b_r, b_d, b_err, b_norm;
+  DevBuf b_fsol, b_b, b_x, b_r, b_d, b_err, b_norm;   // b_fsol: solve arena (blocks, then x)
+  // persistent solve: one cooperative launch per pass (false: one launch per step)
+  bool persistent = false;
+  int persist_grid[2] = {0, 0};          // CTAs of the persistent kernel, FP32 / FP64
+  DevBuf b_bar, b_stamps;                // barrier words {count, gen, err, sticky err}; profiling stamps
+  struct PhaseProfile {                  // one profiled persistent launch
+    size_t stamp0;
+    int nphases;
+    int elem_bytes;
+  };
+  std::vector<PhaseProfile> pending_phases;
+  size_t stamp_next = 0;
   // stats
   double t_analyze_ms = 0, t_factor_ms = 0, t_solve_ms = 0, t_csc_ms = 0;
   int factor_reruns = 0;
+  double growth = 0.0, growth_limit = 1e4;   // mixed form: element growth and the FP64 refactor limit
+  bool refactored_fp64 = false;
   int32_t last_status = 0;
   std::vector<int32_t> last_info;   // per supernode: first zero pivot (block position) or INT32_MAX
   // batched systems analyzed as one block-diagonal matrix
@@ -182,6 +198,7 @@ struct mfgpu_ctx {
   // CUDA graphs of the static launch sequences (keyed by everything a replay
   // bakes in: sizes, flags and buffer addresses)
   bool use_graphs = true;
+  bool solve_graphs = true;   // false once a capture of the persistent solve failed
   std::vector<uintptr_t> factor_key, solve_key;
   cudaGraphExec_t factor_exec = nullptr, solve_exec = nullptr;
   int64_t factor_nodes = 0, solve_nodes = 0;   // kernel launches inside each graph
@@ -238,6 +255,10 @@ void upload_plan(mfgpu_ctx* h) {
   upload(h->b_csr_col, P.csr_col, st);
   upload(h->b_csr_src, P.csr_src, st);
   upload(h->b_dinv_off, P.dinv_off, st);
+  upload(h->b_inv_off, P.inv_off, st);
+  upload(h->b_inv_blocks, P.inv_blocks, st);
+  upload(h->b_inv_tasks, P.inv_tasks, st);
+  upload(h->b_inv_tasks_tc, P.inv_tasks_tc, st);
   DevPlan& d = h->dp;
   d.n = P.n;
   d.ns = P.ns;
@@ -268,6 +289,7 @@ void upload_plan(mfgpu_ctx* h) {
   d.csr_col = h->b_csr_col.as<int32_t>();
   d.csr_src = h->b_csr_src.as<int32_t>();
   d.dinv_off = h->b_dinv_off.as<int64_t>();
+  d.inv_off = h->b_inv_off.as<int64_t>();
 }
 
 void upload_launches(mfgpu_ctx* h) {
@@ -315,7 +337,41 @@ void klaunch(mfgpu_ctx* h, int kc, double flops, double bytes, F&& f, int32_t le
   h->pending.push_back({kc, a, b, flops, bytes, level, tasks});
 }
 
+void prof_flush(mfgpu_ctx* h);
+
+// Kernel class of a solve step / persistent phase kind.
+int phase_class(int kind) {
+  static const int kc[6] = {KC_FWD_SMALL, KC_FWD_ASSEMBLE, KC_FWD_SMALL, KC_GEMM_SOLVE, KC_BWD_SMALL,
+                            KC_BWD_GATHER};
+  return kc[kind];
+}
+
+void prof_book(mfgpu_ctx* h, int kc, float ms, double flops, double bytes, int32_t level, int64_t tasks) {
+  KStat& k = h->kstat[kc];
+  k.ms += ms;
+  k.flops += flops;
+  k.bytes += bytes;
+  ++k.launches;
+  if (h->records.size() < 200000) h->records.push_back({kc, level, tasks, ms, flops, bytes});
+}
+
 void prof_flush(mfgpu_ctx* h) {
+  if (!h->pending_phases.empty()) {
+    // persistent solves: phase p ran between stamps p and p + 1 (block 0, after each grid barrier)
+    std::vector<unsigned long long> stamps(h->stamp_next);
+    CK(cudaMemcpy(stamps.data(), h->b_stamps.p, h->stamp_next * 8, cudaMemcpyDeviceToHost));
+    const auto& S = h->sched;
+    for (const auto& pp : h->pending_phases)
+      for (int p = 0; p < pp.nphases && p < (int)S.steps.size(); ++p) {
+        const auto& st = S.steps[p];
+        const float ms = (float)((double)(stamps[pp.stamp0 + p + 1] - stamps[pp.stamp0 + p]) * 1e-6);
+        const bool work = st.kind != kPhFwdAssemble && st.kind != kPhBwdGather;
+        prof_book(h, phase_class(st.kind), ms, work ? st.flops : 0.0, work ? st.elems * pp.elem_bytes : 0.0, -2,
+                  S.phases[p].items);
+      }
+    h->pending_phases.clear();
+    h->stamp_next = 0;
+  }
   for (auto& p : h->pending) {
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, p.a, p.b));
@@ -354,10 +410,10 @@ void configure_kernels() {
   CK(cudaFuncSetAttribute(k_panel<T, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_smem_bytes<T>(128)));
   CK(cudaFuncSetAttribute(k_panel<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_smem_bytes<T>(256)));
   CK(cudaFuncSetAttribute(k_panel_apply<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem_bytes<T>()));
-  CK(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem_bytes<T>()));
-  CK(cudaFuncSetAttribute(k_bwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem_bytes<T>()));
   CK(cudaFuncSetAttribute(k_gemm_tc<128, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)TcCfg<128, 3>::kSmem));
+  CK(cudaFuncSetAttribute(k_solve_persistent<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)persistent_smem_bytes<T>()));
   done = true;
 }
 
@@ -477,6 +533,35 @@ void run_sequence(mfgpu_ctx* h, std::vector<uintptr_t>& cached_key, cudaGraphExe
   ++h->graph_replays;
 }
 
+// Explicit inverses of the large pivot blocks for the solves: clear, copy
+// the inverted 64 x 64 diagonal blocks, then the merge levels (plan.cpp:
+// build_inverse_steps), each a batched GEMM launch.
+template <typename T>
+void issue_inverses(mfgpu_ctx* h) {
+  const Plan& P = h->plan;
+  cudaStream_t st = h->stream;
+  if (!P.inv_elems) return;
+  T* pool = h->b_pool.as<T>();
+  CK(cudaMemsetAsync(pool + P.inv_base, 0, P.inv_elems * sizeof(T), st));
+  const int64_t nblk = (int64_t)P.inv_blocks.size() / 2;
+  klaunch(h, KC_INVERSE, 0, (double)nblk * 2 * 64 * 64 * sizeof(T) * 2, [&] {
+    k_inv_init<T><<<(unsigned)nblk, 256, 0, st>>>(h->dp, h->b_inv_blocks.as<int32_t>(), h->b_dinv.as<T>(), pool);
+  });
+  for (const InvStep& is : P.inv_steps) {
+    if (!is.count) continue;
+    if (sizeof(T) == 4 && h->use_tc)
+      klaunch(h, KC_INVERSE, is.flops, is.elems * sizeof(T), [&] {
+        k_gemm_tc<128, 3><<<(unsigned)is.tiles_tc, kTcThreads, TcCfg<128, 3>::kSmem, st>>>(
+            h->b_inv_tasks_tc.as<GemmTask>() + is.first, (int)is.count, (const float*)pool, (const float*)pool,
+            (float*)pool, h->b_flags.as<int>());
+      }, -3, is.tiles_tc);
+    else
+      klaunch(h, KC_INVERSE, is.flops, is.elems * sizeof(T), [&] {
+        launch_gemm<T>(h->b_inv_tasks.as<GemmTask>() + is.first, is.count, is.tiles, pool, pool, pool, st);
+      }, -3, is.tiles);
+  }
+}
+
 template <typename T>
 void issue_factor(mfgpu_ctx* h) {
   const Plan& P = h->plan;
@@ -490,6 +575,7 @@ void issue_factor(mfgpu_ctx* h) {
   if (P.ns) k_fill_i32<<<grid1(P.ns, 256), 256, 0, st>>>(h->b_info.as<int32_t>(), P.ns, INT32_MAX);
   CK(cudaMemsetAsync(h->b_flags.p, 0, 16, st));
   run_factor_launches<T>(h);
+  issue_inverses<T>(h);
   if (P.ns)
     klaunch(h, KC_PIVOTS, 0, 16.0 * P.n, [&] { k_finalize_pivots<<<grid1(P.ns, 128), 128, 0, st>>>(h->dp, dev_state(h)); });
   if (P.fc_total)
@@ -506,7 +592,7 @@ int factor_impl(mfgpu_ctx* h, int32_t check) {
   Plan& P = h->plan;
   cudaStream_t st = h->stream;
   configure_kernels<T>();
-  h->b_pool.ensure(std::max<size_t>(P.front_elems * sizeof(T), 16));
+  h->b_pool.ensure(std::max<size_t>(P.pool_elems * sizeof(T), 16));
   h->b_ipiv.ensure(std::max<int64_t>(P.n, 1) * 4);
   h->b_prow.ensure(std::max<int64_t>(P.n, 1) * 4);
   h->b_rowfac.ensure(std::max<int64_t>(P.n, 1) * 4);
@@ -573,9 +659,45 @@ int factor_impl(mfgpu_ctx* h, int32_t check) {
   return status;
 }
 
+// Element growth max|U| / max|Rs .* A| of the last factorization (FP64 on
+// the GPU over the CSC values of U and the scaled values of V = A[qf, qf]).
+double element_growth(mfgpu_ctx* h) {
+  const Plan& P = h->plan;
+  cudaStream_t st = h->stream;
+  h->b_norm.ensure(16);
+  unsigned long long* m = h->b_norm.as<unsigned long long>();
+  CK(cudaMemsetAsync(m, 0, 16, st));
+  k_abs_max<<<4 * 148, 256, 0, st>>>(h->b_ux.as<double>(), P.nnz_u, m);
+  k_abs_max<<<4 * 148, 256, 0, st>>>(h->b_vx.as<double>(), P.nnz_a, m + 1);
+  CK(cudaGetLastError());
+  unsigned long long bits[2];
+  CK(cudaMemcpyAsync(bits, m, 16, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  double u, a;
+  std::memcpy(&u, &bits[0], 8);
+  std::memcpy(&a, &bits[1], 8);
+  return a > 0 ? u / a : 0.0;
+}
+
+// The mixed form factors in FP32, then checks the element growth: when it
+// exceeds the limit (FP32 rounding amplified by the growth would keep the FP64
+// refinement from converging), the matrix is refactored in FP64 and the
+// solves use the FP64 factors.
 int factor_dispatch(mfgpu_ctx* h, int32_t check) {
-  if (h->precision == MFGPU_PRECISION_MIXED) return factor_impl<float>(h, check);
-  return factor_impl<double>(h, check);
+  h->refactored_fp64 = false;
+  h->growth = 0.0;
+  if (h->precision != MFGPU_PRECISION_MIXED) return factor_impl<double>(h, check);
+  const int rc = factor_impl<float>(h, check);
+  if (rc != MFGPU_OK) return rc;
+  h->growth = element_growth(h);
+  if (!(h->growth <= h->growth_limit)) {
+    const double g = h->growth;
+    const int rc64 = factor_impl<double>(h, check);
+    h->growth = g;
+    h->refactored_fp64 = true;
+    return rc64;
+  }
+  return rc;
 }
 
 // ---- solves ---------------------------------------------------------------
@@ -586,21 +708,36 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
   S = SolveSchedule{};
   S.nrhs = R;
   auto ceil_div = [](int64_t a, int64_t b) { return (a + b - 1) / b; };
-  double work_flops = 0, work_elems = 0;
-  auto add_gemm = [&](std::vector<GemmTask>& v, int64_t& tiles, int64_t a, int64_t b, int64_t c, int m, int n, int k,
-                      int lda, int ldb, int ldc) {
-    if (m <= 0 || n <= 0 || k <= 0) return;
+  // offsets: A operands in the front pool (fronts and pivot-block inverses);
+  // B, C and D in the solve arena: the per-supernode blocks (nf x R each,
+  // at colbase * R), then x in factor order (n x R) at xw0
+  const int64_t xw0 = P.fc_total * R;
+  const int n = (int)P.n;
+  auto add_gemm = [&](SolveSchedule::Step& st, int32_t mode, int64_t a, int lda, int64_t b, int ldb, int64_t c,
+                      int ldc, int m, int nn, int k, int64_t d = 0, int ldd = 0) {
+    if (m <= 0 || nn <= 0 || k < 0 || (k == 0 && mode == kGemmSub)) return;
     GemmTask g{};
-    g.a = a; g.b = b; g.c = c;
-    g.m = m; g.n = n; g.k = k;
-    g.lda = lda; g.ldb = ldb; g.ldc = ldc;
+    g.a = a; g.b = b; g.c = c; g.d = d;
+    g.m = m; g.n = nn; g.k = k;
+    g.lda = lda; g.ldb = ldb; g.ldc = ldc; g.ldd = ldd;
+    g.mode = mode;
     g.tiles_m = (int)ceil_div(m, 64);
-    g.tiles_n = (int)ceil_div(n, 64);
-    g.tile_base = tiles;
-    tiles += (int64_t)g.tiles_m * g.tiles_n;
-    v.push_back(g);
-    work_flops += 2.0 * m * n * k;
-    work_elems += 2.0 * m * n + (double)m * k + (double)k * n;
+    g.tiles_n = (int)ceil_div(nn, 64);
+    g.tile_base = st.tiles;
+    st.tiles += (int64_t)g.tiles_m * g.tiles_n;
+    S.gemms.push_back(g);
+    g.tiles_m = (int)ceil_div(m, kTcTile);
+    g.tiles_n = (int)ceil_div(nn, kTcTile);
+    g.tile_base = st.tiles_tc;
+    st.tiles_tc += (int64_t)g.tiles_m * g.tiles_n;
+    S.gemms_tc.push_back(g);
+    ++st.count;
+    st.flops += 2.0 * m * nn * k;
+    st.elems += (double)m * nn * (mode == kGemmSet ? 1 : 2) + (double)m * k + (double)k * nn;
+  };
+  auto gemm_step = [&]() { return SolveSchedule::Step{3, (int64_t)S.gemms.size(), 0, 0}; };
+  auto push = [&](const SolveSchedule::Step& st) {
+    if (st.count) S.steps.push_back(st);
   };
   // small-supernode kernels: L or U panel read once, the rhs block read and written
   auto small_work = [&](SolveSchedule::Step& st, int32_t s) {
@@ -621,50 +758,24 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
     }
     if (e > m) {
       const int64_t first = (int64_t)S.ids.size();
-      int32_t maxnp = 0;
-      for (int32_t i = m; i < e; ++i) {
-        S.ids.push_back(P.slot_super[i]);
-        maxnp = std::max(maxnp, P.np[P.slot_super[i]]);
-      }
+      for (int32_t i = m; i < e; ++i) S.ids.push_back(P.slot_super[i]);
       S.steps.push_back({1, first, e - m, 0});
-      for (int32_t k0 = 0; k0 < maxnp; k0 += kPanel) {
-        SolveSchedule::Step d{2, (int64_t)S.blocks.size(), 0, 0};
-        SolveSchedule::Step g{3, (int64_t)S.gemms.size(), 0, 0};
-        work_flops = work_elems = 0;
-        for (int32_t i = m; i < e; ++i) {
-          const int32_t s = P.slot_super[i];
-          if (P.np[s] <= k0) continue;
-          const int k1 = std::min(k0 + kPanel, P.np[s]);
-          S.blocks.push_back({s, k0});
-          ++d.count;
-          d.flops += (double)(k1 - k0) * (k1 - k0) * R;
-          d.elems += (double)(k1 - k0) * (k1 - k0) + 2.0 * (k1 - k0) * R;
-          const int64_t fb = P.colbase[s] * R;
-          const int nf = P.nf[s];
-          // rows of the pivot block below this block; the update rows are
-          // done once, after the whole pivot block (K = np)
-          add_gemm(S.gemms, g.tiles, P.front_off[s] + k1 + (int64_t)k0 * nf, fb + k0, fb + k1, P.np[s] - k1,
-                   (int)R, k1 - k0, nf, nf, nf);
-        }
-        g.count = (int64_t)S.gemms.size() - g.first;
-        g.flops = work_flops;
-        g.elems = work_elems;
-        if (d.count) S.steps.push_back(d);
-        if (g.count) S.steps.push_back(g);
-      }
-      // w = f[np:] - L21 * y for every large supernode of the level
-      SolveSchedule::Step g{3, (int64_t)S.gemms.size(), 0, 0};
-      work_flops = work_elems = 0;
+      // y = inv(L11) f[0:np], into x's rows c1.. ; then w = f[np:] - L21 y
+      SolveSchedule::Step gy = gemm_step();
       for (int32_t i = m; i < e; ++i) {
         const int32_t s = P.slot_super[i];
         const int nf = P.nf[s], np = P.np[s];
-        const int64_t fb = P.colbase[s] * R;
-        add_gemm(S.gemms, g.tiles, P.front_off[s] + np, fb, fb + np, P.nu[s], (int)R, np, nf, nf, nf);
+        add_gemm(gy, kGemmSet, P.inv_off[s], np, P.colbase[s] * R, nf, xw0 + P.c1[s], n, np, (int)R, np);
       }
-      g.count = (int64_t)S.gemms.size() - g.first;
-      g.flops = work_flops;
-      g.elems = work_elems;
-      if (g.count) S.steps.push_back(g);
+      push(gy);
+      SolveSchedule::Step gw = gemm_step();
+      for (int32_t i = m; i < e; ++i) {
+        const int32_t s = P.slot_super[i];
+        const int nf = P.nf[s], np = P.np[s];
+        add_gemm(gw, kGemmSub, P.front_off[s] + np, nf, xw0 + P.c1[s], n, P.colbase[s] * R + np, nf, P.nu[s],
+                 (int)R, np);
+      }
+      push(gw);
     }
   }
   // backward, root to leaves
@@ -672,47 +783,25 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
     const int32_t a = P.level_slot[L], m = P.level_large[L], e = P.level_slot[L + 1];
     if (e > m) {
       const int64_t first = (int64_t)S.ids.size();
-      int32_t maxblocks = 0;
-      for (int32_t i = m; i < e; ++i) {
-        S.ids.push_back(P.slot_super[i]);
-        maxblocks = std::max<int32_t>(maxblocks, (int32_t)ceil_div(P.np[P.slot_super[i]], kPanel));
-      }
+      for (int32_t i = m; i < e; ++i) S.ids.push_back(P.slot_super[i]);
       S.steps.push_back({5, first, e - m, 0});
-      SolveSchedule::Step g{3, (int64_t)S.gemms.size(), 0, 0};
-      work_flops = work_elems = 0;
+      // g = y - U12 x[upd] into f[0:np]; then x = inv(U11) g into x's rows c1..
+      SolveSchedule::Step gg = gemm_step();
       for (int32_t i = m; i < e; ++i) {
         const int32_t s = P.slot_super[i];
         const int nf = P.nf[s], np = P.np[s];
-        const int64_t fb = P.colbase[s] * R;
-        add_gemm(S.gemms, g.tiles, P.front_off[s] + (int64_t)np * nf, fb + np, fb, np, (int)R, P.nu[s], nf, nf, nf);
+        add_gemm(gg, kGemmFrom, P.front_off[s] + (int64_t)np * nf, nf, P.colbase[s] * R + np, nf,
+                 P.colbase[s] * R, nf, np, (int)R, P.nu[s], xw0 + P.c1[s], n);
       }
-      g.count = (int64_t)S.gemms.size() - g.first;
-      g.flops = work_flops;
-      g.elems = work_elems;
-      if (g.count) S.steps.push_back(g);
-      for (int32_t bi = maxblocks - 1; bi >= 0; --bi) {
-        SolveSchedule::Step d{6, (int64_t)S.blocks.size(), 0, 0};
-        SolveSchedule::Step gg{3, (int64_t)S.gemms.size(), 0, 0};
-        work_flops = work_elems = 0;
-        for (int32_t i = m; i < e; ++i) {
-          const int32_t s = P.slot_super[i];
-          if (ceil_div(P.np[s], kPanel) <= bi) continue;
-          const int k0 = bi * kPanel, k1 = std::min(k0 + kPanel, P.np[s]);
-          S.blocks.push_back({s, k0});
-          ++d.count;
-          d.flops += (double)(k1 - k0) * (k1 - k0) * R;
-          d.elems += (double)(k1 - k0) * (k1 - k0) + 2.0 * (k1 - k0) * R;
-          const int64_t fb = P.colbase[s] * R;
-          const int nf = P.nf[s];
-          add_gemm(S.gemms, gg.tiles, P.front_off[s] + (int64_t)k0 * nf, fb + k0, fb, k0, (int)R, k1 - k0, nf, nf,
-                   nf);
-        }
-        gg.count = (int64_t)S.gemms.size() - gg.first;
-        gg.flops = work_flops;
-        gg.elems = work_elems;
-        if (d.count) S.steps.push_back(d);
-        if (gg.count) S.steps.push_back(gg);
+      push(gg);
+      SolveSchedule::Step gx = gemm_step();
+      for (int32_t i = m; i < e; ++i) {
+        const int32_t s = P.slot_super[i];
+        const int nf = P.nf[s], np = P.np[s];
+        add_gemm(gx, kGemmSet, P.inv_off[s] + (int64_t)np * np, np, P.colbase[s] * R, nf, xw0 + P.c1[s], n, np,
+                 (int)R, np);
       }
+      push(gx);
     }
     if (m > a) {
       SolveSchedule::Step st{4, (int64_t)S.ids.size(), m - a, 0};
@@ -723,9 +812,23 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
       S.steps.push_back(st);
     }
   }
+  // the same steps as phases of the persistent kernel (kSolveThreads per CTA:
+  // kSolveThreads / 32 right-hand sides per gather item)
+  const int64_t ych = ceil_div(R, kSolveCols), wch = ceil_div(R, kSolveThreads / 32);
+  for (const auto& st : S.steps) {
+    SolvePhase ph{st.kind, 1, st.first, st.count, 0};
+    switch (st.kind) {
+      case kPhFwdSmall: case kPhBwdSmall: ph.rows = (int32_t)ych; break;
+      case kPhFwdAssemble: case kPhBwdGather: ph.rows = (int32_t)wch; break;
+      default: break;
+    }
+    ph.items = st.kind == kPhGemm ? st.tiles : st.count * ph.rows;
+    S.phases.push_back(ph);
+  }
   upload(S.d_ids, S.ids, h->stream);
-  upload(S.d_blocks, S.blocks, h->stream);
   upload(S.d_gemms, S.gemms, h->stream);
+  upload(S.d_gemms_tc, S.gemms_tc, h->stream);
+  upload(S.d_phases, S.phases, h->stream);
 }
 
 // One solve A x = b for device b (ldb) into device x (ldx) (x overwritten, or
@@ -734,10 +837,22 @@ template <typename T>
 void prepare_solve(mfgpu_ctx* h, int64_t R, int refine) {
   const Plan& P = h->plan;
   build_solve_schedule(h, R);
-  h->b_fsol.ensure(std::max<size_t>((size_t)P.fc_total * R * sizeof(T), 16));
-  h->b_xw.ensure(std::max<size_t>((size_t)P.n * R * sizeof(T), 16));
+  // solve arena: the per-supernode blocks, then x in factor order
+  h->b_fsol.ensure(std::max<size_t>((size_t)(P.fc_total + P.n) * R * sizeof(T), 16));
   if (refine > 0) h->b_r.ensure(std::max<size_t>((size_t)P.n * R * 8, 16));
   configure_kernels<T>();
+  if (h->persistent) {
+    h->b_bar.ensure(16);
+    if (h->profiling) h->b_stamps.ensure((h->sched.phases.size() + 1) * (size_t)(refine + 1) * 8);
+    int& grid = h->persist_grid[sizeof(T) == 8];
+    if (!grid) {
+      int per_sm = 0, sms = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_persistent<T>, kSolveThreads,
+                                                       persistent_smem_bytes<T>()));
+      CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+      grid = std::max(1, per_sm) * sms;
+    }
+  }
 }
 
 template <typename T>
@@ -748,15 +863,36 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
   SolveSchedule& S = h->sched;
   T* pool = h->b_pool.as<T>();
   T* fsol = h->b_fsol.as<T>();
-  T* xw = h->b_xw.as<T>();
+  T* xw = fsol + P.fc_total * R;
   DevState DS = dev_state(h);
   SolveArgs A{R, d_b, ldb, (use_rs && h->have_rs) ? h->b_rs.as<double>() : nullptr, P.n};
   const unsigned ychunks = (unsigned)((R + kSolveCols - 1) / kSolveCols);
   const unsigned wchunks = (unsigned)((R + 7) / 8);
-  const unsigned tchunks = (unsigned)((R + 63) / 64);
   const int32_t* ids = S.d_ids.as<int32_t>();
-  const SolveBlockTask* blocks = S.d_blocks.as<SolveBlockTask>();
   const GemmTask* gemms = S.d_gemms.as<GemmTask>();
+  if (h->persistent && !S.phases.empty()) {
+    unsigned int* bar = h->b_bar.as<unsigned int>();
+    PersistentArgs X{S.d_phases.as<SolvePhase>(), (int32_t)S.phases.size(), ids, gemms,
+                     GridBarrier{bar, bar + 1, reinterpret_cast<int*>(bar + 2)}, nullptr};
+    if (h->profiling) {
+      X.stamps = h->b_stamps.as<unsigned long long>() + h->stamp_next;
+      h->pending_phases.push_back({h->stamp_next, (int)S.phases.size(), (int)sizeof(T)});
+      h->stamp_next += S.phases.size() + 1;
+    }
+    CK(cudaMemsetAsync(bar, 0, 3 * sizeof(unsigned int), st));
+    ++h->launch_count;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)h->persist_grid[sizeof(T) == 8]);
+    cfg.blockDim = dim3(kSolveThreads);
+    cfg.dynamicSmemBytes = persistent_smem_bytes<T>();
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, k_solve_persistent<T>, h->dp, DS, A, X, (const T*)pool, fsol, xw));
+  } else
   for (const auto& s : S.steps) {
     const double bytes = s.elems * sizeof(T);
     switch (s.kind) {
@@ -771,16 +907,17 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
           k_fwd_assemble<T><<<dim3((unsigned)s.count, wchunks), 256, 0, st>>>(h->dp, DS, A, ids + s.first, fsol);
         });
         break;
-      case 2:
-        klaunch(h, KC_FWD_DIAG, s.flops, bytes, [&] {
-          k_fwd_diag<T><<<dim3((unsigned)s.count, tchunks), kApplyThreads, apply_smem_bytes<T>(), st>>>(
-              h->dp, blocks + s.first, R, h->b_dinv.as<T>(), fsol);
-        });
-        break;
       case 3:
-        klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
-          launch_gemm<T>(gemms + s.first, s.count, s.tiles, pool, fsol, fsol, st);
-        });
+        if (sizeof(T) == 4 && h->use_tc && R >= 64)
+          klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
+            k_gemm_tc<128, 3><<<(unsigned)s.tiles_tc, kTcThreads, TcCfg<128, 3>::kSmem, st>>>(
+                S.d_gemms_tc.as<GemmTask>() + s.first, (int)s.count, (const float*)pool, (const float*)fsol,
+                (float*)fsol, h->b_flags.as<int>());
+          });
+        else
+          klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
+            launch_gemm<T>(gemms + s.first, s.count, s.tiles, pool, fsol, fsol, st);
+          });
         break;
       case 4:
         klaunch(h, KC_BWD_SMALL, s.flops, bytes, [&] {
@@ -791,12 +928,6 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
       case 5:
         klaunch(h, KC_BWD_GATHER, 0, 0, [&] {
           k_bwd_gather<T><<<dim3((unsigned)s.count, wchunks), 256, 0, st>>>(h->dp, A, ids + s.first, fsol, xw);
-        });
-        break;
-      case 6:
-        klaunch(h, KC_BWD_DIAG, s.flops, bytes, [&] {
-          k_bwd_diag<T><<<dim3((unsigned)s.count, tchunks), kApplyThreads, apply_smem_bytes<T>(), st>>>(
-              h->dp, blocks + s.first, R, P.n, h->b_dinv.as<T>(), fsol, xw);
         });
         break;
     }
@@ -813,6 +944,7 @@ void solve_refine(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, doubl
                   bool use_rs) {
   const Plan& P = h->plan;
   cudaStream_t st = h->stream;
+  if (h->persistent) CK(cudaMemsetAsync(h->b_bar.as<unsigned int>() + 3, 0, sizeof(unsigned int), st));
   solve_once<T>(h, R, d_b, ldb, d_x, ldx, use_rs, 0);
   if (refine > 0) {
     double* r = h->b_r.as<double>();
@@ -835,11 +967,37 @@ void solve_graph(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double
   const std::vector<uintptr_t> key = {
       sizeof(T), (uintptr_t)R, (uintptr_t)d_b, (uintptr_t)ldb, (uintptr_t)d_x, (uintptr_t)ldx, (uintptr_t)refine,
       (uintptr_t)h->have_rs, (uintptr_t)h->b_rs.p, (uintptr_t)h->b_pool.p, (uintptr_t)h->b_dinv.p,
-      (uintptr_t)h->b_fsol.p, (uintptr_t)h->b_xw.p, (uintptr_t)h->b_r.p, (uintptr_t)h->b_ax.p,
-      (uintptr_t)S.d_ids.p, (uintptr_t)S.d_blocks.p, (uintptr_t)S.d_gemms.p, (uintptr_t)h->b_prow.p,
+      (uintptr_t)h->b_fsol.p, (uintptr_t)h->b_inv_tasks.p, (uintptr_t)h->b_r.p, (uintptr_t)h->b_ax.p,
+      (uintptr_t)S.d_ids.p, (uintptr_t)S.d_gemms.p, (uintptr_t)S.d_phases.p, (uintptr_t)h->b_prow.p,
+      (uintptr_t)S.d_gemms_tc.p, (uintptr_t)h->use_tc,
       (uintptr_t)h->b_rowfac.p, (uintptr_t)h->stream};
-  run_sequence(h, h->solve_key, h->solve_exec, h->solve_nodes, key,
-               [&] { solve_refine<T>(h, R, d_b, ldb, d_x, ldx, refine, true); });
+  if (!h->solve_graphs) {
+    solve_refine<T>(h, R, d_b, ldb, d_x, ldx, refine, true);
+    return;
+  }
+  try {
+    run_sequence(h, h->solve_key, h->solve_exec, h->solve_nodes, key,
+                 [&] { solve_refine<T>(h, R, d_b, ldb, d_x, ldx, refine, true); });
+  } catch (const CudaError&) {
+    if (!h->persistent || h->solve_exec) throw;
+    // the capture of the cooperative launch failed: solve without a graph
+    cudaGetLastError();
+    h->solve_graphs = false;
+    solve_refine<T>(h, R, d_b, ldb, d_x, ldx, refine, true);
+  }
+}
+
+// After a synchronised solve: MFGPU_ERR_TIMEOUT when a grid barrier of a
+// persistent pass gave up (the solution is then incomplete).
+int solve_status(mfgpu_ctx* h) {
+  int flags[2] = {0, 0};
+  if (h->b_flags.p) CK(cudaMemcpy(flags, h->b_flags.p, sizeof flags, cudaMemcpyDeviceToHost));
+  if (flags[1]) return fail(h, MFGPU_ERR_TIMEOUT, "a tensor-core GEMM gave up a bounded wait");
+  if (!h->persistent || !h->b_bar.p) return MFGPU_OK;
+  int sticky = 0;
+  CK(cudaMemcpy(&sticky, h->b_bar.as<unsigned int>() + 3, sizeof sticky, cudaMemcpyDeviceToHost));
+  if (sticky) return fail(h, MFGPU_ERR_TIMEOUT, "a grid barrier of the persistent solve gave up a bounded wait");
+  return MFGPU_OK;
 }
 
 void solve_dispatch(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double* d_x, int64_t ldx, int refine) {
@@ -891,6 +1049,7 @@ int mfgpu_create(const mfgpu_options* opts, mfgpu_ctx** out) {
     h->device = opts->device;
     h->precision = opts->precision;
     h->use_tc = !(opts->flags & MFGPU_FLAG_NO_TENSOR_CORES);
+    h->persistent = (opts->flags & MFGPU_FLAG_PERSISTENT_SOLVE) != 0;
   }
   int rc = guarded(h, [&]() -> int {
     int ndev = 0;
@@ -926,9 +1085,11 @@ void mfgpu_destroy(mfgpu_ctx* h) {
                     &h->b_lcolptr, &h->b_ucolptr, &h->b_qf, &h->b_csr_ptr, &h->b_csr_col, &h->b_csr_src,
                     &h->b_small, &h->b_panel, &h->b_trsm, &h->b_gemm, &h->b_gemm_tc, &h->b_pool, &h->b_vx, &h->b_ax, &h->b_rs,
                     &h->b_ipiv, &h->b_info, &h->b_prow, &h->b_rowfac, &h->b_flags, &h->b_dinv, &h->b_dinv_off,
+                    &h->b_inv_off, &h->b_inv_blocks, &h->b_inv_tasks, &h->b_inv_tasks_tc,
                     &h->b_li, &h->b_lx, &h->b_ui,
-                    &h->b_ux, &h->b_fsol, &h->b_xw, &h->b_b, &h->b_x, &h->b_r, &h->b_d, &h->b_err, &h->b_norm,
-                    &h->sched.d_ids, &h->sched.d_blocks, &h->sched.d_gemms};
+                    &h->b_ux, &h->b_fsol, &h->b_b, &h->b_x, &h->b_r, &h->b_d, &h->b_err, &h->b_norm,
+                    &h->sched.d_ids, &h->sched.d_gemms, &h->sched.d_gemms_tc, &h->sched.d_phases, &h->b_bar,
+                    &h->b_stamps};
   for (DevBuf* b : bufs) b->release();
   if (h->factor_exec) cudaGraphExecDestroy(h->factor_exec);
   if (h->solve_exec) cudaGraphExecDestroy(h->solve_exec);
@@ -944,6 +1105,12 @@ const char* mfgpu_last_error(const mfgpu_ctx* h) { return h ? h->err.c_str() : "
 int mfgpu_set_stream(mfgpu_ctx* h, void* s) {
   if (!h) return MFGPU_ERR_ARGUMENT;
   h->stream = s ? (cudaStream_t)s : h->own_stream;
+  return MFGPU_OK;
+}
+
+int mfgpu_set_growth_limit(mfgpu_ctx* h, double limit) {
+  if (!h || !(limit > 0)) return MFGPU_ERR_ARGUMENT;
+  h->growth_limit = limit;
   return MFGPU_OK;
 }
 
@@ -1083,7 +1250,7 @@ int mfgpu_solve_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ld
     CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     h->t_solve_ms = ms;
     prof_flush(h);
-    return MFGPU_OK;
+    return solve_status(h);
   });
 }
 
@@ -1104,7 +1271,7 @@ int mfgpu_solve(mfgpu_ctx* h, int64_t nrhs, const double* b, int64_t ldb, double
     CK(cudaMemcpy2DAsync(x, ldx * 8, h->b_x.p, n * 8, n * 8, nrhs, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     prof_flush(h);
-    return MFGPU_OK;
+    return solve_status(h);
   });
 }
 
@@ -1165,12 +1332,14 @@ int mfgpu_stats_json(mfgpu_ctx* h, char* buf, int64_t cap) {
                 "\"flops_getrf\": %.6e, \"flops_trsm\": %.6e, \"flops_gemm\": %.6e, \"assembly_elem_moves\": %.6e, "
                 "\"factor_launches\": %lld, \"small_fronts\": %lld, \"speculative\": %s, \"safe_rerun\": %d, "
                 "\"analyze_ms\": %.3f, \"factor_ms\": %.3f, \"solve_ms\": %.3f, \"precision\": \"%s\", "
-                "\"status\": %d}",
+                "\"status\": %d, \"growth\": %.6e, \"growth_limit\": %.6e, \"refactored_fp64\": %s, "
+                "\"flops_inverse\": %.6e}",
                 (long long)P.n, (long long)P.ns, P.nlevels, (long long)P.nnz_l, (long long)P.nnz_u, P.max_nf,
                 P.max_np, (long long)P.front_elems, P.flops, P.flops_getrf, P.flops_trsm, P.flops_gemm,
                 P.assembly_bytes_per_elem, (long long)nl, (long long)nsmall, P.has_speculative ? "true" : "false",
                 h->factor_reruns, h->t_analyze_ms, h->t_factor_ms, h->t_solve_ms,
-                h->factor_precision == MFGPU_PRECISION_MIXED ? "mixed" : "fp64", h->last_status);
+                h->factor_precision == MFGPU_PRECISION_MIXED ? "mixed" : "fp64", h->last_status, h->growth,
+                h->growth_limit, h->refactored_fp64 ? "true" : "false", P.flops_inverse);
   std::string js(tmp);
   js.pop_back();   // reopen the object
   char item[512];
@@ -1218,6 +1387,8 @@ int mfgpu_set_profiling(mfgpu_ctx* h, int32_t on) {
   h->launch_count = 0;
   for (auto& k : h->kstat) k = KStat{};
   h->pending.clear();
+  h->pending_phases.clear();
+  h->stamp_next = 0;
   h->evnext = 0;
   return MFGPU_OK;
 }

@@ -12,6 +12,91 @@ namespace {
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 }  // namespace
 
+namespace {
+// Record C = f(C, A * B) in both tilings (see push_gemm) into the inverse lists.
+void push_inv(Plan& P, InvStep& st, GemmTask g) {
+  g.tiles_m = (int32_t)ceil_div(g.m, 64);
+  g.tiles_n = (int32_t)ceil_div(g.n, 64);
+  g.tile_base = st.tiles;
+  st.tiles += (int64_t)g.tiles_m * g.tiles_n;
+  P.inv_tasks.push_back(g);
+  g.tiles_m = (int32_t)ceil_div(g.m, kTcTile);
+  g.tiles_n = (int32_t)ceil_div(g.n, kTcTile);
+  g.tile_base = st.tiles_tc;
+  st.tiles_tc += (int64_t)g.tiles_m * g.tiles_n;
+  P.inv_tasks_tc.push_back(g);
+  ++st.count;
+  st.flops += 2.0 * g.m * g.n * g.k;
+  st.elems += (double)g.m * g.n * (g.mode == kGemmSub || g.mode == kGemmFrom ? 2 : 1) + (double)g.m * g.k +
+              (double)g.k * g.n;
+}
+
+// Blocked inversion of every large pivot block.  With the pivot block split
+// into consecutive blocks of s rows, a merge of [A 0; B C] (unit lower) is
+//   inv = [inv(A) 0; -inv(C) B inv(A)  inv(C)]
+// and of [A B; 0 C] (upper)
+//   inv = [inv(A) -inv(A) B inv(C); 0 inv(C)];
+// merge level s = 64, 128, ... pairs blocks (i, i + s) of size s and
+// min(s, np - i - s): first T = B inv(A) (L) and T' = B inv(C) (U) into the
+// scratch, then the off-diagonal block of the inverse = -(inv(C) T) and
+// -(inv(A) T').
+void build_inverse_steps(Plan& P) {
+  int32_t max_np = 0;
+  for (int64_t s = 0; s < P.ns; ++s)
+    if (P.inv_off[s] >= 0) max_np = std::max(max_np, P.np[s]);
+  for (int64_t bs = kPanel; bs < max_np; bs *= 2) {
+    InvStep t1{(int64_t)P.inv_tasks.size(), 0, 0, 0, 0, 0};
+    std::vector<GemmTask> second;
+    int64_t scratch = 0;
+    for (int64_t s = 0; s < P.ns; ++s) {
+      if (P.inv_off[s] < 0 || P.np[s] <= bs) continue;
+      const int32_t npv = P.np[s], nf = P.nf[s];
+      const int64_t fo = P.front_off[s], li = P.inv_off[s], ui = li + (int64_t)npv * npv;
+      for (int64_t i = 0; i + bs < npv; i += 2 * bs) {
+        const int32_t n1 = (int32_t)bs, n2 = (int32_t)std::min<int64_t>(bs, npv - i - bs);
+        const int64_t i2 = i + bs;
+        const int64_t tl = P.inv_scratch + scratch, tu = tl + (int64_t)n2 * n1;
+        scratch += 2 * (int64_t)n1 * n2;
+        GemmTask g{};
+        // L: T = L[i2:, i:i2] * inv(A)   (n2 x n1)
+        g.a = fo + i2 + i * nf; g.lda = nf;
+        g.b = li + i + i * npv; g.ldb = npv;
+        g.c = tl; g.ldc = n2;
+        g.m = n2; g.n = n1; g.k = n1; g.mode = kGemmSet;
+        push_inv(P, t1, g);
+        // L: inv[i2:, i:i2] = -(inv(C) * T)
+        g = GemmTask{};
+        g.a = li + i2 + i2 * npv; g.lda = npv;
+        g.b = tl; g.ldb = n2;
+        g.c = li + i2 + i * npv; g.ldc = npv;
+        g.m = n2; g.n = n1; g.k = n2; g.mode = kGemmNeg;
+        second.push_back(g);
+        // U: T' = U[i:i2, i2:] * inv(C)   (n1 x n2)
+        g = GemmTask{};
+        g.a = fo + i + i2 * nf; g.lda = nf;
+        g.b = ui + i2 + i2 * npv; g.ldb = npv;
+        g.c = tu; g.ldc = n1;
+        g.m = n1; g.n = n2; g.k = n2; g.mode = kGemmSet;
+        push_inv(P, t1, g);
+        // U: inv[i:i2, i2:] = -(inv(A) * T')
+        g = GemmTask{};
+        g.a = ui + i + i * npv; g.lda = npv;
+        g.b = tu; g.ldb = n1;
+        g.c = ui + i + i2 * npv; g.ldc = npv;
+        g.m = n1; g.n = n2; g.k = n1; g.mode = kGemmNeg;
+        second.push_back(g);
+      }
+    }
+    P.inv_scratch_elems = std::max(P.inv_scratch_elems, scratch);
+    P.inv_steps.push_back(t1);
+    InvStep t2{(int64_t)P.inv_tasks.size(), 0, 0, 0, 0, 0};
+    for (const GemmTask& g : second) push_inv(P, t2, g);
+    P.inv_steps.push_back(t2);
+    P.flops_inverse += t1.flops + t2.flops;
+  }
+}
+}  // namespace
+
 void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf, const int64_t* parent,
                 int64_t ns, const int64_t* sstart, const int64_t* upd_ptr, const int64_t* upd_idx, Plan& P) {
   P = Plan();
@@ -267,6 +352,22 @@ void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const i
       P.dinv_off[s] = P.dinv_blocks;
       P.dinv_blocks += ceil_div(P.np[s], kPanel);
     }
+
+  // ---- explicit pivot-block inverses (blocked triangular inversion) ---------
+  P.inv_off.assign(ns, -1);
+  P.inv_base = P.front_elems;
+  for (int64_t s = 0; s < ns; ++s)
+    if (P.nf[s] > kSmallFront) {
+      P.inv_off[s] = P.inv_base + P.inv_elems;
+      P.inv_elems += 2 * (int64_t)P.np[s] * P.np[s];
+      for (int32_t j = 0; j * kPanel < P.np[s]; ++j) {
+        P.inv_blocks.push_back((int32_t)s);
+        P.inv_blocks.push_back(j);
+      }
+    }
+  P.inv_scratch = P.inv_base + P.inv_elems;
+  build_inverse_steps(P);
+  P.pool_elems = P.inv_scratch + P.inv_scratch_elems;
 
   // ---- statistics ------------------------------------------------------------
   for (int64_t s = 0; s < ns; ++s) {

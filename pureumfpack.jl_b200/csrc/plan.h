@@ -44,13 +44,28 @@ struct TrsmTask {        // triangular solves of one panel step
   int64_t tile_base;     // prefix over tasks
 };
 
-struct GemmTask {        // C -= A * B, column-major, offsets in elements of the front pool
+enum GemmMode : int32_t {
+  kGemmSub = 0,          // C = C - A * B
+  kGemmSet = 1,          // C = A * B
+  kGemmFrom = 2,         // C = D - A * B (D: offset d, leading dimension ldc, same base as C)
+  kGemmNeg = 3           // C = -(A * B)
+};
+
+struct GemmTask {        // column-major, offsets in elements of the launch's base pointers
   int64_t a, b, c;
   int32_t m, n, k;
   int32_t lda, ldb, ldc;
   int32_t tiles_m, tiles_n;
-  int32_t pad;
+  int32_t mode;          // GemmMode
   int64_t tile_base;
+  int64_t d;             // kGemmFrom: offset of D (same base as C)
+  int32_t ldd, pad;      // kGemmFrom: leading dimension of D
+};
+
+// One launch of the blocked inversion of the pivot blocks (both tilings).
+struct InvStep {
+  int64_t first, count, tiles, tiles_tc;
+  double flops, elems;
 };
 
 enum LaunchKind : int32_t {
@@ -94,7 +109,8 @@ struct Plan {
   std::vector<int32_t> fc_ch_ptr;     // children contributions (child, child column)
   std::vector<int32_t> fc_ch;         // pairs, flattened
   int64_t fc_total = 0;
-  int64_t front_elems = 0;
+  int64_t front_elems = 0;              // fronts only; the pool also holds the pivot-block inverses
+  int64_t pool_elems = 0;               // fronts + inverses + inversion scratch
   // levels / slots
   int32_t nlevels = 0;
   std::vector<int32_t> slot_super;
@@ -109,6 +125,19 @@ struct Plan {
   // inverted 64x64 diagonal blocks of the large fronts' pivot blocks
   std::vector<int64_t> dinv_off;      // per supernode, -1 for small fronts
   int64_t dinv_blocks = 0;
+  // explicit inverses of the large fronts' pivot blocks, kept after the
+  // fronts in the front pool: inv(L11) (np x np, leading dimension np) at
+  // inv_off[s], inv(U11) right after it; the blocked inversion merges the
+  // inverted 64 x 64 diagonal blocks pairwise (64 -> 128 -> ...), each merge
+  // level one GEMM launch for the products with the off-diagonal block and
+  // one for the negated products with the other inverse, through a scratch
+  // area after the inverses.
+  std::vector<int64_t> inv_off;       // per supernode, -1 for small fronts
+  int64_t inv_base = 0, inv_elems = 0, inv_scratch = 0, inv_scratch_elems = 0;
+  std::vector<int32_t> inv_blocks;    // (supernode, 64-block) pairs, flattened, for the diagonal-block copy
+  std::vector<GemmTask> inv_tasks, inv_tasks_tc;
+  std::vector<InvStep> inv_steps;
+  double flops_inverse = 0;
   // launch sequences
   std::vector<int32_t> small_tasks;
   std::vector<PanelTask> panel_tasks;

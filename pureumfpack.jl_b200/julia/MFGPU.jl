@@ -94,6 +94,37 @@ function solve(h::Handle, B::AbstractVecOrMat{Float64}; refine::Integer = 0)
     return B isa AbstractVector ? vec(X) : X
 end
 
+# --- batched systems (many independent systems through one handle) -------
+# ordering: 0 = AMD (as splu(A; method=:multifrontal)), 1 = COLAMD.
+function batch_analyze!(h::Handle, As::Vector{SparseMatrixCSC{Float64, Int64}}; ordering::Integer = 0)
+    ns = Int64[size(A, 1) for A in As]
+    cps = Ptr{Int64}[pointer(A.colptr) for A in As]
+    rvs = Ptr{Int64}[pointer(rowvals(A)) for A in As]
+    GC.@preserve As _check(h, ccall((:mfgpu_batch_analyze, libmfgpu), Cint,
+        (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Ptr{Int64}}, Ptr{Ptr{Int64}}, Int32),
+        h.ptr, length(As), ns, cps, rvs, Int32(ordering)))
+    return h
+end
+
+# Factor every system with its own row scaling (scale: 0 none, 1 sum, 2 max);
+# returns each system's first singular column (0 = nonsingular).
+function batch_factor!(h::Handle, As::Vector{SparseMatrixCSC{Float64, Int64}}; scale::Integer = 1)
+    vals = Ptr{Float64}[pointer(nonzeros(A)) for A in As]
+    status = zeros(Int64, length(As))
+    GC.@preserve As _check(h, ccall((:mfgpu_batch_factor, libmfgpu), Cint,
+        (Ptr{Cvoid}, Ptr{Ptr{Float64}}, Int32, Int32, Ptr{Int64}), h.ptr, vals, Int32(scale), Int32(0), status))
+    return status
+end
+
+function batch_solve(h::Handle, Bs::Vector{Matrix{Float64}}; refine::Integer = 0)
+    Xs = [similar(B) for B in Bs]
+    GC.@preserve Bs Xs _check(h, ccall((:mfgpu_batch_solve, libmfgpu), Cint,
+        (Ptr{Cvoid}, Int64, Ptr{Ptr{Float64}}, Ptr{Ptr{Float64}}, Int32),
+        h.ptr, size(Bs[1], 2), Ptr{Float64}[pointer(B) for B in Bs], Ptr{Float64}[pointer(X) for X in Xs],
+        Int32(refine)))
+    return Xs
+end
+
 end # module
 
 # --- the reference-side change (in src/interface.jl / src/multifrontal.jl) ---

@@ -45,6 +45,7 @@ SCALE_MAX = ScaleKind.SCALE_MAX
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 FLAG_NO_TENSOR_CORES = 1   # mfgpu_options.flags: SIMT FP32 Schur updates in the mixed form
+FLAG_PERSISTENT_SOLVE = 2  # mfgpu_options.flags: one persistent cooperative launch per solve pass
 
 
 class ArgumentError(ValueError):
@@ -210,9 +211,11 @@ def predicted_fill(S: SymbolicMF) -> int:
 class GpuContext:
     """One libmfgpu handle: analysis, resident factors, solves."""
 
-    def __init__(self, device: int = 0, precision: int = PRECISION_FP64, tensor_cores: bool = True):
+    def __init__(self, device: int = 0, precision: int = PRECISION_FP64, tensor_cores: bool = True,
+                 persistent_solve: bool = False):
         self._lib = L.lib()
-        opts = L.MfOptions(device, precision, 0 if tensor_cores else FLAG_NO_TENSOR_CORES, 0)
+        flags = (0 if tensor_cores else FLAG_NO_TENSOR_CORES) | (FLAG_PERSISTENT_SOLVE if persistent_solve else 0)
+        opts = L.MfOptions(device, precision, flags, 0)
         h = ctypes.c_void_p()
         rc = self._lib.mfgpu_create(ctypes.byref(opts), ctypes.byref(h))
         if rc != 0:
@@ -234,6 +237,11 @@ class GpuContext:
     def set_precision(self, precision: int):
         self._check(self._lib.mfgpu_set_precision(self._h, int(precision)))
         self.precision = precision
+
+    def set_growth_limit(self, limit: float):
+        """Mixed form: refactor in FP64 when the FP32 factors' element growth
+        max|U| / max|Rs .* A| exceeds ``limit``."""
+        self._check(self._lib.mfgpu_set_growth_limit(self._h, float(limit)))
 
     def set_stream(self, stream_ptr: int):
         self._check(self._lib.mfgpu_set_stream(self._h, ctypes.c_void_p(stream_ptr)))

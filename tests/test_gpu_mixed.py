@@ -81,3 +81,32 @@ def test_mixed_refinement_reaches_fp64_backward_error(name, make):
     assert _eta(A, x, B) <= TARGET_ETA
     xo = O.solve(O.splu(A), B, refine=1)
     assert np.linalg.norm(x - xo) <= 1e-10 * np.linalg.norm(xo)
+
+
+def test_growth_check_refactors_in_fp64():
+    """Mixed form: element growth above the limit sends the matrix back to an
+    FP64 factorization; the factors are then exactly the FP64 form's."""
+    A = M.convdiff3d(10)
+    S = symbolic_mf(A)
+    Rs = row_scaling(A, SCALE_SUM)
+    ref = GpuContext(precision=0)
+    ref.analyze(A, S)
+    assert ref.factor(A.nzval, Rs, True) == 0
+    L0, U0 = ref.factors()[:2]
+
+    ctx = GpuContext(precision=PRECISION_MIXED)
+    ctx.analyze(A, S)
+    assert ctx.factor(A.nzval, Rs, True) == 0
+    st = ctx.stats()
+    assert st["refactored_fp64"] is False and 0 < st["growth"] < st["growth_limit"]
+    assert st["precision"] == "mixed"
+
+    ctx.set_growth_limit(1e-30)               # any growth now exceeds the limit
+    assert ctx.factor(A.nzval, Rs, True) == 0
+    st = ctx.stats()
+    assert st["refactored_fp64"] is True and st["precision"] == "fp64"
+    L1, U1 = ctx.factors()[:2]
+    np.testing.assert_array_equal(L1.nzval, L0.nzval)
+    np.testing.assert_array_equal(U1.nzval, U0.nzval)
+    B = M.rhs(A.n, seed=1, nrhs=3)
+    assert _eta(A, ctx.solve(B, 0), B) <= 1e-14
