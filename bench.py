@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--forms", default="fp64,mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="mixed form: keep the built-in GEMM variant rule instead of the learned autotuner")
     return ap.parse_args()
 
 
@@ -78,6 +80,12 @@ def make_workload(name: str, nrhs: int):
     elif kind == "poisson2d":
         A = M.poisson2d(k)
         seed = 0
+    elif kind == "convdiff":
+        A = M.convdiff3d(k)
+        seed = 2
+    elif kind == "random":
+        A = M.random_unsym(k, 5, 10.0, seed=3)
+        seed = 3
     else:
         raise SystemExit(f"unknown workload {name}")
     B = M.rhs(A.n, seed=seed, nrhs=nrhs)
@@ -173,7 +181,7 @@ def fp_peak_tflops(torch, dtype, device) -> float:
 
 
 # ---------------------------------------------------------------------------
-def cpu_baseline(A, B, refine: int, sample_rhs: int = 4):
+def cpu_baseline(A, B, refine: int, sample_rhs: int = 4, order: str = "amd", scale: int = 1):
     """The oracle (C++ restatement of the reference over OpenBLAS, all host
     threads): symbolic + numeric multifrontal_lu of the full matrix, then
     solve(F, b; refine) for `sample_rhs` right-hand sides, scaled to the full
@@ -183,9 +191,9 @@ def cpu_baseline(A, B, refine: int, sample_rhs: int = 4):
     cores = os.cpu_count() or 1
     O.blas_threads(cores)
     t0 = time.perf_counter()
-    S = O.symbolic_mf(A)
+    S = O.symbolic_mf(A, q=O.colamd_order(A) if order == "colamd" else None)
     t1 = time.perf_counter()
-    Rs = O.row_scaling(A, O.SCALE_SUM)
+    Rs = O.row_scaling(A, scale)
     As = O.apply_row_scaling(A, Rs)
     Fo = O.numeric(S, As, check=False)
     t2 = time.perf_counter()
@@ -210,8 +218,9 @@ def run_reference(args):
         return 0
     A, B = make_workload(args.workload, args.nrhs)
     times, det = [], None
+    order, scale = workload_setup(args.workload)
     for i in range(max(1, min(args.warmup, 1)) + args.steps):
-        t, det = cpu_baseline(A, B, refine=1)
+        t, det = cpu_baseline(A, B, refine=1, order=order, scale=scale)
         if i >= max(1, min(args.warmup, 1)):
             times.append(t)
     v = float(np.mean(times))
@@ -231,14 +240,71 @@ def run_reference(args):
 METRIC = "64^3 Poisson factor+solve s at bwd err <=1e-14: mixed vs FP64 on 1 B200; %roofline"
 
 
+def workload_setup(name: str):
+    """(ordering, scale kind) of a workload: the unsymmetric pair runs with
+    COLAMD through multifrontal_lu(As; q) and SCALE_MAX, the rest with AMD
+    (as splu(A; method=:multifrontal)) and SCALE_SUM."""
+    kind = name.rsplit("-", 1)[0]
+    return ("colamd", 2) if kind in ("convdiff", "random") else ("amd", 1)
+
+
 def workload_config(args, A):
-    return {"workload": f"{args.workload} n={A.n} nnz={A.nnz()} nrhs={args.nrhs} AMD SCALE_SUM, numeric factor + "
+    order, scale = workload_setup(args.workload)
+    return {"workload": f"{args.workload} n={A.n} nnz={A.nnz()} nrhs={args.nrhs} {order.upper()} "
+                        f"{'SCALE_MAX' if scale == 2 else 'SCALE_SUM'}, numeric factor + "
                         f"solve(refine) to normwise backward error <= 1e-14",
             "nrhs": args.nrhs, "l2": "working set (fronts) larger than L2; no explicit flush",
             "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "1 GPU"}
 
 
 # ---------------------------------------------------------------------------
+TUNE_TRAIN = ("poisson3d-24", "poisson3d-32", "convdiff-20", "poisson2d-200")
+
+
+def autotune_mixed(ctx, run, R, device):
+    """Learned GEMM-variant schedule for the mixed form: the cost model is
+    trained on the GPU on exhaustive tables of smaller matrices (TUNE_TRAIN,
+    same right-hand-side count), picks each launch's variant here, and this
+    workload's own exhaustive table judges the choice.  The timed steps run
+    the model's schedule."""
+    import torch
+    from pureumfpack import GpuContext, PRECISION_MIXED, row_scaling, symbolic_mf
+    from pureumfpack import autotune as AT
+
+    t0 = time.perf_counter()
+    tables = []
+    for name in TUNE_TRAIN:
+        A, B = make_workload(name, R)
+        c = GpuContext(device=device, precision=PRECISION_MIXED)
+        c.analyze(A, symbolic_mf(A))
+        dv = torch.device("cuda", device)
+        ax = torch.from_numpy(A.nzval).to(dv)
+        rs = torch.from_numpy(row_scaling(A, 1)).to(dv)
+        bb = torch.from_numpy(np.asfortranarray(B).ravel(order="F")).to(dv)
+        xx = torch.empty(A.n * R, dtype=torch.float64, device=dv)
+        torch.cuda.synchronize()
+
+        def r(c=c, ax=ax, rs=rs, bb=bb, xx=xx, n=A.n):
+            c.factor_device(ax.data_ptr(), rs.data_ptr(), True)
+            c.solve_device(R, bb.data_ptr(), n, xx.data_ptr(), n, 0)
+
+        r()
+        tables.append(AT.exhaustive_table(c, r, R))
+        del c
+    tuner = AT.train(tables, hidden=32, iters=3000, lr=3e-3, seed=0, device=device)
+    t_train = time.perf_counter() - t0
+    run()
+    feats = AT.tune_features(ctx, R)
+    choice = tuner.choose(feats)
+    table = AT.exhaustive_table(ctx, run, R)
+    j = AT.judge(tuner, table)
+    AT.set_choice(ctx, choice)
+    return {"launches": j["launches"], "mispredicted": j["mispredicted"], "model_ms": round(j["model_ms"], 3),
+            "exhaustive_ms": round(j["table_ms"], 3), "rule_ms": round(j["rule_ms"], 3),
+            "train_loss": round(tuner.loss, 4), "train_matrices": list(TUNE_TRAIN), "train_s": round(t_train, 2),
+            "tensor_core_launches": int(np.sum(choice == 1))}
+
+
 def roofline_of(P, primary, torch, dev, peaks):
     """Roofline entry for the dominant kernel class of one profiled step."""
     kern = P["stats"]["kernels"]
@@ -285,13 +351,14 @@ def main():
 
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
 
-    from pureumfpack import GpuContext, row_scaling, symbolic_mf, PRECISION_FP64, PRECISION_MIXED
+    from pureumfpack import GpuContext, colamd_order, row_scaling, symbolic_mf, PRECISION_FP64, PRECISION_MIXED
 
     A, B = make_workload(args.workload, args.nrhs)
     n, R = A.n, B.shape[1]
     t0 = time.perf_counter()
-    S = symbolic_mf(A)
-    Rs = row_scaling(A, 1)
+    order, scale = workload_setup(args.workload)
+    S = symbolic_mf(A, q=colamd_order(A) if order == "colamd" else None)
+    Rs = row_scaling(A, scale)
     t_sym = time.perf_counter() - t0
 
     # a dedicated stream shared with the library: CUDA events recorded on it
@@ -318,6 +385,10 @@ def main():
             if st != 0:
                 raise RuntimeError(f"singular pivot at column {st}")
             ctx.solve_device(R, d_b.data_ptr(), n, d_x.data_ptr(), n, refine)
+
+        tune = None
+        if form == "mixed" and not args.no_autotune:
+            tune = autotune_mixed(ctx, lambda: step(0), R, local)
 
         # refinement count that reaches the accuracy target on every rhs
         refine, eta, etas = 0, None, []
@@ -392,7 +463,8 @@ def main():
             e2e = {"value": e2e_s / world, "unit": "s", "h2d_bytes_per_step": 8 * (A.nnz() + n + n * R),
                    "d2h_bytes_per_step": 8 * n * R}
         forms[form] = {"ms_per_step": ms, "refine": refine, "eta": eta, "analyze_s": t_an + t_sym,
-                       "stats": st, "clocks": clk, "launches_timed": launches, "e2e": e2e, "etas": etas}
+                       "stats": st, "clocks": clk, "launches_timed": launches, "e2e": e2e, "etas": etas,
+                       "autotune": tune}
         del ctx
         torch.cuda.empty_cache()
 
@@ -410,7 +482,8 @@ def main():
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         try:
-            v, det = cpu_baseline(A, B, refine=forms.get("fp64", P)["refine"])
+            order, scale = workload_setup(args.workload)
+            v, det = cpu_baseline(A, B, refine=forms.get("fp64", P)["refine"], order=order, scale=scale)
             cpu = {"value": v, "unit": "s", "cores": det["cores"], "kind": "port", "sample": det["sample"],
                    "symbolic_s": det["symbolic_s"], "numeric_s": det["numeric_s"]}
         except Exception as e:  # the baseline must not kill the GPU number
@@ -426,7 +499,8 @@ def main():
                       "bwd_err_by_refine": f.get("etas"),
                       "factor_ms": f["stats"]["factor_ms"], "solve_ms": f["stats"]["solve_ms"],
                       "analyze_s": f["analyze_s"], "e2e_s": f["e2e"]["value"] if f["e2e"] else None,
-                      "kernels_ms": {kk: round(vv["ms"], 3) for kk, vv in f["stats"]["kernels"].items()}}
+                      "kernels_ms": {kk: round(vv["ms"], 3) for kk, vv in f["stats"]["kernels"].items()},
+                      **({"autotune": f["autotune"]} if f.get("autotune") else {})}
                   for k, f in forms.items()},
         "roofline": roof,
         "cpu_baseline": cpu,

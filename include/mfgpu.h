@@ -218,6 +218,42 @@ int mfgpu_batch_get_factors(mfgpu_ctx* h, int64_t sys, int64_t* lcolptr, int64_t
                             int64_t* ucolptr, int64_t* urowval, double* unzval, int64_t* p, int64_t* q,
                             int64_t* pinv);
 
+/* ------------------------------------------------------------------------
+ * Autotuner interface (no counterpart in the reference).  The batched GEMM
+ * launches of the mixed form -- factor updates, pivot-block inversion, and
+ * the solve products for nrhs right-hand sides, in issue order -- can each run
+ * as tcgen05 3xTF32 (128 x 128 tiles) or CUDA-core FP32 (64 x 64 tiles).
+ * ---------------------------------------------------------------------- */
+enum { MFGPU_TUNE_FEATURES = 11 };
+/* Number of tunable launches, and with `feats` (cap floats) their features,
+ * MFGPU_TUNE_FEATURES per launch: kind one-hot (factor, inversion, solve),
+ * log10(1 + x) of flops, bytes, tasks, 64-tiles, 128-tiles, mean m, n, k. */
+int mfgpu_tune_features(mfgpu_ctx* h, int64_t nrhs, int64_t* count, float* feats, int64_t cap);
+/* Variant per tunable launch: 0 built-in rule, 1 tcgen05, 2 CUDA cores
+ * (count 0 restores the rule everywhere).  Profiled launch records carry the
+ * tunable index as their seventh field. */
+int mfgpu_tune_set_choice(mfgpu_ctx* h, const int8_t* choice, int64_t count);
+
+/* ------------------------------------------------------------------------
+ * The autotuner's cost model: a small MLP (nin -> hidden -> hidden -> 1, tanh,
+ * mean-squared error, Adam) trained and evaluated on the GPU by libmfgpu's
+ * own kernels.  All arrays are host float32, samples row-major.
+ * ---------------------------------------------------------------------- */
+typedef struct mfgpu_mlp mfgpu_mlp;
+int mfgpu_mlp_create(int32_t device, int32_t nin, int32_t hidden, uint64_t seed, mfgpu_mlp** out);
+void mfgpu_mlp_destroy(mfgpu_mlp* m);
+const char* mfgpu_mlp_last_error(const mfgpu_mlp* m);
+int32_t mfgpu_mlp_nparams(const mfgpu_mlp* m);
+/* Parameters: W1 (hidden x nin, row-major), b1, W2 (hidden x hidden), b2, w3 (hidden), b3. */
+int mfgpu_mlp_get_params(mfgpu_mlp* m, float* out);
+int mfgpu_mlp_set_params(mfgpu_mlp* m, const float* in);
+int mfgpu_mlp_predict(mfgpu_mlp* m, const float* X, int64_t n, float* out);
+/* Loss (1/n) sum (f(x_i) - y_i)^2 and its gradient with respect to the parameters. */
+int mfgpu_mlp_loss_grad(mfgpu_mlp* m, const float* X, const float* Y, int64_t n, float* loss, float* grad);
+/* iters full-batch Adam steps at learning rate lr; final_loss may be NULL. */
+int mfgpu_mlp_train(mfgpu_mlp* m, const float* X, const float* Y, int64_t n, int32_t iters, float lr,
+                    float* final_loss);
+
 /* JSON object with the last call's phase times, sizes and counters, and the
  * per-kernel-class profile gathered since the last mfgpu_set_profiling. */
 int mfgpu_stats_json(mfgpu_ctx* h, char* buf, int64_t cap);

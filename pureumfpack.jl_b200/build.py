@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "pureumfpack", "libmfgpu.so")
 SOURCES = [
     "csrc/mfgpu.cu",
+    "csrc/costmodel.cu",
     "csrc/plan.cpp",
     "csrc/host/symbolic.cpp",
     "csrc/host/api_host.cpp",

@@ -183,6 +183,7 @@ struct mfgpu_ctx {
     double flops, bytes;
     int32_t level;
     int64_t tasks;
+    int32_t tune;
   };
   std::vector<Pending> pending;
   struct Record {   // one profiled launch
@@ -191,7 +192,14 @@ struct mfgpu_ctx {
     int64_t tasks;
     float ms;
     double flops, bytes;
+    int32_t tune;     // index among the tunable GEMM launches, -1 otherwise
   };
+  // autotuner: kernel variant of every tunable GEMM launch (factor GEMMs,
+  // inversion GEMMs, solve GEMMs for the current right-hand-side count, in
+  // issue order): 0 = built-in rule, 1 = tcgen05 3xTF32, 2 = CUDA-core FP32.
+  std::vector<int8_t> gemm_choice;
+  int64_t choice_version = 0;
+  int32_t cur_tune = -1;      // tunable id of the launch being issued
   std::vector<Record> records;
   std::vector<cudaEvent_t> evpool;
   size_t evnext = 0;
@@ -206,6 +214,8 @@ struct mfgpu_ctx {
 };
 
 namespace {
+
+constexpr int kTuneFeatures = 11;
 
 int fail(mfgpu_ctx* h, int code, const std::string& msg) {
   if (h) h->err = msg;
@@ -334,7 +344,7 @@ void klaunch(mfgpu_ctx* h, int kc, double flops, double bytes, F&& f, int32_t le
   CK(cudaEventRecord(a, h->stream));
   f();
   CK(cudaEventRecord(b, h->stream));
-  h->pending.push_back({kc, a, b, flops, bytes, level, tasks});
+  h->pending.push_back({kc, a, b, flops, bytes, level, tasks, h->cur_tune});
 }
 
 void prof_flush(mfgpu_ctx* h);
@@ -352,7 +362,7 @@ void prof_book(mfgpu_ctx* h, int kc, float ms, double flops, double bytes, int32
   k.flops += flops;
   k.bytes += bytes;
   ++k.launches;
-  if (h->records.size() < 200000) h->records.push_back({kc, level, tasks, ms, flops, bytes});
+  if (h->records.size() < 200000) h->records.push_back({kc, level, tasks, ms, flops, bytes, -1});
 }
 
 void prof_flush(mfgpu_ctx* h) {
@@ -380,7 +390,7 @@ void prof_flush(mfgpu_ctx* h) {
     k.flops += p.flops;
     k.bytes += p.bytes;
     ++k.launches;
-    if (h->records.size() < 200000) h->records.push_back({p.kc, p.level, p.tasks, ms, p.flops, p.bytes});
+    if (h->records.size() < 200000) h->records.push_back({p.kc, p.level, p.tasks, ms, p.flops, p.bytes, p.tune});
   }
   h->pending.clear();
   h->evnext = 0;
@@ -436,6 +446,22 @@ void launch_gemm<float>(const GemmTask* tasks, int64_t count, int64_t tiles, con
   k_gemm_f32<<<(unsigned)tiles, 256, 0, st>>>(tasks, (int)count, pa, pb, pc);
 }
 
+// Kernel variant of tunable GEMM launch `id` with FP32 operands: the
+// autotuner's choice when it made one, else the built-in rule `dflt`.
+bool gemm_use_tc(const mfgpu_ctx* h, int64_t id, bool dflt) {
+  if (!h->use_tc) return false;
+  if (id >= 0 && id < (int64_t)h->gemm_choice.size() && h->gemm_choice[id]) return h->gemm_choice[id] == 1;
+  return dflt;
+}
+
+// Tunable-launch ids: factor GEMM launches first, then the inversion steps,
+// then the solve GEMM steps.
+int64_t tune_factor_count(const Plan& P) {
+  int64_t c = 0;
+  for (const Launch& L : P.launches) c += L.kind == kLaunchGemm;
+  return c;
+}
+
 template <typename T>
 void run_factor_launches(mfgpu_ctx* h) {
   const Plan& P = h->plan;
@@ -443,6 +469,7 @@ void run_factor_launches(mfgpu_ctx* h) {
   T* pool = h->b_pool.as<T>();
   const double* vx = h->b_vx.as<double>();
   DevState S = dev_state(h);
+  int64_t tune_id = 0;
   for (const Launch& L : P.launches) {
     const double bytes = L.elems * sizeof(T) + L.extra_bytes;
     switch (L.kind) {
@@ -478,7 +505,8 @@ void run_factor_launches(mfgpu_ctx* h) {
         }, L.level, L.tiles);
         break;
       case kLaunchGemm:
-        if (sizeof(T) == 4 && h->use_tc)
+        h->cur_tune = (int32_t)tune_id;
+        if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, true))
           klaunch(h, KC_GEMM_FACTOR, L.flops, bytes, [&] {
             k_gemm_tc<128, 3><<<(unsigned)L.tiles_tc, kTcThreads, TcCfg<128, 3>::kSmem, st>>>(
                 h->b_gemm_tc.as<GemmTask>() + L.first, (int)L.count, (const float*)pool, (const float*)pool,
@@ -488,6 +516,8 @@ void run_factor_launches(mfgpu_ctx* h) {
           klaunch(h, KC_GEMM_FACTOR, L.flops, bytes, [&] {
             launch_gemm<T>(h->b_gemm.as<GemmTask>() + L.first, L.count, L.tiles, pool, pool, pool, st);
           }, L.level, L.tiles);
+        h->cur_tune = -1;
+        ++tune_id;
         break;
     }
   }
@@ -547,9 +577,12 @@ void issue_inverses(mfgpu_ctx* h) {
   klaunch(h, KC_INVERSE, 0, (double)nblk * 2 * 64 * 64 * sizeof(T) * 2, [&] {
     k_inv_init<T><<<(unsigned)nblk, 256, 0, st>>>(h->dp, h->b_inv_blocks.as<int32_t>(), h->b_dinv.as<T>(), pool);
   });
+  int64_t tune_id = tune_factor_count(P) - 1;
   for (const InvStep& is : P.inv_steps) {
+    ++tune_id;
     if (!is.count) continue;
-    if (sizeof(T) == 4 && h->use_tc)
+    h->cur_tune = (int32_t)tune_id;
+    if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, true))
       klaunch(h, KC_INVERSE, is.flops, is.elems * sizeof(T), [&] {
         k_gemm_tc<128, 3><<<(unsigned)is.tiles_tc, kTcThreads, TcCfg<128, 3>::kSmem, st>>>(
             h->b_inv_tasks_tc.as<GemmTask>() + is.first, (int)is.count, (const float*)pool, (const float*)pool,
@@ -559,6 +592,7 @@ void issue_inverses(mfgpu_ctx* h) {
       klaunch(h, KC_INVERSE, is.flops, is.elems * sizeof(T), [&] {
         launch_gemm<T>(h->b_inv_tasks.as<GemmTask>() + is.first, is.count, is.tiles, pool, pool, pool, st);
       }, -3, is.tiles);
+    h->cur_tune = -1;
   }
 }
 
@@ -611,7 +645,7 @@ int factor_impl(mfgpu_ctx* h, int32_t check) {
         (uintptr_t)h->b_ax.p, (uintptr_t)h->b_rs.p, (uintptr_t)h->b_dinv.p, (uintptr_t)h->b_li.p,
         (uintptr_t)h->b_lx.p, (uintptr_t)h->b_ui.p, (uintptr_t)h->b_ux.p, (uintptr_t)h->b_small.p,
         (uintptr_t)h->b_panel.p, (uintptr_t)h->b_trsm.p, (uintptr_t)h->b_gemm.p, (uintptr_t)h->b_ipiv.p,
-        (uintptr_t)h->b_gemm_tc.p, (uintptr_t)h->use_tc,
+        (uintptr_t)h->b_gemm_tc.p, (uintptr_t)h->use_tc, (uintptr_t)h->choice_version,
         (uintptr_t)h->b_info.p, (uintptr_t)h->b_flags.p, (uintptr_t)st};
     run_sequence(h, h->factor_key, h->factor_exec, h->factor_nodes, key, [&] { issue_factor<T>(h); });
     if (!P.has_speculative) break;
@@ -870,6 +904,7 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
   const unsigned wchunks = (unsigned)((R + 7) / 8);
   const int32_t* ids = S.d_ids.as<int32_t>();
   const GemmTask* gemms = S.d_gemms.as<GemmTask>();
+  int64_t tune_id = tune_factor_count(P) + (int64_t)P.inv_steps.size();
   if (h->persistent && !S.phases.empty()) {
     unsigned int* bar = h->b_bar.as<unsigned int>();
     PersistentArgs X{S.d_phases.as<SolvePhase>(), (int32_t)S.phases.size(), ids, gemms,
@@ -908,16 +943,19 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
         });
         break;
       case 3:
-        if (sizeof(T) == 4 && h->use_tc && R >= 64)
+        h->cur_tune = (int32_t)tune_id;
+        if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, R >= 64))
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
             k_gemm_tc<128, 3><<<(unsigned)s.tiles_tc, kTcThreads, TcCfg<128, 3>::kSmem, st>>>(
                 S.d_gemms_tc.as<GemmTask>() + s.first, (int)s.count, (const float*)pool, (const float*)fsol,
                 (float*)fsol, h->b_flags.as<int>());
-          });
+          }, -1, s.tiles_tc);
         else
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
             launch_gemm<T>(gemms + s.first, s.count, s.tiles, pool, fsol, fsol, st);
-          });
+          }, -1, s.tiles);
+        h->cur_tune = -1;
+        ++tune_id;
         break;
       case 4:
         klaunch(h, KC_BWD_SMALL, s.flops, bytes, [&] {
@@ -969,7 +1007,7 @@ void solve_graph(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double
       (uintptr_t)h->have_rs, (uintptr_t)h->b_rs.p, (uintptr_t)h->b_pool.p, (uintptr_t)h->b_dinv.p,
       (uintptr_t)h->b_fsol.p, (uintptr_t)h->b_inv_tasks.p, (uintptr_t)h->b_r.p, (uintptr_t)h->b_ax.p,
       (uintptr_t)S.d_ids.p, (uintptr_t)S.d_gemms.p, (uintptr_t)S.d_phases.p, (uintptr_t)h->b_prow.p,
-      (uintptr_t)S.d_gemms_tc.p, (uintptr_t)h->use_tc,
+      (uintptr_t)S.d_gemms_tc.p, (uintptr_t)h->use_tc, (uintptr_t)h->choice_version,
       (uintptr_t)h->b_rowfac.p, (uintptr_t)h->stream};
   if (!h->solve_graphs) {
     solve_refine<T>(h, R, d_b, ldb, d_x, ldx, refine, true);
@@ -1317,6 +1355,65 @@ int mfgpu_backward_error_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, i
   });
 }
 
+// ---- autotuner interface ----------------------------------------------------
+static void tune_row(float* f, int kind, const GemmTask* t, int64_t count, double flops, double elems,
+                     int64_t tiles, int64_t tiles_tc) {
+  double m = 0, n = 0, k = 0;
+  for (int64_t i = 0; i < count; ++i) {
+    m += t[i].m;
+    n += t[i].n;
+    k += t[i].k;
+  }
+  const double c = count > 0 ? (double)count : 1.0;
+  const double v[kTuneFeatures] = {kind == 0 ? 1.0 : 0.0, kind == 1 ? 1.0 : 0.0, kind == 2 ? 1.0 : 0.0,
+                                   std::log10(1 + flops), std::log10(1 + 4.0 * elems), std::log10(1.0 + count),
+                                   std::log10(1.0 + tiles), std::log10(1.0 + tiles_tc), std::log10(1 + m / c),
+                                   std::log10(1 + n / c), std::log10(1 + k / c)};
+  for (int q = 0; q < kTuneFeatures; ++q) f[q] = (float)v[q];
+}
+
+int mfgpu_tune_features(mfgpu_ctx* h, int64_t nrhs, int64_t* count, float* feats, int64_t cap) {
+  if (!h || !count || nrhs < 1) return MFGPU_ERR_ARGUMENT;
+  if (!h->analyzed) return fail(h, MFGPU_ERR_STATE, "tune features before analyze");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->device));
+    const Plan& P = h->plan;
+    build_solve_schedule(h, nrhs);
+    const SolveSchedule& S = h->sched;
+    std::vector<float> f;
+    float row[kTuneFeatures];
+    for (const Launch& L : P.launches)
+      if (L.kind == kLaunchGemm) {
+        tune_row(row, 0, P.gemm_tasks.data() + L.first, L.count, L.flops, L.elems, L.tiles, L.tiles_tc);
+        f.insert(f.end(), row, row + kTuneFeatures);
+      }
+    for (const InvStep& is : P.inv_steps) {
+      tune_row(row, 1, P.inv_tasks.data() + is.first, is.count, is.flops, is.elems, is.tiles, is.tiles_tc);
+      f.insert(f.end(), row, row + kTuneFeatures);
+    }
+    for (const auto& st : S.steps)
+      if (st.kind == 3) {
+        tune_row(row, 2, S.gemms.data() + st.first, st.count, st.flops, st.elems, st.tiles, st.tiles_tc);
+        f.insert(f.end(), row, row + kTuneFeatures);
+      }
+    *count = (int64_t)f.size() / kTuneFeatures;
+    if (feats) {
+      if (cap < (int64_t)f.size()) return fail(h, MFGPU_ERR_ARGUMENT, "feature buffer too small");
+      std::memcpy(feats, f.data(), f.size() * sizeof(float));
+    }
+    return MFGPU_OK;
+  });
+}
+
+int mfgpu_tune_set_choice(mfgpu_ctx* h, const int8_t* choice, int64_t count) {
+  if (!h || count < 0 || (count && !choice)) return MFGPU_ERR_ARGUMENT;
+  for (int64_t i = 0; i < count; ++i)
+    if (choice[i] < 0 || choice[i] > 2) return fail(h, MFGPU_ERR_ARGUMENT, "choice must be 0, 1 or 2");
+  h->gemm_choice.assign(choice, choice + count);
+  ++h->choice_version;
+  return MFGPU_OK;
+}
+
 int mfgpu_stats_json(mfgpu_ctx* h, char* buf, int64_t cap) {
   if (!h || !buf || cap <= 0) return MFGPU_ERR_ARGUMENT;
   const Plan& P = h->plan;
@@ -1370,8 +1467,8 @@ int mfgpu_launch_records(mfgpu_ctx* h, char* buf, int64_t cap) {
   char item[256];
   for (size_t i = 0; i < h->records.size(); ++i) {
     const auto& r = h->records[i];
-    std::snprintf(item, sizeof item, "%s[\"%s\", %d, %lld, %.6f, %.6e, %.6e]", i ? ", " : "",
-                  kKernelClassName[r.kc], r.level, (long long)r.tasks, r.ms, r.flops, r.bytes);
+    std::snprintf(item, sizeof item, "%s[\"%s\", %d, %lld, %.6f, %.6e, %.6e, %d]", i ? ", " : "",
+                  kKernelClassName[r.kc], r.level, (long long)r.tasks, r.ms, r.flops, r.bytes, r.tune);
     js += item;
   }
   js += "]";

@@ -18,6 +18,7 @@ f64 = ctypes.c_double
 vp = ctypes.c_void_p
 i64p = ctypes.POINTER(ctypes.c_int64)
 f64p = ctypes.POINTER(ctypes.c_double)
+f32p = ctypes.POINTER(ctypes.c_float)
 cp = ctypes.c_char_p
 
 # (name, restype, argtypes) for every symbol of include/mfgpu.h
@@ -57,6 +58,17 @@ SIGNATURES = [
     ("mfgpu_batch_solve", ctypes.c_int, [vp, i64, ctypes.POINTER(vp), ctypes.POINTER(vp), i32]),
     ("mfgpu_batch_factor_sizes", ctypes.c_int, [vp, i64, i64p]),
     ("mfgpu_batch_get_factors", ctypes.c_int, [vp, i64, i64p, i64p, f64p, i64p, i64p, f64p, i64p, i64p, i64p]),
+    ("mfgpu_tune_features", ctypes.c_int, [vp, i64, i64p, f32p, i64]),
+    ("mfgpu_tune_set_choice", ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int8), i64]),
+    ("mfgpu_mlp_create", ctypes.c_int, [i32, i32, i32, ctypes.c_uint64, ctypes.POINTER(vp)]),
+    ("mfgpu_mlp_destroy", None, [vp]),
+    ("mfgpu_mlp_last_error", cp, [vp]),
+    ("mfgpu_mlp_nparams", i32, [vp]),
+    ("mfgpu_mlp_get_params", ctypes.c_int, [vp, f32p]),
+    ("mfgpu_mlp_set_params", ctypes.c_int, [vp, f32p]),
+    ("mfgpu_mlp_predict", ctypes.c_int, [vp, f32p, i64, f32p]),
+    ("mfgpu_mlp_loss_grad", ctypes.c_int, [vp, f32p, f32p, i64, f32p, f32p]),
+    ("mfgpu_mlp_train", ctypes.c_int, [vp, f32p, f32p, i64, i32, ctypes.c_float, f32p]),
 ]
 
 _lib = None

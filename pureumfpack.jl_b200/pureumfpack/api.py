@@ -313,7 +313,8 @@ class GpuContext:
         self._check(self._lib.mfgpu_set_profiling(self._h, int(bool(on))))
 
     def launch_records(self) -> list:
-        """Profiled launches: [kernel class, level, tasks, ms, flops, bytes]."""
+        """Profiled launches: [kernel class, level, tasks, ms, flops, bytes,
+        tunable GEMM index or -1]."""
         cap = 1 << 20
         while True:
             buf = ctypes.create_string_buffer(cap)
