@@ -47,6 +47,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path[:0] = [ROOT, os.path.join(ROOT, "pureumfpack.jl_b200")]
 
 TARGET_ETA = 1e-14
+CPU_FRONT_LIMIT = 2e10    # front elements beyond which the CPU oracle baseline is not run
 MAX_REFINE = 8
 
 
@@ -61,6 +62,8 @@ def parse():
     ap.add_argument("--forms", default="fp64,mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--solve-mode", default="auto", choices=["auto", "step", "persistent"],
+                    help="solve launches: library default by rhs count, per step, or one persistent launch per pass")
     ap.add_argument("--no-autotune", action="store_true",
                     help="mixed form: keep the built-in GEMM variant rule instead of the learned autotuner")
     return ap.parse_args()
@@ -258,7 +261,7 @@ def workload_config(args, A):
 
 
 # ---------------------------------------------------------------------------
-TUNE_TRAIN = ("poisson3d-24", "poisson3d-32", "convdiff-20", "poisson2d-200")
+TUNE_TRAIN = ("poisson3d-24", "poisson3d-32", "poisson3d-40", "poisson3d-48", "convdiff-20", "poisson2d-200")
 
 
 def autotune_mixed(ctx, run, R, device):
@@ -295,7 +298,7 @@ def autotune_mixed(ctx, run, R, device):
     t_train = time.perf_counter() - t0
     run()
     feats = AT.tune_features(ctx, R)
-    choice = tuner.choose(feats)
+    choice = tuner.choose(feats, AT.rule_choice(feats, R))
     table = AT.exhaustive_table(ctx, run, R)
     j = AT.judge(tuner, table)
     AT.set_choice(ctx, choice)
@@ -374,7 +377,8 @@ def main():
     peaks = measured_peaks()
     for form in [f for f in args.forms.split(",") if f]:
         prec = PRECISION_MIXED if form == "mixed" else PRECISION_FP64
-        ctx = GpuContext(device=local, precision=prec)
+        ctx = GpuContext(device=local, precision=prec,
+                         persistent_solve={"auto": None, "step": False, "persistent": True}[args.solve_mode])
         ctx.set_stream(stream.cuda_stream)
         t0 = time.perf_counter()
         ctx.analyze(A, S)
@@ -480,7 +484,11 @@ def main():
     roof = roofline_of(P, primary, torch, dev, peaks)
 
     cpu = None
-    if not args.no_cpu_baseline and world == 1:
+    if not args.no_cpu_baseline and world == 1 and P["stats"].get("front_elems_full", 0) > CPU_FRONT_LIMIT:
+        cpu = {"value": None, "skipped": f"the oracle's full numeric factorization would materialise "
+                                         f"{P['stats']['front_elems_full']:.3g} front elements, far beyond a "
+                                         f"bounded CPU sample"}
+    elif not args.no_cpu_baseline and world == 1:
         try:
             order, scale = workload_setup(args.workload)
             v, det = cpu_baseline(A, B, refine=forms.get("fp64", P)["refine"], order=order, scale=scale)
@@ -507,8 +515,9 @@ def main():
         "e2e": P["e2e"],
         "gpu_launches": P["launches_timed"],
         "clocks": P["clocks"],
-        "stats": {k: P["stats"][k] for k in ("n", "nsuper", "levels", "nnz_l", "nnz_u", "max_front", "flops",
-                                             "front_elems")},
+        "stats": {k: P["stats"].get(k) for k in ("n", "nsuper", "levels", "nnz_l", "nnz_u", "max_front", "flops",
+                                                 "front_elems", "front_elems_full", "pool_elems", "lean",
+                                                 "flops_inverse")},
     }
     print(json.dumps(line), flush=True)
     if world > 1:
@@ -703,8 +712,9 @@ def run_batch(args):
                   for k, f in forms.items()},
         "roofline": roof, "cpu_baseline": cpu, "e2e": P["e2e"], "gpu_launches": P["launches_timed"],
         "clocks": P["clocks"], "predicted_gflop": flops_total / 1e9, "cost_model_s": t_cost,
-        "stats": {k: P["stats"][k] for k in ("n", "nsuper", "levels", "nnz_l", "nnz_u", "max_front", "flops",
-                                             "front_elems")},
+        "stats": {k: P["stats"].get(k) for k in ("n", "nsuper", "levels", "nnz_l", "nnz_u", "max_front", "flops",
+                                                 "front_elems", "front_elems_full", "pool_elems", "lean",
+                                                 "flops_inverse")},
     }
     print(json.dumps(line), flush=True)
     if world > 1:

@@ -94,9 +94,14 @@ typedef struct mfgpu_ctx mfgpu_ctx;
 
 /* mfgpu_options.flags */
 enum {
-  MFGPU_FLAG_NO_TENSOR_CORES = 1,  /* FP32 fronts: SIMT FP32 Schur updates instead of tcgen05 3xTF32 */
-  MFGPU_FLAG_PERSISTENT_SOLVE = 2  /* solves: one cooperative persistent launch per pass instead of one launch
-                                      per step (fewer launches, lower occupancy; slower on the measured cases) */
+  MFGPU_FLAG_NO_TENSOR_CORES = 1,  /* FP32 fronts: CUDA-core FP32 GEMMs instead of tcgen05 */
+  MFGPU_FLAG_PERSISTENT_SOLVE = 2, /* solves: one cooperative persistent launch per pass (slower than the
+                                      default per-step launches on every measured case; kept for comparison) */
+  MFGPU_FLAG_TF32_SPLIT = 4,       /* tensor-core GEMMs of FP32 fronts as 3xTF32 (two-part split, about 2^-21)
+                                      instead of BF16x3 (three-part split, FP32 accuracy) */
+  MFGPU_FLAG_STEP_SOLVE = 8,       /* solves: one launch per step (the default) */
+  MFGPU_FLAG_LEAN_FRONTS = 16      /* front memory reused by lifetime with a compact panel pool, whatever the
+                                      size (default: only when all fronts would not fit in 45% of the device) */
 };
 
 typedef struct {

@@ -39,7 +39,12 @@ struct DevPlan {
   const int32_t* csr_src;
   const int64_t* dinv_off;   // per supernode: first 64-block of its inverted diagonal blocks (-1: small front)
   const int64_t* inv_off;    // per supernode: pool offset of inv(L11); inv(U11) follows (-1: small front)
+  const int64_t* lpan_off;   // per supernode: factored first np columns (leading dimension nf)
+  const int64_t* u12_off;    // per supernode: factored U12 (leading dimension lean ? np : nf)
+  int32_t lean;              // panels in the compact panel pool (fronts' memory reused)
 };
+
+__device__ __forceinline__ int u12_ld(const DevPlan& P, int s) { return P.lean ? P.np[s] : P.nf[s]; }
 
 // Per-factorization numeric state.
 struct DevState {

@@ -836,7 +836,8 @@ __global__ void __launch_bounds__(256) k_scatter_csc(DevPlan P, DevState S, cons
   const int s = P.fc_super[fc];
   const int c = (int)(fc - P.colbase[s]);
   const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
-  const T* col = pool + P.front_off[s] + (int64_t)c * nf;
+  const T* col = c < np ? pool + P.lpan_off[s] + (int64_t)c * nf
+                        : pool + P.u12_off[s] + (int64_t)(c - np) * u12_ld(P, s);
   const int32_t* us = P.upd + P.upd_off[s];
   if (c < np) {
     const int a = c, j = c1 + a;
@@ -858,6 +859,23 @@ __global__ void __launch_bounds__(256) k_scatter_csc(DevPlan P, DevState S, cons
       ui[ub + a] = 1 + c1 + a;
     }
   }
+}
+
+// Lean layout: copy the factored panel of every front of a level (one warp
+// per front column: the whole column below the diagonal block's top for the
+// first np columns, the np U12 rows for the rest) to the panel pool.
+template <typename T>
+__global__ void __launch_bounds__(256) k_copy_panels(DevPlan P, int64_t fc0, int64_t count, T* __restrict__ pool) {
+  const int64_t w = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp_id();
+  if (w >= count) return;
+  const int64_t fc = fc0 + w;
+  const int s = P.fc_super[fc];
+  const int c = (int)(fc - P.colbase[s]);
+  const int np = P.np[s], nf = P.nf[s];
+  const T* src = pool + P.front_off[s] + (int64_t)c * nf;
+  T* dst = c < np ? pool + P.lpan_off[s] + (int64_t)c * nf : pool + P.u12_off[s] + (int64_t)(c - np) * np;
+  const int rows = c < np ? nf : np;
+  for (int r = lane_id(); r < rows; r += 32) dst[r] = src[r];
 }
 
 // V = Diagonal(Rs) * A restricted to qf: vx[p] = Rs[row] * A.nzval[src]

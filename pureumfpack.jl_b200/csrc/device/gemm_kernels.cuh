@@ -127,22 +127,25 @@ __device__ __forceinline__ void gemm_tile_f64(const GemmTask* __restrict__ tasks
   __syncthreads();
   // all loads of C before any store: the stores could alias later loads as
   // far as the compiler knows, which would serialise one round trip each
-  constexpr int kPer = BM * BN / kGemmThreads;
+  constexpr int kPer = BM * BN / kGemmThreads / 2;   // two passes of 16 keep the register peak low
   const double* D = tk.mode == kGemmFrom ? pc + tk.d : C;
   const int ldD = tk.mode == kGemmFrom ? tk.ldd : ldc;
   const bool load = tk.mode == kGemmSub || tk.mode == kGemmFrom;
   const double sgn = tk.mode == kGemmSet ? -1.0 : 1.0;   // Set: C = +AB; Neg: C = -AB = 0 - AB
-  double cv[kPer];
+#pragma unroll 1
+  for (int pass = 0; pass < 2; ++pass) {
+    double cv[kPer];
 #pragma unroll
-  for (int i = 0; i < kPer; ++i) {
-    const int idx = tid + i * kGemmThreads, m = idx % BM, n = idx / BM;
-    cv[i] = (load && m0 + m < M && n0 + n < N) ? D[(int64_t)(m0 + m) + (int64_t)(n0 + n) * ldD] : 0.0;
-  }
+    for (int i = 0; i < kPer; ++i) {
+      const int idx = tid + (pass * kPer + i) * kGemmThreads, m = idx % BM, n = idx / BM;
+      cv[i] = (load && m0 + m < M && n0 + n < N) ? D[(int64_t)(m0 + m) + (int64_t)(n0 + n) * ldD] : 0.0;
+    }
 #pragma unroll
-  for (int i = 0; i < kPer; ++i) {
-    const int idx = tid + i * kGemmThreads, m = idx % BM, n = idx / BM;
-    if (m0 + m < M && n0 + n < N)
-      C[(int64_t)(m0 + m) + (int64_t)(n0 + n) * ldc] = cv[i] - sgn * Cs[n * LDC_S + m];
+    for (int i = 0; i < kPer; ++i) {
+      const int idx = tid + (pass * kPer + i) * kGemmThreads, m = idx % BM, n = idx / BM;
+      if (m0 + m < M && n0 + n < N)
+        C[(int64_t)(m0 + m) + (int64_t)(n0 + n) * ldc] = cv[i] - sgn * Cs[n * LDC_S + m];
+    }
   }
   __syncthreads();
 }
@@ -317,6 +320,88 @@ __global__ void __launch_bounds__(256) k_gemm_f32(const GemmTask* __restrict__ t
       const int m = m0 + tm + i, n = n0 + tn + j;
       if (m < M && n < N) C[(int64_t)m + (int64_t)n * ldc] = cv[i][j] - sgn * acc[i][j];
     }
+}
+
+// ---------------------------------------------------------------------------
+// Split-K products for few right-hand sides (N <= NMAX): the solve products
+// g = y - U12 x_u have a handful of rows and thousands of K, which a 64 x 64
+// tile would walk serially.  Stage 1: one CTA per (task, 128-row block,
+// kSkinnyKC-wide K chunk), one thread per row, partial sums of all N columns
+// into a scratch array.  Stage 2: one CTA per (task, row block) sums the
+// chunks in order (deterministic) and applies the task's mode.
+constexpr int kSkinnyRows = 128;
+constexpr int kSkinnyKC = 256;
+constexpr int kSkinnyMaxN = 16;
+
+struct SkinnyTask {
+  int64_t a, b, c, d;
+  int32_t m, n, k, lda, ldb, ldc, ldd, mode;
+  int32_t rblocks, kchunks;
+  int64_t part_base;     // prefix over tasks of rblocks * kchunks (stage-1 CTAs and scratch items)
+  int64_t red_base;      // prefix over tasks of rblocks (stage-2 CTAs)
+};
+
+__device__ __forceinline__ int find_skinny(const SkinnyTask* __restrict__ t, int n, int64_t x, bool red) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if ((red ? t[mid].red_base : t[mid].part_base) <= x) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <typename T, int NMAX>
+__global__ void __launch_bounds__(kSkinnyRows) k_skinny_part(const SkinnyTask* __restrict__ tasks, int ntasks,
+                                                             const T* pa, const T* pb, T* __restrict__ part) {
+  __shared__ T bs[kSkinnyKC * NMAX];
+  const SkinnyTask tk = tasks[find_skinny(tasks, ntasks, blockIdx.x, false)];
+  const int64_t local = blockIdx.x - tk.part_base;
+  const int rb = (int)(local % tk.rblocks), kc = (int)(local / tk.rblocks);
+  const int k0 = kc * kSkinnyKC, kn = min(kSkinnyKC, tk.k - k0), N = tk.n;
+  const T* A = pa + tk.a;
+  const T* B = pb + tk.b;
+  for (int e = threadIdx.x; e < kSkinnyKC * NMAX; e += blockDim.x) {
+    const int k = e % kSkinnyKC, n = e / kSkinnyKC;
+    bs[e] = (k < kn && n < N) ? B[(int64_t)(k0 + k) + (int64_t)n * tk.ldb] : T(0);
+  }
+  __syncthreads();
+  const int row = rb * kSkinnyRows + threadIdx.x;
+  T acc[NMAX];
+#pragma unroll
+  for (int n = 0; n < NMAX; ++n) acc[n] = T(0);
+  if (row < tk.m) {
+    const T* ar = A + row + (int64_t)k0 * tk.lda;
+#pragma unroll 4
+    for (int k = 0; k < kn; ++k) {
+      const T a = ar[(int64_t)k * tk.lda];
+#pragma unroll
+      for (int n = 0; n < NMAX; ++n) acc[n] += a * bs[k + n * kSkinnyKC];
+    }
+  }
+  T* out = part + (tk.part_base + local) * (int64_t)(kSkinnyRows * NMAX);
+#pragma unroll
+  for (int n = 0; n < NMAX; ++n) out[threadIdx.x + n * kSkinnyRows] = acc[n];
+}
+
+template <typename T, int NMAX>
+__global__ void __launch_bounds__(kSkinnyRows) k_skinny_reduce(const SkinnyTask* __restrict__ tasks, int ntasks,
+                                                               const T* __restrict__ part, T* pc) {
+  const SkinnyTask tk = tasks[find_skinny(tasks, ntasks, blockIdx.x, true)];
+  const int rb = (int)(blockIdx.x - tk.red_base);
+  const int row = rb * kSkinnyRows + threadIdx.x;
+  if (row >= tk.m) return;
+  T* C = pc + tk.c;
+  const T* D = tk.mode == kGemmFrom ? pc + tk.d : C;
+  const int ldD = tk.mode == kGemmFrom ? tk.ldd : tk.ldc;
+  for (int n = 0; n < tk.n; ++n) {
+    T sum = T(0);
+    for (int kc = 0; kc < tk.kchunks; ++kc)
+      sum += part[(tk.part_base + rb + (int64_t)kc * tk.rblocks) * (int64_t)(kSkinnyRows * NMAX) + threadIdx.x +
+                  n * kSkinnyRows];
+    const T dv = (tk.mode == kGemmSub || tk.mode == kGemmFrom) ? D[(int64_t)row + (int64_t)n * ldD] : T(0);
+    C[(int64_t)row + (int64_t)n * tk.ldc] = tk.mode == kGemmSet ? sum : dv - sum;
+  }
 }
 
 }  // namespace mfgpu

@@ -85,7 +85,7 @@ __device__ __forceinline__ void fwd_small_item(const DevPlan& P, const DevState&
     }
     __syncthreads();
   }
-  const T* L = pool + P.front_off[s];
+  const T* L = pool + P.lpan_off[s];
   for (int a = 0; a < np; ++a) {
     const int rows = nf - a - 1;
     for (int e = tid; e < rows * rc; e += blockDim.x) {
@@ -179,11 +179,13 @@ __device__ __forceinline__ void bwd_small_item(const DevPlan& P, const SolveArgs
     g[t + c * nu] = xw[us[t] + (int64_t)(c0 + c) * A.ldx];
   }
   __syncthreads();
-  const T* U = pool + P.front_off[s];
+  const T* U = pool + P.lpan_off[s];
+  const T* U12 = pool + P.u12_off[s];
+  const int ldu = u12_ld(P, s);
   for (int e = tid; e < np * rc; e += blockDim.x) {
     const int a = e % np, c = e / np;
     T acc = y[a + c * np];
-    for (int t = 0; t < nu; ++t) acc -= U[a + (int64_t)(np + t) * nf] * g[t + c * nu];
+    for (int t = 0; t < nu; ++t) acc -= U12[a + (int64_t)t * ldu] * g[t + c * nu];
     y[a + c * np] = acc;
   }
   __syncthreads();

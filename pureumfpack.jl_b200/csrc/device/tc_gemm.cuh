@@ -308,4 +308,251 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(const GemmTask* __res
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::kTmemCols));
 }
 
+// ---------------------------------------------------------------------------
+// BF16x3 variant.  Each FP32 operand is split into three bf16 parts,
+// x = b1 + b2 + b3 (b1 = bf16(x), b2 = bf16(x - b1), b3 = bf16(x - b1 - b2)),
+// which represents x to about 2^-24 relative -- FP32's own precision -- and
+// the product keeps the six terms b_i c_j with i + j <= 4 (a1 b1, a1 b2,
+// a2 b1, a1 b3, a3 b1, a2 b2), accumulated in FP32 in tensor memory by
+// tcgen05.mma kind::f16 (M = 128, N = BN, K = 16).  bf16 runs at twice the
+// TF32 rate, so six bf16 products cost what three TF32 products cost, with
+// FP32 accuracy instead of the 2^-21 of the two-part TF32 split.
+//
+// Warps 0-7 stage a 64-wide K block (one 128-byte swizzle row of bf16):
+// thread t converts row t % 128 over K half t / 128 of A, and four 8-value
+// chunks of B; warp 8 issues the MMAs; all eight staging warps then read the
+// accumulator back (warp w: lanes 32 (w % 4).., column half w / 4).
+constexpr int kBxProducers = 256;
+constexpr int kBxThreads = kBxProducers + 32;
+
+template <int BN, int STAGES>
+struct BxCfg {
+  static constexpr int BM = 128, BK = 64;
+  static constexpr int kABytes = BM * BK * 2;     // one bf16 part of A
+  static constexpr int kBBytes = BN * BK * 2;
+  static constexpr int kStageBytes = 3 * kABytes + 3 * kBBytes;
+  static constexpr size_t kSmem = (size_t)STAGES * kStageBytes + 1024;
+  static constexpr int kTmemCols = BN;
+  // D f32, A/B bf16, both K-major, N = BN, M = 128
+  static constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                     ((uint32_t)(BM >> 4) << 24);
+  static_assert(BN == 64 || BN == 128, "BN must be 64 or 128");
+};
+
+// Byte offset of element (row, k) (k < 64) in a K-major, 128-byte-swizzled
+// tile of 2-byte elements.
+__device__ __forceinline__ uint32_t sw128_offset_b16(int row, int k) {
+  const int chunk = (k >> 3) ^ (row & 7);
+  return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + chunk * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ void tc_mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  uint32_t r;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
+}
+
+// Split eight consecutive K values into three bf16 parts and store each part
+// as one 16-byte chunk at byte offset `off` of its part buffer.
+__device__ __forceinline__ void bx_put8(uint32_t p1, uint32_t p2, uint32_t p3, uint32_t off, const float* v) {
+  uint32_t w1[4], w2[4], w3[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float x0 = v[2 * q], x1 = v[2 * q + 1];
+    w1[q] = pack_bf16(x0, x1);
+    const float h0 = __uint_as_float(w1[q] << 16), h1 = __uint_as_float(w1[q] & 0xFFFF0000u);
+    const float r0 = x0 - h0, r1 = x1 - h1;
+    w2[q] = pack_bf16(r0, r1);
+    const float m0 = __uint_as_float(w2[q] << 16), m1 = __uint_as_float(w2[q] & 0xFFFF0000u);
+    w3[q] = pack_bf16(r0 - m0, r1 - m1);
+  }
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(p1 + off), "r"(w1[0]), "r"(w1[1]), "r"(w1[2]),
+               "r"(w1[3]) : "memory");
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(p2 + off), "r"(w2[0]), "r"(w2[1]), "r"(w2[2]),
+               "r"(w2[3]) : "memory");
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(p3 + off), "r"(w3[0]), "r"(w3[1]), "r"(w3[2]),
+               "r"(w3[3]) : "memory");
+}
+
+// Batched C = f(C, A * B) (GemmTask::mode) over tasks whose tiles_m /
+// tiles_n count 128 x BN tiles; flags[1] is set when a bounded wait expired.
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __restrict__ tasks, int ntasks,
+                                                            const float* __restrict__ pa, const float* __restrict__ pb,
+                                                            float* pc, int* __restrict__ flags) {
+  using Cfg = BxCfg<BN, STAGES>;
+  constexpr int BK = Cfg::BK;
+  extern __shared__ __align__(16) uint8_t bx_smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)bx_smem_raw + 1023) & ~(uintptr_t)1023);
+  __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done;
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int failed;
+
+  const int t = threadIdx.x, warp = warp_id(), lane = lane_id();
+  int lo = 0, hi = ntasks - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tasks[mid].tile_base <= (int64_t)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  const GemmTask tk = tasks[lo];
+  const int64_t local = blockIdx.x - tk.tile_base;
+  const int m0 = (int)(local % tk.tiles_m) * Cfg::BM;
+  const int n0 = (int)(local / tk.tiles_m) * BN;
+  const int M = tk.m, N = tk.n, K = tk.k;
+  const int nk = (K + BK - 1) / BK;
+
+  if (t == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], kBxProducers);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(&done, 1);
+    failed = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(Cfg::kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  const uint32_t sbase = smem_u32(smem);
+
+  if (warp < 8) {
+    const float* A = pa + tk.a;
+    const float* B = pb + tk.b;
+    const int arow = t & 127, ak = (t >> 7) * 32;
+    const int row = m0 + arow;
+    constexpr int kBPer = BN * (BK / 8) / kBxProducers;   // (column, 8-chunk) pairs per thread
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % STAGES, k0 = kb * BK;
+      float va[32];
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        const int kk = k0 + ak + k;
+        va[k] = (row < M && kk < K) ? A[(int64_t)row + (int64_t)kk * tk.lda] : 0.0f;
+      }
+      float vb[kBPer][8];
+#pragma unroll
+      for (int i = 0; i < kBPer; ++i) {
+        const int idx = t + i * kBxProducers, n = idx >> 3, c = idx & 7;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int kk = k0 + 8 * c + j;
+          vb[i][j] = (n0 + n < N && kk < K) ? B[(int64_t)kk + (int64_t)(n0 + n) * tk.ldb] : 0.0f;
+        }
+      }
+      if (kb >= STAGES && !mbar_wait(&empty[s], (uint32_t)((kb / STAGES - 1) & 1))) {
+        failed = 1;
+        break;
+      }
+      const uint32_t st = sbase + s * Cfg::kStageBytes;
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        bx_put8(st, st + Cfg::kABytes, st + 2 * Cfg::kABytes, sw128_offset_b16(arow, ak + 8 * c), va + 8 * c);
+      const uint32_t sb = st + 3 * Cfg::kABytes;
+#pragma unroll
+      for (int i = 0; i < kBPer; ++i) {
+        const int idx = t + i * kBxProducers;
+        bx_put8(sb, sb + Cfg::kBBytes, sb + 2 * Cfg::kBBytes, sw128_offset_b16(idx >> 3, 8 * (idx & 7)), vb[i]);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(&full[s]);
+      if (failed) break;
+    }
+  } else if (lane == 0) {
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % STAGES;
+      if (failed || !mbar_wait(&full[s], (uint32_t)((kb / STAGES) & 1))) {
+        failed = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a1 = sbase + s * Cfg::kStageBytes, a2 = a1 + Cfg::kABytes, a3 = a2 + Cfg::kABytes;
+      const uint32_t b1 = a1 + 3 * Cfg::kABytes, b2 = b1 + Cfg::kBBytes, b3 = b2 + Cfg::kBBytes;
+#pragma unroll
+      for (int ks = 0; ks < BK / 16; ++ks) {      // K = 16 per instruction: 32 bytes along the row
+        const uint32_t ko = ks * 32;
+        // smallest terms first
+        tc_mma_bf16(tmem, umma_desc_sw128(a2 + ko), umma_desc_sw128(b2 + ko), Cfg::kIdesc,
+                    (kb > 0 || ks > 0) ? 1u : 0u);
+        tc_mma_bf16(tmem, umma_desc_sw128(a3 + ko), umma_desc_sw128(b1 + ko), Cfg::kIdesc, 1u);
+        tc_mma_bf16(tmem, umma_desc_sw128(a1 + ko), umma_desc_sw128(b3 + ko), Cfg::kIdesc, 1u);
+        tc_mma_bf16(tmem, umma_desc_sw128(a2 + ko), umma_desc_sw128(b1 + ko), Cfg::kIdesc, 1u);
+        tc_mma_bf16(tmem, umma_desc_sw128(a1 + ko), umma_desc_sw128(b2 + ko), Cfg::kIdesc, 1u);
+        tc_mma_bf16(tmem, umma_desc_sw128(a1 + ko), umma_desc_sw128(b1 + ko), Cfg::kIdesc, 1u);
+      }
+      tc_commit(&empty[s]);
+    }
+    tc_commit(&done);
+  }
+
+  if (warp < 8) {
+    const bool ok = mbar_wait(&done, 0u) && !failed;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) {
+      float* C = pc + tk.c;
+      const int q = warp & 3, half = warp >> 2;
+      const int row = m0 + q * 32 + lane;
+      const float* D = tk.mode == kGemmFrom ? pc + tk.d : C;
+      const int ldD = tk.mode == kGemmFrom ? tk.ldd : tk.ldc;
+      const bool ld = tk.mode == kGemmSub || tk.mode == kGemmFrom;
+      const float sgn = tk.mode == kGemmSet ? -1.0f : 1.0f;
+#pragma unroll 1
+      for (int c0 = half * (BN / 2); c0 < (half + 1) * (BN / 2); c0 += 32) {
+        uint32_t v[32];
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0;
+        if (nk == 0) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) v[j] = 0u;
+        } else {
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+              "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+              "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+              : "r"(taddr));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        }
+        if (row < M) {
+          float cv[32];
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int col = n0 + c0 + j;
+            cv[j] = (ld && col < N) ? D[(int64_t)row + (int64_t)col * ldD] : 0.0f;
+          }
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int col = n0 + c0 + j;
+            if (col < N) C[(int64_t)row + (int64_t)col * tk.ldc] = cv[j] - sgn * __uint_as_float(v[j]);
+          }
+        }
+      }
+    } else if (failed && t == 0) {
+      atomicOr(flags + 1, 1);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::kTmemCols));
+}
+
 }  // namespace mfgpu

@@ -88,12 +88,12 @@ inline unsigned grid1(int64_t work, int per) { return (unsigned)((work + per - 1
 enum KernelClass {
   KC_BUILD_VALUES, KC_SMALL, KC_ASSEMBLE, KC_PANEL, KC_TRSM, KC_GEMM_FACTOR, KC_PIVOTS, KC_SCATTER,
   KC_FWD_SMALL, KC_FWD_ASSEMBLE, KC_GEMM_SOLVE, KC_BWD_SMALL, KC_BWD_GATHER,
-  KC_SOLVE_FINISH, KC_RESIDUAL, KC_INVERSE, KC_COUNT
+  KC_SOLVE_FINISH, KC_RESIDUAL, KC_INVERSE, KC_COPY_PANELS, KC_COUNT
 };
 const char* const kKernelClassName[KC_COUNT] = {
     "build_values", "small_fronts", "assemble_columns", "panel", "panel_trsm", "gemm_factor", "finalize_pivots",
     "scatter_csc", "fwd_small", "fwd_assemble", "gemm_solve", "bwd_small", "bwd_gather",
-    "solve_finish", "residual", "gemm_inverse"};
+    "solve_finish", "residual", "gemm_inverse", "copy_panels"};
 
 struct KStat {
   double ms = 0, flops = 0, bytes = 0;
@@ -108,12 +108,15 @@ struct SolveSchedule {
     int64_t first, count, tiles;
     double flops = 0, elems = 0;
     int64_t tiles_tc = 0;   // GEMM steps: grid in 128 x 128 tensor-core tiles (gemms_tc)
+    int64_t sk_first = 0, sk_count = 0, sk_parts = 0, sk_reds = 0;   // split-K form (few rhs)
   };
   std::vector<Step> steps;
   std::vector<int32_t> ids;
   std::vector<GemmTask> gemms, gemms_tc;   // 64 x 64 tiles; 128 x 128 tiles (FP32 on tensor cores)
+  std::vector<SkinnyTask> skinny;          // split-K form of every GEMM step when nrhs <= kSkinnyMaxN
+  int64_t skinny_scratch = 0;              // partial sums, elements
   std::vector<SolvePhase> phases;   // the steps as work-item phases of the persistent solve
-  DevBuf d_ids, d_gemms, d_gemms_tc, d_phases;
+  DevBuf d_ids, d_gemms, d_gemms_tc, d_phases, d_skinny;
 };
 
 }  // namespace
@@ -132,19 +135,26 @@ struct mfgpu_ctx {
       b_v_src, b_v_srow, b_v_frow, b_fc_super, b_fc_vbeg, b_fc_vend, b_fc_ch_ptr, b_fc_ch, b_lcolptr, b_ucolptr, b_qf,
       b_csr_ptr, b_csr_col, b_csr_src;
   DevBuf b_small, b_panel, b_trsm, b_gemm, b_gemm_tc;
-  bool use_tc = true;   // FP32 fronts: Schur updates on tensor cores (3xTF32)
+  bool use_tc = true;      // FP32 fronts: GEMMs on tensor cores
+  bool tc_bf16x3 = true;   // tensor-core split: BF16x3 (FP32 accuracy) or 3xTF32
   bool launches_safe = false;
   // numeric state
   DevBuf b_pool, b_vx, b_ax, b_rs, b_ipiv, b_info, b_prow, b_rowfac, b_flags, b_dinv, b_dinv_off;
   DevBuf b_inv_off, b_inv_blocks, b_inv_tasks, b_inv_tasks_tc;   // pivot-block inversion
+  DevBuf b_lpan_off, b_u12_off;                                   // factored panels
+  DevBuf b_skinny;                                                // split-K partial sums
   bool have_rs = false;
   int factor_precision = MFGPU_PRECISION_FP64;
   DevBuf b_li, b_lx, b_ui, b_ux;
   // solve state
   SolveSchedule sched;
   DevBuf b_fsol, b_b, b_x, b_r, b_d, b_err, b_norm;   // b_fsol: solve arena (blocks, then x)
-  // persistent solve: one cooperative launch per pass (false: one launch per step)
-  bool persistent = false;
+  // persistent solve: one cooperative launch per pass instead of one launch
+  // per step, when the options ask for it (slower than per-step launches on
+  // every measured case, many or few right-hand sides)
+  int persistent_mode = 0;     // 0 default (per step), 1 persistent, 2 per step
+  int lean_mode = 0;           // front layout: 0 by size, 1 always lean
+  bool persistent = false;     // the mode resolved for the current solve
   int persist_grid[2] = {0, 0};          // CTAs of the persistent kernel, FP32 / FP64
   DevBuf b_bar, b_stamps;                // barrier words {count, gen, err, sticky err}; profiling stamps
   struct PhaseProfile {                  // one profiled persistent launch
@@ -266,6 +276,8 @@ void upload_plan(mfgpu_ctx* h) {
   upload(h->b_csr_src, P.csr_src, st);
   upload(h->b_dinv_off, P.dinv_off, st);
   upload(h->b_inv_off, P.inv_off, st);
+  upload(h->b_lpan_off, P.lpan_off, st);
+  upload(h->b_u12_off, P.u12_off, st);
   upload(h->b_inv_blocks, P.inv_blocks, st);
   upload(h->b_inv_tasks, P.inv_tasks, st);
   upload(h->b_inv_tasks_tc, P.inv_tasks_tc, st);
@@ -300,6 +312,9 @@ void upload_plan(mfgpu_ctx* h) {
   d.csr_src = h->b_csr_src.as<int32_t>();
   d.dinv_off = h->b_dinv_off.as<int64_t>();
   d.inv_off = h->b_inv_off.as<int64_t>();
+  d.lpan_off = h->b_lpan_off.as<int64_t>();
+  d.u12_off = h->b_u12_off.as<int64_t>();
+  d.lean = P.lean ? 1 : 0;
 }
 
 void upload_launches(mfgpu_ctx* h) {
@@ -422,6 +437,8 @@ void configure_kernels() {
   CK(cudaFuncSetAttribute(k_panel_apply<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem_bytes<T>()));
   CK(cudaFuncSetAttribute(k_gemm_tc<128, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)TcCfg<128, 3>::kSmem));
+  CK(cudaFuncSetAttribute(k_gemm_bx3<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)BxCfg<128, 2>::kSmem));
   CK(cudaFuncSetAttribute(k_solve_persistent<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)persistent_smem_bytes<T>()));
   done = true;
@@ -452,6 +469,18 @@ bool gemm_use_tc(const mfgpu_ctx* h, int64_t id, bool dflt) {
   if (!h->use_tc) return false;
   if (id >= 0 && id < (int64_t)h->gemm_choice.size() && h->gemm_choice[id]) return h->gemm_choice[id] == 1;
   return dflt;
+}
+
+// One tensor-core GEMM launch over 128 x 128-tiled tasks: BF16x3 (default)
+// or 3xTF32 (MFGPU_FLAG_TF32_SPLIT).
+void launch_tc(const mfgpu_ctx* h, const GemmTask* tasks, int64_t count, int64_t tiles, const float* pa,
+               const float* pb, float* pc, cudaStream_t st) {
+  if (h->tc_bf16x3)
+    k_gemm_bx3<128, 2><<<(unsigned)tiles, kBxThreads, BxCfg<128, 2>::kSmem, st>>>(tasks, (int)count, pa, pb, pc,
+                                                                                  h->b_flags.as<int>());
+  else
+    k_gemm_tc<128, 3><<<(unsigned)tiles, kTcThreads, TcCfg<128, 3>::kSmem, st>>>(tasks, (int)count, pa, pb, pc,
+                                                                                h->b_flags.as<int>());
 }
 
 // Tunable-launch ids: factor GEMM launches first, then the inversion steps,
@@ -504,13 +533,17 @@ void run_factor_launches(mfgpu_ctx* h) {
               h->dp, S, h->b_trsm.as<TrsmTask>() + L.first, (int)L.count, pool, h->b_dinv.as<T>());
         }, L.level, L.tiles);
         break;
+      case kLaunchCopyPanels:
+        klaunch(h, KC_COPY_PANELS, 0, bytes, [&] {
+          k_copy_panels<T><<<grid1(L.count, 8), 256, 0, st>>>(h->dp, L.first, L.count, pool);
+        }, L.level, L.count);
+        break;
       case kLaunchGemm:
         h->cur_tune = (int32_t)tune_id;
         if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, true))
           klaunch(h, KC_GEMM_FACTOR, L.flops, bytes, [&] {
-            k_gemm_tc<128, 3><<<(unsigned)L.tiles_tc, kTcThreads, TcCfg<128, 3>::kSmem, st>>>(
-                h->b_gemm_tc.as<GemmTask>() + L.first, (int)L.count, (const float*)pool, (const float*)pool,
-                (float*)pool, h->b_flags.as<int>());
+            launch_tc(h, h->b_gemm_tc.as<GemmTask>() + L.first, L.count, L.tiles_tc, (const float*)pool,
+                      (const float*)pool, (float*)pool, st);
           }, L.level, L.tiles_tc);
         else
           klaunch(h, KC_GEMM_FACTOR, L.flops, bytes, [&] {
@@ -584,9 +617,8 @@ void issue_inverses(mfgpu_ctx* h) {
     h->cur_tune = (int32_t)tune_id;
     if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, true))
       klaunch(h, KC_INVERSE, is.flops, is.elems * sizeof(T), [&] {
-        k_gemm_tc<128, 3><<<(unsigned)is.tiles_tc, kTcThreads, TcCfg<128, 3>::kSmem, st>>>(
-            h->b_inv_tasks_tc.as<GemmTask>() + is.first, (int)is.count, (const float*)pool, (const float*)pool,
-            (float*)pool, h->b_flags.as<int>());
+        launch_tc(h, h->b_inv_tasks_tc.as<GemmTask>() + is.first, is.count, is.tiles_tc, (const float*)pool,
+                  (const float*)pool, (float*)pool, st);
       }, -3, is.tiles_tc);
     else
       klaunch(h, KC_INVERSE, is.flops, is.elems * sizeof(T), [&] {
@@ -645,7 +677,7 @@ int factor_impl(mfgpu_ctx* h, int32_t check) {
         (uintptr_t)h->b_ax.p, (uintptr_t)h->b_rs.p, (uintptr_t)h->b_dinv.p, (uintptr_t)h->b_li.p,
         (uintptr_t)h->b_lx.p, (uintptr_t)h->b_ui.p, (uintptr_t)h->b_ux.p, (uintptr_t)h->b_small.p,
         (uintptr_t)h->b_panel.p, (uintptr_t)h->b_trsm.p, (uintptr_t)h->b_gemm.p, (uintptr_t)h->b_ipiv.p,
-        (uintptr_t)h->b_gemm_tc.p, (uintptr_t)h->use_tc, (uintptr_t)h->choice_version,
+        (uintptr_t)h->b_gemm_tc.p, (uintptr_t)h->use_tc, (uintptr_t)h->tc_bf16x3, (uintptr_t)h->choice_version,
         (uintptr_t)h->b_info.p, (uintptr_t)h->b_flags.p, (uintptr_t)st};
     run_sequence(h, h->factor_key, h->factor_exec, h->factor_nodes, key, [&] { issue_factor<T>(h); });
     if (!P.has_speculative) break;
@@ -806,7 +838,7 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
       for (int32_t i = m; i < e; ++i) {
         const int32_t s = P.slot_super[i];
         const int nf = P.nf[s], np = P.np[s];
-        add_gemm(gw, kGemmSub, P.front_off[s] + np, nf, xw0 + P.c1[s], n, P.colbase[s] * R + np, nf, P.nu[s],
+        add_gemm(gw, kGemmSub, P.lpan_off[s] + np, nf, xw0 + P.c1[s], n, P.colbase[s] * R + np, nf, P.nu[s],
                  (int)R, np);
       }
       push(gw);
@@ -824,8 +856,8 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
       for (int32_t i = m; i < e; ++i) {
         const int32_t s = P.slot_super[i];
         const int nf = P.nf[s], np = P.np[s];
-        add_gemm(gg, kGemmFrom, P.front_off[s] + (int64_t)np * nf, nf, P.colbase[s] * R + np, nf,
-                 P.colbase[s] * R, nf, np, (int)R, P.nu[s], xw0 + P.c1[s], n);
+        add_gemm(gg, kGemmFrom, P.u12_off[s], u12_ld(P, s), P.colbase[s] * R + np, nf, P.colbase[s] * R, nf, np,
+                 (int)R, P.nu[s], xw0 + P.c1[s], n);
       }
       push(gg);
       SolveSchedule::Step gx = gemm_step();
@@ -846,6 +878,34 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
       S.steps.push_back(st);
     }
   }
+  // split-K form of the GEMM steps for few right-hand sides
+  constexpr int32_t kSkinnyMinK = 512;
+  if (R <= kSkinnyMaxN) {
+    const int nmax = R <= 1 ? 1 : (R <= 4 ? 4 : kSkinnyMaxN);
+    for (auto& st : S.steps) {
+      if (st.kind != 3) continue;
+      // split-K pays only when some task walks a long K
+      int32_t maxk = 0;
+      for (int64_t i = st.first; i < st.first + st.count; ++i) maxk = std::max(maxk, S.gemms[i].k);
+      if (maxk < kSkinnyMinK) continue;
+      st.sk_first = (int64_t)S.skinny.size();
+      for (int64_t i = st.first; i < st.first + st.count; ++i) {
+        const GemmTask& g = S.gemms[i];
+        SkinnyTask t{};
+        t.a = g.a; t.b = g.b; t.c = g.c; t.d = g.d;
+        t.m = g.m; t.n = g.n; t.k = g.k; t.lda = g.lda; t.ldb = g.ldb; t.ldc = g.ldc; t.ldd = g.ldd; t.mode = g.mode;
+        t.rblocks = (int32_t)ceil_div(g.m, kSkinnyRows);
+        t.kchunks = (int32_t)std::max<int64_t>(1, ceil_div(g.k, kSkinnyKC));
+        t.part_base = st.sk_parts;
+        t.red_base = st.sk_reds;
+        st.sk_parts += (int64_t)t.rblocks * t.kchunks;
+        st.sk_reds += t.rblocks;
+        S.skinny.push_back(t);
+      }
+      st.sk_count = (int64_t)S.skinny.size() - st.sk_first;
+      S.skinny_scratch = std::max<int64_t>(S.skinny_scratch, st.sk_parts * kSkinnyRows * nmax);
+    }
+  }
   // the same steps as phases of the persistent kernel (kSolveThreads per CTA:
   // kSolveThreads / 32 right-hand sides per gather item)
   const int64_t ych = ceil_div(R, kSolveCols), wch = ceil_div(R, kSolveThreads / 32);
@@ -862,6 +922,7 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
   upload(S.d_ids, S.ids, h->stream);
   upload(S.d_gemms, S.gemms, h->stream);
   upload(S.d_gemms_tc, S.gemms_tc, h->stream);
+  upload(S.d_skinny, S.skinny, h->stream);
   upload(S.d_phases, S.phases, h->stream);
 }
 
@@ -870,9 +931,11 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
 template <typename T>
 void prepare_solve(mfgpu_ctx* h, int64_t R, int refine) {
   const Plan& P = h->plan;
+  h->persistent = h->persistent_mode == 1;
   build_solve_schedule(h, R);
   // solve arena: the per-supernode blocks, then x in factor order
   h->b_fsol.ensure(std::max<size_t>((size_t)(P.fc_total + P.n) * R * sizeof(T), 16));
+  if (h->sched.skinny_scratch) h->b_skinny.ensure((size_t)h->sched.skinny_scratch * sizeof(T));
   if (refine > 0) h->b_r.ensure(std::max<size_t>((size_t)P.n * R * 8, 16));
   configure_kernels<T>();
   if (h->persistent) {
@@ -944,11 +1007,27 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
         break;
       case 3:
         h->cur_tune = (int32_t)tune_id;
-        if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, R >= 64))
+        if (s.sk_count && !(sizeof(T) == 4 && gemm_use_tc(h, tune_id, false)))
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
-            k_gemm_tc<128, 3><<<(unsigned)s.tiles_tc, kTcThreads, TcCfg<128, 3>::kSmem, st>>>(
-                S.d_gemms_tc.as<GemmTask>() + s.first, (int)s.count, (const float*)pool, (const float*)fsol,
-                (float*)fsol, h->b_flags.as<int>());
+            const SkinnyTask* sk = S.d_skinny.as<SkinnyTask>() + s.sk_first;
+            T* part = h->b_skinny.as<T>();
+            if (R <= 1) {
+              k_skinny_part<T, 1><<<(unsigned)s.sk_parts, kSkinnyRows, 0, st>>>(sk, (int)s.sk_count, pool, fsol, part);
+              k_skinny_reduce<T, 1><<<(unsigned)s.sk_reds, kSkinnyRows, 0, st>>>(sk, (int)s.sk_count, part, fsol);
+            } else if (R <= 4) {
+              k_skinny_part<T, 4><<<(unsigned)s.sk_parts, kSkinnyRows, 0, st>>>(sk, (int)s.sk_count, pool, fsol, part);
+              k_skinny_reduce<T, 4><<<(unsigned)s.sk_reds, kSkinnyRows, 0, st>>>(sk, (int)s.sk_count, part, fsol);
+            } else {
+              k_skinny_part<T, kSkinnyMaxN><<<(unsigned)s.sk_parts, kSkinnyRows, 0, st>>>(sk, (int)s.sk_count, pool,
+                                                                                         fsol, part);
+              k_skinny_reduce<T, kSkinnyMaxN><<<(unsigned)s.sk_reds, kSkinnyRows, 0, st>>>(sk, (int)s.sk_count, part,
+                                                                                           fsol);
+            }
+          }, -1, s.sk_parts);
+        else if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, R >= 64))
+          klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
+            launch_tc(h, S.d_gemms_tc.as<GemmTask>() + s.first, s.count, s.tiles_tc, (const float*)pool,
+                      (const float*)fsol, (float*)fsol, st);
           }, -1, s.tiles_tc);
         else
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
@@ -1007,7 +1086,8 @@ void solve_graph(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double
       (uintptr_t)h->have_rs, (uintptr_t)h->b_rs.p, (uintptr_t)h->b_pool.p, (uintptr_t)h->b_dinv.p,
       (uintptr_t)h->b_fsol.p, (uintptr_t)h->b_inv_tasks.p, (uintptr_t)h->b_r.p, (uintptr_t)h->b_ax.p,
       (uintptr_t)S.d_ids.p, (uintptr_t)S.d_gemms.p, (uintptr_t)S.d_phases.p, (uintptr_t)h->b_prow.p,
-      (uintptr_t)S.d_gemms_tc.p, (uintptr_t)h->use_tc, (uintptr_t)h->choice_version,
+      (uintptr_t)S.d_gemms_tc.p, (uintptr_t)S.d_skinny.p, (uintptr_t)h->b_skinny.p, (uintptr_t)h->use_tc, (uintptr_t)h->tc_bf16x3, (uintptr_t)h->choice_version,
+      (uintptr_t)h->persistent, (uintptr_t)h->b_bar.p,
       (uintptr_t)h->b_rowfac.p, (uintptr_t)h->stream};
   if (!h->solve_graphs) {
     solve_refine<T>(h, R, d_b, ldb, d_x, ldx, refine, true);
@@ -1048,6 +1128,12 @@ int analyze_common(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const int64_t
                    const int64_t* upd_idx) {
   auto t0 = std::chrono::steady_clock::now();
   build_plan(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, h->plan);
+  // all fronts resident when they fit comfortably (FP64 worst case), else
+  // working fronts placed by lifetime and a compact panel pool
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b));
+  if (h->lean_mode == 1 || (h->lean_mode == 0 && (double)h->plan.front_elems_full * 8.0 > 0.45 * (double)total_b))
+    set_layout(h->plan, true);
   upload_plan(h);
   upload_launches(h);
   h->launches_safe = false;
@@ -1087,7 +1173,9 @@ int mfgpu_create(const mfgpu_options* opts, mfgpu_ctx** out) {
     h->device = opts->device;
     h->precision = opts->precision;
     h->use_tc = !(opts->flags & MFGPU_FLAG_NO_TENSOR_CORES);
-    h->persistent = (opts->flags & MFGPU_FLAG_PERSISTENT_SOLVE) != 0;
+    h->persistent_mode = (opts->flags & MFGPU_FLAG_PERSISTENT_SOLVE) ? 1 : (opts->flags & MFGPU_FLAG_STEP_SOLVE) ? 2 : 0;
+    h->tc_bf16x3 = !(opts->flags & MFGPU_FLAG_TF32_SPLIT);
+    h->lean_mode = (opts->flags & MFGPU_FLAG_LEAN_FRONTS) ? 1 : 0;
   }
   int rc = guarded(h, [&]() -> int {
     int ndev = 0;
@@ -1123,7 +1211,8 @@ void mfgpu_destroy(mfgpu_ctx* h) {
                     &h->b_lcolptr, &h->b_ucolptr, &h->b_qf, &h->b_csr_ptr, &h->b_csr_col, &h->b_csr_src,
                     &h->b_small, &h->b_panel, &h->b_trsm, &h->b_gemm, &h->b_gemm_tc, &h->b_pool, &h->b_vx, &h->b_ax, &h->b_rs,
                     &h->b_ipiv, &h->b_info, &h->b_prow, &h->b_rowfac, &h->b_flags, &h->b_dinv, &h->b_dinv_off,
-                    &h->b_inv_off, &h->b_inv_blocks, &h->b_inv_tasks, &h->b_inv_tasks_tc,
+                    &h->b_inv_off, &h->b_inv_blocks, &h->b_inv_tasks, &h->b_inv_tasks_tc, &h->b_lpan_off,
+                    &h->b_u12_off, &h->b_skinny, &h->sched.d_skinny,
                     &h->b_li, &h->b_lx, &h->b_ui,
                     &h->b_ux, &h->b_fsol, &h->b_b, &h->b_x, &h->b_r, &h->b_d, &h->b_err, &h->b_norm,
                     &h->sched.d_ids, &h->sched.d_gemms, &h->sched.d_gemms_tc, &h->sched.d_phases, &h->b_bar,
@@ -1430,13 +1519,14 @@ int mfgpu_stats_json(mfgpu_ctx* h, char* buf, int64_t cap) {
                 "\"factor_launches\": %lld, \"small_fronts\": %lld, \"speculative\": %s, \"safe_rerun\": %d, "
                 "\"analyze_ms\": %.3f, \"factor_ms\": %.3f, \"solve_ms\": %.3f, \"precision\": \"%s\", "
                 "\"status\": %d, \"growth\": %.6e, \"growth_limit\": %.6e, \"refactored_fp64\": %s, "
-                "\"flops_inverse\": %.6e}",
+                "\"flops_inverse\": %.6e, \"lean\": %s, \"pool_elems\": %lld, \"front_elems_full\": %lld}",
                 (long long)P.n, (long long)P.ns, P.nlevels, (long long)P.nnz_l, (long long)P.nnz_u, P.max_nf,
                 P.max_np, (long long)P.front_elems, P.flops, P.flops_getrf, P.flops_trsm, P.flops_gemm,
                 P.assembly_bytes_per_elem, (long long)nl, (long long)nsmall, P.has_speculative ? "true" : "false",
                 h->factor_reruns, h->t_analyze_ms, h->t_factor_ms, h->t_solve_ms,
                 h->factor_precision == MFGPU_PRECISION_MIXED ? "mixed" : "fp64", h->last_status, h->growth,
-                h->growth_limit, h->refactored_fp64 ? "true" : "false", P.flops_inverse);
+                h->growth_limit, h->refactored_fp64 ? "true" : "false", P.flops_inverse, P.lean ? "true" : "false",
+                (long long)P.pool_elems, (long long)P.front_elems_full);
   std::string js(tmp);
   js.pop_back();   // reopen the object
   char item[512];

@@ -3,6 +3,7 @@
 #include "plan.h"
 
 #include <algorithm>
+#include <map>
 #include <numeric>
 #include <stdexcept>
 
@@ -51,7 +52,7 @@ void build_inverse_steps(Plan& P) {
     for (int64_t s = 0; s < P.ns; ++s) {
       if (P.inv_off[s] < 0 || P.np[s] <= bs) continue;
       const int32_t npv = P.np[s], nf = P.nf[s];
-      const int64_t fo = P.front_off[s], li = P.inv_off[s], ui = li + (int64_t)npv * npv;
+      const int64_t fo = P.lpan_off[s], li = P.inv_off[s], ui = li + (int64_t)npv * npv;
       for (int64_t i = 0; i + bs < npv; i += 2 * bs) {
         const int32_t n1 = (int32_t)bs, n2 = (int32_t)std::min<int64_t>(bs, npv - i - bs);
         const int64_t i2 = i + bs;
@@ -353,22 +354,6 @@ void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const i
       P.dinv_blocks += ceil_div(P.np[s], kPanel);
     }
 
-  // ---- explicit pivot-block inverses (blocked triangular inversion) ---------
-  P.inv_off.assign(ns, -1);
-  P.inv_base = P.front_elems;
-  for (int64_t s = 0; s < ns; ++s)
-    if (P.nf[s] > kSmallFront) {
-      P.inv_off[s] = P.inv_base + P.inv_elems;
-      P.inv_elems += 2 * (int64_t)P.np[s] * P.np[s];
-      for (int32_t j = 0; j * kPanel < P.np[s]; ++j) {
-        P.inv_blocks.push_back((int32_t)s);
-        P.inv_blocks.push_back(j);
-      }
-    }
-  P.inv_scratch = P.inv_base + P.inv_elems;
-  build_inverse_steps(P);
-  P.pool_elems = P.inv_scratch + P.inv_scratch_elems;
-
   // ---- statistics ------------------------------------------------------------
   for (int64_t s = 0; s < ns; ++s) {
     const double a = P.np[s], u = P.nu[s];
@@ -383,6 +368,107 @@ void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const i
     P.assembly_bytes_per_elem += moves;
   }
   P.flops = P.flops_getrf + P.flops_trsm + P.flops_gemm;
+  P.front_elems_full = P.front_elems;
+  set_layout(P, false);
+}
+
+void set_layout(Plan& P, bool lean) {
+  const int64_t ns = P.ns;
+  P.lean = lean;
+  // ---- working fronts ---------------------------------------------------------
+  if (!lean) {
+    int64_t fo = 0;
+    for (int64_t i = 0; i < ns; ++i) {
+      const int32_t s = P.slot_super[i];
+      P.front_off[s] = fo;
+      fo += (int64_t)P.nf[s] * P.nf[s];
+    }
+    P.front_elems = fo;
+  } else {
+    // A front lives from its own level until the end of its parent's level
+    // (where the parent assembles its contribution block); roots until the
+    // end of their own level.  First fit over a free list, by level.
+    std::map<int64_t, int64_t> freel;   // offset -> size
+    int64_t end = 0;
+    std::vector<std::vector<int32_t>> dies(P.nlevels + 1);
+    for (int64_t s = 0; s < ns; ++s) {
+      const int32_t last = P.parent_super[s] >= 0 ? P.height[P.parent_super[s]] : P.height[s];
+      dies[last + 1].push_back((int32_t)s);
+    }
+    auto release = [&](int64_t off, int64_t sz) {
+      auto it = freel.emplace(off, sz).first;
+      auto nx = std::next(it);
+      if (nx != freel.end() && it->first + it->second == nx->first) {
+        it->second += nx->second;
+        freel.erase(nx);
+      }
+      if (it != freel.begin()) {
+        auto pv = std::prev(it);
+        if (pv->first + pv->second == it->first) {
+          pv->second += it->second;
+          freel.erase(it);
+        }
+      }
+    };
+    for (int32_t L = 0; L < P.nlevels; ++L) {
+      for (int32_t s : dies[L]) release(P.front_off[s], (int64_t)P.nf[s] * P.nf[s]);
+      for (int32_t i = P.level_slot[L]; i < P.level_slot[L + 1]; ++i) {
+        const int32_t s = P.slot_super[i];
+        const int64_t need = (int64_t)P.nf[s] * P.nf[s];
+        auto it = freel.begin();
+        while (it != freel.end() && it->second < need) ++it;
+        if (it == freel.end()) {
+          P.front_off[s] = end;
+          end += need;
+        } else {
+          P.front_off[s] = it->first;
+          const int64_t off = it->first + need, left = it->second - need;
+          freel.erase(it);
+          if (left > 0) freel.emplace(off, left);
+        }
+      }
+    }
+    P.front_elems = end;
+  }
+  // ---- panels -------------------------------------------------------------------
+  P.lpan_off.assign(ns, 0);
+  P.u12_off.assign(ns, 0);
+  P.panel_base = P.front_elems;
+  P.panel_elems = 0;
+  for (int64_t i = 0; i < ns; ++i) {
+    const int32_t s = P.slot_super[i];
+    const int64_t npv = P.np[s], nf = P.nf[s];
+    if (!lean) {
+      P.lpan_off[s] = P.front_off[s];
+      P.u12_off[s] = P.front_off[s] + npv * nf;
+    } else {
+      P.lpan_off[s] = P.panel_base + P.panel_elems;
+      P.u12_off[s] = P.lpan_off[s] + nf * npv;
+      P.panel_elems += nf * npv + npv * (nf - npv);
+    }
+  }
+  // ---- explicit pivot-block inverses (blocked triangular inversion) -------------
+  P.inv_off.assign(ns, -1);
+  P.inv_blocks.clear();
+  P.inv_tasks.clear();
+  P.inv_tasks_tc.clear();
+  P.inv_steps.clear();
+  P.flops_inverse = 0;
+  P.inv_elems = 0;
+  P.inv_scratch_elems = 0;
+  P.inv_base = P.panel_base + P.panel_elems;
+  for (int64_t s = 0; s < ns; ++s)
+    if (P.nf[s] > kSmallFront) {
+      P.inv_off[s] = P.inv_base + P.inv_elems;
+      P.inv_elems += 2 * (int64_t)P.np[s] * P.np[s];
+      for (int32_t j = 0; j * kPanel < P.np[s]; ++j) {
+        P.inv_blocks.push_back((int32_t)s);
+        P.inv_blocks.push_back(j);
+      }
+    }
+  P.inv_scratch = P.inv_base + P.inv_elems;
+  build_inverse_steps(P);
+  P.pool_elems = P.inv_scratch + P.inv_scratch_elems;
   build_launches(P, false);
 }
 
@@ -426,7 +512,7 @@ void push_gemm(Plan& P, Launch& lg, const GemmTask& g0) {
   ++lg.count;
 }
 
-void build_launches(Plan& P, bool safe) {
+void build_launches_core(Plan& P, bool safe) {
   P.small_tasks.clear();
   P.panel_tasks.clear();
   P.trsm_tasks.clear();
@@ -541,6 +627,39 @@ void build_launches(Plan& P, bool safe) {
     }
     if (lg.count) P.launches.push_back(lg);
   }
+}
+
+void add_copy_launches(Plan& P);
+
+void build_launches(Plan& P, bool safe) {
+  build_launches_core(P, safe);
+  add_copy_launches(P);
+}
+
+// Lean layout: after each level, its fronts' panels go to the panel pool.
+void add_copy_launches(Plan& P) {
+  if (!P.lean) return;
+  std::vector<Launch> out;
+  int32_t cur = -1;
+  auto flush = [&](int32_t L) {
+    const int32_t a = P.level_slot[L], e = P.level_slot[L + 1];
+    if (e <= a) return;
+    const int64_t fc0 = P.colbase[P.slot_super[a]];
+    const int64_t fc1 = P.colbase[P.slot_super[e - 1]] + P.nf[P.slot_super[e - 1]];
+    Launch c{kLaunchCopyPanels, L, fc0, fc1 - fc0, fc1 - fc0};
+    for (int32_t i = a; i < e; ++i) {
+      const int32_t s = P.slot_super[i];
+      c.elems += 2.0 * ((double)P.nf[s] * P.np[s] + (double)P.np[s] * P.nu[s]);
+    }
+    out.push_back(c);
+  };
+  for (const Launch& l : P.launches) {
+    if (cur >= 0 && l.level != cur) flush(cur);
+    cur = l.level;
+    out.push_back(l);
+  }
+  if (cur >= 0) flush(cur);
+  P.launches.swap(out);
 }
 
 }  // namespace mfgpu

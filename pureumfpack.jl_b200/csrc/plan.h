@@ -73,7 +73,8 @@ enum LaunchKind : int32_t {
   kLaunchAssemble = 1,   // column-wise assembly of large fronts (front-column range)
   kLaunchPanel = 2,
   kLaunchTrsm = 3,
-  kLaunchGemm = 4
+  kLaunchGemm = 4,
+  kLaunchCopyPanels = 5  // lean layout: copy the level's factored panels to the panel pool (front-column range)
 };
 
 struct Launch {
@@ -109,8 +110,19 @@ struct Plan {
   std::vector<int32_t> fc_ch_ptr;     // children contributions (child, child column)
   std::vector<int32_t> fc_ch;         // pairs, flattened
   int64_t fc_total = 0;
-  int64_t front_elems = 0;              // fronts only; the pool also holds the pivot-block inverses
-  int64_t pool_elems = 0;               // fronts + inverses + inversion scratch
+  int64_t front_elems = 0;              // working fronts; the pool also holds panels (lean), inverses, scratch
+  int64_t front_elems_full = 0;         // sum of nf^2: every front resident at once
+  int64_t pool_elems = 0;               // fronts + panels + inverses + inversion scratch
+  // Factored panels, where the solves, the inversion and the CSC scatter read
+  // them: the first np columns of the front (leading dimension nf) at
+  // lpan_off[s], U12 (np x nu) at u12_off[s] with leading dimension u12 ld =
+  // lean ? np : nf.  Without `lean` these point into the resident fronts;
+  // with it the fronts' memory is reused once their parent has assembled
+  // their contribution block, and every factored front copies its panel to a
+  // compact panel pool at the end of its level.
+  bool lean = false;
+  std::vector<int64_t> lpan_off, u12_off;
+  int64_t panel_base = 0, panel_elems = 0;
   // levels / slots
   int32_t nlevels = 0;
   std::vector<int32_t> slot_super;
@@ -160,5 +172,13 @@ void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const i
 
 // (Re)build the launch sequence: speculative panels, or only pivoting ones.
 void build_launches(Plan& plan, bool safe);
+
+// Choose the memory layout: every front resident (lean = false), or working
+// fronts placed by lifetime with a compact panel pool (lean = true).  Sets
+// front offsets, panel offsets, the inverses' layout and steps, the pool
+// size, and rebuilds the launch sequence.
+void set_layout(Plan& plan, bool lean);
+
+inline int32_t u12_ld(const Plan& P, int32_t s) { return P.lean ? P.np[s] : P.nf[s]; }
 
 }  // namespace mfgpu

@@ -46,6 +46,9 @@ PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 FLAG_NO_TENSOR_CORES = 1   # mfgpu_options.flags: SIMT FP32 Schur updates in the mixed form
 FLAG_PERSISTENT_SOLVE = 2  # mfgpu_options.flags: one persistent cooperative launch per solve pass
+FLAG_TF32_SPLIT = 4        # mfgpu_options.flags: 3xTF32 instead of BF16x3 tensor-core products
+FLAG_STEP_SOLVE = 8        # mfgpu_options.flags: one launch per solve step, whatever the rhs count
+FLAG_LEAN_FRONTS = 16      # mfgpu_options.flags: reuse front memory by lifetime (compact panel pool)
 
 
 class ArgumentError(ValueError):
@@ -212,9 +215,13 @@ class GpuContext:
     """One libmfgpu handle: analysis, resident factors, solves."""
 
     def __init__(self, device: int = 0, precision: int = PRECISION_FP64, tensor_cores: bool = True,
-                 persistent_solve: bool = False):
+                 persistent_solve: bool | None = None, tf32_split: bool = False, lean_fronts: bool = False):
+        """persistent_solve: True / False forces the solve mode; None lets the
+        library choose by right-hand-side count."""
         self._lib = L.lib()
-        flags = (0 if tensor_cores else FLAG_NO_TENSOR_CORES) | (FLAG_PERSISTENT_SOLVE if persistent_solve else 0)
+        flags = ((0 if tensor_cores else FLAG_NO_TENSOR_CORES) | (FLAG_TF32_SPLIT if tf32_split else 0)
+                 | {None: 0, True: FLAG_PERSISTENT_SOLVE, False: FLAG_STEP_SOLVE}[persistent_solve]
+                 | (FLAG_LEAN_FRONTS if lean_fronts else 0))
         opts = L.MfOptions(device, precision, flags, 0)
         h = ctypes.c_void_p()
         rc = self._lib.mfgpu_create(ctypes.byref(opts), ctypes.byref(h))

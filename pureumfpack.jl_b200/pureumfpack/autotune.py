@@ -139,13 +139,17 @@ def measure(ctx: GpuContext, run, count: int, choice, repeats: int = 2) -> np.nd
     return best
 
 
+def rule_choice(feats: np.ndarray, nrhs: int) -> np.ndarray:
+    """The built-in rule: tcgen05 everywhere, solve products from 64 rhs."""
+    return np.where(feats[:, 2] > 0, np.where(nrhs >= 64, 1, 2), 1)
+
+
 def exhaustive_table(ctx: GpuContext, run, nrhs: int, repeats: int = 2) -> LaunchTable:
     feats = tune_features(ctx, nrhs)
     count = len(feats)
     times = np.stack([measure(ctx, run, count, np.full(count, v), repeats) for v in VARIANTS], axis=1)
     set_choice(ctx, [])
-    rule = np.where(feats[:, 2] > 0, np.where(nrhs >= 64, 1, 2), 1)
-    return LaunchTable(feats, times, rule)
+    return LaunchTable(feats, times, rule_choice(feats, nrhs))
 
 
 def _design(feats: np.ndarray):
@@ -169,8 +173,18 @@ class Tuner:
         y = self.model.predict(X) * self.ysd + self.ymu
         return (10.0 ** y).reshape(-1, 2)
 
-    def choose(self, feats: np.ndarray) -> np.ndarray:
-        return 1 + np.argmin(self.predict_ms(feats), axis=1)
+    def choose(self, feats: np.ndarray, rule=None, margin: float = 0.1) -> np.ndarray:
+        """Variant per launch: the model's faster variant, but with a rule
+        given, only where the model predicts at least `margin` of gain over
+        the rule's variant (mispredictions near the crossover cost little)."""
+        t = self.predict_ms(feats)
+        best = 1 + np.argmin(t, axis=1)
+        if rule is None:
+            return best
+        rule = np.asarray(rule)
+        idx = np.arange(len(rule))
+        gain = 1.0 - t[idx, best - 1] / t[idx, rule - 1]
+        return np.where(gain >= margin, best, rule)
 
 
 def train(tables, hidden: int = 32, iters: int = 3000, lr: float = 3e-3, seed: int = 0, device: int = 0) -> Tuner:
@@ -188,7 +202,7 @@ def train(tables, hidden: int = 32, iters: int = 3000, lr: float = 3e-3, seed: i
 def judge(tuner: Tuner, table: LaunchTable) -> dict:
     """The model's schedule against the exhaustive table (best per launch) and
     the built-in rule, all costed with the table's measured times."""
-    choice = tuner.choose(table.feats)
+    choice = tuner.choose(table.feats, table.rule)
     return {"launches": int(len(choice)), "mispredicted": int(np.sum(choice != table.best)),
             "model_ms": table.cost(choice), "table_ms": table.cost(table.best), "rule_ms": table.cost(table.rule),
             "choice": choice}

@@ -33,10 +33,10 @@ def _eta(A, x, b):
     return float(np.max(np.abs(r).max(axis=0) / (anorm * np.abs(x).max(axis=0) + np.abs(b).max(axis=0))))
 
 
-def _mixed_factors(A, tensor_cores):
+def _mixed_factors(A, tensor_cores, tf32_split=False):
     S = symbolic_mf(A)
     Rs = row_scaling(A, SCALE_SUM)
-    ctx = GpuContext(precision=PRECISION_MIXED, tensor_cores=tensor_cores)
+    ctx = GpuContext(precision=PRECISION_MIXED, tensor_cores=tensor_cores, tf32_split=tf32_split)
     ctx.analyze(A, S)
     assert ctx.factor(A.nzval, Rs, True) == 0
     return ctx.factors()
@@ -46,12 +46,13 @@ CASES = [("poisson3d-20", lambda: M.poisson3d(20)), ("convdiff-14", lambda: M.co
          ("poisson2d-100", lambda: M.poisson2d(100))]
 
 
-@pytest.mark.parametrize("tensor_cores", [True, False], ids=["tcgen05", "simt"])
+@pytest.mark.parametrize("tensor_cores,tf32_split", [(True, False), (True, True), (False, False)],
+                         ids=["bf16x3", "3xtf32", "simt"])
 @pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
-def test_mixed_factors_match_fp64_oracle(name, make, tensor_cores):
+def test_mixed_factors_match_fp64_oracle(name, make, tensor_cores, tf32_split):
     A = make()
     fo = O.splu(A, scale=int(SCALE_SUM)).F
-    L, U, p, q, pinv = _mixed_factors(A, tensor_cores)
+    L, U, p, q, pinv = _mixed_factors(A, tensor_cores, tf32_split)
     np.testing.assert_array_equal(L.colptr, fo.Lcolptr)
     np.testing.assert_array_equal(L.rowval, fo.Lrowval)
     np.testing.assert_array_equal(U.rowval, fo.Urowval)
@@ -61,9 +62,10 @@ def test_mixed_factors_match_fp64_oracle(name, make, tensor_cores):
     assert nl <= MIXED_RTOL and nu <= MIXED_RTOL, (nl, nu)
 
 
-def test_tensor_core_and_simt_updates_agree():
+@pytest.mark.parametrize("tf32_split", [False, True], ids=["bf16x3", "3xtf32"])
+def test_tensor_core_and_simt_updates_agree(tf32_split):
     A = M.poisson3d(22)
-    Lt, Ut = _mixed_factors(A, True)[:2]
+    Lt, Ut = _mixed_factors(A, True, tf32_split)[:2]
     Ls, Us = _mixed_factors(A, False)[:2]
     nl, _ = column_value_errors(Ls.colptr, Ls.nzval, Lt.nzval)
     nu, _ = column_value_errors(Us.colptr, Us.nzval, Ut.nzval)
