@@ -329,10 +329,30 @@ def roofline_of(P, primary, torch, dev, peaks):
         achieved = kd["bytes"] / (kd["ms"] * 1e-3) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback"}
+    traffic, tnote = None, None
+    ratio = gemm_traffic_ratio()
+    if dom == "gemm_factor" and primary == "fp64" and ratio is not None:
+        traffic = ratio * kd["bytes"] / max(kd["launches"], 1)
+        tnote = ("DRAM bytes per launch: ncu dram__bytes_read+write of the factor updates at poisson3d-48 over their "
+                 f"algorithmic bytes ({ratio:.3f}, profiles/k_gemm_f64_poisson3d-48.md) x this class's algorithmic "
+                 "bytes per launch")
     roof.update({"kernel": dom, "launches": kd["launches"], "avg_launch_ms": per_launch_ms,
-                 "traffic": None, "note": "achieved = algorithmic work of the kernel class / its CUDA-event time "
-                                          "over one profiled step"})
+                 "traffic": traffic, "algorithmic_bytes_per_launch": kd["bytes"] / max(kd["launches"], 1),
+                 "note": "achieved = algorithmic work of the kernel class / its CUDA-event time over one profiled step"
+                         + (f"; traffic: {tnote}" if tnote else "")})
     return roof
+
+
+def gemm_traffic_ratio():
+    """DRAM traffic over algorithmic bytes of the FP64 factor updates, from the
+    committed ncu summary (None if absent)."""
+    try:
+        for line in open(os.path.join(ROOT, "profiles", "k_gemm_f64_poisson3d-48.md")):
+            if line.startswith("traffic_ratio"):
+                return float(line.split()[1])
+    except OSError:
+        pass
+    return None
 
 
 def main():
