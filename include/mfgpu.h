@@ -143,6 +143,12 @@ int mfgpu_analyze_symbolic(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const
 int mfgpu_factor(mfgpu_ctx* h, const double* nzval, const double* rs, int32_t check);
 /* Same with device pointers (inputs already resident in HBM). */
 int mfgpu_factor_device(mfgpu_ctx* h, const double* d_nzval, const double* d_rs, int32_t check);
+/* splu's row scaling and factorization in one call: Rs = row_scaling(A,
+ * scale) (MFGPU_SCALE_*) is computed on the device, bitwise equal to
+ * mfgpu_row_scaling, then Diagonal(Rs) * A is factored (src/interface.jl:
+ * 101-105).  mfgpu_get_row_scaling copies that Rs (n entries) to the host. */
+int mfgpu_factor_scaled(mfgpu_ctx* h, const double* nzval, int32_t scale, int32_t check);
+int mfgpu_get_row_scaling(mfgpu_ctx* h, double* rs);
 
 /* out3 = {n, nnz(L), nnz(U)} of the last factorization. */
 int mfgpu_factor_sizes(mfgpu_ctx* h, int64_t* out3);

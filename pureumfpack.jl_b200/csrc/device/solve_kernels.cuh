@@ -306,6 +306,24 @@ __global__ void __launch_bounds__(256) k_abs_max(const double* __restrict__ x, i
   }
 }
 
+// row_scaling(A, kind) (src/scaling.jl:92-115) on the device from A in CSR
+// (each row's entries in increasing column order, the order in which the
+// column-oriented host pass accumulates them, so the result is bitwise the
+// host's): SCALE_SUM 1 / sum |a_ij|, SCALE_MAX 1 / max |a_ij|, 1 for an
+// empty row or SCALE_NONE.
+__global__ void k_row_scaling(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ src,
+                              const double* __restrict__ ax, int kind, double* __restrict__ rs) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double acc = 0.0;
+  if (kind != 0)
+    for (int p = rp[i]; p < rp[i + 1]; ++p) {
+      const double v = fabs(ax[src[p]]);
+      acc = kind == 1 ? acc + v : (v > acc ? v : acc);
+    }
+  rs[i] = acc > 0 ? 1.0 / acc : 1.0;
+}
+
 // ||A||_inf = max row sum of |a_ij|.
 __global__ void k_norm_inf(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ src,
                            const double* __restrict__ ax, unsigned long long* __restrict__ out) {

@@ -121,6 +121,38 @@ struct SolveSchedule {
 
 }  // namespace
 
+// Page-locked host staging buffer (grows, never shrinks).
+struct PinnedBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  PinnedBuf() = default;
+  PinnedBuf(const PinnedBuf&) = delete;
+  PinnedBuf& operator=(const PinnedBuf&) = delete;
+  PinnedBuf& operator=(PinnedBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      cap = o.cap;
+      o.p = nullptr;
+      o.cap = 0;
+    }
+    return *this;
+  }
+  void ensure(size_t bytes) {
+    if (bytes <= cap) return;
+    release();
+    CK(cudaHostAlloc(&p, std::max<size_t>(bytes, 64), cudaHostAllocDefault));
+    cap = std::max<size_t>(bytes, 64);
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+  double* d() const { return static_cast<double*>(p); }
+  ~PinnedBuf() { release(); }
+};
+
 struct mfgpu_ctx {
   int device = 0;
   int precision = MFGPU_PRECISION_FP64;
@@ -177,7 +209,7 @@ struct mfgpu_ctx {
     std::vector<int64_t> off, nz_off;      // column and value offsets of every system (nsys + 1)
     std::vector<int64_t> colptr, rowval;   // the block-diagonal pattern, 1-based
     std::vector<int32_t> super_sys;        // system of every supernode
-    std::vector<double> nz, rs, b, x;      // host staging of the concatenated arrays
+    PinnedBuf nz, b, x;                    // pinned host staging of the concatenated arrays
     bool have_factors = false;             // global factors fetched for per-system slicing
     std::vector<int64_t> lcolptr, lrowval, ucolptr, urowval, p, q;
     std::vector<double> lnzval, unzval;
@@ -1305,6 +1337,43 @@ int mfgpu_factor_device(mfgpu_ctx* h, const double* d_nzval, const double* d_rs,
   });
 }
 
+int mfgpu_factor_scaled(mfgpu_ctx* h, const double* nzval, int32_t scale, int32_t check) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  if (!h->analyzed) return fail(h, MFGPU_ERR_STATE, "factor before analyze");
+  if (scale < MFGPU_SCALE_NONE || scale > MFGPU_SCALE_MAX) return fail(h, MFGPU_ERR_ARGUMENT, "bad scale kind");
+  if (h->plan.nnz_a && !nzval) return fail(h, MFGPU_ERR_ARGUMENT, "null values");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->device));
+    const Plan& P = h->plan;
+    h->b_ax.ensure(std::max<int64_t>(P.nnz_a, 1) * 8);
+    if (P.nnz_a) CK(cudaMemcpyAsync(h->b_ax.p, nzval, P.nnz_a * 8, cudaMemcpyHostToDevice, h->stream));
+    h->have_rs = scale != MFGPU_SCALE_NONE;
+    if (h->have_rs && P.n) {
+      h->b_rs.ensure(std::max<int64_t>(P.n, 1) * 8);
+      k_row_scaling<<<grid1(P.n, 256), 256, 0, h->stream>>>(P.n, h->b_csr_ptr.as<int32_t>(), h->b_csr_src.as<int32_t>(),
+                                                             h->b_ax.as<double>(), scale, h->b_rs.as<double>());
+      CK(cudaGetLastError());
+    }
+    return factor_dispatch(h, check);
+  });
+}
+
+int mfgpu_get_row_scaling(mfgpu_ctx* h, double* rs) {
+  if (!h || !rs) return MFGPU_ERR_ARGUMENT;
+  if (!h->factored) return fail(h, MFGPU_ERR_STATE, "no factorization");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->device));
+    const int64_t n = h->plan.n;
+    if (!h->have_rs) {
+      std::fill(rs, rs + n, 1.0);
+      return MFGPU_OK;
+    }
+    CK(cudaMemcpyAsync(rs, h->b_rs.p, n * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MFGPU_OK;
+  });
+}
+
 int mfgpu_factor(mfgpu_ctx* h, const double* nzval, const double* rs, int32_t check) {
   if (!h) return MFGPU_ERR_ARGUMENT;
   if (!h->analyzed) return fail(h, MFGPU_ERR_STATE, "factor before analyze");
@@ -1727,7 +1796,13 @@ extern "C" int mfgpu_batch_analyze(mfgpu_ctx* h, int64_t nsys, const int64_t* n,
     return fail(h, MFGPU_ERR_ARGUMENT, "batch: ordering must be MFGPU_ORDER_AMD or MFGPU_ORDER_COLAMD");
   return guarded(h, [&]() -> int {
     auto& B = h->batch;
-    B = mfgpu_ctx::Batch{};
+    B.nsys = 0;
+    B.off.clear();
+    B.nz_off.clear();
+    B.colptr.clear();
+    B.rowval.clear();
+    B.super_sys.clear();
+    B.have_factors = false;
     B.off.assign(nsys + 1, 0);
     B.nz_off.assign(nsys + 1, 0);
     for (int64_t i = 0; i < nsys; ++i) {
@@ -1799,20 +1874,14 @@ extern "C" int mfgpu_batch_factor(mfgpu_ctx* h, const double* const* nzval, int3
     return fail(h, MFGPU_ERR_ARGUMENT, "batch: bad values or scale kind");
   return guarded(h, [&]() -> int {
     const int64_t N = B.off[B.nsys];
-    B.nz.resize(std::max<int64_t>(B.nz_off[B.nsys], 1));
+    B.nz.ensure(std::max<int64_t>(B.nz_off[B.nsys], 1) * sizeof(double));
     for (int64_t i = 0; i < B.nsys; ++i) {
       const int64_t cnt = B.nz_off[i + 1] - B.nz_off[i];
       if (cnt && !nzval[i]) return fail(h, MFGPU_ERR_ARGUMENT, "batch: null values for system " + std::to_string(i + 1));
-      if (cnt) std::memcpy(B.nz.data() + B.nz_off[i], nzval[i], cnt * sizeof(double));
+      if (cnt) std::memcpy(B.nz.d() + B.nz_off[i], nzval[i], cnt * sizeof(double));
     }
-    const double* rs = nullptr;
-    if (scale != MFGPU_SCALE_NONE) {
-      B.rs.resize(N);
-      const int rc = mfgpu_row_scaling(N, B.colptr.data(), B.rowval.data(), B.nz.data(), scale, B.rs.data());
-      if (rc != MFGPU_OK) return fail(h, rc, "batch: row scaling failed");
-      rs = B.rs.data();
-    }
-    const int rc = mfgpu_factor(h, B.nz.data(), rs, 0);
+    (void)N;
+    const int rc = mfgpu_factor_scaled(h, B.nz.d(), scale, 0);   // row scaling computed on the device
     if (rc < 0) return rc;
     // per system: the first supernode (postorder) with a zero pivot
     std::vector<int64_t> st(B.nsys, 0);
@@ -1840,18 +1909,18 @@ extern "C" int mfgpu_batch_solve(mfgpu_ctx* h, int64_t nrhs, const double* const
   if (nrhs == 0) return MFGPU_OK;
   return guarded(h, [&]() -> int {
     const int64_t N = B.off[B.nsys];
-    B.b.resize(N * nrhs);
-    B.x.resize(N * nrhs);
+    B.b.ensure(N * nrhs * sizeof(double));
+    B.x.ensure(N * nrhs * sizeof(double));
     for (int64_t i = 0; i < B.nsys; ++i) {
       const int64_t o = B.off[i], ni = B.off[i + 1] - o;
       if (!b[i] || !x[i]) return fail(h, MFGPU_ERR_ARGUMENT, "batch: null rhs or solution for system " + std::to_string(i + 1));
-      for (int64_t k = 0; k < nrhs; ++k) std::memcpy(B.b.data() + k * N + o, b[i] + k * ni, ni * sizeof(double));
+      for (int64_t k = 0; k < nrhs; ++k) std::memcpy(B.b.d() + k * N + o, b[i] + k * ni, ni * sizeof(double));
     }
-    const int rc = mfgpu_solve(h, nrhs, B.b.data(), N, B.x.data(), N, refine);
+    const int rc = mfgpu_solve(h, nrhs, B.b.d(), N, B.x.d(), N, refine);
     if (rc != MFGPU_OK) return rc;
     for (int64_t i = 0; i < B.nsys; ++i) {
       const int64_t o = B.off[i], ni = B.off[i + 1] - o;
-      for (int64_t k = 0; k < nrhs; ++k) std::memcpy(x[i] + k * ni, B.x.data() + k * N + o, ni * sizeof(double));
+      for (int64_t k = 0; k < nrhs; ++k) std::memcpy(x[i] + k * ni, B.x.d() + k * N + o, ni * sizeof(double));
     }
     return MFGPU_OK;
   });

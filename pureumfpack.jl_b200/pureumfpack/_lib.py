@@ -43,6 +43,8 @@ SIGNATURES = [
     ("mfgpu_analyze_symbolic", ctypes.c_int, [vp, i64, i64p, i64p, vp]),
     ("mfgpu_factor", ctypes.c_int, [vp, f64p, f64p, i32]),
     ("mfgpu_factor_device", ctypes.c_int, [vp, vp, vp, i32]),
+    ("mfgpu_factor_scaled", ctypes.c_int, [vp, f64p, i32, i32]),
+    ("mfgpu_get_row_scaling", ctypes.c_int, [vp, f64p]),
     ("mfgpu_factor_sizes", ctypes.c_int, [vp, i64p]),
     ("mfgpu_get_factors", ctypes.c_int, [vp, i64p, i64p, f64p, i64p, i64p, f64p, i64p, i64p, i64p]),
     ("mfgpu_solve", ctypes.c_int, [vp, i64, f64p, i64, f64p, i64, i32]),

@@ -269,6 +269,17 @@ class GpuContext:
         rs = _f(Rs) if Rs is not None else None
         return self._check(self._lib.mfgpu_factor(self._h, L.ptr(_f(nzval), L.f64p), L.ptr(rs, L.f64p), int(check)))
 
+    def factor_scaled(self, nzval, scale, check: bool = True) -> int:
+        """Row scaling of kind ``scale`` computed on the device, then the
+        factorization of Diagonal(Rs) * A."""
+        return self._check(self._lib.mfgpu_factor_scaled(self._h, L.ptr(_f(nzval), L.f64p), int(scale), int(check)))
+
+    def row_scaling(self) -> np.ndarray:
+        """Rs of the last factorization (ones without scaling)."""
+        rs = np.empty(self.n)
+        self._check(self._lib.mfgpu_get_row_scaling(self._h, L.ptr(rs, L.f64p)))
+        return rs
+
     def factor_device(self, nzval_ptr: int, rs_ptr: int | None, check: bool = True) -> int:
         return self._check(self._lib.mfgpu_factor_device(self._h, ctypes.c_void_p(nzval_ptr),
                                                          ctypes.c_void_p(rs_ptr) if rs_ptr else None, int(check)))

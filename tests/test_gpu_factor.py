@@ -163,3 +163,25 @@ def test_doctest_known_answer():
     assert np.allclose(x, [0.6666666666666666, -0.3333333333333333], rtol=0, atol=1e-16)
     x = splu(A, method="multifrontal").ldiv(np.array([1.0, 0.0]))
     assert np.allclose(x, [0.6666666666666666, -0.3333333333333333], rtol=0, atol=1e-16)
+
+
+@pytest.mark.parametrize("scale", [SCALE_NONE, SCALE_SUM, SCALE_MAX])
+def test_device_row_scaling_is_bitwise_the_host_one(scale):
+    """mfgpu_factor_scaled computes Rs on the device in the host's summation
+    order: Rs and the factors equal the host-scaled factorization exactly."""
+    from pureumfpack import GpuContext, symbolic_mf
+
+    A = M.convdiff3d(9)
+    S = symbolic_mf(A)
+    Rs = row_scaling(A, scale)
+    host = GpuContext()
+    host.analyze(A, S)
+    assert host.factor(A.nzval, None if scale == SCALE_NONE else Rs, True) == 0
+    dev = GpuContext()
+    dev.analyze(A, S)
+    assert dev.factor_scaled(A.nzval, scale, True) == 0
+    np.testing.assert_array_equal(dev.row_scaling(), Rs if scale != SCALE_NONE else np.ones(A.n))
+    L0, U0 = host.factors()[:2]
+    L1, U1 = dev.factors()[:2]
+    np.testing.assert_array_equal(L1.nzval, L0.nzval)
+    np.testing.assert_array_equal(U1.nzval, U0.nzval)
