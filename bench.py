@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--solve-mode", default="auto", choices=["auto", "step", "persistent"],
                     help="solve launches: library default by rhs count, per step, or one persistent launch per pass")
+    ap.add_argument("--relax", action="store_true",
+                    help="relaxed amalgamation (opt-in; the factors then store explicit zeros)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="mixed form: keep the built-in GEMM variant rule instead of the learned autotuner")
     return ap.parse_args()
@@ -256,7 +258,8 @@ def workload_config(args, A):
     return {"workload": f"{args.workload} n={A.n} nnz={A.nnz()} nrhs={args.nrhs} {order.upper()} "
                         f"{'SCALE_MAX' if scale == 2 else 'SCALE_SUM'}, numeric factor + "
                         f"solve(refine) to normwise backward error <= 1e-14",
-            "nrhs": args.nrhs, "l2": "working set (fronts) larger than L2; no explicit flush",
+            "nrhs": args.nrhs, "relaxed_amalgamation": bool(getattr(args, "relax", False)),
+            "l2": "working set (fronts) larger than L2; no explicit flush",
             "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "1 GPU"}
 
 
@@ -380,7 +383,7 @@ def main():
     n, R = A.n, B.shape[1]
     t0 = time.perf_counter()
     order, scale = workload_setup(args.workload)
-    S = symbolic_mf(A, q=colamd_order(A) if order == "colamd" else None)
+    S = symbolic_mf(A, q=colamd_order(A) if order == "colamd" else None, relax=args.relax)
     Rs = row_scaling(A, scale)
     t_sym = time.perf_counter() - t0
 

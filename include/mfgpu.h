@@ -72,6 +72,13 @@ typedef struct mfgpu_symbolic mfgpu_symbolic;
 int mfgpu_symbolic_create(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* q,
                           mfgpu_symbolic** out);
 void mfgpu_symbolic_destroy(mfgpu_symbolic* sym);
+/* Opt-in relaxed amalgamation of the supernodes (no counterpart in the
+ * reference, which keeps fundamental supernodes, src/symbolic.jl:178-179): a
+ * supernode ending right before its parent merges into it when the merged
+ * supernode stays small or stores few extra zeros.  Fewer, larger fronts; the
+ * factors then store explicit zeros, so their structure is no longer the
+ * reference's. */
+int mfgpu_symbolic_relax(mfgpu_symbolic* sym);
 /* out4 = {n, nsuper, length(upd_idx), length(child_idx)} */
 int mfgpu_symbolic_sizes(const mfgpu_symbolic* sym, int64_t* out4);
 /* SymbolicMF fields (src/symbolic.jl:203-209), flattened, any pointer may be

@@ -108,6 +108,17 @@ int mfgpu_symbolic_create(int64_t n, const int64_t* colptr, const int64_t* rowva
 
 void mfgpu_symbolic_destroy(mfgpu_symbolic* sym) { delete sym; }
 
+int mfgpu_symbolic_relax(mfgpu_symbolic* sym) {
+  if (!sym) return MFGPU_ERR_ARGUMENT;
+  try {
+    mfgpu::relax_supernodes(sym->s);
+  } catch (const std::exception& e) {
+    g_host_error = e.what();
+    return MFGPU_ERR_INTERNAL;
+  }
+  return MFGPU_OK;
+}
+
 int mfgpu_symbolic_sizes(const mfgpu_symbolic* sym, int64_t* out4) {
   if (!sym || !out4) return MFGPU_ERR_ARGUMENT;
   const auto& s = sym->s;

@@ -603,6 +603,79 @@ SymbolicMF symbolic_mf(idx_t n, const idx_t* colptr, const idx_t* rowind, const 
   return S;
 }
 
+// Relaxed amalgamation (opt-in; the reference has none).  Supernodes are
+// taken bottom-up; a supernode whose columns end right before its parent's
+// (the parent's last child in postorder) merges into it when the merged
+// supernode stays small or the logical zeros it stores stay few (thresholds
+// in the style of CHOLMOD's nrelax / zrelax).  The merged supernode keeps the
+// parent's update set, which contains the child's, so every front of the
+// merged structure holds its children's contribution blocks; the child's
+// columns gain explicit zeros.
+void relax_supernodes(SymbolicMF& S) {
+  const idx_t ns = S.nsuper();
+  if (ns < 2) return;
+  std::vector<idx_t> sparent(ns, -1), gnp(ns), gnu(ns);
+  std::vector<double> gz(ns, 0.0);
+  for (idx_t s = 0; s < ns; ++s) {
+    const idx_t p = S.parent[S.sstart[s + 1] - 1];
+    sparent[s] = p == -1 ? -1 : S.super_of[p];
+    gnp[s] = S.sstart[s + 1] - S.sstart[s];
+    gnu[s] = S.upd_ptr[s + 1] - S.upd_ptr[s];
+  }
+  auto tri = [](double a, double u) { return a * (a + 1) / 2 + a * u; };
+  std::vector<char> merged(ns, 0);   // s merged into its parent
+  for (idx_t s = 0; s < ns; ++s) {
+    const idx_t p = sparent[s];
+    if (p < 0 || S.sstart[s + 1] != S.sstart[p]) continue;   // not adjacent to the parent
+    const double npc = (double)gnp[s], nuc = (double)gnu[s], npp = (double)gnp[p], nup = (double)gnu[p];
+    const double extra = npc * (npp + nup - nuc);
+    const double z = gz[s] + gz[p] + extra, tot = tri(npc + npp, nup);
+    const double npm = npc + npp, zf = tot > 0 ? z / tot : 0.0;
+    const bool ok = npm <= 4 || (npm <= 16 && zf < 0.8) || (npm <= 48 && zf < 0.1) || zf < 0.05;
+    if (!ok) continue;
+    merged[s] = 1;
+    gnp[p] += gnp[s];
+    gz[p] = z;
+  }
+  // rebuild the partition: a group ends at a supernode that is not merged
+  std::vector<idx_t> sstart, upd_ptr{0}, upd_idx;
+  std::vector<idx_t> group_of(ns);
+  idx_t first = 0;
+  for (idx_t s = 0; s < ns; ++s) {
+    group_of[s] = (idx_t)sstart.size();
+    if (merged[s]) continue;
+    sstart.push_back(S.sstart[first]);
+    upd_idx.insert(upd_idx.end(), S.upd_idx.begin() + S.upd_ptr[s], S.upd_idx.begin() + S.upd_ptr[s + 1]);
+    upd_ptr.push_back((idx_t)upd_idx.size());
+    first = s + 1;
+  }
+  sstart.push_back(S.n);
+  const idx_t ng = (idx_t)sstart.size() - 1;
+  S.sstart.swap(sstart);
+  S.upd_ptr.swap(upd_ptr);
+  S.upd_idx.swap(upd_idx);
+  for (idx_t g = 0; g < ng; ++g) {
+    const idx_t c2 = S.sstart[g + 1] - 1, nu = S.upd_ptr[g + 1] - S.upd_ptr[g];
+    for (idx_t j = S.sstart[g]; j <= c2; ++j) {
+      S.super_of[j] = g;
+      S.colcount[j] = (c2 - j) + nu;
+    }
+  }
+  std::vector<idx_t> nkids(ng + 1, 0);
+  for (idx_t g = 0; g < ng; ++g) {
+    const idx_t p = S.parent[S.sstart[g + 1] - 1];
+    if (p != -1) ++nkids[S.super_of[p] + 1];
+  }
+  S.child_ptr.assign(ng + 1, 0);
+  for (idx_t g = 0; g < ng; ++g) S.child_ptr[g + 1] = S.child_ptr[g] + nkids[g + 1];
+  S.child_idx.assign(S.child_ptr[ng], 0);
+  std::vector<idx_t> fill(S.child_ptr.begin(), S.child_ptr.end() - 1);
+  for (idx_t g = 0; g < ng; ++g) {
+    const idx_t p = S.parent[S.sstart[g + 1] - 1];
+    if (p != -1) S.child_idx[fill[S.super_of[p]]++] = g;
+  }
+}
+
 void factor_colptrs(const SymbolicMF& S, std::vector<idx_t>& lp, std::vector<idx_t>& up) {
   const idx_t n = S.n, ns = S.nsuper();
   lp.assign(n + 1, 0);

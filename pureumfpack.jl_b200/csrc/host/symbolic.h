@@ -56,6 +56,10 @@ struct SymbolicMF {
 // symbolic_mf(A; q): q (0-based) or nullptr for AMD.
 SymbolicMF symbolic_mf(idx_t n, const idx_t* colptr, const idx_t* rowind, const idx_t* q);
 
+// Opt-in relaxed amalgamation of the supernodes (changes the factors'
+// structure: merged columns store explicit zeros).
+void relax_supernodes(SymbolicMF& s);
+
 // _factor_colptrs: 0-based Lcolptr / Ucolptr (n+1 each).
 void factor_colptrs(const SymbolicMF& s, std::vector<idx_t>& lcolptr, std::vector<idx_t>& ucolptr);
 

@@ -18,6 +18,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/mfgpu.h"
@@ -120,6 +121,22 @@ struct SolveSchedule {
 };
 
 }  // namespace
+
+// Run body(i) for i in [0, n) on up to 16 host threads (contiguous ranges).
+template <typename F>
+void parallel_for(int64_t n, F&& body) {
+  const int64_t nt = std::min<int64_t>(n, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+  if (nt <= 1) {
+    for (int64_t i = 0; i < n; ++i) body(i);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int64_t t = 0; t < nt; ++t)
+    pool.emplace_back([&, t] {
+      for (int64_t i = n * t / nt; i < n * (t + 1) / nt; ++i) body(i);
+    });
+  for (auto& th : pool) th.join();
+}
 
 // Page-locked host staging buffer (grows, never shrinks).
 struct PinnedBuf {
@@ -1875,11 +1892,13 @@ extern "C" int mfgpu_batch_factor(mfgpu_ctx* h, const double* const* nzval, int3
   return guarded(h, [&]() -> int {
     const int64_t N = B.off[B.nsys];
     B.nz.ensure(std::max<int64_t>(B.nz_off[B.nsys], 1) * sizeof(double));
-    for (int64_t i = 0; i < B.nsys; ++i) {
+    for (int64_t i = 0; i < B.nsys; ++i)
+      if (B.nz_off[i + 1] > B.nz_off[i] && !nzval[i])
+        return fail(h, MFGPU_ERR_ARGUMENT, "batch: null values for system " + std::to_string(i + 1));
+    parallel_for(B.nsys, [&](int64_t i) {
       const int64_t cnt = B.nz_off[i + 1] - B.nz_off[i];
-      if (cnt && !nzval[i]) return fail(h, MFGPU_ERR_ARGUMENT, "batch: null values for system " + std::to_string(i + 1));
       if (cnt) std::memcpy(B.nz.d() + B.nz_off[i], nzval[i], cnt * sizeof(double));
-    }
+    });
     (void)N;
     const int rc = mfgpu_factor_scaled(h, B.nz.d(), scale, 0);   // row scaling computed on the device
     if (rc < 0) return rc;
@@ -1911,17 +1930,18 @@ extern "C" int mfgpu_batch_solve(mfgpu_ctx* h, int64_t nrhs, const double* const
     const int64_t N = B.off[B.nsys];
     B.b.ensure(N * nrhs * sizeof(double));
     B.x.ensure(N * nrhs * sizeof(double));
-    for (int64_t i = 0; i < B.nsys; ++i) {
-      const int64_t o = B.off[i], ni = B.off[i + 1] - o;
+    for (int64_t i = 0; i < B.nsys; ++i)
       if (!b[i] || !x[i]) return fail(h, MFGPU_ERR_ARGUMENT, "batch: null rhs or solution for system " + std::to_string(i + 1));
+    parallel_for(B.nsys, [&](int64_t i) {
+      const int64_t o = B.off[i], ni = B.off[i + 1] - o;
       for (int64_t k = 0; k < nrhs; ++k) std::memcpy(B.b.d() + k * N + o, b[i] + k * ni, ni * sizeof(double));
-    }
+    });
     const int rc = mfgpu_solve(h, nrhs, B.b.d(), N, B.x.d(), N, refine);
     if (rc != MFGPU_OK) return rc;
-    for (int64_t i = 0; i < B.nsys; ++i) {
+    parallel_for(B.nsys, [&](int64_t i) {
       const int64_t o = B.off[i], ni = B.off[i + 1] - o;
       for (int64_t k = 0; k < nrhs; ++k) std::memcpy(x[i] + k * ni, B.x.d() + k * N + o, ni * sizeof(double));
-    }
+    });
     return MFGPU_OK;
   });
 }

@@ -180,13 +180,18 @@ class SymbolicMF:
             self._h = None
 
 
-def symbolic_mf(A: SparseCSC, q=None) -> SymbolicMF:
+def symbolic_mf(A: SparseCSC, q=None, relax: bool = False) -> SymbolicMF:
+    """symbolic_mf(A; q) (src/symbolic.jl:211-226).  ``relax`` (not in the
+    reference) adds relaxed amalgamation: fewer, larger supernodes whose
+    factors store explicit zeros."""
     if A.m != A.n:
         raise DimensionMismatch("symbolic analysis requires a square matrix")
     lib = L.lib()
     h = ctypes.c_void_p()
     qa = _i(q) if q is not None else None
     _check_host(lib.mfgpu_symbolic_create(A.n, L.ptr(_i(A.colptr)), L.ptr(_i(A.rowval)), L.ptr(qa), ctypes.byref(h)))
+    if relax:
+        _check_host(lib.mfgpu_symbolic_relax(h))
     sz = np.empty(4, np.int64)
     lib.mfgpu_symbolic_sizes(h, L.ptr(sz))
     n, ns, nupd, nch = (int(v) for v in sz)
@@ -415,8 +420,8 @@ class PureLU:
         return solve(self, b)
 
 
-def _factor(A: SparseCSC, q, check: bool, Rs, device: int, precision: int):
-    S = symbolic_mf(A, q=q)
+def _factor(A: SparseCSC, q, check: bool, Rs, device: int, precision: int, relax: bool = False):
+    S = symbolic_mf(A, q=q, relax=relax)
     ctx = GpuContext(device=device, precision=precision)
     ctx.analyze(A, S)
     status = ctx.factor(A.nzval, Rs, check)
@@ -436,7 +441,7 @@ def multifrontal_lu(A: SparseCSC, q=None, tol=None, check: bool = True, device: 
 
 
 def splu(A: SparseCSC, method: str = "gplu", ordering: str = "amd", tol: float = 0.1, scale=SCALE_SUM,
-         check: bool = True, device: int = 0, precision: int = PRECISION_FP64) -> PureLU:
+         check: bool = True, device: int = 0, precision: int = PRECISION_FP64, relax: bool = False) -> PureLU:
     """splu(A; method, ordering, tol, scale, check) (src/interface.jl:93-120).
 
     ``method="multifrontal"`` is the path this library implements; as in the
@@ -450,7 +455,7 @@ def splu(A: SparseCSC, method: str = "gplu", ordering: str = "amd", tol: float =
     scale = ScaleKind(int(scale))
     if method == "multifrontal":
         Rs = row_scaling(A, scale)
-        ctx, S = _factor(A, None, check, None if scale == SCALE_NONE else Rs, device, precision)
+        ctx, S = _factor(A, None, check, None if scale == SCALE_NONE else Rs, device, precision, relax)
         return PureLU(ctx, Rs, A, S)
     if method == "gplu":
         raise NotImplementedError("method=:gplu (Gilbert-Peierls) is outside libmfgpu; use method='multifrontal'")
