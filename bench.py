@@ -66,6 +66,8 @@ def parse():
                     help="solve launches: library default by rhs count, per step, or one persistent launch per pass")
     ap.add_argument("--relax", action="store_true",
                     help="relaxed amalgamation (opt-in; the factors then store explicit zeros)")
+    ap.add_argument("--no-merge", action="store_true",
+                    help="one front per supernode (default: supernode chains share a front; same factors)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="mixed form: keep the built-in GEMM variant rule instead of the learned autotuner")
     return ap.parse_args()
@@ -259,6 +261,7 @@ def workload_config(args, A):
                         f"{'SCALE_MAX' if scale == 2 else 'SCALE_SUM'}, numeric factor + "
                         f"solve(refine) to normwise backward error <= 1e-14",
             "nrhs": args.nrhs, "relaxed_amalgamation": bool(getattr(args, "relax", False)),
+            "merged_fronts": not getattr(args, "no_merge", False),
             "l2": "working set (fronts) larger than L2; no explicit flush",
             "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "1 GPU"}
 
@@ -401,7 +404,8 @@ def main():
     for form in [f for f in args.forms.split(",") if f]:
         prec = PRECISION_MIXED if form == "mixed" else PRECISION_FP64
         ctx = GpuContext(device=local, precision=prec,
-                         persistent_solve={"auto": None, "step": False, "persistent": True}[args.solve_mode])
+                         persistent_solve={"auto": None, "step": False, "persistent": True}[args.solve_mode],
+                         merge_fronts=not args.no_merge)
         ctx.set_stream(stream.cuda_stream)
         t0 = time.perf_counter()
         ctx.analyze(A, S)
@@ -540,7 +544,7 @@ def main():
         "clocks": P["clocks"],
         "stats": {k: P["stats"].get(k) for k in ("n", "nsuper", "levels", "nnz_l", "nnz_u", "max_front", "flops",
                                                  "front_elems", "front_elems_full", "pool_elems", "lean",
-                                                 "flops_inverse")},
+                                                 "flops_inverse", "fronts", "merged", "flops_exec")},
     }
     print(json.dumps(line), flush=True)
     if world > 1:
@@ -737,7 +741,7 @@ def run_batch(args):
         "clocks": P["clocks"], "predicted_gflop": flops_total / 1e9, "cost_model_s": t_cost,
         "stats": {k: P["stats"].get(k) for k in ("n", "nsuper", "levels", "nnz_l", "nnz_u", "max_front", "flops",
                                                  "front_elems", "front_elems_full", "pool_elems", "lean",
-                                                 "flops_inverse")},
+                                                 "flops_inverse", "fronts", "merged", "flops_exec")},
     }
     print(json.dumps(line), flush=True)
     if world > 1:

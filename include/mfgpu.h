@@ -107,8 +107,13 @@ enum {
   MFGPU_FLAG_TF32_SPLIT = 4,       /* tensor-core GEMMs of FP32 fronts as 3xTF32 (two-part split, about 2^-21)
                                       instead of BF16x3 (three-part split, FP32 accuracy) */
   MFGPU_FLAG_STEP_SOLVE = 8,       /* solves: one launch per step (the default) */
-  MFGPU_FLAG_LEAN_FRONTS = 16      /* front memory reused by lifetime with a compact panel pool, whatever the
+  MFGPU_FLAG_LEAN_FRONTS = 16,     /* front memory reused by lifetime with a compact panel pool, whatever the
                                       size (default: only when all fronts would not fit in 45% of the device) */
+  MFGPU_FLAG_NO_FRONT_MERGE = 32   /* factor every supernode as its own front.  Default: chains of supernodes
+                                      (a child ending right before its parent) that stay small or store few
+                                      zeros together are factored as one front, with the pivot search kept
+                                      inside each original supernode's pivot rows and the factor's structure
+                                      unchanged; this saves contribution-block hand-overs and tree levels */
 };
 
 typedef struct {

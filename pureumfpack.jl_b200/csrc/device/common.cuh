@@ -42,6 +42,16 @@ struct DevPlan {
   const int64_t* lpan_off;   // per supernode: factored first np columns (leading dimension nf)
   const int64_t* u12_off;    // per supernode: factored U12 (leading dimension lean ? np : nf)
   int32_t lean;              // panels in the compact panel pool (fronts' memory reused)
+  int32_t merged;            // fronts merge original supernodes (o_* and fcu are set)
+  const int32_t* seg_end;    // per column: front-local end of the rows it may pivot on
+  const int32_t* col_orig;   // per column: original supernode (merged plans)
+  const int32_t* o_c1;
+  const int32_t* o_np;
+  const int64_t* o_upd_off;
+  const int32_t* o_upd;
+  const int32_t* o_xpos;     // front-local column of each original update-set entry
+  const int64_t* fcu_ptr;    // per front column: its U blocks
+  const UBlock* fcu;
 };
 
 __device__ __forceinline__ int u12_ld(const DevPlan& P, int s) { return P.lean ? P.np[s] : P.nf[s]; }

@@ -60,9 +60,10 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_fronts(DevPlan P, DevSt
 
   int first_zero = INT32_MAX;
   for (int k = 0; k < np; ++k) {
+    const int seg = P.seg_end[c1 + k];   // pivot rows of column k: k..seg-1
     if (warp_id() == 0) {
       ArgMax a{-1.0, k};
-      for (int i = k + lane_id(); i < np; i += 32) a = better(a, ArgMax{absd(F[i + k * nf]), i});
+      for (int i = k + lane_id(); i < seg; i += 32) a = better(a, ArgMax{absd(F[i + k * nf]), i});
       a = warp_argmax(a);
       if (lane_id() == 0) s_piv = a.i;
     }
@@ -80,7 +81,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_fronts(DevPlan P, DevSt
     if (d == T(0) && first_zero == INT32_MAX) first_zero = k;
     const T rcp = T(1) / d;
     for (int i = k + 1 + tid; i < nf; i += nthr)
-      if (i >= np || d != T(0)) F[i + k * nf] *= rcp;
+      if (i >= seg || d != T(0)) F[i + k * nf] *= rcp;
     __syncthreads();
     const int rows = nf - k - 1;
     for (int e = tid; e < rows * rows; e += nthr) {
@@ -137,15 +138,17 @@ __global__ void __launch_bounds__(256) k_assemble_columns(DevPlan P, int64_t fc0
 }
 
 // Partial-pivot LU of an R x kb panel A (leading dimension lda, shared or
-// global memory); the pivot of column j is searched in rows j..R-1 with
-// idamax's first-maximum rule.  Records local pivots in piv[] (shared) and the
-// first zero pivot (panel-relative) in *first_zero.
+// global memory); the pivot of column j is searched in rows j..seg[j]-1
+// (seg[j] <= R: the pivot rows of the column's supernode) with idamax's
+// first-maximum rule.  Records local pivots in piv[] (shared) and the first
+// zero pivot (panel-relative) in *first_zero.
 template <typename T>
-__device__ void panel_lu_pivot(T* A, int lda, int R, int kb, int* piv, ArgMax* red, int* first_zero) {
+__device__ void panel_lu_pivot(T* A, int lda, int R, int kb, const int* seg, int* piv, ArgMax* red,
+                               int* first_zero) {
   const int tid = threadIdx.x, nthr = blockDim.x;
   for (int j = 0; j < kb; ++j) {
     ArgMax a{-1.0, j};
-    for (int i = j + tid; i < R; i += nthr) a = better(a, ArgMax{absd(A[i + (int64_t)j * lda]), i});
+    for (int i = j + tid; i < seg[j]; i += nthr) a = better(a, ArgMax{absd(A[i + (int64_t)j * lda]), i});
     a = block_argmax(a, red);
     const int p = a.i;
     if (p != j)
@@ -269,12 +272,13 @@ __device__ __forceinline__ void named_barrier(int id, int count) {
 }
 
 // LU of the register panel with the pivot search restricted to rows
-// j..R-1 (PIVOT, LAPACK's first-maximum rule) or without interchanges and
-// with the partial-pivoting order check (!PIVOT).  sm_urow, sm_buf: 64 each;
-// sm_lcol: ROWS.
+// j..seg[j]-1 (PIVOT, LAPACK's first-maximum rule; seg[j] <= R ends the
+// pivot rows of column j's supernode) or without interchanges and with the
+// partial-pivoting order check on those rows (!PIVOT).  sm_urow, sm_buf: 64
+// each; sm_lcol: ROWS.
 template <typename T, int ROWS, bool PIVOT>
-__device__ void tile_lu(T (&a)[8][8], int R, int kb, T* sm_urow, T* sm_buf, T* sm_lcol, int* sm_p, int* piv,
-                        int* first_zero, bool* violated) {
+__device__ void tile_lu(T (&a)[8][8], int R, int kb, const int* seg, T* sm_urow, T* sm_buf, T* sm_lcol, int* sm_p,
+                        int* piv, int* first_zero, bool* violated) {
   constexpr int G = ROWS / 8;
   const int t = threadIdx.x;
   const int rb = t % G, cb = t / G, c0 = cb * 8;
@@ -288,10 +292,11 @@ __device__ void tile_lu(T (&a)[8][8], int R, int kb, T* sm_urow, T* sm_buf, T* s
       // groups); only the owner group of column j has real candidates.
       ArgMax m{-1.0, 0x7fffffff};
       if (cb == jb) {
+        const int sj = seg[j];
 #pragma unroll
         for (int ii = 0; ii < 8; ++ii) {
           const int i = rb + ii * G;
-          if (i >= j && i < R) m = better(m, ArgMax{absd(col_pick(a, ii, jo)), i});
+          if (i >= j && i < sj) m = better(m, ArgMax{absd(col_pick(a, ii, jo)), i});
         }
       }
       m = group_argmax<G>(m);
@@ -338,12 +343,13 @@ __device__ void tile_lu(T (&a)[8][8], int R, int kb, T* sm_urow, T* sm_buf, T* s
     }
     if (cb == jb) {                           // multipliers of column j
       const T rcp = (d != T(0)) ? T(1) / d : T(1);
+      const int sj = seg[j];
 #pragma unroll
       for (int ii = 0; ii < 8; ++ii) {
         const int i = rb + ii * G;
         if (i > j && i < R) {
           const T aj = col_pick(a, ii, jo);
-          if (!PIVOT && absd(aj) > absd(d)) *violated = true;
+          if (!PIVOT && i < sj && absd(aj) > absd(d)) *violated = true;
           const T l = (d != T(0)) ? aj * rcp : aj;
 #pragma unroll
           for (int q = 0; q < 8; ++q)
@@ -456,6 +462,7 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
   T* Ui = Li + 64 * kLdS;                    // inv(U)
   T* Tb = Ui + 64 * kLdS;                    // 2 x 7 x 64 scratch of the inverse assembly
   __shared__ int bad;
+  __shared__ int seg[64];                    // per block column: end of its pivot rows (block-relative)
   const PanelTask tk = tasks[blockIdx.x];
   const int s_ = tk.s, k0 = tk.k0;
   const int np = P.np[s_], nf = P.nf[s_], c1 = P.c1[s_];
@@ -463,6 +470,7 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
   const int t = threadIdx.x, lane = lane_id(), warp = warp_id();
   T* F = pool + P.front_off[s_];
   if (t == 0) bad = 0;
+  if (t < 64) seg[t] = t < kb ? min(kb, P.seg_end[c1 + k0 + t] - k0) : 0;
   for (int e = t; e < 64 * 64; e += kSpecThreads) {
     const int r = e & 63, c = e >> 6;
     A[r + c * kLdS] = (r < kb && c < kb) ? F[(k0 + r) + (int64_t)(k0 + c) * nf] : (r == c ? T(1) : T(0));
@@ -484,7 +492,7 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
         for (int q = 0; q < 8; ++q) u[q] = __shfl_sync(0xffffffffu, a[q], jj);
         const T d = u[jj];
         if (lane > jj && lane < 8) {
-          if (d == T(0) || absd(a[jj]) > absd(d)) violated = true;
+          if (d == T(0) || (s8 + lane < seg[s8 + jj] && absd(a[jj]) > absd(d))) violated = true;
           const T l = d != T(0) ? a[jj] * (T(1) / d) : a[jj];
           a[jj] = l;
 #pragma unroll
@@ -540,7 +548,7 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
 #pragma unroll
         for (int k = 0; k <= q; ++k) v += a[k] * Ui[(s8 + k) + (s8 + q) * kLdS];
         o[q] = v;
-        if (absd(v) > 1.0) violated = true;
+        if (r < seg[s8 + q] && absd(v) > 1.0) violated = true;
       }
 #pragma unroll
       for (int q = 0; q < 8; ++q) A[r + (s8 + q) * kLdS] = o[q];
@@ -626,7 +634,9 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
 }
 
 // Panel factorization of one panel step (k0..k1-1) of one large front.
-//  * kPanelSmemPivot: the R = np-k0 <= 256 candidate rows are held one row
+// The candidate rows of a column are the pivot rows of its supernode
+// (seg_end; all np rows of the front unless fronts are merged).
+//  * kPanelSmemPivot: the R <= 256 candidate rows are held one row
 //    per thread in registers; the pivot of each column is a block-wide
 //    argmax (warp shuffles, LAPACK's first-maximum rule), the pivot row is
 //    broadcast through shared memory, and the interchanges are applied to
@@ -656,6 +666,7 @@ __global__ void __launch_bounds__(ROWS) k_panel(DevPlan P, DevState S, const Pan
   __shared__ int first_zero;
   __shared__ int sm_p;
   __shared__ int any_violation;
+  __shared__ int seg[kPanel];             // per panel column: end of its pivot rows (panel-relative)
   const PanelTask tk = tasks[blockIdx.x];
   const int s = tk.s, k0 = tk.k0, mode = tk.mode;
   const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
@@ -663,15 +674,18 @@ __global__ void __launch_bounds__(ROWS) k_panel(DevPlan P, DevState S, const Pan
   const int t = threadIdx.x, nthr = blockDim.x;
   T* F = pool + P.front_off[s];
   T* dst = dinv + (P.dinv_off[s] + k0 / kPanel) * (int64_t)kDinvElems;
+  // candidate rows: the diagonal block (speculative) or every pivot row of
+  // the panel's columns (their supernodes' pivot rows, np - k0 unmerged)
+  const int R = (mode == kPanelSpeculative) ? kb : P.seg_end[c1 + k0 + kb - 1] - k0;
   if (t == 0) {
     first_zero = INT32_MAX;
     any_violation = 0;
   }
+  for (int c = t; c < kPanel; c += nthr) seg[c] = c < kb ? min(R, P.seg_end[c1 + k0 + c] - k0) : 0;
   __syncthreads();
 
   if (mode != kPanelGlobalPivot) {
     constexpr int G = ROWS / 8;
-    const int R = (mode == kPanelSpeculative) ? kb : np - k0;
     const int rb = t % G, c0 = (t / G) * 8;
     T a[8][8];
 #pragma unroll
@@ -683,9 +697,9 @@ __global__ void __launch_bounds__(ROWS) k_panel(DevPlan P, DevState S, const Pan
       }
     bool violated = false;
     if (mode == kPanelSmemPivot)
-      tile_lu<T, ROWS, true>(a, R, kb, sm_urow, sm_buf, sm_lcol, &sm_p, piv, &first_zero, &violated);
+      tile_lu<T, ROWS, true>(a, R, kb, seg, sm_urow, sm_buf, sm_lcol, &sm_p, piv, &first_zero, &violated);
     else
-      tile_lu<T, ROWS, false>(a, R, kb, sm_urow, sm_buf, sm_lcol, &sm_p, piv, &first_zero, &violated);
+      tile_lu<T, ROWS, false>(a, R, kb, seg, sm_urow, sm_buf, sm_lcol, &sm_p, piv, &first_zero, &violated);
     if (violated) any_violation = 1;
 #pragma unroll
     for (int ii = 0; ii < 8; ++ii)
@@ -701,7 +715,7 @@ __global__ void __launch_bounds__(ROWS) k_panel(DevPlan P, DevState S, const Pan
     if (t == 0 && (any_violation || (mode == kPanelSpeculative && first_zero != INT32_MAX))) atomicOr(S.flags, 1);
     block_inverses<T, ROWS>(stage, ROWS, kb, dst, sm_xrow);
   } else {
-    panel_lu_pivot(F + k0 + (int64_t)k0 * nf, nf, np - k0, kb, piv, red, &first_zero);
+    panel_lu_pivot(F + k0 + (int64_t)k0 * nf, nf, R, kb, seg, piv, red, &first_zero);
     for (int e = t; e < kb * kb; e += nthr) stage[(e % kb) + (e / kb) * ROWS] = F[(k0 + e % kb) + (int64_t)(k0 + e / kb) * nf];
     __syncthreads();
     block_inverses<T, ROWS>(stage, ROWS, kb, dst, sm_xrow);
@@ -767,6 +781,7 @@ __global__ void __launch_bounds__(kApplyThreads) k_panel_apply(DevPlan P, DevSta
   const int t = threadIdx.x;
   T* F = pool + P.front_off[s];
   const T* W = dinv + (P.dinv_off[s] + k0 / kPanel) * (int64_t)kDinvElems;
+  const int32_t* seg = P.seg_end + P.c1[s] + k0;   // per panel column: end of its pivot rows
   const int r = t & 63, cg = t >> 6;   // row of the tile, column parity
   if (local < tk.lrow_tiles) {
     const int i0 = tk.r0 + 64 * local;
@@ -783,7 +798,7 @@ __global__ void __launch_bounds__(kApplyThreads) k_panel_apply(DevPlan P, DevSta
     for (int e = t; e < rows * kb; e += blockDim.x) {
       const int r = e % rows, c = e / rows;
       const T v = sP[r + c * kLdP];
-      if (tk.check && i0 + r < np && absd(v) > 1.0) violated = true;
+      if (tk.check && i0 + r < seg[c] && absd(v) > 1.0) violated = true;
       F[(i0 + r) + (int64_t)(k0 + c) * nf] = v;
     }
     if (violated) atomicOr(S.flags, 1);
@@ -857,6 +872,57 @@ __global__ void __launch_bounds__(256) k_scatter_csc(DevPlan P, DevState S, cons
     for (int a = lane; a < np; a += 32) {
       ux[ub + a] = (double)col[a];
       ui[ub + a] = 1 + c1 + a;
+    }
+  }
+}
+
+// Direct CSC scatter of merged fronts, one warp per front column, in the
+// original supernodes' structure: a pivot column writes its L column (the
+// pivot rows of its supernode from the diagonal down, then the supernode's
+// update rows, found through rowfac for rows that are pivot rows of the same
+// front) and its own U triangle; every front column then writes the U blocks
+// of the original supernodes whose update set holds it (fcu).
+template <typename T>
+__global__ void __launch_bounds__(256) k_scatter_csc_merged(DevPlan P, DevState S, const T* __restrict__ pool,
+                                                            int64_t fc_total, int64_t* __restrict__ li,
+                                                            double* __restrict__ lx, int64_t* __restrict__ ui,
+                                                            double* __restrict__ ux) {
+  const int64_t fc = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp_id();
+  if (fc >= fc_total) return;
+  const int lane = lane_id();
+  const int x = P.fc_super[fc];
+  const int c = (int)(fc - P.colbase[x]);
+  const int np = P.np[x], nf = P.nf[x], c1 = P.c1[x];
+  const T* col = c < np ? pool + P.lpan_off[x] + (int64_t)c * nf
+                        : pool + P.u12_off[x] + (int64_t)(c - np) * u12_ld(P, x);
+  if (c < np) {
+    const int j = c1 + c, s = P.col_orig[j];
+    const int a0 = P.o_c1[s] - c1, a1 = a0 + P.o_np[s];
+    const int64_t lb = P.lcolptr[j];
+    for (int r = lane; r < a1 - c; r += 32) {
+      lx[lb + r] = r == 0 ? 1.0 : (double)col[c + r];
+      li[lb + r] = 1 + (int64_t)(c1 + c + r);
+    }
+    const int64_t ob = P.o_upd_off[s], on = P.o_upd_off[s + 1] - ob;
+    const int64_t lu = lb + (a1 - c);
+    for (int64_t i = lane; i < on; i += 32) {
+      const int u = P.o_upd[ob + i];
+      const int rf = S.rowfac[u];
+      const int pos = u < c1 + np ? rf - c1 : P.o_xpos[ob + i];
+      lx[lu + i] = (double)col[pos];
+      li[lu + i] = 1 + (int64_t)rf;
+    }
+    const int64_t ub = P.ucolptr[j + 1] - (c - a0 + 1);
+    for (int b = lane; b <= c - a0; b += 32) {
+      ux[ub + b] = (double)col[a0 + b];
+      ui[ub + b] = 1 + (int64_t)(c1 + a0 + b);
+    }
+  }
+  for (int64_t e = P.fcu_ptr[fc]; e < P.fcu_ptr[fc + 1]; ++e) {
+    const UBlock blk = P.fcu[e];
+    for (int b = lane; b < blk.rows; b += 32) {
+      ux[blk.uoff + b] = (double)col[blk.row0 + b];
+      ui[blk.uoff + b] = 1 + (int64_t)(c1 + blk.row0 + b);
     }
   }
 }

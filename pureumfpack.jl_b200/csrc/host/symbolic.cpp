@@ -603,30 +603,33 @@ SymbolicMF symbolic_mf(idx_t n, const idx_t* colptr, const idx_t* rowind, const 
   return S;
 }
 
-// Relaxed amalgamation (opt-in; the reference has none).  Supernodes are
-// taken bottom-up; a supernode whose columns end right before its parent's
-// (the parent's last child in postorder) merges into it when the merged
-// supernode stays small or the logical zeros it stores stay few (thresholds
-// in the style of CHOLMOD's nrelax / zrelax).  The merged supernode keeps the
-// parent's update set, which contains the child's, so every front of the
-// merged structure holds its children's contribution blocks; the child's
-// columns gain explicit zeros.
-void relax_supernodes(SymbolicMF& S) {
-  const idx_t ns = S.nsuper();
-  if (ns < 2) return;
-  std::vector<idx_t> sparent(ns, -1), gnp(ns), gnu(ns);
+// Amalgamation decisions (the reference has none).  Supernodes are taken
+// bottom-up; a supernode whose columns end right before its parent's (the
+// parent's last child in postorder) merges into it when the merged supernode
+// stays small or the logical zeros it stores stay few (thresholds in the
+// style of CHOLMOD's nrelax / zrelax).  The merged supernode keeps the
+// parent's update set, which contains the child's, so every merged front
+// holds its children's contribution blocks.  Returns one flag per supernode:
+// merged into its parent.  Inputs 0-based: parent (etree, -1 = root) of the
+// n columns, sstart (ns+1), upd_ptr (ns+1).
+std::vector<char> amalgamation_marks(idx_t n, const idx_t* parent, idx_t ns, const idx_t* sstart,
+                                     const idx_t* upd_ptr) {
+  std::vector<char> merged(ns > 0 ? ns : 0, 0);
+  if (ns < 2) return merged;
+  std::vector<idx_t> super_of(n), sparent(ns, -1), gnp(ns), gnu(ns);
+  for (idx_t s = 0; s < ns; ++s)
+    for (idx_t j = sstart[s]; j < sstart[s + 1]; ++j) super_of[j] = s;
   std::vector<double> gz(ns, 0.0);
   for (idx_t s = 0; s < ns; ++s) {
-    const idx_t p = S.parent[S.sstart[s + 1] - 1];
-    sparent[s] = p == -1 ? -1 : S.super_of[p];
-    gnp[s] = S.sstart[s + 1] - S.sstart[s];
-    gnu[s] = S.upd_ptr[s + 1] - S.upd_ptr[s];
+    const idx_t p = parent[sstart[s + 1] - 1];
+    sparent[s] = p == -1 ? -1 : super_of[p];
+    gnp[s] = sstart[s + 1] - sstart[s];
+    gnu[s] = upd_ptr[s + 1] - upd_ptr[s];
   }
   auto tri = [](double a, double u) { return a * (a + 1) / 2 + a * u; };
-  std::vector<char> merged(ns, 0);   // s merged into its parent
   for (idx_t s = 0; s < ns; ++s) {
     const idx_t p = sparent[s];
-    if (p < 0 || S.sstart[s + 1] != S.sstart[p]) continue;   // not adjacent to the parent
+    if (p < 0 || sstart[s + 1] != sstart[p]) continue;   // not adjacent to the parent
     const double npc = (double)gnp[s], nuc = (double)gnu[s], npp = (double)gnp[p], nup = (double)gnu[p];
     const double extra = npc * (npp + nup - nuc);
     const double z = gz[s] + gz[p] + extra, tot = tri(npc + npp, nup);
@@ -637,6 +640,15 @@ void relax_supernodes(SymbolicMF& S) {
     gnp[p] += gnp[s];
     gz[p] = z;
   }
+  return merged;
+}
+
+// Relaxed amalgamation (opt-in): the supernodes of amalgamation_marks become
+// the factor's supernodes, so the child's columns gain explicit zeros.
+void relax_supernodes(SymbolicMF& S) {
+  const idx_t ns = S.nsuper();
+  if (ns < 2) return;
+  const std::vector<char> merged = amalgamation_marks(S.n, S.parent.data(), ns, S.sstart.data(), S.upd_ptr.data());
   // rebuild the partition: a group ends at a supernode that is not merged
   std::vector<idx_t> sstart, upd_ptr{0}, upd_idx;
   std::vector<idx_t> group_of(ns);

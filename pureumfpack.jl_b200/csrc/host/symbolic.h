@@ -56,6 +56,10 @@ struct SymbolicMF {
 // symbolic_mf(A; q): q (0-based) or nullptr for AMD.
 SymbolicMF symbolic_mf(idx_t n, const idx_t* colptr, const idx_t* rowind, const idx_t* q);
 
+// Amalgamation decisions: flag s = supernode s merges into its parent.
+std::vector<char> amalgamation_marks(idx_t n, const idx_t* parent, idx_t ns, const idx_t* sstart,
+                                     const idx_t* upd_ptr);
+
 // Opt-in relaxed amalgamation of the supernodes (changes the factors'
 // structure: merged columns store explicit zeros).
 void relax_supernodes(SymbolicMF& s);

@@ -191,6 +191,7 @@ struct mfgpu_ctx {
   DevBuf b_pool, b_vx, b_ax, b_rs, b_ipiv, b_info, b_prow, b_rowfac, b_flags, b_dinv, b_dinv_off;
   DevBuf b_inv_off, b_inv_blocks, b_inv_tasks, b_inv_tasks_tc;   // pivot-block inversion
   DevBuf b_lpan_off, b_u12_off;                                   // factored panels
+  DevBuf b_seg_end, b_col_orig, b_o_c1, b_o_np, b_o_upd_off, b_o_upd, b_o_xpos, b_fcu_ptr, b_fcu;   // merged fronts
   DevBuf b_skinny;                                                // split-K partial sums
   bool have_rs = false;
   int factor_precision = MFGPU_PRECISION_FP64;
@@ -203,6 +204,7 @@ struct mfgpu_ctx {
   // every measured case, many or few right-hand sides)
   int persistent_mode = 0;     // 0 default (per step), 1 persistent, 2 per step
   int lean_mode = 0;           // front layout: 0 by size, 1 always lean
+  bool merge_fronts = true;    // factor supernode chains as merged fronts (factor structure unchanged)
   bool persistent = false;     // the mode resolved for the current solve
   int persist_grid[2] = {0, 0};          // CTAs of the persistent kernel, FP32 / FP64
   DevBuf b_bar, b_stamps;                // barrier words {count, gen, err, sticky err}; profiling stamps
@@ -225,7 +227,7 @@ struct mfgpu_ctx {
     int64_t nsys = 0;
     std::vector<int64_t> off, nz_off;      // column and value offsets of every system (nsys + 1)
     std::vector<int64_t> colptr, rowval;   // the block-diagonal pattern, 1-based
-    std::vector<int32_t> super_sys;        // system of every supernode
+    std::vector<int32_t> super_sys;        // system of every front
     PinnedBuf nz, b, x;                    // pinned host staging of the concatenated arrays
     bool have_factors = false;             // global factors fetched for per-system slicing
     std::vector<int64_t> lcolptr, lrowval, ucolptr, urowval, p, q;
@@ -330,6 +332,15 @@ void upload_plan(mfgpu_ctx* h) {
   upload(h->b_inv_blocks, P.inv_blocks, st);
   upload(h->b_inv_tasks, P.inv_tasks, st);
   upload(h->b_inv_tasks_tc, P.inv_tasks_tc, st);
+  upload(h->b_seg_end, P.seg_end, st);
+  upload(h->b_col_orig, P.col_orig, st);
+  upload(h->b_o_c1, P.o_c1, st);
+  upload(h->b_o_np, P.o_np, st);
+  upload(h->b_o_upd_off, P.o_upd_off, st);
+  upload(h->b_o_upd, P.o_upd, st);
+  upload(h->b_o_xpos, P.o_xpos, st);
+  upload(h->b_fcu_ptr, P.fcu_ptr, st);
+  upload(h->b_fcu, P.fcu, st);
   DevPlan& d = h->dp;
   d.n = P.n;
   d.ns = P.ns;
@@ -364,6 +375,16 @@ void upload_plan(mfgpu_ctx* h) {
   d.lpan_off = h->b_lpan_off.as<int64_t>();
   d.u12_off = h->b_u12_off.as<int64_t>();
   d.lean = P.lean ? 1 : 0;
+  d.merged = P.merged ? 1 : 0;
+  d.seg_end = h->b_seg_end.as<int32_t>();
+  d.col_orig = h->b_col_orig.as<int32_t>();
+  d.o_c1 = h->b_o_c1.as<int32_t>();
+  d.o_np = h->b_o_np.as<int32_t>();
+  d.o_upd_off = h->b_o_upd_off.as<int64_t>();
+  d.o_upd = h->b_o_upd.as<int32_t>();
+  d.o_xpos = h->b_o_xpos.as<int32_t>();
+  d.fcu_ptr = h->b_fcu_ptr.as<int64_t>();
+  d.fcu = h->b_fcu.as<UBlock>();
 }
 
 void upload_launches(mfgpu_ctx* h) {
@@ -695,9 +716,14 @@ void issue_factor(mfgpu_ctx* h) {
     klaunch(h, KC_PIVOTS, 0, 16.0 * P.n, [&] { k_finalize_pivots<<<grid1(P.ns, 128), 128, 0, st>>>(h->dp, dev_state(h)); });
   if (P.fc_total)
     klaunch(h, KC_SCATTER, 0, (double)(P.nnz_l + P.nnz_u) * (16.0 + sizeof(T)), [&] {
-      k_scatter_csc<T><<<grid1(P.fc_total, 8), 256, 0, st>>>(h->dp, dev_state(h), h->b_pool.as<T>(), P.fc_total,
-                                                             h->b_li.as<int64_t>(), h->b_lx.as<double>(),
-                                                             h->b_ui.as<int64_t>(), h->b_ux.as<double>());
+      if (P.merged)
+        k_scatter_csc_merged<T><<<grid1(P.fc_total, 8), 256, 0, st>>>(
+            h->dp, dev_state(h), h->b_pool.as<T>(), P.fc_total, h->b_li.as<int64_t>(), h->b_lx.as<double>(),
+            h->b_ui.as<int64_t>(), h->b_ux.as<double>());
+      else
+        k_scatter_csc<T><<<grid1(P.fc_total, 8), 256, 0, st>>>(h->dp, dev_state(h), h->b_pool.as<T>(), P.fc_total,
+                                                               h->b_li.as<int64_t>(), h->b_lx.as<double>(),
+                                                               h->b_ui.as<int64_t>(), h->b_ux.as<double>());
     });
   CK(cudaGetLastError());
 }
@@ -1176,7 +1202,10 @@ int analyze_common(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const int64_t
                    const int64_t* parent, int64_t ns, const int64_t* sstart, const int64_t* upd_ptr,
                    const int64_t* upd_idx) {
   auto t0 = std::chrono::steady_clock::now();
-  build_plan(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, h->plan);
+  if (h->merge_fronts)
+    build_plan_merged(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, h->plan);
+  else
+    build_plan(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, h->plan);
   // all fronts resident when they fit comfortably (FP64 worst case), else
   // working fronts placed by lifetime and a compact panel pool
   size_t free_b = 0, total_b = 0;
@@ -1225,6 +1254,7 @@ int mfgpu_create(const mfgpu_options* opts, mfgpu_ctx** out) {
     h->persistent_mode = (opts->flags & MFGPU_FLAG_PERSISTENT_SOLVE) ? 1 : (opts->flags & MFGPU_FLAG_STEP_SOLVE) ? 2 : 0;
     h->tc_bf16x3 = !(opts->flags & MFGPU_FLAG_TF32_SPLIT);
     h->lean_mode = (opts->flags & MFGPU_FLAG_LEAN_FRONTS) ? 1 : 0;
+    h->merge_fronts = !(opts->flags & MFGPU_FLAG_NO_FRONT_MERGE);
   }
   int rc = guarded(h, [&]() -> int {
     int ndev = 0;
@@ -1261,7 +1291,8 @@ void mfgpu_destroy(mfgpu_ctx* h) {
                     &h->b_small, &h->b_panel, &h->b_trsm, &h->b_gemm, &h->b_gemm_tc, &h->b_pool, &h->b_vx, &h->b_ax, &h->b_rs,
                     &h->b_ipiv, &h->b_info, &h->b_prow, &h->b_rowfac, &h->b_flags, &h->b_dinv, &h->b_dinv_off,
                     &h->b_inv_off, &h->b_inv_blocks, &h->b_inv_tasks, &h->b_inv_tasks_tc, &h->b_lpan_off,
-                    &h->b_u12_off, &h->b_skinny, &h->sched.d_skinny,
+                    &h->b_u12_off, &h->b_skinny, &h->sched.d_skinny, &h->b_seg_end, &h->b_col_orig, &h->b_o_c1,
+                    &h->b_o_np, &h->b_o_upd_off, &h->b_o_upd, &h->b_o_xpos, &h->b_fcu_ptr, &h->b_fcu,
                     &h->b_li, &h->b_lx, &h->b_ui,
                     &h->b_ux, &h->b_fsol, &h->b_b, &h->b_x, &h->b_r, &h->b_d, &h->b_err, &h->b_norm,
                     &h->sched.d_ids, &h->sched.d_gemms, &h->sched.d_gemms_tc, &h->sched.d_phases, &h->b_bar,
@@ -1597,7 +1628,7 @@ int mfgpu_stats_json(mfgpu_ctx* h, char* buf, int64_t cap) {
     ++nl;
     if (l.kind == kLaunchSmall) nsmall += l.count;
   }
-  char tmp[2048];
+  char tmp[2560];
   std::snprintf(tmp, sizeof tmp,
                 "{\"n\": %lld, \"nsuper\": %lld, \"levels\": %d, \"nnz_l\": %lld, \"nnz_u\": %lld, "
                 "\"max_front\": %d, \"max_pivots\": %d, \"front_elems\": %lld, \"flops\": %.6e, "
@@ -1605,14 +1636,17 @@ int mfgpu_stats_json(mfgpu_ctx* h, char* buf, int64_t cap) {
                 "\"factor_launches\": %lld, \"small_fronts\": %lld, \"speculative\": %s, \"safe_rerun\": %d, "
                 "\"analyze_ms\": %.3f, \"factor_ms\": %.3f, \"solve_ms\": %.3f, \"precision\": \"%s\", "
                 "\"status\": %d, \"growth\": %.6e, \"growth_limit\": %.6e, \"refactored_fp64\": %s, "
-                "\"flops_inverse\": %.6e, \"lean\": %s, \"pool_elems\": %lld, \"front_elems_full\": %lld}",
-                (long long)P.n, (long long)P.ns, P.nlevels, (long long)P.nnz_l, (long long)P.nnz_u, P.max_nf,
-                P.max_np, (long long)P.front_elems, P.flops, P.flops_getrf, P.flops_trsm, P.flops_gemm,
+                "\"flops_inverse\": %.6e, \"lean\": %s, \"pool_elems\": %lld, \"front_elems_full\": %lld, "
+                "\"fronts\": %lld, \"merged\": %s, \"flops_exec\": %.6e}",
+                (long long)P.n, (long long)(P.merged ? P.ns_orig : P.ns), P.nlevels, (long long)P.nnz_l,
+                (long long)P.nnz_u, P.max_nf, P.max_np, (long long)P.front_elems, P.flops_orig, P.flops_getrf,
+                P.flops_trsm, P.flops_gemm,
                 P.assembly_bytes_per_elem, (long long)nl, (long long)nsmall, P.has_speculative ? "true" : "false",
                 h->factor_reruns, h->t_analyze_ms, h->t_factor_ms, h->t_solve_ms,
                 h->factor_precision == MFGPU_PRECISION_MIXED ? "mixed" : "fp64", h->last_status, h->growth,
                 h->growth_limit, h->refactored_fp64 ? "true" : "false", P.flops_inverse, P.lean ? "true" : "false",
-                (long long)P.pool_elems, (long long)P.front_elems_full);
+                (long long)P.pool_elems, (long long)P.front_elems_full, (long long)P.ns,
+                P.merged ? "true" : "false", P.flops);
   std::string js(tmp);
   js.pop_back();   // reopen the object
   char item[512];
@@ -1864,6 +1898,14 @@ extern "C" int mfgpu_batch_analyze(mfgpu_ctx* h, int64_t nsys, const int64_t* n,
     if (rc != MFGPU_OK) {
       h->batch.nsys = 0;
       return rc;
+    }
+    // system of every front (merged fronts stay inside one system's tree)
+    const Plan& P = h->plan;
+    B.super_sys.resize(P.ns);
+    sys = 0;
+    for (int64_t x = 0; x < P.ns; ++x) {
+      while (P.c1[x] >= B.off[sys + 1]) ++sys;
+      B.super_sys[x] = (int32_t)sys;
     }
     B.nsys = nsys;
     return MFGPU_OK;

@@ -2,6 +2,8 @@
 
 #include "plan.h"
 
+#include "host/symbolic.h"
+
 #include <algorithm>
 #include <map>
 #include <numeric>
@@ -368,8 +370,118 @@ void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const i
     P.assembly_bytes_per_elem += moves;
   }
   P.flops = P.flops_getrf + P.flops_trsm + P.flops_gemm;
+  P.flops_orig = P.flops;
   P.front_elems_full = P.front_elems;
+  P.seg_end.resize(n);
+  for (int64_t s = 0; s < ns; ++s)
+    for (int32_t a = 0; a < P.np[s]; ++a) P.seg_end[P.c1[s] + a] = P.np[s];
   set_layout(P, false);
+}
+
+namespace {
+// Original supernodes inside the merged fronts of P: pivot segments, the
+// factor's CSC layout, and where each original block sits in its front.
+void attach_original(Plan& P, int64_t ns, const int64_t* sstart, const int64_t* upd_ptr, const int64_t* upd_idx) {
+  const int64_t n = P.n;
+  P.merged = true;
+  P.ns_orig = ns;
+  std::vector<int32_t> front_of(n);
+  for (int64_t x = 0; x < P.ns; ++x)
+    for (int32_t a = 0; a < P.np[x]; ++a) front_of[P.c1[x] + a] = (int32_t)x;
+  P.o_c1.resize(ns);
+  P.o_np.resize(ns);
+  P.o_upd_off.assign(upd_ptr, upd_ptr + ns + 1);
+  P.o_upd.assign(upd_idx, upd_idx + upd_ptr[ns]);
+  P.o_xpos.resize(upd_ptr[ns]);
+  P.col_orig.resize(n);
+  double fl = 0;
+  for (int64_t s = 0; s < ns; ++s) {
+    const int32_t c1 = (int32_t)sstart[s], npv = (int32_t)(sstart[s + 1] - sstart[s]);
+    const int32_t x = front_of[c1], xc1 = P.c1[x], xnp = P.np[x];
+    if (front_of[c1 + npv - 1] != x) throw std::logic_error("original supernode split across fronts");
+    P.o_c1[s] = c1;
+    P.o_np[s] = npv;
+    for (int32_t a = 0; a < npv; ++a) {
+      P.col_orig[c1 + a] = (int32_t)s;
+      P.seg_end[c1 + a] = c1 + npv - xc1;
+    }
+    const int32_t* xu = P.upd.data() + P.upd_off[x];
+    for (int64_t p = upd_ptr[s]; p < upd_ptr[s + 1]; ++p) {
+      const int32_t u = (int32_t)upd_idx[p];
+      if (u < c1 + npv) throw std::logic_error("update row inside its supernode");
+      if (u < xc1 + xnp) {
+        P.o_xpos[p] = u - xc1;
+      } else {
+        const int32_t* it = std::lower_bound(xu, xu + P.nu[x], u);
+        if (it == xu + P.nu[x] || *it != u) throw std::logic_error("update row missing from the merged front");
+        P.o_xpos[p] = xnp + (int32_t)(it - xu);
+      }
+    }
+    const double a = npv, u = (double)(upd_ptr[s + 1] - upd_ptr[s]);
+    fl += 2.0 / 3.0 * a * a * a + 2.0 * a * a * u + 2.0 * a * u * u;
+  }
+  P.flops_orig = fl;
+  // factor CSC layout of the original structure (as build_plan's)
+  P.lcolptr.assign(n + 1, 0);
+  P.ucolptr.assign(n + 1, 0);
+  for (int64_t s = 0; s < ns; ++s) {
+    const int32_t c1 = P.o_c1[s], c2 = c1 + P.o_np[s] - 1;
+    const int64_t nu = upd_ptr[s + 1] - upd_ptr[s];
+    for (int32_t j = c1; j <= c2; ++j) {
+      P.lcolptr[j + 1] = 1 + (c2 - j) + nu;
+      P.ucolptr[j + 1] += j - c1 + 1;
+    }
+    for (int64_t p = upd_ptr[s]; p < upd_ptr[s + 1]; ++p) P.ucolptr[upd_idx[p] + 1] += P.o_np[s];
+  }
+  for (int64_t j = 0; j < n; ++j) {
+    P.lcolptr[j + 1] += P.lcolptr[j];
+    P.ucolptr[j + 1] += P.ucolptr[j];
+  }
+  P.nnz_l = P.lcolptr[n];
+  P.nnz_u = P.ucolptr[n];
+  // U blocks per front column, in the order of the original supernodes
+  P.fcu_ptr.assign(P.fc_total + 1, 0);
+  auto fcol = [&](int64_t s, int64_t p) { return P.colbase[front_of[P.o_c1[s]]] + P.o_xpos[p]; };
+  for (int64_t s = 0; s < ns; ++s)
+    for (int64_t p = upd_ptr[s]; p < upd_ptr[s + 1]; ++p) ++P.fcu_ptr[fcol(s, p) + 1];
+  for (int64_t f = 0; f < P.fc_total; ++f) P.fcu_ptr[f + 1] += P.fcu_ptr[f];
+  P.fcu.resize(P.fcu_ptr[P.fc_total]);
+  std::vector<int64_t> ucur(P.ucolptr.begin(), P.ucolptr.end() - 1);
+  std::vector<int64_t> fcur(P.fcu_ptr.begin(), P.fcu_ptr.end() - 1);
+  for (int64_t s = 0; s < ns; ++s) {
+    const int32_t row0 = P.o_c1[s] - P.c1[front_of[P.o_c1[s]]];
+    for (int64_t p = upd_ptr[s]; p < upd_ptr[s + 1]; ++p) {
+      const int64_t u = upd_idx[p];
+      P.fcu[fcur[fcol(s, p)]++] = UBlock{row0, P.o_np[s], ucur[u]};
+      ucur[u] += P.o_np[s];
+    }
+  }
+}
+}  // namespace
+
+void build_plan_merged(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf,
+                       const int64_t* parent, int64_t ns, const int64_t* sstart, const int64_t* upd_ptr,
+                       const int64_t* upd_idx, Plan& P) {
+  const std::vector<char> marks = amalgamation_marks(n, parent, ns, sstart, upd_ptr);
+  if (std::find(marks.begin(), marks.end(), 1) == marks.end()) {
+    build_plan(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, P);
+    return;
+  }
+  // merged partition: a group ends at a supernode that is not merged, and
+  // keeps that supernode's update set
+  std::vector<int64_t> ms, mup{0}, mui;
+  int64_t first = 0;
+  for (int64_t s = 0; s < ns; ++s) {
+    if (marks[s]) continue;
+    ms.push_back(sstart[first]);
+    mui.insert(mui.end(), upd_idx + upd_ptr[s], upd_idx + upd_ptr[s + 1]);
+    mup.push_back((int64_t)mui.size());
+    first = s + 1;
+  }
+  ms.push_back(n);
+  build_plan(n, colptr, rowval, qf, parent, (int64_t)ms.size() - 1, ms.data(), mup.data(), mui.data(), P);
+  attach_original(P, ns, sstart, upd_ptr, upd_idx);
+  build_launches(P, false);
 }
 
 void set_layout(Plan& P, bool lean) {
@@ -555,15 +667,18 @@ void build_launches_core(Plan& P, bool safe) {
         const int32_t kb = std::min(kPanel, npv - k0), k1 = k0 + kb;
         // Speculative panels everywhere; the pivoting variants only run in
         // the safe rerun after a speculative panel met a larger candidate.
-        int32_t mode = !safe ? kPanelSpeculative : (npv - k0 <= kPivRowsSmem ? kPanelSmemPivot : kPanelGlobalPivot);
+        // pivot rows of the panel's columns: up to the end of the last
+        // column's segment (npv unless fronts are merged)
+        const int32_t seg = P.seg_end[P.c1[s] + k1 - 1];
+        int32_t mode = !safe ? kPanelSpeculative : (seg - k0 <= kPivRowsSmem ? kPanelSmemPivot : kPanelGlobalPivot);
         if (mode == kPanelSpeculative) P.has_speculative = true;
-        const int32_t R = (mode == kPanelSpeculative) ? kb : npv - k0;
+        const int32_t R = (mode == kPanelSpeculative) ? kb : seg - k0;
         const int c = mode == kPanelSpeculative ? 3 : ((mode == kPanelGlobalPivot || R > 128) ? 2 : (R > 64 ? 1 : 0));
         cls[c].push_back(PanelTask{s, k0, mode, 0});
         TrsmTask tt{};
         tt.s = s;
         tt.k0 = k0;
-        tt.r0 = (mode == kPanelSpeculative) ? k1 : npv;
+        tt.r0 = (mode == kPanelSpeculative) ? k1 : seg;
         tt.lrow_tiles = (int32_t)ceil_div(nf - tt.r0, 64);
         tt.ucol_tiles = (int32_t)ceil_div(nf - k1, 64);
         tt.check = (mode == kPanelSpeculative) ? 1 : 0;
@@ -599,7 +714,7 @@ void build_launches_core(Plan& P, bool safe) {
         lp.rows = c < 3 ? 64 << c : 0;   // 0: speculative kernel
         for (const PanelTask& pt : cls[c]) {
           const int32_t kb = std::min(kPanel, P.np[pt.s] - pt.k0);
-          const double R = (pt.mode == kPanelSpeculative) ? kb : (P.np[pt.s] - pt.k0);
+          const double R = (pt.mode == kPanelSpeculative) ? kb : (P.seg_end[P.c1[pt.s] + pt.k0 + kb - 1] - pt.k0);
           lp.flops += 2.0 * (R * kb * kb - (double)kb * kb * kb / 3.0) + 4.0 / 3.0 * kb * kb * kb;
           lp.elems += 2.0 * R * kb + 2.0 * 64 * 64;
           P.panel_tasks.push_back(pt);

@@ -37,11 +37,19 @@ struct PanelTask {       // one panel step of one large front
 
 struct TrsmTask {        // triangular solves of one panel step
   int32_t s, k0;
-  int32_t r0;            // first row of the L-part solve (k0+kb or np)
+  int32_t r0;            // first row of the L-part solve (k0+kb, or the end of the panel's pivot rows)
   int32_t lrow_tiles;    // 64-row tiles of the L part
   int32_t ucol_tiles;    // 64-column tiles of the U part
-  int32_t check;         // speculative: check pivot order on rows < np
+  int32_t check;         // speculative: check pivot order on each column's pivot rows
   int64_t tile_base;     // prefix over tasks
+};
+
+// A U block of the factor's CSC written from one front column: the rows
+// row0 .. row0+rows-1 of the front (one original supernode's pivot rows) go
+// to U's CSC at uoff.
+struct UBlock {
+  int32_t row0, rows;
+  int64_t uoff;
 };
 
 enum GemmMode : int32_t {
@@ -158,6 +166,25 @@ struct Plan {
   std::vector<GemmTask> gemm_tasks_tc;   // the same updates tiled 128 x 128 (FP32 fronts, tensor cores)
   std::vector<Launch> launches;
   bool has_speculative = false;
+  // Front merging (execution only).  Chains of supernodes (a child whose
+  // columns end right before its parent's) are factored as one front, which
+  // saves the child's contribution-block hand-over and the launches of a
+  // tree level; the merged front stores the child's logical zeros.  The
+  // factor keeps the original supernodes: pivots are searched only among
+  // the pivot rows of the column's original supernode (seg_end), and the CSC
+  // layout and scatter follow the original structure.  Without merging,
+  // seg_end[j] is np of j's front and the o_* arrays stay empty.
+  bool merged = false;
+  int64_t ns_orig = 0;
+  std::vector<int32_t> seg_end;        // per column: front-local end of its pivot-row segment
+  std::vector<int32_t> col_orig;       // per column: original supernode
+  std::vector<int32_t> o_c1, o_np;     // per original supernode
+  std::vector<int64_t> o_upd_off;      // ns_orig + 1
+  std::vector<int32_t> o_upd;          // original update sets
+  std::vector<int32_t> o_xpos;         // front-local column of each update-set entry
+  std::vector<int64_t> fcu_ptr;        // per front column (fc_total + 1)
+  std::vector<UBlock> fcu;             // U blocks written from each front column
+  double flops_orig = 0;               // flops of the original structure (no merged zeros)
   // statistics
   double flops = 0, flops_getrf = 0, flops_trsm = 0, flops_gemm = 0;
   double assembly_bytes_per_elem = 0;  // sum of nf^2 + 3 m^2 + nu^2 element moves (x sizeof(T) for bytes)
@@ -169,6 +196,14 @@ struct Plan {
 // `safe` replaces speculative panels by global-memory partial pivoting.
 void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf, const int64_t* parent,
                 int64_t ns, const int64_t* sstart, const int64_t* upd_ptr, const int64_t* upd_idx, Plan& plan);
+
+// The plan with front merging: the supernodes that amalgamation_marks
+// merges are factored as one front; the factor's structure, pivot segments
+// and CSC scatter stay those of (sstart, upd_ptr, upd_idx).  Falls back to
+// build_plan when nothing merges.
+void build_plan_merged(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf,
+                       const int64_t* parent, int64_t ns, const int64_t* sstart, const int64_t* upd_ptr,
+                       const int64_t* upd_idx, Plan& plan);
 
 // (Re)build the launch sequence: speculative panels, or only pivoting ones.
 void build_launches(Plan& plan, bool safe);

@@ -49,6 +49,7 @@ FLAG_PERSISTENT_SOLVE = 2  # mfgpu_options.flags: one persistent cooperative lau
 FLAG_TF32_SPLIT = 4        # mfgpu_options.flags: 3xTF32 instead of BF16x3 tensor-core products
 FLAG_STEP_SOLVE = 8        # mfgpu_options.flags: one launch per solve step, whatever the rhs count
 FLAG_LEAN_FRONTS = 16      # mfgpu_options.flags: reuse front memory by lifetime (compact panel pool)
+FLAG_NO_FRONT_MERGE = 32   # mfgpu_options.flags: one front per supernode (no merged supernode chains)
 
 
 class ArgumentError(ValueError):
@@ -220,13 +221,16 @@ class GpuContext:
     """One libmfgpu handle: analysis, resident factors, solves."""
 
     def __init__(self, device: int = 0, precision: int = PRECISION_FP64, tensor_cores: bool = True,
-                 persistent_solve: bool | None = None, tf32_split: bool = False, lean_fronts: bool = False):
+                 persistent_solve: bool | None = None, tf32_split: bool = False, lean_fronts: bool = False,
+                 merge_fronts: bool = True):
         """persistent_solve: True / False forces the solve mode; None lets the
-        library choose by right-hand-side count."""
+        library choose by right-hand-side count.  merge_fronts: factor chains
+        of supernodes as merged fronts (pivots and factor structure stay the
+        original supernodes')."""
         self._lib = L.lib()
         flags = ((0 if tensor_cores else FLAG_NO_TENSOR_CORES) | (FLAG_TF32_SPLIT if tf32_split else 0)
                  | {None: 0, True: FLAG_PERSISTENT_SOLVE, False: FLAG_STEP_SOLVE}[persistent_solve]
-                 | (FLAG_LEAN_FRONTS if lean_fronts else 0))
+                 | (FLAG_LEAN_FRONTS if lean_fronts else 0) | (0 if merge_fronts else FLAG_NO_FRONT_MERGE))
         opts = L.MfOptions(device, precision, flags, 0)
         h = ctypes.c_void_p()
         rc = self._lib.mfgpu_create(ctypes.byref(opts), ctypes.byref(h))

@@ -1,0 +1,188 @@
+// plan_emulator.cpp -- test infrastructure: a CPU emulation of libmfgpu's
+// factorization semantics over its Plan, so that the host-side plan maps
+// (merged fronts, pivot segments, assembly and CSC scatter maps) can be
+// checked against the oracle without a GPU.  Per front, in postorder:
+//   * assembly of the original entries (v_frow) and of the children's
+//     contribution blocks (rel, last child first), as k_assemble_columns and
+//     k_small_fronts do;
+//   * right-looking partial-pivot LU, the pivot of column k searched in rows
+//     k..seg_end-1 (k_small_fronts, k_panel);
+//   * _pivot_rows (k_finalize_pivots);
+//   * the CSC scatter of k_scatter_csc (one front per supernode) or of
+//     k_scatter_csc_merged (merged fronts).
+// Built by the tests with g++ against the library's plan.cpp and
+// host/symbolic.cpp; never linked into the library.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <utility>
+#include <vector>
+
+#include "host/symbolic.h"
+#include "plan.h"
+
+using namespace mfgpu;
+
+namespace {
+
+struct Result {
+  std::vector<int64_t> lp, li, up, ui, p, q;
+  std::vector<double> lx, ux;
+  int64_t stats[6] = {0, 0, 0, 0, 0, 0};
+};
+Result g_result;
+
+// Dense LU of every front; returns the fronts (column-major, nf x nf).
+std::vector<std::vector<double>> factor_fronts(const Plan& P, const double* nzval, std::vector<int32_t>& ipiv) {
+  std::vector<double> vx(P.nnz_a);
+  for (int64_t p = 0; p < P.nnz_a; ++p) vx[p] = nzval[P.v_src[p]];
+  std::vector<std::vector<double>> F(P.ns);
+  for (int64_t x = 0; x < P.ns; ++x) {
+    const int nf = P.nf[x], np = P.np[x], c1 = P.c1[x];
+    std::vector<double>& G = F[x];
+    G.assign((size_t)nf * nf, 0.0);
+    auto at = [&](int r, int c) -> double& { return G[r + (size_t)c * nf]; };
+    for (int c = 0; c < nf; ++c) {
+      const int64_t fc = P.colbase[x] + c;
+      for (int p = P.fc_vbeg[fc]; p < P.fc_vend[fc]; ++p) at(P.v_frow[p], c) = vx[p];
+    }
+    for (int ci = P.child_ptr[x + 1] - 1; ci >= P.child_ptr[x]; --ci) {
+      const int k = P.child_idx[ci];
+      const int m = P.nu[k], nfk = P.nf[k], npk = P.np[k];
+      const int32_t* rl = P.rel.data() + P.upd_off[k];
+      for (int t = 0; t < m; ++t)
+        for (int r = 0; r < m; ++r) at(rl[r], rl[t]) += F[k][npk + r + (size_t)(npk + t) * nfk];
+    }
+    for (int k = 0; k < np; ++k) {
+      const int seg = P.seg_end[c1 + k];
+      int piv = k;
+      double best = -1.0;
+      for (int i = k; i < seg; ++i)
+        if (std::fabs(at(i, k)) > best) {
+          best = std::fabs(at(i, k));
+          piv = i;
+        }
+      if (piv != k)
+        for (int j = 0; j < nf; ++j) std::swap(at(k, j), at(piv, j));
+      ipiv[c1 + k] = piv;
+      const double d = at(k, k);
+      for (int i = k + 1; i < nf; ++i)
+        if (i >= seg || d != 0.0) at(i, k) /= d;
+      for (int j = k + 1; j < nf; ++j) {
+        const double u = at(k, j);
+        if (u == 0.0) continue;
+        for (int i = k + 1; i < nf; ++i) at(i, j) -= at(i, k) * u;
+      }
+    }
+  }
+  return F;
+}
+
+}  // namespace
+
+// Factor A (0-based CSC pattern, values) with symbolic_mf(A; q) (q 0-based
+// or null for AMD), merged fronts or one front per supernode.  stats: nnz_l,
+// nnz_u, fronts, original supernodes, max front, max pivots.
+extern "C" int emu_factor(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+                          const int64_t* q, int merge, int64_t* stats) {
+  const SymbolicMF S = symbolic_mf(n, colptr, rowval, q);
+  Plan P;
+  if (merge)
+    build_plan_merged(n, colptr, rowval, S.qf.data(), S.parent.data(), S.nsuper(), S.sstart.data(),
+                      S.upd_ptr.data(), S.upd_idx.data(), P);
+  else
+    build_plan(n, colptr, rowval, S.qf.data(), S.parent.data(), S.nsuper(), S.sstart.data(), S.upd_ptr.data(),
+               S.upd_idx.data(), P);
+  std::vector<int32_t> ipiv(n);
+  const std::vector<std::vector<double>> F = factor_fronts(P, nzval, ipiv);
+
+  std::vector<int32_t> prow(n), rowfac(n);
+  for (int64_t x = 0; x < P.ns; ++x) {
+    const int c1 = P.c1[x], np = P.np[x];
+    for (int a = 0; a < np; ++a) prow[c1 + a] = c1 + a;
+    for (int a = 0; a < np; ++a)
+      if (ipiv[c1 + a] != a) std::swap(prow[c1 + a], prow[c1 + ipiv[c1 + a]]);
+    for (int a = 0; a < np; ++a) rowfac[prow[c1 + a]] = c1 + a;
+  }
+
+  Result& R = g_result;
+  R.lp.assign(P.lcolptr.begin(), P.lcolptr.end());
+  R.up.assign(P.ucolptr.begin(), P.ucolptr.end());
+  R.li.assign(P.nnz_l, -1);
+  R.lx.assign(P.nnz_l, NAN);
+  R.ui.assign(P.nnz_u, -1);
+  R.ux.assign(P.nnz_u, NAN);
+  auto put_l = [&](int64_t at, int64_t row, double v) {
+    R.li[at] = 1 + row;
+    R.lx[at] = v;
+  };
+  auto put_u = [&](int64_t at, int64_t row, double v) {
+    R.ui[at] = 1 + row;
+    R.ux[at] = v;
+  };
+  for (int64_t fc = 0; fc < P.fc_total; ++fc) {
+    const int x = P.fc_super[fc];
+    const int c = (int)(fc - P.colbase[x]);
+    const int np = P.np[x], nf = P.nf[x], c1 = P.c1[x];
+    const double* col = F[x].data() + (size_t)c * nf;   // L column, or U12 rows 0..np-1
+    if (P.merged) {
+      if (c < np) {
+        const int j = c1 + c, s = P.col_orig[j];
+        const int a0 = P.o_c1[s] - c1, a1 = a0 + P.o_np[s];
+        const int64_t lb = P.lcolptr[j];
+        for (int r = 0; r < a1 - c; ++r) put_l(lb + r, c1 + c + r, r == 0 ? 1.0 : col[c + r]);
+        const int64_t ob = P.o_upd_off[s], on = P.o_upd_off[s + 1] - ob, lu = lb + (a1 - c);
+        for (int64_t i = 0; i < on; ++i) {
+          const int u = P.o_upd[ob + i], rf = rowfac[u];
+          put_l(lu + i, rf, col[u < c1 + np ? rf - c1 : P.o_xpos[ob + i]]);
+        }
+        const int64_t ub = P.ucolptr[j + 1] - (c - a0 + 1);
+        for (int b = 0; b <= c - a0; ++b) put_u(ub + b, c1 + a0 + b, col[a0 + b]);
+      }
+      for (int64_t e = P.fcu_ptr[fc]; e < P.fcu_ptr[fc + 1]; ++e) {
+        const UBlock blk = P.fcu[e];
+        for (int b = 0; b < blk.rows; ++b) put_u(blk.uoff + b, c1 + blk.row0 + b, col[blk.row0 + b]);
+      }
+    } else {
+      const int32_t* us = P.upd.data() + P.upd_off[x];
+      if (c < np) {
+        const int64_t lb = P.lcolptr[c1 + c];
+        for (int r = 0; r < nf - c; ++r) {
+          const int fr = c + r;
+          put_l(lb + r, fr < np ? c1 + fr : rowfac[us[fr - np]], r == 0 ? 1.0 : col[fr]);
+        }
+        const int64_t ub = P.ucolptr[c1 + c + 1] - (c + 1);
+        for (int b = 0; b <= c; ++b) put_u(ub + b, c1 + b, col[b]);
+      } else {
+        const int64_t ub = P.uoff[P.upd_off[x] + (c - np)];
+        for (int a = 0; a < np; ++a) put_u(ub + a, c1 + a, col[a]);
+      }
+    }
+  }
+  R.p.resize(n);
+  R.q.resize(n);
+  for (int64_t k = 0; k < n; ++k) {
+    R.p[k] = P.qf[prow[k]] + 1;   // p = qf[prow] (src/multifrontal.jl:355-356)
+    R.q[k] = P.qf[k] + 1;
+  }
+  const int64_t st[6] = {P.nnz_l, P.nnz_u, P.ns, P.merged ? P.ns_orig : P.ns, P.max_nf, P.max_np};
+  std::memcpy(R.stats, st, sizeof st);
+  std::memcpy(stats, st, sizeof st);
+  return 0;
+}
+
+// The last factorization, 1-based as the library returns it.
+extern "C" void emu_get(int64_t* lp, int64_t* li, double* lx, int64_t* up, int64_t* ui, double* ux, int64_t* p,
+                        int64_t* q) {
+  const Result& R = g_result;
+  for (size_t k = 0; k < R.lp.size(); ++k) {
+    lp[k] = R.lp[k] + 1;
+    up[k] = R.up[k] + 1;
+  }
+  std::memcpy(li, R.li.data(), R.li.size() * 8);
+  std::memcpy(lx, R.lx.data(), R.lx.size() * 8);
+  std::memcpy(ui, R.ui.data(), R.ui.size() * 8);
+  std::memcpy(ux, R.ux.data(), R.ux.size() * 8);
+  std::memcpy(p, R.p.data(), R.p.size() * 8);
+  std::memcpy(q, R.q.data(), R.q.size() * 8);
+}

@@ -56,9 +56,10 @@ def test_lean_layout_is_bitwise_identical(name, make, colamd, precision):
 def test_lean_layout_shrinks_working_memory_of_a_deep_tree():
     A = M.random_unsym(3000, 5, 10.0, seed=3)
     S = symbolic_mf(A, q=colamd_order(A))
-    ctx = GpuContext(lean_fronts=True)
+    ctx = GpuContext(lean_fronts=True, merge_fronts=False)
     ctx.analyze(A, S)
     st = ctx.stats()
     # the resident layout needs the sum of nf^2; the lean pool (working fronts
-    # + panels + inverses) needs a fraction of it
+    # + panels + inverses) needs a fraction of it (one front per supernode:
+    # merged fronts make this tree shallow)
     assert st["pool_elems"] < 0.5 * st["front_elems_full"], (st["pool_elems"], st["front_elems_full"])
