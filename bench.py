@@ -324,11 +324,17 @@ def roofline_of(P, primary, torch, dev, peaks):
         if primary == "fp64":
             peak = fp_peak_tflops(torch, torch.float64, dev)
             peak_src = "in-run cuBLAS DGEMM 8192^3 (FP64 peak is not in MEASURED_PEAKS.json)"
+        elif "bf16_tflops_sustained" in peaks:
+            # FP32 fronts: the large updates run as BF16x3 tcgen05 products
+            # (three BF16 tensor-core products per useful FP32 product)
+            peak = peaks["bf16_tflops_sustained"] / 3.0
+            peak_src = ("MEASURED_PEAKS.json bf16_tflops_sustained / 3 (of measured): BF16x3 needs three BF16 "
+                        "tensor-core products per useful product")
         else:
-            peak = fp_peak_tflops(torch, torch.float32, dev)
-            peak_src = "in-run cuBLAS SGEMM 8192^3, TF32 off (FP32 SIMT peak)"
+            peak = 1400.0 / 3.0
+            peak_src = "fallback sustained bf16 1.4 PFLOP/s / 3 (BF16x3)"
         achieved = kd["flops"] / (kd["ms"] * 1e-3) / 1e12
-        roof = {"bound": "tensor" if primary == "fp64" else "compute", "achieved": achieved, "peak": peak,
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak,
                 "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": peak_src}
     else:
         peak = peaks.get("hbm_gbs", 6650.0)

@@ -609,11 +609,12 @@ SymbolicMF symbolic_mf(idx_t n, const idx_t* colptr, const idx_t* rowind, const 
 // stays small or the logical zeros it stores stay few (thresholds in the
 // style of CHOLMOD's nrelax / zrelax).  The merged supernode keeps the
 // parent's update set, which contains the child's, so every merged front
-// holds its children's contribution blocks.  Returns one flag per supernode:
-// merged into its parent.  Inputs 0-based: parent (etree, -1 = root) of the
-// n columns, sstart (ns+1), upd_ptr (ns+1).
+// holds its children's contribution blocks.  No merged supernode exceeds
+// max_pivots columns.  Returns one flag per supernode: merged into its
+// parent.  Inputs 0-based: parent (etree, -1 = root) of the n columns,
+// sstart (ns+1), upd_ptr (ns+1).
 std::vector<char> amalgamation_marks(idx_t n, const idx_t* parent, idx_t ns, const idx_t* sstart,
-                                     const idx_t* upd_ptr) {
+                                     const idx_t* upd_ptr, idx_t max_pivots) {
   std::vector<char> merged(ns > 0 ? ns : 0, 0);
   if (ns < 2) return merged;
   std::vector<idx_t> super_of(n), sparent(ns, -1), gnp(ns), gnu(ns);
@@ -634,6 +635,7 @@ std::vector<char> amalgamation_marks(idx_t n, const idx_t* parent, idx_t ns, con
     const double extra = npc * (npp + nup - nuc);
     const double z = gz[s] + gz[p] + extra, tot = tri(npc + npp, nup);
     const double npm = npc + npp, zf = tot > 0 ? z / tot : 0.0;
+    if (npm > (double)max_pivots) continue;
     const bool ok = npm <= 4 || (npm <= 16 && zf < 0.8) || (npm <= 48 && zf < 0.1) || zf < 0.05;
     if (!ok) continue;
     merged[s] = 1;
@@ -648,7 +650,8 @@ std::vector<char> amalgamation_marks(idx_t n, const idx_t* parent, idx_t ns, con
 void relax_supernodes(SymbolicMF& S) {
   const idx_t ns = S.nsuper();
   if (ns < 2) return;
-  const std::vector<char> merged = amalgamation_marks(S.n, S.parent.data(), ns, S.sstart.data(), S.upd_ptr.data());
+  const std::vector<char> merged =
+      amalgamation_marks(S.n, S.parent.data(), ns, S.sstart.data(), S.upd_ptr.data(), S.n);
   // rebuild the partition: a group ends at a supernode that is not merged
   std::vector<idx_t> sstart, upd_ptr{0}, upd_idx;
   std::vector<idx_t> group_of(ns);

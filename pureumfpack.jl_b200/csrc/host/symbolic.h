@@ -56,9 +56,10 @@ struct SymbolicMF {
 // symbolic_mf(A; q): q (0-based) or nullptr for AMD.
 SymbolicMF symbolic_mf(idx_t n, const idx_t* colptr, const idx_t* rowind, const idx_t* q);
 
-// Amalgamation decisions: flag s = supernode s merges into its parent.
+// Amalgamation decisions: flag s = supernode s merges into its parent; no
+// merged supernode gets more than max_pivots columns.
 std::vector<char> amalgamation_marks(idx_t n, const idx_t* parent, idx_t ns, const idx_t* sstart,
-                                     const idx_t* upd_ptr);
+                                     const idx_t* upd_ptr, idx_t max_pivots);
 
 // Opt-in relaxed amalgamation of the supernodes (changes the factors'
 // structure: merged columns store explicit zeros).

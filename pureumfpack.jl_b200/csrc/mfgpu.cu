@@ -1203,7 +1203,7 @@ int analyze_common(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const int64_t
                    const int64_t* upd_idx) {
   auto t0 = std::chrono::steady_clock::now();
   if (h->merge_fronts)
-    build_plan_merged(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, h->plan);
+    build_plan_merged(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, h->plan, kMergeMaxPivots);
   else
     build_plan(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, h->plan);
   // all fronts resident when they fit comfortably (FP64 worst case), else

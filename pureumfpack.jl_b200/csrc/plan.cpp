@@ -461,8 +461,8 @@ void attach_original(Plan& P, int64_t ns, const int64_t* sstart, const int64_t* 
 
 void build_plan_merged(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf,
                        const int64_t* parent, int64_t ns, const int64_t* sstart, const int64_t* upd_ptr,
-                       const int64_t* upd_idx, Plan& P) {
-  const std::vector<char> marks = amalgamation_marks(n, parent, ns, sstart, upd_ptr);
+                       const int64_t* upd_idx, Plan& P, int64_t max_pivots) {
+  const std::vector<char> marks = amalgamation_marks(n, parent, ns, sstart, upd_ptr, max_pivots);
   if (std::find(marks.begin(), marks.end(), 1) == marks.end()) {
     build_plan(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, P);
     return;

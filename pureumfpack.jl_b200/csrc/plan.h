@@ -19,6 +19,11 @@ namespace mfgpu {
 // Front size limits of the kernel classes.
 constexpr int kSmallFront = 64;      // fronts with nf <= this are factored in one CTA, in shared memory
 constexpr int kPanel = 64;           // panel width of the blocked large-front factorization
+// Largest pivot block a merged front may get: the explicit pivot-block
+// inverses cost (4/3) np^3, so merging into already large supernodes would
+// cost more than the hand-overs it saves (64^3 Poisson: 0.31 TFLOP of
+// inverses with this limit, 1.06 without).
+constexpr int64_t kMergeMaxPivots = 1024;
 constexpr int kPivRowsSmem = 256;    // pivot rows a partial-pivoting panel keeps in shared memory
 constexpr int kTcTile = 128;         // tile edge of the tensor-core GEMM of the FP32 fronts
 
@@ -198,12 +203,12 @@ void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const i
                 int64_t ns, const int64_t* sstart, const int64_t* upd_ptr, const int64_t* upd_idx, Plan& plan);
 
 // The plan with front merging: the supernodes that amalgamation_marks
-// merges are factored as one front; the factor's structure, pivot segments
-// and CSC scatter stay those of (sstart, upd_ptr, upd_idx).  Falls back to
-// build_plan when nothing merges.
+// merges (up to max_pivots columns each) are factored as one front; the
+// factor's structure, pivot segments and CSC scatter stay those of (sstart,
+// upd_ptr, upd_idx).  Falls back to build_plan when nothing merges.
 void build_plan_merged(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf,
                        const int64_t* parent, int64_t ns, const int64_t* sstart, const int64_t* upd_ptr,
-                       const int64_t* upd_idx, Plan& plan);
+                       const int64_t* upd_idx, Plan& plan, int64_t max_pivots);
 
 // (Re)build the launch sequence: speculative panels, or only pivoting ones.
 void build_launches(Plan& plan, bool safe);

@@ -89,7 +89,7 @@ extern "C" int emu_factor(int64_t n, const int64_t* colptr, const int64_t* rowva
   Plan P;
   if (merge)
     build_plan_merged(n, colptr, rowval, S.qf.data(), S.parent.data(), S.nsuper(), S.sstart.data(),
-                      S.upd_ptr.data(), S.upd_idx.data(), P);
+                      S.upd_ptr.data(), S.upd_idx.data(), P, kMergeMaxPivots);
   else
     build_plan(n, colptr, rowval, S.qf.data(), S.parent.data(), S.nsuper(), S.sstart.data(), S.upd_ptr.data(),
                S.upd_idx.data(), P);
