@@ -326,9 +326,12 @@ __global__ void __launch_bounds__(256) k_gemm_f32(const GemmTask* __restrict__ t
 // Split-K products for few right-hand sides (N <= NMAX): the solve products
 // g = y - U12 x_u have a handful of rows and thousands of K, which a 64 x 64
 // tile would walk serially.  Stage 1: one CTA per (task, 128-row block,
-// kSkinnyKC-wide K chunk), one thread per row, partial sums of all N columns
-// into a scratch array.  Stage 2: one CTA per (task, row block) sums the
-// chunks in order (deterministic) and applies the task's mode.
+// K chunk), one thread per row, partial sums of all N columns into a scratch
+// array.  The chunk width (kc, at most kSkinnyKC) is chosen per step so that
+// the step has enough CTAs to cover the GPU: one front's products are a
+// latency-bound walk down K otherwise.  Stage 2: one CTA per (task, row
+// block) sums the chunks in order (deterministic) and applies the task's
+// mode.
 constexpr int kSkinnyRows = 128;
 constexpr int kSkinnyKC = 256;
 constexpr int kSkinnyMaxN = 16;
@@ -337,6 +340,7 @@ struct SkinnyTask {
   int64_t a, b, c, d;
   int32_t m, n, k, lda, ldb, ldc, ldd, mode;
   int32_t rblocks, kchunks;
+  int32_t kc, pad;       // K-chunk width (<= kSkinnyKC)
   int64_t part_base;     // prefix over tasks of rblocks * kchunks (stage-1 CTAs and scratch items)
   int64_t red_base;      // prefix over tasks of rblocks (stage-2 CTAs)
 };
@@ -358,7 +362,7 @@ __global__ void __launch_bounds__(kSkinnyRows) k_skinny_part(const SkinnyTask* _
   const SkinnyTask tk = tasks[find_skinny(tasks, ntasks, blockIdx.x, false)];
   const int64_t local = blockIdx.x - tk.part_base;
   const int rb = (int)(local % tk.rblocks), kc = (int)(local / tk.rblocks);
-  const int k0 = kc * kSkinnyKC, kn = min(kSkinnyKC, tk.k - k0), N = tk.n;
+  const int k0 = kc * tk.kc, kn = min(tk.kc, tk.k - k0), N = tk.n;
   const T* A = pa + tk.a;
   const T* B = pb + tk.b;
   for (int e = threadIdx.x; e < kSkinnyKC * NMAX; e += blockDim.x) {
@@ -372,7 +376,7 @@ __global__ void __launch_bounds__(kSkinnyRows) k_skinny_part(const SkinnyTask* _
   for (int n = 0; n < NMAX; ++n) acc[n] = T(0);
   if (row < tk.m) {
     const T* ar = A + row + (int64_t)k0 * tk.lda;
-#pragma unroll 4
+#pragma unroll 8
     for (int k = 0; k < kn; ++k) {
       const T a = ar[(int64_t)k * tk.lda];
 #pragma unroll

@@ -205,6 +205,7 @@ struct mfgpu_ctx {
   int persistent_mode = 0;     // 0 default (per step), 1 persistent, 2 per step
   int lean_mode = 0;           // front layout: 0 by size, 1 always lean
   bool merge_fronts = true;    // factor supernode chains as merged fronts (factor structure unchanged)
+  int num_sms = 148;           // SMs of the device (split-K chunk choice)
   bool persistent = false;     // the mode resolved for the current solve
   int persist_grid[2] = {0, 0};          // CTAs of the persistent kernel, FP32 / FP64
   DevBuf b_bar, b_stamps;                // barrier words {count, gen, err, sticky err}; profiling stamps
@@ -963,6 +964,15 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
       int32_t maxk = 0;
       for (int64_t i = st.first; i < st.first + st.count; ++i) maxk = std::max(maxk, S.gemms[i].k);
       if (maxk < kSkinnyMinK) continue;
+      // the widest K chunk that still gives two CTAs per SM (down to 32)
+      int32_t kc = kSkinnyKC;
+      auto parts = [&](int32_t w) {
+        int64_t c = 0;
+        for (int64_t i = st.first; i < st.first + st.count; ++i)
+          c += ceil_div(S.gemms[i].m, kSkinnyRows) * std::max<int64_t>(1, ceil_div(S.gemms[i].k, w));
+        return c;
+      };
+      while (kc > 32 && parts(kc) < 2 * (int64_t)h->num_sms) kc /= 2;
       st.sk_first = (int64_t)S.skinny.size();
       for (int64_t i = st.first; i < st.first + st.count; ++i) {
         const GemmTask& g = S.gemms[i];
@@ -970,7 +980,8 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
         t.a = g.a; t.b = g.b; t.c = g.c; t.d = g.d;
         t.m = g.m; t.n = g.n; t.k = g.k; t.lda = g.lda; t.ldb = g.ldb; t.ldc = g.ldc; t.ldd = g.ldd; t.mode = g.mode;
         t.rblocks = (int32_t)ceil_div(g.m, kSkinnyRows);
-        t.kchunks = (int32_t)std::max<int64_t>(1, ceil_div(g.k, kSkinnyKC));
+        t.kc = kc;
+        t.kchunks = (int32_t)std::max<int64_t>(1, ceil_div(g.k, kc));
         t.part_base = st.sk_parts;
         t.red_base = st.sk_reds;
         st.sk_parts += (int64_t)t.rblocks * t.kchunks;
@@ -1266,6 +1277,7 @@ int mfgpu_create(const mfgpu_options* opts, mfgpu_ctx** out) {
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, h->device));
     if (prop.major != 10) return fail(h, MFGPU_ERR_NO_DEVICE, "libmfgpu is built for sm_100a (B200)");
+    h->num_sms = prop.multiProcessorCount;
     CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
     h->stream = h->own_stream;
     CK(cudaEventCreate(&h->ev0));
