@@ -517,9 +517,13 @@ def main():
     roof = roofline_of(P, primary, torch, dev, peaks)
 
     cpu = None
-    if not args.no_cpu_baseline and world == 1 and P["stats"].get("front_elems_full", 0) > CPU_FRONT_LIMIT:
+    # the oracle factors one front per supernode of the reference's structure
+    # (no merged fronts): sum of (np + nu)^2 over the original supernodes
+    npv, nuv = np.diff(S.sstart).astype(np.float64), np.diff(S.upd_ptr).astype(np.float64)
+    oracle_front_elems = float(np.sum((npv + nuv) ** 2))
+    if not args.no_cpu_baseline and world == 1 and oracle_front_elems > CPU_FRONT_LIMIT:
         cpu = {"value": None, "skipped": f"the oracle's full numeric factorization would materialise "
-                                         f"{P['stats']['front_elems_full']:.3g} front elements, far beyond a "
+                                         f"{oracle_front_elems:.3g} front elements, far beyond a "
                                          f"bounded CPU sample"}
     elif not args.no_cpu_baseline and world == 1:
         try:
