@@ -30,7 +30,7 @@ __device__ __forceinline__ int find_task(const GemmTask* __restrict__ tasks, int
   return lo;
 }
 
-constexpr int kGemmSmemF64 = 2 * kGemmBK * (kGemmBM + 8) + 2 * kGemmBN * (kGemmBK + 4);   // doubles
+constexpr int kGemmSmemF64 = 2 * kGemmBK * (kGemmBM + 4) + 2 * kGemmBN * (kGemmBK + 4);   // doubles
 
 // One 64 x 64 tile (index `tile` of the launch) of C -= A * B, 128 threads.
 // pa / pb / pc: base pointers the task offsets refer to; smem: kGemmSmemF64
@@ -40,7 +40,11 @@ __device__ __forceinline__ void gemm_tile_f64(const GemmTask* __restrict__ tasks
                                               const double* pa, const double* pb, double* pc, int64_t tile,
                                               double* smem) {
   constexpr int BM = kGemmBM, BN = kGemmBN, BK = kGemmBK;
-  constexpr int LDA_S = BM + 8;   // A tile stored k-major: As[k][m]
+  // A tile stored k-major: As[k][m].  A fragment load reads rows k..k+3 of
+  // the tile at 8 consecutive m per row; a row stride of 68 doubles puts the
+  // four rows of a half-warp on distinct banks (72 put rows k and k+2 on the
+  // same ones: a 2-way conflict on every A fragment).
+  constexpr int LDA_S = BM + 4;
   constexpr int LDB_S = BK + 4;   // B tile stored n-major: Bs[n][k]
   double* As = smem;
   double* Bs = smem + 2 * BK * LDA_S;
