@@ -59,6 +59,11 @@ enum {
 int mfgpu_row_scaling(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval, int32_t kind,
                       double* rs);
 
+/* row_scaling of a Float32 matrix in Float32 arithmetic (src/scaling.jl:92-115
+ * with R = real(Tv) = Float32). */
+int mfgpu_row_scaling_f32(int64_t n, const int64_t* colptr, const int64_t* rowval, const float* nzval,
+                          int32_t kind, float* rs);
+
 /* amd_order_sym(A; dense) (src/amd.jl:141-148): perm of 1:n. */
 int mfgpu_amd_order(int64_t n, const int64_t* colptr, const int64_t* rowval, double dense, int64_t* perm);
 
@@ -179,6 +184,23 @@ int mfgpu_solve(mfgpu_ctx* h, int64_t nrhs, const double* b, int64_t ldb, double
 /* Same with device pointers. */
 int mfgpu_solve_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ldb, double* d_x, int64_t ldx,
                        int32_t refine);
+
+/* Float32 matrices (the reference's generic Tv = Float32:
+ * multifrontal_lu / splu of a SparseMatrixCSC{Float32}, test/
+ * multifrontal_test.jl and bench/mf_verify.jl:33-37).  mfgpu_factor_f32
+ * factors Diagonal(rs) * A from Float32 values and Float32 rs (NULL: no
+ * scaling) with Float32 fronts -- assembly, pivoting and updates in FP32, the
+ * large updates as BF16x3 tensor-core products unless
+ * MFGPU_FLAG_NO_TENSOR_CORES -- and no FP64 refactor; the products
+ * rs[i] * a_ij round exactly as Float32 multiplications.
+ * mfgpu_get_factors_f32 returns the Float32 factor values;
+ * mfgpu_solve_f32 is solve(F, b; refine) for Float32 b (n x nrhs,
+ * column-major, leading dimension n) with the refinement residual in FP64,
+ * rounded to Float32 x. */
+int mfgpu_factor_f32(mfgpu_ctx* h, const float* nzval, const float* rs, int32_t check);
+int mfgpu_get_factors_f32(mfgpu_ctx* h, int64_t* lcolptr, int64_t* lrowval, float* lnzval, int64_t* ucolptr,
+                          int64_t* urowval, float* unzval, int64_t* p, int64_t* q, int64_t* pinv);
+int mfgpu_solve_f32(mfgpu_ctx* h, int64_t nrhs, const float* b, float* x, int32_t refine);
 
 /* Normwise backward error max_k ||b_k - A x_k||_inf / (||A||_inf ||x_k||_inf + ||b_k||_inf)
  * of device arrays, computed in FP64 on the GPU with the analyzed pattern. */

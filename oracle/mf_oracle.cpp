@@ -43,12 +43,23 @@ typedef void (*dtrsm_fn)(const char*, const char*, const char*, const char*, con
 typedef void (*dgemm_fn)(const char*, const char*, const i64*, const i64*, const i64*,
                          const double*, const double*, const i64*, const double*, const i64*,
                          const double*, double*, const i64*, size_t, size_t);
+// single-precision variants (Float32 factorizations)
+typedef void (*sgetrf_fn)(const i64*, const i64*, float*, const i64*, i64*, i64*);
+typedef void (*strsm_fn)(const char*, const char*, const char*, const char*, const i64*,
+                         const i64*, const float*, const float*, const i64*, float*,
+                         const i64*, size_t, size_t, size_t, size_t);
+typedef void (*sgemm_fn)(const char*, const char*, const i64*, const i64*, const i64*,
+                         const float*, const float*, const i64*, const float*, const i64*,
+                         const float*, float*, const i64*, size_t, size_t);
 typedef void (*setthreads_fn)(int);
 typedef int (*getthreads_fn)(void);
 
 static dgetrf_fn g_dgetrf = nullptr;
 static dtrsm_fn g_dtrsm = nullptr;
 static dgemm_fn g_dgemm = nullptr;
+static sgetrf_fn g_sgetrf = nullptr;
+static strsm_fn g_strsm = nullptr;
+static sgemm_fn g_sgemm = nullptr;
 static setthreads_fn g_setthreads = nullptr;
 static getthreads_fn g_getthreads = nullptr;
 static std::string g_err;
@@ -708,9 +719,48 @@ void factor_colptrs(const Symbolic& S, vector<i64>& Lp, vector<i64>& Up) {
   for (i64 j = 0; j < n; ++j) Up[j + 1] = Up[j] + ucount[j];
 }
 
+// getrf / trsm / gemm of the element type: the factorization of a Float32
+// matrix runs in Float32 (the reference's generic Tv, multifrontal.jl with
+// Tv = Float32: lu! / rdiv! / ldiv! / mul! on Matrix{Float32}).
+template <typename T>
+struct Blas;
+template <>
+struct Blas<double> {
+  static bool ok() { return g_dgetrf && g_dtrsm && g_dgemm; }
+  static void getrf(const i64* m, const i64* n, double* a, const i64* ld, i64* ipiv, i64* info) {
+    g_dgetrf(m, n, a, ld, ipiv, info);
+  }
+  static void trsm(const char* sd, const char* ul, const char* tr, const char* dg, const i64* m, const i64* n,
+                   const double* al, const double* a, const i64* lda, double* b, const i64* ldb) {
+    g_dtrsm(sd, ul, tr, dg, m, n, al, a, lda, b, ldb, 1, 1, 1, 1);
+  }
+  static void gemm(const i64* m, const i64* n, const i64* k, const double* al, const double* a, const i64* lda,
+                   const double* b, const i64* ldb, const double* be, double* c, const i64* ldc) {
+    g_dgemm("N", "N", m, n, k, al, a, lda, b, ldb, be, c, ldc, 1, 1);
+  }
+};
+template <>
+struct Blas<float> {
+  static bool ok() { return g_sgetrf && g_strsm && g_sgemm; }
+  static void getrf(const i64* m, const i64* n, float* a, const i64* ld, i64* ipiv, i64* info) {
+    g_sgetrf(m, n, a, ld, ipiv, info);
+  }
+  static void trsm(const char* sd, const char* ul, const char* tr, const char* dg, const i64* m, const i64* n,
+                   const float* al, const float* a, const i64* lda, float* b, const i64* ldb) {
+    g_strsm(sd, ul, tr, dg, m, n, al, a, lda, b, ldb, 1, 1, 1, 1);
+  }
+  static void gemm(const i64* m, const i64* n, const i64* k, const float* al, const float* a, const i64* lda,
+                   const float* b, const i64* ldb, const float* be, float* c, const i64* ldc) {
+    g_sgemm("N", "N", m, n, k, al, a, lda, b, ldb, be, c, ldc, 1, 1);
+  }
+};
+
+// Fronts, contribution blocks and all arithmetic in T; x holds the matrix
+// values (Float32 values widen exactly), the factor keeps them as double.
+template <typename T>
 int numeric_mf(i64 n, const i64* cp, const i64* ri, const double* x, const Symbolic& S, bool check,
                Factor& F) {
-  if (!g_dgetrf || !g_dtrsm || !g_dgemm) {
+  if (!Blas<T>::ok()) {
     g_err = "BLAS not loaded (call orc_set_blas first)";
     return -1;
   }
@@ -726,8 +776,8 @@ int numeric_mf(i64 n, const i64* cp, const i64* ri, const double* x, const Symbo
     i64 nfk = (c2 + 1 - S.sstart[sk]) + (S.cs_ptr[c2 + 1] - S.cs_ptr[c2]);
     maxnf = std::max(maxnf, nfk);
   }
-  vector<double> Fbuf((size_t)std::max<i64>(maxnf * maxnf, 1));
-  vector<double> cbval((size_t)std::max<i64>(64, maxnf * maxnf));
+  vector<T> Fbuf((size_t)std::max<i64>(maxnf * maxnf, 1));
+  vector<T> cbval((size_t)std::max<i64>(64, maxnf * maxnf));
   i64 cbtop = 0;
   vector<i64> cboff(nsuper, 0);
   factor_colptrs(S, F.Lp, F.Up);
@@ -748,19 +798,19 @@ int numeric_mf(i64 n, const i64* cp, const i64* ri, const double* x, const Symbo
     i64 ld = nf;
     for (i64 a = 0; a < np; ++a) loc[c1 + a] = a;
     for (i64 t = 0; t < nu; ++t) loc[upd[t]] = np + t;
-    double* Fm = Fbuf.data();
-    std::fill(Fm, Fm + nf * nf, 0.0);
+    T* Fm = Fbuf.data();
+    std::fill(Fm, Fm + nf * nf, T(0));
 #define FE(r, c) Fm[(r) + (c) * ld]
     // assemble original entries (multifrontal.jl:217-231)
     for (i64 a = 0; a < np; ++a) {
       i64 j = c1 + a;
       for (i64 p = V.cp[j]; p < V.cp[j + 1]; ++p) {
         i64 i = V.ri[p];
-        if (i >= j && loc[i] != -1) FE(loc[i], a) += V.x[p];
+        if (i >= j && loc[i] != -1) FE(loc[i], a) += (T)V.x[p];
       }
       for (i64 p = Vt.cp[j]; p < Vt.cp[j + 1]; ++p) {
         i64 k = Vt.ri[p];
-        if (k > j && loc[k] != -1) FE(a, loc[k]) += Vt.x[p];
+        if (k > j && loc[k] != -1) FE(a, loc[k]) += (T)Vt.x[p];
       }
     }
     // extend-add children, last child first (multifrontal.jl:235-243)
@@ -770,7 +820,7 @@ int numeric_mf(i64 n, const i64* cp, const i64* ri, const double* x, const Symbo
       const i64* crows = S.cs_idx.data() + S.cs_ptr[cl];
       i64 m = S.cs_ptr[cl + 1] - S.cs_ptr[cl];
       if (m == 0) continue;
-      const double* cb = cbval.data() + cboff[ck];
+      const T* cb = cbval.data() + cboff[ck];
       for (i64 s = 0; s < m; ++s) {
         i64 cs = loc[crows[s]];
         for (i64 r = 0; r < m; ++r) FE(loc[crows[r]], cs) += cb[r + s * m];
@@ -780,7 +830,7 @@ int numeric_mf(i64 n, const i64* cp, const i64* ri, const double* x, const Symbo
     // getrf on the pivot block (multifrontal.jl:247-252)
     ipiv.assign(std::max<i64>(np, 1), 0);
     i64 info = 0;
-    g_dgetrf(&np, &np, Fm, &ld, ipiv.data(), &info);
+    Blas<T>::getrf(&np, &np, Fm, &ld, ipiv.data(), &info);
     if (check && info != 0) {
       F.status = c1 + info;   // 1-based column, = c1 + info - 1 in 1-based c1
       return 1;
@@ -791,12 +841,11 @@ int numeric_mf(i64 n, const i64* cp, const i64* ri, const double* x, const Symbo
         if (pk != k)
           for (i64 col = 0; col < nu; ++col) std::swap(FE(k, np + col), FE(pk, np + col));
       }
-      const double one = 1.0, mone = -1.0;
+      const T one = 1, mone = -1;
       // L21 = A21 * U11^{-1}; U12 = L11^{-1} * A12; F22 -= L21 * U12
-      g_dtrsm("R", "U", "N", "N", &nu, &np, &one, Fm, &ld, &FE(np, 0), &ld, 1, 1, 1, 1);
-      g_dtrsm("L", "L", "N", "U", &np, &nu, &one, Fm, &ld, &FE(0, np), &ld, 1, 1, 1, 1);
-      g_dgemm("N", "N", &nu, &nu, &np, &mone, &FE(np, 0), &ld, &FE(0, np), &ld, &one, &FE(np, np), &ld,
-              1, 1);
+      Blas<T>::trsm("R", "U", "N", "N", &nu, &np, &one, Fm, &ld, &FE(np, 0), &ld);
+      Blas<T>::trsm("L", "L", "N", "U", &np, &nu, &one, Fm, &ld, &FE(0, np), &ld);
+      Blas<T>::gemm(&nu, &nu, &np, &mone, &FE(np, 0), &ld, &FE(0, np), &ld, &one, &FE(np, np), &ld);
     }
     // _pivot_rows (multifrontal.jl:363-375)
     orig.resize(np);
@@ -862,18 +911,20 @@ int numeric_mf(i64 n, const i64* cp, const i64* ri, const double* x, const Symbo
 }
 
 // solve.jl:10-22 and 25-39
-void lsolve(const Factor& F, double* y) {
+template <typename T>
+void lsolve(const Factor& F, T* y) {
   for (i64 j = 0; j < F.n; ++j) {
-    double yj = y[j];
-    for (i64 p = F.Lp[j] + 1; p < F.Lp[j + 1]; ++p) y[F.Li[p]] -= F.Lx[p] * yj;
+    T yj = y[j];
+    for (i64 p = F.Lp[j] + 1; p < F.Lp[j + 1]; ++p) y[F.Li[p]] -= (T)F.Lx[p] * yj;
   }
 }
-void usolve(const Factor& F, double* y) {
+template <typename T>
+void usolve(const Factor& F, T* y) {
   for (i64 j = F.n - 1; j >= 0; --j) {
     i64 pd = F.Up[j + 1] - 1;
-    double yj = y[j] / F.Ux[pd];
+    T yj = y[j] / (T)F.Ux[pd];
     y[j] = yj;
-    for (i64 p = F.Up[j]; p < pd; ++p) y[F.Ui[p]] -= F.Ux[p] * yj;
+    for (i64 p = F.Up[j]; p < pd; ++p) y[F.Ui[p]] -= (T)F.Ux[p] * yj;
   }
 }
 
@@ -895,6 +946,9 @@ int orc_set_blas(const char* path) {
   g_dgetrf = (dgetrf_fn)dlsym(h, "scipy_dgetrf_64_");
   g_dtrsm = (dtrsm_fn)dlsym(h, "scipy_dtrsm_64_");
   g_dgemm = (dgemm_fn)dlsym(h, "scipy_dgemm_64_");
+  g_sgetrf = (sgetrf_fn)dlsym(h, "scipy_sgetrf_64_");
+  g_strsm = (strsm_fn)dlsym(h, "scipy_strsm_64_");
+  g_sgemm = (sgemm_fn)dlsym(h, "scipy_sgemm_64_");
   g_setthreads = (setthreads_fn)dlsym(h, "scipy_openblas_set_num_threads64_");
   g_getthreads = (getthreads_fn)dlsym(h, "scipy_openblas_get_num_threads64_");
   if (!g_dgetrf || !g_dtrsm || !g_dgemm) {
@@ -1005,7 +1059,7 @@ void* orc_multifrontal_lu(i64 n, const i64* colptr, const i64* rowval, const dou
   }
   Symbolic S = symbolic_mf0(n, cp.data(), ri.data(), q1 ? &q : nullptr);
   Factor* F = new Factor();
-  int rc = numeric_mf(n, cp.data(), ri.data(), nzval, S, check != 0, *F);
+  int rc = numeric_mf<double>(n, cp.data(), ri.data(), nzval, S, check != 0, *F);
   *status = rc < 0 ? rc : F->status;
   return F;
 }
@@ -1016,7 +1070,7 @@ void* orc_numeric(void* sym, const double* nzval, const i64* colptr, const i64* 
   vector<i64> cp, ri;
   to0(S->n, colptr, rowval, cp, ri);
   Factor* F = new Factor();
-  int rc = numeric_mf(S->n, cp.data(), ri.data(), nzval, *S, check != 0, *F);
+  int rc = numeric_mf<double>(S->n, cp.data(), ri.data(), nzval, *S, check != 0, *F);
   *status = rc < 0 ? rc : F->status;
   return F;
 }
@@ -1081,6 +1135,75 @@ void orc_solve(void* h, const double* Rs, i64 n, const i64* colptr, const i64* r
       }
       for (i64 i = 0; i < n; ++i) r[i] = b[i] - ax[i];
       orc_solve_factor(h, Rs, r.data(), d.data());
+      for (i64 i = 0; i < n; ++i) x[i] = x[i] + d[i];
+    }
+  }
+}
+
+// ---- Float32 (the reference's generic Tv = Float32) ---------------------------
+// row_scaling in Float32 arithmetic (scaling.jl:92-115 with R = Float32).
+void orc_row_scaling_f32(i64 n, const i64* colptr, const i64* rowval, const float* nzval, int kind, float* Rs) {
+  for (i64 i = 0; i < n; ++i) Rs[i] = 1.0f;
+  if (kind == 0) return;
+  vector<float> acc(n, 0.0f);
+  i64 nz = colptr[n] - 1;
+  if (kind == 1) {
+    for (i64 p = 0; p < nz; ++p) acc[rowval[p] - 1] += std::fabs(nzval[p]);
+  } else {
+    for (i64 p = 0; p < nz; ++p) {
+      i64 i = rowval[p] - 1;
+      float v = std::fabs(nzval[p]);
+      acc[i] = v > acc[i] ? v : acc[i];
+    }
+  }
+  for (i64 i = 0; i < n; ++i) Rs[i] = acc[i] > 0 ? 1.0f / acc[i] : 1.0f;
+}
+
+// multifrontal_lu of a Float32 matrix (already scaled by the caller): the
+// whole numeric phase in Float32; the factor handle stores the Float32 values
+// widened to double (exact).
+void* orc_multifrontal_lu_f32(i64 n, const i64* colptr, const i64* rowval, const float* nzval, const i64* q1,
+                              int check, i64* status) {
+  vector<i64> cp, ri;
+  to0(n, colptr, rowval, cp, ri);
+  vector<i64> q;
+  if (q1) {
+    q.resize(n);
+    for (i64 k = 0; k < n; ++k) q[k] = q1[k] - 1;
+  }
+  Symbolic S = symbolic_mf0(n, cp.data(), ri.data(), q1 ? &q : nullptr);
+  vector<double> xd(nzval, nzval + cp[n]);
+  Factor* F = new Factor();
+  int rc = numeric_mf<float>(n, cp.data(), ri.data(), xd.data(), S, check != 0, *F);
+  *status = rc < 0 ? rc : F->status;
+  return F;
+}
+
+// solve(F::PureLU{Float32}, b::Vector{Float32}; refine) (interface.jl:123-177)
+// in Float32: scaling, triangular solves, the residual b - A x and the update.
+void orc_solve_f32(void* h, const float* Rs, i64 n, const i64* colptr, const i64* rowval, const float* nzval,
+                   i64 nrhs, const float* B, float* X, int refine) {
+  Factor* F = (Factor*)h;
+  vector<float> c(n), r(n), ax(n);
+  auto solve1 = [&](const float* b, float* x) {
+    for (i64 k = 0; k < n; ++k) c[k] = Rs ? Rs[F->p[k]] * b[F->p[k]] : b[F->p[k]];
+    lsolve(*F, c.data());
+    usolve(*F, c.data());
+    for (i64 k = 0; k < n; ++k) x[F->q[k]] = c[k];
+  };
+  vector<float> d(n);
+  for (i64 col = 0; col < nrhs; ++col) {
+    const float* b = B + col * n;
+    float* x = X + col * n;
+    solve1(b, x);
+    for (int it = 0; it < refine; ++it) {
+      std::fill(ax.begin(), ax.end(), 0.0f);
+      for (i64 j = 0; j < n; ++j) {
+        float xj = x[j];
+        for (i64 p = colptr[j] - 1; p < colptr[j + 1] - 1; ++p) ax[rowval[p] - 1] += nzval[p] * xj;
+      }
+      for (i64 i = 0; i < n; ++i) r[i] = b[i] - ax[i];
+      solve1(r.data(), d.data());
       for (i64 i = 0; i < n; ++i) x[i] = x[i] + d[i];
     }
   }

@@ -13,6 +13,9 @@ its 1-based Int64 index convention:
 * ``symbolic_mf``        src/symbolic.jl:211-226
 * ``multifrontal_lu``    src/multifrontal.jl:146-358
 * ``solve``              src/interface.jl:170-177 (with ``_solve_factor`` :123-138)
+* ``*_f32``              the same for the reference's generic Tv = Float32: row
+  scaling, the numeric phase (sgetrf / strsm / sgemm fronts) and the solve
+  with its refinement, all in Float32 arithmetic
 """
 
 from __future__ import annotations
@@ -33,6 +36,7 @@ SCALE_NONE, SCALE_SUM, SCALE_MAX = 0, 1, 2
 
 _i64p = ctypes.POINTER(ctypes.c_int64)
 _f64p = ctypes.POINTER(ctypes.c_double)
+_f32p = ctypes.POINTER(ctypes.c_float)
 
 
 def openblas_path() -> str:
@@ -81,6 +85,11 @@ def lib():
         L.orc_row_scaling.argtypes = [ctypes.c_int64, _i64p, _i64p, _f64p, ctypes.c_int, _f64p]
         L.orc_amd_order_sym.argtypes = [ctypes.c_int64, _i64p, _i64p, ctypes.c_double, _i64p]
         L.orc_colamd_order.argtypes = [ctypes.c_int64, ctypes.c_int64, _i64p, _i64p, ctypes.c_double, _i64p]
+        L.orc_row_scaling_f32.argtypes = [ctypes.c_int64, _i64p, _i64p, _f32p, ctypes.c_int, _f32p]
+        L.orc_multifrontal_lu_f32.restype = ctypes.c_void_p
+        L.orc_multifrontal_lu_f32.argtypes = [ctypes.c_int64, _i64p, _i64p, _f32p, _i64p, ctypes.c_int, _i64p]
+        L.orc_solve_f32.argtypes = [ctypes.c_void_p, _f32p, ctypes.c_int64, _i64p, _i64p, _f32p, ctypes.c_int64,
+                                    _f32p, _f32p, ctypes.c_int]
         rc = L.orc_set_blas(openblas_path().encode())
         if rc != 0:
             raise RuntimeError("oracle: cannot load OpenBLAS: " + L.orc_last_error().decode())
@@ -301,3 +310,55 @@ def solve_raw(F: Factor, b: np.ndarray) -> np.ndarray:
     bb = _f(b)
     lib().orc_solve_factor(ctypes.c_void_p(F.handle), None, _p(bb, _f64p), _p(x, _f64p))
     return x
+
+
+# ---------------------------------------------------------------------------
+# Float32 (the reference's generic Tv = Float32)
+# ---------------------------------------------------------------------------
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def row_scaling_f32(A, kind: int) -> np.ndarray:
+    """row_scaling of a Float32 matrix, in Float32 (scaling.jl:92-115)."""
+    Rs = np.empty(A.m, np.float32)
+    lib().orc_row_scaling_f32(A.m, _p(_i(A.colptr)), _p(_i(A.rowval)), _p(_f32(A.nzval), _f32p), int(kind),
+                              _p(Rs, _f32p))
+    return Rs
+
+
+def multifrontal_lu_f32(A, q=None, check: bool = True) -> Factor:
+    """multifrontal_lu of a Float32 matrix: every front operation in Float32
+    (values returned widened to Float64, exactly)."""
+    st = np.zeros(1, np.int64)
+    qa = _i(q) if q is not None else None
+    h = lib().orc_multifrontal_lu_f32(A.n, _p(_i(A.colptr)), _p(_i(A.rowval)), _p(_f32(A.nzval), _f32p), _p(qa),
+                                      int(check), _p(st))
+    if st[0] < 0:
+        lib().orc_factor_free(ctypes.c_void_p(h))
+        raise RuntimeError("oracle: " + lib().orc_last_error().decode())
+    if st[0] > 0:
+        lib().orc_factor_free(ctypes.c_void_p(h))
+        raise SingularException(int(st[0]))
+    return _extract(h)
+
+
+def splu_f32(A, scale: int = SCALE_SUM, check: bool = True, q=None) -> PureLU:
+    """splu(A::SparseMatrixCSC{Float32}; method=:multifrontal, scale)."""
+    Rs = row_scaling_f32(A, scale)
+    As = A.copy()
+    if scale != SCALE_NONE:
+        As.nzval = (_f32(As.nzval) * Rs[As.rowval - 1]).astype(np.float32)
+    F = multifrontal_lu_f32(As, q=q, check=check)
+    return PureLU(F, Rs, A)
+
+
+def solve_f32(F: PureLU, b: np.ndarray, refine: int = 0) -> np.ndarray:
+    """solve(F::PureLU{Float32}, b::Vector{Float32}; refine), all in Float32."""
+    A = F.A
+    B = np.asfortranarray(b, dtype=np.float32)
+    nrhs = 1 if B.ndim == 1 else B.shape[1]
+    X = np.empty_like(B)
+    lib().orc_solve_f32(ctypes.c_void_p(F.F.handle), _p(_f32(F.Rs), _f32p), A.n, _p(_i(A.colptr)),
+                        _p(_i(A.rowval)), _p(_f32(A.nzval), _f32p), nrhs, _p(B, _f32p), _p(X, _f32p), int(refine))
+    return X

@@ -50,6 +50,16 @@ int mfgpu_row_scaling(int64_t n, const int64_t* colptr, const int64_t* rowval, c
   return MFGPU_OK;
 }
 
+int mfgpu_row_scaling_f32(int64_t n, const int64_t* colptr, const int64_t* rowval, const float* nzval,
+                          int32_t kind, float* rs) {
+  if (!valid_csc(n, n, colptr, rowval) || !rs || kind < 0 || kind > 2) return MFGPU_ERR_ARGUMENT;
+  const int64_t nz = colptr[n] - 1;
+  std::vector<idx_t> ri(nz);
+  for (int64_t p = 0; p < nz; ++p) ri[p] = rowval[p] - 1;
+  mfgpu::row_scaling(n, nz, ri.data(), nzval, kind, rs);
+  return MFGPU_OK;
+}
+
 int mfgpu_amd_order(int64_t n, const int64_t* colptr, const int64_t* rowval, double dense, int64_t* perm) {
   if (!valid_csc(n, n, colptr, rowval) || !perm) return MFGPU_ERR_ARGUMENT;
   try {

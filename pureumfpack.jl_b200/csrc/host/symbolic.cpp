@@ -421,20 +421,31 @@ std::vector<idx_t> colamd_order(idx_t m, idx_t n, const idx_t* colptr, const idx
   return amd_order(g, dense);
 }
 
-void row_scaling(idx_t n, idx_t nnz, const idx_t* rowind, const double* nzval, int kind, double* rs) {
-  std::fill(rs, rs + n, 1.0);
+// In the element type's arithmetic: R = real(Tv) accumulates (Float32 sums
+// for a Float32 matrix, as the reference's generic code does).
+template <typename T>
+static void row_scaling_t(idx_t n, idx_t nnz, const idx_t* rowind, const T* nzval, int kind, T* rs) {
+  std::fill(rs, rs + n, T(1));
   if (kind == 0) return;
-  std::vector<double> acc(n, 0.0);
+  std::vector<T> acc(n, T(0));
   if (kind == 1) {
     for (idx_t p = 0; p < nnz; ++p) acc[rowind[p]] += std::fabs(nzval[p]);
   } else {
     for (idx_t p = 0; p < nnz; ++p) {
-      const double v = std::fabs(nzval[p]);
-      double& a = acc[rowind[p]];
+      const T v = std::fabs(nzval[p]);
+      T& a = acc[rowind[p]];
       a = v > a ? v : a;
     }
   }
-  for (idx_t i = 0; i < n; ++i) rs[i] = acc[i] > 0 ? 1.0 / acc[i] : 1.0;
+  for (idx_t i = 0; i < n; ++i) rs[i] = acc[i] > 0 ? T(1) / acc[i] : T(1);
+}
+
+void row_scaling(idx_t n, idx_t nnz, const idx_t* rowind, const double* nzval, int kind, double* rs) {
+  row_scaling_t(n, nnz, rowind, nzval, kind, rs);
+}
+
+void row_scaling(idx_t n, idx_t nnz, const idx_t* rowind, const float* nzval, int kind, float* rs) {
+  row_scaling_t(n, nnz, rowind, nzval, kind, rs);
 }
 
 // ---------------------------------------------------------------------------

@@ -34,6 +34,7 @@ std::vector<idx_t> amd_order_sym(idx_t n, const idx_t* colptr, const idx_t* rowi
 std::vector<idx_t> colamd_order(idx_t m, idx_t n, const idx_t* colptr, const idx_t* rowind, double dense);
 
 void row_scaling(idx_t n, idx_t nnz, const idx_t* rowind, const double* nzval, int kind, double* rs);
+void row_scaling(idx_t n, idx_t nnz, const idx_t* rowind, const float* nzval, int kind, float* rs);
 
 // The symbolic factorization in supernodal form.  Column j of supernode s
 // (first_col[s] <= j <= last) has the L row structure {j+1..last} followed by

@@ -206,6 +206,7 @@ struct mfgpu_ctx {
   int lean_mode = 0;           // front layout: 0 by size, 1 always lean
   bool merge_fronts = true;    // factor supernode chains as merged fronts (factor structure unchanged)
   int num_sms = 148;           // SMs of the device (split-K chunk choice)
+  bool f32_values = false;     // the last factorization is of a Float32 matrix (mfgpu_factor_f32)
   bool persistent = false;     // the mode resolved for the current solve
   int persist_grid[2] = {0, 0};          // CTAs of the persistent kernel, FP32 / FP64
   DevBuf b_bar, b_stamps;                // barrier words {count, gen, err, sticky err}; profiling stamps
@@ -828,6 +829,7 @@ double element_growth(mfgpu_ctx* h) {
 int factor_dispatch(mfgpu_ctx* h, int32_t check) {
   h->refactored_fp64 = false;
   h->growth = 0.0;
+  if (h->f32_values) return factor_impl<float>(h, check);   // Float32 matrix: FP32 factors, no refactor
   if (h->precision != MFGPU_PRECISION_MIXED) return factor_impl<double>(h, check);
   const int rc = factor_impl<float>(h, check);
   if (rc != MFGPU_OK) return rc;
@@ -1383,6 +1385,7 @@ int mfgpu_analyze_symbolic(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const
 int mfgpu_factor_device(mfgpu_ctx* h, const double* d_nzval, const double* d_rs, int32_t check) {
   if (!h) return MFGPU_ERR_ARGUMENT;
   if (!h->analyzed) return fail(h, MFGPU_ERR_STATE, "factor before analyze");
+  h->f32_values = false;
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->device));
     const Plan& P = h->plan;
@@ -1400,6 +1403,7 @@ int mfgpu_factor_device(mfgpu_ctx* h, const double* d_nzval, const double* d_rs,
 int mfgpu_factor_scaled(mfgpu_ctx* h, const double* nzval, int32_t scale, int32_t check) {
   if (!h) return MFGPU_ERR_ARGUMENT;
   if (!h->analyzed) return fail(h, MFGPU_ERR_STATE, "factor before analyze");
+  h->f32_values = false;
   if (scale < MFGPU_SCALE_NONE || scale > MFGPU_SCALE_MAX) return fail(h, MFGPU_ERR_ARGUMENT, "bad scale kind");
   if (h->plan.nnz_a && !nzval) return fail(h, MFGPU_ERR_ARGUMENT, "null values");
   return guarded(h, [&]() -> int {
@@ -1434,9 +1438,11 @@ int mfgpu_get_row_scaling(mfgpu_ctx* h, double* rs) {
   });
 }
 
-int mfgpu_factor(mfgpu_ctx* h, const double* nzval, const double* rs, int32_t check) {
+// Host values (FP64, or Float32 values widened) -> factorization.
+static int factor_host(mfgpu_ctx* h, const double* nzval, const double* rs, int32_t check, bool f32) {
   if (!h) return MFGPU_ERR_ARGUMENT;
   if (!h->analyzed) return fail(h, MFGPU_ERR_STATE, "factor before analyze");
+  h->f32_values = f32;
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->device));
     const Plan& P = h->plan;
@@ -1449,6 +1455,50 @@ int mfgpu_factor(mfgpu_ctx* h, const double* nzval, const double* rs, int32_t ch
     }
     return factor_dispatch(h, check);
   });
+}
+
+int mfgpu_factor(mfgpu_ctx* h, const double* nzval, const double* rs, int32_t check) {
+  return factor_host(h, nzval, rs, check, false);
+}
+
+int mfgpu_factor_f32(mfgpu_ctx* h, const float* nzval, const float* rs, int32_t check) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  if (!h->analyzed) return fail(h, MFGPU_ERR_STATE, "factor before analyze");
+  const Plan& P = h->plan;
+  if (P.nnz_a && !nzval) return fail(h, MFGPU_ERR_ARGUMENT, "null values");
+  // Float32 values and scaling widen exactly; the device forms rs * a in
+  // FP64 (exact for two Float32 factors) and the FP32 fronts round it once,
+  // as a Float32 multiplication would
+  std::vector<double> vx(nzval, nzval + P.nnz_a), rsx;
+  if (rs) rsx.assign(rs, rs + P.n);
+  return factor_host(h, vx.data(), rs ? rsx.data() : nullptr, check, true);
+}
+
+int mfgpu_get_factors_f32(mfgpu_ctx* h, int64_t* lcolptr, int64_t* lrowval, float* lnzval, int64_t* ucolptr,
+                          int64_t* urowval, float* unzval, int64_t* p, int64_t* q, int64_t* pinv) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  if (!h->factored) return fail(h, MFGPU_ERR_STATE, "no factorization");
+  if (!h->f32_values) return fail(h, MFGPU_ERR_STATE, "the last factorization is not of a Float32 matrix");
+  std::vector<double> lx(lnzval ? h->plan.nnz_l : 0), ux(unzval ? h->plan.nnz_u : 0);
+  const int rc = mfgpu_get_factors(h, lcolptr, lrowval, lnzval ? lx.data() : nullptr, ucolptr, urowval,
+                                   unzval ? ux.data() : nullptr, p, q, pinv);
+  if (rc != MFGPU_OK) return rc;
+  for (size_t k = 0; k < lx.size(); ++k) lnzval[k] = (float)lx[k];   // FP32 values: exact
+  for (size_t k = 0; k < ux.size(); ++k) unzval[k] = (float)ux[k];
+  return MFGPU_OK;
+}
+
+int mfgpu_solve_f32(mfgpu_ctx* h, int64_t nrhs, const float* b, float* x, int32_t refine) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  if (!h->factored) return fail(h, MFGPU_ERR_STATE, "solve before factor");
+  const int64_t n = h->plan.n;
+  if (nrhs < 0 || refine < 0 || (nrhs && n && (!b || !x))) return fail(h, MFGPU_ERR_ARGUMENT, "bad solve sizes");
+  if (nrhs == 0 || n == 0) return MFGPU_OK;
+  std::vector<double> bd(b, b + n * nrhs), xd((size_t)(n * nrhs));
+  const int rc = mfgpu_solve(h, nrhs, bd.data(), n, xd.data(), n, refine);
+  if (rc != MFGPU_OK) return rc;
+  for (size_t k = 0; k < xd.size(); ++k) x[k] = (float)xd[k];
+  return MFGPU_OK;
 }
 
 int mfgpu_factor_sizes(mfgpu_ctx* h, int64_t* out3) {

@@ -24,6 +24,7 @@ cp = ctypes.c_char_p
 # (name, restype, argtypes) for every symbol of include/mfgpu.h
 SIGNATURES = [
     ("mfgpu_row_scaling", ctypes.c_int, [i64, i64p, i64p, f64p, i32, f64p]),
+    ("mfgpu_row_scaling_f32", ctypes.c_int, [i64, i64p, i64p, f32p, i32, f32p]),
     ("mfgpu_amd_order", ctypes.c_int, [i64, i64p, i64p, f64, i64p]),
     ("mfgpu_colamd_order", ctypes.c_int, [i64, i64, i64p, i64p, f64, i64p]),
     ("mfgpu_symbolic_create", ctypes.c_int, [i64, i64p, i64p, i64p, ctypes.POINTER(vp)]),
@@ -48,6 +49,9 @@ SIGNATURES = [
     ("mfgpu_get_row_scaling", ctypes.c_int, [vp, f64p]),
     ("mfgpu_factor_sizes", ctypes.c_int, [vp, i64p]),
     ("mfgpu_get_factors", ctypes.c_int, [vp, i64p, i64p, f64p, i64p, i64p, f64p, i64p, i64p, i64p]),
+    ("mfgpu_factor_f32", ctypes.c_int, [vp, f32p, f32p, i32]),
+    ("mfgpu_get_factors_f32", ctypes.c_int, [vp, i64p, i64p, f32p, i64p, i64p, f32p, i64p, i64p, i64p]),
+    ("mfgpu_solve_f32", ctypes.c_int, [vp, i64, f32p, f32p, i32]),
     ("mfgpu_solve", ctypes.c_int, [vp, i64, f64p, i64, f64p, i64, i32]),
     ("mfgpu_solve_device", ctypes.c_int, [vp, i64, vp, i64, vp, i64, i32]),
     ("mfgpu_backward_error_device", ctypes.c_int, [vp, i64, vp, i64, vp, i64, f64p]),

@@ -103,6 +103,12 @@ def row_scaling(A: SparseCSC, kind: ScaleKind) -> np.ndarray:
         elif kind == SCALE_MAX:
             np.maximum.at(acc, A.rowval - 1, np.abs(A.nzval))
         return np.where(acc > 0, 1.0 / np.where(acc > 0, acc, 1.0), 1.0) if kind != SCALE_NONE else np.ones(A.m)
+    if A.nzval.dtype == np.float32:   # Float32 matrix: Float32 arithmetic (R = real(Tv))
+        rs = np.empty(A.n, np.float32)
+        _check_host(L.lib().mfgpu_row_scaling_f32(A.n, L.ptr(_i(A.colptr)), L.ptr(_i(A.rowval)),
+                                                  L.ptr(np.ascontiguousarray(A.nzval), L.f32p), int(kind),
+                                                  L.ptr(rs, L.f32p)))
+        return rs
     rs = np.empty(A.n)
     _check_host(L.lib().mfgpu_row_scaling(A.n, L.ptr(_i(A.colptr)), L.ptr(_i(A.rowval)),
                                           L.ptr(_f(A.nzval), L.f64p), int(kind), L.ptr(rs, L.f64p)))
@@ -112,7 +118,7 @@ def row_scaling(A: SparseCSC, kind: ScaleKind) -> np.ndarray:
 def apply_row_scaling(A: SparseCSC, Rs) -> SparseCSC:
     """Diagonal(Rs) * A with the same pattern (src/scaling.jl:118-126)."""
     B = A.copy()
-    B.nzval = B.nzval * np.asarray(Rs, dtype=np.float64)[B.rowval - 1]
+    B.nzval = B.nzval * np.asarray(Rs, dtype=B.nzval.dtype)[B.rowval - 1]
     return B
 
 
@@ -239,6 +245,7 @@ class GpuContext:
         self._h = h
         self.n = 0
         self.precision = precision
+        self.f32 = False   # the last factorization is of a Float32 matrix
 
     def _check(self, rc: int):
         if rc < 0:
@@ -276,7 +283,15 @@ class GpuContext:
 
     def factor(self, nzval, Rs=None, check: bool = True) -> int:
         rs = _f(Rs) if Rs is not None else None
+        self.f32 = False
         return self._check(self._lib.mfgpu_factor(self._h, L.ptr(_f(nzval), L.f64p), L.ptr(rs, L.f64p), int(check)))
+
+    def factor_f32(self, nzval, Rs=None, check: bool = True) -> int:
+        """Factorization of a Float32 matrix: Float32 fronts, Float32 factors."""
+        v = np.ascontiguousarray(nzval, dtype=np.float32)
+        rs = np.ascontiguousarray(Rs, dtype=np.float32) if Rs is not None else None
+        self.f32 = True
+        return self._check(self._lib.mfgpu_factor_f32(self._h, L.ptr(v, L.f32p), L.ptr(rs, L.f32p), int(check)))
 
     def factor_scaled(self, nzval, scale, check: bool = True) -> int:
         """Row scaling of kind ``scale`` computed on the device, then the
@@ -300,20 +315,29 @@ class GpuContext:
 
     def factors(self):
         n, nl, nu = self.sizes()
+        f32 = getattr(self, "f32", False)
+        dt, vp = (np.float32, L.f32p) if f32 else (np.float64, L.f64p)
         Lp = np.empty(n + 1, np.int64)
         Li = np.empty(nl, np.int64)
-        Lx = np.empty(nl)
+        Lx = np.empty(nl, dt)
         Up = np.empty(n + 1, np.int64)
         Ui = np.empty(nu, np.int64)
-        Ux = np.empty(nu)
+        Ux = np.empty(nu, dt)
         p = np.empty(n, np.int64)
         q = np.empty(n, np.int64)
         pinv = np.empty(n, np.int64)
-        self._check(self._lib.mfgpu_get_factors(self._h, L.ptr(Lp), L.ptr(Li), L.ptr(Lx, L.f64p), L.ptr(Up),
-                                                L.ptr(Ui), L.ptr(Ux, L.f64p), L.ptr(p), L.ptr(q), L.ptr(pinv)))
+        get = self._lib.mfgpu_get_factors_f32 if f32 else self._lib.mfgpu_get_factors
+        self._check(get(self._h, L.ptr(Lp), L.ptr(Li), L.ptr(Lx, vp), L.ptr(Up), L.ptr(Ui), L.ptr(Ux, vp), L.ptr(p),
+                        L.ptr(q), L.ptr(pinv)))
         return SparseCSC(n, n, Lp, Li, Lx), SparseCSC(n, n, Up, Ui, Ux), p, q, pinv
 
     def solve(self, b, refine: int = 0) -> np.ndarray:
+        if getattr(self, "f32", False):
+            B = np.asfortranarray(b, dtype=np.float32)
+            X = np.empty_like(B)
+            nrhs = 1 if B.ndim == 1 else B.shape[1]
+            self._check(self._lib.mfgpu_solve_f32(self._h, nrhs, L.ptr(B, L.f32p), L.ptr(X, L.f32p), int(refine)))
+            return X
         B = np.asfortranarray(b, dtype=np.float64)
         nrhs = 1 if B.ndim == 1 else B.shape[1]
         X = np.empty_like(B)
@@ -428,7 +452,9 @@ def _factor(A: SparseCSC, q, check: bool, Rs, device: int, precision: int, relax
     S = symbolic_mf(A, q=q, relax=relax)
     ctx = GpuContext(device=device, precision=precision)
     ctx.analyze(A, S)
-    status = ctx.factor(A.nzval, Rs, check)
+    # a Float32 matrix is factored in Float32 (the reference's generic Tv)
+    fac = ctx.factor_f32 if A.nzval.dtype == np.float32 else ctx.factor
+    status = fac(A.nzval, Rs, check)
     if status > 0:
         raise SingularException(status)
     return ctx, S
@@ -584,7 +610,7 @@ def solve(F, b, refine: int = 0) -> np.ndarray:
         if refine:
             raise ArgumentError("refinement needs a PureLU (it keeps A and Rs)")
         return F.ldiv(b)
-    b = np.asarray(b, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float32 if F.A.nzval.dtype == np.float32 else np.float64)
     if b.shape[0] != F.A.n:
         raise DimensionMismatch("length(b) must equal size(F, 1)")
     return F.ctx.solve(b, refine)

@@ -1,9 +1,9 @@
 """SparseCSC: the host-side matrix type, laid out as Julia's SparseMatrixCSC.
 
-``colptr`` (n+1) and ``rowval`` (nnz) are 1-based Int64, ``nzval`` is Float64,
-rows ascend within each column, exactly the layout
-``SparseMatrixCSC{Float64,Int64}`` hands to ``ccall`` -- so buffers pass to
-the C ABI without conversion.
+``colptr`` (n+1) and ``rowval`` (nnz) are 1-based Int64, ``nzval`` is Float64
+(or Float32 when given Float32 values, as ``SparseMatrixCSC{Float32,Int64}``),
+rows ascend within each column, exactly the layout ``SparseMatrixCSC`` hands
+to ``ccall`` -- so buffers pass to the C ABI without conversion.
 """
 
 from __future__ import annotations
@@ -19,7 +19,8 @@ class SparseCSC:
         self.n = int(n)
         self.colptr = np.ascontiguousarray(colptr, dtype=np.int64)
         self.rowval = np.ascontiguousarray(rowval, dtype=np.int64)
-        self.nzval = np.ascontiguousarray(nzval, dtype=np.float64)
+        nzval = np.asarray(nzval)
+        self.nzval = np.ascontiguousarray(nzval, dtype=np.float32 if nzval.dtype == np.float32 else np.float64)
         if self.colptr.shape != (self.n + 1,):
             raise ValueError("colptr must have n+1 entries")
         if self.colptr[0] != 1 or self.colptr[-1] - 1 != len(self.rowval) or len(self.rowval) != len(self.nzval):
@@ -56,7 +57,7 @@ class SparseCSC:
         S.sort_indices()
         S.sum_duplicates()
         return SparseCSC(S.shape[0], S.shape[1], S.indptr.astype(np.int64) + 1, S.indices.astype(np.int64) + 1,
-                         S.data.astype(np.float64))
+                         S.data.astype(np.float32 if S.dtype == np.float32 else np.float64))
 
     def to_scipy(self):
         import scipy.sparse as sp
@@ -67,6 +68,15 @@ class SparseCSC:
     @property
     def shape(self):
         return (self.m, self.n)
+
+    @property
+    def eltype(self):
+        """Element type of the stored values (numpy float64 or float32)."""
+        return self.nzval.dtype.type
+
+    def astype(self, dtype) -> "SparseCSC":
+        """Copy with values converted to ``dtype`` (Float64 or Float32)."""
+        return SparseCSC(self.m, self.n, self.colptr.copy(), self.rowval.copy(), self.nzval.astype(dtype))
 
     def nnz(self) -> int:
         return int(len(self.rowval))
