@@ -68,6 +68,9 @@ def parse():
                     help="relaxed amalgamation (opt-in; the factors then store explicit zeros)")
     ap.add_argument("--no-merge", action="store_true",
                     help="one front per supernode (default: supernode chains share a front; same factors)")
+    ap.add_argument("--dtype", default="float64", choices=["float64", "float32"],
+                    help="float32: the workload as a Float32 matrix through the Float32 C ABI (a side line, "
+                         "not the headline metric)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="mixed form: keep the built-in GEMM variant rule instead of the learned autotuner")
     return ap.parse_args()
@@ -367,8 +370,90 @@ def gemm_traffic_ratio():
     return None
 
 
+def run_f32(args):
+    """The workload as a Float32 matrix (the reference's generic Tv =
+    Float32): splu's Float32 row scaling on the host, mfgpu_factor_f32 +
+    mfgpu_solve_f32 with host buffers, copies included, timed with CUDA events
+    on the library's stream; beside it the oracle's Float32 path (sgetrf /
+    strsm / sgemm fronts, Float32 solve) on the host cores.  One GPU."""
+    import torch
+
+    from pureumfpack import GpuContext, colamd_order, row_scaling, symbolic_mf
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    A64, B64 = make_workload(args.workload, args.nrhs)
+    A = A64.astype(np.float32)
+    B = np.asfortranarray(B64.astype(np.float32))
+    n, R = A.n, B.shape[1]
+    order, scale = workload_setup(args.workload)
+    q = colamd_order(A) if order == "colamd" else None
+    S = symbolic_mf(A, q=q)
+    Rs = row_scaling(A, scale)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    ctx = GpuContext(device=0)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.analyze(A, S)
+    Sd = A64.to_scipy()
+    refine = 0
+
+    def step(r):
+        ctx.factor_f32(A.nzval, Rs, False)
+        return ctx.solve(B, r)   # Float32 b and x after factor_f32
+
+    # fewest refinements reaching the Float32 residual level of the reference
+    # check (normwise relative residual <= 1e-6, i.e. a few Float32 ulps)
+    for r in range(4):
+        x = step(r)
+        res = float(np.max(np.linalg.norm(Sd @ x.astype(np.float64) - B, axis=0) / np.linalg.norm(B, axis=0)))
+        refine = r
+        if res <= 1e-6:
+            break
+    for _ in range(args.warmup):
+        step(refine)
+    clk = ClockSampler(0)
+    clk.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step(refine)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    sec = ev0.elapsed_time(ev1) / 1e3 / args.steps
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        cores = os.cpu_count() or 1
+        O.blas_threads(cores)
+        k = min(4, R)
+        t0 = time.perf_counter()
+        Fo = O.splu_f32(A, scale=scale, check=False, q=q)
+        t1 = time.perf_counter()
+        O.solve_f32(Fo, np.asfortranarray(B[:, :k]), refine=refine)
+        t2 = time.perf_counter()
+        cpu = {"value": (t1 - t0) + (t2 - t1) * R / k, "unit": "s", "cores": cores, "kind": "port",
+               "sample": f"oracle Float32 splu (symbolic + numeric, OpenBLAS sgetrf/strsm/sgemm, {cores} threads) "
+                         f"+ Float32 solve(refine={refine}) of {k} of {R} right-hand sides, scaled x{R / k:g}"}
+    line = {"metric": f"{args.workload} Float32 factor+solve s (host buffers, copies included)", "value": sec,
+            "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+            "dtype": "f32", "data": "synthetic", "refine": refine, "residual": res,
+            "config": {"workload": f"{args.workload} as Float32, n={n}, nrhs={R}, {order.upper()}",
+                       "l2": "working set (fronts) larger than L2; no explicit flush"},
+            "e2e": {"value": sec, "unit": "s", "h2d_bytes_per_step": int(A.nnz() * 4 + Rs.size * 4 + B.nbytes),
+                    "d2h_bytes_per_step": int(B.nbytes)},
+            "cpu_baseline": cpu, "clocks": clocks, "stats": {k: ctx.stats().get(k) for k in ("nsuper", "fronts", "nnz_l")}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.dtype == "float32":
+        return run_f32(args)
     if args.workload.startswith("batch-"):
         return run_batch(args)
     if args.impl == "reference":

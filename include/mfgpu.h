@@ -77,6 +77,14 @@ typedef struct mfgpu_symbolic mfgpu_symbolic;
 int mfgpu_symbolic_create(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* q,
                           mfgpu_symbolic** out);
 void mfgpu_symbolic_destroy(mfgpu_symbolic* sym);
+/* Symbolic analysis of nsys independent systems (1-based CSC each) as one
+ * block-diagonal forest: every system ordered (MFGPU_ORDER_AMD or
+ * MFGPU_ORDER_COLAMD, dense = 10) and analysed by symbolic_mf on its own,
+ * on all host cores, then concatenated -- the same object as symbolic_mf of
+ * the block-diagonal matrix with the concatenated orders.  The batch API
+ * analyses through it. */
+int mfgpu_symbolic_create_batch(int64_t nsys, const int64_t* n, const int64_t* const* colptr,
+                                const int64_t* const* rowval, int32_t ordering, mfgpu_symbolic** out);
 /* Opt-in relaxed amalgamation of the supernodes (no counterpart in the
  * reference, which keeps fundamental supernodes, src/symbolic.jl:178-179): a
  * supernode ending right before its parent merges into it when the merged

@@ -1,9 +1,11 @@
 // api_host.cpp -- C ABI of libmfgpu's host-side ordering and symbolic code.
 // Index arrays crossing the ABI are 1-based int64 (SparseMatrixCSC{Float64,Int64}).
 
+#include <atomic>
 #include <cstring>
 #include <exception>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../../include/mfgpu.h"
@@ -108,6 +110,53 @@ int mfgpu_symbolic_create(int64_t n, const int64_t* colptr, const int64_t* rowva
     }
     auto* h = new mfgpu_symbolic();
     h->s = mfgpu::symbolic_mf(n, cp.data(), ri.data(), q ? q0.data() : nullptr);
+    *out = h;
+  } catch (const std::exception& e) {
+    g_host_error = e.what();
+    return MFGPU_ERR_INTERNAL;
+  }
+  return MFGPU_OK;
+}
+
+int mfgpu_symbolic_create_batch(int64_t nsys, const int64_t* n, const int64_t* const* colptr,
+                                const int64_t* const* rowval, int32_t ordering, mfgpu_symbolic** out) {
+  if (!out) return MFGPU_ERR_ARGUMENT;
+  *out = nullptr;
+  if (nsys < 1 || !n || !colptr || !rowval || (ordering != MFGPU_ORDER_AMD && ordering != MFGPU_ORDER_COLAMD))
+    return MFGPU_ERR_ARGUMENT;
+  for (int64_t i = 0; i < nsys; ++i)
+    if (n[i] < 1 || !valid_csc(n[i], n[i], colptr[i], rowval[i])) return MFGPU_ERR_ARGUMENT;
+  std::vector<mfgpu::SymbolicMF> parts(nsys);
+  std::vector<std::string> errs(nsys);
+  // one task per system, handed out dynamically (the systems' sizes vary)
+  std::atomic<int64_t> next{0};
+  auto work = [&] {
+    for (int64_t i; (i = next.fetch_add(1)) < nsys;) {
+      try {
+        std::vector<idx_t> cp, ri;
+        to_zero_based(n[i], colptr[i], rowval[i], cp, ri);
+        const std::vector<idx_t> q = ordering == MFGPU_ORDER_AMD
+                                         ? mfgpu::amd_order_sym(n[i], cp.data(), ri.data(), 10.0)
+                                         : mfgpu::colamd_order(n[i], n[i], cp.data(), ri.data(), 10.0);
+        parts[i] = mfgpu::symbolic_mf(n[i], cp.data(), ri.data(), q.data());
+      } catch (const std::exception& e) {
+        errs[i] = e.what();
+      }
+    }
+  };
+  const int64_t nt = std::min<int64_t>(nsys, std::max(1u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  for (int64_t t = 1; t < nt; ++t) pool.emplace_back(work);
+  work();
+  for (auto& th : pool) th.join();
+  for (int64_t i = 0; i < nsys; ++i)
+    if (!errs[i].empty()) {
+      g_host_error = "system " + std::to_string(i + 1) + ": " + errs[i];
+      return MFGPU_ERR_INTERNAL;
+    }
+  try {
+    auto* h = new mfgpu_symbolic();
+    h->s = mfgpu::concat_symbolic(parts);
     *out = h;
   } catch (const std::exception& e) {
     g_host_error = e.what();

@@ -702,6 +702,52 @@ void relax_supernodes(SymbolicMF& S) {
   }
 }
 
+SymbolicMF concat_symbolic(const std::vector<SymbolicMF>& parts) {
+  SymbolicMF S;
+  idx_t n = 0, ns = 0, nu = 0, nc = 0;
+  for (const SymbolicMF& P : parts) {
+    n += P.n;
+    ns += P.nsuper();
+    nu += (idx_t)P.upd_idx.size();
+    nc += (idx_t)P.child_idx.size();
+  }
+  S.n = n;
+  S.qf.reserve(n);
+  S.parent.reserve(n);
+  S.colcount.reserve(n);
+  S.super_of.reserve(n);
+  S.sstart.reserve(ns + 1);
+  S.upd_ptr.reserve(ns + 1);
+  S.upd_idx.reserve(nu);
+  S.child_ptr.reserve(ns + 1);
+  S.child_idx.reserve(nc);
+  idx_t co = 0, so = 0, uo = 0, ko = 0;   // column, supernode, update entry, child entry offsets
+  for (const SymbolicMF& P : parts) {
+    for (idx_t j = 0; j < P.n; ++j) {
+      S.qf.push_back(P.qf[j] + co);
+      S.parent.push_back(P.parent[j] < 0 ? -1 : P.parent[j] + co);
+      S.colcount.push_back(P.colcount[j]);
+      S.super_of.push_back(P.super_of[j] + so);
+    }
+    const idx_t pns = P.nsuper();
+    for (idx_t k = 0; k < pns; ++k) {
+      S.sstart.push_back(P.sstart[k] + co);
+      S.upd_ptr.push_back(P.upd_ptr[k] + uo);
+      S.child_ptr.push_back(P.child_ptr[k] + ko);
+    }
+    for (idx_t u : P.upd_idx) S.upd_idx.push_back(u + co);
+    for (idx_t c : P.child_idx) S.child_idx.push_back(c + so);
+    co += P.n;
+    so += pns;
+    uo += (idx_t)P.upd_idx.size();
+    ko += (idx_t)P.child_idx.size();
+  }
+  S.sstart.push_back(n);
+  S.upd_ptr.push_back(uo);
+  S.child_ptr.push_back(ko);
+  return S;
+}
+
 void factor_colptrs(const SymbolicMF& S, std::vector<idx_t>& lp, std::vector<idx_t>& up) {
   const idx_t n = S.n, ns = S.nsuper();
   lp.assign(n + 1, 0);

@@ -57,6 +57,14 @@ struct SymbolicMF {
 // symbolic_mf(A; q): q (0-based) or nullptr for AMD.
 SymbolicMF symbolic_mf(idx_t n, const idx_t* colptr, const idx_t* rowind, const idx_t* q);
 
+// Independent systems as one block-diagonal forest: the parts' symbolic
+// objects concatenated with column, supernode and update-set offsets.  This
+// is the block-diagonal matrix's own symbolic_mf with the concatenated
+// orders: its postorder visits the trees root by root in column order, so
+// every system keeps its columns together and its own postorder, and no
+// fundamental supernode spans two systems.
+SymbolicMF concat_symbolic(const std::vector<SymbolicMF>& parts);
+
 // Amalgamation decisions: flag s = supernode s merges into its parent; no
 // merged supernode gets more than max_pivots columns.
 std::vector<char> amalgamation_marks(idx_t n, const idx_t* parent, idx_t ns, const idx_t* sstart,

@@ -199,6 +199,7 @@ struct mfgpu_ctx {
   // solve state
   SolveSchedule sched;
   DevBuf b_fsol, b_b, b_x, b_r, b_d, b_err, b_norm;   // b_fsol: solve arena (blocks, then x)
+  DevBuf b_f32;                                       // Float32 right-hand sides / solutions in transit
   // persistent solve: one cooperative launch per pass instead of one launch
   // per step, when the options ask for it (slower than per-step launches on
   // every measured case, many or few right-hand sides)
@@ -514,6 +515,13 @@ void configure_kernels() {
   CK(cudaFuncSetAttribute(k_solve_persistent<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)persistent_smem_bytes<T>()));
   done = true;
+}
+
+// dst[i] = (To)src[i] (Float32 right-hand sides in, Float32 solutions out).
+template <typename Ti, typename To>
+__global__ void k_convert(int64_t n, const Ti* __restrict__ src, To* __restrict__ dst) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (To)src[i];
 }
 
 __global__ void k_fill_i32(int32_t* p, int64_t n, int32_t v) {
@@ -1308,7 +1316,7 @@ void mfgpu_destroy(mfgpu_ctx* h) {
                     &h->b_u12_off, &h->b_skinny, &h->sched.d_skinny, &h->b_seg_end, &h->b_col_orig, &h->b_o_c1,
                     &h->b_o_np, &h->b_o_upd_off, &h->b_o_upd, &h->b_o_xpos, &h->b_fcu_ptr, &h->b_fcu,
                     &h->b_li, &h->b_lx, &h->b_ui,
-                    &h->b_ux, &h->b_fsol, &h->b_b, &h->b_x, &h->b_r, &h->b_d, &h->b_err, &h->b_norm,
+                    &h->b_ux, &h->b_fsol, &h->b_b, &h->b_x, &h->b_f32, &h->b_r, &h->b_d, &h->b_err, &h->b_norm,
                     &h->sched.d_ids, &h->sched.d_gemms, &h->sched.d_gemms_tc, &h->sched.d_phases, &h->b_bar,
                     &h->b_stamps};
   for (DevBuf* b : bufs) b->release();
@@ -1494,11 +1502,24 @@ int mfgpu_solve_f32(mfgpu_ctx* h, int64_t nrhs, const float* b, float* x, int32_
   const int64_t n = h->plan.n;
   if (nrhs < 0 || refine < 0 || (nrhs && n && (!b || !x))) return fail(h, MFGPU_ERR_ARGUMENT, "bad solve sizes");
   if (nrhs == 0 || n == 0) return MFGPU_OK;
-  std::vector<double> bd(b, b + n * nrhs), xd((size_t)(n * nrhs));
-  const int rc = mfgpu_solve(h, nrhs, bd.data(), n, xd.data(), n, refine);
-  if (rc != MFGPU_OK) return rc;
-  for (size_t k = 0; k < xd.size(); ++k) x[k] = (float)xd[k];
-  return MFGPU_OK;
+  // Float32 b crosses the bus and is widened on the device; x is rounded to
+  // Float32 there and copied back
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    const int64_t len = n * nrhs;
+    h->b_f32.ensure((size_t)len * 4);
+    h->b_b.ensure((size_t)len * 8);
+    h->b_x.ensure((size_t)len * 8);
+    CK(cudaMemcpyAsync(h->b_f32.p, b, len * 4, cudaMemcpyHostToDevice, st));
+    k_convert<float, double><<<grid1(len, 256), 256, 0, st>>>(len, h->b_f32.as<float>(), h->b_b.as<double>());
+    solve_dispatch(h, nrhs, h->b_b.as<double>(), n, h->b_x.as<double>(), n, refine);
+    k_convert<double, float><<<grid1(len, 256), 256, 0, st>>>(len, h->b_x.as<double>(), h->b_f32.as<float>());
+    CK(cudaMemcpyAsync(x, h->b_f32.p, len * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    prof_flush(h);
+    return solve_status(h);
+  });
 }
 
 int mfgpu_factor_sizes(mfgpu_ctx* h, int64_t* out3) {
@@ -1927,20 +1948,17 @@ extern "C" int mfgpu_batch_analyze(mfgpu_ctx* h, int64_t nsys, const int64_t* n,
     const int64_t N = B.off[nsys];
     B.colptr.resize(N + 1);
     B.rowval.resize(B.nz_off[nsys]);
-    std::vector<int64_t> q(N);
     B.colptr[0] = 1;
-    for (int64_t i = 0; i < nsys; ++i) {
+    parallel_for(nsys, [&](int64_t i) {
       const int64_t o = B.off[i], z = B.nz_off[i], ni = n[i];
       for (int64_t j = 1; j <= ni; ++j) B.colptr[o + j] = z + colptr[i][j];
       for (int64_t k = 0; k < colptr[i][ni] - 1; ++k) B.rowval[z + k] = rowval[i][k] + o;
-      const int rc = ordering == MFGPU_ORDER_AMD ? mfgpu_amd_order(ni, colptr[i], rowval[i], 10.0, q.data() + o)
-                                                 : mfgpu_colamd_order(ni, ni, colptr[i], rowval[i], 10.0, q.data() + o);
-      if (rc != MFGPU_OK) return fail(h, rc, "batch: ordering of system " + std::to_string(i + 1) + " failed");
-      for (int64_t k = 0; k < ni; ++k) q[o + k] += o;
-    }
+    });
+    // orderings and symbolic analyses per system on all host cores, then one
+    // block-diagonal forest
     mfgpu_symbolic* sym = nullptr;
-    int rc = mfgpu_symbolic_create(N, B.colptr.data(), B.rowval.data(), q.data(), &sym);
-    if (rc != MFGPU_OK) return fail(h, rc, "batch: symbolic analysis failed");
+    int rc = mfgpu_symbolic_create_batch(nsys, n, colptr, rowval, ordering, &sym);
+    if (rc != MFGPU_OK) return fail(h, rc, std::string("batch: symbolic analysis failed: ") + mfgpu_host_last_error());
     std::unique_ptr<mfgpu_symbolic, void (*)(mfgpu_symbolic*)> guard(sym, mfgpu_symbolic_destroy);
     // the forest keeps every system's columns together and in system order
     const auto& S = sym->s;

@@ -5,14 +5,45 @@
 #include "host/symbolic.h"
 
 #include <algorithm>
+#include <atomic>
+#include <exception>
 #include <map>
 #include <numeric>
 #include <stdexcept>
+#include <thread>
 
 namespace mfgpu {
 
 namespace {
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// body(i) for i in [0, n) on the host's cores (independent iterations, each
+// writing its own outputs); the first exception is rethrown after the join.
+template <typename F>
+void parallel_range(int64_t n, F&& body) {
+  const int64_t grain = 4096;
+  const int64_t nt = std::min<int64_t>(std::max<int64_t>(1, n / grain), std::max(1u, std::thread::hardware_concurrency()));
+  if (nt <= 1) {
+    for (int64_t i = 0; i < n; ++i) body(i);
+    return;
+  }
+  std::atomic<int64_t> next{0};
+  std::exception_ptr err;
+  std::atomic<bool> failed{false};
+  auto work = [&] {
+    try {
+      for (int64_t b; !failed && (b = next.fetch_add(grain)) < n;)
+        for (int64_t i = b; i < std::min(n, b + grain); ++i) body(i);
+    } catch (...) {
+      if (!failed.exchange(true)) err = std::current_exception();
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int64_t t = 1; t < nt; ++t) pool.emplace_back(work);
+  work();
+  for (auto& th : pool) th.join();
+  if (err) std::rethrow_exception(err);
+}
 }  // namespace
 
 namespace {
@@ -100,7 +131,8 @@ void build_inverse_steps(Plan& P) {
 }
 }  // namespace
 
-void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf, const int64_t* parent,
+namespace {
+void build_plan_core(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf, const int64_t* parent,
                 int64_t ns, const int64_t* sstart, const int64_t* upd_ptr, const int64_t* upd_idx, Plan& P) {
   P = Plan();
   P.n = n;
@@ -166,9 +198,9 @@ void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const i
 
   // relative maps: position of each child update row in the parent front
   P.rel.assign(P.upd.size(), -1);
-  for (int64_t k = 0; k < ns; ++k) {
+  parallel_range(ns, [&](int64_t k) {
     const int32_t ps = P.parent_super[k];
-    if (ps < 0) continue;
+    if (ps < 0) return;
     const int32_t pc1 = P.c1[ps], pc2 = P.c1[ps] + P.np[ps] - 1;
     const int32_t* pu = P.upd.data() + P.upd_off[ps];
     for (int64_t p = P.upd_off[k]; p < P.upd_off[k + 1]; ++p) {
@@ -182,7 +214,7 @@ void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const i
         P.rel[p] = P.np[ps] + (int32_t)(it - pu);
       }
     }
-  }
+  });
 
   // ---- slots: supernodes ordered by (height, small before large, id) -------
   P.slot_super.resize(ns);
@@ -235,25 +267,22 @@ void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const i
   P.v_srow.resize(nz);
   P.v_frow.assign(nz, -1);
   std::vector<int32_t> vrow(nz);
-  {
-    std::vector<std::pair<int64_t, int64_t>> tmp;
-    for (int64_t g = 0; g < n; ++g) {
-      tmp.clear();
-      for (int64_t p = colptr[qf[g]]; p < colptr[qf[g] + 1]; ++p) tmp.push_back({pinv[rowval[p]], p});
-      std::sort(tmp.begin(), tmp.end());
-      for (size_t t = 0; t < tmp.size(); ++t) {
-        if (t && tmp[t].first == tmp[t - 1].first) throw std::invalid_argument("duplicate entries in A");
-        const int64_t q = vcol[g] + (int64_t)t;
-        vrow[q] = (int32_t)tmp[t].first;
-        P.v_src[q] = (int32_t)tmp[t].second;
-        P.v_srow[q] = (int32_t)rowval[tmp[t].second];
-      }
+  parallel_range(n, [&](int64_t g) {
+    thread_local std::vector<std::pair<int64_t, int64_t>> tmp;
+    tmp.clear();
+    for (int64_t p = colptr[qf[g]]; p < colptr[qf[g] + 1]; ++p) tmp.push_back({pinv[rowval[p]], p});
+    std::sort(tmp.begin(), tmp.end());
+    for (size_t t = 0; t < tmp.size(); ++t) {
+      if (t && tmp[t].first == tmp[t - 1].first) throw std::invalid_argument("duplicate entries in A");
+      const int64_t q = vcol[g] + (int64_t)t;
+      vrow[q] = (int32_t)tmp[t].first;
+      P.v_src[q] = (int32_t)tmp[t].second;
+      P.v_srow[q] = (int32_t)rowval[tmp[t].second];
     }
-  }
+  });
   P.fc_vbeg.assign(cb, 0);
   P.fc_vend.assign(cb, 0);
-  int64_t assigned = 0;
-  for (int64_t s = 0; s < ns; ++s) {
+  parallel_range(ns, [&](int64_t s) {
     const int32_t c1 = P.c1[s], c2 = c1 + P.np[s] - 1, npv = P.np[s];
     const int32_t* us = P.upd.data() + P.upd_off[s];
     auto front_row = [&](int32_t i) -> int32_t {
@@ -275,11 +304,11 @@ void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const i
         const int64_t q = vcol[g] + (r - rb);
         if (P.v_frow[q] != -1) throw std::logic_error("V entry assembled twice");
         P.v_frow[q] = front_row(*r);
-        ++assigned;
       }
     }
-  }
-  if (assigned != nz) throw std::invalid_argument("pattern of A is not covered by the symbolic structure");
+  });
+  if (std::count(P.v_frow.begin(), P.v_frow.end(), -1) != 0)
+    throw std::invalid_argument("pattern of A is not covered by the symbolic structure");
 
   // ---- children contributions per parent front column ------------------------
   P.fc_ch_ptr.assign(cb + 1, 0);
@@ -375,6 +404,16 @@ void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const i
   P.seg_end.resize(n);
   for (int64_t s = 0; s < ns; ++s)
     for (int32_t a = 0; a < P.np[s]; ++a) P.seg_end[P.c1[s] + a] = P.np[s];
+  // original entries assembled into each front (launch traffic accounting)
+  P.front_nv.assign(ns, 0);
+  for (int64_t s = 0; s < ns; ++s)
+    for (int32_t c = 0; c < P.nf[s]; ++c) P.front_nv[s] += P.fc_vend[P.colbase[s] + c] - P.fc_vbeg[P.colbase[s] + c];
+}
+}  // namespace
+
+void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf, const int64_t* parent,
+                int64_t ns, const int64_t* sstart, const int64_t* upd_ptr, const int64_t* upd_idx, Plan& P) {
+  build_plan_core(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, P);
   set_layout(P, false);
 }
 
@@ -394,8 +433,7 @@ void attach_original(Plan& P, int64_t ns, const int64_t* sstart, const int64_t* 
   P.o_upd.assign(upd_idx, upd_idx + upd_ptr[ns]);
   P.o_xpos.resize(upd_ptr[ns]);
   P.col_orig.resize(n);
-  double fl = 0;
-  for (int64_t s = 0; s < ns; ++s) {
+  parallel_range(ns, [&](int64_t s) {
     const int32_t c1 = (int32_t)sstart[s], npv = (int32_t)(sstart[s + 1] - sstart[s]);
     const int32_t x = front_of[c1], xc1 = P.c1[x], xnp = P.np[x];
     if (front_of[c1 + npv - 1] != x) throw std::logic_error("original supernode split across fronts");
@@ -417,7 +455,10 @@ void attach_original(Plan& P, int64_t ns, const int64_t* sstart, const int64_t* 
         P.o_xpos[p] = xnp + (int32_t)(it - xu);
       }
     }
-    const double a = npv, u = (double)(upd_ptr[s + 1] - upd_ptr[s]);
+  });
+  double fl = 0;
+  for (int64_t s = 0; s < ns; ++s) {
+    const double a = P.o_np[s], u = (double)(upd_ptr[s + 1] - upd_ptr[s]);
     fl += 2.0 / 3.0 * a * a * a + 2.0 * a * a * u + 2.0 * a * u * u;
   }
   P.flops_orig = fl;
@@ -479,9 +520,9 @@ void build_plan_merged(int64_t n, const int64_t* colptr, const int64_t* rowval, 
     first = s + 1;
   }
   ms.push_back(n);
-  build_plan(n, colptr, rowval, qf, parent, (int64_t)ms.size() - 1, ms.data(), mup.data(), mui.data(), P);
+  build_plan_core(n, colptr, rowval, qf, parent, (int64_t)ms.size() - 1, ms.data(), mup.data(), mui.data(), P);
   attach_original(P, ns, sstart, upd_ptr, upd_idx);
-  build_launches(P, false);
+  set_layout(P, false);
 }
 
 void set_layout(Plan& P, bool lean) {
@@ -595,9 +636,7 @@ void assembly_work(const Plan& P, int32_t s, Launch& l) {
     e += 3.0 * m * m;
   }
   l.elems += e;
-  int64_t nv = 0;
-  for (int32_t c = 0; c < P.nf[s]; ++c) nv += P.fc_vend[P.colbase[s] + c] - P.fc_vbeg[P.colbase[s] + c];
-  l.extra_bytes += 12.0 * nv;
+  l.extra_bytes += 12.0 * P.front_nv[s];
 }
 // Small fronts: assembly plus the dense factorization in shared memory.
 void front_work(const Plan& P, int32_t s, Launch& l) {
@@ -633,6 +672,7 @@ void build_launches_core(Plan& P, bool safe) {
   P.launches.clear();
   P.has_speculative = false;
   std::vector<int32_t> large;
+  std::vector<PanelTask> cls[4];   // pivoting panels by row class, then speculative (reused per step)
   for (int32_t L = 0; L < P.nlevels; ++L) {
     // fused small fronts
     if (P.level_large[L] > P.level_slot[L]) {
@@ -660,7 +700,7 @@ void build_launches_core(Plan& P, bool safe) {
       Launch lt{kLaunchTrsm, L, (int64_t)P.trsm_tasks.size(), 0, 0};
       Launch lg{kLaunchGemm, L, (int64_t)P.gemm_tasks.size(), 0, 0};
       // panel tasks of this step, one launch per row class (64 / 128 / 256)
-      std::vector<PanelTask> cls[4];   // pivoting panels by row class, then speculative
+      for (auto& c : cls) c.clear();
       for (int32_t s : large) {
         const int32_t npv = P.np[s], nf = P.nf[s];
         if (npv <= k0) continue;

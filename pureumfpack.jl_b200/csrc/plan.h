@@ -190,6 +190,7 @@ struct Plan {
   std::vector<int64_t> fcu_ptr;        // per front column (fc_total + 1)
   std::vector<UBlock> fcu;             // U blocks written from each front column
   double flops_orig = 0;               // flops of the original structure (no merged zeros)
+  std::vector<int64_t> front_nv;       // original entries assembled into each front
   // statistics
   double flops = 0, flops_getrf = 0, flops_trsm = 0, flops_gemm = 0;
   double assembly_bytes_per_elem = 0;  // sum of nf^2 + 3 m^2 + nu^2 element moves (x sizeof(T) for bytes)

@@ -28,6 +28,8 @@ SIGNATURES = [
     ("mfgpu_amd_order", ctypes.c_int, [i64, i64p, i64p, f64, i64p]),
     ("mfgpu_colamd_order", ctypes.c_int, [i64, i64, i64p, i64p, f64, i64p]),
     ("mfgpu_symbolic_create", ctypes.c_int, [i64, i64p, i64p, i64p, ctypes.POINTER(vp)]),
+    ("mfgpu_symbolic_create_batch", ctypes.c_int, [i64, i64p, ctypes.POINTER(vp), ctypes.POINTER(vp), i32,
+                                                   ctypes.POINTER(vp)]),
     ("mfgpu_symbolic_destroy", None, [vp]),
     ("mfgpu_symbolic_relax", ctypes.c_int, [vp]),
     ("mfgpu_symbolic_sizes", ctypes.c_int, [vp, i64p]),

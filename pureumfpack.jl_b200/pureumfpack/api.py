@@ -199,6 +199,26 @@ def symbolic_mf(A: SparseCSC, q=None, relax: bool = False) -> SymbolicMF:
     _check_host(lib.mfgpu_symbolic_create(A.n, L.ptr(_i(A.colptr)), L.ptr(_i(A.rowval)), L.ptr(qa), ctypes.byref(h)))
     if relax:
         _check_host(lib.mfgpu_symbolic_relax(h))
+    return _symbolic_from_handle(h)
+
+
+def symbolic_batch(As, ordering: str = "amd") -> SymbolicMF:
+    """Symbolic analysis of independent square systems as one block-diagonal
+    forest: each system ordered (AMD or COLAMD) and analysed by symbolic_mf
+    on its own, on all host cores, then concatenated -- equal to
+    symbolic_mf of the block-diagonal matrix with the concatenated orders."""
+    lib = L.lib()
+    cps = [_i(A.colptr) for A in As]
+    rvs = [_i(A.rowval) for A in As]
+    ns = np.array([A.n for A in As], dtype=np.int64)
+    h = ctypes.c_void_p()
+    _check_host(lib.mfgpu_symbolic_create_batch(len(As), L.ptr(ns), L.ptr_array(cps), L.ptr_array(rvs),
+                                                {"amd": 0, "colamd": 1}[ordering], ctypes.byref(h)))
+    return _symbolic_from_handle(h)
+
+
+def _symbolic_from_handle(h) -> SymbolicMF:
+    lib = L.lib()
     sz = np.empty(4, np.int64)
     lib.mfgpu_symbolic_sizes(h, L.ptr(sz))
     n, ns, nupd, nch = (int(v) for v in sz)

@@ -57,6 +57,21 @@ def test_forest_symbolic_equals_per_system(ordering):
     assert total == pytest.approx(sum(system_cost(A, ordering) for A in As), rel=1e-12)
 
 
+@pytest.mark.parametrize("ordering", ["amd", "colamd"])
+def test_parallel_batch_symbolic_equals_block_diagonal(ordering):
+    """symbolic_batch (every system ordered and analysed on its own thread,
+    then concatenated) is field for field the block-diagonal analysis."""
+    from pureumfpack.api import symbolic_batch
+
+    As = _batch(40, seed=5) + [M.convdiff3d(5), M.random_unsym(120, 4, 10.0, seed=2)]
+    order = amd_order_sym if ordering == "amd" else colamd_order
+    Abd, offs = _block_diag(As)
+    S = symbolic_mf(Abd, q=np.concatenate([order(A) + o for A, o in zip(As, offs)]))
+    P = symbolic_batch(As, ordering)
+    for f in ("qf", "parent", "colcount", "sstart", "upd_ptr", "upd_idx", "child_ptr", "child_idx"):
+        np.testing.assert_array_equal(getattr(P, f), getattr(S, f), err_msg=f)
+
+
 def test_partition_covers_and_balances():
     rng = np.random.default_rng(3)
     costs = rng.pareto(1.5, 300) + 1.0
