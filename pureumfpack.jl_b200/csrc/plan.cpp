@@ -696,15 +696,25 @@ void build_launches_core(Plan& P, bool safe) {
     }
     int32_t maxnp = 0;
     for (int32_t s : large) maxnp = std::max(maxnp, P.np[s]);
+    // Blocked right-looking LU of each pivot block: 64-column panels grouped
+    // into blocks of kUpdateBlock columns.  Inside a block the updates stay
+    // on the block's own columns (K = 64); the rows of the next panel get the
+    // block's earlier panels applied to the columns right of the block just
+    // before their triangular solve (K <= kUpdateBlock - 64); the rest of the
+    // pivot block and the U12 rows receive the whole block at once
+    // (K = kUpdateBlock) when its last panel is done.
+    std::vector<GemmTask> g_left, g_step;
     for (int32_t k0 = 0; k0 < maxnp; k0 += kPanel) {
       Launch lt{kLaunchTrsm, L, (int64_t)P.trsm_tasks.size(), 0, 0};
-      Launch lg{kLaunchGemm, L, (int64_t)P.gemm_tasks.size(), 0, 0};
       // panel tasks of this step, one launch per row class (64 / 128 / 256)
       for (auto& c : cls) c.clear();
+      g_left.clear();
+      g_step.clear();
       for (int32_t s : large) {
         const int32_t npv = P.np[s], nf = P.nf[s];
         if (npv <= k0) continue;
         const int32_t kb = std::min(kPanel, npv - k0), k1 = k0 + kb;
+        const int32_t b0 = k0 - k0 % kUpdateBlock, b1 = std::min(b0 + kUpdateBlock, npv);
         // Speculative panels everywhere; the pivoting variants only run in
         // the safe rerun after a speculative panel met a larger candidate.
         // pivot rows of the panel's columns: up to the end of the last
@@ -731,23 +741,44 @@ void build_launches_core(Plan& P, bool safe) {
           ++lt.count;
         }
         const int64_t base = P.front_off[s];
-        auto add_gemm = [&](int64_t a, int64_t b, int64_t c, int32_t m, int32_t n, int32_t k) {
+        // C(r, c) -= A(r, kk) * B(kk, c) on front entries (row, column)
+        auto upd = [&](std::vector<GemmTask>& into, int32_t r, int32_t cc, int32_t kk, int32_t m, int32_t n,
+                       int32_t k) {
           if (m <= 0 || n <= 0 || k <= 0) return;
           GemmTask g{};
-          g.a = a; g.b = b; g.c = c;
+          g.a = base + r + (int64_t)kk * nf;
+          g.b = base + kk + (int64_t)cc * nf;
+          g.c = base + r + (int64_t)cc * nf;
           g.m = m; g.n = n; g.k = k;
           g.lda = g.ldb = g.ldc = nf;
-          lg.flops += 2.0 * m * n * k;
-          lg.elems += 2.0 * m * n + (double)m * k + (double)k * n;
-          push_gemm(P, lg, g);
+          into.push_back(g);
         };
-        if (npv > k1) {
-          add_gemm(base + k1 + (int64_t)k0 * nf, base + k0 + (int64_t)k1 * nf, base + k1 + (int64_t)k1 * nf, nf - k1,
-                   npv - k1, kb);
-          add_gemm(base + k1 + (int64_t)k0 * nf, base + k0 + (int64_t)npv * nf, base + k1 + (int64_t)npv * nf,
-                   npv - k1, nf - npv, kb);
+        // the rows of this panel, right of the block: the block's earlier
+        // panels (after this panel's interchanges, so its own launch in the
+        // pivoting rerun; speculative panels do not interchange, so the
+        // previous step's update launch carries it)
+        if (safe && k0 > b0) upd(g_left, k0, b1, b0, kb, nf - b1, k0 - b0);
+        // this panel on the block's remaining columns, every row below
+        upd(g_step, k1, k1, k0, nf - k1, b1 - k1, kb);
+        if (!safe && k1 < b1) {
+          const int32_t kbn = std::min(kPanel, npv - k1);
+          upd(g_step, k1, b1, b0, kbn, nf - b1, k1 - b0);   // the next panel's rows, right of the block
+        }
+        if (k1 == b1) {   // block done: the rest of the pivot block and the U12 rows
+          upd(g_step, b1, b1, b0, nf - b1, npv - b1, b1 - b0);
+          upd(g_step, b1, npv, b0, npv - b1, nf - npv, b1 - b0);
         }
       }
+      auto emit_gemms = [&](const std::vector<GemmTask>& tasks) {
+        if (tasks.empty()) return;
+        Launch lg{kLaunchGemm, L, (int64_t)P.gemm_tasks.size(), 0, 0};
+        for (const GemmTask& g : tasks) {
+          lg.flops += 2.0 * g.m * g.n * g.k;
+          lg.elems += 2.0 * g.m * g.n + (double)g.m * g.k + (double)g.k * g.n;
+          push_gemm(P, lg, g);
+        }
+        P.launches.push_back(lg);
+      };
       for (int c = 0; c < 4; ++c) {
         if (cls[c].empty()) continue;
         Launch lp{kLaunchPanel, L, (int64_t)P.panel_tasks.size(), (int64_t)cls[c].size(), (int64_t)cls[c].size()};
@@ -761,8 +792,9 @@ void build_launches_core(Plan& P, bool safe) {
         }
         P.launches.push_back(lp);
       }
+      emit_gemms(g_left);
       if (lt.count) P.launches.push_back(lt);
-      if (lg.count) P.launches.push_back(lg);
+      emit_gemms(g_step);
     }
     // deferred Schur update of every large front: F22 -= L21 * U12
     Launch lg{kLaunchGemm, L, (int64_t)P.gemm_tasks.size(), 0, 0};

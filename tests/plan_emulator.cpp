@@ -14,6 +14,7 @@
 // host/symbolic.cpp; never linked into the library.
 #include <cmath>
 #include <cstdint>
+#include <algorithm>
 #include <cstring>
 #include <utility>
 #include <vector>
@@ -78,7 +79,180 @@ std::vector<std::vector<double>> factor_fronts(const Plan& P, const double* nzva
   return F;
 }
 
+// The same factorization executed launch by launch from the plan's launch
+// list (the device's sequence): small fronts, column assembly, panels
+// (speculative: no interchanges and the partial-pivoting order check;
+// pivoting: rows k0..seg-1 with the interchanges applied to the whole rows),
+// the panel triangular solves (L rows r0.. times inv(U_kk), inv(L_kk) times
+// the U rows right of the panel) and every GEMM task C -= A B.  Returns false
+// when a speculative panel met a larger candidate (the device then reruns
+// with the pivoting launch list).
+bool run_launches(const Plan& P, const double* nzval, std::vector<double>& pool, std::vector<int32_t>& ipiv) {
+  std::vector<double> vx(P.nnz_a);
+  for (int64_t p = 0; p < P.nnz_a; ++p) vx[p] = nzval[P.v_src[p]];
+  pool.assign((size_t)P.front_elems, 0.0);
+  bool ok = true;
+  auto F = [&](int s, int r, int c) -> double& { return pool[P.front_off[s] + r + (size_t)c * P.nf[s]]; };
+  auto assemble = [&](int s) {
+    const int nf = P.nf[s];
+    for (int c = 0; c < nf; ++c)
+      for (int r = 0; r < nf; ++r) F(s, r, c) = 0.0;
+    for (int c = 0; c < nf; ++c) {
+      const int64_t fc = P.colbase[s] + c;
+      for (int p = P.fc_vbeg[fc]; p < P.fc_vend[fc]; ++p) F(s, P.v_frow[p], c) = vx[p];
+    }
+    for (int ci = P.child_ptr[s + 1] - 1; ci >= P.child_ptr[s]; --ci) {
+      const int k = P.child_idx[ci], m = P.nu[k], npk = P.np[k];
+      const int32_t* rl = P.rel.data() + P.upd_off[k];
+      for (int t = 0; t < m; ++t)
+        for (int r = 0; r < m; ++r) F(s, rl[r], rl[t]) += F(k, npk + r, npk + t);
+    }
+  };
+  for (const Launch& l : P.launches) {
+    if (l.kind == kLaunchSmall) {
+      for (int64_t i = l.first; i < l.first + l.count; ++i) {
+        const int s = P.small_tasks[i], nf = P.nf[s], np = P.np[s], c1 = P.c1[s];
+        assemble(s);
+        for (int k = 0; k < np; ++k) {
+          const int seg = P.seg_end[c1 + k];
+          int piv = k;
+          double best = -1.0;
+          for (int i2 = k; i2 < seg; ++i2)
+            if (std::fabs(F(s, i2, k)) > best) {
+              best = std::fabs(F(s, i2, k));
+              piv = i2;
+            }
+          if (piv != k)
+            for (int j = 0; j < nf; ++j) std::swap(F(s, k, j), F(s, piv, j));
+          ipiv[c1 + k] = piv;
+          const double d = F(s, k, k);
+          for (int i2 = k + 1; i2 < nf; ++i2)
+            if (i2 >= seg || d != 0.0) F(s, i2, k) /= d;
+          for (int j = k + 1; j < nf; ++j)
+            for (int i2 = k + 1; i2 < nf; ++i2) F(s, i2, j) -= F(s, i2, k) * F(s, k, j);
+        }
+      }
+    } else if (l.kind == kLaunchAssemble) {
+      int last = -1;
+      for (int64_t fc = l.first; fc < l.first + l.count; ++fc)
+        if (P.fc_super[fc] != last) assemble(last = P.fc_super[fc]);
+    } else if (l.kind == kLaunchPanel) {
+      for (int64_t i = l.first; i < l.first + l.count; ++i) {
+        const PanelTask pt = P.panel_tasks[i];
+        const int s = pt.s, k0 = pt.k0, nf = P.nf[s], np = P.np[s], c1 = P.c1[s];
+        const int kb = std::min(kPanel, np - k0), k1 = k0 + kb;
+        const bool spec = pt.mode == kPanelSpeculative;
+        const int R = spec ? kb : P.seg_end[c1 + k1 - 1] - k0;
+        for (int j = k0; j < k1; ++j) {
+          const int seg = std::min(k0 + R, P.seg_end[c1 + j]);
+          int piv = j;
+          if (!spec) {
+            double best = -1.0;
+            for (int i2 = j; i2 < seg; ++i2)
+              if (std::fabs(F(s, i2, j)) > best) {
+                best = std::fabs(F(s, i2, j));
+                piv = i2;
+              }
+            if (piv != j)
+              for (int c = 0; c < nf; ++c) std::swap(F(s, j, c), F(s, piv, c));
+          } else {
+            for (int i2 = j + 1; i2 < seg; ++i2)
+              if (std::fabs(F(s, i2, j)) > std::fabs(F(s, j, j))) ok = false;
+            if (F(s, j, j) == 0.0) ok = false;
+          }
+          ipiv[c1 + j] = piv;   // front-local
+          const double d = F(s, j, j);
+          for (int i2 = j + 1; i2 < k0 + R; ++i2)
+            if (d != 0.0) F(s, i2, j) /= d;
+          for (int c = j + 1; c < k1; ++c)
+            for (int i2 = j + 1; i2 < k0 + R; ++i2) F(s, i2, c) -= F(s, i2, j) * F(s, j, c);
+        }
+      }
+    } else if (l.kind == kLaunchTrsm) {
+      for (int64_t i = l.first; i < l.first + l.count; ++i) {
+        const TrsmTask t = P.trsm_tasks[i];
+        const int s = t.s, k0 = t.k0, nf = P.nf[s], np = P.np[s], c1 = P.c1[s];
+        const int kb = std::min(kPanel, np - k0), k1 = k0 + kb;
+        // L rows r0..nf-1: X U_kk = A  (column by column)
+        for (int r = t.r0; r < nf; ++r)
+          for (int j = k0; j < k1; ++j) {
+            double v = F(s, r, j);
+            for (int q = k0; q < j; ++q) v -= F(s, r, q) * F(s, q, j);
+            F(s, r, j) = v / F(s, j, j);
+            if (t.check && r < P.seg_end[c1 + j] && std::fabs(F(s, r, j)) > 1.0) ok = false;
+          }
+        // U rows k0..k1-1 right of the panel: L_kk X = A (unit lower)
+        for (int c = k1; c < nf; ++c)
+          for (int r = k0; r < k1; ++r) {
+            double v = F(s, r, c);
+            for (int q = k0; q < r; ++q) v -= F(s, r, q) * F(s, q, c);
+            F(s, r, c) = v;
+          }
+      }
+    } else if (l.kind == kLaunchGemm) {
+      for (int64_t i = l.first; i < l.first + l.count; ++i) {
+        const GemmTask& g = P.gemm_tasks[i];
+        double* A = pool.data() + g.a;
+        double* B = pool.data() + g.b;
+        double* C = pool.data() + g.c;
+        for (int c = 0; c < g.n; ++c)
+          for (int k = 0; k < g.k; ++k) {
+            const double b = B[k + (int64_t)c * g.ldb];
+            if (b == 0.0) continue;
+            for (int r = 0; r < g.m; ++r) C[r + (int64_t)c * g.ldc] -= A[r + (int64_t)k * g.lda] * b;
+          }
+      }
+    }
+  }
+  return ok;
+}
+
 }  // namespace
+
+// Run the plan's launch list (speculative, then the pivoting rerun when a
+// speculative panel fails, as the device does) and return the maximum
+// difference of every front against the dense emulation above, relative to
+// the front's largest entry; ipiv must agree exactly (out[1] = mismatches,
+// out[2] = 1 if the pivoting rerun ran, out[3] = GEMM launches).
+extern "C" int emu_check_launches(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+                                  const int64_t* q, int merge, double* out) {
+  const SymbolicMF S = symbolic_mf(n, colptr, rowval, q);
+  Plan P;
+  if (merge)
+    build_plan_merged(n, colptr, rowval, S.qf.data(), S.parent.data(), S.nsuper(), S.sstart.data(),
+                      S.upd_ptr.data(), S.upd_idx.data(), P, kMergeMaxPivots);
+  else
+    build_plan(n, colptr, rowval, S.qf.data(), S.parent.data(), S.nsuper(), S.sstart.data(), S.upd_ptr.data(),
+               S.upd_idx.data(), P);
+  std::vector<int32_t> ipiv_ref(n), ipiv(n);
+  const std::vector<std::vector<double>> F = factor_fronts(P, nzval, ipiv_ref);
+  std::vector<double> pool;
+  bool reran = false;
+  if (!run_launches(P, nzval, pool, ipiv)) {
+    build_launches(P, true);
+    reran = true;
+    run_launches(P, nzval, pool, ipiv);
+  }
+  double worst = 0;
+  for (int64_t x = 0; x < P.ns; ++x) {
+    const int nf = P.nf[x];
+    double mx = 0, d = 0;
+    for (int64_t e = 0; e < (int64_t)nf * nf; ++e) {
+      mx = std::max(mx, std::fabs(F[x][e]));
+      d = std::max(d, std::fabs(F[x][e] - pool[P.front_off[x] + e]));
+    }
+    if (mx > 0) worst = std::max(worst, d / mx);
+  }
+  int64_t mism = 0;
+  for (int64_t j = 0; j < n; ++j) mism += ipiv[j] != ipiv_ref[j];
+  int64_t ng = 0;
+  for (const Launch& l : P.launches) ng += l.kind == kLaunchGemm;
+  out[0] = worst;
+  out[1] = (double)mism;
+  out[2] = reran ? 1.0 : 0.0;
+  out[3] = (double)ng;
+  return 0;
+}
 
 // Factor A (0-based CSC pattern, values) with symbolic_mf(A; q) (q 0-based
 // or null for AMD), merged fronts or one front per supernode.  stats: nnz_l,
