@@ -24,10 +24,10 @@ constexpr int kPanel = 64;           // panel width of the blocked large-front f
 // cost more than the hand-overs it saves (64^3 Poisson: 0.31 TFLOP of
 // inverses with this limit, 1.06 without).
 constexpr int64_t kMergeMaxPivots = 1024;
-constexpr int kPivRowsSmem = 256;
+constexpr int kPivRowsSmem = 256;    // pivot rows a partial-pivoting panel keeps in shared memory
 // Pivot-block columns whose panel updates are applied together beyond the
 // block (blocked right-looking LU; a multiple of the 64-column panel).
-constexpr int32_t kUpdateBlock = 256;    // pivot rows a partial-pivoting panel keeps in shared memory
+constexpr int32_t kUpdateBlock = 256;
 constexpr int kTcTile = 128;         // tile edge of the tensor-core GEMM of the FP32 fronts
 
 enum PanelMode : int32_t {
