@@ -17,6 +17,7 @@ const libmfgpu = get(ENV, "PUREUMFPACK_MFGPU", joinpath(@__DIR__, "..", "pureumf
 mutable struct Handle
     ptr::Ptr{Cvoid}
     n::Int
+    f32::Bool   # the last factorization is of a Float32 matrix
 end
 
 function _check(h::Handle, rc::Cint)
@@ -32,14 +33,14 @@ function create(; device::Integer = 0, precision::Integer = 0)
     out = Ref{Ptr{Cvoid}}(C_NULL)
     rc = ccall((:mfgpu_create, libmfgpu), Cint, (Ref{NTuple{4, Int32}}, Ref{Ptr{Cvoid}}), opts, out)
     rc == 0 || error("mfgpu_create failed ($rc)")
-    h = Handle(out[], 0)
+    h = Handle(out[], 0, false)
     finalizer(x -> ccall((:mfgpu_destroy, libmfgpu), Cvoid, (Ptr{Cvoid},), x.ptr), h)
     return h
 end
 
 # mfgpu_analyze from the reference's SymbolicMF (src/symbolic.jl:203-209):
 # update set of supernode s = colstruct[sstart[s+1]-1].
-function analyze!(h::Handle, A::SparseMatrixCSC{Float64, Int64}, S)
+function analyze!(h::Handle, A::SparseMatrixCSC{<:Union{Float64, Float32}, Int64}, S)
     n = size(A, 2)
     nsuper = length(S.sstart) - 1
     upd_ptr = Vector{Int64}(undef, nsuper + 1)
@@ -67,11 +68,25 @@ function factor!(h::Handle, A::SparseMatrixCSC{Float64, Int64}, Rs, check::Bool)
         h.ptr, nonzeros(A), rs, Int32(check))
     st = _check(h, rc)
     st > 0 && throw(Main.LinearAlgebra.SingularException(st))
+    h.f32 = false
+    return h
+end
+
+# Float32 matrices (the reference's generic Tv = Float32): Float32 values,
+# Rs, factors, right-hand sides and solutions.
+function factor!(h::Handle, A::SparseMatrixCSC{Float32, Int64}, Rs, check::Bool)
+    rs = Rs === nothing ? C_NULL : pointer(Rs)
+    rc = GC.@preserve Rs ccall((:mfgpu_factor_f32, libmfgpu), Cint, (Ptr{Cvoid}, Ptr{Float32}, Ptr{Float32}, Int32),
+        h.ptr, nonzeros(A), rs, Int32(check))
+    st = _check(h, rc)
+    st > 0 && throw(Main.LinearAlgebra.SingularException(st))
+    h.f32 = true
     return h
 end
 
 # GPLUFactorization fields (src/gplu.jl:45-51) copied back from the GPU.
 function factors(h::Handle)
+    h.f32 && return factors_f32(h)
     sz = Vector{Int64}(undef, 3)
     _check(h, ccall((:mfgpu_factor_sizes, libmfgpu), Cint, (Ptr{Cvoid}, Ptr{Int64}), h.ptr, sz))
     n, nl, nu = sz
@@ -82,6 +97,27 @@ function factors(h::Handle)
         (Ptr{Cvoid}, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}, Ptr{Int64},
          Ptr{Int64}, Ptr{Int64}), h.ptr, Lp, Li, Lx, Up, Ui, Ux, p, q, pinv))
     return SparseMatrixCSC(n, n, Lp, Li, Lx), SparseMatrixCSC(n, n, Up, Ui, Ux), p, q, pinv
+end
+
+function factors_f32(h::Handle)
+    sz = Vector{Int64}(undef, 3)
+    _check(h, ccall((:mfgpu_factor_sizes, libmfgpu), Cint, (Ptr{Cvoid}, Ptr{Int64}), h.ptr, sz))
+    n, nl, nu = sz
+    Lp = Vector{Int64}(undef, n + 1); Li = Vector{Int64}(undef, nl); Lx = Vector{Float32}(undef, nl)
+    Up = Vector{Int64}(undef, n + 1); Ui = Vector{Int64}(undef, nu); Ux = Vector{Float32}(undef, nu)
+    p = Vector{Int64}(undef, n); q = Vector{Int64}(undef, n); pinv = Vector{Int64}(undef, n)
+    _check(h, ccall((:mfgpu_get_factors_f32, libmfgpu), Cint,
+        (Ptr{Cvoid}, Ptr{Int64}, Ptr{Int64}, Ptr{Float32}, Ptr{Int64}, Ptr{Int64}, Ptr{Float32}, Ptr{Int64},
+         Ptr{Int64}, Ptr{Int64}), h.ptr, Lp, Li, Lx, Up, Ui, Ux, p, q, pinv))
+    return SparseMatrixCSC(n, n, Lp, Li, Lx), SparseMatrixCSC(n, n, Up, Ui, Ux), p, q, pinv
+end
+
+function solve(h::Handle, B::AbstractVecOrMat{Float32}; refine::Integer = 0)
+    Bc = Matrix{Float32}(reshape(B, size(B, 1), :))
+    X = similar(Bc)
+    _check(h, ccall((:mfgpu_solve_f32, libmfgpu), Cint, (Ptr{Cvoid}, Int64, Ptr{Float32}, Ptr{Float32}, Int32),
+        h.ptr, size(Bc, 2), Bc, X, Int32(refine)))
+    return B isa AbstractVector ? vec(X) : X
 end
 
 # solve(F, b; refine) for a vector or an n x k matrix of right-hand sides.
