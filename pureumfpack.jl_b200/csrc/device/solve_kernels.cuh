@@ -33,15 +33,31 @@ struct SolveArgs {
   int64_t ldb;
   const double* rs;     // row scaling or nullptr
   int64_t ldx;          // leading dimension of x (factor order), = n
+  const void* bfo;      // c = Rs[p] .* b[p] in factor order and the front type (n x nrhs, ld ldx)
 };
 
-// Pivot-row value of block position a: the scaled rhs at V-row prow[c1+a].
-__device__ __forceinline__ double rhs_value(const DevPlan& P, const DevState& S, const SolveArgs& A, int c1, int a,
-                                            int64_t col) {
-  const int g = S.prow[c1 + a];
-  const int orow = P.qf[g];
-  const double v = A.b[orow + col * A.ldb];
-  return A.rs ? A.rs[orow] * v : v;
+// c = Rs[p] .* b[p] (interface.jl:127-130) in factor order, once per solve:
+// bfo[k, col] = Rs[orow] * b[orow, col] with orow = qf[prow[k]].  Columns
+// advance slowest over the grid, so the gathered column of b stays in L2
+// while its rows are read in factor order; the fronts then read their pivot
+// rows of c contiguously.  Each factor row is read by its own supernode only,
+// before that supernode writes the same rows of x, so c lives in x's storage.
+template <typename T>
+__global__ void k_rhs_factor_order(int64_t n, int64_t nrhs, const double* __restrict__ b, int64_t ldb,
+                                   const double* __restrict__ rs, const int32_t* __restrict__ qf,
+                                   const int32_t* __restrict__ prow, T* __restrict__ bfo, int64_t ldo) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n * nrhs) return;
+  const int64_t k = e % n, c = e / n;
+  const int orow = qf[prow[k]];
+  const double v = b[orow + c * ldb];
+  bfo[k + c * ldo] = (T)(rs ? rs[orow] * v : v);
+}
+
+// Pivot-row value of block position a: the scaled rhs of factor row c1 + a.
+template <typename T>
+__device__ __forceinline__ T rhs_value(const SolveArgs& A, int c1, int a, int64_t col) {
+  return static_cast<const T*>(A.bfo)[c1 + a + col * A.ldx];
 }
 
 // Block position of V-row position r (0..nf) of a child contribution: pivot
@@ -71,7 +87,7 @@ __device__ __forceinline__ void fwd_small_item(const DevPlan& P, const DevState&
   const int64_t R = A.nrhs;
   for (int e = tid; e < nf * rc; e += blockDim.x) {
     const int r = e % nf, c = e / nf;
-    f[e] = r < np ? (T)rhs_value(P, S, A, c1, r, c0 + c) : T(0);
+    f[e] = r < np ? rhs_value<T>(A, c1, r, c0 + c) : T(0);
   }
   __syncthreads();
   for (int ci = P.child_ptr[s + 1] - 1; ci >= P.child_ptr[s]; --ci) {
@@ -122,7 +138,7 @@ __device__ __forceinline__ void fwd_assemble_item(const DevPlan& P, const DevSta
   const int lane = lane_id();
   const int64_t R = A.nrhs;
   T* f = fsol + P.colbase[s] * R + col * nf;
-  for (int r = lane; r < nf; r += 32) f[r] = r < np ? (T)rhs_value(P, S, A, c1, r, col) : T(0);
+  for (int r = lane; r < nf; r += 32) f[r] = r < np ? rhs_value<T>(A, c1, r, col) : T(0);
   __syncwarp();
   for (int ci = P.child_ptr[s + 1] - 1; ci >= P.child_ptr[s]; --ci) {
     const int k = P.child_idx[ci];

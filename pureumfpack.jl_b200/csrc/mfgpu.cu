@@ -1058,7 +1058,11 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
   T* fsol = h->b_fsol.as<T>();
   T* xw = fsol + P.fc_total * R;
   DevState DS = dev_state(h);
-  SolveArgs A{R, d_b, ldb, (use_rs && h->have_rs) ? h->b_rs.as<double>() : nullptr, P.n};
+  SolveArgs A{R, d_b, ldb, (use_rs && h->have_rs) ? h->b_rs.as<double>() : nullptr, P.n, xw};
+  klaunch(h, KC_FWD_ASSEMBLE, 0, (double)P.n * R * (16.0 + sizeof(T)), [&] {
+    k_rhs_factor_order<T><<<grid1(P.n * R, 256), 256, 0, st>>>(P.n, R, d_b, ldb, A.rs, h->b_qf.as<int32_t>(),
+                                                              h->b_prow.as<int32_t>(), xw, P.n);
+  });
   const unsigned ychunks = (unsigned)((R + kSolveCols - 1) / kSolveCols);
   const unsigned wchunks = (unsigned)((R + 7) / 8);
   const int32_t* ids = S.d_ids.as<int32_t>();
