@@ -126,6 +126,108 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd_small(DevPlan P, DevState
   fwd_small_item<T>(P, S, A, tasks, pool, fsol, blockIdx.x, blockIdx.y, f);
 }
 
+// Tiny supernodes (nf <= kTinyFront), the bulk of the leaf levels: one warp
+// per (supernode, 32 right-hand sides), four supernodes per CTA, no block
+// barriers.  The warp loads its block cooperatively (coalesced), then each
+// lane runs the substitution of its own right-hand side; the arithmetic and
+// its order are those of fwd_small_item / bwd_small_item.  Shared block:
+// row-major, leading dimension kTinyLd (conflict-free both ways).
+constexpr int kTinyFront = 32;
+constexpr int kTinyLd = 33;
+constexpr int kTinyWarps = 4;
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kTinyWarps) k_fwd_tiny(DevPlan P, DevState S, SolveArgs A,
+                                                              const int32_t* __restrict__ tasks, int ntasks,
+                                                              const T* __restrict__ pool, T* fsol) {
+  __shared__ T buf[kTinyWarps][kTinyFront * kTinyLd];
+  const int w = warp_id(), lane = lane_id();
+  const int ti = blockIdx.x * kTinyWarps + w;
+  if (ti >= ntasks) return;                 // warp-uniform; no block barrier below
+  T* f = buf[w];
+  const int s = tasks[ti];
+  const int c0 = blockIdx.y * 32;
+  const int rc = min(32, (int)(A.nrhs - c0));
+  const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
+  const int64_t R = A.nrhs;
+  for (int e = lane; e < nf * rc; e += 32) {
+    const int r = e % nf, c = e / nf;
+    f[r * kTinyLd + c] = r < np ? rhs_value<T>(A, c1, r, c0 + c) : T(0);
+  }
+  __syncwarp();
+  for (int ci = P.child_ptr[s + 1] - 1; ci >= P.child_ptr[s]; --ci) {
+    const int k = P.child_idx[ci];
+    const int m = P.nu[k], nfk = P.nf[k], npk = P.np[k];
+    const T* wv = fsol + P.colbase[k] * R + npk;
+    const int32_t* rl = P.rel + P.upd_off[k];
+    for (int e = lane; e < m * rc; e += 32) {
+      const int r = e % m, c = e / m;
+      f[front_pos(S, c1, np, rl[r]) * kTinyLd + c] += wv[r + (int64_t)(c0 + c) * nfk];
+    }
+    __syncwarp();
+  }
+  if (lane < rc) {
+    const T* L = pool + P.lpan_off[s];
+    for (int a = 0; a < np; ++a) {
+      const T fa = f[a * kTinyLd + lane];
+      for (int i = a + 1; i < nf; ++i) f[i * kTinyLd + lane] -= L[i + (int64_t)a * nf] * fa;
+    }
+  }
+  __syncwarp();
+  T* out = fsol + P.colbase[s] * R;
+  for (int e = lane; e < nf * rc; e += 32) {
+    const int r = e % nf, c = e / nf;
+    out[r + (int64_t)(c0 + c) * nf] = f[r * kTinyLd + c];
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kTinyWarps) k_bwd_tiny(DevPlan P, SolveArgs A,
+                                                              const int32_t* __restrict__ tasks, int ntasks,
+                                                              const T* __restrict__ pool, const T* fsol, T* xw) {
+  __shared__ T buf[kTinyWarps][kTinyFront * kTinyLd];   // rows 0..np-1: y; np..nf-1: x of the update rows
+  const int w = warp_id(), lane = lane_id();
+  const int ti = blockIdx.x * kTinyWarps + w;
+  if (ti >= ntasks) return;
+  T* f = buf[w];
+  const int s = tasks[ti];
+  const int c0 = blockIdx.y * 32;
+  const int rc = min(32, (int)(A.nrhs - c0));
+  const int np = P.np[s], nu = P.nu[s], nf = P.nf[s], c1 = P.c1[s];
+  const int64_t R = A.nrhs;
+  const T* fs = fsol + P.colbase[s] * R;
+  const int32_t* us = P.upd + P.upd_off[s];
+  for (int e = lane; e < np * rc; e += 32) {
+    const int r = e % np, c = e / np;
+    f[r * kTinyLd + c] = fs[r + (int64_t)(c0 + c) * nf];
+  }
+  for (int e = lane; e < nu * rc; e += 32) {
+    const int t = e % nu, c = e / nu;
+    f[(np + t) * kTinyLd + c] = xw[us[t] + (int64_t)(c0 + c) * A.ldx];
+  }
+  __syncwarp();
+  if (lane < rc) {
+    const T* U = pool + P.lpan_off[s];
+    const T* U12 = pool + P.u12_off[s];
+    const int ldu = u12_ld(P, s);
+    for (int a = 0; a < np; ++a) {
+      T acc = f[a * kTinyLd + lane];
+      for (int t = 0; t < nu; ++t) acc -= U12[a + (int64_t)t * ldu] * f[(np + t) * kTinyLd + lane];
+      f[a * kTinyLd + lane] = acc;
+    }
+    for (int a = np - 1; a >= 0; --a) {
+      f[a * kTinyLd + lane] /= U[a + (int64_t)a * nf];
+      const T ya = f[a * kTinyLd + lane];
+      for (int i = 0; i < a; ++i) f[i * kTinyLd + lane] -= U[i + (int64_t)a * nf] * ya;
+    }
+  }
+  __syncwarp();
+  for (int e = lane; e < np * rc; e += 32) {
+    const int r = e % np, c = e / np;
+    xw[c1 + r + (int64_t)(c0 + c) * A.ldx] = f[r * kTinyLd + c];
+  }
+}
+
 // Large supernodes: gather the rhs block, one warp per right-hand side;
 // item (bx, by) covers columns by * warps .. of supernode tasks[bx].
 template <typename T>

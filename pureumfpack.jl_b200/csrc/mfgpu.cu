@@ -105,7 +105,7 @@ struct SolveSchedule {
   int64_t nrhs = -1;
   struct Step {
     int kind;        // 0 fwd_small, 1 fwd_assemble, 3 gemm (A: pool; B, C, D: solve arena), 4 bwd_small,
-                     // 5 bwd_gather
+                     // 5 bwd_gather, 6 fwd_tiny, 7 bwd_tiny (nf <= kTinyFront, one warp per supernode)
     int64_t first, count, tiles;
     double flops = 0, elems = 0;
     int64_t tiles_tc = 0;   // GEMM steps: grid in 128 x 128 tensor-core tiles (gemms_tc)
@@ -439,8 +439,8 @@ void prof_flush(mfgpu_ctx* h);
 
 // Kernel class of a solve step / persistent phase kind.
 int phase_class(int kind) {
-  static const int kc[6] = {KC_FWD_SMALL, KC_FWD_ASSEMBLE, KC_FWD_SMALL, KC_GEMM_SOLVE, KC_BWD_SMALL,
-                            KC_BWD_GATHER};
+  static const int kc[8] = {KC_FWD_SMALL, KC_FWD_ASSEMBLE, KC_FWD_SMALL, KC_GEMM_SOLVE, KC_BWD_SMALL,
+                            KC_BWD_GATHER, KC_FWD_SMALL, KC_BWD_SMALL};
   return kc[kind];
 }
 
@@ -897,17 +897,25 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
     st.flops += (a * a + 2.0 * a * u) * R;
     st.elems += (a * a / 2 + a * u) + 2.0 * (a + u) * R;
   };
+  // the small supernodes of slots [a, m): the tiny ones (one warp each) and
+  // the rest (one CTA each), as two independent steps
+  auto small_steps = [&](int32_t a, int32_t m, int tiny_kind, int small_kind) {
+    for (int pass = 0; pass < 2; ++pass) {
+      SolveSchedule::Step st{pass == 0 ? tiny_kind : small_kind, (int64_t)S.ids.size(), 0, 0};
+      for (int32_t i = a; i < m; ++i) {
+        const int32_t s = P.slot_super[i];
+        if ((P.nf[s] <= kTinyFront) != (pass == 0)) continue;
+        S.ids.push_back(s);
+        small_work(st, s);
+        ++st.count;
+      }
+      if (st.count) S.steps.push_back(st);
+    }
+  };
   // forward, leaves to root
   for (int32_t L = 0; L < P.nlevels; ++L) {
     const int32_t a = P.level_slot[L], m = P.level_large[L], e = P.level_slot[L + 1];
-    if (m > a) {
-      SolveSchedule::Step st{0, (int64_t)S.ids.size(), m - a, 0};
-      for (int32_t i = a; i < m; ++i) {
-        S.ids.push_back(P.slot_super[i]);
-        small_work(st, P.slot_super[i]);
-      }
-      S.steps.push_back(st);
-    }
+    if (m > a) small_steps(a, m, 6, 0);
     if (e > m) {
       const int64_t first = (int64_t)S.ids.size();
       for (int32_t i = m; i < e; ++i) S.ids.push_back(P.slot_super[i]);
@@ -955,14 +963,7 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
       }
       push(gx);
     }
-    if (m > a) {
-      SolveSchedule::Step st{4, (int64_t)S.ids.size(), m - a, 0};
-      for (int32_t i = a; i < m; ++i) {
-        S.ids.push_back(P.slot_super[i]);
-        small_work(st, P.slot_super[i]);
-      }
-      S.steps.push_back(st);
-    }
+    if (m > a) small_steps(a, m, 7, 4);
   }
   // split-K form of the GEMM steps for few right-hand sides
   constexpr int32_t kSkinnyMinK = 512;
@@ -1006,13 +1007,15 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
   // kSolveThreads / 32 right-hand sides per gather item)
   const int64_t ych = ceil_div(R, kSolveCols), wch = ceil_div(R, kSolveThreads / 32);
   for (const auto& st : S.steps) {
-    SolvePhase ph{st.kind, 1, st.first, st.count, 0};
-    switch (st.kind) {
+    // tiny steps run as the small-supernode phases (the item handles any nf <= 64)
+    const int pk = st.kind == 6 ? kPhFwdSmall : (st.kind == 7 ? kPhBwdSmall : st.kind);
+    SolvePhase ph{pk, 1, st.first, st.count, 0};
+    switch (pk) {
       case kPhFwdSmall: case kPhBwdSmall: ph.rows = (int32_t)ych; break;
       case kPhFwdAssemble: case kPhBwdGather: ph.rows = (int32_t)wch; break;
       default: break;
     }
-    ph.items = st.kind == kPhGemm ? st.tiles : st.count * ph.rows;
+    ph.items = pk == kPhGemm ? st.tiles : st.count * ph.rows;
     S.phases.push_back(ph);
   }
   upload(S.d_ids, S.ids, h->stream);
@@ -1135,6 +1138,18 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
           }, -1, s.tiles);
         h->cur_tune = -1;
         ++tune_id;
+        break;
+      case 6:
+        klaunch(h, KC_FWD_SMALL, s.flops, bytes, [&] {
+          k_fwd_tiny<T><<<dim3((unsigned)((s.count + kTinyWarps - 1) / kTinyWarps), (unsigned)((R + 31) / 32)),
+                          32 * kTinyWarps, 0, st>>>(h->dp, DS, A, ids + s.first, (int)s.count, pool, fsol);
+        });
+        break;
+      case 7:
+        klaunch(h, KC_BWD_SMALL, s.flops, bytes, [&] {
+          k_bwd_tiny<T><<<dim3((unsigned)((s.count + kTinyWarps - 1) / kTinyWarps), (unsigned)((R + 31) / 32)),
+                          32 * kTinyWarps, 0, st>>>(h->dp, A, ids + s.first, (int)s.count, pool, fsol, xw);
+        });
         break;
       case 4:
         klaunch(h, KC_BWD_SMALL, s.flops, bytes, [&] {
