@@ -110,6 +110,7 @@ struct SolveSchedule {
     double flops = 0, elems = 0;
     int64_t tiles_tc = 0;   // GEMM steps: grid in 128 x 128 tensor-core tiles (gemms_tc)
     int64_t sk_first = 0, sk_count = 0, sk_parts = 0, sk_reds = 0;   // split-K form (few rhs)
+    int32_t level = -1;     // tree level (small-supernode steps run beside the level's large ones)
   };
   std::vector<Step> steps;
   std::vector<int32_t> ids;
@@ -174,6 +175,8 @@ struct mfgpu_ctx {
   int device = 0;
   int precision = MFGPU_PRECISION_FP64;
   cudaStream_t own_stream = nullptr;
+  cudaStream_t side_stream = nullptr;     // a level's small supernodes, beside its large ones
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaStream_t stream = nullptr;
   std::string err;
   bool analyzed = false, factored = false, csc_ready = false;
@@ -571,6 +574,41 @@ int64_t tune_factor_count(const Plan& P) {
   return c;
 }
 
+// The small and the large supernodes of one tree level touch disjoint
+// fronts and read only lower levels (factor, forward solve) or higher ones
+// (backward solve), so a level's small-supernode launch runs on a second
+// stream beside the level's large-supernode launches; the two streams join
+// at every level change (and in a CUDA graph this is a fork / join of
+// branches).  Off when profiling, whose per-launch events sit on one stream.
+struct LevelFork {
+  mfgpu_ctx* h;
+  bool on;
+  int level = -1;
+  bool open = false;
+  LevelFork(mfgpu_ctx* hh) : h(hh), on(!hh->profiling && hh->side_stream) {}
+  void at(int L) {
+    if (L != level) {
+      join();
+      level = L;
+    }
+  }
+  cudaStream_t side() {   // the stream for this level's small supernodes
+    if (!on) return h->stream;
+    if (!open) {
+      CK(cudaEventRecord(h->ev_fork, h->stream));
+      CK(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
+      open = true;
+    }
+    return h->side_stream;
+  }
+  void join() {
+    if (!open) return;
+    CK(cudaEventRecord(h->ev_join, h->side_stream));
+    CK(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+    open = false;
+  }
+};
+
 template <typename T>
 void run_factor_launches(mfgpu_ctx* h) {
   const Plan& P = h->plan;
@@ -579,15 +617,19 @@ void run_factor_launches(mfgpu_ctx* h) {
   const double* vx = h->b_vx.as<double>();
   DevState S = dev_state(h);
   int64_t tune_id = 0;
+  LevelFork fork(h);
   for (const Launch& L : P.launches) {
     const double bytes = L.elems * sizeof(T) + L.extra_bytes;
+    fork.at(L.level);
     switch (L.kind) {
-      case kLaunchSmall:
+      case kLaunchSmall: {
+        cudaStream_t ss = fork.side();
         klaunch(h, KC_SMALL, L.flops, bytes, [&] {
-          k_small_fronts<T><<<(unsigned)L.count, kSmallThreads, kSmallFront * kSmallFront * sizeof(T), st>>>(
+          k_small_fronts<T><<<(unsigned)L.count, kSmallThreads, kSmallFront * kSmallFront * sizeof(T), ss>>>(
               h->dp, S, h->b_small.as<int32_t>() + L.first, pool, vx);
         }, L.level, L.count);
         break;
+      }
       case kLaunchAssemble:
         klaunch(h, KC_ASSEMBLE, 0, bytes, [&] {
           k_assemble_columns<T><<<grid1(L.count, 8), 256, 0, st>>>(h->dp, L.first, L.count, pool, vx);
@@ -614,6 +656,7 @@ void run_factor_launches(mfgpu_ctx* h) {
         }, L.level, L.tiles);
         break;
       case kLaunchCopyPanels:
+        fork.join();   // the level's panels, small fronts' included
         klaunch(h, KC_COPY_PANELS, 0, bytes, [&] {
           k_copy_panels<T><<<grid1(L.count, 8), 256, 0, st>>>(h->dp, L.first, L.count, pool);
         }, L.level, L.count);
@@ -634,6 +677,7 @@ void run_factor_launches(mfgpu_ctx* h) {
         break;
     }
   }
+  fork.join();
   CK(cudaGetLastError());
 }
 
@@ -887,7 +931,12 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
     st.flops += 2.0 * m * nn * k;
     st.elems += (double)m * nn * (mode == kGemmSet ? 1 : 2) + (double)m * k + (double)k * nn;
   };
-  auto gemm_step = [&]() { return SolveSchedule::Step{3, (int64_t)S.gemms.size(), 0, 0}; };
+  int32_t cur_level = -1;   // level of the steps being built
+  auto gemm_step = [&]() {
+    SolveSchedule::Step st{3, (int64_t)S.gemms.size(), 0, 0};
+    st.level = cur_level;
+    return st;
+  };
   auto push = [&](const SolveSchedule::Step& st) {
     if (st.count) S.steps.push_back(st);
   };
@@ -899,9 +948,10 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
   };
   // the small supernodes of slots [a, m): the tiny ones (one warp each) and
   // the rest (one CTA each), as two independent steps
-  auto small_steps = [&](int32_t a, int32_t m, int tiny_kind, int small_kind) {
+  auto small_steps = [&](int32_t a, int32_t m, int tiny_kind, int small_kind, int32_t level) {
     for (int pass = 0; pass < 2; ++pass) {
       SolveSchedule::Step st{pass == 0 ? tiny_kind : small_kind, (int64_t)S.ids.size(), 0, 0};
+      st.level = level;
       for (int32_t i = a; i < m; ++i) {
         const int32_t s = P.slot_super[i];
         if ((P.nf[s] <= kTinyFront) != (pass == 0)) continue;
@@ -915,11 +965,13 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
   // forward, leaves to root
   for (int32_t L = 0; L < P.nlevels; ++L) {
     const int32_t a = P.level_slot[L], m = P.level_large[L], e = P.level_slot[L + 1];
-    if (m > a) small_steps(a, m, 6, 0);
+    cur_level = L;
+    if (m > a) small_steps(a, m, 6, 0, L);
     if (e > m) {
       const int64_t first = (int64_t)S.ids.size();
       for (int32_t i = m; i < e; ++i) S.ids.push_back(P.slot_super[i]);
       S.steps.push_back({1, first, e - m, 0});
+      S.steps.back().level = L;
       // y = inv(L11) f[0:np], into x's rows c1.. ; then w = f[np:] - L21 y
       SolveSchedule::Step gy = gemm_step();
       for (int32_t i = m; i < e; ++i) {
@@ -941,10 +993,15 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
   // backward, root to leaves
   for (int32_t L = P.nlevels - 1; L >= 0; --L) {
     const int32_t a = P.level_slot[L], m = P.level_large[L], e = P.level_slot[L + 1];
+    cur_level = L;
+    // the level's small supernodes read x of higher levels only: independent
+    // of the level's large ones
+    if (m > a) small_steps(a, m, 7, 4, L);
     if (e > m) {
       const int64_t first = (int64_t)S.ids.size();
       for (int32_t i = m; i < e; ++i) S.ids.push_back(P.slot_super[i]);
       S.steps.push_back({5, first, e - m, 0});
+      S.steps.back().level = L;
       // g = y - U12 x[upd] into f[0:np]; then x = inv(U11) g into x's rows c1..
       SolveSchedule::Step gg = gemm_step();
       for (int32_t i = m; i < e; ++i) {
@@ -963,7 +1020,7 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
       }
       push(gx);
     }
-    if (m > a) small_steps(a, m, 7, 4);
+
   }
   // split-K form of the GEMM steps for few right-hand sides
   constexpr int32_t kSkinnyMinK = 512;
@@ -1093,13 +1150,17 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     CK(cudaLaunchKernelEx(&cfg, k_solve_persistent<T>, h->dp, DS, A, X, (const T*)pool, fsol, xw));
-  } else
+  } else {
+  LevelFork fork(h);
   for (const auto& s : S.steps) {
     const double bytes = s.elems * sizeof(T);
+    fork.at(s.level);
+    const bool side = s.kind == 0 || s.kind == 4 || s.kind == 6 || s.kind == 7;
+    const cudaStream_t ss = side ? fork.side() : st;
     switch (s.kind) {
       case 0:
         klaunch(h, KC_FWD_SMALL, s.flops, bytes, [&] {
-          k_fwd_small<T><<<dim3((unsigned)s.count, ychunks), kSolveThreads, 0, st>>>(h->dp, DS, A, ids + s.first,
+          k_fwd_small<T><<<dim3((unsigned)s.count, ychunks), kSolveThreads, 0, ss>>>(h->dp, DS, A, ids + s.first,
                                                                                      pool, fsol);
         });
         break;
@@ -1142,18 +1203,18 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
       case 6:
         klaunch(h, KC_FWD_SMALL, s.flops, bytes, [&] {
           k_fwd_tiny<T><<<dim3((unsigned)((s.count + kTinyWarps - 1) / kTinyWarps), (unsigned)((R + 31) / 32)),
-                          32 * kTinyWarps, 0, st>>>(h->dp, DS, A, ids + s.first, (int)s.count, pool, fsol);
+                          32 * kTinyWarps, 0, ss>>>(h->dp, DS, A, ids + s.first, (int)s.count, pool, fsol);
         });
         break;
       case 7:
         klaunch(h, KC_BWD_SMALL, s.flops, bytes, [&] {
           k_bwd_tiny<T><<<dim3((unsigned)((s.count + kTinyWarps - 1) / kTinyWarps), (unsigned)((R + 31) / 32)),
-                          32 * kTinyWarps, 0, st>>>(h->dp, A, ids + s.first, (int)s.count, pool, fsol, xw);
+                          32 * kTinyWarps, 0, ss>>>(h->dp, A, ids + s.first, (int)s.count, pool, fsol, xw);
         });
         break;
       case 4:
         klaunch(h, KC_BWD_SMALL, s.flops, bytes, [&] {
-          k_bwd_small<T><<<dim3((unsigned)s.count, ychunks), kSolveThreads, 0, st>>>(h->dp, A, ids + s.first, pool,
+          k_bwd_small<T><<<dim3((unsigned)s.count, ychunks), kSolveThreads, 0, ss>>>(h->dp, A, ids + s.first, pool,
                                                                                      fsol, xw);
         });
         break;
@@ -1163,6 +1224,8 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
         });
         break;
     }
+  }
+  fork.join();
   }
   klaunch(h, KC_SOLVE_FINISH, 0, (double)P.n * R * (sizeof(T) + 8.0 * (1 + accumulate)), [&] {
     k_solve_finish<T><<<grid1(P.n * R, 256), 256, 0, st>>>(P.n, R, h->b_qf.as<int32_t>(), xw, P.n, d_x, ldx,
@@ -1308,6 +1371,9 @@ int mfgpu_create(const mfgpu_options* opts, mfgpu_ctx** out) {
     if (prop.major != 10) return fail(h, MFGPU_ERR_NO_DEVICE, "libmfgpu is built for sm_100a (B200)");
     h->num_sms = prop.multiProcessorCount;
     CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
     h->stream = h->own_stream;
     CK(cudaEventCreate(&h->ev0));
     CK(cudaEventCreate(&h->ev1));
@@ -1345,6 +1411,9 @@ void mfgpu_destroy(mfgpu_ctx* h) {
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  if (h->side_stream) cudaStreamDestroy(h->side_stream);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
   delete h;
 }
 
