@@ -329,13 +329,14 @@ def roofline_of(P, primary, torch, dev, peaks):
             peak_src = "in-run cuBLAS DGEMM 8192^3 (FP64 peak is not in MEASURED_PEAKS.json)"
         elif "bf16_tflops_sustained" in peaks:
             # FP32 fronts: the large updates run as BF16x3 tcgen05 products
-            # (three BF16 tensor-core products per useful FP32 product)
-            peak = peaks["bf16_tflops_sustained"] / 3.0
-            peak_src = ("MEASURED_PEAKS.json bf16_tflops_sustained / 3 (of measured): BF16x3 needs three BF16 "
-                        "tensor-core products per useful product")
+            # (each operand split into three bf16 parts; six bf16 products
+            # per useful FP32 product)
+            peak = peaks["bf16_tflops_sustained"] / 6.0
+            peak_src = ("MEASURED_PEAKS.json bf16_tflops_sustained / 6 (of measured): BF16x3 issues six BF16 "
+                        "tensor-core products per useful FP32 product")
         else:
-            peak = 1400.0 / 3.0
-            peak_src = "fallback sustained bf16 1.4 PFLOP/s / 3 (BF16x3)"
+            peak = 1400.0 / 6.0
+            peak_src = "fallback sustained bf16 1.4 PFLOP/s / 6 (BF16x3: six bf16 products per useful product)"
         achieved = kd["flops"] / (kd["ms"] * 1e-3) / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak,
                 "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": peak_src}
