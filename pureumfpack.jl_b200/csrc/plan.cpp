@@ -132,8 +132,11 @@ void build_inverse_steps(Plan& P) {
 }  // namespace
 
 namespace {
+// csc: lay out the factor's CSC for this partition (merged plans lay it out
+// for the original supernodes instead, in attach_original).
 void build_plan_core(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf, const int64_t* parent,
-                int64_t ns, const int64_t* sstart, const int64_t* upd_ptr, const int64_t* upd_idx, Plan& P) {
+                int64_t ns, const int64_t* sstart, const int64_t* upd_ptr, const int64_t* upd_idx, Plan& P,
+                bool csc) {
   P = Plan();
   P.n = n;
   P.ns = ns;
@@ -335,6 +338,7 @@ void build_plan_core(int64_t n, const int64_t* colptr, const int64_t* rowval, co
   }
 
   // ---- factor CSC layout -------------------------------------------------
+  if (csc) {
   P.lcolptr.assign(n + 1, 0);
   P.ucolptr.assign(n + 1, 0);
   for (int64_t s = 0; s < ns; ++s) {
@@ -359,6 +363,7 @@ void build_plan_core(int64_t n, const int64_t* colptr, const int64_t* rowval, co
         P.uoff[p] = cur[P.upd[p]];
         cur[P.upd[p]] += P.np[s];
       }
+  }
   }
 
   // ---- A in CSR (residual r = b - A x) ------------------------------------
@@ -413,7 +418,7 @@ void build_plan_core(int64_t n, const int64_t* colptr, const int64_t* rowval, co
 
 void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf, const int64_t* parent,
                 int64_t ns, const int64_t* sstart, const int64_t* upd_ptr, const int64_t* upd_idx, Plan& P) {
-  build_plan_core(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, P);
+  build_plan_core(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, P, true);
   set_layout(P, false);
 }
 
@@ -520,7 +525,8 @@ void build_plan_merged(int64_t n, const int64_t* colptr, const int64_t* rowval, 
     first = s + 1;
   }
   ms.push_back(n);
-  build_plan_core(n, colptr, rowval, qf, parent, (int64_t)ms.size() - 1, ms.data(), mup.data(), mui.data(), P);
+  build_plan_core(n, colptr, rowval, qf, parent, (int64_t)ms.size() - 1, ms.data(), mup.data(), mui.data(), P,
+                  false);
   attach_original(P, ns, sstart, upd_ptr, upd_idx);
   set_layout(P, false);
 }
