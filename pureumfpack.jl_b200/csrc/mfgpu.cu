@@ -1305,16 +1305,24 @@ int analyze_common(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const int64_t
                    const int64_t* parent, int64_t ns, const int64_t* sstart, const int64_t* upd_ptr,
                    const int64_t* upd_idx) {
   auto t0 = std::chrono::steady_clock::now();
+  // until this analysis has completed, the handle holds no usable plan: a
+  // failure below (an inconsistent symbolic analysis, an allocation) leaves
+  // it unanalyzed rather than with a host plan that its device maps do not
+  // match; a batch analysis sets its own state after this returns
+  h->analyzed = h->factored = h->csc_ready = false;
+  h->batch.nsys = 0;
+  Plan plan;
   if (h->merge_fronts)
-    build_plan_merged(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, h->plan, kMergeMaxPivots);
+    build_plan_merged(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, plan, kMergeMaxPivots);
   else
-    build_plan(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, h->plan);
+    build_plan(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, plan);
   // all fronts resident when they fit comfortably (FP64 worst case), else
   // working fronts placed by lifetime and a compact panel pool
   size_t free_b = 0, total_b = 0;
   CK(cudaMemGetInfo(&free_b, &total_b));
-  if (h->lean_mode == 1 || (h->lean_mode == 0 && (double)h->plan.front_elems_full * 8.0 > 0.45 * (double)total_b))
-    set_layout(h->plan, true);
+  if (h->lean_mode == 1 || (h->lean_mode == 0 && (double)plan.front_elems_full * 8.0 > 0.45 * (double)total_b))
+    set_layout(plan, true);
+  h->plan = std::move(plan);
   upload_plan(h);
   upload_launches(h);
   h->launches_safe = false;
@@ -1443,8 +1451,8 @@ int mfgpu_analyze(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const int64_t*
   if (!h) return MFGPU_ERR_ARGUMENT;
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->device));
-    if (!valid_csc(n, colptr, rowval) || !qf || !parent || !sstart || !upd_ptr || nsuper < 0 ||
-        (upd_ptr[nsuper] > 1 && !upd_idx))
+    if (!valid_csc(n, colptr, rowval) || !qf || !parent || !sstart || !upd_ptr || nsuper < 0 || upd_ptr[0] != 1 ||
+        upd_ptr[nsuper] < 1 || (upd_ptr[nsuper] > 1 && !upd_idx))
       return fail(h, MFGPU_ERR_ARGUMENT, "invalid analyze arguments");
     std::vector<int64_t> cp(n + 1), ri(colptr[n] - 1), q(n), par(n), ss(nsuper + 1), up(nsuper + 1),
         ui(upd_ptr[nsuper] - 1);

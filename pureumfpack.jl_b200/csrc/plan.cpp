@@ -416,8 +416,39 @@ void build_plan_core(int64_t n, const int64_t* colptr, const int64_t* rowval, co
 }
 }  // namespace
 
+void check_symbolic(int64_t n, const int64_t* qf, const int64_t* parent, int64_t ns, const int64_t* sstart,
+                    const int64_t* upd_ptr, const int64_t* upd_idx) {
+  auto bad = [](const char* what) { throw std::invalid_argument(what); };
+  if (n < 0 || ns < 0 || (n > 0) != (ns > 0)) bad("supernode count does not match n");
+  if (n >= (int64_t(1) << 31)) bad("n exceeds the 32-bit index maps");
+  if (!sstart || !upd_ptr || (n > 0 && (!qf || !parent))) bad("null symbolic array");
+  if (sstart[0] != 0 || sstart[ns] != n) bad("supernode partition does not cover 1:n");
+  for (int64_t s = 0; s < ns; ++s)
+    if (sstart[s + 1] <= sstart[s]) bad("empty supernode");
+  if (upd_ptr[0] != 0) bad("update pointers do not start at 1");
+  for (int64_t s = 0; s < ns; ++s)
+    if (upd_ptr[s + 1] < upd_ptr[s]) bad("update pointers decrease");
+  if (upd_ptr[ns] >= (int64_t(1) << 31)) bad("update sets exceed the 32-bit index maps");
+  if (upd_ptr[ns] > 0 && !upd_idx) bad("null symbolic array");
+  for (int64_t s = 0; s < ns; ++s) {
+    const int64_t c2 = sstart[s + 1] - 1;
+    for (int64_t p = upd_ptr[s]; p < upd_ptr[s + 1]; ++p)
+      if (upd_idx[p] <= c2 || upd_idx[p] >= n || (p > upd_ptr[s] && upd_idx[p] <= upd_idx[p - 1]))
+        bad("update set must be sorted rows below the supernode");
+  }
+  // an elimination tree of the permuted matrix: every parent comes later
+  for (int64_t j = 0; j < n; ++j)
+    if (parent[j] < -1 || parent[j] >= n || (parent[j] >= 0 && parent[j] <= j)) bad("parent is not an elimination tree");
+  std::vector<char> seen(n, 0);
+  for (int64_t k = 0; k < n; ++k) {
+    if (qf[k] < 0 || qf[k] >= n || seen[qf[k]]) bad("qf is not a permutation");
+    seen[qf[k]] = 1;
+  }
+}
+
 void build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf, const int64_t* parent,
                 int64_t ns, const int64_t* sstart, const int64_t* upd_ptr, const int64_t* upd_idx, Plan& P) {
+  check_symbolic(n, qf, parent, ns, sstart, upd_ptr, upd_idx);
   build_plan_core(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, P, true);
   set_layout(P, false);
 }
@@ -508,9 +539,11 @@ void attach_original(Plan& P, int64_t ns, const int64_t* sstart, const int64_t* 
 void build_plan_merged(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf,
                        const int64_t* parent, int64_t ns, const int64_t* sstart, const int64_t* upd_ptr,
                        const int64_t* upd_idx, Plan& P, int64_t max_pivots) {
+  check_symbolic(n, qf, parent, ns, sstart, upd_ptr, upd_idx);
   const std::vector<char> marks = amalgamation_marks(n, parent, ns, sstart, upd_ptr, max_pivots);
   if (std::find(marks.begin(), marks.end(), 1) == marks.end()) {
-    build_plan(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, P);
+    build_plan_core(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, P, true);
+    set_layout(P, false);
     return;
   }
   // merged partition: a group ends at a supernode that is not merged, and

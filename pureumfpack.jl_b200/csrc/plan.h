@@ -200,6 +200,16 @@ struct Plan {
   int32_t max_nf = 0, max_np = 0;
 };
 
+// Checks a caller's symbolic analysis before anything is indexed by it:
+// sstart partitions 0..n-1 into nonempty supernodes, upd_ptr is a monotone
+// pointer array from 0, every update set holds sorted rows below its
+// supernode, parent is an elimination tree (-1 or a later column) and qf a
+// permutation.  Throws std::invalid_argument.  Both plan builders call it;
+// the consistency of A's pattern with the fronts is checked while the maps
+// are built.
+void check_symbolic(int64_t n, const int64_t* qf, const int64_t* parent, int64_t ns, const int64_t* sstart,
+                    const int64_t* upd_ptr, const int64_t* upd_idx);
+
 // Build the plan.  All inputs 0-based: A pattern (n x n CSC), qf, parent
 // (-1 = root), sstart (ns+1), upd_ptr (ns+1), upd_idx.
 // `safe` replaces speculative panels by global-memory partial pivoting.

@@ -296,6 +296,9 @@ class GpuContext:
     def analyze_arrays(self, A: SparseCSC, qf, parent, sstart, upd_ptr, upd_idx):
         """mfgpu_analyze with the reference's own symbolic arrays (1-based)."""
         ns = len(sstart) - 1
+        if (len(qf) != A.n or len(parent) != A.n or ns < 0 or len(upd_ptr) != ns + 1
+                or len(upd_idx) < int(upd_ptr[-1]) - 1):
+            raise ArgumentError("symbolic arrays do not match n and the supernode count")
         self._check(self._lib.mfgpu_analyze(self._h, A.n, L.ptr(_i(A.colptr)), L.ptr(_i(A.rowval)), L.ptr(_i(qf)),
                                             L.ptr(_i(parent)), ns, L.ptr(_i(sstart)), L.ptr(_i(upd_ptr)),
                                             L.ptr(_i(upd_idx))))

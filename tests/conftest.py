@@ -5,6 +5,7 @@ rest run on the CPU (oracle against its golden vectors, host symbolic code,
 ABI exports, multi-process host logic).
 """
 
+import ctypes
 import os
 import subprocess
 import sys
@@ -42,3 +43,17 @@ def has_gpu():
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+@pytest.fixture(scope="session")
+def emu(tmp_path_factory):
+    """tests/plan_emulator.cpp with the library's plan and symbolic sources:
+    the device factorization's semantics run over the library's own Plan on
+    the CPU."""
+    here = os.path.dirname(os.path.abspath(__file__))
+    csrc = os.path.join(PKG, "csrc")
+    out = str(tmp_path_factory.mktemp("emu") / "libplanemu.so")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-I", csrc, "-o", out,
+                    os.path.join(here, "plan_emulator.cpp"), os.path.join(csrc, "plan.cpp"),
+                    os.path.join(csrc, "host", "symbolic.cpp"), "-lpthread"], check=True)
+    return ctypes.CDLL(out)

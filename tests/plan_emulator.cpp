@@ -16,6 +16,7 @@
 #include <cstdint>
 #include <algorithm>
 #include <cstring>
+#include <stdexcept>
 #include <utility>
 #include <vector>
 
@@ -359,4 +360,34 @@ extern "C" void emu_get(int64_t* lp, int64_t* li, double* lx, int64_t* up, int64
   std::memcpy(ux, R.ux.data(), R.ux.size() * 8);
   std::memcpy(p, R.p.data(), R.p.size() * 8);
   std::memcpy(q, R.q.data(), R.q.size() * 8);
+}
+
+// Build a plan from a caller's symbolic arrays (0-based), merged fronts or
+// one front per supernode, as mfgpu_analyze does before anything reaches the
+// device.  Returns 0 when the plan builds, 1 when the arrays are rejected as
+// invalid (message in msg), 2 on any other exception.
+extern "C" int emu_build_plan(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf,
+                              const int64_t* parent, int64_t ns, const int64_t* sstart, const int64_t* upd_ptr,
+                              const int64_t* upd_idx, int merge, char* msg, int64_t cap) {
+  auto say = [&](const char* what) {
+    if (cap > 0) {
+      std::strncpy(msg, what, (size_t)cap - 1);
+      msg[cap - 1] = 0;
+    }
+  };
+  try {
+    Plan P;
+    if (merge)
+      build_plan_merged(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, P, kMergeMaxPivots);
+    else
+      build_plan(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, P);
+    say("");
+    return 0;
+  } catch (const std::invalid_argument& e) {
+    say(e.what());
+    return 1;
+  } catch (const std::exception& e) {
+    say(e.what());
+    return 2;
+  }
 }

@@ -11,8 +11,6 @@ from other supernodes' rows.
 """
 
 import ctypes
-import os
-import subprocess
 
 import numpy as np
 import pytest
@@ -21,18 +19,6 @@ from helpers import column_value_errors
 from oracle import oracle as O
 from pureumfpack import colamd_order
 from pureumfpack import matrices as M
-
-HERE = os.path.dirname(os.path.abspath(__file__))
-CSRC = os.path.join(os.path.dirname(HERE), "pureumfpack.jl_b200", "csrc")
-
-
-@pytest.fixture(scope="module")
-def emu(tmp_path_factory):
-    out = str(tmp_path_factory.mktemp("emu") / "libplanemu.so")
-    subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-I", CSRC, "-o", out,
-                    os.path.join(HERE, "plan_emulator.cpp"), os.path.join(CSRC, "plan.cpp"),
-                    os.path.join(CSRC, "host", "symbolic.cpp")], check=True)
-    return ctypes.CDLL(out)
 
 
 def _ptr(a):

@@ -10,26 +10,12 @@ ordered schedule reproduces it exactly; a missing, duplicated or early task
 shows up as a difference."""
 
 import ctypes
-import os
-import subprocess
 
 import numpy as np
 import pytest
 
 from pureumfpack import colamd_order
 from pureumfpack import matrices as M
-
-HERE = os.path.dirname(os.path.abspath(__file__))
-CSRC = os.path.join(os.path.dirname(HERE), "pureumfpack.jl_b200", "csrc")
-
-
-@pytest.fixture(scope="module")
-def emu(tmp_path_factory):
-    out = str(tmp_path_factory.mktemp("emu") / "libplanemu.so")
-    subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-I", CSRC, "-o", out,
-                    os.path.join(HERE, "plan_emulator.cpp"), os.path.join(CSRC, "plan.cpp"),
-                    os.path.join(CSRC, "host", "symbolic.cpp"), "-lpthread"], check=True)
-    return ctypes.CDLL(out)
 
 
 def _ptr(a):
