@@ -786,6 +786,7 @@ template <typename T>
 int factor_impl(mfgpu_ctx* h, int32_t check) {
   Plan& P = h->plan;
   cudaStream_t st = h->stream;
+  h->factored = h->csc_ready = false;   // until this factorization completes
   configure_kernels<T>();
   h->b_pool.ensure(std::max<size_t>(P.pool_elems * sizeof(T), 16));
   h->b_ipiv.ensure(std::max<int64_t>(P.n, 1) * 4);
@@ -1489,6 +1490,8 @@ int mfgpu_analyze_symbolic(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const
 int mfgpu_factor_device(mfgpu_ctx* h, const double* d_nzval, const double* d_rs, int32_t check) {
   if (!h) return MFGPU_ERR_ARGUMENT;
   if (!h->analyzed) return fail(h, MFGPU_ERR_STATE, "factor before analyze");
+  if (h->plan.nnz_a && !d_nzval) return fail(h, MFGPU_ERR_ARGUMENT, "null values");
+  h->factored = h->csc_ready = false;
   h->f32_values = false;
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->device));
@@ -1510,6 +1513,7 @@ int mfgpu_factor_scaled(mfgpu_ctx* h, const double* nzval, int32_t scale, int32_
   h->f32_values = false;
   if (scale < MFGPU_SCALE_NONE || scale > MFGPU_SCALE_MAX) return fail(h, MFGPU_ERR_ARGUMENT, "bad scale kind");
   if (h->plan.nnz_a && !nzval) return fail(h, MFGPU_ERR_ARGUMENT, "null values");
+  h->factored = h->csc_ready = false;
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->device));
     const Plan& P = h->plan;
@@ -1546,6 +1550,9 @@ int mfgpu_get_row_scaling(mfgpu_ctx* h, double* rs) {
 static int factor_host(mfgpu_ctx* h, const double* nzval, const double* rs, int32_t check, bool f32) {
   if (!h) return MFGPU_ERR_ARGUMENT;
   if (!h->analyzed) return fail(h, MFGPU_ERR_STATE, "factor before analyze");
+  if (h->plan.nnz_a && !nzval) return fail(h, MFGPU_ERR_ARGUMENT, "null values");
+  // the previous factors stop being valid once A's values are overwritten
+  h->factored = h->csc_ready = false;
   h->f32_values = f32;
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->device));
@@ -1661,7 +1668,8 @@ int mfgpu_solve_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ld
                        int32_t refine) {
   if (!h) return MFGPU_ERR_ARGUMENT;
   if (!h->factored) return fail(h, MFGPU_ERR_STATE, "solve before factor");
-  if (nrhs < 0 || ldb < h->plan.n || ldx < h->plan.n || refine < 0) return fail(h, MFGPU_ERR_ARGUMENT, "bad solve sizes");
+  if (nrhs < 0 || ldb < h->plan.n || ldx < h->plan.n || refine < 0 || (nrhs && h->plan.n && (!d_b || !d_x)))
+    return fail(h, MFGPU_ERR_ARGUMENT, "bad solve sizes");
   if (nrhs == 0 || h->plan.n == 0) return MFGPU_OK;
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->device));
@@ -1706,6 +1714,8 @@ int mfgpu_backward_error_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, i
     *out = 0.0;
     return MFGPU_OK;
   }
+  if (!d_b || !d_x || ldb < h->plan.n || ldx < h->plan.n)
+    return fail(h, MFGPU_ERR_ARGUMENT, "null vectors or leading dimension below n");
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->device));
     const Plan& P = h->plan;

@@ -1,5 +1,5 @@
 """mfgpu_analyze with the reference's own symbolic arrays, and the state a
-failed analysis leaves behind.
+rejected call leaves behind.
 
 The Julia host hands libmfgpu the SymbolicMF it computed itself
 (src/symbolic.jl:203-209: qf, parent, sstart and the update sets); the
@@ -7,7 +7,9 @@ factorization from those arrays must equal the oracle's.  An inconsistent
 set is rejected on the host before any map reaches the device, and the
 handle is then unanalyzed: factor and solve report a call-order error
 instead of running the previous analysis's device maps against a
-half-built plan.  A single-system analysis also ends a batch analysis.
+half-built plan.  A single-system analysis also ends a batch analysis.  A
+factor call rejected for its arguments leaves the previous factorization
+in place.
 None of these cases hands a kernel an inconsistent map: the rejections
 happen in host code before the first upload.
 """
@@ -80,3 +82,47 @@ def test_single_system_analysis_ends_the_batch():
         splu_batch(As, ctx=ctx, check=False)
     assert e.value.code == ERR_STATE
     assert ctx.factor(A.nzval, None, False) == 0
+
+
+def test_rejected_factor_call_keeps_the_factorization():
+    A = M.poisson3d(8)
+    ctx = GpuContext()
+    ctx.analyze(A, symbolic_mf(A))
+    assert ctx.factor(A.nzval, None, False) == 0
+    b = M.rhs(A.n, seed=2)
+    x0 = ctx.solve(b, 0)
+    assert ctx._lib.mfgpu_factor(ctx._h, None, None, 0) == -1
+    assert ctx._lib.mfgpu_factor_scaled(ctx._h, None, 1, 0) == -1
+    assert ctx._lib.mfgpu_factor_device(ctx._h, None, None, 0) == -1
+    assert ctx._lib.mfgpu_factor_f32(ctx._h, None, None, 0) == -1
+    np.testing.assert_array_equal(ctx.solve(b, 0), x0)
+
+
+def test_device_entry_points_check_pointers_and_leading_dimensions():
+    import ctypes
+
+    import torch
+
+    A = M.poisson3d(8)
+    n, k = A.n, 2
+    ctx = GpuContext()
+    ctx.analyze(A, symbolic_mf(A))
+    assert ctx.factor(A.nzval, None, False) == 0
+    B = M.rhs(n, seed=4, nrhs=k)
+    d_b = torch.from_numpy(np.asfortranarray(B).ravel(order="F")).cuda()
+    d_x = torch.zeros_like(d_b)
+    out = ctypes.c_double()
+    lib, h = ctx._lib, ctx._h
+    null = ctypes.c_void_p(None)
+    # rejected on the host before any launch (the buffers hold n * k values,
+    # so even the short leading dimension would read in bounds)
+    assert lib.mfgpu_solve_device(h, k, null, n, d_x.data_ptr(), n, 0) == -1
+    assert lib.mfgpu_solve_device(h, k, d_b.data_ptr(), n, null, n, 0) == -1
+    assert lib.mfgpu_solve_device(h, k, d_b.data_ptr(), n - 1, d_x.data_ptr(), n, 0) == -1
+    assert lib.mfgpu_backward_error_device(h, k, null, n, d_x.data_ptr(), n, ctypes.byref(out)) == -1
+    assert lib.mfgpu_backward_error_device(h, k, d_b.data_ptr(), n, d_x.data_ptr(), n - 1, ctypes.byref(out)) == -1
+    # the handle still solves, and the backward error of that solve is tiny
+    assert lib.mfgpu_solve_device(h, k, d_b.data_ptr(), n, d_x.data_ptr(), n, 0) == 0
+    torch.cuda.synchronize()
+    assert lib.mfgpu_backward_error_device(h, k, d_b.data_ptr(), n, d_x.data_ptr(), n, ctypes.byref(out)) == 0
+    assert out.value <= 1e-14
