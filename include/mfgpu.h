@@ -153,7 +153,13 @@ int mfgpu_set_growth_limit(mfgpu_ctx* h, double limit);
  * result: A's pattern (colptr, rowval, n x n), SymbolicMF.qf, .parent,
  * .sstart, and the update set of every supernode, i.e. colstruct[sstart[s+1]-1]
  * flattened into upd_ptr (nsuper+1) / upd_idx.  Replaces the pattern-only part
- * of multifrontal_lu (src/multifrontal.jl:152-196). */
+ * of multifrontal_lu (src/multifrontal.jl:152-196).
+ * The arrays are checked before use (a partition of 1:n, monotone upd_ptr,
+ * sorted update rows below their supernode that lie in the parent's front,
+ * parent an elimination tree, qf a permutation, A's pattern inside the
+ * fronts); an inconsistent set returns MFGPU_ERR_ARGUMENT.  Any failed
+ * analysis leaves the handle unanalyzed (factor and solve then return
+ * MFGPU_ERR_STATE) and ends a batch analysis. */
 int mfgpu_analyze(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf,
                   const int64_t* parent, int64_t nsuper, const int64_t* sstart, const int64_t* upd_ptr,
                   const int64_t* upd_idx);
