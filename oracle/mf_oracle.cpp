@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -51,6 +52,16 @@ typedef void (*strsm_fn)(const char*, const char*, const char*, const char*, con
 typedef void (*sgemm_fn)(const char*, const char*, const i64*, const i64*, const i64*,
                          const float*, const float*, const i64*, const float*, const i64*,
                          const float*, float*, const i64*, size_t, size_t);
+// double-complex variants (ComplexF64 factorizations); Fortran COMPLEX*16 has
+// std::complex<double>'s layout
+typedef std::complex<double> cplx;
+typedef void (*zgetrf_fn)(const i64*, const i64*, cplx*, const i64*, i64*, i64*);
+typedef void (*ztrsm_fn)(const char*, const char*, const char*, const char*, const i64*,
+                         const i64*, const cplx*, const cplx*, const i64*, cplx*,
+                         const i64*, size_t, size_t, size_t, size_t);
+typedef void (*zgemm_fn)(const char*, const char*, const i64*, const i64*, const i64*,
+                         const cplx*, const cplx*, const i64*, const cplx*, const i64*,
+                         const cplx*, cplx*, const i64*, size_t, size_t);
 typedef void (*setthreads_fn)(int);
 typedef int (*getthreads_fn)(void);
 
@@ -60,6 +71,9 @@ static dgemm_fn g_dgemm = nullptr;
 static sgetrf_fn g_sgetrf = nullptr;
 static strsm_fn g_strsm = nullptr;
 static sgemm_fn g_sgemm = nullptr;
+static zgetrf_fn g_zgetrf = nullptr;
+static ztrsm_fn g_ztrsm = nullptr;
+static zgemm_fn g_zgemm = nullptr;
 static setthreads_fn g_setthreads = nullptr;
 static getthreads_fn g_getthreads = nullptr;
 static std::string g_err;
@@ -642,36 +656,43 @@ Symbolic symbolic_mf0(i64 n, const i64* cp, const i64* ri, const vector<i64>* q)
 // ---------------------------------------------------------------------------
 // Numeric multifrontal (multifrontal.jl:45-375)
 // ---------------------------------------------------------------------------
-struct Factor {
+// Factor values of type Xv: double for Float64 and Float32 matrices (Float32
+// values widen exactly), complex for ComplexF64 ones.
+template <typename Xv>
+struct FactorT {
   i64 n = 0;
   vector<i64> Lp, Li, Up, Ui;           // 0-based
-  vector<double> Lx, Ux;
+  vector<Xv> Lx, Ux;
   vector<i64> p, q, pinv;               // 0-based
   i64 status = 0;                       // 0 ok, k>0: singular at column k (1-based)
 };
+using Factor = FactorT<double>;
+using FactorC = FactorT<cplx>;
 
 // A[qf,qf] as CSC (sorted rows) plus its transpose.
-struct Csc {
+template <typename Xv>
+struct CscT {
   i64 n = 0;
   vector<i64> cp, ri;
-  vector<double> x;
+  vector<Xv> x;
 };
 
-Csc permute_csc(i64 n, const i64* cp, const i64* ri, const double* x, const vector<i64>& q) {
+template <typename Xv>
+CscT<Xv> permute_csc(i64 n, const i64* cp, const i64* ri, const Xv* x, const vector<i64>& q) {
   vector<i64> pinv(n);
   for (i64 k = 0; k < n; ++k) pinv[q[k]] = k;
-  Csc v;
+  CscT<Xv> v;
   v.n = n;
   v.cp.assign(n + 1, 0);
   for (i64 j = 0; j < n; ++j) v.cp[j + 1] = v.cp[j] + (cp[q[j] + 1] - cp[q[j]]);
   v.ri.resize(v.cp[n]);
   v.x.resize(v.cp[n]);
-  vector<std::pair<i64, double>> tmp;
+  vector<std::pair<i64, Xv>> tmp;
   for (i64 j = 0; j < n; ++j) {
     tmp.clear();
     for (i64 p = cp[q[j]]; p < cp[q[j] + 1]; ++p) tmp.push_back({pinv[ri[p]], x[p]});
     std::sort(tmp.begin(), tmp.end(),
-              [](const std::pair<i64, double>& a, const std::pair<i64, double>& b) { return a.first < b.first; });
+              [](const std::pair<i64, Xv>& a, const std::pair<i64, Xv>& b) { return a.first < b.first; });
     for (size_t t = 0; t < tmp.size(); ++t) {
       v.ri[v.cp[j] + t] = tmp[t].first;
       v.x[v.cp[j] + t] = tmp[t].second;
@@ -680,8 +701,9 @@ Csc permute_csc(i64 n, const i64* cp, const i64* ri, const double* x, const vect
   return v;
 }
 
-Csc transpose_csc(const Csc& a) {
-  Csc t;
+template <typename Xv>
+CscT<Xv> transpose_csc(const CscT<Xv>& a) {
+  CscT<Xv> t;
   i64 n = a.n;
   t.n = n;
   t.cp.assign(n + 1, 0);
@@ -755,18 +777,34 @@ struct Blas<float> {
   }
 };
 
+template <>
+struct Blas<cplx> {
+  static bool ok() { return g_zgetrf && g_ztrsm && g_zgemm; }
+  static void getrf(const i64* m, const i64* n, cplx* a, const i64* ld, i64* ipiv, i64* info) {
+    g_zgetrf(m, n, a, ld, ipiv, info);
+  }
+  static void trsm(const char* sd, const char* ul, const char* tr, const char* dg, const i64* m, const i64* n,
+                   const cplx* al, const cplx* a, const i64* lda, cplx* b, const i64* ldb) {
+    g_ztrsm(sd, ul, tr, dg, m, n, al, a, lda, b, ldb, 1, 1, 1, 1);
+  }
+  static void gemm(const i64* m, const i64* n, const i64* k, const cplx* al, const cplx* a, const i64* lda,
+                   const cplx* b, const i64* ldb, const cplx* be, cplx* c, const i64* ldc) {
+    g_zgemm("N", "N", m, n, k, al, a, lda, b, ldb, be, c, ldc, 1, 1);
+  }
+};
+
 // Fronts, contribution blocks and all arithmetic in T; x holds the matrix
-// values (Float32 values widen exactly), the factor keeps them as double.
-template <typename T>
-int numeric_mf(i64 n, const i64* cp, const i64* ri, const double* x, const Symbolic& S, bool check,
-               Factor& F) {
+// values in Xv (Float32 values widen exactly to double), the factor keeps Xv.
+template <typename T, typename Xv = double>
+int numeric_mf(i64 n, const i64* cp, const i64* ri, const Xv* x, const Symbolic& S, bool check,
+               FactorT<Xv>& F) {
   if (!Blas<T>::ok()) {
     g_err = "BLAS not loaded (call orc_set_blas first)";
     return -1;
   }
   F.n = n;
-  Csc V = permute_csc(n, cp, ri, x, S.qf);
-  Csc Vt = transpose_csc(V);
+  CscT<Xv> V = permute_csc(n, cp, ri, x, S.qf);
+  CscT<Xv> Vt = transpose_csc(V);
   i64 nsuper = (i64)S.sstart.size() - 1;
   vector<i64> loc(n, -1), prow(n);
   for (i64 k = 0; k < n; ++k) prow[k] = k;
@@ -911,15 +949,15 @@ int numeric_mf(i64 n, const i64* cp, const i64* ri, const double* x, const Symbo
 }
 
 // solve.jl:10-22 and 25-39
-template <typename T>
-void lsolve(const Factor& F, T* y) {
+template <typename T, typename FT>
+void lsolve(const FT& F, T* y) {
   for (i64 j = 0; j < F.n; ++j) {
     T yj = y[j];
     for (i64 p = F.Lp[j] + 1; p < F.Lp[j + 1]; ++p) y[F.Li[p]] -= (T)F.Lx[p] * yj;
   }
 }
-template <typename T>
-void usolve(const Factor& F, T* y) {
+template <typename T, typename FT>
+void usolve(const FT& F, T* y) {
   for (i64 j = F.n - 1; j >= 0; --j) {
     i64 pd = F.Up[j + 1] - 1;
     T yj = y[j] / (T)F.Ux[pd];
@@ -949,6 +987,9 @@ int orc_set_blas(const char* path) {
   g_sgetrf = (sgetrf_fn)dlsym(h, "scipy_sgetrf_64_");
   g_strsm = (strsm_fn)dlsym(h, "scipy_strsm_64_");
   g_sgemm = (sgemm_fn)dlsym(h, "scipy_sgemm_64_");
+  g_zgetrf = (zgetrf_fn)dlsym(h, "scipy_zgetrf_64_");
+  g_ztrsm = (ztrsm_fn)dlsym(h, "scipy_ztrsm_64_");
+  g_zgemm = (zgemm_fn)dlsym(h, "scipy_zgemm_64_");
   g_setthreads = (setthreads_fn)dlsym(h, "scipy_openblas_set_num_threads64_");
   g_getthreads = (getthreads_fn)dlsym(h, "scipy_openblas_get_num_threads64_");
   if (!g_dgetrf || !g_dtrsm || !g_dgemm) {
@@ -1205,6 +1246,117 @@ void orc_solve_f32(void* h, const float* Rs, i64 n, const i64* colptr, const i64
       for (i64 i = 0; i < n; ++i) r[i] = b[i] - ax[i];
       solve1(r.data(), d.data());
       for (i64 i = 0; i < n; ++i) x[i] = x[i] + d[i];
+    }
+  }
+}
+
+
+// ---- ComplexF64 (the reference's generic Tv = ComplexF64) ---------------------
+// Values cross as interleaved (re, im) doubles, the memory layout of Julia's
+// ComplexF64 and of std::complex<double>.  The fronts run through zgetrf /
+// ztrsm / zgemm, the calls Julia's lu! / rdiv! / ldiv! / mul! make on a
+// Matrix{ComplexF64} (multifrontal.jl:247-275): zgetrf chooses the pivot of
+// largest |re| + |im| (LAPACK's izamax), first on ties.
+
+// row_scaling with R = real(Tv) = Float64 and abs(z) = hypot(re, im)
+// (scaling.jl:92-115).
+void orc_row_scaling_c64(i64 n, const i64* colptr, const i64* rowval, const double* nzval_ri, int kind, double* Rs) {
+  for (i64 i = 0; i < n; ++i) Rs[i] = 1.0;
+  if (kind == 0) return;
+  vector<double> acc(n, 0.0);
+  i64 nz = colptr[n] - 1;
+  for (i64 p = 0; p < nz; ++p) {
+    i64 i = rowval[p] - 1;
+    double v = std::hypot(nzval_ri[2 * p], nzval_ri[2 * p + 1]);
+    if (kind == 1)
+      acc[i] += v;
+    else
+      acc[i] = v > acc[i] ? v : acc[i];
+  }
+  for (i64 i = 0; i < n; ++i) Rs[i] = acc[i] > 0 ? 1.0 / acc[i] : 1.0;
+}
+
+// multifrontal_lu of a ComplexF64 matrix (already scaled by the caller).
+void* orc_multifrontal_lu_c64(i64 n, const i64* colptr, const i64* rowval, const double* nzval_ri, const i64* q1,
+                              int check, i64* status) {
+  vector<i64> cp, ri;
+  to0(n, colptr, rowval, cp, ri);
+  vector<i64> q;
+  if (q1) {
+    q.resize(n);
+    for (i64 k = 0; k < n; ++k) q[k] = q1[k] - 1;
+  }
+  Symbolic S = symbolic_mf0(n, cp.data(), ri.data(), q1 ? &q : nullptr);
+  vector<cplx> xz(cp[n]);
+  for (i64 p = 0; p < cp[n]; ++p) xz[p] = cplx(nzval_ri[2 * p], nzval_ri[2 * p + 1]);
+  FactorC* F = new FactorC();
+  int rc = numeric_mf<cplx, cplx>(n, cp.data(), ri.data(), xz.data(), S, check != 0, *F);
+  *status = rc < 0 ? rc : F->status;
+  return F;
+}
+void orc_factor_free_c64(void* h) { delete (FactorC*)h; }
+void orc_factor_sizes_c64(void* h, i64* out) {
+  FactorC* F = (FactorC*)h;
+  out[0] = F->n;
+  out[1] = F->Lp.empty() ? 0 : F->Lp[F->n];
+  out[2] = F->Up.empty() ? 0 : F->Up[F->n];
+}
+void orc_factor_get_c64(void* h, i64* Lp, i64* Li, double* Lx_ri, i64* Up, i64* Ui, double* Ux_ri, i64* p, i64* q,
+                        i64* pinv) {
+  FactorC* F = (FactorC*)h;
+  i64 n = F->n;
+  for (i64 k = 0; k <= n; ++k) {
+    Lp[k] = F->Lp[k] + 1;
+    Up[k] = F->Up[k] + 1;
+  }
+  for (size_t k = 0; k < F->Li.size(); ++k) {
+    Li[k] = F->Li[k] + 1;
+    Lx_ri[2 * k] = F->Lx[k].real();
+    Lx_ri[2 * k + 1] = F->Lx[k].imag();
+  }
+  for (size_t k = 0; k < F->Ui.size(); ++k) {
+    Ui[k] = F->Ui[k] + 1;
+    Ux_ri[2 * k] = F->Ux[k].real();
+    Ux_ri[2 * k + 1] = F->Ux[k].imag();
+  }
+  for (i64 k = 0; k < n; ++k) {
+    p[k] = F->p[k] + 1;
+    q[k] = F->q[k] + 1;
+    pinv[k] = F->pinv[k] + 1;
+  }
+}
+
+// solve(F::PureLU{ComplexF64}, b; refine) (interface.jl:123-177): real Rs
+// (NULL = none), complex b and x, the residual b - A x with the unscaled A.
+void orc_solve_c64(void* h, const double* Rs, i64 n, const i64* colptr, const i64* rowval, const double* nzval_ri,
+                   i64 nrhs, const double* B_ri, double* X_ri, int refine) {
+  FactorC* F = (FactorC*)h;
+  vector<cplx> c(n), r(n), d(n), ax(n), b(n), x(n);
+  auto solve1 = [&](const cplx* bb, cplx* xx) {
+    for (i64 k = 0; k < n; ++k) c[k] = Rs ? Rs[F->p[k]] * bb[F->p[k]] : bb[F->p[k]];
+    lsolve(*F, c.data());
+    usolve(*F, c.data());
+    for (i64 k = 0; k < n; ++k) xx[F->q[k]] = c[k];
+  };
+  for (i64 col = 0; col < nrhs; ++col) {
+    const double* bc = B_ri + 2 * col * n;
+    for (i64 i = 0; i < n; ++i) b[i] = cplx(bc[2 * i], bc[2 * i + 1]);
+    solve1(b.data(), x.data());
+    for (int it = 0; it < refine; ++it) {
+      std::fill(ax.begin(), ax.end(), cplx(0.0, 0.0));
+      for (i64 j = 0; j < n; ++j) {
+        const cplx xj = x[j];
+        for (i64 p = colptr[j] - 1; p < colptr[j + 1] - 1; ++p)
+          ax[rowval[p] - 1] += cplx(nzval_ri[2 * p], nzval_ri[2 * p + 1]) * xj;
+      }
+      for (i64 i = 0; i < n; ++i) r[i] = b[i] - ax[i];
+      solve1(r.data(), d.data());
+      for (i64 i = 0; i < n; ++i) x[i] = x[i] + d[i];
+    }
+    double* xc = X_ri + 2 * col * n;
+    for (i64 i = 0; i < n; ++i) {
+      xc[2 * i] = x[i].real();
+      xc[2 * i + 1] = x[i].imag();
     }
   }
 }

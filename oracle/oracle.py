@@ -16,6 +16,10 @@ its 1-based Int64 index convention:
 * ``*_f32``              the same for the reference's generic Tv = Float32: row
   scaling, the numeric phase (sgetrf / strsm / sgemm fronts) and the solve
   with its refinement, all in Float32 arithmetic
+* ``*_c64``              the same for Tv = ComplexF64 (``ComplexCSC`` values):
+  real row scaling from |z| = hypot(re, im), zgetrf / ztrsm / zgemm fronts
+  (pivot of largest |re| + |im|, LAPACK's rule, as Julia's lu! uses), complex
+  solves and refinement
 """
 
 from __future__ import annotations
@@ -90,6 +94,15 @@ def lib():
         L.orc_multifrontal_lu_f32.argtypes = [ctypes.c_int64, _i64p, _i64p, _f32p, _i64p, ctypes.c_int, _i64p]
         L.orc_solve_f32.argtypes = [ctypes.c_void_p, _f32p, ctypes.c_int64, _i64p, _i64p, _f32p, ctypes.c_int64,
                                     _f32p, _f32p, ctypes.c_int]
+        L.orc_row_scaling_c64.argtypes = [ctypes.c_int64, _i64p, _i64p, _f64p, ctypes.c_int, _f64p]
+        L.orc_multifrontal_lu_c64.restype = ctypes.c_void_p
+        L.orc_multifrontal_lu_c64.argtypes = [ctypes.c_int64, _i64p, _i64p, _f64p, _i64p, ctypes.c_int, _i64p]
+        L.orc_factor_free_c64.argtypes = [ctypes.c_void_p]
+        L.orc_factor_sizes_c64.argtypes = [ctypes.c_void_p, _i64p]
+        L.orc_factor_get_c64.argtypes = [ctypes.c_void_p, _i64p, _i64p, _f64p, _i64p, _i64p, _f64p, _i64p, _i64p,
+                                         _i64p]
+        L.orc_solve_c64.argtypes = [ctypes.c_void_p, _f64p, ctypes.c_int64, _i64p, _i64p, _f64p, ctypes.c_int64,
+                                    _f64p, _f64p, ctypes.c_int]
         rc = L.orc_set_blas(openblas_path().encode())
         if rc != 0:
             raise RuntimeError("oracle: cannot load OpenBLAS: " + L.orc_last_error().decode())
@@ -361,4 +374,112 @@ def solve_f32(F: PureLU, b: np.ndarray, refine: int = 0) -> np.ndarray:
     X = np.empty_like(B)
     lib().orc_solve_f32(ctypes.c_void_p(F.F.handle), _p(_f32(F.Rs), _f32p), A.n, _p(_i(A.colptr)),
                         _p(_i(A.rowval)), _p(_f32(A.nzval), _f32p), nrhs, _p(B, _f32p), _p(X, _f32p), int(refine))
+    return X
+
+
+# ---------------------------------------------------------------------------
+# ComplexF64 (the reference's generic Tv = ComplexF64)
+# ---------------------------------------------------------------------------
+@dataclass
+class ComplexCSC:
+    """SparseMatrixCSC{ComplexF64, Int64}: 1-based pattern, complex values."""
+
+    m: int
+    n: int
+    colptr: np.ndarray
+    rowval: np.ndarray
+    nzval: np.ndarray
+
+    @staticmethod
+    def from_scipy(S) -> "ComplexCSC":
+        S = S.tocsc()
+        S.sort_indices()
+        S.sum_duplicates()
+        return ComplexCSC(S.shape[0], S.shape[1], S.indptr.astype(np.int64) + 1, S.indices.astype(np.int64) + 1,
+                          np.ascontiguousarray(S.data, dtype=np.complex128))
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+
+        return sp.csc_matrix((self.nzval, self.rowval - 1, self.colptr - 1), shape=(self.m, self.n))
+
+    def nnz(self) -> int:
+        return len(self.rowval)
+
+
+def _ri(z) -> np.ndarray:
+    """Complex values as interleaved (re, im) doubles."""
+    return np.ascontiguousarray(z, dtype=np.complex128).view(np.float64)
+
+
+@dataclass
+class FactorC(Factor):
+    """Factor of a ComplexF64 matrix (complex Lnzval / Unzval)."""
+
+    def __del__(self):
+        if self.handle and _lib is not None:
+            _lib.orc_factor_free_c64(ctypes.c_void_p(self.handle))
+            self.handle = 0
+
+
+def row_scaling_c64(A: ComplexCSC, kind: int) -> np.ndarray:
+    """row_scaling of a ComplexF64 matrix: Float64 Rs from |z| = hypot(re, im)
+    (scaling.jl:92-115 with R = real(Tv))."""
+    Rs = np.empty(A.m)
+    lib().orc_row_scaling_c64(A.m, _p(_i(A.colptr)), _p(_i(A.rowval)), _p(_ri(A.nzval), _f64p), int(kind),
+                              _p(Rs, _f64p))
+    return Rs
+
+
+def multifrontal_lu_c64(A: ComplexCSC, q=None, check: bool = True) -> FactorC:
+    """multifrontal_lu of a ComplexF64 matrix (multifrontal.jl:146-358 with
+    Tv = ComplexF64): every front operation in complex double."""
+    st = np.zeros(1, np.int64)
+    qa = _i(q) if q is not None else None
+    h = lib().orc_multifrontal_lu_c64(A.n, _p(_i(A.colptr)), _p(_i(A.rowval)), _p(_ri(A.nzval), _f64p), _p(qa),
+                                      int(check), _p(st))
+    if st[0] != 0:
+        lib().orc_factor_free_c64(ctypes.c_void_p(h))
+        if st[0] > 0:
+            raise SingularException(int(st[0]))
+        raise RuntimeError("oracle: " + lib().orc_last_error().decode())
+    sz = np.empty(3, dtype=np.int64)
+    lib().orc_factor_sizes_c64(ctypes.c_void_p(h), _p(sz))
+    n, nl, nu = (int(v) for v in sz)
+    Lp, Up = np.empty(n + 1, np.int64), np.empty(n + 1, np.int64)
+    Li, Ui = np.empty(nl, np.int64), np.empty(nu, np.int64)
+    Lx, Ux = np.empty(nl, np.complex128), np.empty(nu, np.complex128)
+    p, qq, pinv = np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.int64)
+    lib().orc_factor_get_c64(ctypes.c_void_p(h), _p(Lp), _p(Li), _p(Lx.view(np.float64), _f64p), _p(Up), _p(Ui),
+                             _p(Ux.view(np.float64), _f64p), _p(p), _p(qq), _p(pinv))
+    return FactorC(Lp, Li, Lx, Up, Ui, Ux, p, qq, pinv, handle=h)
+
+
+def apply_row_scaling_c64(A: ComplexCSC, Rs) -> ComplexCSC:
+    """Rs .* A: each part of a value times its row's real factor."""
+    r = np.asarray(Rs, dtype=np.float64)[A.rowval - 1]
+    z = np.empty(len(A.nzval), np.complex128)
+    z.real = A.nzval.real * r
+    z.imag = A.nzval.imag * r
+    return ComplexCSC(A.m, A.n, A.colptr.copy(), A.rowval.copy(), z)
+
+
+def splu_c64(A: ComplexCSC, scale: int = SCALE_SUM, check: bool = True, q=None) -> PureLU:
+    """splu(A::SparseMatrixCSC{ComplexF64}; method=:multifrontal, scale)."""
+    if A.m != A.n:
+        raise ValueError("DimensionMismatch: splu requires a square matrix")
+    Rs = row_scaling_c64(A, scale)
+    As = A if scale == SCALE_NONE else apply_row_scaling_c64(A, Rs)
+    return PureLU(multifrontal_lu_c64(As, q=q, check=check), Rs, A)
+
+
+def solve_c64(F: PureLU, b: np.ndarray, refine: int = 0) -> np.ndarray:
+    """solve(F::PureLU{ComplexF64}, b; refine) (interface.jl:170-177)."""
+    A = F.A
+    B = np.asfortranarray(b, dtype=np.complex128)
+    nrhs = 1 if B.ndim == 1 else B.shape[1]
+    X = np.empty_like(B)
+    lib().orc_solve_c64(ctypes.c_void_p(F.F.handle), _p(_f(F.Rs), _f64p), A.n, _p(_i(A.colptr)), _p(_i(A.rowval)),
+                        _p(_ri(A.nzval), _f64p), nrhs, _p(B.ravel(order="F").view(np.float64), _f64p),
+                        _p(X.ravel(order="F").view(np.float64), _f64p), int(refine))
     return X
