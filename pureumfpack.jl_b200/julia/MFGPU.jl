@@ -20,6 +20,14 @@ mutable struct Handle
     f32::Bool   # the last factorization is of a Float32 matrix
 end
 
+# The C ABI takes Int64 indices; a SparseMatrixCSC{Tv, Int32} (the reference's
+# generic Ti, test/robustness.jl) is widened on the way in and its factors
+# are returned with the caller's index type.
+_i64(v::Vector{Int64}) = v
+_i64(v::AbstractVector{<:Integer}) = Vector{Int64}(v)
+_ti(::Type{Int64}, v::Vector{Int64}) = v
+_ti(::Type{Ti}, v::Vector{Int64}) where {Ti <: Integer} = Vector{Ti}(v)
+
 function _check(h::Handle, rc::Cint)
     rc >= 0 && return Int(rc)
     msg = unsafe_string(ccall((:mfgpu_last_error, libmfgpu), Cstring, (Ptr{Cvoid},), h.ptr))
@@ -40,7 +48,7 @@ end
 
 # mfgpu_analyze from the reference's SymbolicMF (src/symbolic.jl:203-209):
 # update set of supernode s = colstruct[sstart[s+1]-1].
-function analyze!(h::Handle, A::SparseMatrixCSC{<:Union{Float64, Float32}, Int64}, S)
+function analyze!(h::Handle, A::SparseMatrixCSC{<:Union{Float64, Float32}, <:Integer}, S)
     n = size(A, 2)
     nsuper = length(S.sstart) - 1
     upd_ptr = Vector{Int64}(undef, nsuper + 1)
@@ -54,7 +62,7 @@ function analyze!(h::Handle, A::SparseMatrixCSC{<:Union{Float64, Float32}, Int64
     end
     rc = ccall((:mfgpu_analyze, libmfgpu), Cint,
         (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}),
-        h.ptr, n, A.colptr, rowvals(A), collect(Int64, S.qf), collect(Int64, S.parent), nsuper,
+        h.ptr, n, _i64(A.colptr), _i64(rowvals(A)), collect(Int64, S.qf), collect(Int64, S.parent), nsuper,
         collect(Int64, S.sstart), upd_ptr, upd_idx)
     _check(h, rc)
     h.n = n
@@ -62,7 +70,7 @@ function analyze!(h::Handle, A::SparseMatrixCSC{<:Union{Float64, Float32}, Int64
 end
 
 # Numeric factorization of Diagonal(Rs) * A (Rs === nothing: no scaling).
-function factor!(h::Handle, A::SparseMatrixCSC{Float64, Int64}, Rs, check::Bool)
+function factor!(h::Handle, A::SparseMatrixCSC{Float64, <:Integer}, Rs, check::Bool)
     rs = Rs === nothing ? C_NULL : pointer(Rs)
     rc = GC.@preserve Rs ccall((:mfgpu_factor, libmfgpu), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int32),
         h.ptr, nonzeros(A), rs, Int32(check))
@@ -74,7 +82,7 @@ end
 
 # Float32 matrices (the reference's generic Tv = Float32): Float32 values,
 # Rs, factors, right-hand sides and solutions.
-function factor!(h::Handle, A::SparseMatrixCSC{Float32, Int64}, Rs, check::Bool)
+function factor!(h::Handle, A::SparseMatrixCSC{Float32, <:Integer}, Rs, check::Bool)
     rs = Rs === nothing ? C_NULL : pointer(Rs)
     rc = GC.@preserve Rs ccall((:mfgpu_factor_f32, libmfgpu), Cint, (Ptr{Cvoid}, Ptr{Float32}, Ptr{Float32}, Int32),
         h.ptr, nonzeros(A), rs, Int32(check))
@@ -84,9 +92,10 @@ function factor!(h::Handle, A::SparseMatrixCSC{Float32, Int64}, Rs, check::Bool)
     return h
 end
 
-# GPLUFactorization fields (src/gplu.jl:45-51) copied back from the GPU.
-function factors(h::Handle)
-    h.f32 && return factors_f32(h)
+# GPLUFactorization fields (src/gplu.jl:45-51) copied back from the GPU, with
+# index type Ti (that of the factored matrix).
+function factors(h::Handle; indextype::Type{<:Integer} = Int64)
+    h.f32 && return factors_f32(h; indextype = indextype)
     sz = Vector{Int64}(undef, 3)
     _check(h, ccall((:mfgpu_factor_sizes, libmfgpu), Cint, (Ptr{Cvoid}, Ptr{Int64}), h.ptr, sz))
     n, nl, nu = sz
@@ -96,10 +105,12 @@ function factors(h::Handle)
     _check(h, ccall((:mfgpu_get_factors, libmfgpu), Cint,
         (Ptr{Cvoid}, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}, Ptr{Int64},
          Ptr{Int64}, Ptr{Int64}), h.ptr, Lp, Li, Lx, Up, Ui, Ux, p, q, pinv))
-    return SparseMatrixCSC(n, n, Lp, Li, Lx), SparseMatrixCSC(n, n, Up, Ui, Ux), p, q, pinv
+    T = indextype
+    return SparseMatrixCSC(n, n, _ti(T, Lp), _ti(T, Li), Lx), SparseMatrixCSC(n, n, _ti(T, Up), _ti(T, Ui), Ux),
+           _ti(T, p), _ti(T, q), _ti(T, pinv)
 end
 
-function factors_f32(h::Handle)
+function factors_f32(h::Handle; indextype::Type{<:Integer} = Int64)
     sz = Vector{Int64}(undef, 3)
     _check(h, ccall((:mfgpu_factor_sizes, libmfgpu), Cint, (Ptr{Cvoid}, Ptr{Int64}), h.ptr, sz))
     n, nl, nu = sz
@@ -109,7 +120,9 @@ function factors_f32(h::Handle)
     _check(h, ccall((:mfgpu_get_factors_f32, libmfgpu), Cint,
         (Ptr{Cvoid}, Ptr{Int64}, Ptr{Int64}, Ptr{Float32}, Ptr{Int64}, Ptr{Int64}, Ptr{Float32}, Ptr{Int64},
          Ptr{Int64}, Ptr{Int64}), h.ptr, Lp, Li, Lx, Up, Ui, Ux, p, q, pinv))
-    return SparseMatrixCSC(n, n, Lp, Li, Lx), SparseMatrixCSC(n, n, Up, Ui, Ux), p, q, pinv
+    T = indextype
+    return SparseMatrixCSC(n, n, _ti(T, Lp), _ti(T, Li), Lx), SparseMatrixCSC(n, n, _ti(T, Up), _ti(T, Ui), Ux),
+           _ti(T, p), _ti(T, q), _ti(T, pinv)
 end
 
 function solve(h::Handle, B::AbstractVecOrMat{Float32}; refine::Integer = 0)
@@ -132,11 +145,13 @@ end
 
 # --- batched systems (many independent systems through one handle) -------
 # ordering: 0 = AMD (as splu(A; method=:multifrontal)), 1 = COLAMD.
-function batch_analyze!(h::Handle, As::Vector{SparseMatrixCSC{Float64, Int64}}; ordering::Integer = 0)
+function batch_analyze!(h::Handle, As::AbstractVector{<:SparseMatrixCSC{Float64, <:Integer}}; ordering::Integer = 0)
     ns = Int64[size(A, 1) for A in As]
-    cps = Ptr{Int64}[pointer(A.colptr) for A in As]
-    rvs = Ptr{Int64}[pointer(rowvals(A)) for A in As]
-    GC.@preserve As _check(h, ccall((:mfgpu_batch_analyze, libmfgpu), Cint,
+    cols = [_i64(A.colptr) for A in As]
+    rows = [_i64(rowvals(A)) for A in As]
+    cps = Ptr{Int64}[pointer(c) for c in cols]
+    rvs = Ptr{Int64}[pointer(r) for r in rows]
+    GC.@preserve cols rows _check(h, ccall((:mfgpu_batch_analyze, libmfgpu), Cint,
         (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Ptr{Int64}}, Ptr{Ptr{Int64}}, Int32),
         h.ptr, length(As), ns, cps, rvs, Int32(ordering)))
     return h
@@ -144,7 +159,7 @@ end
 
 # Factor every system with its own row scaling (scale: 0 none, 1 sum, 2 max);
 # returns each system's first singular column (0 = nonsingular).
-function batch_factor!(h::Handle, As::Vector{SparseMatrixCSC{Float64, Int64}}; scale::Integer = 1)
+function batch_factor!(h::Handle, As::AbstractVector{<:SparseMatrixCSC{Float64, <:Integer}}; scale::Integer = 1)
     vals = Ptr{Float64}[pointer(nonzeros(A)) for A in As]
     status = zeros(Int64, length(As))
     GC.@preserve As _check(h, ccall((:mfgpu_batch_factor, libmfgpu), Cint,
@@ -174,7 +189,7 @@ end # module
 #   S = symbolic_mf(A)                       # the reference's own host code
 #   h = MFGPU.analyze!(MFGPU.create(), A, S)
 #   MFGPU.factor!(h, A, scale == SCALE_NONE ? nothing : Rs, check)
-#   L, U, p, q, _ = MFGPU.factors(h)
+#   L, U, p, q, _ = MFGPU.factors(h; indextype = Ti)
 #   return GPUPureLU(PureLU(L, U, p, q, Rs, A), h)
 #
 #   solve(F::GPUPureLU, b; refine=0) = MFGPU.solve(F.h, b; refine = refine)
