@@ -18,10 +18,10 @@ namespace {
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 // body(i) for i in [0, n) on the host's cores (independent iterations, each
-// writing its own outputs); the first exception is rethrown after the join.
+// writing its own outputs), handed out `grain` at a time; the first exception
+// is rethrown after the join.
 template <typename F>
-void parallel_range(int64_t n, F&& body) {
-  const int64_t grain = 4096;
+void parallel_range(int64_t n, F&& body, int64_t grain = 4096) {
   const int64_t nt = std::min<int64_t>(std::max<int64_t>(1, n / grain), std::max(1u, std::thread::hardware_concurrency()));
   if (nt <= 1) {
     for (int64_t i = 0; i < n; ++i) body(i);
@@ -43,6 +43,34 @@ void parallel_range(int64_t n, F&& body) {
   work();
   for (auto& th : pool) th.join();
   if (err) std::rethrow_exception(err);
+}
+
+// Boundaries [b[c], b[c+1]) of consecutive supernode ranges that are closed
+// under the parent relation (a cut after x only where no supernode <= x has
+// a parent > x), grouped to about 16 ranges per host thread of similar work
+// (1 + update rows per supernode).  Every update row of a supernode is a
+// column of one of its ancestors, so the ranges own disjoint columns, fronts
+// and front columns: loops that fill per-column arrays in ascending supernode
+// order can run range by range in parallel and give the sequential result.
+// A single tree is a single range.
+std::vector<int64_t> tree_chunks(const std::vector<int32_t>& parent, const std::vector<int32_t>& nu) {
+  const int64_t ns = (int64_t)parent.size();
+  int64_t total = ns;
+  for (int32_t u : nu) total += u;
+  const int64_t nt = std::max(1u, std::thread::hardware_concurrency());
+  const int64_t target = std::max<int64_t>(1, total / (16 * nt));
+  std::vector<int64_t> b{0};
+  int64_t acc = 0, reach = -1;
+  for (int64_t x = 0; x < ns; ++x) {
+    acc += 1 + nu[x];
+    reach = std::max<int64_t>(reach, parent[x]);
+    if (reach <= x && acc >= target) {
+      b.push_back(x + 1);
+      acc = 0;
+    }
+  }
+  if (b.back() != ns) b.push_back(ns);
+  return b;
 }
 }  // namespace
 
@@ -220,13 +248,15 @@ void build_plan_core(int64_t n, const int64_t* colptr, const int64_t* rowval, co
   });
 
   // ---- slots: supernodes ordered by (height, small before large, id) -------
-  P.slot_super.resize(ns);
-  std::iota(P.slot_super.begin(), P.slot_super.end(), 0);
-  std::stable_sort(P.slot_super.begin(), P.slot_super.end(), [&](int32_t a, int32_t b) {
-    if (P.height[a] != P.height[b]) return P.height[a] < P.height[b];
-    const bool la = P.nf[a] > kSmallFront, lb = P.nf[b] > kSmallFront;
-    return la < lb;
-  });
+  // (a stable counting sort of the ids on the key 2 * height + large)
+  {
+    auto key = [&](int64_t s) { return 2 * (int64_t)P.height[s] + (P.nf[s] > kSmallFront ? 1 : 0); };
+    std::vector<int64_t> start(2 * (int64_t)P.nlevels + 1, 0);
+    for (int64_t s = 0; s < ns; ++s) ++start[key(s) + 1];
+    for (size_t k = 1; k < start.size(); ++k) start[k] += start[k - 1];
+    P.slot_super.resize(ns);
+    for (int64_t s = 0; s < ns; ++s) P.slot_super[start[key(s)]++] = (int32_t)s;
+  }
   P.slot.resize(ns);
   P.level_slot.assign(P.nlevels + 1, 0);
   P.level_large.assign(P.nlevels, 0);
@@ -314,41 +344,50 @@ void build_plan_core(int64_t n, const int64_t* colptr, const int64_t* rowval, co
     throw std::invalid_argument("pattern of A is not covered by the symbolic structure");
 
   // ---- children contributions per parent front column ------------------------
+  // (tree ranges in parallel: a child and its parent share a range)
+  const std::vector<int64_t> chunks = tree_chunks(P.parent_super, P.nu);
+  const int64_t nchunks = (int64_t)chunks.size() - 1;
   P.fc_ch_ptr.assign(cb + 1, 0);
-  for (int64_t k = 0; k < ns; ++k) {
-    const int32_t ps = P.parent_super[k];
-    if (ps < 0) continue;
-    for (int64_t p = P.upd_off[k]; p < P.upd_off[k + 1]; ++p) ++P.fc_ch_ptr[P.colbase[ps] + P.rel[p] + 1];
-  }
+  parallel_range(nchunks, [&](int64_t c) {
+    for (int64_t k = chunks[c]; k < chunks[c + 1]; ++k) {
+      const int32_t ps = P.parent_super[k];
+      if (ps < 0) continue;
+      for (int64_t p = P.upd_off[k]; p < P.upd_off[k + 1]; ++p) ++P.fc_ch_ptr[P.colbase[ps] + P.rel[p] + 1];
+    }
+  }, 1);
   for (int64_t f = 0; f < cb; ++f) P.fc_ch_ptr[f + 1] += P.fc_ch_ptr[f];
   P.fc_ch.resize(2 * (size_t)P.fc_ch_ptr[cb]);
-  {
-    std::vector<int32_t> cur(P.fc_ch_ptr.begin(), P.fc_ch_ptr.end() - 1);
-    for (int64_t ps = 0; ps < ns; ++ps) {
+  // fc_ch_ptr[f] serves as column f's cursor, then shifts back by one
+  parallel_range(nchunks, [&](int64_t c) {
+    for (int64_t ps = chunks[c]; ps < chunks[c + 1]; ++ps) {
       for (int32_t ci = P.child_ptr[ps + 1] - 1; ci >= P.child_ptr[ps]; --ci) {   // last child first
         const int32_t k = P.child_idx[ci];
         for (int32_t t = 0; t < P.nu[k]; ++t) {
           const int64_t f = P.colbase[ps] + P.rel[P.upd_off[k] + t];
-          const int32_t at = cur[f]++;
+          const int32_t at = P.fc_ch_ptr[f]++;
           P.fc_ch[2 * (size_t)at] = k;
           P.fc_ch[2 * (size_t)at + 1] = t;
         }
       }
     }
-  }
+  }, 1);
+  for (int64_t f = cb; f > 0; --f) P.fc_ch_ptr[f] = P.fc_ch_ptr[f - 1];
+  P.fc_ch_ptr[0] = 0;
 
   // ---- factor CSC layout -------------------------------------------------
   if (csc) {
   P.lcolptr.assign(n + 1, 0);
   P.ucolptr.assign(n + 1, 0);
-  for (int64_t s = 0; s < ns; ++s) {
-    const int32_t c1 = P.c1[s], c2 = c1 + P.np[s] - 1;
-    for (int32_t j = c1; j <= c2; ++j) {
-      P.lcolptr[j + 1] = 1 + (c2 - j) + P.nu[s];
-      P.ucolptr[j + 1] += j - c1 + 1;
+  parallel_range(nchunks, [&](int64_t c) {
+    for (int64_t s = chunks[c]; s < chunks[c + 1]; ++s) {
+      const int32_t c1 = P.c1[s], c2 = c1 + P.np[s] - 1;
+      for (int32_t j = c1; j <= c2; ++j) {
+        P.lcolptr[j + 1] = 1 + (c2 - j) + P.nu[s];
+        P.ucolptr[j + 1] += j - c1 + 1;
+      }
+      for (int64_t p = P.upd_off[s]; p < P.upd_off[s + 1]; ++p) P.ucolptr[P.upd[p] + 1] += P.np[s];
     }
-    for (int64_t p = P.upd_off[s]; p < P.upd_off[s + 1]; ++p) P.ucolptr[P.upd[p] + 1] += P.np[s];
-  }
+  }, 1);
   for (int64_t j = 0; j < n; ++j) {
     P.lcolptr[j + 1] += P.lcolptr[j];
     P.ucolptr[j + 1] += P.ucolptr[j];
@@ -358,11 +397,13 @@ void build_plan_core(int64_t n, const int64_t* colptr, const int64_t* rowval, co
   P.uoff.resize(P.upd.size());
   {
     std::vector<int64_t> cur(P.ucolptr.begin(), P.ucolptr.end() - 1);
-    for (int64_t s = 0; s < ns; ++s)
-      for (int64_t p = P.upd_off[s]; p < P.upd_off[s + 1]; ++p) {
-        P.uoff[p] = cur[P.upd[p]];
-        cur[P.upd[p]] += P.np[s];
-      }
+    parallel_range(nchunks, [&](int64_t c) {
+      for (int64_t s = chunks[c]; s < chunks[c + 1]; ++s)
+        for (int64_t p = P.upd_off[s]; p < P.upd_off[s + 1]; ++p) {
+          P.uoff[p] = cur[P.upd[p]];
+          cur[P.upd[p]] += P.np[s];
+        }
+    }, 1);
   }
   }
 
@@ -498,41 +539,55 @@ void attach_original(Plan& P, int64_t ns, const int64_t* sstart, const int64_t* 
     fl += 2.0 / 3.0 * a * a * a + 2.0 * a * a * u + 2.0 * a * u * u;
   }
   P.flops_orig = fl;
-  // factor CSC layout of the original structure (as build_plan's)
+  // factor CSC layout of the original structure (as build_plan's) and the U
+  // blocks per front column in the order of the original supernodes, by the
+  // fronts' tree ranges (every update row of an original supernode lies in
+  // its front, checked above), mapped to the original supernodes they hold
+  const std::vector<int64_t> fch = tree_chunks(P.parent_super, P.nu);
+  const int64_t nchunks = (int64_t)fch.size() - 1;
+  std::vector<int64_t> och(nchunks + 1, ns);
+  for (int64_t c = 0; c < nchunks; ++c) och[c] = P.col_orig[P.c1[fch[c]]];
   P.lcolptr.assign(n + 1, 0);
   P.ucolptr.assign(n + 1, 0);
-  for (int64_t s = 0; s < ns; ++s) {
-    const int32_t c1 = P.o_c1[s], c2 = c1 + P.o_np[s] - 1;
-    const int64_t nu = upd_ptr[s + 1] - upd_ptr[s];
-    for (int32_t j = c1; j <= c2; ++j) {
-      P.lcolptr[j + 1] = 1 + (c2 - j) + nu;
-      P.ucolptr[j + 1] += j - c1 + 1;
+  parallel_range(nchunks, [&](int64_t c) {
+    for (int64_t s = och[c]; s < och[c + 1]; ++s) {
+      const int32_t c1 = P.o_c1[s], c2 = c1 + P.o_np[s] - 1;
+      const int64_t nu = upd_ptr[s + 1] - upd_ptr[s];
+      for (int32_t j = c1; j <= c2; ++j) {
+        P.lcolptr[j + 1] = 1 + (c2 - j) + nu;
+        P.ucolptr[j + 1] += j - c1 + 1;
+      }
+      for (int64_t p = upd_ptr[s]; p < upd_ptr[s + 1]; ++p) P.ucolptr[upd_idx[p] + 1] += P.o_np[s];
     }
-    for (int64_t p = upd_ptr[s]; p < upd_ptr[s + 1]; ++p) P.ucolptr[upd_idx[p] + 1] += P.o_np[s];
-  }
+  }, 1);
   for (int64_t j = 0; j < n; ++j) {
     P.lcolptr[j + 1] += P.lcolptr[j];
     P.ucolptr[j + 1] += P.ucolptr[j];
   }
   P.nnz_l = P.lcolptr[n];
   P.nnz_u = P.ucolptr[n];
-  // U blocks per front column, in the order of the original supernodes
   P.fcu_ptr.assign(P.fc_total + 1, 0);
   auto fcol = [&](int64_t s, int64_t p) { return P.colbase[front_of[P.o_c1[s]]] + P.o_xpos[p]; };
-  for (int64_t s = 0; s < ns; ++s)
-    for (int64_t p = upd_ptr[s]; p < upd_ptr[s + 1]; ++p) ++P.fcu_ptr[fcol(s, p) + 1];
+  parallel_range(nchunks, [&](int64_t c) {
+    for (int64_t s = och[c]; s < och[c + 1]; ++s)
+      for (int64_t p = upd_ptr[s]; p < upd_ptr[s + 1]; ++p) ++P.fcu_ptr[fcol(s, p) + 1];
+  }, 1);
   for (int64_t f = 0; f < P.fc_total; ++f) P.fcu_ptr[f + 1] += P.fcu_ptr[f];
   P.fcu.resize(P.fcu_ptr[P.fc_total]);
+  // fcu_ptr[f] serves as front column f's cursor, then shifts back by one
   std::vector<int64_t> ucur(P.ucolptr.begin(), P.ucolptr.end() - 1);
-  std::vector<int64_t> fcur(P.fcu_ptr.begin(), P.fcu_ptr.end() - 1);
-  for (int64_t s = 0; s < ns; ++s) {
-    const int32_t row0 = P.o_c1[s] - P.c1[front_of[P.o_c1[s]]];
-    for (int64_t p = upd_ptr[s]; p < upd_ptr[s + 1]; ++p) {
-      const int64_t u = upd_idx[p];
-      P.fcu[fcur[fcol(s, p)]++] = UBlock{row0, P.o_np[s], ucur[u]};
-      ucur[u] += P.o_np[s];
+  parallel_range(nchunks, [&](int64_t c) {
+    for (int64_t s = och[c]; s < och[c + 1]; ++s) {
+      const int32_t row0 = P.o_c1[s] - P.c1[front_of[P.o_c1[s]]];
+      for (int64_t p = upd_ptr[s]; p < upd_ptr[s + 1]; ++p) {
+        const int64_t u = upd_idx[p];
+        P.fcu[P.fcu_ptr[fcol(s, p)]++] = UBlock{row0, P.o_np[s], ucur[u]};
+        ucur[u] += P.o_np[s];
+      }
     }
-  }
+  }, 1);
+  for (int64_t f = P.fc_total; f > 0; --f) P.fcu_ptr[f] = P.fcu_ptr[f - 1];
+  P.fcu_ptr[0] = 0;
 }
 }  // namespace
 
@@ -548,16 +603,20 @@ void build_plan_merged(int64_t n, const int64_t* colptr, const int64_t* rowval, 
   }
   // merged partition: a group ends at a supernode that is not merged, and
   // keeps that supernode's update set
-  std::vector<int64_t> ms, mup{0}, mui;
+  std::vector<int64_t> ends, ms, mup{0};
   int64_t first = 0;
   for (int64_t s = 0; s < ns; ++s) {
     if (marks[s]) continue;
+    ends.push_back(s);
     ms.push_back(sstart[first]);
-    mui.insert(mui.end(), upd_idx + upd_ptr[s], upd_idx + upd_ptr[s + 1]);
-    mup.push_back((int64_t)mui.size());
+    mup.push_back(mup.back() + (upd_ptr[s + 1] - upd_ptr[s]));
     first = s + 1;
   }
   ms.push_back(n);
+  std::vector<int64_t> mui(mup.back());
+  parallel_range((int64_t)ends.size(), [&](int64_t g) {
+    std::copy(upd_idx + upd_ptr[ends[g]], upd_idx + upd_ptr[ends[g] + 1], mui.begin() + mup[g]);
+  }, 256);
   build_plan_core(n, colptr, rowval, qf, parent, (int64_t)ms.size() - 1, ms.data(), mup.data(), mui.data(), P,
                   false);
   attach_original(P, ns, sstart, upd_ptr, upd_idx);
