@@ -26,7 +26,7 @@ def column_value_errors(colptr, ref, got):
     colmax = np.zeros(n)
     np.maximum.at(colmax, col, np.abs(ref))
     coln2 = np.zeros(n)
-    np.add.at(coln2, col, ref * ref)
+    np.add.at(coln2, col, np.abs(ref) ** 2)
     errn2 = np.zeros(n)
     np.add.at(errn2, col, d * d)
     nz = coln2 > 0

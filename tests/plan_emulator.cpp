@@ -13,6 +13,7 @@
 // Built by the tests with g++ against the library's plan.cpp and
 // host/symbolic.cpp; never linked into the library.
 #include <cmath>
+#include <complex>
 #include <cstdint>
 #include <algorithm>
 #include <cstring>
@@ -27,23 +28,33 @@ using namespace mfgpu;
 
 namespace {
 
-struct Result {
+typedef std::complex<double> cplx;
+
+template <typename T>
+struct ResultT {
   std::vector<int64_t> lp, li, up, ui, p, q;
-  std::vector<double> lx, ux;
+  std::vector<T> lx, ux;
   int64_t stats[6] = {0, 0, 0, 0, 0, 0};
 };
-Result g_result;
+ResultT<double> g_result;
+ResultT<cplx> g_result_c;
+
+// Pivot magnitude: |x|, and |re| + |im| for complex values (the rule of
+// LAPACK's zgetrf, which Julia's lu! on a ComplexF64 front uses).
+inline double magnitude(double v) { return std::fabs(v); }
+inline double magnitude(const cplx& z) { return std::fabs(z.real()) + std::fabs(z.imag()); }
 
 // Dense LU of every front; returns the fronts (column-major, nf x nf).
-std::vector<std::vector<double>> factor_fronts(const Plan& P, const double* nzval, std::vector<int32_t>& ipiv) {
-  std::vector<double> vx(P.nnz_a);
+template <typename T>
+std::vector<std::vector<T>> factor_fronts(const Plan& P, const T* nzval, std::vector<int32_t>& ipiv) {
+  std::vector<T> vx(P.nnz_a);
   for (int64_t p = 0; p < P.nnz_a; ++p) vx[p] = nzval[P.v_src[p]];
-  std::vector<std::vector<double>> F(P.ns);
+  std::vector<std::vector<T>> F(P.ns);
   for (int64_t x = 0; x < P.ns; ++x) {
     const int nf = P.nf[x], np = P.np[x], c1 = P.c1[x];
-    std::vector<double>& G = F[x];
-    G.assign((size_t)nf * nf, 0.0);
-    auto at = [&](int r, int c) -> double& { return G[r + (size_t)c * nf]; };
+    std::vector<T>& G = F[x];
+    G.assign((size_t)nf * nf, T(0));
+    auto at = [&](int r, int c) -> T& { return G[r + (size_t)c * nf]; };
     for (int c = 0; c < nf; ++c) {
       const int64_t fc = P.colbase[x] + c;
       for (int p = P.fc_vbeg[fc]; p < P.fc_vend[fc]; ++p) at(P.v_frow[p], c) = vx[p];
@@ -60,19 +71,19 @@ std::vector<std::vector<double>> factor_fronts(const Plan& P, const double* nzva
       int piv = k;
       double best = -1.0;
       for (int i = k; i < seg; ++i)
-        if (std::fabs(at(i, k)) > best) {
-          best = std::fabs(at(i, k));
+        if (magnitude(at(i, k)) > best) {
+          best = magnitude(at(i, k));
           piv = i;
         }
       if (piv != k)
         for (int j = 0; j < nf; ++j) std::swap(at(k, j), at(piv, j));
       ipiv[c1 + k] = piv;
-      const double d = at(k, k);
+      const T d = at(k, k);
       for (int i = k + 1; i < nf; ++i)
-        if (i >= seg || d != 0.0) at(i, k) /= d;
+        if (i >= seg || d != T(0)) at(i, k) /= d;
       for (int j = k + 1; j < nf; ++j) {
-        const double u = at(k, j);
-        if (u == 0.0) continue;
+        const T u = at(k, j);
+        if (u == T(0)) continue;
         for (int i = k + 1; i < nf; ++i) at(i, j) -= at(i, k) * u;
       }
     }
@@ -258,8 +269,10 @@ extern "C" int emu_check_launches(int64_t n, const int64_t* colptr, const int64_
 // Factor A (0-based CSC pattern, values) with symbolic_mf(A; q) (q 0-based
 // or null for AMD), merged fronts or one front per supernode.  stats: nnz_l,
 // nnz_u, fronts, original supernodes, max front, max pivots.
-extern "C" int emu_factor(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
-                          const int64_t* q, int merge, int64_t* stats) {
+namespace {
+template <typename T>
+void emulate(int64_t n, const int64_t* colptr, const int64_t* rowval, const T* nzval, const int64_t* q, int merge,
+             int64_t* stats, ResultT<T>& R) {
   const SymbolicMF S = symbolic_mf(n, colptr, rowval, q);
   Plan P;
   if (merge)
@@ -269,7 +282,7 @@ extern "C" int emu_factor(int64_t n, const int64_t* colptr, const int64_t* rowva
     build_plan(n, colptr, rowval, S.qf.data(), S.parent.data(), S.nsuper(), S.sstart.data(), S.upd_ptr.data(),
                S.upd_idx.data(), P);
   std::vector<int32_t> ipiv(n);
-  const std::vector<std::vector<double>> F = factor_fronts(P, nzval, ipiv);
+  const std::vector<std::vector<T>> F = factor_fronts(P, nzval, ipiv);
 
   std::vector<int32_t> prow(n), rowfac(n);
   for (int64_t x = 0; x < P.ns; ++x) {
@@ -280,18 +293,17 @@ extern "C" int emu_factor(int64_t n, const int64_t* colptr, const int64_t* rowva
     for (int a = 0; a < np; ++a) rowfac[prow[c1 + a]] = c1 + a;
   }
 
-  Result& R = g_result;
   R.lp.assign(P.lcolptr.begin(), P.lcolptr.end());
   R.up.assign(P.ucolptr.begin(), P.ucolptr.end());
   R.li.assign(P.nnz_l, -1);
-  R.lx.assign(P.nnz_l, NAN);
+  R.lx.assign(P.nnz_l, T(NAN));
   R.ui.assign(P.nnz_u, -1);
-  R.ux.assign(P.nnz_u, NAN);
-  auto put_l = [&](int64_t at, int64_t row, double v) {
+  R.ux.assign(P.nnz_u, T(NAN));
+  auto put_l = [&](int64_t at, int64_t row, T v) {
     R.li[at] = 1 + row;
     R.lx[at] = v;
   };
-  auto put_u = [&](int64_t at, int64_t row, double v) {
+  auto put_u = [&](int64_t at, int64_t row, T v) {
     R.ui[at] = 1 + row;
     R.ux[at] = v;
   };
@@ -299,13 +311,13 @@ extern "C" int emu_factor(int64_t n, const int64_t* colptr, const int64_t* rowva
     const int x = P.fc_super[fc];
     const int c = (int)(fc - P.colbase[x]);
     const int np = P.np[x], nf = P.nf[x], c1 = P.c1[x];
-    const double* col = F[x].data() + (size_t)c * nf;   // L column, or U12 rows 0..np-1
+    const T* col = F[x].data() + (size_t)c * nf;   // L column, or U12 rows 0..np-1
     if (P.merged) {
       if (c < np) {
         const int j = c1 + c, s = P.col_orig[j];
         const int a0 = P.o_c1[s] - c1, a1 = a0 + P.o_np[s];
         const int64_t lb = P.lcolptr[j];
-        for (int r = 0; r < a1 - c; ++r) put_l(lb + r, c1 + c + r, r == 0 ? 1.0 : col[c + r]);
+        for (int r = 0; r < a1 - c; ++r) put_l(lb + r, c1 + c + r, r == 0 ? T(1) : col[c + r]);
         const int64_t ob = P.o_upd_off[s], on = P.o_upd_off[s + 1] - ob, lu = lb + (a1 - c);
         for (int64_t i = 0; i < on; ++i) {
           const int u = P.o_upd[ob + i], rf = rowfac[u];
@@ -324,7 +336,7 @@ extern "C" int emu_factor(int64_t n, const int64_t* colptr, const int64_t* rowva
         const int64_t lb = P.lcolptr[c1 + c];
         for (int r = 0; r < nf - c; ++r) {
           const int fr = c + r;
-          put_l(lb + r, fr < np ? c1 + fr : rowfac[us[fr - np]], r == 0 ? 1.0 : col[fr]);
+          put_l(lb + r, fr < np ? c1 + fr : rowfac[us[fr - np]], r == 0 ? T(1) : col[fr]);
         }
         const int64_t ub = P.ucolptr[c1 + c + 1] - (c + 1);
         for (int b = 0; b <= c; ++b) put_u(ub + b, c1 + b, col[b]);
@@ -343,13 +355,44 @@ extern "C" int emu_factor(int64_t n, const int64_t* colptr, const int64_t* rowva
   const int64_t st[6] = {P.nnz_l, P.nnz_u, P.ns, P.merged ? P.ns_orig : P.ns, P.max_nf, P.max_np};
   std::memcpy(R.stats, st, sizeof st);
   std::memcpy(stats, st, sizeof st);
+}
+}  // namespace
+
+extern "C" int emu_factor(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+                          const int64_t* q, int merge, int64_t* stats) {
+  emulate<double>(n, colptr, rowval, nzval, q, merge, stats, g_result);
   return 0;
+}
+
+// The same for a ComplexF64 matrix, values as interleaved (re, im) doubles.
+extern "C" int emu_factor_c64(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval_ri,
+                              const int64_t* q, int merge, int64_t* stats) {
+  std::vector<cplx> z(colptr[n]);
+  for (int64_t k = 0; k < colptr[n]; ++k) z[k] = cplx(nzval_ri[2 * k], nzval_ri[2 * k + 1]);
+  emulate<cplx>(n, colptr, rowval, z.data(), q, merge, stats, g_result_c);
+  return 0;
+}
+
+// The last ComplexF64 factorization, 1-based, values as (re, im) pairs.
+extern "C" void emu_get_c64(int64_t* lp, int64_t* li, double* lx_ri, int64_t* up, int64_t* ui, double* ux_ri,
+                            int64_t* p, int64_t* q) {
+  const ResultT<cplx>& R = g_result_c;
+  for (size_t k = 0; k < R.lp.size(); ++k) {
+    lp[k] = R.lp[k] + 1;
+    up[k] = R.up[k] + 1;
+  }
+  std::memcpy(li, R.li.data(), R.li.size() * 8);
+  std::memcpy(ui, R.ui.data(), R.ui.size() * 8);
+  std::memcpy(lx_ri, R.lx.data(), R.lx.size() * 16);   // std::complex<double>: (re, im)
+  std::memcpy(ux_ri, R.ux.data(), R.ux.size() * 16);
+  std::memcpy(p, R.p.data(), R.p.size() * 8);
+  std::memcpy(q, R.q.data(), R.q.size() * 8);
 }
 
 // The last factorization, 1-based as the library returns it.
 extern "C" void emu_get(int64_t* lp, int64_t* li, double* lx, int64_t* up, int64_t* ui, double* ux, int64_t* p,
                         int64_t* q) {
-  const Result& R = g_result;
+  const ResultT<double>& R = g_result;
   for (size_t k = 0; k < R.lp.size(); ++k) {
     lp[k] = R.lp[k] + 1;
     up[k] = R.up[k] + 1;

@@ -10,13 +10,22 @@ of the Float64 path, and LAPACK's complex pivot rule (largest |re| + |im|,
 which differs from the largest modulus).  Matrices are seeded stand-ins with
 the reference tests' shapes and value distribution: sprand(ComplexF64, n, n,
 8/n) draws uniform [0, 1) real and imaginary parts, plus 5I.
+
+The last test runs the device algorithm on complex values through
+tests/plan_emulator.cpp (the library's own plan: merged fronts with the
+pivot search kept inside each original supernode, assembly and extend-add
+maps, CSC scatter) and checks it against the oracle's ComplexF64
+factorization: the plan and the pivot rule carry over to complex fronts.
 """
+
+import ctypes
 
 import numpy as np
 import pytest
 import scipy.sparse as sp
 import scipy.sparse.linalg as sla
 
+from helpers import column_value_errors
 from oracle import oracle as O
 from pureumfpack.sparse import SparseCSC
 
@@ -157,3 +166,44 @@ def test_refinement_and_many_right_hand_sides():
     for k in range(3):
         np.testing.assert_allclose(X0[:, k], O.solve_c64(F, B[:, k]), rtol=0, atol=0)
         assert rel_resid(S, X2[:, k], B[:, k]) <= max(rel_resid(S, X0[:, k], B[:, k]), 1e-15) * 1.5
+
+
+def _emulate_c64(emu, A, merge):
+    cp = np.ascontiguousarray(A.colptr - 1)
+    rv = np.ascontiguousarray(A.rowval - 1)
+    z = np.ascontiguousarray(A.nzval, dtype=np.complex128)
+    st = np.zeros(6, np.int64)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    emu.emu_factor_c64(ctypes.c_int64(A.n), P(cp), P(rv), P(z.view(np.float64)), None, ctypes.c_int(merge), P(st))
+    n, nl, nu = A.n, int(st[0]), int(st[1])
+    out = dict(Lcolptr=np.empty(n + 1, np.int64), Lrowval=np.empty(nl, np.int64), Lnzval=np.empty(nl, np.complex128),
+               Ucolptr=np.empty(n + 1, np.int64), Urowval=np.empty(nu, np.int64), Unzval=np.empty(nu, np.complex128),
+               p=np.empty(n, np.int64), q=np.empty(n, np.int64))
+    emu.emu_get_c64(P(out["Lcolptr"]), P(out["Lrowval"]), P(out["Lnzval"].view(np.float64)), P(out["Ucolptr"]),
+                    P(out["Urowval"]), P(out["Unzval"].view(np.float64)), P(out["p"]), P(out["q"]))
+    return out, dict(fronts=int(st[2]), nsuper=int(st[3]))
+
+
+EMU_CASES = [
+    ("hermitian-pattern-300", lambda: (lambda S: (S + S.conj().T).tocsc())(sprand_c(300, 8 / 300, seed=11)), 1e-12),
+    ("sprand-1200", lambda: sprand_c(1200, 6 / 1200, seed=3), 1e-12),
+    # small shift: most pivots leave the diagonal, merged pivot blocks span
+    # several supernodes
+    ("pivoting-1500", lambda: sprand_c(1500, 5 / 1500, seed=5, shift=0.5), 1e-8),
+]
+
+
+@pytest.mark.parametrize("merge", [1, 0])
+@pytest.mark.parametrize("name,make,rtol", EMU_CASES, ids=[c[0] for c in EMU_CASES])
+def test_device_algorithm_on_complex_fronts_matches_the_oracle(emu, name, make, rtol, merge):
+    A = O.ComplexCSC.from_scipy(make())
+    fo = O.multifrontal_lu_c64(A, check=False)
+    got, st = _emulate_c64(emu, A, merge)
+    assert st["fronts"] < st["nsuper"] if merge else st["fronts"] == st["nsuper"]
+    for key in ("Lcolptr", "Lrowval", "Ucolptr", "Urowval", "p", "q"):
+        np.testing.assert_array_equal(got[key], getattr(fo, key), err_msg=key)
+    nl, _ = column_value_errors(fo.Lcolptr, fo.Lnzval, got["Lnzval"])
+    nu, _ = column_value_errors(fo.Ucolptr, fo.Unzval, got["Unzval"])
+    assert max(nl, nu) <= rtol, (nl, nu)
+    if name.startswith("pivoting"):
+        assert np.count_nonzero(fo.p != fo.q) > A.n // 4   # the pivoting is real
