@@ -882,6 +882,15 @@ double element_growth(mfgpu_ctx* h) {
 int factor_dispatch(mfgpu_ctx* h, int32_t check) {
   h->refactored_fp64 = false;
   h->growth = 0.0;
+  if (h->plan.n == 0) {   // a 0 x 0 matrix: empty factors, nothing to launch
+    h->factored = h->csc_ready = true;
+    h->factor_precision = h->f32_values || h->precision == MFGPU_PRECISION_MIXED ? MFGPU_PRECISION_MIXED
+                                                                                 : MFGPU_PRECISION_FP64;
+    h->last_status = 0;
+    h->last_info.clear();
+    h->t_factor_ms = 0;
+    return MFGPU_OK;
+  }
   if (h->f32_values) return factor_impl<float>(h, check);   // Float32 matrix: FP32 factors, no refactor
   if (h->precision != MFGPU_PRECISION_MIXED) return factor_impl<double>(h, check);
   const int rc = factor_impl<float>(h, check);

@@ -126,3 +126,16 @@ def test_device_entry_points_check_pointers_and_leading_dimensions():
     torch.cuda.synchronize()
     assert lib.mfgpu_backward_error_device(h, k, d_b.data_ptr(), n, d_x.data_ptr(), n, ctypes.byref(out)) == 0
     assert out.value <= 1e-14
+
+
+def test_empty_matrix():
+    # a 0 x 0 matrix: empty factors and solutions, as the oracle gives them
+    from helpers import assert_same_structure
+    from pureumfpack import SparseCSC, multifrontal_lu, splu
+
+    A = SparseCSC(0, 0, np.array([1]), np.zeros(0, np.int64), np.zeros(0))
+    x = splu(A, method="multifrontal").ldiv(np.zeros(0))
+    assert x.shape == (0,)
+    G = multifrontal_lu(A)
+    fo = O.multifrontal_lu(A)
+    assert_same_structure(fo, G.L, G.U, G.p, G.q, G.pinv)
