@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
 #include <exception>
 #include <map>
 #include <numeric>
@@ -17,12 +18,23 @@ namespace mfgpu {
 namespace {
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Host threads for the plan's parallel loops: the hardware's, capped by the
+// environment variable MFGPU_HOST_THREADS when it holds a positive number.
+int64_t host_threads() {
+  int64_t nt = std::max(1u, std::thread::hardware_concurrency());
+  if (const char* e = std::getenv("MFGPU_HOST_THREADS")) {
+    const long v = std::strtol(e, nullptr, 10);
+    if (v > 0) nt = std::min<int64_t>(nt, v);
+  }
+  return nt;
+}
+
 // body(i) for i in [0, n) on the host's cores (independent iterations, each
 // writing its own outputs), handed out `grain` at a time; the first exception
 // is rethrown after the join.
 template <typename F>
 void parallel_range(int64_t n, F&& body, int64_t grain = 4096) {
-  const int64_t nt = std::min<int64_t>(std::max<int64_t>(1, n / grain), std::max(1u, std::thread::hardware_concurrency()));
+  const int64_t nt = std::min<int64_t>(std::max<int64_t>(1, n / grain), host_threads());
   if (nt <= 1) {
     for (int64_t i = 0; i < n; ++i) body(i);
     return;
@@ -57,7 +69,7 @@ std::vector<int64_t> tree_chunks(const std::vector<int32_t>& parent, const std::
   const int64_t ns = (int64_t)parent.size();
   int64_t total = ns;
   for (int32_t u : nu) total += u;
-  const int64_t nt = std::max(1u, std::thread::hardware_concurrency());
+  const int64_t nt = host_threads();
   const int64_t target = std::max<int64_t>(1, total / (16 * nt));
   std::vector<int64_t> b{0};
   int64_t acc = 0, reach = -1;

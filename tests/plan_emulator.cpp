@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cstring>
 #include <stdexcept>
+#include <string>
 #include <utility>
 #include <vector>
 
@@ -433,4 +434,78 @@ extern "C" int emu_build_plan(int64_t n, const int64_t* colptr, const int64_t* r
     say(e.what());
     return 2;
   }
+}
+
+namespace {
+uint64_t fnv(const void* p, size_t n, uint64_t h) {
+  const unsigned char* c = (const unsigned char*)p;
+  for (size_t i = 0; i < n; ++i) {
+    h ^= c[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+template <typename T>
+uint64_t hash_vec(const std::vector<T>& v) {   // element types without padding
+  return fnv(v.data(), v.size() * sizeof(T), 1469598103934665603ull ^ v.size());
+}
+uint64_t hash_gemms(const std::vector<GemmTask>& v) {   // field by field (GemmTask has padding)
+  uint64_t h = 1469598103934665603ull ^ v.size();
+  for (const GemmTask& g : v) {
+    const int64_t a[] = {g.a, g.b, g.c, g.m, g.n, g.k, g.lda, g.ldb, g.ldc, g.tiles_m, g.tiles_n, g.mode,
+                         g.tile_base, g.d, g.ldd, g.pad};
+    h = fnv(a, sizeof a, h);
+  }
+  return h;
+}
+uint64_t hash_launches(const std::vector<Launch>& v) {
+  uint64_t h = 1469598103934665603ull ^ v.size();
+  for (const Launch& l : v) {
+    const int64_t a[] = {l.kind, l.level, l.first, l.count, l.tiles, l.tiles_tc, l.rows};
+    const double d[] = {l.flops, l.elems, l.extra_bytes};
+    h = fnv(a, sizeof a, h);
+    h = fnv(d, sizeof d, h);
+  }
+  return h;
+}
+std::string g_digest;
+}  // namespace
+
+// A digest of every field of the plan built from a caller's symbolic arrays
+// (0-based), "name=hash;" per field: two plans are equal field by field when
+// their digests are.
+extern "C" const char* emu_plan_digest(int64_t n, const int64_t* colptr, const int64_t* rowval, const int64_t* qf,
+                                       const int64_t* parent, int64_t ns, const int64_t* sstart,
+                                       const int64_t* upd_ptr, const int64_t* upd_idx, int merge) {
+  Plan P;
+  if (merge)
+    build_plan_merged(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, P, kMergeMaxPivots);
+  else
+    build_plan(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, P);
+  std::string s;
+  auto put = [&](const char* name, uint64_t h) { s += std::string(name) + "=" + std::to_string(h) + ";"; };
+  auto num = [&](const char* name, double v) { put(name, fnv(&v, sizeof v, 0)); };
+#define VEC(f) put(#f, hash_vec(P.f))
+#define NUM(f) num(#f, (double)P.f)
+  NUM(n); NUM(ns); NUM(nnz_a); VEC(c1); VEC(np); VEC(nu); VEC(nf); VEC(height); VEC(slot); VEC(upd_off);
+  VEC(front_off); VEC(colbase); VEC(child_ptr); VEC(child_idx); VEC(parent_super); VEC(upd); VEC(rel); VEC(uoff);
+  VEC(v_src); VEC(v_srow); VEC(v_frow); VEC(fc_super); VEC(fc_vbeg); VEC(fc_vend); VEC(fc_ch_ptr); VEC(fc_ch);
+  NUM(fc_total); NUM(front_elems); NUM(front_elems_full); NUM(pool_elems); NUM(lean); VEC(lpan_off); VEC(u12_off);
+  NUM(panel_base); NUM(panel_elems); NUM(nlevels); VEC(slot_super); VEC(level_slot); VEC(level_large);
+  VEC(lcolptr); VEC(ucolptr); NUM(nnz_l); NUM(nnz_u); VEC(qf); VEC(csr_ptr); VEC(csr_col); VEC(csr_src);
+  VEC(dinv_off); NUM(dinv_blocks); VEC(inv_off); NUM(inv_base); NUM(inv_elems); NUM(inv_scratch);
+  NUM(inv_scratch_elems); VEC(inv_blocks); VEC(inv_steps); NUM(flops_inverse); VEC(small_tasks); VEC(panel_tasks);
+  VEC(trsm_tasks); NUM(has_speculative); NUM(merged); NUM(ns_orig); VEC(seg_end); VEC(col_orig); VEC(o_c1);
+  VEC(o_np); VEC(o_upd_off); VEC(o_upd); VEC(o_xpos); VEC(fcu_ptr); VEC(fcu); NUM(flops_orig); VEC(front_nv);
+  NUM(flops); NUM(flops_getrf); NUM(flops_trsm); NUM(flops_gemm); NUM(assembly_bytes_per_elem); NUM(max_nf);
+  NUM(max_np);
+#undef VEC
+#undef NUM
+  put("inv_tasks", hash_gemms(P.inv_tasks));
+  put("inv_tasks_tc", hash_gemms(P.inv_tasks_tc));
+  put("gemm_tasks", hash_gemms(P.gemm_tasks));
+  put("gemm_tasks_tc", hash_gemms(P.gemm_tasks_tc));
+  put("launches", hash_launches(P.launches));
+  g_digest = s;
+  return g_digest.c_str();
 }
