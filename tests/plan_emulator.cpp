@@ -478,10 +478,15 @@ extern "C" const char* emu_plan_digest(int64_t n, const int64_t* colptr, const i
                                        const int64_t* parent, int64_t ns, const int64_t* sstart,
                                        const int64_t* upd_ptr, const int64_t* upd_idx, int merge) {
   Plan P;
-  if (merge)
-    build_plan_merged(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, P, kMergeMaxPivots);
-  else
-    build_plan(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, P);
+  try {
+    if (merge)
+      build_plan_merged(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, P, kMergeMaxPivots);
+    else
+      build_plan(n, colptr, rowval, qf, parent, ns, sstart, upd_ptr, upd_idx, P);
+  } catch (const std::exception& e) {
+    g_digest = std::string("error=") + e.what() + ";";
+    return g_digest.c_str();
+  }
   std::string s;
   auto put = [&](const char* name, uint64_t h) { s += std::string(name) + "=" + std::to_string(h) + ";"; };
   auto num = [&](const char* name, double v) { put(name, fnv(&v, sizeof v, 0)); };

@@ -30,7 +30,10 @@ def digest(emu, A, S, merge):
 
 
 def batch(count):
-    As = [A for A, _ in M.batched_set(count, seed=0, nrhs=1)]
+    return block_diagonal([A for A, _ in M.batched_set(count, seed=0, nrhs=1)])
+
+
+def block_diagonal(As):
     offs = np.cumsum([0] + [A.n for A in As])
     nzo = np.cumsum([0] + [A.nnz() for A in As])
     cp = np.concatenate([[1]] + [A.colptr[1:] + z for A, z in zip(As, nzo[:-1])])
@@ -60,4 +63,64 @@ def test_parallel_plan_equals_the_sequential_one(emu, monkeypatch, name, make, m
     monkeypatch.delenv("MFGPU_HOST_THREADS")
     many = digest(emu, A, S, merge)
     assert len(one) >= 86   # every Plan field
+    assert one == many, [k for k in one if one[k] != many.get(k)]
+
+
+def interleave_pairs(A, S, sys_cols):
+    """The same factorization with the supernodes of systems 2i and 2i+1
+    interleaved: a topological order of the forest that is not a postorder
+    (each system keeps its own order; a pair's trees overlap)."""
+    ns = S.nsuper
+    sst = S.sstart - 1
+    sys_of = np.searchsorted(sys_cols, sst[:-1], side="right") - 1
+    order = []
+    for a in range(0, len(sys_cols) - 1, 2):
+        s1 = list(np.flatnonzero(sys_of == a))
+        s2 = list(np.flatnonzero(sys_of == a + 1))
+        while s1 or s2:
+            if s1:
+                order.append(s1.pop(0))
+            if s2:
+                order.append(s2.pop(0))
+    assert sorted(order) == list(range(ns)) and order != sorted(order)
+    newcol = np.empty(A.n, np.int64)
+    sstart, at = [0], 0
+    for s in order:
+        w = sst[s + 1] - sst[s]
+        newcol[sst[s]:sst[s + 1]] = np.arange(at, at + w)
+        at += w
+        sstart.append(at)
+    qf = np.empty(A.n, np.int64)
+    qf[newcol] = S.qf - 1
+    par0 = S.parent - 1
+    parent = np.full(A.n, -1, np.int64)
+    parent[newcol] = np.where(par0 >= 0, newcol[np.maximum(par0, 0)], -1)
+    upd_ptr, upd_idx = [0], []
+    for s in order:
+        u = newcol[S.upd_idx[S.upd_ptr[s] - 1:S.upd_ptr[s + 1] - 1] - 1]
+        assert np.all(np.diff(u) > 0)
+        upd_idx.extend(u.tolist())
+        upd_ptr.append(len(upd_idx))
+
+    class Sym:
+        pass
+
+    T = Sym()
+    T.qf, T.parent = qf + 1, parent + 1
+    T.sstart, T.upd_ptr = np.array(sstart) + 1, np.array(upd_ptr) + 1
+    T.upd_idx = np.array(upd_idx, np.int64) + 1
+    return T
+
+
+@pytest.mark.parametrize("merge", [1, 0])
+def test_interleaved_trees(emu, monkeypatch, merge):
+    As = [A for A, _ in M.batched_set(48, seed=1, nrhs=1)]
+    sys_cols = np.cumsum([0] + [A.n for A in As])
+    B, S = block_diagonal(As)
+    T = interleave_pairs(B, S, sys_cols)
+    monkeypatch.setenv("MFGPU_HOST_THREADS", "1")
+    one = digest(emu, B, T, merge)
+    monkeypatch.delenv("MFGPU_HOST_THREADS")
+    many = digest(emu, B, T, merge)
+    assert "error" not in one and len(one) >= 86, one
     assert one == many, [k for k in one if one[k] != many.get(k)]
