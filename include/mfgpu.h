@@ -64,6 +64,13 @@ int mfgpu_row_scaling(int64_t n, const int64_t* colptr, const int64_t* rowval, c
 int mfgpu_row_scaling_f32(int64_t n, const int64_t* colptr, const int64_t* rowval, const float* nzval,
                           int32_t kind, float* rs);
 
+/* row_scaling of a ComplexF64 matrix (src/scaling.jl:92-115 with
+ * R = real(Tv) = Float64): values as interleaved (re, im) doubles, Julia's
+ * ComplexF64 layout; |z| = hypot(re, im); Float64 Rs.  (The numeric phase
+ * has no ComplexF64 entry points yet.) */
+int mfgpu_row_scaling_c64(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval_ri,
+                          int32_t kind, double* rs);
+
 /* amd_order_sym(A; dense) (src/amd.jl:141-148): perm of 1:n. */
 int mfgpu_amd_order(int64_t n, const int64_t* colptr, const int64_t* rowval, double dense, int64_t* perm);
 

@@ -2,6 +2,7 @@
 // Index arrays crossing the ABI are 1-based int64 (SparseMatrixCSC{Float64,Int64}).
 
 #include <atomic>
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <string>
@@ -59,6 +60,21 @@ int mfgpu_row_scaling_f32(int64_t n, const int64_t* colptr, const int64_t* rowva
   std::vector<idx_t> ri(nz);
   for (int64_t p = 0; p < nz; ++p) ri[p] = rowval[p] - 1;
   mfgpu::row_scaling(n, nz, ri.data(), nzval, kind, rs);
+  return MFGPU_OK;
+}
+
+int mfgpu_row_scaling_c64(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval_ri,
+                          int32_t kind, double* rs) {
+  if (!valid_csc(n, n, colptr, rowval) || !rs || kind < 0 || kind > 2 || (colptr[n] > 1 && !nzval_ri))
+    return MFGPU_ERR_ARGUMENT;
+  const int64_t nz = colptr[n] - 1;
+  std::vector<idx_t> ri(nz);
+  std::vector<double> mag(nz);
+  for (int64_t p = 0; p < nz; ++p) {
+    ri[p] = rowval[p] - 1;
+    mag[p] = std::hypot(nzval_ri[2 * p], nzval_ri[2 * p + 1]);   // abs(::ComplexF64)
+  }
+  mfgpu::row_scaling(n, nz, ri.data(), mag.data(), kind, rs);
   return MFGPU_OK;
 }
 

@@ -25,6 +25,7 @@ cp = ctypes.c_char_p
 SIGNATURES = [
     ("mfgpu_row_scaling", ctypes.c_int, [i64, i64p, i64p, f64p, i32, f64p]),
     ("mfgpu_row_scaling_f32", ctypes.c_int, [i64, i64p, i64p, f32p, i32, f32p]),
+    ("mfgpu_row_scaling_c64", ctypes.c_int, [i64, i64p, i64p, f64p, i32, f64p]),
     ("mfgpu_amd_order", ctypes.c_int, [i64, i64p, i64p, f64, i64p]),
     ("mfgpu_colamd_order", ctypes.c_int, [i64, i64, i64p, i64p, f64, i64p]),
     ("mfgpu_symbolic_create", ctypes.c_int, [i64, i64p, i64p, i64p, ctypes.POINTER(vp)]),

@@ -207,3 +207,19 @@ def test_device_algorithm_on_complex_fronts_matches_the_oracle(emu, name, make, 
     assert max(nl, nu) <= rtol, (nl, nu)
     if name.startswith("pivoting"):
         assert np.count_nonzero(fo.p != fo.q) > A.n // 4   # the pivoting is real
+
+
+@pytest.mark.parametrize("kind", [O.SCALE_NONE, O.SCALE_SUM, O.SCALE_MAX])
+def test_library_row_scaling_c64_is_the_oracles(kind):
+    # mfgpu_row_scaling_c64 (host code of libmfgpu) against the oracle: bitwise
+    from pureumfpack import _lib
+
+    L = _lib.lib()
+    S = sprand_c(500, 8 / 500, seed=71)
+    A = O.ComplexCSC.from_scipy(S)
+    rs = np.empty(A.n)
+    z = np.ascontiguousarray(A.nzval, dtype=np.complex128)
+    rc = L.mfgpu_row_scaling_c64(A.n, _lib.ptr(np.ascontiguousarray(A.colptr)), _lib.ptr(np.ascontiguousarray(A.rowval)),
+                                 _lib.ptr(z.view(np.float64), _lib.f64p), kind, _lib.ptr(rs, _lib.f64p))
+    assert rc == 0
+    np.testing.assert_array_equal(rs, O.row_scaling_c64(A, kind))
