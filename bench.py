@@ -49,6 +49,7 @@ sys.path[:0] = [ROOT, os.path.join(ROOT, "pureumfpack.jl_b200")]
 TARGET_ETA = 1e-14
 CPU_FRONT_LIMIT = 2e10    # front elements beyond which the CPU oracle baseline is not run
 MAX_REFINE = 8
+REF_TIMED_STEPS = 3       # timed oracle steps of the reference arm (each is a full CPU factorization)
 
 
 def parse():
@@ -62,6 +63,8 @@ def parse():
     ap.add_argument("--forms", default="fp64,mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the untimed comparison of the GPU factors with the oracle's (and mixed with FP64)")
     ap.add_argument("--solve-mode", default="auto", choices=["auto", "step", "persistent"],
                     help="solve launches: library default by rhs count, per step, or one persistent launch per pass")
     ap.add_argument("--relax", action="store_true",
@@ -191,14 +194,27 @@ def fp_peak_tflops(torch, dtype, device) -> float:
 
 
 # ---------------------------------------------------------------------------
-def cpu_baseline(A, B, refine: int, sample_rhs: int = 4, order: str = "amd", scale: int = 1):
-    """The oracle (C++ restatement of the reference over OpenBLAS, all host
-    threads): symbolic + numeric multifrontal_lu of the full matrix, then
-    solve(F, b; refine) for `sample_rhs` right-hand sides, scaled to the full
-    RHS count.  Returns (seconds per step, details)."""
+def _oracle_eta(A, X, B):
+    """Largest normwise backward error over the columns (host, FP64)."""
+    S = A.to_scipy()
+    r = B - S @ X
+    anorm = np.max(np.asarray(abs(S).sum(axis=1)).ravel())
+    return float(np.max(np.abs(r).max(axis=0) / (anorm * np.abs(X).max(axis=0) + np.abs(B).max(axis=0))))
+
+
+def cpu_baseline(A, B, sample_rhs: int = 4, order: str = "amd", scale: int = 1, threads: int = 0,
+                 refine: int | None = None, keep_factors: bool = False):
+    """The oracle (C++ restatement of the reference over OpenBLAS): symbolic +
+    numeric multifrontal_lu of the full matrix, then solve(F, b; refine) for
+    `sample_rhs` right-hand sides, scaled to the full RHS count.  `refine`
+    None: the fewest refinements that bring the sampled right-hand sides to
+    backward error <= TARGET_ETA, the oracle's own need (the same rule the GPU
+    forms follow); only the solve with that count is timed.  threads 0: all
+    host cores for BLAS.  Returns (seconds per step, details, oracle factors
+    or None)."""
     from oracle import oracle as O
 
-    cores = os.cpu_count() or 1
+    cores = threads or (os.cpu_count() or 1)
     O.blas_threads(cores)
     t0 = time.perf_counter()
     S = O.symbolic_mf(A, q=O.colamd_order(A) if order == "colamd" else None)
@@ -210,37 +226,57 @@ def cpu_baseline(A, B, refine: int, sample_rhs: int = 4, order: str = "amd", sca
     F = O.PureLU(Fo, Rs, A)
     nrhs = B.shape[1]
     k = min(sample_rhs, nrhs)
+    Bk = np.asfortranarray(B[:, :k])
+    etas = []
+    if refine is None:
+        for refine in range(MAX_REFINE + 1):
+            etas.append(_oracle_eta(A, O.solve(F, Bk, refine=refine), Bk))
+            if etas[-1] <= TARGET_ETA:
+                break
     t3 = time.perf_counter()
-    O.solve(F, np.asfortranarray(B[:, :k]), refine=refine)
+    X = O.solve(F, Bk, refine=refine)
     t4 = time.perf_counter()
     numeric = t2 - t1
     solve_full = (t4 - t3) * nrhs / k
     return numeric + solve_full, {
         "symbolic_s": t1 - t0, "numeric_s": numeric, "solve_s_per_rhs": (t4 - t3) / k, "cores": cores,
-        "sample": f"full {A.n}-unknown numeric factorization (OpenBLAS, {cores} threads) + solve(refine={refine}) "
-                  f"of {k} of {nrhs} right-hand sides, scaled x{nrhs / k:g}; symbolic phase reported separately",
-    }
+        "refine": refine, "bwd_err": _oracle_eta(A, X, Bk), "bwd_err_by_refine": etas or None,
+        "sample": f"full {A.n}-unknown numeric factorization (OpenBLAS, {cores} threads) + solve(refine={refine}, "
+                  f"the oracle's fewest refinements to backward error <= {TARGET_ETA:g}) of {k} of {nrhs} "
+                  f"right-hand sides, scaled x{nrhs / k:g}; symbolic phase reported separately",
+    }, (Fo if keep_factors else None)
 
 
 def run_reference(args):
+    """The reference's CPU path on the host cores: the oracle, all host
+    threads, on this arm's workload.  Each timed step is one full numeric
+    factorization plus the sampled solve (about 15-20 s at poisson3d-64), so
+    at most REF_TIMED_STEPS of the requested steps are timed; one extra
+    untimed run measures the same step with one BLAS thread."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     A, B = make_workload(args.workload, args.nrhs)
-    times, det = [], None
     order, scale = workload_setup(args.workload)
-    for i in range(max(1, min(args.warmup, 1)) + args.steps):
-        t, det = cpu_baseline(A, B, refine=1, order=order, scale=scale)
-        if i >= max(1, min(args.warmup, 1)):
-            times.append(t)
+    _, det0, _ = cpu_baseline(A, B, order=order, scale=scale)        # warm-up; fixes the refine count
+    refine = det0["refine"]
+    times, det = [], None
+    timed = max(1, min(args.steps, REF_TIMED_STEPS))
+    for _ in range(timed):
+        t, det, _ = cpu_baseline(A, B, order=order, scale=scale, refine=refine)
+        times.append(t)
     v = float(np.mean(times))
+    t1, det1, _ = cpu_baseline(A, B, order=order, scale=scale, refine=refine, threads=1)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(args, A),
         "cpu_baseline": {"value": v, "unit": "s", "cores": det["cores"], "kind": "port", "sample": det["sample"],
-                         "symbolic_s": det["symbolic_s"]},
+                         "symbolic_s": det["symbolic_s"], "numeric_s": det["numeric_s"], "refine": refine,
+                         "bwd_err": det["bwd_err"], "timed_steps": timed,
+                         "threads_1": {"value": t1, "unit": "s", "cores": 1, "numeric_s": det1["numeric_s"],
+                                       "sample": det1["sample"]}},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -317,7 +353,17 @@ def autotune_mixed(ctx, run, R, device):
             "tensor_core_launches": int(np.sum(choice == 1))}
 
 
-def roofline_of(P, primary, torch, dev, peaks):
+def bx3_peak(peaks):
+    """Useful FP32 TFLOP/s ceiling of the BF16x3 tensor-core GEMMs: six bf16
+    products per useful product on the sustained bf16 rate."""
+    if "bf16_tflops_sustained" in peaks:
+        return peaks["bf16_tflops_sustained"] / 6.0, ("MEASURED_PEAKS.json bf16_tflops_sustained / 6 (of measured): "
+                                                       "BF16x3 issues six BF16 tensor-core products per useful "
+                                                       "FP32 product")
+    return 1400.0 / 6.0, "fallback sustained bf16 1.4 PFLOP/s / 6 (BF16x3: six bf16 products per useful product)"
+
+
+def roofline_of(P, primary, fp64_peak, peaks):
     """Roofline entry for the dominant kernel class of one profiled step."""
     kern = P["stats"]["kernels"]
     dom = max(kern, key=lambda k: kern[k]["ms"])
@@ -325,18 +371,9 @@ def roofline_of(P, primary, torch, dev, peaks):
     per_launch_ms = kd["ms"] / max(kd["launches"], 1)
     if dom.startswith("gemm"):
         if primary == "fp64":
-            peak = fp_peak_tflops(torch, torch.float64, dev)
-            peak_src = "in-run cuBLAS DGEMM 8192^3 (FP64 peak is not in MEASURED_PEAKS.json)"
-        elif "bf16_tflops_sustained" in peaks:
-            # FP32 fronts: the large updates run as BF16x3 tcgen05 products
-            # (each operand split into three bf16 parts; six bf16 products
-            # per useful FP32 product)
-            peak = peaks["bf16_tflops_sustained"] / 6.0
-            peak_src = ("MEASURED_PEAKS.json bf16_tflops_sustained / 6 (of measured): BF16x3 issues six BF16 "
-                        "tensor-core products per useful FP32 product")
+            peak, peak_src = fp64_peak, "in-run cuBLAS DGEMM 8192^3 (FP64 peak is not in MEASURED_PEAKS.json)"
         else:
-            peak = 1400.0 / 6.0
-            peak_src = "fallback sustained bf16 1.4 PFLOP/s / 6 (BF16x3: six bf16 products per useful product)"
+            peak, peak_src = bx3_peak(peaks)
         achieved = kd["flops"] / (kd["ms"] * 1e-3) / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak,
                 "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": peak_src}
@@ -346,12 +383,11 @@ def roofline_of(P, primary, torch, dev, peaks):
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback"}
     traffic, tnote = None, None
-    ratio = gemm_traffic_ratio()
-    if dom == "gemm_factor" and primary == "fp64" and ratio is not None:
-        traffic = ratio * kd["bytes"] / max(kd["launches"], 1)
-        tnote = ("DRAM bytes per launch: ncu dram__bytes_read+write of the factor updates at poisson3d-48 over their "
-                 f"algorithmic bytes ({ratio:.3f}, profiles/k_gemm_f64_poisson3d-48.md) x this class's algorithmic "
-                 "bytes per launch")
+    ratio = NCU_TRAFFIC_RATIO.get((dom, primary))
+    if ratio is not None:
+        traffic = ratio[0] * kd["bytes"] / max(kd["launches"], 1)
+        tnote = (f"DRAM bytes per launch: ncu dram__bytes_read+write over algorithmic bytes ({ratio[0]:.3f}, "
+                 f"{ratio[1]}) x this class's algorithmic bytes per launch")
     roof.update({"kernel": dom, "launches": kd["launches"], "avg_launch_ms": per_launch_ms,
                  "traffic": traffic, "algorithmic_bytes_per_launch": kd["bytes"] / max(kd["launches"], 1),
                  "note": "achieved = algorithmic work of the kernel class / its CUDA-event time over one profiled step"
@@ -359,16 +395,98 @@ def roofline_of(P, primary, torch, dev, peaks):
     return roof
 
 
-def gemm_traffic_ratio():
-    """DRAM traffic over algorithmic bytes of the FP64 factor updates, from the
-    committed ncu summary (None if absent)."""
-    try:
-        for line in open(os.path.join(ROOT, "profiles", "k_gemm_f64_poisson3d-48.md")):
-            if line.startswith("traffic_ratio"):
-                return float(line.split()[1])
-    except OSError:
-        pass
-    return None
+SOLVE_CLASSES = ("fwd_small", "fwd_assemble", "gemm_solve", "bwd_small", "bwd_gather", "solve_finish")
+
+
+def class_rooflines(f, form, fp64_peak, peaks, nrhs):
+    """Per-class roofline entries of one form's profiled step: the factor
+    GEMMs against the tensor peak of their precision, assembly and the CSC
+    scatter against HBM bandwidth, and one solve pass (forward + backward
+    over the resident fronts) both in GB/s and in TFLOP/s.  A solve pass's
+    algorithmic work: flops 2 (nnz(L) + nnz(U)) nrhs; bytes: the factor values
+    read once plus the right-hand side, solution and factor-order copy
+    (es (nnz(L) + nnz(U)) + 24 n nrhs)."""
+    st = f["stats"]
+    kern = st["kernels"]
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    es = 8 if form == "fp64" else 4
+    tpeak, tsrc = (fp64_peak, "in-run cuBLAS DGEMM") if form == "fp64" else bx3_peak(peaks)
+    out = {}
+    if "gemm_factor" in kern:
+        k = kern["gemm_factor"]
+        a = k["flops"] / (k["ms"] * 1e-3) / 1e12
+        out["gemm_factor"] = {"bound": "tensor", "achieved": a, "peak": tpeak, "unit": "TFLOP/s", "frac": a / tpeak,
+                              "ms": k["ms"], "launches": k["launches"], "peak_source": tsrc}
+    for name in ("assemble_columns", "scatter_csc"):
+        if name in kern and kern[name]["bytes"] > 0:
+            k = kern[name]
+            a = k["bytes"] / (k["ms"] * 1e-3) / 1e9
+            out[name] = {"bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s", "frac": a / hbm, "ms": k["ms"],
+                         "launches": k["launches"], "algorithmic_bytes": k["bytes"]}
+    passes = f["refine"] + 1
+    ms = sum(kern[c]["ms"] for c in SOLVE_CLASSES if c in kern) / passes
+    if ms > 0:
+        nnz = float(st["nnz_l"] + st["nnz_u"])
+        flops = 2.0 * nnz * nrhs
+        by = es * nnz + 24.0 * st["n"] * nrhs
+        gbs = by / (ms * 1e-3) / 1e9
+        tfs = flops / (ms * 1e-3) / 1e12
+        out["solve_pass"] = {"ms": ms, "passes": passes, "GB/s": gbs, "hbm_frac": gbs / hbm, "TFLOP/s": tfs,
+                             "tensor_frac": tfs / tpeak, "algorithmic_bytes": by, "flops": flops,
+                             "bound": "tensor" if flops / by > tpeak * 1e3 / hbm else "hbm"}
+    return out
+
+
+def _colwise(colptr, ref, got):
+    """(max over columns of ||got - ref|| / ||ref||, max entry-wise relative
+    error over entries with |ref| > 1e-6 max|column|) for CSC values."""
+    ref = np.asarray(ref, dtype=np.float64)
+    got = np.asarray(got, dtype=np.float64)
+    cnt = np.diff(np.asarray(colptr, np.int64))
+    if ref.size == 0:
+        return 0.0, 0.0
+    starts = np.asarray(colptr, np.int64)[:-1][cnt > 0] - 1
+    aref = np.abs(ref)
+    d = np.abs(got - ref)
+    colmax = np.maximum.reduceat(aref, starts)
+    c2 = np.add.reduceat(aref * aref, starts)
+    e2 = np.add.reduceat(d * d, starts)
+    nz = c2 > 0
+    big = aref > np.repeat(1e-6 * colmax, cnt[cnt > 0])
+    return (float(np.max(np.sqrt(e2[nz] / c2[nz]))) if nz.any() else 0.0,
+            float(np.max(d[big] / aref[big])) if big.any() else 0.0)
+
+
+def factor_parity(ref, got):
+    """Structure and values of factors `got` against `ref` (dicts of 1-based
+    CSC arrays Lcolptr, Lrowval, Lnzval, Ucolptr, Urowval, Unzval, p, q,
+    pinv): fill, patterns and pivots bit-equal, values per column."""
+    eq = lambda k: bool(np.array_equal(ref[k], got[k]))  # noqa: E731
+    fill = int(ref["Lcolptr"][-1] - 1 + ref["Ucolptr"][-1] - 1)
+    out = {"fill": fill, "fill_equal": fill == int(got["Lcolptr"][-1] - 1 + got["Ucolptr"][-1] - 1),
+           "pattern_equal": all(eq(k) for k in ("Lcolptr", "Lrowval", "Ucolptr", "Urowval")),
+           "pivots_equal": all(eq(k) for k in ("p", "q", "pinv"))}
+    if out["pattern_equal"]:
+        ln, le = _colwise(ref["Lcolptr"], ref["Lnzval"], got["Lnzval"])
+        un, ue = _colwise(ref["Ucolptr"], ref["Unzval"], got["Unzval"])
+        out.update({"max_colwise": max(ln, un), "max_entrywise": max(le, ue)})
+    return out
+
+
+def gpu_factors(ctx):
+    L, U, p, q, pinv = ctx.factors()
+    return {"Lcolptr": L.colptr, "Lrowval": L.rowval, "Lnzval": L.nzval, "Ucolptr": U.colptr, "Urowval": U.rowval,
+            "Unzval": U.nzval, "p": p, "q": q, "pinv": pinv}
+
+
+# DRAM traffic over algorithmic bytes per kernel class, from ncu captures of
+# a few launches on smaller cases (dram__bytes_read.sum + dram__bytes_write.sum
+# over the class's algorithmic bytes of the same launches); scaled to this
+# run's launches by their algorithmic bytes.  The captures' commands and
+# figures are summarised under profiles/.
+NCU_TRAFFIC_RATIO = {
+    ("gemm_factor", "fp64"): (0.743, "k_gemm_f64 factor updates, poisson3d-48"),
+}
 
 
 def run_f32(args):
@@ -492,6 +610,7 @@ def main():
     d_x = torch.empty(n * R, dtype=torch.float64, device=dev)
 
     forms = {}
+    kept, par_mixed = {}, None
     peaks = measured_peaks()
     for form in [f for f in args.forms.split(",") if f]:
         prec = PRECISION_MIXED if form == "mixed" else PRECISION_FP64
@@ -588,6 +707,16 @@ def main():
         forms[form] = {"ms_per_step": ms, "refine": refine, "eta": eta, "analyze_s": t_an + t_sym,
                        "stats": st, "clocks": clk, "launches_timed": launches, "e2e": e2e, "etas": etas,
                        "autotune": tune}
+        # parity (untimed): the FP64 form's factors are kept for the oracle
+        # comparison; the mixed form's structure and values are compared with
+        # the FP64 form's at once
+        if world == 1 and not args.no_parity:
+            fac = gpu_factors(ctx)
+            if form == "fp64":
+                kept["fp64"] = fac
+            elif "fp64" in kept:
+                par_mixed = factor_parity(kept["fp64"], fac)
+            del fac
         del ctx
         torch.cuda.empty_cache()
 
@@ -600,9 +729,13 @@ def main():
     ok = [k for k, f in forms.items() if f["eta"] is not None and f["eta"] <= TARGET_ETA]
     primary = min(ok or list(forms), key=lambda k: forms[k]["ms_per_step"])
     P = forms[primary]
-    roof = roofline_of(P, primary, torch, dev, peaks)
+    fp64_peak = fp_peak_tflops(torch, torch.float64, dev)
+    roof = roofline_of(P, primary, fp64_peak, peaks)
+    classes = {k: class_rooflines(f, k, fp64_peak, peaks, R) for k, f in forms.items()}
 
-    cpu = None
+    cpu, parity = None, {}
+    if par_mixed is not None:
+        parity["mixed_vs_fp64"] = par_mixed
     # the oracle factors one front per supernode of the reference's structure
     # (no merged fronts): sum of (np + nu)^2 over the original supernodes
     npv, nuv = np.diff(S.sstart).astype(np.float64), np.diff(S.upd_ptr).astype(np.float64)
@@ -614,11 +747,18 @@ def main():
     elif not args.no_cpu_baseline and world == 1:
         try:
             order, scale = workload_setup(args.workload)
-            v, det = cpu_baseline(A, B, refine=forms.get("fp64", P)["refine"], order=order, scale=scale)
+            v, det, Fo = cpu_baseline(A, B, order=order, scale=scale, keep_factors="fp64" in kept)
             cpu = {"value": v, "unit": "s", "cores": det["cores"], "kind": "port", "sample": det["sample"],
-                   "symbolic_s": det["symbolic_s"], "numeric_s": det["numeric_s"]}
+                   "symbolic_s": det["symbolic_s"], "numeric_s": det["numeric_s"], "refine": det["refine"],
+                   "bwd_err": det["bwd_err"]}
+            if Fo is not None:
+                ref = {k: getattr(Fo, k) for k in ("Lcolptr", "Lrowval", "Lnzval", "Ucolptr", "Urowval", "Unzval",
+                                                    "p", "q", "pinv")}
+                parity["fp64_vs_oracle"] = factor_parity(ref, kept.pop("fp64"))
+                del ref, Fo
         except Exception as e:  # the baseline must not kill the GPU number
             cpu = {"value": None, "error": str(e)}
+    kept.clear()
 
     value = P["ms_per_step"] / 1e3 / world
     line = {
@@ -634,6 +774,8 @@ def main():
                       **({"autotune": f["autotune"]} if f.get("autotune") else {})}
                   for k, f in forms.items()},
         "roofline": roof,
+        "roofline_classes": classes,
+        "parity": parity or None,
         "cpu_baseline": cpu,
         "e2e": P["e2e"],
         "gpu_launches": P["launches_timed"],
@@ -698,7 +840,7 @@ def run_batch(args):
     if args.impl == "reference":
         if rank != 0:
             return 0
-        v, det = batch_cpu_baseline(sysl, costs, refine=1)
+        v, det = batch_cpu_baseline(sysl, costs)
         line = {"impl": "reference", "metric": BATCH_METRIC.format(count), "value": v, "unit": "s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
                 "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
@@ -815,11 +957,13 @@ def run_batch(args):
     ok = [k for k, f in forms.items() if f["eta"] is not None and f["eta"] <= TARGET_ETA]
     primary = min(ok or list(forms), key=lambda k: forms[k]["ms_per_step"])
     P = forms[primary]
-    roof = roofline_of(P, primary, torch, dev, peaks)
+    fp64_peak = fp_peak_tflops(torch, torch.float64, dev)
+    roof = roofline_of(P, primary, fp64_peak, peaks)
+    classes = {k: class_rooflines(f, k, fp64_peak, peaks, R) for k, f in forms.items()}
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         try:
-            v, det = batch_cpu_baseline(sysl, costs, refine=forms.get("fp64", P)["refine"])
+            v, det = batch_cpu_baseline(sysl, costs)
             cpu = {"value": v, "unit": "s", "kind": "port", **det}
         except Exception as e:
             cpu = {"value": None, "error": str(e)}
@@ -833,7 +977,8 @@ def run_batch(args):
                       "analyze_s": f["analyze_s"], "e2e_s": f["e2e"]["value"] if f["e2e"] else None,
                       "kernels_ms": {kk: round(vv["ms"], 3) for kk, vv in f["stats"]["kernels"].items()}}
                   for k, f in forms.items()},
-        "roofline": roof, "cpu_baseline": cpu, "e2e": P["e2e"], "gpu_launches": P["launches_timed"],
+        "roofline": roof, "roofline_classes": classes, "cpu_baseline": cpu, "e2e": P["e2e"],
+        "gpu_launches": P["launches_timed"],
         "clocks": P["clocks"], "predicted_gflop": flops_total / 1e9, "cost_model_s": t_cost,
         "stats": {k: P["stats"].get(k) for k in ("n", "nsuper", "levels", "nnz_l", "nnz_u", "max_front", "flops",
                                                  "front_elems", "front_elems_full", "pool_elems", "lean",
@@ -845,15 +990,29 @@ def run_batch(args):
     return 0
 
 
-def batch_cpu_baseline(sysl, costs, refine: int, stride: int = 16):
+def batch_cpu_baseline(sysl, costs, refine: int | None = None, stride: int = 16):
     """The oracle on every `stride`-th system of the batch (numeric factor +
     solve(refine) of its 4 right-hand sides, all host threads for BLAS),
-    scaled to the whole batch by predicted flops."""
+    scaled to the whole batch by predicted flops.  `refine` None: the fewest
+    refinements that bring every sampled system to backward error <=
+    TARGET_ETA (untimed search), then the timed pass with that count."""
     from oracle import oracle as O
 
     cores = os.cpu_count() or 1
     O.blas_threads(cores)
     idx = list(range(0, len(sysl), stride))
+    facs = []
+    for i in idx:
+        A, B = sysl[i]
+        Rs = O.row_scaling(A, O.SCALE_SUM)
+        facs.append(O.PureLU(O.numeric(O.symbolic_mf(A), O.apply_row_scaling(A, Rs), check=False), Rs, A))
+    if refine is None:
+        for refine in range(MAX_REFINE + 1):
+            worst = max(_oracle_eta(sysl[i][0], O.solve(F, sysl[i][1], refine=refine), sysl[i][1])
+                        for i, F in zip(idx, facs))
+            if worst <= TARGET_ETA:
+                break
+    del facs
     t = 0.0
     for i in idx:
         A, B = sysl[i]
@@ -864,10 +1023,11 @@ def batch_cpu_baseline(sysl, costs, refine: int, stride: int = 16):
         O.solve(O.PureLU(Fo, Rs, A), B, refine=refine)
         t += time.perf_counter() - t0
     scale = float(sum(costs)) / float(sum(costs[i] for i in idx))
-    return t * scale, {"cores": cores,
+    return t * scale, {"cores": cores, "refine": refine,
                        "sample": f"{len(idx)} of {len(sysl)} systems (every {stride}th): numeric factor + "
-                                 f"solve(refine={refine}) of 4 rhs, symbolic excluded; scaled x{scale:.2f} by "
-                                 f"predicted flops"}
+                                 f"solve(refine={refine}, the oracle's fewest refinements to backward error <= "
+                                 f"{TARGET_ETA:g}) of 4 rhs, symbolic excluded; scaled x{scale:.2f} by predicted "
+                                 f"flops"}
 
 
 if __name__ == "__main__":

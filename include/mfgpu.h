@@ -155,6 +155,14 @@ int mfgpu_set_precision(mfgpu_ctx* h, int32_t precision);
  * "growth" and "refactored_fp64").  No counterpart in the reference, which
  * factors in the input precision only. */
 int mfgpu_set_growth_limit(mfgpu_ctx* h, double limit);
+/* Bound (seconds, > 0 and <= 3600; default 4) on every device-side wait of
+ * this handle's kernels: the tensor-core GEMMs' mbarrier waits and the
+ * persistent solve's grid barriers.  A wait that runs out ends its kernel
+ * cleanly (issued tensor-core work drained, tensor memory freed) and the call
+ * returns MFGPU_ERR_TIMEOUT; the handle stays usable (a factorization that
+ * timed out leaves no factors: factor again).  The reference's counterpart is
+ * a status, not a trap (src/multifrontal.jl:250-252). */
+int mfgpu_set_wait_limit(mfgpu_ctx* h, double seconds);
 
 /* Pattern analysis for the numeric phase, from the reference's own symbolic
  * result: A's pattern (colptr, rowval, n x n), SymbolicMF.qf, .parent,
@@ -224,7 +232,9 @@ int mfgpu_get_factors_f32(mfgpu_ctx* h, int64_t* lcolptr, int64_t* lrowval, floa
 int mfgpu_solve_f32(mfgpu_ctx* h, int64_t nrhs, const float* b, float* x, int32_t refine);
 
 /* Normwise backward error max_k ||b_k - A x_k||_inf / (||A||_inf ||x_k||_inf + ||b_k||_inf)
- * of device arrays, computed in FP64 on the GPU with the analyzed pattern. */
+ * of device arrays, computed in FP64 on the GPU with the analyzed pattern.
+ * A NaN or Inf in x, b or A's values (or an overflow of the denominator)
+ * gives NaN, so a broken solution never passes an accuracy check. */
 int mfgpu_backward_error_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ldb, const double* d_x,
                                 int64_t ldx, double* out);
 
@@ -238,7 +248,12 @@ int mfgpu_backward_error_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, i
  * process exits), shared by all calls and all handles of a device.
  *   - nrhs must be 1..4096; larger counts return MFGPU_ERR_ARGUMENT.
  *   - The first call on a device looks up that array's device address; make
- *     that first call before any stream capture.
+ *     that first call before any stream capture.  The address is kept for the
+ *     life of the process, so a cudaDeviceReset after that first call is not
+ *     supported (the array's memory is gone and later calls would use a
+ *     stale address).
+ *   - A 0 x 0 system gives 0; non-finite inputs give NaN, as
+ *     mfgpu_backward_error_device.
  *   - The array keeps the last call's contents; each call clears it first.
  *     Calls whose GPU work overlaps (other streams, other handles on the same
  *     device, other host threads) race on it: serialise them.

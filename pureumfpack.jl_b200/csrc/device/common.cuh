@@ -68,6 +68,12 @@ struct DevState {
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 __device__ __forceinline__ int warp_id() { return threadIdx.x >> 5; }
 
+// Maximum that keeps a NaN (fmax drops it): a reduction over magnitudes
+// reports a NaN anywhere in its input.  The arguments are magnitudes (fabs
+// clears the sign), so a NaN result is a positive NaN, whose bit pattern
+// orders above +Inf's: atomicMax on the bits keeps it too.
+__device__ __forceinline__ double max_keep_nan(double a, double b) { return (a != a || b != b) ? a + b : fmax(a, b); }
+
 // (|value|, index) argmax with LAPACK idamax tie-breaking: the first (lowest)
 // index among equal magnitudes wins.
 struct ArgMax {

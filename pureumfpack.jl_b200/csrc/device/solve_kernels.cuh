@@ -378,7 +378,8 @@ __global__ void k_residual(int64_t n, int64_t nrhs, const int32_t* __restrict__ 
 // Per-column maxima of |r|, |x|, |b| for the normwise backward error: a
 // 256-row slice of one column per CTA (grid: row slices x columns), reduced
 // in the CTA, then one atomic per quantity and CTA.  Non-negative doubles
-// order like their bit patterns, so the maxima are atomicMax on the bits.
+// order like their bit patterns, so the maxima are atomicMax on the bits; a
+// NaN anywhere in a column is kept (max_keep_nan) and makes its maximum NaN.
 __global__ void __launch_bounds__(256) k_bwd_error_parts(int64_t n, int64_t nrhs, const double* __restrict__ r,
                                                          int64_t ldr, const double* __restrict__ x, int64_t ldx,
                                                          const double* __restrict__ b, int64_t ldb,
@@ -394,13 +395,13 @@ __global__ void __launch_bounds__(256) k_bwd_error_parts(int64_t n, int64_t nrhs
     }
 #pragma unroll
     for (int q = 0; q < 3; ++q)
-      for (int o = 16; o > 0; o >>= 1) v[q] = fmax(v[q], __shfl_xor_sync(0xffffffffu, v[q], o));
+      for (int o = 16; o > 0; o >>= 1) v[q] = max_keep_nan(v[q], __shfl_xor_sync(0xffffffffu, v[q], o));
     if (lane_id() == 0)
       for (int q = 0; q < 3; ++q) red[q][warp_id()] = v[q];
     __syncthreads();
     if (threadIdx.x < 3) {
       double m = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[threadIdx.x][w]);
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = max_keep_nan(m, red[threadIdx.x][w]);
       atomicMax(out + 3 * c + threadIdx.x, (unsigned long long)__double_as_longlong(m));
     }
     __syncthreads();
@@ -408,18 +409,19 @@ __global__ void __launch_bounds__(256) k_bwd_error_parts(int64_t n, int64_t nrhs
 }
 
 // max |x_i| over n doubles into out (as bits; non-negative doubles order like
-// their bit patterns): grid-stride, reduced per CTA, one atomic per CTA.
+// their bit patterns): grid-stride, reduced per CTA, one atomic per CTA.  A
+// NaN in x gives NaN (so a NaN factor entry reads as unbounded growth).
 __global__ void __launch_bounds__(256) k_abs_max(const double* __restrict__ x, int64_t n,
                                                  unsigned long long* __restrict__ out) {
   __shared__ double red[8];
   double m = 0.0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    m = fmax(m, fabs(x[i]));
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    m = max_keep_nan(m, fabs(x[i]));
+  for (int o = 16; o > 0; o >>= 1) m = max_keep_nan(m, __shfl_xor_sync(0xffffffffu, m, o));
   if (lane_id() == 0) red[warp_id()] = m;
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = max_keep_nan(m, red[w]);
     atomicMax(out, (unsigned long long)__double_as_longlong(m));
   }
 }

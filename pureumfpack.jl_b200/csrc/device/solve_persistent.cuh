@@ -9,9 +9,10 @@
 // table: each step's work items (supernode x right-hand-side chunk, GEMM
 // tile) are spread over the CTAs, and a grid barrier
 // separates dependent steps.  The barrier is this library's own and is
-// bounded in time: a CTA that waits longer than kBarrierWaitNs raises the
-// error word and leaves, so a stuck launch turns into an error status, and
-// every later barrier of the launch fails at once.
+// bounded in time: a CTA that waits longer than the handle's wait limit
+// (GridBarrier::wait_ns, kBarrierWaitNs unless set) raises the error word and
+// leaves, so a stuck launch turns into an error status, and every later
+// barrier of the launch fails at once.
 #pragma once
 
 #include "gemm_kernels.cuh"
@@ -37,6 +38,7 @@ struct GridBarrier {
   unsigned int* count;   // arrivals of the current barrier
   unsigned int* gen;     // barrier generation
   int* err;              // err[0]: a barrier of this launch failed; err[1]: sticky over launches
+  uint64_t wait_ns;      // bound on one CTA's wait at a barrier
 };
 
 __device__ __forceinline__ uint64_t solve_ns() {
@@ -63,7 +65,7 @@ __device__ __forceinline__ bool grid_barrier(const GridBarrier& b) {
     } else {
       const uint64_t t0 = solve_ns();
       for (unsigned int i = 1; *vgen == g; ++i) {
-        if ((i & 63u) == 0u && (*verr || solve_ns() - t0 > kBarrierWaitNs)) {
+        if ((i & 63u) == 0u && (*verr || solve_ns() - t0 > b.wait_ns)) {
           good = 0;
           break;
         }

@@ -19,16 +19,18 @@
 // which the producers wait on before they refill it.  A final commit marks
 // the accumulator complete; warps 0-3 then read their 32 accumulator lanes
 // with tcgen05.ld for the C -= acc epilogue.  There is no block-wide barrier
-// inside the K loop, and every mbarrier wait is bounded: on expiry the
-// kernel records the failure in flags[1], lets the issued MMAs drain, frees
-// its tensor memory and returns.
+// inside the K loop, and every mbarrier wait is bounded by the handle's wait
+// limit (wait_ns, 4 s unless set): on expiry the kernel records the failure
+// in flags[1], waits (bounded by kTcDrainNs) for the MMAs it issued to
+// complete, leaves C unwritten, frees its tensor memory and returns.
 #pragma once
 
 #include "common.cuh"
 
 namespace mfgpu {
 
-constexpr uint64_t kTcWaitNs = 4000000000ull;        // 4 s bound on every mbarrier wait
+constexpr uint64_t kTcWaitNs = 4000000000ull;        // default bound on every mbarrier wait (4 s)
+constexpr uint64_t kTcDrainNs = 4000000000ull;       // bound on the wait for issued MMAs after a failure
 constexpr int kTcProducers = 128;                    // warps 0-3: operand staging, then the epilogue
 constexpr int kTcThreads = kTcProducers + 32;        // warp 4: the MMA issuer
 
@@ -86,8 +88,8 @@ __device__ __forceinline__ uint64_t global_ns() {
 }
 
 // Bounded wait for phase `parity` of an mbarrier: non-blocking polls until
-// the phase completes (true) or kTcWaitNs of wall time pass (false).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// the phase completes (true) or limit_ns of wall time pass (false).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
   const uint32_t a = smem_u32(bar);
   const uint64_t start = global_ns();
   for (uint32_t i = 0;; ++i) {
@@ -100,8 +102,34 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
-    if ((i & 255) == 255 && global_ns() - start > kTcWaitNs) return false;
+    if ((i & 255) == 255 && global_ns() - start > limit_ns) return false;
   }
+}
+
+// Epilogue threads: wait for the final commit (the accumulator complete).
+// When that wait runs out, the failure is recorded and the thread keeps
+// waiting, bounded by kTcDrainNs, for the issued MMAs to complete, so that
+// the tensor memory is idle before it is freed.
+__device__ __forceinline__ void tc_wait_done(uint64_t* done, uint64_t wait_ns, volatile int* failed) {
+  if (!mbar_wait(done, 0u, wait_ns)) {
+    *failed = 1;
+    mbar_wait(done, 0u, kTcDrainNs);
+  }
+}
+
+// 32 consecutive accumulator columns of this warp's 32 lanes (32x32b.x32),
+// complete on return.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
 __device__ __forceinline__ void tc_mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -145,7 +173,7 @@ __device__ __forceinline__ void tc_put4(uint32_t hi_base, uint32_t lo_base, int 
 template <int BN, int STAGES>
 __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(const GemmTask* __restrict__ tasks, int ntasks,
                                                         const float* __restrict__ pa, const float* __restrict__ pb,
-                                                        float* pc, int* __restrict__ flags) {
+                                                        float* pc, int* __restrict__ flags, uint64_t wait_ns) {
   using Cfg = TcCfg<BN, STAGES>;
   constexpr int BK = Cfg::BK;
   extern __shared__ __align__(16) uint8_t tc_smem_raw[];
@@ -210,7 +238,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(const GemmTask* __res
           vb[i][j] = (n0 + n < N && kk < K) ? B[(int64_t)kk + (int64_t)(n0 + n) * tk.ldb] : 0.0f;
         }
       }
-      if (kb >= STAGES && !mbar_wait(&empty[s], (uint32_t)((kb / STAGES - 1) & 1))) {
+      if (kb >= STAGES && !mbar_wait(&empty[s], (uint32_t)((kb / STAGES - 1) & 1), wait_ns)) {
         failed = 1;
         break;
       }
@@ -231,7 +259,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(const GemmTask* __res
     int kb = 0;
     for (; kb < nk; ++kb) {
       const int s = kb % STAGES;
-      if (failed || !mbar_wait(&full[s], (uint32_t)((kb / STAGES) & 1))) {
+      if (failed || !mbar_wait(&full[s], (uint32_t)((kb / STAGES) & 1), wait_ns)) {
         failed = 1;
         break;
       }
@@ -253,9 +281,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(const GemmTask* __res
     tc_commit(&done);
   }
 
+  // the accumulator is complete (or, after a failure, every issued MMA has
+  // drained) before any thread goes on; `failed` is then block-uniform
+  if (warp < 4) tc_wait_done(&done, wait_ns, &failed);
+  __syncthreads();
+  const bool ok = !failed;
   if (warp < 4) {
     // ---- epilogue: warp w reads accumulator lanes 32w..32w+31 (rows of the tile)
-    const bool ok = mbar_wait(&done, 0u) && !failed;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok) {
       float* C = pc + tk.c;
@@ -322,6 +354,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(const GemmTask* __res
 // thread t converts row t % 128 over K half t / 128 of A, and four 8-value
 // chunks of B; warp 8 issues the MMAs; all eight staging warps then read the
 // accumulator back (warp w: lanes 32 (w % 4).., column half w / 4).
+//
+// The tensor core's FP32 accumulation rounds every addition towards zero,
+// so over a long K its error is a bias that grows with the number of
+// accumulation steps, and FP64 iterative refinement converges more slowly
+// against such factors than against CUDA-core FP32 ones.  The K blocks are
+// therefore spread round-robin over kAccs accumulators in tensor memory (all
+// 512 columns for BN = 128): each sees a quarter of the steps and a quarter
+// of the running sum, and the epilogue adds the partial sums in FP32 with
+// round-to-nearest.
 constexpr int kBxProducers = 256;
 constexpr int kBxThreads = kBxProducers + 32;
 
@@ -332,7 +373,8 @@ struct BxCfg {
   static constexpr int kBBytes = BN * BK * 2;
   static constexpr int kStageBytes = 3 * kABytes + 3 * kBBytes;
   static constexpr size_t kSmem = (size_t)STAGES * kStageBytes + 1024;
-  static constexpr int kTmemCols = BN;
+  static constexpr int kAccs = 4;                  // accumulators, K blocks round-robin
+  static constexpr int kTmemCols = kAccs * BN;     // 512 or 256 columns (power of two)
   // D f32, A/B bf16, both K-major, N = BN, M = 128
   static constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
                                      ((uint32_t)(BM >> 4) << 24);
@@ -388,7 +430,7 @@ __device__ __forceinline__ void bx_put8(uint32_t p1, uint32_t p2, uint32_t p3, u
 template <int BN, int STAGES>
 __global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __restrict__ tasks, int ntasks,
                                                             const float* __restrict__ pa, const float* __restrict__ pb,
-                                                            float* pc, int* __restrict__ flags) {
+                                                            float* pc, int* __restrict__ flags, uint64_t wait_ns) {
   using Cfg = BxCfg<BN, STAGES>;
   constexpr int BK = Cfg::BK;
   extern __shared__ __align__(16) uint8_t bx_smem_raw[];
@@ -455,7 +497,7 @@ __global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __re
           vb[i][j] = (n0 + n < N && kk < K) ? B[(int64_t)kk + (int64_t)(n0 + n) * tk.ldb] : 0.0f;
         }
       }
-      if (kb >= STAGES && !mbar_wait(&empty[s], (uint32_t)((kb / STAGES - 1) & 1))) {
+      if (kb >= STAGES && !mbar_wait(&empty[s], (uint32_t)((kb / STAGES - 1) & 1), wait_ns)) {
         failed = 1;
         break;
       }
@@ -476,7 +518,7 @@ __global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __re
   } else if (lane == 0) {
     for (int kb = 0; kb < nk; ++kb) {
       const int s = kb % STAGES;
-      if (failed || !mbar_wait(&full[s], (uint32_t)((kb / STAGES) & 1))) {
+      if (failed || !mbar_wait(&full[s], (uint32_t)((kb / STAGES) & 1), wait_ns)) {
         failed = 1;
         break;
       }
@@ -486,22 +528,25 @@ __global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __re
 #pragma unroll
       for (int ks = 0; ks < BK / 16; ++ks) {      // K = 16 per instruction: 32 bytes along the row
         const uint32_t ko = ks * 32;
-        // smallest terms first
-        tc_mma_bf16(tmem, umma_desc_sw128(a2 + ko), umma_desc_sw128(b2 + ko), Cfg::kIdesc,
-                    (kb > 0 || ks > 0) ? 1u : 0u);
-        tc_mma_bf16(tmem, umma_desc_sw128(a3 + ko), umma_desc_sw128(b1 + ko), Cfg::kIdesc, 1u);
-        tc_mma_bf16(tmem, umma_desc_sw128(a1 + ko), umma_desc_sw128(b3 + ko), Cfg::kIdesc, 1u);
-        tc_mma_bf16(tmem, umma_desc_sw128(a2 + ko), umma_desc_sw128(b1 + ko), Cfg::kIdesc, 1u);
-        tc_mma_bf16(tmem, umma_desc_sw128(a1 + ko), umma_desc_sw128(b2 + ko), Cfg::kIdesc, 1u);
-        tc_mma_bf16(tmem, umma_desc_sw128(a1 + ko), umma_desc_sw128(b1 + ko), Cfg::kIdesc, 1u);
+        // smallest terms first, into accumulator kb % kAccs
+        const uint32_t acc = tmem + (uint32_t)((kb % Cfg::kAccs) * BN);
+        tc_mma_bf16(acc, umma_desc_sw128(a2 + ko), umma_desc_sw128(b2 + ko), Cfg::kIdesc,
+                    (kb >= Cfg::kAccs || ks > 0) ? 1u : 0u);
+        tc_mma_bf16(acc, umma_desc_sw128(a3 + ko), umma_desc_sw128(b1 + ko), Cfg::kIdesc, 1u);
+        tc_mma_bf16(acc, umma_desc_sw128(a1 + ko), umma_desc_sw128(b3 + ko), Cfg::kIdesc, 1u);
+        tc_mma_bf16(acc, umma_desc_sw128(a2 + ko), umma_desc_sw128(b1 + ko), Cfg::kIdesc, 1u);
+        tc_mma_bf16(acc, umma_desc_sw128(a1 + ko), umma_desc_sw128(b2 + ko), Cfg::kIdesc, 1u);
+        tc_mma_bf16(acc, umma_desc_sw128(a1 + ko), umma_desc_sw128(b1 + ko), Cfg::kIdesc, 1u);
       }
       tc_commit(&empty[s]);
     }
     tc_commit(&done);
   }
 
+  if (warp < 8) tc_wait_done(&done, wait_ns, &failed);
+  __syncthreads();
+  const bool ok = !failed;
   if (warp < 8) {
-    const bool ok = mbar_wait(&done, 0u) && !failed;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok) {
       float* C = pc + tk.c;
@@ -512,24 +557,16 @@ __global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __re
       const bool ld = tk.mode == kGemmSub || tk.mode == kGemmFrom;
       const float sgn = tk.mode == kGemmSet ? -1.0f : 1.0f;
 #pragma unroll 1
+      const int nacc = nk < Cfg::kAccs ? nk : Cfg::kAccs;   // accumulators that K blocks reached
       for (int c0 = half * (BN / 2); c0 < (half + 1) * (BN / 2); c0 += 32) {
-        uint32_t v[32];
-        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0;
-        if (nk == 0) {
+        float acc[32];
 #pragma unroll
-          for (int j = 0; j < 32; ++j) v[j] = 0u;
-        } else {
-          asm volatile(
-              "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-              "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-              "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-                "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
-                "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
-                "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-              : "r"(taddr));
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        for (int j = 0; j < 32; ++j) acc[j] = 0.0f;   // K = 0: the product is zero (C = D or C = 0)
+        for (int b = 0; b < nacc; ++b) {
+          uint32_t v[32];
+          tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + c0), v);
+#pragma unroll
+          for (int j = 0; j < 32; ++j) acc[j] += __uint_as_float(v[j]);
         }
         if (row < M) {
           float cv[32];
@@ -541,11 +578,11 @@ __global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __re
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const int col = n0 + c0 + j;
-            if (col < N) C[(int64_t)row + (int64_t)col * tk.ldc] = cv[j] - sgn * __uint_as_float(v[j]);
+            if (col < N) C[(int64_t)row + (int64_t)col * tk.ldc] = cv[j] - sgn * acc[j];
           }
         }
       }
-    } else if (failed && t == 0) {
+    } else if (t == 0) {
       atomicOr(flags + 1, 1);
     }
   }

@@ -188,6 +188,7 @@ struct mfgpu_ctx {
       b_csr_ptr, b_csr_col, b_csr_src;
   DevBuf b_small, b_panel, b_trsm, b_gemm, b_gemm_tc;
   bool use_tc = true;      // FP32 fronts: GEMMs on tensor cores
+  uint64_t wait_ns = kTcWaitNs;   // bound on every device-side wait (mbarriers, grid barriers)
   bool tc_bf16x3 = true;   // tensor-core split: BF16x3 (FP32 accuracy) or 3xTF32
   bool launches_safe = false;
   // numeric state
@@ -560,10 +561,10 @@ void launch_tc(const mfgpu_ctx* h, const GemmTask* tasks, int64_t count, int64_t
                const float* pb, float* pc, cudaStream_t st) {
   if (h->tc_bf16x3)
     k_gemm_bx3<128, 2><<<(unsigned)tiles, kBxThreads, BxCfg<128, 2>::kSmem, st>>>(tasks, (int)count, pa, pb, pc,
-                                                                                  h->b_flags.as<int>());
+                                                                                  h->b_flags.as<int>(), h->wait_ns);
   else
     k_gemm_tc<128, 3><<<(unsigned)tiles, kTcThreads, TcCfg<128, 3>::kSmem, st>>>(tasks, (int)count, pa, pb, pc,
-                                                                                h->b_flags.as<int>());
+                                                                                h->b_flags.as<int>(), h->wait_ns);
 }
 
 // Tunable-launch ids: factor GEMM launches first, then the inversion steps,
@@ -808,13 +809,14 @@ int factor_impl(mfgpu_ctx* h, int32_t check) {
         (uintptr_t)h->b_lx.p, (uintptr_t)h->b_ui.p, (uintptr_t)h->b_ux.p, (uintptr_t)h->b_small.p,
         (uintptr_t)h->b_panel.p, (uintptr_t)h->b_trsm.p, (uintptr_t)h->b_gemm.p, (uintptr_t)h->b_ipiv.p,
         (uintptr_t)h->b_gemm_tc.p, (uintptr_t)h->use_tc, (uintptr_t)h->tc_bf16x3, (uintptr_t)h->choice_version,
+        (uintptr_t)h->wait_ns,
         (uintptr_t)h->b_info.p, (uintptr_t)h->b_flags.p, (uintptr_t)st};
     run_sequence(h, h->factor_key, h->factor_exec, h->factor_nodes, key, [&] { issue_factor<T>(h); });
     if (!P.has_speculative) break;
-    int32_t flag = 0;
-    CK(cudaMemcpyAsync(&flag, h->b_flags.p, 4, cudaMemcpyDeviceToHost, st));
+    int32_t flag[2] = {0, 0};
+    CK(cudaMemcpyAsync(flag, h->b_flags.p, 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (!flag) break;
+    if (!flag[0] || flag[1]) break;   // no pivoting needed, or a bounded wait ran out (reported below)
     // a speculative panel met a row that partial pivoting would have chosen:
     // redo the factorization with pivoting panels everywhere.
     prof_flush(h);
@@ -1141,7 +1143,7 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
   if (h->persistent && !S.phases.empty()) {
     unsigned int* bar = h->b_bar.as<unsigned int>();
     PersistentArgs X{S.d_phases.as<SolvePhase>(), (int32_t)S.phases.size(), ids, gemms,
-                     GridBarrier{bar, bar + 1, reinterpret_cast<int*>(bar + 2)}, nullptr};
+                     GridBarrier{bar, bar + 1, reinterpret_cast<int*>(bar + 2), h->wait_ns}, nullptr};
     if (h->profiling) {
       X.stamps = h->b_stamps.as<unsigned long long>() + h->stamp_next;
       h->pending_phases.push_back({h->stamp_next, (int)S.phases.size(), (int)sizeof(T)});
@@ -1250,6 +1252,7 @@ void solve_refine(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, doubl
   const Plan& P = h->plan;
   cudaStream_t st = h->stream;
   if (h->persistent) CK(cudaMemsetAsync(h->b_bar.as<unsigned int>() + 3, 0, sizeof(unsigned int), st));
+  CK(cudaMemsetAsync(h->b_flags.as<int>() + 1, 0, sizeof(int), st));   // this solve's timeout flag
   solve_once<T>(h, R, d_b, ldb, d_x, ldx, use_rs, 0);
   if (refine > 0) {
     double* r = h->b_r.as<double>();
@@ -1274,7 +1277,8 @@ void solve_graph(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double
       (uintptr_t)h->have_rs, (uintptr_t)h->b_rs.p, (uintptr_t)h->b_pool.p, (uintptr_t)h->b_dinv.p,
       (uintptr_t)h->b_fsol.p, (uintptr_t)h->b_inv_tasks.p, (uintptr_t)h->b_r.p, (uintptr_t)h->b_ax.p,
       (uintptr_t)S.d_ids.p, (uintptr_t)S.d_gemms.p, (uintptr_t)S.d_phases.p, (uintptr_t)h->b_prow.p,
-      (uintptr_t)S.d_gemms_tc.p, (uintptr_t)S.d_skinny.p, (uintptr_t)h->b_skinny.p, (uintptr_t)h->use_tc, (uintptr_t)h->tc_bf16x3, (uintptr_t)h->choice_version,
+      (uintptr_t)S.d_gemms_tc.p, (uintptr_t)S.d_skinny.p, (uintptr_t)h->b_skinny.p, (uintptr_t)h->use_tc,
+      (uintptr_t)h->tc_bf16x3, (uintptr_t)h->choice_version, (uintptr_t)h->wait_ns,
       (uintptr_t)h->persistent, (uintptr_t)h->b_bar.p,
       (uintptr_t)h->b_rowfac.p, (uintptr_t)h->stream};
   if (!h->solve_graphs) {
@@ -1348,6 +1352,17 @@ int analyze_common(mfgpu_ctx* h, int64_t n, const int64_t* colptr, const int64_t
   CK(cudaStreamSynchronize(h->stream));
   h->t_analyze_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return MFGPU_OK;
+}
+
+// One right-hand side's backward error r / den folded into the running
+// maximum.  A non-finite residual or denominator (a NaN or Inf in x, b or A,
+// or an overflow) gives NaN, and a NaN stays the maximum: an accuracy check
+// can never pass on a broken solution.  den = 0 means b = 0 and A x = 0.
+__host__ __device__ inline double worst_eta(double worst, double r, double den) {
+  const bool finite = r - r == 0.0 && den - den == 0.0;   // false for NaN and +-Inf
+  const double eta = finite ? (den > 0 ? r / den : 0.0) : nan("");
+  if (worst != worst) return worst;
+  return (eta != eta || eta > worst) ? eta : worst;
 }
 
 bool valid_csc(int64_t n, const int64_t* colptr, const int64_t* rowval) {
@@ -1446,6 +1461,12 @@ int mfgpu_set_stream(mfgpu_ctx* h, void* s) {
 int mfgpu_set_growth_limit(mfgpu_ctx* h, double limit) {
   if (!h || !(limit > 0)) return MFGPU_ERR_ARGUMENT;
   h->growth_limit = limit;
+  return MFGPU_OK;
+}
+
+int mfgpu_set_wait_limit(mfgpu_ctx* h, double seconds) {
+  if (!h || !(seconds > 0) || !(seconds <= 3600)) return MFGPU_ERR_ARGUMENT;
+  h->wait_ns = std::max<uint64_t>(1, (uint64_t)(seconds * 1e9));   // part of the graph keys
   return MFGPU_OK;
 }
 
@@ -1749,11 +1770,7 @@ int mfgpu_backward_error_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, i
     CK(cudaMemcpyAsync(&anorm, h->b_norm.p, 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     double worst = 0;
-    for (int64_t c = 0; c < nrhs; ++c) {
-      const double den = anorm * parts[3 * c + 1] + parts[3 * c + 2];
-      const double eta = den > 0 ? parts[3 * c] / den : 0.0;
-      worst = std::max(worst, eta);
-    }
+    for (int64_t c = 0; c < nrhs; ++c) worst = worst_eta(worst, parts[3 * c], anorm * parts[3 * c + 1] + parts[3 * c + 2]);
     *out = worst;
     return MFGPU_OK;
   });
@@ -1937,22 +1954,47 @@ void* noalloc_scratch(int device) {
   return g_noalloc_ptr[device];
 }
 
-__global__ void k_noalloc_residual_max(int64_t n, int64_t nrhs, const int32_t* __restrict__ rp,
-                                       const int32_t* __restrict__ ci, const int32_t* __restrict__ src,
-                                       const double* __restrict__ ax, const double* __restrict__ b, int64_t ldb,
-                                       const double* __restrict__ x, int64_t ldx,
-                                       unsigned long long* __restrict__ scratch) {
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n * nrhs) return;
-  const int64_t i = e % n, c = e / n;
-  double acc = 0.0;
-  for (int p = rp[i]; p < rp[i + 1]; ++p) acc += ax[src[p]] * x[ci[p] + c * ldx];
-  const double bi = b[i + c * ldb];
-  atomicMax(scratch + 3 * c + 0, (unsigned long long)__double_as_longlong(fabs(bi - acc)));
-  atomicMax(scratch + 3 * c + 1, (unsigned long long)__double_as_longlong(fabs(x[i + c * ldx])));
-  atomicMax(scratch + 3 * c + 2, (unsigned long long)__double_as_longlong(fabs(bi)));
+// Per right-hand side: max|b - A x|, max|x|, max|b| of a 256-row slice of
+// one column per CTA (grid: row slices x columns).  The residual of each row
+// is formed in registers with k_residual's arithmetic (same order, so the
+// same bits) and never stored; the slice is reduced in the CTA and each
+// quantity takes one atomicMax per CTA.  A NaN is kept (max_keep_nan).
+__global__ void __launch_bounds__(256) k_noalloc_residual_max(int64_t n, int64_t nrhs, const int32_t* __restrict__ rp,
+                                                              const int32_t* __restrict__ ci,
+                                                              const int32_t* __restrict__ src,
+                                                              const double* __restrict__ ax,
+                                                              const double* __restrict__ b, int64_t ldb,
+                                                              const double* __restrict__ x, int64_t ldx,
+                                                              unsigned long long* __restrict__ scratch) {
+  __shared__ double red[3][8];
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t c = blockIdx.y; c < nrhs; c += gridDim.y) {
+    double v[3] = {0.0, 0.0, 0.0};
+    if (i < n) {
+      double acc = 0.0;
+      for (int p = rp[i]; p < rp[i + 1]; ++p) acc += ax[src[p]] * x[ci[p] + c * ldx];
+      const double bi = b[i + c * ldb];
+      v[0] = fabs(bi - acc);
+      v[1] = fabs(x[i + c * ldx]);
+      v[2] = fabs(bi);
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+      for (int o = 16; o > 0; o >>= 1) v[q] = max_keep_nan(v[q], __shfl_xor_sync(0xffffffffu, v[q], o));
+    if (lane_id() == 0)
+      for (int q = 0; q < 3; ++q) red[q][warp_id()] = v[q];
+    __syncthreads();
+    if (threadIdx.x < 3) {
+      double m = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = max_keep_nan(m, red[threadIdx.x][w]);
+      atomicMax(scratch + 3 * c + threadIdx.x, (unsigned long long)__double_as_longlong(m));
+    }
+    __syncthreads();
+  }
 }
 
+// The largest backward error over the right-hand sides, folded by
+// worst_eta (a NaN in any column makes the result NaN), into the result slot.
 __global__ void k_noalloc_finish(int64_t nrhs, unsigned long long* __restrict__ scratch) {
   __shared__ double red[256];
   const double anorm = __longlong_as_double((long long)scratch[3 * kNoAllocMaxRhs]);
@@ -1961,13 +2003,12 @@ __global__ void k_noalloc_finish(int64_t nrhs, unsigned long long* __restrict__ 
     const double r = __longlong_as_double((long long)scratch[3 * c]);
     const double xn = __longlong_as_double((long long)scratch[3 * c + 1]);
     const double bn = __longlong_as_double((long long)scratch[3 * c + 2]);
-    const double den = anorm * xn + bn;
-    worst = fmax(worst, den > 0 ? r / den : 0.0);
+    worst = worst_eta(worst, r, anorm * xn + bn);
   }
   red[threadIdx.x] = worst;
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+    if (threadIdx.x < o) red[threadIdx.x] = max_keep_nan(red[threadIdx.x], red[threadIdx.x + o]);
     __syncthreads();
   }
   if (threadIdx.x == 0) scratch[3 * kNoAllocMaxRhs + 1] = (unsigned long long)__double_as_longlong(red[0]);
@@ -1977,11 +2018,16 @@ __global__ void k_noalloc_finish(int64_t nrhs, unsigned long long* __restrict__ 
 
 extern "C" int mfgpu_backward_error_noalloc(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ldb,
                                             const double* d_x, int64_t ldx, double* out) {
-  if (!h || !out || !d_b || !d_x) return MFGPU_ERR_ARGUMENT;
+  if (!h || !out) return MFGPU_ERR_ARGUMENT;
   if (!h->factored) return fail(h, MFGPU_ERR_STATE, "no matrix values (factor first)");
   if (nrhs < 1 || nrhs > kNoAllocMaxRhs)
     return fail(h, MFGPU_ERR_ARGUMENT, "mfgpu_backward_error_noalloc: nrhs must be in 1.." +
                                            std::to_string(kNoAllocMaxRhs));
+  if (h->plan.n == 0) {   // a 0 x 0 system: nothing to launch, as mfgpu_backward_error_device
+    *out = 0.0;
+    return MFGPU_OK;
+  }
+  if (!d_b || !d_x) return fail(h, MFGPU_ERR_ARGUMENT, "null vectors");
   if (ldb < h->plan.n || ldx < h->plan.n) return fail(h, MFGPU_ERR_ARGUMENT, "leading dimension below n");
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->device));
@@ -1990,7 +2036,7 @@ extern "C" int mfgpu_backward_error_noalloc(mfgpu_ctx* h, int64_t nrhs, const do
     cudaStream_t st = h->stream;
     const int64_t n = P.n;
     CK(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long) * (3 * kNoAllocMaxRhs + 2), st));
-    k_noalloc_residual_max<<<grid1(n * nrhs, 256), 256, 0, st>>>(
+    k_noalloc_residual_max<<<dim3((unsigned)((n + 255) / 256), (unsigned)nrhs), 256, 0, st>>>(
         n, nrhs, h->b_csr_ptr.as<int32_t>(), h->b_csr_col.as<int32_t>(), h->b_csr_src.as<int32_t>(),
         h->b_ax.as<double>(), d_b, ldb, d_x, ldx, scratch);
     k_norm_inf<<<grid1(n, 256), 256, 0, st>>>(n, h->b_csr_ptr.as<int32_t>(), h->b_csr_src.as<int32_t>(),

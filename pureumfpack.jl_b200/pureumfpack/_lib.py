@@ -44,6 +44,7 @@ SIGNATURES = [
     ("mfgpu_set_stream", ctypes.c_int, [vp, vp]),
     ("mfgpu_set_precision", ctypes.c_int, [vp, i32]),
     ("mfgpu_set_growth_limit", ctypes.c_int, [vp, f64]),
+    ("mfgpu_set_wait_limit", ctypes.c_int, [vp, f64]),
     ("mfgpu_analyze", ctypes.c_int, [vp, i64, i64p, i64p, i64p, i64p, i64, i64p, i64p, i64p]),
     ("mfgpu_analyze_symbolic", ctypes.c_int, [vp, i64, i64p, i64p, vp]),
     ("mfgpu_factor", ctypes.c_int, [vp, f64p, f64p, i32]),

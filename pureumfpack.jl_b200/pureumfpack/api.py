@@ -286,6 +286,11 @@ class GpuContext:
         max|U| / max|Rs .* A| exceeds ``limit``."""
         self._check(self._lib.mfgpu_set_growth_limit(self._h, float(limit)))
 
+    def set_wait_limit(self, seconds: float):
+        """Bound on every device-side wait of this handle's kernels (default
+        4 s); a wait that runs out makes the call raise MfgpuError(-5)."""
+        self._check(self._lib.mfgpu_set_wait_limit(self._h, ctypes.c_double(seconds)))
+
     def set_stream(self, stream_ptr: int):
         self._check(self._lib.mfgpu_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
 

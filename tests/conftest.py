@@ -24,12 +24,13 @@ def pytest_configure(config):
 
 
 def _ensure_built():
-    lib = os.path.join(PKG, "pureumfpack", "libmfgpu.so")
-    if not os.path.exists(lib):
-        subprocess.run([sys.executable, os.path.join(PKG, "build.py")], check=True)
-    orc = os.path.join(ROOT, "oracle", "_build", "libmforacle.so")
-    if not os.path.exists(orc):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    """Rebuild libmfgpu.so when any of its sources or headers is newer than
+    the library (build.up_to_date compares them), and the oracle through its
+    Makefile, so the tests never run a stale binary."""
+    import build
+
+    build.build()
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
 
 
 _ensure_built()
