@@ -66,8 +66,8 @@ int mfgpu_row_scaling_f32(int64_t n, const int64_t* colptr, const int64_t* rowva
 
 /* row_scaling of a ComplexF64 matrix (src/scaling.jl:92-115 with
  * R = real(Tv) = Float64): values as interleaved (re, im) doubles, Julia's
- * ComplexF64 layout; |z| = hypot(re, im); Float64 Rs.  (The numeric phase
- * has no ComplexF64 entry points yet.) */
+ * ComplexF64 layout; |z| = hypot(re, im); Float64 Rs (the Rs that
+ * mfgpu_factor_c64 takes). */
 int mfgpu_row_scaling_c64(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval_ri,
                           int32_t kind, double* rs);
 
@@ -163,6 +163,13 @@ int mfgpu_set_growth_limit(mfgpu_ctx* h, double limit);
  * timed out leaves no factors: factor again).  The reference's counterpart is
  * a status, not a trap (src/multifrontal.jl:250-252). */
 int mfgpu_set_wait_limit(mfgpu_ctx* h, double seconds);
+/* Test hook for the bounded waits (no counterpart in the reference): with
+ * on != 0 the handle's tensor-core GEMMs first wait on a barrier that nothing
+ * arrives at, and CTA 0 of a persistent solve never arrives at its grid
+ * barrier, so those waits run out after the wait limit and the calls return
+ * MFGPU_ERR_TIMEOUT; on = 0 restores normal operation.  No fault is raised:
+ * the waits end by the kernels' own clocks. */
+int mfgpu_test_stall(mfgpu_ctx* h, int32_t on);
 
 /* Pattern analysis for the numeric phase, from the reference's own symbolic
  * result: A's pattern (colptr, rowval, n x n), SymbolicMF.qf, .parent,
@@ -230,6 +237,23 @@ int mfgpu_factor_f32(mfgpu_ctx* h, const float* nzval, const float* rs, int32_t 
 int mfgpu_get_factors_f32(mfgpu_ctx* h, int64_t* lcolptr, int64_t* lrowval, float* lnzval, int64_t* ucolptr,
                           int64_t* urowval, float* unzval, int64_t* p, int64_t* q, int64_t* pinv);
 int mfgpu_solve_f32(mfgpu_ctx* h, int64_t nrhs, const float* b, float* x, int32_t refine);
+
+/* ComplexF64 matrices (the reference's generic Tv = ComplexF64:
+ * multifrontal_lu / splu of a SparseMatrixCSC{ComplexF64},
+ * test/multifrontal_test.jl:63-75, bench/mf_verify.jl:27-31).  Values,
+ * factors, b and x are interleaved (re, im) doubles -- Julia's ComplexF64
+ * layout -- and Rs is real (mfgpu_row_scaling_c64).  The fronts are complex
+ * FP64 on the GPU: every panel is factored with partial pivoting on the
+ * first largest |re| + |im| of its pivot rows (LAPACK zgetrf's rule, as
+ * Julia's lu!), the updates are complex products on the CUDA cores, and the
+ * solves and refinement residuals are complex.  mfgpu_solve_c64 is
+ * solve(F, b; refine) for nrhs right-hand sides (n x nrhs, column-major,
+ * leading dimension n).  The real-valued entry points refuse complex
+ * factors (MFGPU_ERR_STATE) and the complex ones real factors. */
+int mfgpu_factor_c64(mfgpu_ctx* h, const double* nzval_ri, const double* rs, int32_t check);
+int mfgpu_get_factors_c64(mfgpu_ctx* h, int64_t* lcolptr, int64_t* lrowval, double* lnzval_ri, int64_t* ucolptr,
+                          int64_t* urowval, double* unzval_ri, int64_t* p, int64_t* q, int64_t* pinv);
+int mfgpu_solve_c64(mfgpu_ctx* h, int64_t nrhs, const double* b_ri, double* x_ri, int32_t refine);
 
 /* Normwise backward error max_k ||b_k - A x_k||_inf / (||A||_inf ||x_k||_inf + ||b_k||_inf)
  * of device arrays, computed in FP64 on the GPU with the analyzed pattern.

@@ -117,6 +117,69 @@ __device__ __forceinline__ double absd(T x) {
   return fabs((double)x);
 }
 
+// ---------------------------------------------------------------------------
+// ComplexF64 fronts: (re, im) pairs in Julia's ComplexF64 memory layout.  The
+// factor and solve kernels are templates over the front element type, so
+// they run on complex fronts through these operators.  The pivot magnitude
+// is |re| + |im|, the one LAPACK's izamax (dcabs1) and so Julia's lu! on a
+// ComplexF64 block use; division follows Smith's scaled formula.
+// ---------------------------------------------------------------------------
+struct __align__(16) zc {
+  double re, im;
+  zc() = default;
+  __host__ __device__ constexpr zc(double r) : re(r), im(0.0) {}
+  __host__ __device__ constexpr zc(double r, double i) : re(r), im(i) {}
+};
+__host__ __device__ __forceinline__ zc operator+(zc a, zc b) { return zc(a.re + b.re, a.im + b.im); }
+__host__ __device__ __forceinline__ zc operator-(zc a, zc b) { return zc(a.re - b.re, a.im - b.im); }
+__host__ __device__ __forceinline__ zc operator-(zc a) { return zc(-a.re, -a.im); }
+__host__ __device__ __forceinline__ zc operator*(zc a, zc b) {
+  return zc(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
+}
+__host__ __device__ __forceinline__ zc operator/(zc a, zc b) {
+  if (fabs(b.re) >= fabs(b.im)) {
+    const double r = b.im / b.re, d = b.re + b.im * r;
+    return zc((a.re + a.im * r) / d, (a.im - a.re * r) / d);
+  }
+  const double r = b.re / b.im, d = b.im + b.re * r;
+  return zc((a.re * r + a.im) / d, (a.im * r - a.re) / d);
+}
+__host__ __device__ __forceinline__ zc& operator+=(zc& a, zc b) { return a = a + b; }
+__host__ __device__ __forceinline__ zc& operator-=(zc& a, zc b) { return a = a - b; }
+__host__ __device__ __forceinline__ zc& operator*=(zc& a, zc b) { return a = a * b; }
+__host__ __device__ __forceinline__ zc& operator/=(zc& a, zc b) { return a = a / b; }
+__host__ __device__ __forceinline__ bool operator==(zc a, zc b) { return a.re == b.re && a.im == b.im; }
+__host__ __device__ __forceinline__ bool operator!=(zc a, zc b) { return !(a == b); }
+template <>
+__device__ __forceinline__ double absd<zc>(zc x) {
+  return fabs(x.re) + fabs(x.im);
+}
+
+// Element type of the caller's vectors and of A's values for fronts of type
+// T: FP64 for the FP64 and FP32 fronts (right-hand sides, solutions,
+// residuals and the values V = A[qf, qf] stay FP64), ComplexF64 for complex
+// fronts.
+template <typename T>
+struct WideOf {
+  using type = double;
+};
+template <>
+struct WideOf<zc> {
+  using type = zc;
+};
+template <typename T>
+using Wide = typename WideOf<T>::type;
+template <typename T>
+constexpr bool is_complex_v = false;
+template <>
+constexpr bool is_complex_v<zc> = true;
+
+// A value of V (Wide<T>) into a front of type T (FP32 fronts round it once).
+template <typename T>
+__device__ __forceinline__ T to_front(Wide<T> v) {
+  return (T)v;
+}
+
 // 8-byte asynchronous global->shared copy with zero fill when !pred.
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -203,6 +266,37 @@ __device__ __forceinline__ void mm64<float>(const float* P, const float* Q, floa
     for (int i = 0; i < 4; ++i)
 #pragma unroll
       for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) D[tm + i + (tn + j) * ldd] = acc[i][j];
+  __syncthreads();
+}
+
+// ComplexF64 tiles on the CUDA cores (no complex tensor-core kind): the FP32
+// form's thread layout, a 4 x 8 block of complex accumulators per thread.
+template <>
+__device__ __forceinline__ void mm64<zc>(const zc* P, const zc* Q, zc* D, int ldd) {
+  const int t = threadIdx.x;
+  const int tm = (t & 15) * 4, tn = (t >> 4) * 8;
+  zc acc[4][8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = zc(0.0);
+#pragma unroll 2
+  for (int k = 0; k < 64; ++k) {
+    zc a[4], b[8];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = P[tm + i + k * kLdP];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) b[j] = Q[k + (tn + j) * kLdQ];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * b[j];
   }
   __syncthreads();
 #pragma unroll

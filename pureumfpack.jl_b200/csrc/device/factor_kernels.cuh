@@ -30,7 +30,7 @@ constexpr int kSmallThreads = 128;
 
 template <typename T>
 __global__ void __launch_bounds__(kSmallThreads) k_small_fronts(DevPlan P, DevState S, const int32_t* __restrict__ tasks,
-                                                                 T* __restrict__ pool, const double* __restrict__ vx) {
+                                                                 T* __restrict__ pool, const Wide<T>* __restrict__ vx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* F = reinterpret_cast<T*>(smem_raw);
   __shared__ int s_piv;
@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_fronts(DevPlan P, DevSt
   __syncthreads();
   for (int c = warp_id(); c < nf; c += nthr >> 5) {
     const int b = P.fc_vbeg[fb + c], e = P.fc_vend[fb + c];
-    for (int p = b + lane_id(); p < e; p += 32) F[P.v_frow[p] + c * nf] = (T)vx[p];
+    for (int p = b + lane_id(); p < e; p += 32) F[P.v_frow[p] + c * nf] = to_front<T>(vx[p]);
   }
   __syncthreads();
   for (int ci = P.child_ptr[s + 1] - 1; ci >= P.child_ptr[s]; --ci) {
@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_fronts(DevPlan P, DevSt
 // One warp per front column of the large fronts of a level.
 template <typename T>
 __global__ void __launch_bounds__(256) k_assemble_columns(DevPlan P, int64_t fc0, int64_t count, T* __restrict__ pool,
-                                                          const double* __restrict__ vx) {
+                                                          const Wide<T>* __restrict__ vx) {
   const int64_t w = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp_id();
   if (w >= count) return;
   const int64_t fc = fc0 + w;
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(256) k_assemble_columns(DevPlan P, int64_t fc0
   T* col = pool + P.front_off[s] + (int64_t)c * nf;
   for (int r = lane; r < nf; r += 32) col[r] = T(0);
   __syncwarp();
-  for (int p = P.fc_vbeg[fc] + lane; p < P.fc_vend[fc]; p += 32) col[P.v_frow[p]] = (T)vx[p];
+  for (int p = P.fc_vbeg[fc] + lane; p < P.fc_vend[fc]; p += 32) col[P.v_frow[p]] = to_front<T>(vx[p]);
   __syncwarp();
   for (int e = P.fc_ch_ptr[fc]; e < P.fc_ch_ptr[fc + 1]; ++e) {
     const int k = P.fc_ch[2 * (int64_t)e], t = P.fc_ch[2 * (int64_t)e + 1];
@@ -843,8 +843,8 @@ __global__ void k_finalize_pivots(DevPlan P, DevState S) {
 template <typename T>
 __global__ void __launch_bounds__(256) k_scatter_csc(DevPlan P, DevState S, const T* __restrict__ pool,
                                                      int64_t fc_total, int64_t* __restrict__ li,
-                                                     double* __restrict__ lx, int64_t* __restrict__ ui,
-                                                     double* __restrict__ ux) {
+                                                     Wide<T>* __restrict__ lx, int64_t* __restrict__ ui,
+                                                     Wide<T>* __restrict__ ux) {
   const int64_t fc = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp_id();
   if (fc >= fc_total) return;
   const int lane = lane_id();
@@ -859,18 +859,18 @@ __global__ void __launch_bounds__(256) k_scatter_csc(DevPlan P, DevState S, cons
     const int64_t lb = P.lcolptr[j];
     for (int r = lane; r < nf - a; r += 32) {
       const int fr = a + r;
-      lx[lb + r] = r == 0 ? 1.0 : (double)col[fr];
+      lx[lb + r] = r == 0 ? Wide<T>(1.0) : (Wide<T>)col[fr];
       li[lb + r] = 1 + (fr < np ? (int64_t)(c1 + fr) : (int64_t)S.rowfac[us[fr - np]]);
     }
     const int64_t ub = P.ucolptr[j + 1] - (a + 1);
     for (int b = lane; b <= a; b += 32) {
-      ux[ub + b] = (double)col[b];
+      ux[ub + b] = (Wide<T>)col[b];
       ui[ub + b] = 1 + c1 + b;
     }
   } else {
     const int64_t ub = P.uoff[P.upd_off[s] + (c - np)];
     for (int a = lane; a < np; a += 32) {
-      ux[ub + a] = (double)col[a];
+      ux[ub + a] = (Wide<T>)col[a];
       ui[ub + a] = 1 + c1 + a;
     }
   }
@@ -885,8 +885,8 @@ __global__ void __launch_bounds__(256) k_scatter_csc(DevPlan P, DevState S, cons
 template <typename T>
 __global__ void __launch_bounds__(256) k_scatter_csc_merged(DevPlan P, DevState S, const T* __restrict__ pool,
                                                             int64_t fc_total, int64_t* __restrict__ li,
-                                                            double* __restrict__ lx, int64_t* __restrict__ ui,
-                                                            double* __restrict__ ux) {
+                                                            Wide<T>* __restrict__ lx, int64_t* __restrict__ ui,
+                                                            Wide<T>* __restrict__ ux) {
   const int64_t fc = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp_id();
   if (fc >= fc_total) return;
   const int lane = lane_id();
@@ -900,7 +900,7 @@ __global__ void __launch_bounds__(256) k_scatter_csc_merged(DevPlan P, DevState 
     const int a0 = P.o_c1[s] - c1, a1 = a0 + P.o_np[s];
     const int64_t lb = P.lcolptr[j];
     for (int r = lane; r < a1 - c; r += 32) {
-      lx[lb + r] = r == 0 ? 1.0 : (double)col[c + r];
+      lx[lb + r] = r == 0 ? Wide<T>(1.0) : (Wide<T>)col[c + r];
       li[lb + r] = 1 + (int64_t)(c1 + c + r);
     }
     const int64_t ob = P.o_upd_off[s], on = P.o_upd_off[s + 1] - ob;
@@ -909,19 +909,19 @@ __global__ void __launch_bounds__(256) k_scatter_csc_merged(DevPlan P, DevState 
       const int u = P.o_upd[ob + i];
       const int rf = S.rowfac[u];
       const int pos = u < c1 + np ? rf - c1 : P.o_xpos[ob + i];
-      lx[lu + i] = (double)col[pos];
+      lx[lu + i] = (Wide<T>)col[pos];
       li[lu + i] = 1 + (int64_t)rf;
     }
     const int64_t ub = P.ucolptr[j + 1] - (c - a0 + 1);
     for (int b = lane; b <= c - a0; b += 32) {
-      ux[ub + b] = (double)col[a0 + b];
+      ux[ub + b] = (Wide<T>)col[a0 + b];
       ui[ub + b] = 1 + (int64_t)(c1 + a0 + b);
     }
   }
   for (int64_t e = P.fcu_ptr[fc]; e < P.fcu_ptr[fc + 1]; ++e) {
     const UBlock blk = P.fcu[e];
     for (int b = lane; b < blk.rows; b += 32) {
-      ux[blk.uoff + b] = (double)col[blk.row0 + b];
+      ux[blk.uoff + b] = (Wide<T>)col[blk.row0 + b];
       ui[blk.uoff + b] = 1 + (int64_t)(c1 + blk.row0 + b);
     }
   }
@@ -952,6 +952,69 @@ __global__ void k_build_values(int64_t nnz, const int32_t* __restrict__ src, con
   if (p >= nnz) return;
   const double v = ax[src[p]];
   vx[p] = rs ? rs[srow[p]] * v : v;
+}
+
+// The same for ComplexF64 values (interleaved re, im) and a real Rs.
+__global__ void k_build_values_z(int64_t nnz, const int32_t* __restrict__ src, const int32_t* __restrict__ srow,
+                                 const zc* __restrict__ ax, const double* __restrict__ rs, zc* __restrict__ vx) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nnz) return;
+  const zc v = ax[src[p]];
+  vx[p] = rs ? zc(rs[srow[p]] * v.re, rs[srow[p]] * v.im) : v;
+}
+
+// Panel step of a ComplexF64 front: partial-pivot LU of the panel's R
+// candidate rows in global memory (panel_lu_pivot: the pivot of column j is
+// the first of largest |re| + |im| among its supernode's pivot rows), the
+// inverses of the diagonal block's two triangles into dinv by column
+// substitution, then the interchanges on the columns outside the panel.
+// Complex register tiles would not fit the register file, so the complex
+// fronts take this global-memory variant for every panel (the pivoting
+// launches of the plan; no speculative panels).
+template <typename T>
+__global__ void __launch_bounds__(kPanelThreads) k_panel_global(DevPlan P, DevState S,
+                                                                const PanelTask* __restrict__ tasks,
+                                                                T* __restrict__ pool, T* __restrict__ dinv) {
+  __shared__ ArgMax red[kPanelThreads / 32];
+  __shared__ int piv[kPanel];
+  __shared__ int first_zero;
+  __shared__ int seg[kPanel];
+  __shared__ int nswap;
+  __shared__ int swaps[kPanel];
+  const PanelTask tk = tasks[blockIdx.x];
+  const int s = tk.s, k0 = tk.k0;
+  const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
+  const int kb = min(kPanel, np - k0);
+  const int t = threadIdx.x, nthr = blockDim.x;
+  T* F = pool + P.front_off[s];
+  T* dst = dinv + (P.dinv_off[s] + k0 / kPanel) * (int64_t)kDinvElems;
+  const int R = P.seg_end[c1 + k0 + kb - 1] - k0;
+  if (t == 0) first_zero = INT32_MAX;
+  for (int c = t; c < kPanel; c += nthr) seg[c] = c < kb ? min(R, P.seg_end[c1 + k0 + c] - k0) : 0;
+  __syncthreads();
+  T* D = F + k0 + (int64_t)k0 * nf;
+  panel_lu_pivot(D, nf, R, kb, seg, piv, red, &first_zero);
+  diag_block_inverses(D, nf, kb, dst, dst + 4096);
+  for (int j = t; j < kb; j += nthr) S.ipiv[c1 + k0 + j] = k0 + piv[j];
+  if (t == 0) {
+    if (first_zero != INT32_MAX) atomicMin(S.info + s, k0 + first_zero);
+    int c = 0;
+    for (int j = 0; j < kb; ++j)
+      if (piv[j] != j) swaps[c++] = j;
+    nswap = c;
+  }
+  __syncthreads();
+  const int ns = nswap;
+  for (int cc = t; ns && cc < nf - kb; cc += nthr) {
+    const int c = cc < k0 ? cc : cc + kb;
+    T* col = F + (int64_t)c * nf;
+    for (int q = 0; q < ns; ++q) {
+      const int j = swaps[q], p = piv[j];
+      const T tmp = col[k0 + j];
+      col[k0 + j] = col[k0 + p];
+      col[k0 + p] = tmp;
+    }
+  }
 }
 
 }  // namespace mfgpu

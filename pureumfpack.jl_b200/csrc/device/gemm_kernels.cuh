@@ -412,4 +412,70 @@ __global__ void __launch_bounds__(kSkinnyRows) k_skinny_reduce(const SkinnyTask*
   }
 }
 
+// ---------------------------------------------------------------------------
+// ComplexF64 C = f(C, A * B) (GemmTask::mode) for complex fronts, on the CUDA
+// cores: 64 x 64 tiles located like k_gemm_f64's, 128 threads with a 4 x 8
+// block of complex accumulators each, operands staged through shared memory
+// kGemmZK values of K at a time.
+// ---------------------------------------------------------------------------
+constexpr int kGemmZK = 16;
+
+__global__ void __launch_bounds__(kGemmThreads) k_gemm_z(const GemmTask* __restrict__ tasks, int ntasks,
+                                                         const zc* pa, const zc* pb, zc* pc) {
+  __shared__ zc As[kGemmZK][kGemmBM + 1];   // As[k][m]
+  __shared__ zc Bs[kGemmBN][kGemmZK + 1];   // Bs[n][k]
+  const GemmTask tk = tasks[find_task(tasks, ntasks, blockIdx.x)];
+  const int64_t local = blockIdx.x - tk.tile_base;
+  const int m0 = (int)(local % tk.tiles_m) * kGemmBM;
+  const int n0 = (int)(local / tk.tiles_m) * kGemmBN;
+  const zc* A = pa + tk.a;
+  const zc* B = pb + tk.b;
+  zc* C = pc + tk.c;
+  const int M = tk.m, N = tk.n, K = tk.k;
+  const int t = threadIdx.x;
+  const int tm = (t & 15) * 4, tn = (t >> 4) * 8;
+  zc acc[4][8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = zc(0.0);
+  for (int k0 = 0; k0 < K; k0 += kGemmZK) {
+    for (int e = t; e < kGemmBM * kGemmZK; e += kGemmThreads) {
+      const int m = e % kGemmBM, k = e / kGemmBM;
+      As[k][m] = (m0 + m < M && k0 + k < K) ? A[(int64_t)(m0 + m) + (int64_t)(k0 + k) * tk.lda] : zc(0.0);
+    }
+    for (int e = t; e < kGemmBN * kGemmZK; e += kGemmThreads) {
+      const int k = e % kGemmZK, n = e / kGemmZK;
+      Bs[n][k] = (n0 + n < N && k0 + k < K) ? B[(int64_t)(k0 + k) + (int64_t)(n0 + n) * tk.ldb] : zc(0.0);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < kGemmZK; ++k) {
+      zc a[4], b[8];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[k][tm + i];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) b[j] = Bs[tn + j][k];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * b[j];
+    }
+    __syncthreads();
+  }
+  const zc* D = tk.mode == kGemmFrom ? pc + tk.d : C;
+  const int ldD = tk.mode == kGemmFrom ? tk.ldd : tk.ldc;
+  const bool ld = tk.mode == kGemmSub || tk.mode == kGemmFrom;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int r = m0 + tm + i, c = n0 + tn + j;
+      if (r < M && c < N) {
+        const zc dv = ld ? D[(int64_t)r + (int64_t)c * ldD] : zc(0.0);
+        C[(int64_t)r + (int64_t)c * tk.ldc] = tk.mode == kGemmSet ? acc[i][j] : dv - acc[i][j];
+      }
+    }
+}
+
 }  // namespace mfgpu

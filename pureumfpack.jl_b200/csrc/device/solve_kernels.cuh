@@ -26,6 +26,12 @@ namespace mfgpu {
 
 constexpr int kSolveCols = 32;      // right-hand sides per CTA in the small-supernode kernels
 constexpr int kSolveThreads = 128;
+// Right-hand sides per small-supernode CTA for fronts of type T: half as
+// many for ComplexF64, whose blocks take twice the shared memory.
+template <typename T>
+__host__ __device__ constexpr int solve_cols() {
+  return sizeof(T) > 8 ? kSolveCols / 2 : kSolveCols;
+}
 
 struct SolveArgs {
   int64_t nrhs;
@@ -43,15 +49,15 @@ struct SolveArgs {
 // rows of c contiguously.  Each factor row is read by its own supernode only,
 // before that supernode writes the same rows of x, so c lives in x's storage.
 template <typename T>
-__global__ void k_rhs_factor_order(int64_t n, int64_t nrhs, const double* __restrict__ b, int64_t ldb,
+__global__ void k_rhs_factor_order(int64_t n, int64_t nrhs, const Wide<T>* __restrict__ b, int64_t ldb,
                                    const double* __restrict__ rs, const int32_t* __restrict__ qf,
                                    const int32_t* __restrict__ prow, T* __restrict__ bfo, int64_t ldo) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n * nrhs) return;
   const int64_t k = e % n, c = e / n;
   const int orow = qf[prow[k]];
-  const double v = b[orow + c * ldb];
-  bfo[k + c * ldo] = (T)(rs ? rs[orow] * v : v);
+  const Wide<T> v = b[orow + c * ldb];
+  bfo[k + c * ldo] = (T)(rs ? Wide<T>(rs[orow]) * v : v);
 }
 
 // Pivot-row value of block position a: the scaled rhs of factor row c1 + a.
@@ -80,8 +86,8 @@ __device__ __forceinline__ void fwd_small_item(const DevPlan& P, const DevState&
                                                const int32_t* __restrict__ tasks, const T* __restrict__ pool,
                                                T* fsol, int bx, int by, T* f) {
   const int s = tasks[bx];
-  const int c0 = by * kSolveCols;
-  const int rc = min(kSolveCols, (int)(A.nrhs - c0));
+  const int c0 = by * solve_cols<T>();
+  const int rc = min(solve_cols<T>(), (int)(A.nrhs - c0));
   const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
   const int tid = threadIdx.x;
   const int64_t R = A.nrhs;
@@ -122,7 +128,7 @@ template <typename T>
 __global__ void __launch_bounds__(kSolveThreads) k_fwd_small(DevPlan P, DevState S, SolveArgs A,
                                                              const int32_t* __restrict__ tasks,
                                                              const T* __restrict__ pool, T* fsol) {
-  __shared__ T f[kSmallFront * kSolveCols];
+  __shared__ T f[kSmallFront * solve_cols<T>()];
   fwd_small_item<T>(P, S, A, tasks, pool, fsol, blockIdx.x, blockIdx.y, f);
 }
 
@@ -135,14 +141,20 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd_small(DevPlan P, DevState
 constexpr int kTinyFront = 32;
 constexpr int kTinyLd = 33;
 constexpr int kTinyWarps = 4;
+// Supernodes (warps) per tiny-supernode CTA for fronts of type T (complex
+// blocks take twice the shared memory).
+template <typename T>
+__host__ __device__ constexpr int tiny_warps() {
+  return sizeof(T) > 8 ? kTinyWarps / 2 : kTinyWarps;
+}
 
 template <typename T>
-__global__ void __launch_bounds__(32 * kTinyWarps) k_fwd_tiny(DevPlan P, DevState S, SolveArgs A,
+__global__ void __launch_bounds__(32 * tiny_warps<T>()) k_fwd_tiny(DevPlan P, DevState S, SolveArgs A,
                                                               const int32_t* __restrict__ tasks, int ntasks,
                                                               const T* __restrict__ pool, T* fsol) {
-  __shared__ T buf[kTinyWarps][kTinyFront * kTinyLd];
+  __shared__ T buf[tiny_warps<T>()][kTinyFront * kTinyLd];
   const int w = warp_id(), lane = lane_id();
-  const int ti = blockIdx.x * kTinyWarps + w;
+  const int ti = blockIdx.x * tiny_warps<T>() + w;
   if (ti >= ntasks) return;                 // warp-uniform; no block barrier below
   T* f = buf[w];
   const int s = tasks[ti];
@@ -182,12 +194,12 @@ __global__ void __launch_bounds__(32 * kTinyWarps) k_fwd_tiny(DevPlan P, DevStat
 }
 
 template <typename T>
-__global__ void __launch_bounds__(32 * kTinyWarps) k_bwd_tiny(DevPlan P, SolveArgs A,
+__global__ void __launch_bounds__(32 * tiny_warps<T>()) k_bwd_tiny(DevPlan P, SolveArgs A,
                                                               const int32_t* __restrict__ tasks, int ntasks,
                                                               const T* __restrict__ pool, const T* fsol, T* xw) {
-  __shared__ T buf[kTinyWarps][kTinyFront * kTinyLd];   // rows 0..np-1: y; np..nf-1: x of the update rows
+  __shared__ T buf[tiny_warps<T>()][kTinyFront * kTinyLd];   // rows 0..np-1: y; np..nf-1: x of the update rows
   const int w = warp_id(), lane = lane_id();
-  const int ti = blockIdx.x * kTinyWarps + w;
+  const int ti = blockIdx.x * tiny_warps<T>() + w;
   if (ti >= ntasks) return;
   T* f = buf[w];
   const int s = tasks[ti];
@@ -279,10 +291,10 @@ template <typename T>
 __device__ __forceinline__ void bwd_small_item(const DevPlan& P, const SolveArgs& A,
                                                const int32_t* __restrict__ tasks, const T* __restrict__ pool,
                                                const T* fsol, T* xw, int bx, int by, T* y) {
-  T* g = y + kSmallFront * kSolveCols;
+  T* g = y + kSmallFront * solve_cols<T>();
   const int s = tasks[bx];
-  const int c0 = by * kSolveCols;
-  const int rc = min(kSolveCols, (int)(A.nrhs - c0));
+  const int c0 = by * solve_cols<T>();
+  const int rc = min(solve_cols<T>(), (int)(A.nrhs - c0));
   const int np = P.np[s], nu = P.nu[s], nf = P.nf[s], c1 = P.c1[s];
   const int tid = threadIdx.x;
   const int64_t R = A.nrhs;
@@ -326,7 +338,7 @@ __device__ __forceinline__ void bwd_small_item(const DevPlan& P, const SolveArgs
 template <typename T>
 __global__ void __launch_bounds__(kSolveThreads) k_bwd_small(DevPlan P, SolveArgs A, const int32_t* __restrict__ tasks,
                                                              const T* __restrict__ pool, const T* fsol, T* xw) {
-  __shared__ T y[2 * kSmallFront * kSolveCols];
+  __shared__ T y[2 * kSmallFront * solve_cols<T>()];
   bwd_small_item<T>(P, A, tasks, pool, fsol, xw, blockIdx.x, blockIdx.y, y);
 }
 
@@ -353,12 +365,12 @@ __global__ void __launch_bounds__(256) k_bwd_gather(DevPlan P, SolveArgs A, cons
 // x[q[k]] = x_factor[k] (interface.jl:134-136); optionally accumulate (x += d).
 template <typename T>
 __global__ void k_solve_finish(int64_t n, int64_t nrhs, const int32_t* __restrict__ qf, const T* __restrict__ xw,
-                               int64_t ldw, double* __restrict__ x, int64_t ldx, int accumulate) {
+                               int64_t ldw, Wide<T>* __restrict__ x, int64_t ldx, int accumulate) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n * nrhs) return;
   const int64_t k = e % n, c = e / n;
-  const double v = (double)xw[k + c * ldw];
-  double* dst = x + qf[k] + c * ldx;
+  const Wide<T> v = (Wide<T>)xw[k + c * ldw];
+  Wide<T>* dst = x + qf[k] + c * ldx;
   *dst = accumulate ? *dst + v : v;
 }
 
@@ -371,6 +383,18 @@ __global__ void k_residual(int64_t n, int64_t nrhs, const int32_t* __restrict__ 
   if (e >= n * nrhs) return;
   const int64_t i = e % n, c = e / n;
   double acc = 0.0;
+  for (int p = rp[i]; p < rp[i + 1]; ++p) acc += ax[src[p]] * x[ci[p] + c * ldx];
+  r[i + c * ldr] = b[i + c * ldb] - acc;
+}
+
+// The same for ComplexF64 A (values interleaved re, im), b, x and r.
+__global__ void k_residual_z(int64_t n, int64_t nrhs, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                             const int32_t* __restrict__ src, const zc* __restrict__ ax, const zc* __restrict__ b,
+                             int64_t ldb, const zc* __restrict__ x, int64_t ldx, zc* __restrict__ r, int64_t ldr) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n * nrhs) return;
+  const int64_t i = e % n, c = e / n;
+  zc acc(0.0);
   for (int p = rp[i]; p < rp[i + 1]; ++p) acc += ax[src[p]] * x[ci[p] + c * ldx];
   r[i + c * ldr] = b[i + c * ldb] - acc;
 }

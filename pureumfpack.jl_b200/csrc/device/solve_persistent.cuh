@@ -39,6 +39,7 @@ struct GridBarrier {
   unsigned int* gen;     // barrier generation
   int* err;              // err[0]: a barrier of this launch failed; err[1]: sticky over launches
   uint64_t wait_ns;      // bound on one CTA's wait at a barrier
+  const int* stall;      // test hook (mfgpu_test_stall): CTA 0 never arrives, the others' waits expire
 };
 
 __device__ __forceinline__ uint64_t solve_ns() {
@@ -58,7 +59,9 @@ __device__ __forceinline__ bool grid_barrier(const GridBarrier& b) {
     volatile int* verr = b.err;
     const unsigned int g = *vgen;
     __threadfence();
-    if (atomicAdd(b.count, 1u) + 1u == gridDim.x) {
+    if (*b.stall && blockIdx.x == 0) {
+      good = -1;   // never arrives and leaves without a word: every other CTA's wait runs out by the clock
+    } else if (atomicAdd(b.count, 1u) + 1u == gridDim.x) {
       atomicExch(b.count, 0u);
       __threadfence();
       atomicAdd(b.gen, 1u);
@@ -72,12 +75,12 @@ __device__ __forceinline__ bool grid_barrier(const GridBarrier& b) {
       }
     }
     __threadfence();
-    if (!good || *verr) {
+    if (good == 0 || (good > 0 && *verr)) {
       atomicOr(b.err, 1);
       atomicOr(b.err + 1, 1);
       good = 0;
     }
-    ok = good;
+    ok = good > 0;
   }
   __syncthreads();
   return ok != 0;

@@ -102,7 +102,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
-    if ((i & 255) == 255 && global_ns() - start > limit_ns) return false;
+    if ((i & 31) == 31 && global_ns() - start > limit_ns) return false;
   }
 }
 
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(const GemmTask* __res
   constexpr int BK = Cfg::BK;
   extern __shared__ __align__(16) uint8_t tc_smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023);
-  __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done;
+  __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done, stall;
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int failed;
 
@@ -202,6 +202,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(const GemmTask* __res
       mbar_init(&empty[s], 1);
     }
     mbar_init(&done, 1);
+    mbar_init(&stall, 1);   // nothing arrives on it (test hook, flags[2])
     failed = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -256,8 +257,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(const GemmTask* __res
     }
   } else if (lane == 0) {
     // ---- MMA issuer: 3 TF32 products per K step into the TMEM accumulator
+    if (flags[2] && !mbar_wait(&stall, 0u, wait_ns)) failed = 1;   // test hook: a wait that runs out
     int kb = 0;
-    for (; kb < nk; ++kb) {
+    for (; kb < nk && !failed; ++kb) {
       const int s = kb % STAGES;
       if (failed || !mbar_wait(&full[s], (uint32_t)((kb / STAGES) & 1), wait_ns)) {
         failed = 1;
@@ -435,7 +437,7 @@ __global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __re
   constexpr int BK = Cfg::BK;
   extern __shared__ __align__(16) uint8_t bx_smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)bx_smem_raw + 1023) & ~(uintptr_t)1023);
-  __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done;
+  __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done, stall;
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int failed;
 
@@ -459,6 +461,7 @@ __global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __re
       mbar_init(&empty[s], 1);
     }
     mbar_init(&done, 1);
+    mbar_init(&stall, 1);   // nothing arrives on it (test hook, flags[2])
     failed = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -516,7 +519,8 @@ __global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __re
       if (failed) break;
     }
   } else if (lane == 0) {
-    for (int kb = 0; kb < nk; ++kb) {
+    if (flags[2] && !mbar_wait(&stall, 0u, wait_ns)) failed = 1;   // test hook: a wait that runs out
+    for (int kb = 0; kb < nk && !failed; ++kb) {
       const int s = kb % STAGES;
       if (failed || !mbar_wait(&full[s], (uint32_t)((kb / STAGES) & 1), wait_ns)) {
         failed = 1;
@@ -556,8 +560,8 @@ __global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __re
       const int ldD = tk.mode == kGemmFrom ? tk.ldd : tk.ldc;
       const bool ld = tk.mode == kGemmSub || tk.mode == kGemmFrom;
       const float sgn = tk.mode == kGemmSet ? -1.0f : 1.0f;
-#pragma unroll 1
       const int nacc = nk < Cfg::kAccs ? nk : Cfg::kAccs;   // accumulators that K blocks reached
+#pragma unroll 1
       for (int c0 = half * (BN / 2); c0 < (half + 1) * (BN / 2); c0 += 32) {
         float acc[32];
 #pragma unroll

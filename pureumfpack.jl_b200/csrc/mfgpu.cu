@@ -212,6 +212,8 @@ struct mfgpu_ctx {
   bool merge_fronts = true;    // factor supernode chains as merged fronts (factor structure unchanged)
   int num_sms = 148;           // SMs of the device (split-K chunk choice)
   bool f32_values = false;     // the last factorization is of a Float32 matrix (mfgpu_factor_f32)
+  bool c64_values = false;     // the values given are ComplexF64 (mfgpu_factor_c64)
+  bool c64_factors = false;    // the last completed factorization has ComplexF64 fronts
   bool persistent = false;     // the mode resolved for the current solve
   int persist_grid[2] = {0, 0};          // CTAs of the persistent kernel, FP32 / FP64
   DevBuf b_bar, b_stamps;                // barrier words {count, gen, err, sticky err}; profiling stamps
@@ -507,6 +509,13 @@ template <typename T>
 void configure_kernels() {
   static bool done = false;
   if (done) return;
+  if constexpr (is_complex_v<T>) {   // complex fronts: no speculative, register-tiled or tensor-core kernels
+    CK(cudaFuncSetAttribute(k_small_fronts<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)(kSmallFront * kSmallFront * sizeof(T))));
+    CK(cudaFuncSetAttribute(k_panel_apply<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem_bytes<T>()));
+    done = true;
+    return;
+  } else {
   CK(cudaFuncSetAttribute(k_panel_spec<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)spec_smem_bytes<T>()));
   CK(cudaFuncSetAttribute(k_panel<T, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_smem_bytes<T>(64)));
   CK(cudaFuncSetAttribute(k_panel<T, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_smem_bytes<T>(128)));
@@ -519,6 +528,7 @@ void configure_kernels() {
   CK(cudaFuncSetAttribute(k_solve_persistent<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)persistent_smem_bytes<T>()));
   done = true;
+  }
 }
 
 // dst[i] = (To)src[i] (Float32 right-hand sides in, Float32 solutions out).
@@ -545,6 +555,12 @@ template <>
 void launch_gemm<float>(const GemmTask* tasks, int64_t count, int64_t tiles, const float* pa, const float* pb,
                         float* pc, cudaStream_t st) {
   k_gemm_f32<<<(unsigned)tiles, 256, 0, st>>>(tasks, (int)count, pa, pb, pc);
+}
+
+template <>
+void launch_gemm<zc>(const GemmTask* tasks, int64_t count, int64_t tiles, const zc* pa, const zc* pb, zc* pc,
+                     cudaStream_t st) {
+  k_gemm_z<<<(unsigned)tiles, kGemmThreads, 0, st>>>(tasks, (int)count, pa, pb, pc);
 }
 
 // Kernel variant of tunable GEMM launch `id` with FP32 operands: the
@@ -615,7 +631,7 @@ void run_factor_launches(mfgpu_ctx* h) {
   const Plan& P = h->plan;
   cudaStream_t st = h->stream;
   T* pool = h->b_pool.as<T>();
-  const double* vx = h->b_vx.as<double>();
+  const Wide<T>* vx = h->b_vx.as<Wide<T>>();
   DevState S = dev_state(h);
   int64_t tune_id = 0;
   LevelFork fork(h);
@@ -640,7 +656,9 @@ void run_factor_launches(mfgpu_ctx* h) {
         klaunch(h, KC_PANEL, L.flops, bytes, [&] {
           const PanelTask* pt = h->b_panel.as<PanelTask>() + L.first;
           T* dinv = h->b_dinv.as<T>();
-          if (L.rows == 0)
+          if constexpr (is_complex_v<T>)
+            k_panel_global<T><<<(unsigned)L.count, kPanelThreads, 0, st>>>(h->dp, S, pt, pool, dinv);
+          else if (L.rows == 0)
             k_panel_spec<T><<<(unsigned)L.count, kSpecThreads, spec_smem_bytes<T>(), st>>>(h->dp, S, pt, pool, dinv);
           else if (L.rows <= 64)
             k_panel<T, 64><<<(unsigned)L.count, 64, panel_smem_bytes<T>(64), st>>>(h->dp, S, pt, pool, dinv);
@@ -758,27 +776,33 @@ void issue_factor(mfgpu_ctx* h) {
   const Plan& P = h->plan;
   cudaStream_t st = h->stream;
   klaunch(h, KC_BUILD_VALUES, P.nnz_a, 32.0 * P.nnz_a, [&] {
-    k_build_values<<<grid1(P.nnz_a, 256), 256, 0, st>>>(P.nnz_a, h->b_v_src.as<int32_t>(), h->b_v_srow.as<int32_t>(),
-                                                          h->b_ax.as<double>(),
-                                                          h->have_rs ? h->b_rs.as<double>() : nullptr,
-                                                          h->b_vx.as<double>());
+    if constexpr (is_complex_v<T>)
+      k_build_values_z<<<grid1(P.nnz_a, 256), 256, 0, st>>>(P.nnz_a, h->b_v_src.as<int32_t>(),
+                                                              h->b_v_srow.as<int32_t>(), h->b_ax.as<zc>(),
+                                                              h->have_rs ? h->b_rs.as<double>() : nullptr,
+                                                              h->b_vx.as<zc>());
+    else
+      k_build_values<<<grid1(P.nnz_a, 256), 256, 0, st>>>(P.nnz_a, h->b_v_src.as<int32_t>(),
+                                                            h->b_v_srow.as<int32_t>(), h->b_ax.as<double>(),
+                                                            h->have_rs ? h->b_rs.as<double>() : nullptr,
+                                                            h->b_vx.as<double>());
   });
   if (P.ns) k_fill_i32<<<grid1(P.ns, 256), 256, 0, st>>>(h->b_info.as<int32_t>(), P.ns, INT32_MAX);
-  CK(cudaMemsetAsync(h->b_flags.p, 0, 16, st));
+  CK(cudaMemsetAsync(h->b_flags.p, 0, 8, st));   // flags[2] is the test hook's stall request
   run_factor_launches<T>(h);
   issue_inverses<T>(h);
   if (P.ns)
     klaunch(h, KC_PIVOTS, 0, 16.0 * P.n, [&] { k_finalize_pivots<<<grid1(P.ns, 128), 128, 0, st>>>(h->dp, dev_state(h)); });
   if (P.fc_total)
-    klaunch(h, KC_SCATTER, 0, (double)(P.nnz_l + P.nnz_u) * (16.0 + sizeof(T)), [&] {
+    klaunch(h, KC_SCATTER, 0, (double)(P.nnz_l + P.nnz_u) * (8.0 + sizeof(Wide<T>) + sizeof(T)), [&] {
       if (P.merged)
         k_scatter_csc_merged<T><<<grid1(P.fc_total, 8), 256, 0, st>>>(
-            h->dp, dev_state(h), h->b_pool.as<T>(), P.fc_total, h->b_li.as<int64_t>(), h->b_lx.as<double>(),
-            h->b_ui.as<int64_t>(), h->b_ux.as<double>());
+            h->dp, dev_state(h), h->b_pool.as<T>(), P.fc_total, h->b_li.as<int64_t>(), h->b_lx.as<Wide<T>>(),
+            h->b_ui.as<int64_t>(), h->b_ux.as<Wide<T>>());
       else
         k_scatter_csc<T><<<grid1(P.fc_total, 8), 256, 0, st>>>(h->dp, dev_state(h), h->b_pool.as<T>(), P.fc_total,
-                                                               h->b_li.as<int64_t>(), h->b_lx.as<double>(),
-                                                               h->b_ui.as<int64_t>(), h->b_ux.as<double>());
+                                                               h->b_li.as<int64_t>(), h->b_lx.as<Wide<T>>(),
+                                                               h->b_ui.as<int64_t>(), h->b_ux.as<Wide<T>>());
     });
   CK(cudaGetLastError());
 }
@@ -794,13 +818,25 @@ int factor_impl(mfgpu_ctx* h, int32_t check) {
   h->b_prow.ensure(std::max<int64_t>(P.n, 1) * 4);
   h->b_rowfac.ensure(std::max<int64_t>(P.n, 1) * 4);
   h->b_info.ensure(std::max<int64_t>(P.ns, 1) * 4);
-  h->b_flags.ensure(16);
-  h->b_vx.ensure(std::max<int64_t>(P.nnz_a, 1) * 8);
+  if (!h->b_flags.p) {
+    h->b_flags.ensure(16);
+    CK(cudaMemsetAsync(h->b_flags.p, 0, 16, st));
+  }
+  h->b_vx.ensure(std::max<int64_t>(P.nnz_a, 1) * sizeof(Wide<T>));
   h->b_dinv.ensure(std::max<size_t>((size_t)P.dinv_blocks * kDinvElems * sizeof(T), 16));
   h->b_li.ensure(std::max<int64_t>(P.nnz_l, 1) * 8);
-  h->b_lx.ensure(std::max<int64_t>(P.nnz_l, 1) * 8);
+  h->b_lx.ensure(std::max<int64_t>(P.nnz_l, 1) * sizeof(Wide<T>));
   h->b_ui.ensure(std::max<int64_t>(P.nnz_u, 1) * 8);
-  h->b_ux.ensure(std::max<int64_t>(P.nnz_u, 1) * 8);
+  h->b_ux.ensure(std::max<int64_t>(P.nnz_u, 1) * sizeof(Wide<T>));
+  if constexpr (is_complex_v<T>) {
+    // complex fronts factor every panel with partial pivoting (no speculative
+    // panels): the plan's pivoting launch list
+    if (!h->launches_safe) {
+      build_launches(P, true);
+      upload_launches(h);
+      h->launches_safe = true;
+    }
+  }
   CK(cudaEventRecord(h->ev0, st));
   for (int attempt = 0; attempt < 2; ++attempt) {
     const std::vector<uintptr_t> key = {
@@ -843,7 +879,8 @@ int factor_impl(mfgpu_ctx* h, int32_t check) {
   prof_flush(h);
   h->factored = true;
   h->csc_ready = true;
-  h->factor_precision = (sizeof(T) == 8) ? MFGPU_PRECISION_FP64 : MFGPU_PRECISION_MIXED;
+  h->factor_precision = (sizeof(T) == 4) ? MFGPU_PRECISION_MIXED : MFGPU_PRECISION_FP64;
+  h->c64_factors = is_complex_v<T>;
   int32_t status = 0;
   if (check)
     for (int64_t s = 0; s < P.ns; ++s)
@@ -886,13 +923,15 @@ int factor_dispatch(mfgpu_ctx* h, int32_t check) {
   h->growth = 0.0;
   if (h->plan.n == 0) {   // a 0 x 0 matrix: empty factors, nothing to launch
     h->factored = h->csc_ready = true;
-    h->factor_precision = h->f32_values || h->precision == MFGPU_PRECISION_MIXED ? MFGPU_PRECISION_MIXED
-                                                                                 : MFGPU_PRECISION_FP64;
+    h->c64_factors = h->c64_values;
+    h->factor_precision = !h->c64_values && (h->f32_values || h->precision == MFGPU_PRECISION_MIXED)
+                              ? MFGPU_PRECISION_MIXED : MFGPU_PRECISION_FP64;
     h->last_status = 0;
     h->last_info.clear();
     h->t_factor_ms = 0;
     return MFGPU_OK;
   }
+  if (h->c64_values) return factor_impl<zc>(h, check);     // ComplexF64 matrix: complex FP64 fronts
   if (h->f32_values) return factor_impl<float>(h, check);   // Float32 matrix: FP32 factors, no refactor
   if (h->precision != MFGPU_PRECISION_MIXED) return factor_impl<double>(h, check);
   const int rc = factor_impl<float>(h, check);
@@ -1099,13 +1138,14 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
 template <typename T>
 void prepare_solve(mfgpu_ctx* h, int64_t R, int refine) {
   const Plan& P = h->plan;
-  h->persistent = h->persistent_mode == 1;
+  h->persistent = h->persistent_mode == 1 && !is_complex_v<T>;   // complex fronts: per-step launches
   build_solve_schedule(h, R);
   // solve arena: the per-supernode blocks, then x in factor order
   h->b_fsol.ensure(std::max<size_t>((size_t)(P.fc_total + P.n) * R * sizeof(T), 16));
   if (h->sched.skinny_scratch) h->b_skinny.ensure((size_t)h->sched.skinny_scratch * sizeof(T));
-  if (refine > 0) h->b_r.ensure(std::max<size_t>((size_t)P.n * R * 8, 16));
+  if (refine > 0) h->b_r.ensure(std::max<size_t>((size_t)P.n * R * sizeof(Wide<T>), 16));
   configure_kernels<T>();
+  if constexpr (!is_complex_v<T>)
   if (h->persistent) {
     h->b_bar.ensure(16);
     if (h->profiling) h->b_stamps.ensure((h->sched.phases.size() + 1) * (size_t)(refine + 1) * 8);
@@ -1121,7 +1161,7 @@ void prepare_solve(mfgpu_ctx* h, int64_t R, int refine) {
 }
 
 template <typename T>
-void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double* d_x, int64_t ldx, bool use_rs,
+void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T>* d_x, int64_t ldx, bool use_rs,
                 int accumulate) {
   const Plan& P = h->plan;
   cudaStream_t st = h->stream;
@@ -1130,20 +1170,23 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
   T* fsol = h->b_fsol.as<T>();
   T* xw = fsol + P.fc_total * R;
   DevState DS = dev_state(h);
-  SolveArgs A{R, d_b, ldb, (use_rs && h->have_rs) ? h->b_rs.as<double>() : nullptr, P.n, xw};
+  SolveArgs A{R, reinterpret_cast<const double*>(d_b), ldb, (use_rs && h->have_rs) ? h->b_rs.as<double>() : nullptr,
+              P.n, xw};
   klaunch(h, KC_FWD_ASSEMBLE, 0, (double)P.n * R * (16.0 + sizeof(T)), [&] {
     k_rhs_factor_order<T><<<grid1(P.n * R, 256), 256, 0, st>>>(P.n, R, d_b, ldb, A.rs, h->b_qf.as<int32_t>(),
                                                               h->b_prow.as<int32_t>(), xw, P.n);
   });
-  const unsigned ychunks = (unsigned)((R + kSolveCols - 1) / kSolveCols);
+  const unsigned ychunks = (unsigned)((R + solve_cols<T>() - 1) / solve_cols<T>());
   const unsigned wchunks = (unsigned)((R + 7) / 8);
   const int32_t* ids = S.d_ids.as<int32_t>();
   const GemmTask* gemms = S.d_gemms.as<GemmTask>();
   int64_t tune_id = tune_factor_count(P) + (int64_t)P.inv_steps.size();
-  if (h->persistent && !S.phases.empty()) {
+  if constexpr (is_complex_v<T>) {
+  } else if (h->persistent && !S.phases.empty()) {
     unsigned int* bar = h->b_bar.as<unsigned int>();
     PersistentArgs X{S.d_phases.as<SolvePhase>(), (int32_t)S.phases.size(), ids, gemms,
-                     GridBarrier{bar, bar + 1, reinterpret_cast<int*>(bar + 2), h->wait_ns}, nullptr};
+                     GridBarrier{bar, bar + 1, reinterpret_cast<int*>(bar + 2), h->wait_ns, h->b_flags.as<int>() + 2},
+                     nullptr};
     if (h->profiling) {
       X.stamps = h->b_stamps.as<unsigned long long>() + h->stamp_next;
       h->pending_phases.push_back({h->stamp_next, (int)S.phases.size(), (int)sizeof(T)});
@@ -1162,7 +1205,8 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     CK(cudaLaunchKernelEx(&cfg, k_solve_persistent<T>, h->dp, DS, A, X, (const T*)pool, fsol, xw));
-  } else {
+  }
+  if (is_complex_v<T> || !(h->persistent && !S.phases.empty())) {
   LevelFork fork(h);
   for (const auto& s : S.steps) {
     const double bytes = s.elems * sizeof(T);
@@ -1183,7 +1227,11 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
         break;
       case 3:
         h->cur_tune = (int32_t)tune_id;
-        if (s.sk_count && !(sizeof(T) == 4 && gemm_use_tc(h, tune_id, false)))
+        if constexpr (is_complex_v<T>)
+          klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
+            launch_gemm<T>(gemms + s.first, s.count, s.tiles, pool, fsol, fsol, st);
+          }, -1, s.tiles);
+        else if (s.sk_count && !(sizeof(T) == 4 && gemm_use_tc(h, tune_id, false)))
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
             const SkinnyTask* sk = S.d_skinny.as<SkinnyTask>() + s.sk_first;
             T* part = h->b_skinny.as<T>();
@@ -1214,14 +1262,14 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
         break;
       case 6:
         klaunch(h, KC_FWD_SMALL, s.flops, bytes, [&] {
-          k_fwd_tiny<T><<<dim3((unsigned)((s.count + kTinyWarps - 1) / kTinyWarps), (unsigned)((R + 31) / 32)),
-                          32 * kTinyWarps, 0, ss>>>(h->dp, DS, A, ids + s.first, (int)s.count, pool, fsol);
+          k_fwd_tiny<T><<<dim3((unsigned)((s.count + tiny_warps<T>() - 1) / tiny_warps<T>()), (unsigned)((R + 31) / 32)),
+                          32 * tiny_warps<T>(), 0, ss>>>(h->dp, DS, A, ids + s.first, (int)s.count, pool, fsol);
         });
         break;
       case 7:
         klaunch(h, KC_BWD_SMALL, s.flops, bytes, [&] {
-          k_bwd_tiny<T><<<dim3((unsigned)((s.count + kTinyWarps - 1) / kTinyWarps), (unsigned)((R + 31) / 32)),
-                          32 * kTinyWarps, 0, ss>>>(h->dp, A, ids + s.first, (int)s.count, pool, fsol, xw);
+          k_bwd_tiny<T><<<dim3((unsigned)((s.count + tiny_warps<T>() - 1) / tiny_warps<T>()), (unsigned)((R + 31) / 32)),
+                          32 * tiny_warps<T>(), 0, ss>>>(h->dp, A, ids + s.first, (int)s.count, pool, fsol, xw);
         });
         break;
       case 4:
@@ -1239,7 +1287,7 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
   }
   fork.join();
   }
-  klaunch(h, KC_SOLVE_FINISH, 0, (double)P.n * R * (sizeof(T) + 8.0 * (1 + accumulate)), [&] {
+  klaunch(h, KC_SOLVE_FINISH, 0, (double)P.n * R * (sizeof(T) + sizeof(Wide<T>) * (1.0 + accumulate)), [&] {
     k_solve_finish<T><<<grid1(P.n * R, 256), 256, 0, st>>>(P.n, R, h->b_qf.as<int32_t>(), xw, P.n, d_x, ldx,
                                                            accumulate);
   });
@@ -1247,7 +1295,7 @@ void solve_once(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double*
 }
 
 template <typename T>
-void solve_refine(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double* d_x, int64_t ldx, int refine,
+void solve_refine(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T>* d_x, int64_t ldx, int refine,
                   bool use_rs) {
   const Plan& P = h->plan;
   cudaStream_t st = h->stream;
@@ -1255,12 +1303,18 @@ void solve_refine(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, doubl
   CK(cudaMemsetAsync(h->b_flags.as<int>() + 1, 0, sizeof(int), st));   // this solve's timeout flag
   solve_once<T>(h, R, d_b, ldb, d_x, ldx, use_rs, 0);
   if (refine > 0) {
-    double* r = h->b_r.as<double>();
+    Wide<T>* r = h->b_r.as<Wide<T>>();
     for (int it = 0; it < refine; ++it) {
-      klaunch(h, KC_RESIDUAL, 2.0 * P.nnz_a * R, 16.0 * P.nnz_a + 24.0 * P.n * R, [&] {
-        k_residual<<<grid1(P.n * R, 256), 256, 0, st>>>(P.n, R, h->b_csr_ptr.as<int32_t>(),
-                                                        h->b_csr_col.as<int32_t>(), h->b_csr_src.as<int32_t>(),
-                                                        h->b_ax.as<double>(), d_b, ldb, d_x, ldx, r, P.n);
+      klaunch(h, KC_RESIDUAL, 2.0 * P.nnz_a * R, (8.0 + sizeof(Wide<T>)) * P.nnz_a + 3.0 * sizeof(Wide<T>) * P.n * R,
+              [&] {
+        if constexpr (is_complex_v<T>)
+          k_residual_z<<<grid1(P.n * R, 256), 256, 0, st>>>(P.n, R, h->b_csr_ptr.as<int32_t>(),
+                                                            h->b_csr_col.as<int32_t>(), h->b_csr_src.as<int32_t>(),
+                                                            h->b_ax.as<zc>(), d_b, ldb, d_x, ldx, r, P.n);
+        else
+          k_residual<<<grid1(P.n * R, 256), 256, 0, st>>>(P.n, R, h->b_csr_ptr.as<int32_t>(),
+                                                          h->b_csr_col.as<int32_t>(), h->b_csr_src.as<int32_t>(),
+                                                          h->b_ax.as<double>(), d_b, ldb, d_x, ldx, r, P.n);
       });
       solve_once<T>(h, R, r, P.n, d_x, ldx, use_rs, 1);
     }
@@ -1269,7 +1323,7 @@ void solve_refine(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, doubl
 }
 
 template <typename T>
-void solve_graph(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double* d_x, int64_t ldx, int refine) {
+void solve_graph(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T>* d_x, int64_t ldx, int refine) {
   prepare_solve<T>(h, R, refine);
   const SolveSchedule& S = h->sched;
   const std::vector<uintptr_t> key = {
@@ -1311,6 +1365,7 @@ int solve_status(mfgpu_ctx* h) {
 }
 
 void solve_dispatch(mfgpu_ctx* h, int64_t R, const double* d_b, int64_t ldb, double* d_x, int64_t ldx, int refine) {
+  if (h->c64_factors) throw std::invalid_argument("the factorization is complex: use mfgpu_solve_c64");
   if (h->factor_precision == MFGPU_PRECISION_MIXED) solve_graph<float>(h, R, d_b, ldb, d_x, ldx, refine);
   else solve_graph<double>(h, R, d_b, ldb, d_x, ldx, refine);
 }
@@ -1470,6 +1525,21 @@ int mfgpu_set_wait_limit(mfgpu_ctx* h, double seconds) {
   return MFGPU_OK;
 }
 
+int mfgpu_test_stall(mfgpu_ctx* h, int32_t on) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->device));
+    if (!h->b_flags.p) {
+      h->b_flags.ensure(16);
+      CK(cudaMemsetAsync(h->b_flags.p, 0, 16, h->stream));
+    }
+    const int v = on ? 1 : 0;
+    CK(cudaMemcpyAsync(h->b_flags.as<int>() + 2, &v, sizeof v, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MFGPU_OK;
+  });
+}
+
 int mfgpu_set_precision(mfgpu_ctx* h, int32_t p) {
   if (!h || (p != MFGPU_PRECISION_FP64 && p != MFGPU_PRECISION_MIXED)) return MFGPU_ERR_ARGUMENT;
   h->precision = p;
@@ -1522,7 +1592,7 @@ int mfgpu_factor_device(mfgpu_ctx* h, const double* d_nzval, const double* d_rs,
   if (!h->analyzed) return fail(h, MFGPU_ERR_STATE, "factor before analyze");
   if (h->plan.nnz_a && !d_nzval) return fail(h, MFGPU_ERR_ARGUMENT, "null values");
   h->factored = h->csc_ready = false;
-  h->f32_values = false;
+  h->f32_values = h->c64_values = false;
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->device));
     const Plan& P = h->plan;
@@ -1540,7 +1610,7 @@ int mfgpu_factor_device(mfgpu_ctx* h, const double* d_nzval, const double* d_rs,
 int mfgpu_factor_scaled(mfgpu_ctx* h, const double* nzval, int32_t scale, int32_t check) {
   if (!h) return MFGPU_ERR_ARGUMENT;
   if (!h->analyzed) return fail(h, MFGPU_ERR_STATE, "factor before analyze");
-  h->f32_values = false;
+  h->f32_values = h->c64_values = false;
   if (scale < MFGPU_SCALE_NONE || scale > MFGPU_SCALE_MAX) return fail(h, MFGPU_ERR_ARGUMENT, "bad scale kind");
   if (h->plan.nnz_a && !nzval) return fail(h, MFGPU_ERR_ARGUMENT, "null values");
   h->factored = h->csc_ready = false;
@@ -1576,19 +1646,23 @@ int mfgpu_get_row_scaling(mfgpu_ctx* h, double* rs) {
   });
 }
 
-// Host values (FP64, or Float32 values widened) -> factorization.
-static int factor_host(mfgpu_ctx* h, const double* nzval, const double* rs, int32_t check, bool f32) {
+// Host values (FP64, Float32 values widened, or ComplexF64 as interleaved
+// (re, im) doubles) -> factorization.
+static int factor_host(mfgpu_ctx* h, const double* nzval, const double* rs, int32_t check, bool f32,
+                       bool c64 = false) {
   if (!h) return MFGPU_ERR_ARGUMENT;
   if (!h->analyzed) return fail(h, MFGPU_ERR_STATE, "factor before analyze");
   if (h->plan.nnz_a && !nzval) return fail(h, MFGPU_ERR_ARGUMENT, "null values");
   // the previous factors stop being valid once A's values are overwritten
   h->factored = h->csc_ready = false;
   h->f32_values = f32;
+  h->c64_values = c64;
+  const int64_t vb = c64 ? 16 : 8;
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->device));
     const Plan& P = h->plan;
-    h->b_ax.ensure(std::max<int64_t>(P.nnz_a, 1) * 8);
-    if (P.nnz_a) CK(cudaMemcpyAsync(h->b_ax.p, nzval, P.nnz_a * 8, cudaMemcpyHostToDevice, h->stream));
+    h->b_ax.ensure(std::max<int64_t>(P.nnz_a, 1) * vb);
+    if (P.nnz_a) CK(cudaMemcpyAsync(h->b_ax.p, nzval, P.nnz_a * vb, cudaMemcpyHostToDevice, h->stream));
     h->have_rs = rs != nullptr;
     if (rs) {
       h->b_rs.ensure(std::max<int64_t>(P.n, 1) * 8);
@@ -1632,6 +1706,7 @@ int mfgpu_get_factors_f32(mfgpu_ctx* h, int64_t* lcolptr, int64_t* lrowval, floa
 int mfgpu_solve_f32(mfgpu_ctx* h, int64_t nrhs, const float* b, float* x, int32_t refine) {
   if (!h) return MFGPU_ERR_ARGUMENT;
   if (!h->factored) return fail(h, MFGPU_ERR_STATE, "solve before factor");
+  if (h->c64_factors) return fail(h, MFGPU_ERR_STATE, "the factorization is complex: use mfgpu_solve_c64");
   const int64_t n = h->plan.n;
   if (nrhs < 0 || refine < 0 || (nrhs && n && (!b || !x))) return fail(h, MFGPU_ERR_ARGUMENT, "bad solve sizes");
   if (nrhs == 0 || n == 0) return MFGPU_OK;
@@ -1664,18 +1739,23 @@ int mfgpu_factor_sizes(mfgpu_ctx* h, int64_t* out3) {
   return MFGPU_OK;
 }
 
-int mfgpu_get_factors(mfgpu_ctx* h, int64_t* lcolptr, int64_t* lrowval, double* lnzval, int64_t* ucolptr,
-                      int64_t* urowval, double* unzval, int64_t* p, int64_t* q, int64_t* pinv) {
+// The CSC factors of the last factorization into host buffers; vbytes is
+// the size of one value (8, or 16 for ComplexF64 factors).
+static int get_factors_impl(mfgpu_ctx* h, int64_t* lcolptr, int64_t* lrowval, void* lnzval, int64_t* ucolptr,
+                            int64_t* urowval, void* unzval, int64_t* p, int64_t* q, int64_t* pinv, int64_t vbytes) {
   if (!h) return MFGPU_ERR_ARGUMENT;
   if (!h->factored) return fail(h, MFGPU_ERR_STATE, "no factorization");
+  if (h->c64_factors != (vbytes == 16))
+    return fail(h, MFGPU_ERR_STATE, h->c64_factors ? "the factorization is complex: use mfgpu_get_factors_c64"
+                                                   : "the factorization is not complex: use mfgpu_get_factors");
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->device));
     const Plan& P = h->plan;
     cudaStream_t st = h->stream;
     if (lrowval && P.nnz_l) CK(cudaMemcpyAsync(lrowval, h->b_li.p, P.nnz_l * 8, cudaMemcpyDeviceToHost, st));
-    if (lnzval && P.nnz_l) CK(cudaMemcpyAsync(lnzval, h->b_lx.p, P.nnz_l * 8, cudaMemcpyDeviceToHost, st));
+    if (lnzval && P.nnz_l) CK(cudaMemcpyAsync(lnzval, h->b_lx.p, P.nnz_l * vbytes, cudaMemcpyDeviceToHost, st));
     if (urowval && P.nnz_u) CK(cudaMemcpyAsync(urowval, h->b_ui.p, P.nnz_u * 8, cudaMemcpyDeviceToHost, st));
-    if (unzval && P.nnz_u) CK(cudaMemcpyAsync(unzval, h->b_ux.p, P.nnz_u * 8, cudaMemcpyDeviceToHost, st));
+    if (unzval && P.nnz_u) CK(cudaMemcpyAsync(unzval, h->b_ux.p, P.nnz_u * vbytes, cudaMemcpyDeviceToHost, st));
     std::vector<int32_t> prow(P.n);
     if (P.n) CK(cudaMemcpyAsync(prow.data(), h->b_prow.p, P.n * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -1694,10 +1774,52 @@ int mfgpu_get_factors(mfgpu_ctx* h, int64_t* lcolptr, int64_t* lrowval, double* 
   });
 }
 
+int mfgpu_get_factors(mfgpu_ctx* h, int64_t* lcolptr, int64_t* lrowval, double* lnzval, int64_t* ucolptr,
+                      int64_t* urowval, double* unzval, int64_t* p, int64_t* q, int64_t* pinv) {
+  return get_factors_impl(h, lcolptr, lrowval, lnzval, ucolptr, urowval, unzval, p, q, pinv, 8);
+}
+
+int mfgpu_factor_c64(mfgpu_ctx* h, const double* nzval_ri, const double* rs, int32_t check) {
+  return factor_host(h, nzval_ri, rs, check, false, true);
+}
+
+int mfgpu_get_factors_c64(mfgpu_ctx* h, int64_t* lcolptr, int64_t* lrowval, double* lnzval_ri, int64_t* ucolptr,
+                          int64_t* urowval, double* unzval_ri, int64_t* p, int64_t* q, int64_t* pinv) {
+  return get_factors_impl(h, lcolptr, lrowval, lnzval_ri, ucolptr, urowval, unzval_ri, p, q, pinv, 16);
+}
+
+int mfgpu_solve_c64(mfgpu_ctx* h, int64_t nrhs, const double* b_ri, double* x_ri, int32_t refine) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  if (!h->factored) return fail(h, MFGPU_ERR_STATE, "solve before factor");
+  if (!h->c64_factors) return fail(h, MFGPU_ERR_STATE, "the factorization is not complex: use mfgpu_solve");
+  const int64_t n = h->plan.n;
+  if (nrhs < 0 || refine < 0 || (nrhs && n && (!b_ri || !x_ri))) return fail(h, MFGPU_ERR_ARGUMENT, "bad solve sizes");
+  if (nrhs == 0 || n == 0) return MFGPU_OK;
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    const int64_t len = n * nrhs;
+    h->b_b.ensure((size_t)len * 16);
+    h->b_x.ensure((size_t)len * 16);
+    CK(cudaMemcpyAsync(h->b_b.p, b_ri, len * 16, cudaMemcpyHostToDevice, st));
+    CK(cudaEventRecord(h->ev0, st));
+    solve_graph<zc>(h, nrhs, h->b_b.as<zc>(), n, h->b_x.as<zc>(), n, refine);
+    CK(cudaEventRecord(h->ev1, st));
+    CK(cudaMemcpyAsync(x_ri, h->b_x.p, len * 16, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->t_solve_ms = ms;
+    prof_flush(h);
+    return solve_status(h);
+  });
+}
+
 int mfgpu_solve_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ldb, double* d_x, int64_t ldx,
                        int32_t refine) {
   if (!h) return MFGPU_ERR_ARGUMENT;
   if (!h->factored) return fail(h, MFGPU_ERR_STATE, "solve before factor");
+  if (h->c64_factors) return fail(h, MFGPU_ERR_STATE, "the factorization is complex: use mfgpu_solve_c64");
   if (nrhs < 0 || ldb < h->plan.n || ldx < h->plan.n || refine < 0 || (nrhs && h->plan.n && (!d_b || !d_x)))
     return fail(h, MFGPU_ERR_ARGUMENT, "bad solve sizes");
   if (nrhs == 0 || h->plan.n == 0) return MFGPU_OK;
@@ -1718,6 +1840,7 @@ int mfgpu_solve_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ld
 int mfgpu_solve(mfgpu_ctx* h, int64_t nrhs, const double* b, int64_t ldb, double* x, int64_t ldx, int32_t refine) {
   if (!h) return MFGPU_ERR_ARGUMENT;
   if (!h->factored) return fail(h, MFGPU_ERR_STATE, "solve before factor");
+  if (h->c64_factors) return fail(h, MFGPU_ERR_STATE, "the factorization is complex: use mfgpu_solve_c64");
   const int64_t n = h->plan.n;
   if (nrhs < 0 || ldb < n || ldx < n || refine < 0 || (nrhs && (!b || !x)))
     return fail(h, MFGPU_ERR_ARGUMENT, "bad solve sizes");
@@ -1740,6 +1863,7 @@ int mfgpu_backward_error_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, i
                                 int64_t ldx, double* out) {
   if (!h || !out) return MFGPU_ERR_ARGUMENT;
   if (!h->factored) return fail(h, MFGPU_ERR_STATE, "no matrix values");
+  if (h->c64_factors) return fail(h, MFGPU_ERR_STATE, "real vectors only: the factorization is complex");
   if (nrhs < 1 || h->plan.n == 0) {
     *out = 0.0;
     return MFGPU_OK;
@@ -2020,6 +2144,7 @@ extern "C" int mfgpu_backward_error_noalloc(mfgpu_ctx* h, int64_t nrhs, const do
                                             const double* d_x, int64_t ldx, double* out) {
   if (!h || !out) return MFGPU_ERR_ARGUMENT;
   if (!h->factored) return fail(h, MFGPU_ERR_STATE, "no matrix values (factor first)");
+  if (h->c64_factors) return fail(h, MFGPU_ERR_STATE, "real vectors only: the factorization is complex");
   if (nrhs < 1 || nrhs > kNoAllocMaxRhs)
     return fail(h, MFGPU_ERR_ARGUMENT, "mfgpu_backward_error_noalloc: nrhs must be in 1.." +
                                            std::to_string(kNoAllocMaxRhs));

@@ -45,6 +45,7 @@ SIGNATURES = [
     ("mfgpu_set_precision", ctypes.c_int, [vp, i32]),
     ("mfgpu_set_growth_limit", ctypes.c_int, [vp, f64]),
     ("mfgpu_set_wait_limit", ctypes.c_int, [vp, f64]),
+    ("mfgpu_test_stall", ctypes.c_int, [vp, ctypes.c_int32]),
     ("mfgpu_analyze", ctypes.c_int, [vp, i64, i64p, i64p, i64p, i64p, i64, i64p, i64p, i64p]),
     ("mfgpu_analyze_symbolic", ctypes.c_int, [vp, i64, i64p, i64p, vp]),
     ("mfgpu_factor", ctypes.c_int, [vp, f64p, f64p, i32]),
@@ -56,6 +57,9 @@ SIGNATURES = [
     ("mfgpu_factor_f32", ctypes.c_int, [vp, f32p, f32p, i32]),
     ("mfgpu_get_factors_f32", ctypes.c_int, [vp, i64p, i64p, f32p, i64p, i64p, f32p, i64p, i64p, i64p]),
     ("mfgpu_solve_f32", ctypes.c_int, [vp, i64, f32p, f32p, i32]),
+    ("mfgpu_factor_c64", ctypes.c_int, [vp, f64p, f64p, i32]),
+    ("mfgpu_get_factors_c64", ctypes.c_int, [vp, i64p, i64p, f64p, i64p, i64p, f64p, i64p, i64p, i64p]),
+    ("mfgpu_solve_c64", ctypes.c_int, [vp, i64, f64p, f64p, i32]),
     ("mfgpu_solve", ctypes.c_int, [vp, i64, f64p, i64, f64p, i64, i32]),
     ("mfgpu_solve_device", ctypes.c_int, [vp, i64, vp, i64, vp, i64, i32]),
     ("mfgpu_backward_error_device", ctypes.c_int, [vp, i64, vp, i64, vp, i64, f64p]),

@@ -78,6 +78,11 @@ def _i(a):
     return np.ascontiguousarray(a, dtype=np.int64)
 
 
+def _z(a):
+    """ComplexF64 values as interleaved (re, im) doubles (Julia's layout)."""
+    return np.ascontiguousarray(a, dtype=np.complex128).view(np.float64)
+
+
 def _f(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
@@ -103,6 +108,11 @@ def row_scaling(A: SparseCSC, kind: ScaleKind) -> np.ndarray:
         elif kind == SCALE_MAX:
             np.maximum.at(acc, A.rowval - 1, np.abs(A.nzval))
         return np.where(acc > 0, 1.0 / np.where(acc > 0, acc, 1.0), 1.0) if kind != SCALE_NONE else np.ones(A.m)
+    if np.iscomplexobj(A.nzval):      # ComplexF64 matrix: Float64 Rs from |z| (R = real(Tv))
+        rs = np.empty(A.n)
+        _check_host(L.lib().mfgpu_row_scaling_c64(A.n, L.ptr(_i(A.colptr)), L.ptr(_i(A.rowval)),
+                                                  L.ptr(_z(A.nzval), L.f64p), int(kind), L.ptr(rs, L.f64p)))
+        return rs
     if A.nzval.dtype == np.float32:   # Float32 matrix: Float32 arithmetic (R = real(Tv))
         rs = np.empty(A.n, np.float32)
         _check_host(L.lib().mfgpu_row_scaling_f32(A.n, L.ptr(_i(A.colptr)), L.ptr(_i(A.rowval)),
@@ -266,6 +276,7 @@ class GpuContext:
         self.n = 0
         self.precision = precision
         self.f32 = False   # the last factorization is of a Float32 matrix
+        self.c64 = False   # the last factorization is of a ComplexF64 matrix
 
     def _check(self, rc: int):
         if rc < 0:
@@ -291,6 +302,10 @@ class GpuContext:
         4 s); a wait that runs out makes the call raise MfgpuError(-5)."""
         self._check(self._lib.mfgpu_set_wait_limit(self._h, ctypes.c_double(seconds)))
 
+    def test_stall(self, on: bool):
+        """Test hook: the kernels' bounded waits run out (mfgpu_test_stall)."""
+        self._check(self._lib.mfgpu_test_stall(self._h, int(bool(on))))
+
     def set_stream(self, stream_ptr: int):
         self._check(self._lib.mfgpu_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
 
@@ -311,15 +326,22 @@ class GpuContext:
 
     def factor(self, nzval, Rs=None, check: bool = True) -> int:
         rs = _f(Rs) if Rs is not None else None
-        self.f32 = False
+        self.f32 = self.c64 = False
         return self._check(self._lib.mfgpu_factor(self._h, L.ptr(_f(nzval), L.f64p), L.ptr(rs, L.f64p), int(check)))
 
     def factor_f32(self, nzval, Rs=None, check: bool = True) -> int:
         """Factorization of a Float32 matrix: Float32 fronts, Float32 factors."""
         v = np.ascontiguousarray(nzval, dtype=np.float32)
         rs = np.ascontiguousarray(Rs, dtype=np.float32) if Rs is not None else None
-        self.f32 = True
+        self.f32, self.c64 = True, False
         return self._check(self._lib.mfgpu_factor_f32(self._h, L.ptr(v, L.f32p), L.ptr(rs, L.f32p), int(check)))
+
+    def factor_c64(self, nzval, Rs=None, check: bool = True) -> int:
+        """Factorization of a ComplexF64 matrix: complex fronts, complex factors."""
+        rs = _f(Rs) if Rs is not None else None
+        self.f32, self.c64 = False, True
+        return self._check(self._lib.mfgpu_factor_c64(self._h, L.ptr(_z(nzval), L.f64p), L.ptr(rs, L.f64p),
+                                                      int(check)))
 
     def factor_scaled(self, nzval, scale, check: bool = True) -> int:
         """Row scaling of kind ``scale`` computed on the device, then the
@@ -343,6 +365,8 @@ class GpuContext:
 
     def factors(self):
         n, nl, nu = self.sizes()
+        if getattr(self, "c64", False):
+            return self._factors_c64(n, nl, nu)
         f32 = getattr(self, "f32", False)
         dt, vp = (np.float32, L.f32p) if f32 else (np.float64, L.f64p)
         Lp = np.empty(n + 1, np.int64)
@@ -359,7 +383,25 @@ class GpuContext:
                         L.ptr(q), L.ptr(pinv)))
         return SparseCSC(n, n, Lp, Li, Lx), SparseCSC(n, n, Up, Ui, Ux), p, q, pinv
 
+    def _factors_c64(self, n, nl, nu):
+        Lp, Li, Lx = np.empty(n + 1, np.int64), np.empty(nl, np.int64), np.empty(nl, np.complex128)
+        Up, Ui, Ux = np.empty(n + 1, np.int64), np.empty(nu, np.int64), np.empty(nu, np.complex128)
+        p, q, pinv = np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.int64)
+        self._check(self._lib.mfgpu_get_factors_c64(self._h, L.ptr(Lp), L.ptr(Li), L.ptr(Lx.view(np.float64), L.f64p),
+                                                    L.ptr(Up), L.ptr(Ui), L.ptr(Ux.view(np.float64), L.f64p),
+                                                    L.ptr(p), L.ptr(q), L.ptr(pinv)))
+        return SparseCSC(n, n, Lp, Li, Lx), SparseCSC(n, n, Up, Ui, Ux), p, q, pinv
+
     def solve(self, b, refine: int = 0) -> np.ndarray:
+        if getattr(self, "c64", False):
+            B = np.asfortranarray(b, dtype=np.complex128)
+            X = np.empty_like(B)
+            nrhs = 1 if B.ndim == 1 else B.shape[1]
+            self._check(self._lib.mfgpu_solve_c64(self._h, nrhs, L.ptr(B.reshape(-1, order="F").view(np.float64),
+                                                                       L.f64p),
+                                                  L.ptr(X.reshape(-1, order="F").view(np.float64), L.f64p),
+                                                  int(refine)))
+            return X
         if getattr(self, "f32", False):
             B = np.asfortranarray(b, dtype=np.float32)
             X = np.empty_like(B)
@@ -480,8 +522,10 @@ def _factor(A: SparseCSC, q, check: bool, Rs, device: int, precision: int, relax
     S = symbolic_mf(A, q=q, relax=relax)
     ctx = GpuContext(device=device, precision=precision)
     ctx.analyze(A, S)
-    # a Float32 matrix is factored in Float32 (the reference's generic Tv)
-    fac = ctx.factor_f32 if A.nzval.dtype == np.float32 else ctx.factor
+    # a Float32 (ComplexF64) matrix is factored in Float32 (ComplexF64), the
+    # reference's generic Tv
+    fac = (ctx.factor_c64 if np.iscomplexobj(A.nzval) else
+           ctx.factor_f32 if A.nzval.dtype == np.float32 else ctx.factor)
     status = fac(A.nzval, Rs, check)
     if status > 0:
         raise SingularException(status)
@@ -638,7 +682,8 @@ def solve(F, b, refine: int = 0) -> np.ndarray:
         if refine:
             raise ArgumentError("refinement needs a PureLU (it keeps A and Rs)")
         return F.ldiv(b)
-    b = np.asarray(b, dtype=np.float32 if F.A.nzval.dtype == np.float32 else np.float64)
+    dt = np.complex128 if np.iscomplexobj(F.A.nzval) else (np.float32 if F.A.nzval.dtype == np.float32 else np.float64)
+    b = np.asarray(b, dtype=dt)
     if b.shape[0] != F.A.n:
         raise DimensionMismatch("length(b) must equal size(F, 1)")
     return F.ctx.solve(b, refine)

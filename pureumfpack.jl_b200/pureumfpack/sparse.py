@@ -20,7 +20,8 @@ class SparseCSC:
         self.colptr = np.ascontiguousarray(colptr, dtype=np.int64)
         self.rowval = np.ascontiguousarray(rowval, dtype=np.int64)
         nzval = np.asarray(nzval)
-        self.nzval = np.ascontiguousarray(nzval, dtype=np.float32 if nzval.dtype == np.float32 else np.float64)
+        dt = np.float32 if nzval.dtype == np.float32 else (np.complex128 if np.iscomplexobj(nzval) else np.float64)
+        self.nzval = np.ascontiguousarray(nzval, dtype=dt)
         if self.colptr.shape != (self.n + 1,):
             raise ValueError("colptr must have n+1 entries")
         if self.colptr[0] != 1 or self.colptr[-1] - 1 != len(self.rowval) or len(self.rowval) != len(self.nzval):
@@ -56,8 +57,9 @@ class SparseCSC:
         S = S.tocsc()
         S.sort_indices()
         S.sum_duplicates()
+        dt = np.float32 if S.dtype == np.float32 else (np.complex128 if np.iscomplexobj(S.data) else np.float64)
         return SparseCSC(S.shape[0], S.shape[1], S.indptr.astype(np.int64) + 1, S.indices.astype(np.int64) + 1,
-                         S.data.astype(np.float32 if S.dtype == np.float32 else np.float64))
+                         S.data.astype(dt))
 
     def to_scipy(self):
         import scipy.sparse as sp
@@ -71,11 +73,11 @@ class SparseCSC:
 
     @property
     def eltype(self):
-        """Element type of the stored values (numpy float64 or float32)."""
+        """Element type of the stored values (numpy float64, float32 or complex128)."""
         return self.nzval.dtype.type
 
     def astype(self, dtype) -> "SparseCSC":
-        """Copy with values converted to ``dtype`` (Float64 or Float32)."""
+        """Copy with values converted to ``dtype`` (Float64, Float32 or ComplexF64)."""
         return SparseCSC(self.m, self.n, self.colptr.copy(), self.rowval.copy(), self.nzval.astype(dtype))
 
     def nnz(self) -> int:
