@@ -504,7 +504,17 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
 #pragma unroll
         for (int q = 0; q < 8; ++q) A[(s8 + lane) + (s8 + q) * kLdS] = a[q];
       }
-      __syncwarp();
+      // the factored 8 x 8 block to every lane's registers (row i from lane
+      // i), and the reciprocals of its pivots, for the triangular inverses:
+      // no shared-memory loads or divisions inside their dependent chains
+      T blk[8][8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) blk[i][q] = __shfl_sync(0xffffffffu, a[q], i);
+      T rd[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) rd[i] = T(1) / blk[i][i];
       if (lane < 8) {          // column `lane` of inv(L_ss)
         const int c = lane;
         T x[8];
@@ -514,7 +524,7 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
         for (int i = 1; i < 8; ++i) {
           T v = x[i];
 #pragma unroll
-          for (int k = 0; k < i; ++k) v -= A[(s8 + i) + (s8 + k) * kLdS] * x[k];
+          for (int k = 0; k < i; ++k) v -= blk[i][k] * x[k];
           x[i] = (i > c) ? v : x[i];
         }
 #pragma unroll
@@ -528,8 +538,8 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
         for (int i = 7; i >= 0; --i) {
           T v = (i == c) ? T(1) : T(0);
 #pragma unroll
-          for (int k = i + 1; k < 8; ++k) v -= A[(s8 + i) + (s8 + k) * kLdS] * x[k];
-          x[i] = (i <= c) ? v / A[(s8 + i) + (s8 + i) * kLdS] : T(0);
+          for (int k = i + 1; k < 8; ++k) v -= blk[i][k] * x[k];
+          x[i] = (i <= c) ? v * rd[i] : T(0);
         }
 #pragma unroll
         for (int i = 0; i < 8; ++i) Ui[(s8 + i) + (s8 + c) * kLdS] = x[i];

@@ -26,12 +26,6 @@ namespace mfgpu {
 
 constexpr int kSolveCols = 32;      // right-hand sides per CTA in the small-supernode kernels
 constexpr int kSolveThreads = 128;
-// Thin large supernodes -- few pivots over a front of moderate height, the
-// bulk of the lower tree levels -- are solved by the small-supernode
-// substitution kernels too: as batched GEMMs their tasks fill a few rows of
-// each 64 x 64 (or 128 x 128) tile and need separate gather launches.
-constexpr int kThinPivots = 32;
-constexpr int kThinFront = 256;
 // Right-hand sides per small-supernode CTA for fronts of type T: half as
 // many for ComplexF64, whose blocks take twice the shared memory.
 template <typename T>
@@ -130,16 +124,12 @@ __device__ __forceinline__ void fwd_small_item(const DevPlan& P, const DevState&
   __syncthreads();
 }
 
-// One CTA per (supernode, column chunk); dynamic shared memory: the step's
-// largest front rows x solve_cols<T>() elements.  Besides the small fronts
-// (nf <= kSmallFront) a step may hold thin large supernodes (np <=
-// kThinPivots, nf <= kThinFront): their solve is the same substitution.
 template <typename T>
 __global__ void __launch_bounds__(kSolveThreads) k_fwd_small(DevPlan P, DevState S, SolveArgs A,
                                                              const int32_t* __restrict__ tasks,
                                                              const T* __restrict__ pool, T* fsol) {
-  extern __shared__ __align__(16) unsigned char fwd_smem[];
-  fwd_small_item<T>(P, S, A, tasks, pool, fsol, blockIdx.x, blockIdx.y, reinterpret_cast<T*>(fwd_smem));
+  __shared__ T f[kSmallFront * solve_cols<T>()];
+  fwd_small_item<T>(P, S, A, tasks, pool, fsol, blockIdx.x, blockIdx.y, f);
 }
 
 // Tiny supernodes (nf <= kTinyFront), the bulk of the leaf levels: one warp
@@ -296,13 +286,12 @@ __global__ void __launch_bounds__(256) k_fwd_assemble(DevPlan P, DevState S, Sol
   fwd_assemble_item<T>(P, S, A, tasks, fsol, blockIdx.x, blockIdx.y);
 }
 
-// Small supernodes, backward.  smem: y (np x columns) then g (nu x columns);
-// g starts `goff` elements after y.
+// Small supernodes, backward.  smem: 2 * kSmallFront * kSolveCols elements.
 template <typename T>
 __device__ __forceinline__ void bwd_small_item(const DevPlan& P, const SolveArgs& A,
                                                const int32_t* __restrict__ tasks, const T* __restrict__ pool,
-                                               const T* fsol, T* xw, int bx, int by, T* y, int goff) {
-  T* g = y + goff;
+                                               const T* fsol, T* xw, int bx, int by, T* y) {
+  T* g = y + kSmallFront * solve_cols<T>();
   const int s = tasks[bx];
   const int c0 = by * solve_cols<T>();
   const int rc = min(solve_cols<T>(), (int)(A.nrhs - c0));
@@ -346,14 +335,11 @@ __device__ __forceinline__ void bwd_small_item(const DevPlan& P, const SolveArgs
   __syncthreads();
 }
 
-// Dynamic shared memory: (pivots + update rows) x solve_cols<T>() elements;
-// `goff` = the step's largest pivot count x solve_cols<T>().
 template <typename T>
 __global__ void __launch_bounds__(kSolveThreads) k_bwd_small(DevPlan P, SolveArgs A, const int32_t* __restrict__ tasks,
-                                                             const T* __restrict__ pool, const T* fsol, T* xw,
-                                                             int goff) {
-  extern __shared__ __align__(16) unsigned char bwd_smem[];
-  bwd_small_item<T>(P, A, tasks, pool, fsol, xw, blockIdx.x, blockIdx.y, reinterpret_cast<T*>(bwd_smem), goff);
+                                                             const T* __restrict__ pool, const T* fsol, T* xw) {
+  __shared__ T y[2 * kSmallFront * solve_cols<T>()];
+  bwd_small_item<T>(P, A, tasks, pool, fsol, xw, blockIdx.x, blockIdx.y, y);
 }
 
 // Large supernodes: gather x of the update columns into the w rows.

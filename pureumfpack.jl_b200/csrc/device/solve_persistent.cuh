@@ -135,9 +135,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_persistent(DevPlan P, D
       switch (ph.kind) {
         case kPhFwdSmall: fwd_small_item<T>(P, S, A, X.ids + ph.first, pool, fsol, bx, by, sm); break;
         case kPhFwdAssemble: fwd_assemble_item<T>(P, S, A, X.ids + ph.first, fsol, bx, by); break;
-        case kPhBwdSmall:
-          bwd_small_item<T>(P, A, X.ids + ph.first, pool, fsol, xw, bx, by, sm, kSmallFront * kSolveCols);
-          break;
+        case kPhBwdSmall: bwd_small_item<T>(P, A, X.ids + ph.first, pool, fsol, xw, bx, by, sm); break;
         case kPhBwdGather: bwd_gather_item<T>(P, A, X.ids + ph.first, fsol, xw, bx, by); break;
         default: break;
       }

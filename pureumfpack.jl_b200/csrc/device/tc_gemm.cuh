@@ -482,15 +482,16 @@ __global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __re
     const int arow = t & 127, ak = (t >> 7) * 32;
     const int row = m0 + arow;
     constexpr int kBPer = BN * (BK / 8) / kBxProducers;   // (column, 8-chunk) pairs per thread
-    for (int kb = 0; kb < nk; ++kb) {
-      const int s = kb % STAGES, k0 = kb * BK;
-      float va[32];
+    // Software pipeline over K blocks: the global loads of block kb + 1 are
+    // issued before block kb is split and stored, so their latency hides
+    // behind that work and the wait for a free stage (two register buffers).
+    auto load = [&](int kb, float (&va)[32], float (&vb)[kBPer][8]) {
+      const int k0 = kb * BK;
 #pragma unroll
       for (int k = 0; k < 32; ++k) {
         const int kk = k0 + ak + k;
         va[k] = (row < M && kk < K) ? A[(int64_t)row + (int64_t)kk * tk.lda] : 0.0f;
       }
-      float vb[kBPer][8];
 #pragma unroll
       for (int i = 0; i < kBPer; ++i) {
         const int idx = t + i * kBxProducers, n = idx >> 3, c = idx & 7;
@@ -500,9 +501,13 @@ __global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __re
           vb[i][j] = (n0 + n < N && kk < K) ? B[(int64_t)kk + (int64_t)(n0 + n) * tk.ldb] : 0.0f;
         }
       }
+    };
+    // wait for a free stage, split and store block kb, mark the stage full
+    auto produce = [&](int kb, const float (&va)[32], const float (&vb)[kBPer][8]) -> bool {
+      const int s = kb % STAGES;
       if (kb >= STAGES && !mbar_wait(&empty[s], (uint32_t)((kb / STAGES - 1) & 1), wait_ns)) {
         failed = 1;
-        break;
+        return false;
       }
       const uint32_t st = sbase + s * Cfg::kStageBytes;
 #pragma unroll
@@ -516,7 +521,15 @@ __global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __re
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(&full[s]);
-      if (failed) break;
+      return !failed;
+    };
+    float va0[32], vb0[kBPer][8], va1[32], vb1[kBPer][8];
+    if (nk > 0) load(0, va0, vb0);
+    for (int kb = 0; kb < nk; kb += 2) {
+      if (kb + 1 < nk) load(kb + 1, va1, vb1);
+      if (!produce(kb, va0, vb0) || kb + 1 >= nk) break;
+      if (kb + 2 < nk) load(kb + 2, va0, vb0);
+      if (!produce(kb + 1, va1, vb1)) break;
     }
   } else if (lane == 0) {
     if (flags[2] && !mbar_wait(&stall, 0u, wait_ns)) failed = 1;   // test hook: a wait that runs out

@@ -111,7 +111,6 @@ struct SolveSchedule {
     int64_t tiles_tc = 0;   // GEMM steps: grid in 128 x 128 tensor-core tiles (gemms_tc)
     int64_t sk_first = 0, sk_count = 0, sk_parts = 0, sk_reds = 0;   // split-K form (few rhs)
     int32_t level = -1;     // tree level (small-supernode steps run beside the level's large ones)
-    int32_t nf_max = 0, np_max = 0;   // small-supernode steps: largest front and pivot block (shared memory)
   };
   std::vector<Step> steps;
   std::vector<int32_t> ids;
@@ -510,11 +509,6 @@ template <typename T>
 void configure_kernels() {
   static bool done = false;
   if (done) return;
-  CK(cudaFuncSetAttribute(k_fwd_small<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)(kThinFront * solve_cols<T>() * sizeof(T))));
-  // y of up to kSmallFront pivots (small fronts) and g of up to kThinFront rows
-  CK(cudaFuncSetAttribute(k_bwd_small<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)((kSmallFront + kThinFront) * solve_cols<T>() * sizeof(T))));
   if constexpr (is_complex_v<T>) {   // complex fronts: no speculative, register-tiled or tensor-core kernels
     CK(cudaFuncSetAttribute(k_small_fronts<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)(kSmallFront * kSmallFront * sizeof(T))));
@@ -567,6 +561,15 @@ template <>
 void launch_gemm<zc>(const GemmTask* tasks, int64_t count, int64_t tiles, const zc* pa, const zc* pb, zc* pc,
                      cudaStream_t st) {
   k_gemm_z<<<(unsigned)tiles, kGemmThreads, 0, st>>>(tasks, (int)count, pa, pb, pc);
+}
+
+// Built-in rule for a batched FP32 GEMM launch: the tcgen05 kernel (one CTA
+// of 288 threads per SM, 128 x 128 tiles) when its mean work per tile is at
+// least that of a full tile over K = 64; launches of many small tasks (a few
+// rows in each tile) run on the CUDA-core kernel, which keeps several CTAs
+// per SM.
+bool tc_worthwhile(double flops, int64_t tiles_tc) {
+  return tiles_tc > 0 && flops >= 2.0 * kTcTile * kTcTile * 64.0 * (double)tiles_tc;
 }
 
 // Kernel variant of tunable GEMM launch `id` with FP32 operands: the
@@ -688,7 +691,7 @@ void run_factor_launches(mfgpu_ctx* h) {
         break;
       case kLaunchGemm:
         h->cur_tune = (int32_t)tune_id;
-        if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, true))
+        if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, tc_worthwhile(L.flops, L.tiles_tc)))
           klaunch(h, KC_GEMM_FACTOR, L.flops, bytes, [&] {
             launch_tc(h, h->b_gemm_tc.as<GemmTask>() + L.first, L.count, L.tiles_tc, (const float*)pool,
                       (const float*)pool, (float*)pool, st);
@@ -764,7 +767,7 @@ void issue_inverses(mfgpu_ctx* h) {
     ++tune_id;
     if (!is.count) continue;
     h->cur_tune = (int32_t)tune_id;
-    if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, true))
+    if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, tc_worthwhile(is.flops, is.tiles_tc)))
       klaunch(h, KC_INVERSE, is.flops, is.elems * sizeof(T), [&] {
         launch_tc(h, h->b_inv_tasks_tc.as<GemmTask>() + is.first, is.count, is.tiles_tc, (const float*)pool,
                   (const float*)pool, (float*)pool, st);
@@ -1003,27 +1006,17 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
     st.flops += (a * a + 2.0 * a * u) * R;
     st.elems += (a * a / 2 + a * u) + 2.0 * (a + u) * R;
   };
-  // thin large supernodes (few pivots, moderate front) go to the
-  // small-supernode kernels (not in the persistent solve, whose shared memory
-  // is sized for the small fronts)
-  const bool thin_ok = h->persistent_mode != 1;
-  auto thin = [&](int32_t s) {
-    return thin_ok && P.nf[s] > kSmallFront && P.nf[s] <= kThinFront && P.np[s] <= kThinPivots;
-  };
-  // the small supernodes of slots [a, m) and the thin ones of [m, e): the
-  // tiny ones (one warp each) and the rest (one CTA each), as two
-  // independent steps
-  auto small_steps = [&](int32_t a, int32_t m, int32_t e, int tiny_kind, int small_kind, int32_t level) {
+  // the small supernodes of slots [a, m): the tiny ones (one warp each) and
+  // the rest (one CTA each), as two independent steps
+  auto small_steps = [&](int32_t a, int32_t m, int tiny_kind, int small_kind, int32_t level) {
     for (int pass = 0; pass < 2; ++pass) {
       SolveSchedule::Step st{pass == 0 ? tiny_kind : small_kind, (int64_t)S.ids.size(), 0, 0};
       st.level = level;
-      for (int32_t i = a; i < e; ++i) {
+      for (int32_t i = a; i < m; ++i) {
         const int32_t s = P.slot_super[i];
-        if (i >= m ? (pass == 0 || !thin(s)) : ((P.nf[s] <= kTinyFront) != (pass == 0))) continue;
+        if ((P.nf[s] <= kTinyFront) != (pass == 0)) continue;
         S.ids.push_back(s);
         small_work(st, s);
-        st.nf_max = std::max(st.nf_max, P.nf[s]);
-        st.np_max = std::max(st.np_max, P.np[s]);
         ++st.count;
       }
       if (st.count) S.steps.push_back(st);
@@ -1033,20 +1026,16 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
   for (int32_t L = 0; L < P.nlevels; ++L) {
     const int32_t a = P.level_slot[L], m = P.level_large[L], e = P.level_slot[L + 1];
     cur_level = L;
-    small_steps(a, m, e, 6, 0, L);
-    int32_t nlarge = 0;
-    for (int32_t i = m; i < e; ++i) nlarge += !thin(P.slot_super[i]);
-    if (nlarge) {
+    if (m > a) small_steps(a, m, 6, 0, L);
+    if (e > m) {
       const int64_t first = (int64_t)S.ids.size();
-      for (int32_t i = m; i < e; ++i)
-        if (!thin(P.slot_super[i])) S.ids.push_back(P.slot_super[i]);
-      S.steps.push_back({1, first, nlarge, 0});
+      for (int32_t i = m; i < e; ++i) S.ids.push_back(P.slot_super[i]);
+      S.steps.push_back({1, first, e - m, 0});
       S.steps.back().level = L;
       // y = inv(L11) f[0:np], into x's rows c1.. ; then w = f[np:] - L21 y
       SolveSchedule::Step gy = gemm_step();
       for (int32_t i = m; i < e; ++i) {
         const int32_t s = P.slot_super[i];
-        if (thin(s)) continue;
         const int nf = P.nf[s], np = P.np[s];
         add_gemm(gy, kGemmSet, P.inv_off[s], np, P.colbase[s] * R, nf, xw0 + P.c1[s], n, np, (int)R, np);
       }
@@ -1054,7 +1043,6 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
       SolveSchedule::Step gw = gemm_step();
       for (int32_t i = m; i < e; ++i) {
         const int32_t s = P.slot_super[i];
-        if (thin(s)) continue;
         const int nf = P.nf[s], np = P.np[s];
         add_gemm(gw, kGemmSub, P.lpan_off[s] + np, nf, xw0 + P.c1[s], n, P.colbase[s] * R + np, nf, P.nu[s],
                  (int)R, np);
@@ -1068,20 +1056,16 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
     cur_level = L;
     // the level's small supernodes read x of higher levels only: independent
     // of the level's large ones
-    small_steps(a, m, e, 7, 4, L);
-    int32_t nlarge = 0;
-    for (int32_t i = m; i < e; ++i) nlarge += !thin(P.slot_super[i]);
-    if (nlarge) {
+    if (m > a) small_steps(a, m, 7, 4, L);
+    if (e > m) {
       const int64_t first = (int64_t)S.ids.size();
-      for (int32_t i = m; i < e; ++i)
-        if (!thin(P.slot_super[i])) S.ids.push_back(P.slot_super[i]);
-      S.steps.push_back({5, first, nlarge, 0});
+      for (int32_t i = m; i < e; ++i) S.ids.push_back(P.slot_super[i]);
+      S.steps.push_back({5, first, e - m, 0});
       S.steps.back().level = L;
       // g = y - U12 x[upd] into f[0:np]; then x = inv(U11) g into x's rows c1..
       SolveSchedule::Step gg = gemm_step();
       for (int32_t i = m; i < e; ++i) {
         const int32_t s = P.slot_super[i];
-        if (thin(s)) continue;
         const int nf = P.nf[s], np = P.np[s];
         add_gemm(gg, kGemmFrom, P.u12_off[s], u12_ld(P, s), P.colbase[s] * R + np, nf, P.colbase[s] * R, nf, np,
                  (int)R, P.nu[s], xw0 + P.c1[s], n);
@@ -1090,7 +1074,6 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
       SolveSchedule::Step gx = gemm_step();
       for (int32_t i = m; i < e; ++i) {
         const int32_t s = P.slot_super[i];
-        if (thin(s)) continue;
         const int nf = P.nf[s], np = P.np[s];
         add_gemm(gx, kGemmSet, P.inv_off[s] + (int64_t)np * np, np, P.colbase[s] * R, nf, xw0 + P.c1[s], n, np,
                  (int)R, np);
@@ -1242,9 +1225,8 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
     switch (s.kind) {
       case 0:
         klaunch(h, KC_FWD_SMALL, s.flops, bytes, [&] {
-          const size_t smem = (size_t)std::max(s.nf_max, kSmallFront) * solve_cols<T>() * sizeof(T);
-          k_fwd_small<T><<<dim3((unsigned)s.count, ychunks), kSolveThreads, smem, ss>>>(h->dp, DS, A, ids + s.first,
-                                                                                        pool, fsol);
+          k_fwd_small<T><<<dim3((unsigned)s.count, ychunks), kSolveThreads, 0, ss>>>(h->dp, DS, A, ids + s.first,
+                                                                                     pool, fsol);
         });
         break;
       case 1:
@@ -1275,7 +1257,7 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
                                                                                            fsol);
             }
           }, -1, s.sk_parts);
-        else if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, R >= 64))
+        else if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, R >= 64 && tc_worthwhile(s.flops, s.tiles_tc)))
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
             launch_tc(h, S.d_gemms_tc.as<GemmTask>() + s.first, s.count, s.tiles_tc, (const float*)pool,
                       (const float*)fsol, (float*)fsol, st);
@@ -1301,10 +1283,8 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
         break;
       case 4:
         klaunch(h, KC_BWD_SMALL, s.flops, bytes, [&] {
-          const int goff = s.np_max * solve_cols<T>();
-          const size_t smem = (size_t)(goff + s.nf_max * solve_cols<T>()) * sizeof(T);
-          k_bwd_small<T><<<dim3((unsigned)s.count, ychunks), kSolveThreads, smem, ss>>>(h->dp, A, ids + s.first,
-                                                                                        pool, fsol, xw, goff);
+          k_bwd_small<T><<<dim3((unsigned)s.count, ychunks), kSolveThreads, 0, ss>>>(h->dp, A, ids + s.first, pool,
+                                                                                     fsol, xw);
         });
         break;
       case 5:

@@ -140,8 +140,14 @@ def measure(ctx: GpuContext, run, count: int, choice, repeats: int = 2) -> np.nd
 
 
 def rule_choice(feats: np.ndarray, nrhs: int) -> np.ndarray:
-    """The built-in rule: tcgen05 everywhere, solve products from 64 rhs."""
-    return np.where(feats[:, 2] > 0, np.where(nrhs >= 64, 1, 2), 1)
+    """The library's built-in rule (mfgpu.cu: tc_worthwhile): tcgen05 when a
+    launch's mean work per 128 x 128 tile is at least a full tile's over
+    K = 64, CUDA cores otherwise; solve products on tcgen05 only from 64
+    right-hand sides."""
+    flops = np.power(10.0, feats[:, 3].astype(np.float64)) - 1.0
+    tiles_tc = np.power(10.0, feats[:, 7].astype(np.float64)) - 1.0
+    big = (tiles_tc > 0.5) & (flops >= 2.0 * 128 * 128 * 64 * tiles_tc * (1 - 1e-6))
+    return np.where(big & ((feats[:, 2] == 0) | (nrhs >= 64)), 1, 2)
 
 
 def exhaustive_table(ctx: GpuContext, run, nrhs: int, repeats: int = 2) -> LaunchTable:
