@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--forms", default="fp64,mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--records", default=None,
+                    help="write the profiled step's launch records of every form (kernel class, level, tasks, ms, "
+                         "algorithmic flops and bytes, tunable index) as JSON to this path")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the untimed comparison of the GPU factors with the oracle's (and mixed with FP64)")
     ap.add_argument("--solve-mode", default="auto", choices=["auto", "step", "persistent"],
@@ -610,6 +613,7 @@ def main():
     d_x = torch.empty(n * R, dtype=torch.float64, device=dev)
 
     forms = {}
+    all_records = {}
     kept, par_mixed = {}, None
     peaks = measured_peaks()
     for form in [f for f in args.forms.split(",") if f]:
@@ -670,6 +674,8 @@ def main():
         step(refine)
         torch.cuda.synchronize()
         st = ctx.stats()
+        if args.records:
+            all_records[form] = ctx.launch_records()
         ctx.set_profiling(False)
         # end to end through the C ABI with pinned host buffers
         e2e = None
@@ -724,6 +730,9 @@ def main():
         if world > 1:
             dist.destroy_process_group()
         return 0
+    if args.records:
+        with open(args.records, "w") as fh:
+            json.dump(all_records, fh)
 
     # the headline form: the fastest one whose solution meets the accuracy target
     ok = [k for k, f in forms.items() if f["eta"] is not None and f["eta"] <= TARGET_ETA]

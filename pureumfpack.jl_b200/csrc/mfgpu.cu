@@ -1227,19 +1227,19 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
         klaunch(h, KC_FWD_SMALL, s.flops, bytes, [&] {
           k_fwd_small<T><<<dim3((unsigned)s.count, ychunks), kSolveThreads, 0, ss>>>(h->dp, DS, A, ids + s.first,
                                                                                      pool, fsol);
-        });
+        }, s.level, s.count);
         break;
       case 1:
         klaunch(h, KC_FWD_ASSEMBLE, 0, 0, [&] {
           k_fwd_assemble<T><<<dim3((unsigned)s.count, wchunks), 256, 0, st>>>(h->dp, DS, A, ids + s.first, fsol);
-        });
+        }, s.level, s.count);
         break;
       case 3:
         h->cur_tune = (int32_t)tune_id;
         if constexpr (is_complex_v<T>)
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
             launch_gemm<T>(gemms + s.first, s.count, s.tiles, pool, fsol, fsol, st);
-          }, -1, s.tiles);
+          }, s.level, s.tiles);
         else if (s.sk_count && !(sizeof(T) == 4 && gemm_use_tc(h, tune_id, false)))
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
             const SkinnyTask* sk = S.d_skinny.as<SkinnyTask>() + s.sk_first;
@@ -1256,16 +1256,16 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
               k_skinny_reduce<T, kSkinnyMaxN><<<(unsigned)s.sk_reds, kSkinnyRows, 0, st>>>(sk, (int)s.sk_count, part,
                                                                                            fsol);
             }
-          }, -1, s.sk_parts);
+          }, s.level, s.sk_parts);
         else if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, R >= 64 && tc_worthwhile(s.flops, s.tiles_tc)))
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
             launch_tc(h, S.d_gemms_tc.as<GemmTask>() + s.first, s.count, s.tiles_tc, (const float*)pool,
                       (const float*)fsol, (float*)fsol, st);
-          }, -1, s.tiles_tc);
+          }, s.level, s.tiles_tc);
         else
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
             launch_gemm<T>(gemms + s.first, s.count, s.tiles, pool, fsol, fsol, st);
-          }, -1, s.tiles);
+          }, s.level, s.tiles);
         h->cur_tune = -1;
         ++tune_id;
         break;
@@ -1273,24 +1273,24 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
         klaunch(h, KC_FWD_SMALL, s.flops, bytes, [&] {
           k_fwd_tiny<T><<<dim3((unsigned)((s.count + tiny_warps<T>() - 1) / tiny_warps<T>()), (unsigned)((R + 31) / 32)),
                           32 * tiny_warps<T>(), 0, ss>>>(h->dp, DS, A, ids + s.first, (int)s.count, pool, fsol);
-        });
+        }, s.level, s.count);
         break;
       case 7:
         klaunch(h, KC_BWD_SMALL, s.flops, bytes, [&] {
           k_bwd_tiny<T><<<dim3((unsigned)((s.count + tiny_warps<T>() - 1) / tiny_warps<T>()), (unsigned)((R + 31) / 32)),
                           32 * tiny_warps<T>(), 0, ss>>>(h->dp, A, ids + s.first, (int)s.count, pool, fsol, xw);
-        });
+        }, s.level, s.count);
         break;
       case 4:
         klaunch(h, KC_BWD_SMALL, s.flops, bytes, [&] {
           k_bwd_small<T><<<dim3((unsigned)s.count, ychunks), kSolveThreads, 0, ss>>>(h->dp, A, ids + s.first, pool,
                                                                                      fsol, xw);
-        });
+        }, s.level, s.count);
         break;
       case 5:
         klaunch(h, KC_BWD_GATHER, 0, 0, [&] {
           k_bwd_gather<T><<<dim3((unsigned)s.count, wchunks), 256, 0, st>>>(h->dp, A, ids + s.first, fsol, xw);
-        });
+        }, s.level, s.count);
         break;
     }
   }
