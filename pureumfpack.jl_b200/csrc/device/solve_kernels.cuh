@@ -124,17 +124,12 @@ __device__ __forceinline__ void fwd_small_item(const DevPlan& P, const DevState&
   __syncthreads();
 }
 
-// Column chunks [blockIdx.y * cpb, +cpb) of supernode tasks[blockIdx.x]: on
-// levels with many small supernodes one CTA walks several chunks (fewer,
-// longer CTAs; the supernode's L panel stays in L1 between chunks).
 template <typename T>
 __global__ void __launch_bounds__(kSolveThreads) k_fwd_small(DevPlan P, DevState S, SolveArgs A,
                                                              const int32_t* __restrict__ tasks,
-                                                             const T* __restrict__ pool, T* fsol, int cpb) {
+                                                             const T* __restrict__ pool, T* fsol) {
   __shared__ T f[kSmallFront * solve_cols<T>()];
-  const int nch = (int)((A.nrhs + solve_cols<T>() - 1) / solve_cols<T>());
-  for (int by = blockIdx.y * cpb; by < min(nch, (int)(blockIdx.y + 1) * cpb); ++by)
-    fwd_small_item<T>(P, S, A, tasks, pool, fsol, blockIdx.x, by, f);
+  fwd_small_item<T>(P, S, A, tasks, pool, fsol, blockIdx.x, blockIdx.y, f);
 }
 
 // Tiny supernodes (nf <= kTinyFront), the bulk of the leaf levels: one warp
@@ -156,14 +151,14 @@ __host__ __device__ constexpr int tiny_warps() {
 template <typename T>
 __global__ void __launch_bounds__(32 * tiny_warps<T>()) k_fwd_tiny(DevPlan P, DevState S, SolveArgs A,
                                                               const int32_t* __restrict__ tasks, int ntasks,
-                                                              const T* __restrict__ pool, T* fsol, int cpb) {
+                                                              const T* __restrict__ pool, T* fsol) {
   __shared__ T buf[tiny_warps<T>()][kTinyFront * kTinyLd];
   const int w = warp_id(), lane = lane_id();
   const int ti = blockIdx.x * tiny_warps<T>() + w;
   if (ti >= ntasks) return;                 // warp-uniform; no block barrier below
   T* f = buf[w];
   const int s = tasks[ti];
-  for (int c0 = (int)blockIdx.y * cpb * 32; c0 < min((int)A.nrhs, ((int)blockIdx.y + 1) * cpb * 32); c0 += 32) {
+  const int c0 = blockIdx.y * 32;
   const int rc = min(32, (int)(A.nrhs - c0));
   const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
   const int64_t R = A.nrhs;
@@ -196,22 +191,19 @@ __global__ void __launch_bounds__(32 * tiny_warps<T>()) k_fwd_tiny(DevPlan P, De
     const int r = e % nf, c = e / nf;
     out[r + (int64_t)(c0 + c) * nf] = f[r * kTinyLd + c];
   }
-  __syncwarp();
-  }
 }
 
 template <typename T>
 __global__ void __launch_bounds__(32 * tiny_warps<T>()) k_bwd_tiny(DevPlan P, SolveArgs A,
                                                               const int32_t* __restrict__ tasks, int ntasks,
-                                                              const T* __restrict__ pool, const T* fsol, T* xw,
-                                                              int cpb) {
+                                                              const T* __restrict__ pool, const T* fsol, T* xw) {
   __shared__ T buf[tiny_warps<T>()][kTinyFront * kTinyLd];   // rows 0..np-1: y; np..nf-1: x of the update rows
   const int w = warp_id(), lane = lane_id();
   const int ti = blockIdx.x * tiny_warps<T>() + w;
   if (ti >= ntasks) return;
   T* f = buf[w];
   const int s = tasks[ti];
-  for (int c0 = (int)blockIdx.y * cpb * 32; c0 < min((int)A.nrhs, ((int)blockIdx.y + 1) * cpb * 32); c0 += 32) {
+  const int c0 = blockIdx.y * 32;
   const int rc = min(32, (int)(A.nrhs - c0));
   const int np = P.np[s], nu = P.nu[s], nf = P.nf[s], c1 = P.c1[s];
   const int64_t R = A.nrhs;
@@ -245,8 +237,6 @@ __global__ void __launch_bounds__(32 * tiny_warps<T>()) k_bwd_tiny(DevPlan P, So
   for (int e = lane; e < np * rc; e += 32) {
     const int r = e % np, c = e / np;
     xw[c1 + r + (int64_t)(c0 + c) * A.ldx] = f[r * kTinyLd + c];
-  }
-  __syncwarp();
   }
 }
 
@@ -347,12 +337,9 @@ __device__ __forceinline__ void bwd_small_item(const DevPlan& P, const SolveArgs
 
 template <typename T>
 __global__ void __launch_bounds__(kSolveThreads) k_bwd_small(DevPlan P, SolveArgs A, const int32_t* __restrict__ tasks,
-                                                             const T* __restrict__ pool, const T* fsol, T* xw,
-                                                             int cpb) {
+                                                             const T* __restrict__ pool, const T* fsol, T* xw) {
   __shared__ T y[2 * kSmallFront * solve_cols<T>()];
-  const int nch = (int)((A.nrhs + solve_cols<T>() - 1) / solve_cols<T>());
-  for (int by = blockIdx.y * cpb; by < min(nch, (int)(blockIdx.y + 1) * cpb); ++by)
-    bwd_small_item<T>(P, A, tasks, pool, fsol, xw, blockIdx.x, by, y);
+  bwd_small_item<T>(P, A, tasks, pool, fsol, xw, blockIdx.x, blockIdx.y, y);
 }
 
 // Large supernodes: gather x of the update columns into the w rows.

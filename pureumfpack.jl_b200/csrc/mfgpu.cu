@@ -592,15 +592,6 @@ void launch_tc(const mfgpu_ctx* h, const GemmTask* tasks, int64_t count, int64_t
                                                                                 h->b_flags.as<int>(), h->wait_ns);
 }
 
-// Right-hand-side chunks per CTA of a small-supernode solve step with
-// `units` CTAs per chunk column: all of a supernode's chunks in one CTA when
-// the step still has `target` CTAs without splitting them (fewer, longer
-// CTAs that read the supernode's panel once), one chunk per CTA otherwise.
-int chunks_per_block(int64_t units, int64_t chunks, int64_t target) {
-  if (chunks <= 1) return 1;
-  return (int)std::min<int64_t>(chunks, std::max<int64_t>(1, units * chunks / target));
-}
-
 // Tunable-launch ids: factor GEMM launches first, then the inversion steps,
 // then the solve GEMM steps.
 int64_t tune_factor_count(const Plan& P) {
@@ -1234,9 +1225,8 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
     switch (s.kind) {
       case 0:
         klaunch(h, KC_FWD_SMALL, s.flops, bytes, [&] {
-          const int cpb = chunks_per_block(s.count, ychunks, 8LL * h->num_sms);
-          k_fwd_small<T><<<dim3((unsigned)s.count, (ychunks + cpb - 1) / cpb), kSolveThreads, 0, ss>>>(
-              h->dp, DS, A, ids + s.first, pool, fsol, cpb);
+          k_fwd_small<T><<<dim3((unsigned)s.count, ychunks), kSolveThreads, 0, ss>>>(h->dp, DS, A, ids + s.first,
+                                                                                     pool, fsol);
         }, s.level, s.count);
         break;
       case 1:
@@ -1280,24 +1270,21 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
         ++tune_id;
         break;
       case 6:
+        klaunch(h, KC_FWD_SMALL, s.flops, bytes, [&] {
+          k_fwd_tiny<T><<<dim3((unsigned)((s.count + tiny_warps<T>() - 1) / tiny_warps<T>()), (unsigned)((R + 31) / 32)),
+                          32 * tiny_warps<T>(), 0, ss>>>(h->dp, DS, A, ids + s.first, (int)s.count, pool, fsol);
+        }, s.level, s.count);
+        break;
       case 7:
-        klaunch(h, s.kind == 6 ? KC_FWD_SMALL : KC_BWD_SMALL, s.flops, bytes, [&] {
-          const int64_t blocks = (s.count + tiny_warps<T>() - 1) / tiny_warps<T>(), chunks = (R + 31) / 32;
-          const int cpb = chunks_per_block(blocks, chunks, 8LL * h->num_sms);
-          const dim3 grid((unsigned)blocks, (unsigned)((chunks + cpb - 1) / cpb));
-          if (s.kind == 6)
-            k_fwd_tiny<T><<<grid, 32 * tiny_warps<T>(), 0, ss>>>(h->dp, DS, A, ids + s.first, (int)s.count, pool,
-                                                                   fsol, cpb);
-          else
-            k_bwd_tiny<T><<<grid, 32 * tiny_warps<T>(), 0, ss>>>(h->dp, A, ids + s.first, (int)s.count, pool, fsol,
-                                                                   xw, cpb);
+        klaunch(h, KC_BWD_SMALL, s.flops, bytes, [&] {
+          k_bwd_tiny<T><<<dim3((unsigned)((s.count + tiny_warps<T>() - 1) / tiny_warps<T>()), (unsigned)((R + 31) / 32)),
+                          32 * tiny_warps<T>(), 0, ss>>>(h->dp, A, ids + s.first, (int)s.count, pool, fsol, xw);
         }, s.level, s.count);
         break;
       case 4:
         klaunch(h, KC_BWD_SMALL, s.flops, bytes, [&] {
-          const int cpb = chunks_per_block(s.count, ychunks, 8LL * h->num_sms);
-          k_bwd_small<T><<<dim3((unsigned)s.count, (ychunks + cpb - 1) / cpb), kSolveThreads, 0, ss>>>(
-              h->dp, A, ids + s.first, pool, fsol, xw, cpb);
+          k_bwd_small<T><<<dim3((unsigned)s.count, ychunks), kSolveThreads, 0, ss>>>(h->dp, A, ids + s.first, pool,
+                                                                                     fsol, xw);
         }, s.level, s.count);
         break;
       case 5:
