@@ -445,13 +445,61 @@ __device__ void block_inverses(const T* D, int ldd, int kb, T* dst, T* sm_xrow2)
 // 8 x 8 diagonal block with shuffles and inverts its triangles; then the
 // block column below (L_rs = A_rs inv(U_ss)) and the block row to the right
 // (U_sc = inv(L_ss) A_sc) are formed, and the trailing blocks updated.  The
-// off-diagonal blocks of inv(L) and inv(U) are built by block substitution.
+// off-diagonal blocks of inv(L) (by block rows) and inv(U) (by block
+// columns) are built by block substitution one step behind, by warps 1-7
+// while warp 0 factors the next diagonal block.
 // Every multiplier is checked against the partial-pivoting order (|l| <= 1);
 // a violation or a zero pivot raises flags[0] and the factorization is redone
 // with pivoting panels.
 // ---------------------------------------------------------------------------
 constexpr int kSpecThreads = 256;
 constexpr int kLdS = 65;   // shared leading dimension of the 64 x 64 blocks
+
+// Off-diagonal blocks of block row i of inv(L) and block column i of inv(U)
+// (8 x 8 blocks, i >= 1) of the speculative panel, from the finished blocks
+// of L, U and of both inverses with smaller block index: thread u < 8i forms
+// column b of Li(i, s) = -Li_ii (sum_{s<=k<i} L_ik Li_ks), thread
+// 8i <= u < 16i row a of Ui(s, i) = -(sum_{s<=k<i} Ui_sk U_ki) Ui_ii.  No
+// thread reads another's output, so block i can be formed while warp 0
+// factors diagonal block i + 1.
+template <typename T>
+__device__ __forceinline__ void spec_inverse_blocks(const T* A, T* Li, T* Ui, int i, int u) {
+  if (u < 8 * i) {
+    const int s = u >> 3, b = u & 7;
+    T col[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) col[a] = T(0);
+    for (int k = 8 * s; k < 8 * i; ++k) {
+      const T lk = Li[k + (8 * s + b) * kLdS];
+#pragma unroll
+      for (int a = 0; a < 8; ++a) col[a] += A[(8 * i + a) + k * kLdS] * lk;
+    }
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      T v = T(0);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v -= Li[(8 * i + a) + (8 * i + k) * kLdS] * col[k];
+      Li[(8 * i + a) + (8 * s + b) * kLdS] = v;
+    }
+  } else if (u < 16 * i) {
+    const int s = (u - 8 * i) >> 3, a = (u - 8 * i) & 7;
+    T row[8];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) row[b] = T(0);
+    for (int k = 8 * s; k < 8 * i; ++k) {
+      const T uk = Ui[(8 * s + a) + k * kLdS];
+#pragma unroll
+      for (int b = 0; b < 8; ++b) row[b] += uk * A[k + (8 * i + b) * kLdS];
+    }
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      T v = T(0);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v -= row[k] * Ui[(8 * i + k) + (8 * i + b) * kLdS];
+      Ui[(8 * s + a) + (8 * i + b) * kLdS] = v;
+    }
+  }
+}
 
 template <typename T>
 __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState S, const PanelTask* __restrict__ tasks,
@@ -460,7 +508,6 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
   T* A = reinterpret_cast<T*>(smem_raw);     // 64 x 64, ld kLdS: L\U
   T* Li = A + 64 * kLdS;                     // inv(L)
   T* Ui = Li + 64 * kLdS;                    // inv(U)
-  T* Tb = Ui + 64 * kLdS;                    // 2 x 7 x 64 scratch of the inverse assembly
   __shared__ int bad;
   __shared__ int seg[64];                    // per block column: end of its pivot rows (block-relative)
   const PanelTask tk = tasks[blockIdx.x];
@@ -471,11 +518,21 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
   T* F = pool + P.front_off[s_];
   if (t == 0) bad = 0;
   if (t < 64) seg[t] = t < kb ? min(kb, P.seg_end[c1 + k0 + t] - k0) : 0;
-  for (int e = t; e < 64 * 64; e += kSpecThreads) {
-    const int r = e & 63, c = e >> 6;
-    A[r + c * kLdS] = (r < kb && c < kb) ? F[(k0 + r) + (int64_t)(k0 + c) * nf] : (r == c ? T(1) : T(0));
-    Li[r + c * kLdS] = T(0);
-    Ui[r + c * kLdS] = T(0);
+  {
+    // all 16 of this thread's block values in flight before any store
+    T v[64 * 64 / kSpecThreads];
+#pragma unroll
+    for (int q = 0; q < 64 * 64 / kSpecThreads; ++q) {
+      const int e = t + q * kSpecThreads, r = e & 63, c = e >> 6;
+      v[q] = (r < kb && c < kb) ? F[(k0 + r) + (int64_t)(k0 + c) * nf] : (r == c ? T(1) : T(0));
+    }
+#pragma unroll
+    for (int q = 0; q < 64 * 64 / kSpecThreads; ++q) {
+      const int e = t + q * kSpecThreads, r = e & 63, c = e >> 6;
+      A[r + c * kLdS] = v[q];
+      Li[r + c * kLdS] = T(0);
+      Ui[r + c * kLdS] = T(0);
+    }
   }
   __syncthreads();
   bool violated = false;
@@ -544,6 +601,10 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
 #pragma unroll
         for (int i = 0; i < 8; ++i) Ui[(s8 + i) + (s8 + c) * kLdS] = x[i];
       }
+    } else if (sb >= 2) {
+      // meanwhile the other warps form the off-diagonal inverse blocks of
+      // block row / column sb - 1, whose inputs are all final
+      spec_inverse_blocks<T>(A, Li, Ui, sb - 1, t - 32);
     }
     __syncthreads();
     const int rest = 56 - s8;   // rows / columns after this block
@@ -587,46 +648,9 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
     }
     __syncthreads();
   }
-  // off-diagonal blocks of the inverses, one block row of each per iteration
-  T* Tl = Tb;
-  T* Tu = Tb + 7 * 64;
-  for (int i = 1; i < 8; ++i) {
-    const int ur = 7 - i;       // block row of inv(U) done this iteration
-    if (t < 128) {              // T_l(i, s) = sum_{s<=k<i} L_ik Li_ks, s < i
-      for (int e = t; e < i * 64; e += 128) {
-        const int sb = e >> 6, a = (e >> 3) & 7, b = e & 7;
-        T v = T(0);
-        for (int k = 8 * sb; k < 8 * i; ++k) v += A[(8 * i + a) + k * kLdS] * Li[k + (8 * sb + b) * kLdS];
-        Tl[e] = v;
-      }
-    } else {                    // T_u(ur, c) = sum_{ur<k<=c} U_{ur,k} Ui_kc, c > ur
-      for (int e = t - 128; e < i * 64; e += 128) {
-        const int cb = ur + 1 + (e >> 6), a = (e >> 3) & 7, b = e & 7;
-        T v = T(0);
-        for (int k = 8 * (ur + 1); k < 8 * (cb + 1); ++k) v += A[(8 * ur + a) + k * kLdS] * Ui[k + (8 * cb + b) * kLdS];
-        Tu[e] = v;
-      }
-    }
-    __syncthreads();
-    if (t < 128) {              // Li(i, s) = -Li_ii T_l(i, s)
-      for (int e = t; e < i * 64; e += 128) {
-        const int sb = e >> 6, a = (e >> 3) & 7, b = e & 7;
-        T v = T(0);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) v -= Li[(8 * i + a) + (8 * i + k) * kLdS] * Tl[(sb << 6) + (k << 3) + b];
-        Li[(8 * i + a) + (8 * sb + b) * kLdS] = v;
-      }
-    } else {                    // Ui(ur, c) = -Ui_{ur,ur} T_u(ur, c)
-      for (int e = t - 128; e < i * 64; e += 128) {
-        const int cb = ur + 1 + (e >> 6), a = (e >> 3) & 7, b = e & 7;
-        T v = T(0);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) v -= Ui[(8 * ur + a) + (8 * ur + k) * kLdS] * Tu[((e >> 6) << 6) + (k << 3) + b];
-        Ui[(8 * ur + a) + (8 * cb + b) * kLdS] = v;
-      }
-    }
-    __syncthreads();
-  }
+  // the last block row of inv(L) and block column of inv(U)
+  spec_inverse_blocks<T>(A, Li, Ui, 7, t);
+  __syncthreads();
   if (violated) bad = 1;
   __syncthreads();
   if (t == 0 && bad) atomicOr(S.flags, 1);

@@ -497,7 +497,7 @@ size_t panel_smem_bytes(int rows) {
 
 template <typename T>
 size_t spec_smem_bytes() {
-  return ((size_t)3 * 64 * kLdS + 2 * 7 * 64) * sizeof(T);
+  return (size_t)3 * 64 * kLdS * sizeof(T);
 }
 
 template <typename T>
