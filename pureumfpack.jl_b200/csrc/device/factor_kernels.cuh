@@ -116,21 +116,23 @@ __global__ void __launch_bounds__(256) k_assemble_columns(DevPlan P, int64_t fc0
     const int m = P.nu[k], nfk = P.nf[k], npk = P.np[k];
     const T* cb = pool + P.front_off[k] + npk + (int64_t)(npk + t) * nfk;
     const int32_t* rl = P.rel + P.upd_off[k];
-    // four rows per lane in flight (a child's rows map to distinct rows of
-    // this column, so all loads may precede the stores)
+    // kU rows per lane in flight (a child's rows map to distinct rows of
+    // this column, so all loads may precede the stores); 4-byte fronts move
+    // half the bytes per access, so they keep twice as many in flight
+    constexpr int kU = sizeof(T) == 4 ? 8 : 4;
     int r = lane;
-    for (; r + 96 < m; r += 128) {
-      int pos[4];
-      T v[4], o[4];
+    for (; r + 32 * (kU - 1) < m; r += 32 * kU) {
+      int pos[kU];
+      T v[kU], o[kU];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < kU; ++q) {
         pos[q] = rl[r + 32 * q];
         v[q] = cb[r + 32 * q];
       }
 #pragma unroll
-      for (int q = 0; q < 4; ++q) o[q] = col[pos[q]];
+      for (int q = 0; q < kU; ++q) o[q] = col[pos[q]];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) col[pos[q]] = o[q] + v[q];
+      for (int q = 0; q < kU; ++q) col[pos[q]] = o[q] + v[q];
     }
     for (; r < m; r += 32) col[rl[r]] += cb[r];
     __syncwarp();

@@ -259,21 +259,23 @@ __device__ __forceinline__ void fwd_assemble_item(const DevPlan& P, const DevSta
     const int m = P.nu[k], nfk = P.nf[k], npk = P.np[k];
     const T* w = fsol + P.colbase[k] * R + npk + col * nfk;
     const int32_t* rl = P.rel + P.upd_off[k];
-    // four rows per lane in flight: a child's rows map to distinct front
-    // rows, so the loads may all precede the stores
+    // kU rows per lane in flight: a child's rows map to distinct front
+    // rows, so the loads may all precede the stores (4-byte values: twice
+    // as many, they move half the bytes per access)
+    constexpr int kU = sizeof(T) == 4 ? 8 : 4;
     int r = lane;
-    for (; r + 96 < m; r += 128) {
-      int pos[4];
-      T v[4], o[4];
+    for (; r + 32 * (kU - 1) < m; r += 32 * kU) {
+      int pos[kU];
+      T v[kU], o[kU];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < kU; ++q) {
         pos[q] = front_pos(S, c1, np, rl[r + 32 * q]);
         v[q] = w[r + 32 * q];
       }
 #pragma unroll
-      for (int q = 0; q < 4; ++q) o[q] = f[pos[q]];
+      for (int q = 0; q < kU; ++q) o[q] = f[pos[q]];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) f[pos[q]] = o[q] + v[q];
+      for (int q = 0; q < kU; ++q) f[pos[q]] = o[q] + v[q];
     }
     for (; r < m; r += 32) f[front_pos(S, c1, np, rl[r])] += w[r];
     __syncwarp();
@@ -353,6 +355,8 @@ __device__ __forceinline__ void bwd_gather_item(const DevPlan& P, const SolveArg
   const int np = P.np[s], nu = P.nu[s], nf = P.nf[s];
   T* f = fsol + P.colbase[s] * A.nrhs + col * nf + np;
   const int32_t* us = P.upd + P.upd_off[s];
+  // independent gathers: several in flight per lane
+#pragma unroll 4
   for (int t = lane_id(); t < nu; t += 32) f[t] = xw[us[t] + col * A.ldx];
 }
 

@@ -368,15 +368,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(const GemmTask* __res
 constexpr int kBxProducers = 256;
 constexpr int kBxThreads = kBxProducers + 32;
 
-template <int BN, int STAGES>
+template <int BN, int STAGES, int ACCS = 4>
 struct BxCfg {
   static constexpr int BM = 128, BK = 64;
   static constexpr int kABytes = BM * BK * 2;     // one bf16 part of A
   static constexpr int kBBytes = BN * BK * 2;
   static constexpr int kStageBytes = 3 * kABytes + 3 * kBBytes;
   static constexpr size_t kSmem = (size_t)STAGES * kStageBytes + 1024;
-  static constexpr int kAccs = 4;                  // accumulators, K blocks round-robin
-  static constexpr int kTmemCols = kAccs * BN;     // 512 or 256 columns (power of two)
+  static constexpr int kAccs = ACCS;               // accumulators, K blocks round-robin
+  static constexpr int kTmemCols = kAccs * BN;     // a power of two >= 32
   // D f32, A/B bf16, both K-major, N = BN, M = 128
   static constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
                                      ((uint32_t)(BM >> 4) << 24);
@@ -429,11 +429,14 @@ __device__ __forceinline__ void bx_put8(uint32_t p1, uint32_t p2, uint32_t p3, u
 
 // Batched C = f(C, A * B) (GemmTask::mode) over tasks whose tiles_m /
 // tiles_n count 128 x BN tiles; flags[1] is set when a bounded wait expired.
-template <int BN, int STAGES>
-__global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __restrict__ tasks, int ntasks,
-                                                            const float* __restrict__ pa, const float* __restrict__ pb,
-                                                            float* pc, int* __restrict__ flags, uint64_t wait_ns) {
-  using Cfg = BxCfg<BN, STAGES>;
+// The short-K form (STAGES = 1, ACCS = 1: launches whose tasks all have
+// K <= BK) holds one stage and one accumulator and stages one K block
+// without a second register buffer, so two CTAs share an SM.
+template <int BN, int STAGES, int ACCS = 4>
+__global__ void __launch_bounds__(kBxThreads, STAGES == 1 ? 2 : 1)
+    k_gemm_bx3(const GemmTask* __restrict__ tasks, int ntasks, const float* __restrict__ pa,
+               const float* __restrict__ pb, float* pc, int* __restrict__ flags, uint64_t wait_ns) {
+  using Cfg = BxCfg<BN, STAGES, ACCS>;
   constexpr int BK = Cfg::BK;
   extern __shared__ __align__(16) uint8_t bx_smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)bx_smem_raw + 1023) & ~(uintptr_t)1023);
@@ -523,13 +526,21 @@ __global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __re
       mbar_arrive(&full[s]);
       return !failed;
     };
-    float va0[32], vb0[kBPer][8], va1[32], vb1[kBPer][8];
-    if (nk > 0) load(0, va0, vb0);
-    for (int kb = 0; kb < nk; kb += 2) {
-      if (kb + 1 < nk) load(kb + 1, va1, vb1);
-      if (!produce(kb, va0, vb0) || kb + 1 >= nk) break;
-      if (kb + 2 < nk) load(kb + 2, va0, vb0);
-      if (!produce(kb + 1, va1, vb1)) break;
+    if constexpr (STAGES == 1) {
+      float va[32], vb[kBPer][8];
+      for (int kb = 0; kb < nk; ++kb) {
+        load(kb, va, vb);
+        if (!produce(kb, va, vb)) break;
+      }
+    } else {
+      float va0[32], vb0[kBPer][8], va1[32], vb1[kBPer][8];
+      if (nk > 0) load(0, va0, vb0);
+      for (int kb = 0; kb < nk; kb += 2) {
+        if (kb + 1 < nk) load(kb + 1, va1, vb1);
+        if (!produce(kb, va0, vb0) || kb + 1 >= nk) break;
+        if (kb + 2 < nk) load(kb + 2, va0, vb0);
+        if (!produce(kb + 1, va1, vb1)) break;
+      }
     }
   } else if (lane == 0) {
     if (flags[2] && !mbar_wait(&stall, 0u, wait_ns)) failed = 1;   // test hook: a wait that runs out
@@ -576,26 +587,31 @@ __global__ void __launch_bounds__(kBxThreads, 1) k_gemm_bx3(const GemmTask* __re
       const int nacc = nk < Cfg::kAccs ? nk : Cfg::kAccs;   // accumulators that K blocks reached
 #pragma unroll 1
       for (int c0 = half * (BN / 2); c0 < (half + 1) * (BN / 2); c0 += 32) {
+        uint32_t v[32];
         float acc[32];
 #pragma unroll
         for (int j = 0; j < 32; ++j) acc[j] = 0.0f;   // K = 0: the product is zero (C = D or C = 0)
         for (int b = 0; b < nacc; ++b) {
-          uint32_t v[32];
           tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + c0), v);
 #pragma unroll
           for (int j = 0; j < 32; ++j) acc[j] += __uint_as_float(v[j]);
         }
         if (row < M) {
-          float cv[32];
+          // eight columns at a time: their C (or D) values are all loaded
+          // before any of them is stored
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int col = n0 + c0 + j;
-            cv[j] = (ld && col < N) ? D[(int64_t)row + (int64_t)col * ldD] : 0.0f;
-          }
+          for (int g = 0; g < 32; g += 8) {
+            float cv[8];
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int col = n0 + c0 + j;
-            if (col < N) C[(int64_t)row + (int64_t)col * tk.ldc] = cv[j] - sgn * acc[j];
+            for (int j = 0; j < 8; ++j) {
+              const int col = n0 + c0 + g + j;
+              cv[j] = (ld && col < N) ? D[(int64_t)row + (int64_t)col * ldD] : 0.0f;
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const int col = n0 + c0 + g + j;
+              if (col < N) C[(int64_t)row + (int64_t)col * tk.ldc] = cv[j] - sgn * acc[g + j];
+            }
           }
         }
       }

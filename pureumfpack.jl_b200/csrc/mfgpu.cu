@@ -111,6 +111,7 @@ struct SolveSchedule {
     int64_t tiles_tc = 0;   // GEMM steps: grid in 128 x 128 tensor-core tiles (gemms_tc)
     int64_t sk_first = 0, sk_count = 0, sk_parts = 0, sk_reds = 0;   // split-K form (few rhs)
     int32_t level = -1;     // tree level (small-supernode steps run beside the level's large ones)
+    int32_t max_k = 0;      // GEMM steps: largest K of their tasks
   };
   std::vector<Step> steps;
   std::vector<int32_t> ids;
@@ -525,6 +526,8 @@ void configure_kernels() {
                           (int)TcCfg<128, 3>::kSmem));
   CK(cudaFuncSetAttribute(k_gemm_bx3<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)BxCfg<128, 2>::kSmem));
+  CK(cudaFuncSetAttribute(k_gemm_bx3<128, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)BxCfg<128, 1, 1>::kSmem));
   CK(cudaFuncSetAttribute(k_solve_persistent<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)persistent_smem_bytes<T>()));
   done = true;
@@ -581,10 +584,14 @@ bool gemm_use_tc(const mfgpu_ctx* h, int64_t id, bool dflt) {
 }
 
 // One tensor-core GEMM launch over 128 x 128-tiled tasks: BF16x3 (default)
-// or 3xTF32 (MFGPU_FLAG_TF32_SPLIT).
+// or 3xTF32 (MFGPU_FLAG_TF32_SPLIT); BF16x3 launches whose tasks all have
+// K <= 64 (max_k) take the one-stage, one-accumulator form, two CTAs per SM.
 void launch_tc(const mfgpu_ctx* h, const GemmTask* tasks, int64_t count, int64_t tiles, const float* pa,
-               const float* pb, float* pc, cudaStream_t st) {
-  if (h->tc_bf16x3)
+               const float* pb, float* pc, cudaStream_t st, int32_t max_k) {
+  if (h->tc_bf16x3 && max_k <= BxCfg<128, 1, 1>::BK)
+    k_gemm_bx3<128, 1, 1><<<(unsigned)tiles, kBxThreads, BxCfg<128, 1, 1>::kSmem, st>>>(
+        tasks, (int)count, pa, pb, pc, h->b_flags.as<int>(), h->wait_ns);
+  else if (h->tc_bf16x3)
     k_gemm_bx3<128, 2><<<(unsigned)tiles, kBxThreads, BxCfg<128, 2>::kSmem, st>>>(tasks, (int)count, pa, pb, pc,
                                                                                   h->b_flags.as<int>(), h->wait_ns);
   else
@@ -694,7 +701,7 @@ void run_factor_launches(mfgpu_ctx* h) {
         if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, tc_worthwhile(L.flops, L.tiles_tc)))
           klaunch(h, KC_GEMM_FACTOR, L.flops, bytes, [&] {
             launch_tc(h, h->b_gemm_tc.as<GemmTask>() + L.first, L.count, L.tiles_tc, (const float*)pool,
-                      (const float*)pool, (float*)pool, st);
+                      (const float*)pool, (float*)pool, st, L.max_k);
           }, L.level, L.tiles_tc);
         else
           klaunch(h, KC_GEMM_FACTOR, L.flops, bytes, [&] {
@@ -770,7 +777,7 @@ void issue_inverses(mfgpu_ctx* h) {
     if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, tc_worthwhile(is.flops, is.tiles_tc)))
       klaunch(h, KC_INVERSE, is.flops, is.elems * sizeof(T), [&] {
         launch_tc(h, h->b_inv_tasks_tc.as<GemmTask>() + is.first, is.count, is.tiles_tc, (const float*)pool,
-                  (const float*)pool, (float*)pool, st);
+                  (const float*)pool, (float*)pool, st, is.max_k);
       }, -3, is.tiles_tc);
     else
       klaunch(h, KC_INVERSE, is.flops, is.elems * sizeof(T), [&] {
@@ -988,6 +995,7 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
     st.tiles_tc += (int64_t)g.tiles_m * g.tiles_n;
     S.gemms_tc.push_back(g);
     ++st.count;
+    st.max_k = std::max(st.max_k, k);
     st.flops += 2.0 * m * nn * k;
     st.elems += (double)m * nn * (mode == kGemmSet ? 1 : 2) + (double)m * k + (double)k * nn;
   };
@@ -1260,7 +1268,7 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
         else if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, R >= 64 && tc_worthwhile(s.flops, s.tiles_tc)))
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
             launch_tc(h, S.d_gemms_tc.as<GemmTask>() + s.first, s.count, s.tiles_tc, (const float*)pool,
-                      (const float*)fsol, (float*)fsol, st);
+                      (const float*)fsol, (float*)fsol, st, s.max_k);
           }, s.level, s.tiles_tc);
         else
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {

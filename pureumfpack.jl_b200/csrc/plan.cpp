@@ -100,6 +100,7 @@ void push_inv(Plan& P, InvStep& st, GemmTask g) {
   st.tiles_tc += (int64_t)g.tiles_m * g.tiles_n;
   P.inv_tasks_tc.push_back(g);
   ++st.count;
+  st.max_k = std::max(st.max_k, g.k);
   st.flops += 2.0 * g.m * g.n * g.k;
   st.elems += (double)g.m * g.n * (g.mode == kGemmSub || g.mode == kGemmFrom ? 2 : 1) + (double)g.m * g.k +
               (double)g.k * g.n;
@@ -771,6 +772,7 @@ void push_gemm(Plan& P, Launch& lg, const GemmTask& g0) {
   lg.tiles_tc += (int64_t)g.tiles_m * g.tiles_n;
   P.gemm_tasks_tc.push_back(g);
   ++lg.count;
+  lg.max_k = std::max(lg.max_k, g.k);
 }
 
 void build_launches_core(Plan& P, bool safe) {

@@ -82,6 +82,7 @@ struct GemmTask {        // column-major, offsets in elements of the launch's ba
 struct InvStep {
   int64_t first, count, tiles, tiles_tc;
   double flops, elems;
+  int32_t max_k = 0;     // largest K of its tasks
 };
 
 enum LaunchKind : int32_t {
@@ -101,6 +102,7 @@ struct Launch {
   int64_t tiles;         // grid size in tiles for TRSM / GEMM
   int64_t tiles_tc = 0;  // GEMM launches: grid size in 128 x 128 tensor-core tiles
   int32_t rows = 0;      // panel launches: row capacity (threads) of the kernel variant
+  int32_t max_k = 0;     // GEMM launches: largest K of its tasks
   double flops = 0;      // algorithmic flops of the launch
   double elems = 0;      // algorithmic element moves (x sizeof(front type) = bytes)
   double extra_bytes = 0;// index / FP64 input bytes

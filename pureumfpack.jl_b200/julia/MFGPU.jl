@@ -18,6 +18,7 @@ mutable struct Handle
     ptr::Ptr{Cvoid}
     n::Int
     f32::Bool   # the last factorization is of a Float32 matrix
+    c64::Bool   # the last factorization is of a ComplexF64 matrix
 end
 
 # The C ABI takes Int64 indices; a SparseMatrixCSC{Tv, Int32} (the reference's
@@ -41,14 +42,14 @@ function create(; device::Integer = 0, precision::Integer = 0)
     out = Ref{Ptr{Cvoid}}(C_NULL)
     rc = ccall((:mfgpu_create, libmfgpu), Cint, (Ref{NTuple{4, Int32}}, Ref{Ptr{Cvoid}}), opts, out)
     rc == 0 || error("mfgpu_create failed ($rc)")
-    h = Handle(out[], 0, false)
+    h = Handle(out[], 0, false, false)
     finalizer(x -> ccall((:mfgpu_destroy, libmfgpu), Cvoid, (Ptr{Cvoid},), x.ptr), h)
     return h
 end
 
 # mfgpu_analyze from the reference's SymbolicMF (src/symbolic.jl:203-209):
 # update set of supernode s = colstruct[sstart[s+1]-1].
-function analyze!(h::Handle, A::SparseMatrixCSC{<:Union{Float64, Float32}, <:Integer}, S)
+function analyze!(h::Handle, A::SparseMatrixCSC{<:Union{Float64, Float32, ComplexF64}, <:Integer}, S)
     n = size(A, 2)
     nsuper = length(S.sstart) - 1
     upd_ptr = Vector{Int64}(undef, nsuper + 1)
@@ -77,6 +78,7 @@ function factor!(h::Handle, A::SparseMatrixCSC{Float64, <:Integer}, Rs, check::B
     st = _check(h, rc)
     st > 0 && throw(Main.LinearAlgebra.SingularException(st))
     h.f32 = false
+    h.c64 = false
     return h
 end
 
@@ -89,6 +91,21 @@ function factor!(h::Handle, A::SparseMatrixCSC{Float32, <:Integer}, Rs, check::B
     st = _check(h, rc)
     st > 0 && throw(Main.LinearAlgebra.SingularException(st))
     h.f32 = true
+    h.c64 = false
+    return h
+end
+
+# ComplexF64 matrices (the reference's generic Tv = ComplexF64): complex
+# values, factors, right-hand sides and solutions in Julia's own layout; real
+# Rs (row_scaling with R = real(Tv)).
+function factor!(h::Handle, A::SparseMatrixCSC{ComplexF64, <:Integer}, Rs, check::Bool)
+    rs = Rs === nothing ? C_NULL : pointer(Rs)
+    rc = GC.@preserve Rs ccall((:mfgpu_factor_c64, libmfgpu), Cint, (Ptr{Cvoid}, Ptr{ComplexF64}, Ptr{Float64}, Int32),
+        h.ptr, nonzeros(A), rs, Int32(check))
+    st = _check(h, rc)
+    st > 0 && throw(Main.LinearAlgebra.SingularException(st))
+    h.f32 = false
+    h.c64 = true
     return h
 end
 
@@ -96,6 +113,7 @@ end
 # index type Ti (that of the factored matrix).
 function factors(h::Handle; indextype::Type{<:Integer} = Int64)
     h.f32 && return factors_f32(h; indextype = indextype)
+    h.c64 && return factors_c64(h; indextype = indextype)
     sz = Vector{Int64}(undef, 3)
     _check(h, ccall((:mfgpu_factor_sizes, libmfgpu), Cint, (Ptr{Cvoid}, Ptr{Int64}), h.ptr, sz))
     n, nl, nu = sz
@@ -123,6 +141,29 @@ function factors_f32(h::Handle; indextype::Type{<:Integer} = Int64)
     T = indextype
     return SparseMatrixCSC(n, n, _ti(T, Lp), _ti(T, Li), Lx), SparseMatrixCSC(n, n, _ti(T, Up), _ti(T, Ui), Ux),
            _ti(T, p), _ti(T, q), _ti(T, pinv)
+end
+
+function factors_c64(h::Handle; indextype::Type{<:Integer} = Int64)
+    sz = Vector{Int64}(undef, 3)
+    _check(h, ccall((:mfgpu_factor_sizes, libmfgpu), Cint, (Ptr{Cvoid}, Ptr{Int64}), h.ptr, sz))
+    n, nl, nu = sz
+    Lp = Vector{Int64}(undef, n + 1); Li = Vector{Int64}(undef, nl); Lx = Vector{ComplexF64}(undef, nl)
+    Up = Vector{Int64}(undef, n + 1); Ui = Vector{Int64}(undef, nu); Ux = Vector{ComplexF64}(undef, nu)
+    p = Vector{Int64}(undef, n); q = Vector{Int64}(undef, n); pinv = Vector{Int64}(undef, n)
+    _check(h, ccall((:mfgpu_get_factors_c64, libmfgpu), Cint,
+        (Ptr{Cvoid}, Ptr{Int64}, Ptr{Int64}, Ptr{ComplexF64}, Ptr{Int64}, Ptr{Int64}, Ptr{ComplexF64}, Ptr{Int64},
+         Ptr{Int64}, Ptr{Int64}), h.ptr, Lp, Li, Lx, Up, Ui, Ux, p, q, pinv))
+    T = indextype
+    return SparseMatrixCSC(n, n, _ti(T, Lp), _ti(T, Li), Lx), SparseMatrixCSC(n, n, _ti(T, Up), _ti(T, Ui), Ux),
+           _ti(T, p), _ti(T, q), _ti(T, pinv)
+end
+
+function solve(h::Handle, B::AbstractVecOrMat{ComplexF64}; refine::Integer = 0)
+    Bc = Matrix{ComplexF64}(reshape(B, size(B, 1), :))
+    X = similar(Bc)
+    _check(h, ccall((:mfgpu_solve_c64, libmfgpu), Cint, (Ptr{Cvoid}, Int64, Ptr{ComplexF64}, Ptr{ComplexF64}, Int32),
+        h.ptr, size(Bc, 2), Bc, X, Int32(refine)))
+    return B isa AbstractVector ? vec(X) : X
 end
 
 function solve(h::Handle, B::AbstractVecOrMat{Float32}; refine::Integer = 0)
