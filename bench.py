@@ -687,15 +687,16 @@ def main():
             lib = ctx._lib
             import ctypes
 
+            dp = ctypes.POINTER(ctypes.c_double)
+
             def e2e_step():
-                rc = lib.mfgpu_factor(ctx._h, ctypes.cast(h_ax.data_ptr(), ctypes.POINTER(ctypes.c_double)),
-                                      ctypes.cast(h_rs.data_ptr(), ctypes.POINTER(ctypes.c_double)), 1)
+                # solve(splu(A), B; refine) through one C-ABI call: the
+                # right-hand sides cross the bus while the factorization runs
+                rc = lib.mfgpu_factor_solve(ctx._h, ctypes.cast(h_ax.data_ptr(), dp),
+                                            ctypes.cast(h_rs.data_ptr(), dp), 1, R, ctypes.cast(h_b.data_ptr(), dp),
+                                            n, ctypes.cast(h_x.data_ptr(), dp), n, refine)
                 if rc != 0:
-                    raise RuntimeError(f"mfgpu_factor -> {rc}")
-                rc = lib.mfgpu_solve(ctx._h, R, ctypes.cast(h_b.data_ptr(), ctypes.POINTER(ctypes.c_double)), n,
-                                     ctypes.cast(h_x.data_ptr(), ctypes.POINTER(ctypes.c_double)), n, refine)
-                if rc != 0:
-                    raise RuntimeError(f"mfgpu_solve -> {rc}")
+                    raise RuntimeError(f"mfgpu_factor_solve -> {rc}")
 
             e2e_step()
             torch.cuda.synchronize()

@@ -217,6 +217,13 @@ int mfgpu_get_factors(mfgpu_ctx* h, int64_t* lcolptr, int64_t* lrowval, double* 
  * residual r = b - A x uses the unscaled A values given there
  * (src/interface.jl:123-138, 170-177; src/solve.jl:10-39). */
 int mfgpu_solve(mfgpu_ctx* h, int64_t nrhs, const double* b, int64_t ldb, double* x, int64_t ldx, int32_t refine);
+/* mfgpu_factor then mfgpu_solve in one call -- solve(splu(A), b; refine) --
+ * with the right-hand sides' host-to-device copy on a stream of its own,
+ * overlapped with the factorization (fully when b is page-locked).  Returns
+ * the factor status (a positive singular column when check is set: no solve
+ * is done) or the solve's status; x is that of mfgpu_solve, bit for bit. */
+int mfgpu_factor_solve(mfgpu_ctx* h, const double* nzval, const double* rs, int32_t check, int64_t nrhs,
+                       const double* b, int64_t ldb, double* x, int64_t ldx, int32_t refine);
 /* Same with device pointers. */
 int mfgpu_solve_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, int64_t ldb, double* d_x, int64_t ldx,
                        int32_t refine);

@@ -177,6 +177,8 @@ struct mfgpu_ctx {
   int precision = MFGPU_PRECISION_FP64;
   cudaStream_t own_stream = nullptr;
   cudaStream_t side_stream = nullptr;     // a level's small supernodes, beside its large ones
+  cudaStream_t copy_stream = nullptr;     // right-hand sides in flight during a factorization
+  cudaEvent_t ev_copy = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaStream_t stream = nullptr;
   std::string err;
@@ -1477,6 +1479,8 @@ int mfgpu_create(const mfgpu_options* opts, mfgpu_ctx** out) {
     h->num_sms = prop.multiProcessorCount;
     CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h->ev_copy, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
     h->stream = h->own_stream;
@@ -1517,6 +1521,8 @@ void mfgpu_destroy(mfgpu_ctx* h) {
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   if (h->side_stream) cudaStreamDestroy(h->side_stream);
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  if (h->ev_copy) cudaEventDestroy(h->ev_copy);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
   if (h->ev_join) cudaEventDestroy(h->ev_join);
   delete h;
@@ -1788,6 +1794,43 @@ static int get_factors_impl(mfgpu_ctx* h, int64_t* lcolptr, int64_t* lrowval, vo
       if (pinv) pinv[pk] = k + 1;
     }
     return MFGPU_OK;
+  });
+}
+
+int mfgpu_factor_solve(mfgpu_ctx* h, const double* nzval, const double* rs, int32_t check, int64_t nrhs,
+                       const double* b, int64_t ldb, double* x, int64_t ldx, int32_t refine) {
+  if (!h) return MFGPU_ERR_ARGUMENT;
+  if (!h->analyzed) return fail(h, MFGPU_ERR_STATE, "factor before analyze");
+  const int64_t n = h->plan.n;
+  if (nrhs < 0 || ldb < n || ldx < n || refine < 0 || (nrhs && n && (!b || !x)))
+    return fail(h, MFGPU_ERR_ARGUMENT, "bad solve sizes");
+  // the right-hand sides cross the bus on their own stream while the
+  // factorization runs (overlapped when b is page-locked)
+  const bool copy = nrhs > 0 && n > 0;
+  int rc = guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->device));
+    if (copy) {
+      h->b_b.ensure((size_t)n * nrhs * 8);
+      h->b_x.ensure((size_t)n * nrhs * 8);
+      CK(cudaMemcpy2DAsync(h->b_b.p, n * 8, b, ldb * 8, n * 8, nrhs, cudaMemcpyHostToDevice, h->copy_stream));
+      CK(cudaEventRecord(h->ev_copy, h->copy_stream));
+    }
+    return MFGPU_OK;
+  });
+  if (rc != MFGPU_OK) return rc;
+  rc = factor_host(h, nzval, rs, check, false);
+  if (rc != MFGPU_OK || !copy) {
+    if (copy) cudaStreamSynchronize(h->copy_stream);   // b's buffer is not reused while the copy runs
+    return rc;   // a singular column (check) or an error: no solve
+  }
+  return guarded(h, [&]() -> int {
+    cudaStream_t st = h->stream;
+    CK(cudaStreamWaitEvent(st, h->ev_copy, 0));
+    solve_dispatch(h, nrhs, h->b_b.as<double>(), n, h->b_x.as<double>(), n, refine);
+    CK(cudaMemcpy2DAsync(x, ldx * 8, h->b_x.p, n * 8, n * 8, nrhs, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    prof_flush(h);
+    return solve_status(h);
   });
 }
 

@@ -61,6 +61,7 @@ SIGNATURES = [
     ("mfgpu_get_factors_c64", ctypes.c_int, [vp, i64p, i64p, f64p, i64p, i64p, f64p, i64p, i64p, i64p]),
     ("mfgpu_solve_c64", ctypes.c_int, [vp, i64, f64p, f64p, i32]),
     ("mfgpu_solve", ctypes.c_int, [vp, i64, f64p, i64, f64p, i64, i32]),
+    ("mfgpu_factor_solve", ctypes.c_int, [vp, f64p, f64p, i32, i64, f64p, i64, f64p, i64, i32]),
     ("mfgpu_solve_device", ctypes.c_int, [vp, i64, vp, i64, vp, i64, i32]),
     ("mfgpu_backward_error_device", ctypes.c_int, [vp, i64, vp, i64, vp, i64, f64p]),
     ("mfgpu_backward_error_noalloc", ctypes.c_int, [vp, i64, vp, i64, vp, i64, f64p]),

@@ -415,6 +415,20 @@ class GpuContext:
         self._check(self._lib.mfgpu_solve(self._h, nrhs, L.ptr(B, L.f64p), n, L.ptr(X, L.f64p), n, int(refine)))
         return X
 
+    def factor_solve(self, nzval, Rs, b, refine: int = 0, check: bool = True):
+        """factor(nzval, Rs) then solve(b, refine) in one call, the
+        right-hand sides' copy overlapped with the factorization.  Returns
+        (status, x); x is None when the factorization found a singular column."""
+        rs = _f(Rs) if Rs is not None else None
+        B = np.asfortranarray(b, dtype=np.float64)
+        nrhs = 1 if B.ndim == 1 else B.shape[1]
+        X = np.empty_like(B)
+        self.f32 = self.c64 = False
+        st = self._check(self._lib.mfgpu_factor_solve(self._h, L.ptr(_f(nzval), L.f64p), L.ptr(rs, L.f64p),
+                                                      int(check), nrhs, L.ptr(B, L.f64p), B.shape[0],
+                                                      L.ptr(X, L.f64p), B.shape[0], int(refine)))
+        return st, (X if st == 0 else None)
+
     def solve_device(self, nrhs: int, b_ptr: int, ldb: int, x_ptr: int, ldx: int, refine: int = 0):
         self._check(self._lib.mfgpu_solve_device(self._h, nrhs, ctypes.c_void_p(b_ptr), ldb, ctypes.c_void_p(x_ptr),
                                                  ldx, int(refine)))
