@@ -241,7 +241,8 @@ __global__ void __launch_bounds__(32 * tiny_warps<T>()) k_bwd_tiny(DevPlan P, So
 }
 
 // Large supernodes: gather the rhs block, one warp per right-hand side;
-// item (bx, by) covers columns by * warps .. of supernode tasks[bx].
+// item (bx, by) covers columns by * warps .. of supernode tasks[bx] (the
+// persistent solve's form; the step launches use k_fwd_assemble_rows).
 template <typename T>
 __device__ __forceinline__ void fwd_assemble_item(const DevPlan& P, const DevState& S, const SolveArgs& A,
                                                   const int32_t* __restrict__ tasks, T* fsol, int bx, int by) {
@@ -280,12 +281,6 @@ __device__ __forceinline__ void fwd_assemble_item(const DevPlan& P, const DevSta
     for (; r < m; r += 32) f[front_pos(S, c1, np, rl[r])] += w[r];
     __syncwarp();
   }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(256) k_fwd_assemble(DevPlan P, DevState S, SolveArgs A,
-                                                      const int32_t* __restrict__ tasks, T* fsol) {
-  fwd_assemble_item<T>(P, S, A, tasks, fsol, blockIdx.x, blockIdx.y);
 }
 
 // Small supernodes, backward.  smem: 2 * kSmallFront * kSolveCols elements.
@@ -344,7 +339,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_small(DevPlan P, SolveArg
   bwd_small_item<T>(P, A, tasks, pool, fsol, xw, blockIdx.x, blockIdx.y, y);
 }
 
-// Large supernodes: gather x of the update columns into the w rows.
+// Large supernodes: gather x of the update columns into the w rows (the
+// persistent solve's form; the step launches use k_bwd_gather_rows).
 template <typename T>
 __device__ __forceinline__ void bwd_gather_item(const DevPlan& P, const SolveArgs& A,
                                                 const int32_t* __restrict__ tasks, T* fsol, const T* xw, int bx,
@@ -360,10 +356,124 @@ __device__ __forceinline__ void bwd_gather_item(const DevPlan& P, const SolveArg
   for (int t = lane_id(); t < nu; t += 32) f[t] = xw[us[t] + col * A.ldx];
 }
 
+// Row-parallel forms of the two gathers above, for the one-launch-per-step
+// solve.  The per-column warps above walk a whole front per column, which
+// leaves the GPU idle at the top of the tree (one front: nrhs warps).  Here
+// a CTA takes four 64-row tasks (supernode s, first row r0) and kAsmCols
+// right-hand sides; each thread owns one row.
+constexpr int kAsmRows = 64;
+constexpr int kAsmCols = 8;
+
+struct RowTask {
+  int32_t s, r0;
+  int64_t pbase;          // forward: index of the front's row 0 in the pull map's row pointers
+};
+
+// Forward assembly pulled per front row.  The pull map lists, for V-row
+// position v of front s (rows aptr[pbase + v] .. aptr[pbase + v + 1] of
+// asrc), the (child, update row) pairs that land on v, children in the LIFO
+// order of the extend-add; the thread owning v starts from the pivot row's
+// rhs (or 0) and adds them in that order, so every front row gets the same
+// sum, in the same order, as fwd_assemble_item, and v -> front_pos(v) is a
+// bijection: no two threads write one element.
 template <typename T>
-__global__ void __launch_bounds__(256) k_bwd_gather(DevPlan P, SolveArgs A, const int32_t* __restrict__ tasks,
-                                                    T* fsol, const T* xw) {
-  bwd_gather_item<T>(P, A, tasks, fsol, xw, blockIdx.x, blockIdx.y);
+__global__ void __launch_bounds__(256) k_fwd_assemble_rows(DevPlan P, DevState S, SolveArgs A,
+                                                           const RowTask* __restrict__ tasks, int ntasks,
+                                                           const int64_t* __restrict__ aptr,
+                                                           const int2* __restrict__ asrc, T* fsol) {
+  const int ti = blockIdx.x * 4 + (threadIdx.x >> 6);
+  if (ti >= ntasks) return;
+  const RowTask rt = tasks[ti];
+  const int s = rt.s;
+  const int v = rt.r0 + (threadIdx.x & 63);
+  const int nf = P.nf[s];
+  if (v >= nf) return;
+  const int np = P.np[s], c1 = P.c1[s];
+  const int p = front_pos(S, c1, np, v);
+  const int64_t R = A.nrhs;
+  const int64_t c0 = (int64_t)blockIdx.y * kAsmCols;
+  const int cc = (int)(R - c0 < kAsmCols ? R - c0 : kAsmCols);
+  T acc[kAsmCols];
+#pragma unroll
+  for (int c = 0; c < kAsmCols; ++c) acc[c] = (c < cc && p < np) ? rhs_value<T>(A, c1, p, c0 + c) : T(0);
+  const int64_t e1 = aptr[rt.pbase + v + 1];
+  for (int64_t e = aptr[rt.pbase + v]; e < e1; ++e) {
+    const int2 src = asrc[e];
+    const int nfk = P.nf[src.x];
+    const T* w = fsol + P.colbase[src.x] * R + P.np[src.x] + src.y + c0 * nfk;
+    T t[kAsmCols];
+#pragma unroll
+    for (int c = 0; c < kAsmCols; ++c) t[c] = c < cc ? w[(int64_t)c * nfk] : T(0);
+#pragma unroll
+    for (int c = 0; c < kAsmCols; ++c) acc[c] += t[c];
+  }
+  T* f = fsol + P.colbase[s] * R + p + c0 * nf;
+#pragma unroll
+  for (int c = 0; c < kAsmCols; ++c)
+    if (c < cc) f[(int64_t)c * nf] = acc[c];
+}
+
+// Backward gather, one update row per thread (tasks cover 0 .. nu).
+template <typename T>
+__global__ void __launch_bounds__(256) k_bwd_gather_rows(DevPlan P, SolveArgs A, const RowTask* __restrict__ tasks,
+                                                         int ntasks, T* fsol, const T* xw) {
+  const int ti = blockIdx.x * 4 + (threadIdx.x >> 6);
+  if (ti >= ntasks) return;
+  const RowTask rt = tasks[ti];
+  const int s = rt.s;
+  const int t = rt.r0 + (threadIdx.x & 63);
+  const int nu = P.nu[s];
+  if (t >= nu) return;
+  const int np = P.np[s], nf = P.nf[s];
+  const int64_t R = A.nrhs;
+  const int64_t c0 = (int64_t)blockIdx.y * kAsmCols;
+  const int cc = (int)(R - c0 < kAsmCols ? R - c0 : kAsmCols);
+  const T* src = xw + P.upd[P.upd_off[s] + t] + c0 * A.ldx;
+  T* f = fsol + P.colbase[s] * R + np + t + c0 * nf;
+  T v[kAsmCols];
+#pragma unroll
+  for (int c = 0; c < kAsmCols; ++c) v[c] = c < cc ? src[(int64_t)c * A.ldx] : T(0);
+#pragma unroll
+  for (int c = 0; c < kAsmCols; ++c)
+    if (c < cc) f[(int64_t)c * nf] = v[c];
+}
+
+// Split-K solve products: a product with few output tiles and a long K runs
+// as K chunks -- the first in the task's own mode on C, the others as plain
+// products into a scratch area -- and this kernel then folds the partial
+// products into C in chunk order: C += sign * P_1, C += sign * P_2, ...
+// (sign -1 for the C - A*B modes and C = -(A*B), +1 for C = A*B).  One
+// thread per element of C; deterministic.
+struct SplitRed {
+  int64_t c, p;           // C's offset (leading dimension ldc); the partial products (m x n each, ld m)
+  int32_t m, n, ldc, parts;
+  int32_t sign, pad;
+  int64_t elem_base;      // prefix of m * n over the step's reductions
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_split_reduce(const SplitRed* __restrict__ reds, int nreds, int64_t total,
+                                                      T* base) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= total) return;
+  int lo = 0, hi = nreds - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (reds[mid].elem_base <= e) lo = mid;
+    else hi = mid - 1;
+  }
+  const SplitRed rd = reds[lo];
+  const int64_t l = e - rd.elem_base;
+  const int64_t i = l % rd.m, j = l / rd.m;
+  const int64_t mn = (int64_t)rd.m * rd.n;
+  T* c = base + rd.c + i + j * rd.ldc;
+  const T* p = base + rd.p + l;
+  T acc = *c;
+  if (rd.sign < 0)
+    for (int q = 0; q < rd.parts; ++q) acc -= p[q * mn];
+  else
+    for (int q = 0; q < rd.parts; ++q) acc += p[q * mn];
+  *c = acc;
 }
 
 // x[q[k]] = x_factor[k] (interface.jl:134-136); optionally accumulate (x += d).

@@ -112,6 +112,12 @@ struct SolveSchedule {
     int64_t sk_first = 0, sk_count = 0, sk_parts = 0, sk_reds = 0;   // split-K form (few rhs)
     int32_t level = -1;     // tree level (small-supernode steps run beside the level's large ones)
     int32_t max_k = 0;      // GEMM steps: largest K of their tasks
+    int64_t rt_first = 0, rt_count = 0;   // assemble / gather steps: their row tasks
+    // GEMM steps with few tiles and a long K: the K-chunked form (tasks in
+    // sgemms / sgemms_tc, then the reductions sreds[rd_first ..])
+    int64_t sp_first = 0, sp_count = 0, sp_tiles = 0, sp_tiles_tc = 0;
+    int32_t sp_max_k = 0;
+    int64_t rd_first = 0, rd_count = 0, rd_elems = 0;
   };
   std::vector<Step> steps;
   std::vector<int32_t> ids;
@@ -119,7 +125,16 @@ struct SolveSchedule {
   std::vector<SkinnyTask> skinny;          // split-K form of every GEMM step when nrhs <= kSkinnyMaxN
   int64_t skinny_scratch = 0;              // partial sums, elements
   std::vector<SolvePhase> phases;   // the steps as work-item phases of the persistent solve
-  DevBuf d_ids, d_gemms, d_gemms_tc, d_phases, d_skinny;
+  // one-launch-per-step solve only: row tasks of the assemble / gather
+  // steps, the forward pull map, the K-chunked GEMM steps
+  std::vector<RowTask> rows;
+  std::vector<int64_t> aptr;
+  std::vector<int2> asrc;
+  std::vector<GemmTask> sgemms, sgemms_tc;
+  std::vector<SplitRed> sreds;
+  int64_t split_scratch = 0;        // partial products, elements (after x in the solve arena)
+  int elem = 0;                     // front element size the K chunks were chosen for
+  DevBuf d_ids, d_gemms, d_gemms_tc, d_phases, d_skinny, d_rows, d_aptr, d_asrc, d_sgemms, d_sgemms_tc, d_sreds;
 };
 
 }  // namespace
@@ -966,12 +981,19 @@ int factor_dispatch(mfgpu_ctx* h, int32_t check) {
 }
 
 // ---- solves ---------------------------------------------------------------
-void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
+// Product steps of the one-launch-per-step solve with fewer output tiles
+// than SMs and a K of at least kSplitMinK run K-chunked: chunks of at least
+// kSplitMinKC (a multiple of 64), as many as give about two tiles per SM.
+constexpr int32_t kSplitMinK = 384;
+constexpr int32_t kSplitMinKC = 128;
+
+void build_solve_schedule(mfgpu_ctx* h, int64_t R, int elem) {
   SolveSchedule& S = h->sched;
-  if (S.nrhs == R) return;
+  if (S.nrhs == R && S.elem == elem) return;
   const Plan& P = h->plan;
   S = SolveSchedule{};
   S.nrhs = R;
+  S.elem = elem;
   auto ceil_div = [](int64_t a, int64_t b) { return (a + b - 1) / b; };
   // offsets: A operands in the front pool (fronts and pivot-block inverses);
   // B, C and D in the solve arena: the per-supernode blocks (nf x R each,
@@ -1130,6 +1152,111 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
       S.skinny_scratch = std::max<int64_t>(S.skinny_scratch, st.sk_parts * kSkinnyRows * nmax);
     }
   }
+  // row tasks of the assemble / gather steps, and the forward pull map: for
+  // each V-row position v of a large front, the (child, update row) pairs
+  // that the extend-add adds at v, children in LIFO order
+  for (auto& st : S.steps) {
+    if (st.kind != 1 && st.kind != 5) continue;
+    st.rt_first = (int64_t)S.rows.size();
+    for (int64_t i = st.first; i < st.first + st.count; ++i) {
+      const int32_t s = S.ids[i];
+      const int nf = P.nf[s];
+      int64_t pbase = 0;
+      if (st.kind == 1) {
+        pbase = (int64_t)S.aptr.size();
+        std::vector<int64_t> pos(nf + 1, 0);
+        for (int32_t ci = P.child_ptr[s]; ci < P.child_ptr[s + 1]; ++ci) {
+          const int32_t k = P.child_idx[ci];
+          for (int32_t r = 0; r < P.nu[k]; ++r) ++pos[P.rel[P.upd_off[k] + r] + 1];
+        }
+        const int64_t e0 = (int64_t)S.asrc.size();
+        for (int v = 0; v < nf; ++v) {
+          pos[v + 1] += pos[v];
+          S.aptr.push_back(e0 + pos[v]);
+        }
+        S.asrc.resize(e0 + pos[nf]);
+        for (int32_t ci = P.child_ptr[s + 1] - 1; ci >= P.child_ptr[s]; --ci) {
+          const int32_t k = P.child_idx[ci];
+          for (int32_t r = 0; r < P.nu[k]; ++r) S.asrc[e0 + pos[P.rel[P.upd_off[k] + r]]++] = make_int2(k, r);
+          st.elems += (double)P.nu[k] * R;
+        }
+        st.elems += ((double)nf + P.np[s]) * R;
+      } else {
+        st.elems += 2.0 * P.nu[s] * R;
+      }
+      const int rows = st.kind == 1 ? nf : P.nu[s];
+      for (int r0 = 0; r0 < rows; r0 += kAsmRows) S.rows.push_back({s, r0, pbase});
+    }
+    st.rt_count = (int64_t)S.rows.size() - st.rt_first;
+  }
+  S.aptr.push_back((int64_t)S.asrc.size());
+  // K-chunked form of the product steps with few tiles (many right-hand
+  // sides; the split-K form above serves few): tiles counted in the tiling
+  // the element type runs on (128 x 128 for FP32 fronts, else 64 x 64)
+  if (R > kSkinnyMaxN) {
+    const int64_t scratch_base = xw0 + P.n * R;
+    for (auto& st : S.steps) {
+      if (st.kind != 3 || st.max_k < kSplitMinK) continue;
+      const int64_t tiles = elem == 4 ? st.tiles_tc : st.tiles;
+      if (tiles >= h->num_sms) continue;
+      const int64_t parts = ceil_div(2 * (int64_t)h->num_sms, std::max<int64_t>(1, tiles));
+      const int32_t kc = std::max<int32_t>(kSplitMinKC, (int32_t)(ceil_div(ceil_div(st.max_k, parts), 64) * 64));
+      if (kc >= st.max_k) continue;
+      st.sp_first = (int64_t)S.sgemms.size();
+      st.rd_first = (int64_t)S.sreds.size();
+      int64_t scratch = 0;
+      auto push_tiled = [&](GemmTask t) {
+        t.tiles_m = (int)ceil_div(t.m, 64);
+        t.tiles_n = (int)ceil_div(t.n, 64);
+        t.tile_base = st.sp_tiles;
+        st.sp_tiles += (int64_t)t.tiles_m * t.tiles_n;
+        S.sgemms.push_back(t);
+        t.tiles_m = (int)ceil_div(t.m, kTcTile);
+        t.tiles_n = (int)ceil_div(t.n, kTcTile);
+        t.tile_base = st.sp_tiles_tc;
+        st.sp_tiles_tc += (int64_t)t.tiles_m * t.tiles_n;
+        S.sgemms_tc.push_back(t);
+        st.sp_max_k = std::max(st.sp_max_k, t.k);
+      };
+      for (int64_t i = st.first; i < st.first + st.count; ++i) {
+        const GemmTask g = S.gemms[i];
+        const int32_t nch = (int32_t)std::max<int64_t>(1, ceil_div(g.k, kc));
+        const int64_t mn = (int64_t)g.m * g.n;
+        for (int32_t q = 0; q < nch; ++q) {
+          GemmTask t = g;
+          const int32_t k0 = q * kc;
+          t.k = std::min(kc, g.k - k0);
+          t.a = g.a + (int64_t)k0 * g.lda;
+          t.b = g.b + k0;
+          if (q > 0) {   // a plain product into the scratch area
+            t.mode = kGemmSet;
+            t.c = scratch_base + scratch + (q - 1) * mn;
+            t.ldc = g.m;
+            t.d = 0;
+            t.ldd = 0;
+          }
+          push_tiled(t);
+        }
+        if (nch > 1) {
+          SplitRed rd{};
+          rd.c = g.c;
+          rd.p = scratch_base + scratch;
+          rd.m = g.m;
+          rd.n = g.n;
+          rd.ldc = g.ldc;
+          rd.parts = nch - 1;
+          rd.sign = g.mode == kGemmSet ? 1 : -1;
+          rd.elem_base = st.rd_elems;
+          st.rd_elems += mn;
+          S.sreds.push_back(rd);
+          scratch += (nch - 1) * mn;
+        }
+      }
+      st.sp_count = (int64_t)S.sgemms.size() - st.sp_first;
+      st.rd_count = (int64_t)S.sreds.size() - st.rd_first;
+      S.split_scratch = std::max(S.split_scratch, scratch);
+    }
+  }
   // the same steps as phases of the persistent kernel (kSolveThreads per CTA:
   // kSolveThreads / 32 right-hand sides per gather item)
   const int64_t ych = ceil_div(R, kSolveCols), wch = ceil_div(R, kSolveThreads / 32);
@@ -1150,6 +1277,12 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R) {
   upload(S.d_gemms_tc, S.gemms_tc, h->stream);
   upload(S.d_skinny, S.skinny, h->stream);
   upload(S.d_phases, S.phases, h->stream);
+  upload(S.d_rows, S.rows, h->stream);
+  upload(S.d_aptr, S.aptr, h->stream);
+  upload(S.d_asrc, S.asrc, h->stream);
+  upload(S.d_sgemms, S.sgemms, h->stream);
+  upload(S.d_sgemms_tc, S.sgemms_tc, h->stream);
+  upload(S.d_sreds, S.sreds, h->stream);
 }
 
 // One solve A x = b for device b (ldb) into device x (ldx) (x overwritten, or
@@ -1158,9 +1291,10 @@ template <typename T>
 void prepare_solve(mfgpu_ctx* h, int64_t R, int refine) {
   const Plan& P = h->plan;
   h->persistent = h->persistent_mode == 1 && !is_complex_v<T>;   // complex fronts: per-step launches
-  build_solve_schedule(h, R);
-  // solve arena: the per-supernode blocks, then x in factor order
-  h->b_fsol.ensure(std::max<size_t>((size_t)(P.fc_total + P.n) * R * sizeof(T), 16));
+  build_solve_schedule(h, R, (int)sizeof(T));
+  // solve arena: the per-supernode blocks, then x in factor order, then the
+  // partial products of the K-chunked steps
+  h->b_fsol.ensure(std::max<size_t>(((size_t)(P.fc_total + P.n) * R + h->sched.split_scratch) * sizeof(T), 16));
   if (h->sched.skinny_scratch) h->b_skinny.ensure((size_t)h->sched.skinny_scratch * sizeof(T));
   if (refine > 0) h->b_r.ensure(std::max<size_t>((size_t)P.n * R * sizeof(Wide<T>), 16));
   configure_kernels<T>();
@@ -1196,7 +1330,8 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
                                                               h->b_prow.as<int32_t>(), xw, P.n);
   });
   const unsigned ychunks = (unsigned)((R + solve_cols<T>() - 1) / solve_cols<T>());
-  const unsigned wchunks = (unsigned)((R + 7) / 8);
+  const unsigned acols = (unsigned)((R + kAsmCols - 1) / kAsmCols);
+  const RowTask* rows = S.d_rows.as<RowTask>();
   const int32_t* ids = S.d_ids.as<int32_t>();
   const GemmTask* gemms = S.d_gemms.as<GemmTask>();
   int64_t tune_id = tune_factor_count(P) + (int64_t)P.inv_steps.size();
@@ -1240,16 +1375,33 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
         }, s.level, s.count);
         break;
       case 1:
-        klaunch(h, KC_FWD_ASSEMBLE, 0, 0, [&] {
-          k_fwd_assemble<T><<<dim3((unsigned)s.count, wchunks), 256, 0, st>>>(h->dp, DS, A, ids + s.first, fsol);
+        if (!s.rt_count) break;
+        klaunch(h, KC_FWD_ASSEMBLE, 0, bytes, [&] {
+          k_fwd_assemble_rows<T><<<dim3((unsigned)((s.rt_count + 3) / 4), acols), 256, 0, st>>>(
+              h->dp, DS, A, rows + s.rt_first, (int)s.rt_count, S.d_aptr.as<int64_t>(), S.d_asrc.as<int2>(), fsol);
         }, s.level, s.count);
         break;
-      case 3:
+      case 3: {
         h->cur_tune = (int32_t)tune_id;
+        // the K-chunked form when the step has one, its partial products
+        // folded into C right after the chunks
+        const bool split = s.sp_count > 0;
+        const GemmTask* g64 = split ? S.d_sgemms.as<GemmTask>() + s.sp_first : gemms + s.first;
+        const GemmTask* gtc = split ? S.d_sgemms_tc.as<GemmTask>() + s.sp_first
+                                    : S.d_gemms_tc.as<GemmTask>() + s.first;
+        const int64_t gcount = split ? s.sp_count : s.count;
+        const int64_t t64 = split ? s.sp_tiles : s.tiles, ttc = split ? s.sp_tiles_tc : s.tiles_tc;
+        const int32_t gmaxk = split ? s.sp_max_k : s.max_k;
+        auto fold = [&] {
+          if (split)
+            k_split_reduce<T><<<grid1(s.rd_elems, 256), 256, 0, st>>>(S.d_sreds.as<SplitRed>() + s.rd_first,
+                                                                      (int)s.rd_count, s.rd_elems, fsol);
+        };
         if constexpr (is_complex_v<T>)
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
-            launch_gemm<T>(gemms + s.first, s.count, s.tiles, pool, fsol, fsol, st);
-          }, s.level, s.tiles);
+            launch_gemm<T>(g64, gcount, t64, pool, fsol, fsol, st);
+            fold();
+          }, s.level, t64);
         else if (s.sk_count && !(sizeof(T) == 4 && gemm_use_tc(h, tune_id, false)))
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
             const SkinnyTask* sk = S.d_skinny.as<SkinnyTask>() + s.sk_first;
@@ -1267,18 +1419,20 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
                                                                                            fsol);
             }
           }, s.level, s.sk_parts);
-        else if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, R >= 64 && tc_worthwhile(s.flops, s.tiles_tc)))
+        else if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, R >= 64 && tc_worthwhile(s.flops, ttc)))
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
-            launch_tc(h, S.d_gemms_tc.as<GemmTask>() + s.first, s.count, s.tiles_tc, (const float*)pool,
-                      (const float*)fsol, (float*)fsol, st, s.max_k);
-          }, s.level, s.tiles_tc);
+            launch_tc(h, gtc, gcount, ttc, (const float*)pool, (const float*)fsol, (float*)fsol, st, gmaxk);
+            fold();
+          }, s.level, ttc);
         else
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
-            launch_gemm<T>(gemms + s.first, s.count, s.tiles, pool, fsol, fsol, st);
-          }, s.level, s.tiles);
+            launch_gemm<T>(g64, gcount, t64, pool, fsol, fsol, st);
+            fold();
+          }, s.level, t64);
         h->cur_tune = -1;
         ++tune_id;
         break;
+      }
       case 6:
         klaunch(h, KC_FWD_SMALL, s.flops, bytes, [&] {
           k_fwd_tiny<T><<<dim3((unsigned)((s.count + tiny_warps<T>() - 1) / tiny_warps<T>()), (unsigned)((R + 31) / 32)),
@@ -1298,8 +1452,10 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
         }, s.level, s.count);
         break;
       case 5:
-        klaunch(h, KC_BWD_GATHER, 0, 0, [&] {
-          k_bwd_gather<T><<<dim3((unsigned)s.count, wchunks), 256, 0, st>>>(h->dp, A, ids + s.first, fsol, xw);
+        if (!s.rt_count) break;   // roots only: no update rows to gather
+        klaunch(h, KC_BWD_GATHER, 0, bytes, [&] {
+          k_bwd_gather_rows<T><<<dim3((unsigned)((s.rt_count + 3) / 4), acols), 256, 0, st>>>(
+              h->dp, A, rows + s.rt_first, (int)s.rt_count, fsol, xw);
         }, s.level, s.count);
         break;
     }
@@ -1351,6 +1507,8 @@ void solve_graph(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<
       (uintptr_t)h->b_fsol.p, (uintptr_t)h->b_inv_tasks.p, (uintptr_t)h->b_r.p, (uintptr_t)h->b_ax.p,
       (uintptr_t)S.d_ids.p, (uintptr_t)S.d_gemms.p, (uintptr_t)S.d_phases.p, (uintptr_t)h->b_prow.p,
       (uintptr_t)S.d_gemms_tc.p, (uintptr_t)S.d_skinny.p, (uintptr_t)h->b_skinny.p, (uintptr_t)h->use_tc,
+      (uintptr_t)S.d_rows.p, (uintptr_t)S.d_aptr.p, (uintptr_t)S.d_asrc.p, (uintptr_t)S.d_sgemms.p,
+      (uintptr_t)S.d_sgemms_tc.p, (uintptr_t)S.d_sreds.p,
       (uintptr_t)h->tc_bf16x3, (uintptr_t)h->choice_version, (uintptr_t)h->wait_ns,
       (uintptr_t)h->persistent, (uintptr_t)h->b_bar.p,
       (uintptr_t)h->b_rowfac.p, (uintptr_t)h->stream};
@@ -1511,7 +1669,9 @@ void mfgpu_destroy(mfgpu_ctx* h) {
                     &h->b_o_np, &h->b_o_upd_off, &h->b_o_upd, &h->b_o_xpos, &h->b_fcu_ptr, &h->b_fcu,
                     &h->b_li, &h->b_lx, &h->b_ui,
                     &h->b_ux, &h->b_fsol, &h->b_b, &h->b_x, &h->b_f32, &h->b_r, &h->b_d, &h->b_err, &h->b_norm,
-                    &h->sched.d_ids, &h->sched.d_gemms, &h->sched.d_gemms_tc, &h->sched.d_phases, &h->b_bar,
+                    &h->sched.d_ids, &h->sched.d_gemms, &h->sched.d_gemms_tc, &h->sched.d_phases,
+                    &h->sched.d_rows, &h->sched.d_aptr, &h->sched.d_asrc, &h->sched.d_sgemms, &h->sched.d_sgemms_tc,
+                    &h->sched.d_sreds, &h->b_bar,
                     &h->b_stamps};
   for (DevBuf* b : bufs) b->release();
   if (h->factor_exec) cudaGraphExecDestroy(h->factor_exec);
@@ -1983,7 +2143,7 @@ int mfgpu_tune_features(mfgpu_ctx* h, int64_t nrhs, int64_t* count, float* feats
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->device));
     const Plan& P = h->plan;
-    build_solve_schedule(h, nrhs);
+    build_solve_schedule(h, nrhs, 4);
     const SolveSchedule& S = h->sched;
     std::vector<float> f;
     float row[kTuneFeatures];
@@ -1998,7 +2158,11 @@ int mfgpu_tune_features(mfgpu_ctx* h, int64_t nrhs, int64_t* count, float* feats
     }
     for (const auto& st : S.steps)
       if (st.kind == 3) {
-        tune_row(row, 2, S.gemms.data() + st.first, st.count, st.flops, st.elems, st.tiles, st.tiles_tc);
+        if (st.sp_count)   // the K-chunked form is the one that runs
+          tune_row(row, 2, S.sgemms.data() + st.sp_first, st.sp_count, st.flops, st.elems, st.sp_tiles,
+                   st.sp_tiles_tc);
+        else
+          tune_row(row, 2, S.gemms.data() + st.first, st.count, st.flops, st.elems, st.tiles, st.tiles_tc);
         f.insert(f.end(), row, row + kTuneFeatures);
       }
     *count = (int64_t)f.size() / kTuneFeatures;
