@@ -398,7 +398,8 @@ def roofline_of(P, primary, fp64_peak, peaks):
     return roof
 
 
-SOLVE_CLASSES = ("fwd_small", "fwd_assemble", "gemm_solve", "bwd_small", "bwd_gather", "solve_finish")
+SOLVE_CLASSES = ("fwd_small", "fwd_assemble", "fwd_thin", "gemm_solve", "bwd_small", "bwd_gather",
+                 "solve_finish")
 
 
 def class_rooflines(f, form, fp64_peak, peaks, nrhs):

@@ -60,6 +60,23 @@ __global__ void k_rhs_factor_order(int64_t n, int64_t nrhs, const Wide<T>* __res
   bfo[k + c * ldo] = (T)(rs ? Wide<T>(rs[orow]) * v : v);
 }
 
+// Element walk of a column-major rows x cols block by n threads with one
+// division per thread instead of one per element: thread t takes row
+// t % rows at columns t / rows, t / rows + n / rows, ... (threads from
+// (n / rows) * rows on take none).  Requires 0 < rows <= n.
+struct RowWalk {
+  int r, c, dc;
+  bool on;
+};
+__device__ __forceinline__ RowWalk row_walk(int t, int n, int rows) {
+  RowWalk w;
+  w.dc = n / rows;
+  w.r = t % rows;
+  w.c = t / rows;
+  w.on = w.c < w.dc;
+  return w;
+}
+
 // Pivot-row value of block position a: the scaled rhs of factor row c1 + a.
 template <typename T>
 __device__ __forceinline__ T rhs_value(const SolveArgs& A, int c1, int a, int64_t col) {
@@ -91,36 +108,35 @@ __device__ __forceinline__ void fwd_small_item(const DevPlan& P, const DevState&
   const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
   const int tid = threadIdx.x;
   const int64_t R = A.nrhs;
-  for (int e = tid; e < nf * rc; e += blockDim.x) {
-    const int r = e % nf, c = e / nf;
-    f[e] = r < np ? rhs_value<T>(A, c1, r, c0 + c) : T(0);
-  }
+  // every thread keeps one front row (and its columns) for the whole item
+  const RowWalk mf = row_walk(tid, blockDim.x, nf);
+  if (mf.on)
+    for (int c = mf.c; c < rc; c += mf.dc) f[mf.r + c * nf] = mf.r < np ? rhs_value<T>(A, c1, mf.r, c0 + c) : T(0);
   __syncthreads();
   for (int ci = P.child_ptr[s + 1] - 1; ci >= P.child_ptr[s]; --ci) {
     const int k = P.child_idx[ci];
     const int m = P.nu[k], nfk = P.nf[k], npk = P.np[k];
-    const T* w = fsol + P.colbase[k] * R + npk;
-    const int32_t* rl = P.rel + P.upd_off[k];
-    for (int e = tid; e < m * rc; e += blockDim.x) {
-      const int r = e % m, c = e / m;
-      f[front_pos(S, c1, np, rl[r]) + c * nf] += w[r + (int64_t)(c0 + c) * nfk];
+    if (m > 0) {
+      const T* w = fsol + P.colbase[k] * R + npk;
+      const RowWalk mc = row_walk(tid, blockDim.x, m);
+      if (mc.on) {
+        const int pos = front_pos(S, c1, np, P.rel[P.upd_off[k] + mc.r]);
+        for (int c = mc.c; c < rc; c += mc.dc) f[pos + c * nf] += w[mc.r + (int64_t)(c0 + c) * nfk];
+      }
     }
     __syncthreads();
   }
   const T* L = pool + P.lpan_off[s];
   for (int a = 0; a < np; ++a) {
-    const int rows = nf - a - 1;
-    for (int e = tid; e < rows * rc; e += blockDim.x) {
-      const int i = a + 1 + e % rows, c = e / rows;
-      f[i + c * nf] -= L[i + (int64_t)a * nf] * f[a + c * nf];
+    if (mf.on && mf.r > a) {
+      const T l = L[mf.r + (int64_t)a * nf];
+      for (int c = mf.c; c < rc; c += mf.dc) f[mf.r + c * nf] -= l * f[a + c * nf];
     }
     __syncthreads();
   }
   T* out = fsol + P.colbase[s] * R;
-  for (int e = tid; e < nf * rc; e += blockDim.x) {
-    const int r = e % nf, c = e / nf;
-    out[r + (int64_t)(c0 + c) * nf] = f[e];
-  }
+  if (mf.on)
+    for (int c = mf.c; c < rc; c += mf.dc) out[mf.r + (int64_t)(c0 + c) * nf] = f[mf.r + c * nf];
   __syncthreads();
 }
 
@@ -297,38 +313,38 @@ __device__ __forceinline__ void bwd_small_item(const DevPlan& P, const SolveArgs
   const int64_t R = A.nrhs;
   const T* f = fsol + P.colbase[s] * R;
   const int32_t* us = P.upd + P.upd_off[s];
-  for (int e = tid; e < np * rc; e += blockDim.x) {
-    const int r = e % np, c = e / np;
-    y[r + c * np] = f[r + (int64_t)(c0 + c) * nf];
-  }
-  for (int e = tid; e < nu * rc; e += blockDim.x) {
-    const int t = e % nu, c = e / nu;
-    g[t + c * nu] = xw[us[t] + (int64_t)(c0 + c) * A.ldx];
+  const RowWalk mp = row_walk(tid, blockDim.x, np);
+  if (mp.on)
+    for (int c = mp.c; c < rc; c += mp.dc) y[mp.r + c * np] = f[mp.r + (int64_t)(c0 + c) * nf];
+  if (nu > 0) {
+    const RowWalk mu = row_walk(tid, blockDim.x, nu);
+    if (mu.on) {
+      const int32_t u = us[mu.r];
+      for (int c = mu.c; c < rc; c += mu.dc) g[mu.r + c * nu] = xw[u + (int64_t)(c0 + c) * A.ldx];
+    }
   }
   __syncthreads();
   const T* U = pool + P.lpan_off[s];
   const T* U12 = pool + P.u12_off[s];
   const int ldu = u12_ld(P, s);
-  for (int e = tid; e < np * rc; e += blockDim.x) {
-    const int a = e % np, c = e / np;
-    T acc = y[a + c * np];
-    for (int t = 0; t < nu; ++t) acc -= U12[a + (int64_t)t * ldu] * g[t + c * nu];
-    y[a + c * np] = acc;
-  }
+  if (mp.on)
+    for (int c = mp.c; c < rc; c += mp.dc) {
+      T acc = y[mp.r + c * np];
+      for (int t = 0; t < nu; ++t) acc -= U12[mp.r + (int64_t)t * ldu] * g[t + c * nu];
+      y[mp.r + c * np] = acc;
+    }
   __syncthreads();
   for (int a = np - 1; a >= 0; --a) {
     for (int c = tid; c < rc; c += blockDim.x) y[a + c * np] /= U[a + (int64_t)a * nf];
     __syncthreads();
-    for (int e = tid; e < a * rc; e += blockDim.x) {
-      const int i = e % a, c = e / a;
-      y[i + c * np] -= U[i + (int64_t)a * nf] * y[a + c * np];
+    if (mp.on && mp.r < a) {
+      const T ua = U[mp.r + (int64_t)a * nf];
+      for (int c = mp.c; c < rc; c += mp.dc) y[mp.r + c * np] -= ua * y[a + c * np];
     }
     __syncthreads();
   }
-  for (int e = tid; e < np * rc; e += blockDim.x) {
-    const int r = e % np, c = e / np;
-    xw[c1 + r + (int64_t)(c0 + c) * A.ldx] = y[r + c * np];
-  }
+  if (mp.on)
+    for (int c = mp.c; c < rc; c += mp.dc) xw[c1 + mp.r + (int64_t)(c0 + c) * A.ldx] = y[mp.r + c * np];
   __syncthreads();
 }
 
@@ -436,6 +452,57 @@ __global__ void __launch_bounds__(256) k_bwd_gather_rows(DevPlan P, SolveArgs A,
 #pragma unroll
   for (int c = 0; c < kAsmCols; ++c)
     if (c < cc) f[(int64_t)c * nf] = v[c];
+}
+
+// Thin large supernodes, forward (nf > kSmallFront, np <= kThinNp, nu <=
+// kThinNu): most of the large fronts low in the tree have a few pivots and a
+// hundred or so update rows, so their forward products y = inv(L11) f[0:np]
+// and w = f[np:] - L21 y have K of a few units, and as 64 x 64 GEMM tiles
+// most of every tile is idle.  One CTA per (supernode, kThinCols right-hand
+// sides) forms y (into x's rows c1..) and then w in place, one update row
+// per thread, in a fixed order.  (With many update rows the tiled products,
+// K-chunked, keep more of the GPU busy.)
+constexpr int kThinNp = 64;
+constexpr int kThinNu = 192;
+constexpr int kThinCols = 32;
+constexpr int kThinLd = kThinCols + 1;
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_fwd_thin(DevPlan P, SolveArgs A, const int32_t* __restrict__ tasks,
+                                                  const T* __restrict__ pool, T* fsol, T* xw) {
+  __shared__ T ys[kThinNp * kThinLd];
+  const int s = tasks[blockIdx.x];
+  const int64_t R = A.nrhs, c0 = (int64_t)blockIdx.y * kThinCols;
+  const int cc = (int)(R - c0 < kThinCols ? R - c0 : kThinCols);
+  const int np = P.np[s], nu = P.nu[s], nf = P.nf[s], c1 = P.c1[s];
+  T* f = fsol + P.colbase[s] * R + c0 * nf;
+  const T* Li = pool + P.inv_off[s];
+  const int tid = threadIdx.x;
+  for (int e = tid; e < np * cc; e += blockDim.x) {
+    const int a = e % np, c = e / np;
+    const T* fc = f + (int64_t)c * nf;
+    T acc = T(0);
+    for (int b = 0; b < np; ++b) acc += Li[a + b * np] * fc[b];
+    ys[a * kThinLd + c] = acc;
+    xw[c1 + a + (c0 + c) * A.ldx] = acc;
+  }
+  __syncthreads();
+  // 64 update rows x 4 groups of 8 columns per pass
+  const T* L21 = pool + P.lpan_off[s] + np;
+  const int cg = (tid >> 6) * 8;
+  for (int r = tid & 63; r < nu; r += 64) {
+    T acc[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[c] = cg + c < cc ? f[np + r + (int64_t)(cg + c) * nf] : T(0);
+    for (int a = 0; a < np; ++a) {
+      const T l = L21[r + (int64_t)a * nf];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) acc[c] -= l * ys[a * kThinLd + cg + c];
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+      if (cg + c < cc) f[np + r + (int64_t)(cg + c) * nf] = acc[c];
+  }
 }
 
 // Split-K solve products: a product with few output tiles and a long K runs

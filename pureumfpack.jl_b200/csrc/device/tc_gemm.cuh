@@ -352,10 +352,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(const GemmTask* __res
 // TF32 rate, so six bf16 products cost what three TF32 products cost, with
 // FP32 accuracy instead of the 2^-21 of the two-part TF32 split.
 //
-// Warps 0-7 stage a 64-wide K block (one 128-byte swizzle row of bf16):
-// thread t converts row t % 128 over K half t / 128 of A, and four 8-value
-// chunks of B; warp 8 issues the MMAs; all eight staging warps then read the
-// accumulator back (warp w: lanes 32 (w % 4).., column half w / 4).
+// The staging warps (16 in the two-stage form, 8 in the short-K form) stage
+// a 64-wide K block (one 128-byte swizzle row of bf16): thread t converts
+// row t % 128 over K quarter (half) t / 128 of A, and two (four) 8-value
+// chunks of B; the next warp issues the MMAs; all staging warps then read
+// the accumulator back (warp w: lanes 32 (w % 4).., column group w / 4).
+// Sixteen staging warps keep twice the loads and conversions in flight per
+// SM (the staging, not the tensor pipe, limits the one-CTA-per-SM form); the
+// short-K form keeps eight so that two CTAs fit an SM's registers.
 //
 // The tensor core's FP32 accumulation rounds every addition towards zero,
 // so over a long K its error is a bias that grows with the number of
@@ -365,12 +369,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(const GemmTask* __res
 // 512 columns for BN = 128): each sees a quarter of the steps and a quarter
 // of the running sum, and the epilogue adds the partial sums in FP32 with
 // round-to-nearest.
-constexpr int kBxProducers = 256;
-constexpr int kBxThreads = kBxProducers + 32;
-
 template <int BN, int STAGES, int ACCS = 4>
 struct BxCfg {
   static constexpr int BM = 128, BK = 64;
+  static constexpr int kProducers = STAGES == 1 ? 256 : 512;   // staging threads
+  static constexpr int kProdWarps = kProducers / 32;
+  static constexpr int kThreads = kProducers + 32;              // + the MMA-issuing warp
+  static constexpr int kAPer = BM * BK / kProducers;            // A values per staging thread (one row)
   static constexpr int kABytes = BM * BK * 2;     // one bf16 part of A
   static constexpr int kBBytes = BN * BK * 2;
   static constexpr int kStageBytes = 3 * kABytes + 3 * kBBytes;
@@ -433,7 +438,7 @@ __device__ __forceinline__ void bx_put8(uint32_t p1, uint32_t p2, uint32_t p3, u
 // K <= BK) holds one stage and one accumulator and stages one K block
 // without a second register buffer, so two CTAs share an SM.
 template <int BN, int STAGES, int ACCS = 4>
-__global__ void __launch_bounds__(kBxThreads, STAGES == 1 ? 2 : 1)
+__global__ void __launch_bounds__(BxCfg<BN, STAGES, ACCS>::kThreads, STAGES == 1 ? 2 : 1)
     k_gemm_bx3(const GemmTask* __restrict__ tasks, int ntasks, const float* __restrict__ pa,
                const float* __restrict__ pb, float* pc, int* __restrict__ flags, uint64_t wait_ns) {
   using Cfg = BxCfg<BN, STAGES, ACCS>;
@@ -460,7 +465,7 @@ __global__ void __launch_bounds__(kBxThreads, STAGES == 1 ? 2 : 1)
 
   if (t == 0) {
     for (int s = 0; s < STAGES; ++s) {
-      mbar_init(&full[s], kBxProducers);
+      mbar_init(&full[s], Cfg::kProducers);
       mbar_init(&empty[s], 1);
     }
     mbar_init(&done, 1);
@@ -479,25 +484,26 @@ __global__ void __launch_bounds__(kBxThreads, STAGES == 1 ? 2 : 1)
   const uint32_t tmem = tmem_slot;
   const uint32_t sbase = smem_u32(smem);
 
-  if (warp < 8) {
+  constexpr int kAPer = Cfg::kAPer;
+  if (warp < Cfg::kProdWarps) {
     const float* A = pa + tk.a;
     const float* B = pb + tk.b;
-    const int arow = t & 127, ak = (t >> 7) * 32;
+    const int arow = t & 127, ak = (t >> 7) * kAPer;
     const int row = m0 + arow;
-    constexpr int kBPer = BN * (BK / 8) / kBxProducers;   // (column, 8-chunk) pairs per thread
+    constexpr int kBPer = BN * (BK / 8) / Cfg::kProducers;   // (column, 8-chunk) pairs per thread
     // Software pipeline over K blocks: the global loads of block kb + 1 are
     // issued before block kb is split and stored, so their latency hides
     // behind that work and the wait for a free stage (two register buffers).
-    auto load = [&](int kb, float (&va)[32], float (&vb)[kBPer][8]) {
+    auto load = [&](int kb, float (&va)[kAPer], float (&vb)[kBPer][8]) {
       const int k0 = kb * BK;
 #pragma unroll
-      for (int k = 0; k < 32; ++k) {
+      for (int k = 0; k < kAPer; ++k) {
         const int kk = k0 + ak + k;
         va[k] = (row < M && kk < K) ? A[(int64_t)row + (int64_t)kk * tk.lda] : 0.0f;
       }
 #pragma unroll
       for (int i = 0; i < kBPer; ++i) {
-        const int idx = t + i * kBxProducers, n = idx >> 3, c = idx & 7;
+        const int idx = t + i * Cfg::kProducers, n = idx >> 3, c = idx & 7;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
           const int kk = k0 + 8 * c + j;
@@ -506,7 +512,7 @@ __global__ void __launch_bounds__(kBxThreads, STAGES == 1 ? 2 : 1)
       }
     };
     // wait for a free stage, split and store block kb, mark the stage full
-    auto produce = [&](int kb, const float (&va)[32], const float (&vb)[kBPer][8]) -> bool {
+    auto produce = [&](int kb, const float (&va)[kAPer], const float (&vb)[kBPer][8]) -> bool {
       const int s = kb % STAGES;
       if (kb >= STAGES && !mbar_wait(&empty[s], (uint32_t)((kb / STAGES - 1) & 1), wait_ns)) {
         failed = 1;
@@ -514,12 +520,12 @@ __global__ void __launch_bounds__(kBxThreads, STAGES == 1 ? 2 : 1)
       }
       const uint32_t st = sbase + s * Cfg::kStageBytes;
 #pragma unroll
-      for (int c = 0; c < 4; ++c)
+      for (int c = 0; c < kAPer / 8; ++c)
         bx_put8(st, st + Cfg::kABytes, st + 2 * Cfg::kABytes, sw128_offset_b16(arow, ak + 8 * c), va + 8 * c);
       const uint32_t sb = st + 3 * Cfg::kABytes;
 #pragma unroll
       for (int i = 0; i < kBPer; ++i) {
-        const int idx = t + i * kBxProducers;
+        const int idx = t + i * Cfg::kProducers;
         bx_put8(sb, sb + Cfg::kBBytes, sb + 2 * Cfg::kBBytes, sw128_offset_b16(idx >> 3, 8 * (idx & 7)), vb[i]);
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -527,13 +533,13 @@ __global__ void __launch_bounds__(kBxThreads, STAGES == 1 ? 2 : 1)
       return !failed;
     };
     if constexpr (STAGES == 1) {
-      float va[32], vb[kBPer][8];
+      float va[kAPer], vb[kBPer][8];
       for (int kb = 0; kb < nk; ++kb) {
         load(kb, va, vb);
         if (!produce(kb, va, vb)) break;
       }
     } else {
-      float va0[32], vb0[kBPer][8], va1[32], vb1[kBPer][8];
+      float va0[kAPer], vb0[kBPer][8], va1[kAPer], vb1[kBPer][8];
       if (nk > 0) load(0, va0, vb0);
       for (int kb = 0; kb < nk; kb += 2) {
         if (kb + 1 < nk) load(kb + 1, va1, vb1);
@@ -571,14 +577,15 @@ __global__ void __launch_bounds__(kBxThreads, STAGES == 1 ? 2 : 1)
     tc_commit(&done);
   }
 
-  if (warp < 8) tc_wait_done(&done, wait_ns, &failed);
+  if (warp < Cfg::kProdWarps) tc_wait_done(&done, wait_ns, &failed);
   __syncthreads();
   const bool ok = !failed;
-  if (warp < 8) {
+  if (warp < Cfg::kProdWarps) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok) {
       float* C = pc + tk.c;
-      const int q = warp & 3, half = warp >> 2;
+      constexpr int kGroupCols = BN / (Cfg::kProdWarps / 4);   // columns per warp group
+      const int q = warp & 3, grp = warp >> 2;
       const int row = m0 + q * 32 + lane;
       const float* D = tk.mode == kGemmFrom ? pc + tk.d : C;
       const int ldD = tk.mode == kGemmFrom ? tk.ldd : tk.ldc;
@@ -586,7 +593,7 @@ __global__ void __launch_bounds__(kBxThreads, STAGES == 1 ? 2 : 1)
       const float sgn = tk.mode == kGemmSet ? -1.0f : 1.0f;
       const int nacc = nk < Cfg::kAccs ? nk : Cfg::kAccs;   // accumulators that K blocks reached
 #pragma unroll 1
-      for (int c0 = half * (BN / 2); c0 < (half + 1) * (BN / 2); c0 += 32) {
+      for (int c0 = grp * kGroupCols; c0 < (grp + 1) * kGroupCols; c0 += 32) {
         uint32_t v[32];
         float acc[32];
 #pragma unroll

@@ -89,12 +89,12 @@ inline unsigned grid1(int64_t work, int per) { return (unsigned)((work + per - 1
 enum KernelClass {
   KC_BUILD_VALUES, KC_SMALL, KC_ASSEMBLE, KC_PANEL, KC_TRSM, KC_GEMM_FACTOR, KC_PIVOTS, KC_SCATTER,
   KC_FWD_SMALL, KC_FWD_ASSEMBLE, KC_GEMM_SOLVE, KC_BWD_SMALL, KC_BWD_GATHER,
-  KC_SOLVE_FINISH, KC_RESIDUAL, KC_INVERSE, KC_COPY_PANELS, KC_COUNT
+  KC_SOLVE_FINISH, KC_RESIDUAL, KC_INVERSE, KC_COPY_PANELS, KC_FWD_THIN, KC_COUNT
 };
 const char* const kKernelClassName[KC_COUNT] = {
     "build_values", "small_fronts", "assemble_columns", "panel", "panel_trsm", "gemm_factor", "finalize_pivots",
     "scatter_csc", "fwd_small", "fwd_assemble", "gemm_solve", "bwd_small", "bwd_gather",
-    "solve_finish", "residual", "gemm_inverse", "copy_panels"};
+    "solve_finish", "residual", "gemm_inverse", "copy_panels", "fwd_thin"};
 
 struct KStat {
   double ms = 0, flops = 0, bytes = 0;
@@ -105,7 +105,8 @@ struct SolveSchedule {
   int64_t nrhs = -1;
   struct Step {
     int kind;        // 0 fwd_small, 1 fwd_assemble, 3 gemm (A: pool; B, C, D: solve arena), 4 bwd_small,
-                     // 5 bwd_gather, 6 fwd_tiny, 7 bwd_tiny (nf <= kTinyFront, one warp per supernode)
+                     // 5 bwd_gather, 6 fwd_tiny, 7 bwd_tiny (nf <= kTinyFront, one warp per supernode),
+                     // 8 fwd_thin (thin large supernodes; step launches only)
     int64_t first, count, tiles;
     double flops = 0, elems = 0;
     int64_t tiles_tc = 0;   // GEMM steps: grid in 128 x 128 tensor-core tiles (gemms_tc)
@@ -134,6 +135,7 @@ struct SolveSchedule {
   std::vector<SplitRed> sreds;
   int64_t split_scratch = 0;        // partial products, elements (after x in the solve arena)
   int elem = 0;                     // front element size the K chunks were chosen for
+  bool thin = false;                // thin supernodes have their own steps (not in the persistent solve)
   DevBuf d_ids, d_gemms, d_gemms_tc, d_phases, d_skinny, d_rows, d_aptr, d_asrc, d_sgemms, d_sgemms_tc, d_sreds;
 };
 
@@ -606,10 +608,10 @@ bool gemm_use_tc(const mfgpu_ctx* h, int64_t id, bool dflt) {
 void launch_tc(const mfgpu_ctx* h, const GemmTask* tasks, int64_t count, int64_t tiles, const float* pa,
                const float* pb, float* pc, cudaStream_t st, int32_t max_k) {
   if (h->tc_bf16x3 && max_k <= BxCfg<128, 1, 1>::BK)
-    k_gemm_bx3<128, 1, 1><<<(unsigned)tiles, kBxThreads, BxCfg<128, 1, 1>::kSmem, st>>>(
+    k_gemm_bx3<128, 1, 1><<<(unsigned)tiles, BxCfg<128, 1, 1>::kThreads, BxCfg<128, 1, 1>::kSmem, st>>>(
         tasks, (int)count, pa, pb, pc, h->b_flags.as<int>(), h->wait_ns);
   else if (h->tc_bf16x3)
-    k_gemm_bx3<128, 2><<<(unsigned)tiles, kBxThreads, BxCfg<128, 2>::kSmem, st>>>(tasks, (int)count, pa, pb, pc,
+    k_gemm_bx3<128, 2><<<(unsigned)tiles, BxCfg<128, 2>::kThreads, BxCfg<128, 2>::kSmem, st>>>(tasks, (int)count, pa, pb, pc,
                                                                                   h->b_flags.as<int>(), h->wait_ns);
   else
     k_gemm_tc<128, 3><<<(unsigned)tiles, kTcThreads, TcCfg<128, 3>::kSmem, st>>>(tasks, (int)count, pa, pb, pc,
@@ -989,11 +991,14 @@ constexpr int32_t kSplitMinKC = 128;
 
 void build_solve_schedule(mfgpu_ctx* h, int64_t R, int elem) {
   SolveSchedule& S = h->sched;
-  if (S.nrhs == R && S.elem == elem) return;
+  const bool thin = !h->persistent;
+  if (S.nrhs == R && S.elem == elem && S.thin == thin) return;
   const Plan& P = h->plan;
   S = SolveSchedule{};
   S.nrhs = R;
   S.elem = elem;
+  S.thin = thin;
+  auto is_thin = [&](int32_t s) { return thin && P.np[s] <= kThinNp && P.nu[s] <= kThinNu; };
   auto ceil_div = [](int64_t a, int64_t b) { return (a + b - 1) / b; };
   // offsets: A operands in the front pool (fronts and pivot-block inverses);
   // B, C and D in the solve arena: the per-supernode blocks (nf x R each,
@@ -1054,6 +1059,22 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R, int elem) {
       if (st.count) S.steps.push_back(st);
     }
   };
+  // the thin large supernodes of slots [m, e): one CTA per (supernode,
+  // kThinCols right-hand sides), forward (kind 8)
+  auto thin_step = [&](int32_t m, int32_t e, int kind, int32_t level) {
+    SolveSchedule::Step st{kind, (int64_t)S.ids.size(), 0, 0};
+    st.level = level;
+    for (int32_t i = m; i < e; ++i) {
+      const int32_t s = P.slot_super[i];
+      if (!is_thin(s)) continue;
+      S.ids.push_back(s);
+      const double a = P.np[s], u = P.nu[s];
+      st.flops += 2.0 * (a * a + a * u) * R;
+      st.elems += a * a + a * u + 2.0 * (a + u) * R;
+      ++st.count;
+    }
+    if (st.count) S.steps.push_back(st);
+  };
   // forward, leaves to root
   for (int32_t L = 0; L < P.nlevels; ++L) {
     const int32_t a = P.level_slot[L], m = P.level_large[L], e = P.level_slot[L + 1];
@@ -1064,10 +1085,12 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R, int elem) {
       for (int32_t i = m; i < e; ++i) S.ids.push_back(P.slot_super[i]);
       S.steps.push_back({1, first, e - m, 0});
       S.steps.back().level = L;
+      thin_step(m, e, 8, L);
       // y = inv(L11) f[0:np], into x's rows c1.. ; then w = f[np:] - L21 y
       SolveSchedule::Step gy = gemm_step();
       for (int32_t i = m; i < e; ++i) {
         const int32_t s = P.slot_super[i];
+        if (is_thin(s)) continue;
         const int nf = P.nf[s], np = P.np[s];
         add_gemm(gy, kGemmSet, P.inv_off[s], np, P.colbase[s] * R, nf, xw0 + P.c1[s], n, np, (int)R, np);
       }
@@ -1075,6 +1098,7 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R, int elem) {
       SolveSchedule::Step gw = gemm_step();
       for (int32_t i = m; i < e; ++i) {
         const int32_t s = P.slot_super[i];
+        if (is_thin(s)) continue;
         const int nf = P.nf[s], np = P.np[s];
         add_gemm(gw, kGemmSub, P.lpan_off[s] + np, nf, xw0 + P.c1[s], n, P.colbase[s] * R + np, nf, P.nu[s],
                  (int)R, np);
@@ -1261,6 +1285,7 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R, int elem) {
   // kSolveThreads / 32 right-hand sides per gather item)
   const int64_t ych = ceil_div(R, kSolveCols), wch = ceil_div(R, kSolveThreads / 32);
   for (const auto& st : S.steps) {
+    if (thin) break;   // the persistent solve runs the schedule without thin steps
     // tiny steps run as the small-supernode phases (the item handles any nf <= 64)
     const int pk = st.kind == 6 ? kPhFwdSmall : (st.kind == 7 ? kPhBwdSmall : st.kind);
     SolvePhase ph{pk, 1, st.first, st.count, 0};
@@ -1331,6 +1356,7 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
   });
   const unsigned ychunks = (unsigned)((R + solve_cols<T>() - 1) / solve_cols<T>());
   const unsigned acols = (unsigned)((R + kAsmCols - 1) / kAsmCols);
+  const unsigned tchunks = (unsigned)((R + kThinCols - 1) / kThinCols);
   const RowTask* rows = S.d_rows.as<RowTask>();
   const int32_t* ids = S.d_ids.as<int32_t>();
   const GemmTask* gemms = S.d_gemms.as<GemmTask>();
@@ -1449,6 +1475,11 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
         klaunch(h, KC_BWD_SMALL, s.flops, bytes, [&] {
           k_bwd_small<T><<<dim3((unsigned)s.count, ychunks), kSolveThreads, 0, ss>>>(h->dp, A, ids + s.first, pool,
                                                                                      fsol, xw);
+        }, s.level, s.count);
+        break;
+      case 8:
+        klaunch(h, KC_FWD_THIN, s.flops, bytes, [&] {
+          k_fwd_thin<T><<<dim3((unsigned)s.count, tchunks), 256, 0, st>>>(h->dp, A, ids + s.first, pool, fsol, xw);
         }, s.level, s.count);
         break;
       case 5:
