@@ -421,12 +421,20 @@ def class_rooflines(f, form, fp64_peak, peaks, nrhs):
         a = k["flops"] / (k["ms"] * 1e-3) / 1e12
         out["gemm_factor"] = {"bound": "tensor", "achieved": a, "peak": tpeak, "unit": "TFLOP/s", "frac": a / tpeak,
                               "ms": k["ms"], "launches": k["launches"], "peak_source": tsrc}
+        ratio = NCU_TRAFFIC_RATIO.get(("gemm_factor", form))
+        if ratio is not None:
+            out["gemm_factor"]["traffic_per_launch"] = ratio[0] * k["bytes"] / max(k["launches"], 1)
+            out["gemm_factor"]["traffic_source"] = f"ncu DRAM / algorithmic bytes {ratio[0]:.3f} ({ratio[1]})"
     for name in ("assemble_columns", "scatter_csc"):
         if name in kern and kern[name]["bytes"] > 0:
             k = kern[name]
             a = k["bytes"] / (k["ms"] * 1e-3) / 1e9
             out[name] = {"bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s", "frac": a / hbm, "ms": k["ms"],
                          "launches": k["launches"], "algorithmic_bytes": k["bytes"]}
+            ratio = NCU_TRAFFIC_RATIO.get((name, form))
+            if ratio is not None:
+                out[name]["traffic_per_launch"] = ratio[0] * k["bytes"] / max(k["launches"], 1)
+                out[name]["traffic_source"] = f"ncu DRAM / algorithmic bytes {ratio[0]:.3f} ({ratio[1]})"
     passes = f["refine"] + 1
     ms = sum(kern[c]["ms"] for c in SOLVE_CLASSES if c in kern) / passes
     if ms > 0:
@@ -490,6 +498,8 @@ def gpu_factors(ctx):
 # figures are summarised under profiles/.
 NCU_TRAFFIC_RATIO = {
     ("gemm_factor", "fp64"): (0.743, "k_gemm_f64 factor updates, poisson3d-48"),
+    ("gemm_factor", "mixed"): (0.673, "five k_gemm_bx3 factor-update launches of 112-1305 tiles, poisson3d-48"),
+    ("assemble_columns", "mixed"): (0.732, "one k_assemble_columns launch (4821 front columns), poisson3d-48"),
 }
 
 

@@ -326,6 +326,100 @@ __global__ void __launch_bounds__(256) k_gemm_f32(const GemmTask* __restrict__ t
     }
 }
 
+// Products with few rows (the solve products whose M is a supernode's pivot
+// count, low in the tree: g = y - U12 x_u, x = inv(U11) g, y = inv(L11) f):
+// a 64 x 64 tile would leave most of its rows idle and its CTAs would each
+// re-stream the B operand.  BM x 128 tiles (BM = 16 or 32, tiles counted by
+// tiles_m / tiles_n in that tiling), CUDA-core FMA, cp.async double buffer;
+// thread (ty, tx) holds rows ty * BM/8 .. and columns tx + 32 j, so the B
+// reads from shared memory are conflict-free and the A reads broadcast.
+constexpr int kSkinnyMBN = 128;
+
+template <typename T, int BM>
+__global__ void __launch_bounds__(256) k_gemm_skinny_m(const GemmTask* __restrict__ tasks, int ntasks,
+                                                       const T* __restrict__ pa, const T* pb, T* pc) {
+  constexpr int BN = kSkinnyMBN, BK = 16, TM = BM / 8;
+  __shared__ T As[2][BK][BM];
+  __shared__ T Bs[2][BK][BN + 1];
+  const GemmTask tk = tasks[find_task(tasks, ntasks, blockIdx.x)];
+  const int64_t local = blockIdx.x - tk.tile_base;
+  const int m0 = (int)(local % tk.tiles_m) * BM;
+  const int n0 = (int)(local / tk.tiles_m) * BN;
+  const T* A = pa + tk.a;
+  const T* B = pb + tk.b;
+  T* C = pc + tk.c;
+  const int M = tk.m, N = tk.n, K = tk.k, lda = tk.lda, ldb = tk.ldb, ldc = tk.ldc;
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  T acc[TM][4];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
+  auto cp = [](T* dst, const T* src, bool ok) {
+    if constexpr (sizeof(T) == 8) cp_async8(dst, src, ok);
+    else cp_async4(dst, src, ok);
+  };
+  auto load = [&](int st, int k0) {
+    for (int idx = tid; idx < BM * BK; idx += 256) {
+      const int m = idx % BM, k = idx / BM;
+      const bool ok = (m0 + m < M) && (k0 + k < K);
+      cp(&As[st][k][m], ok ? A + (int64_t)(m0 + m) + (int64_t)(k0 + k) * lda : A, ok);
+    }
+#pragma unroll
+    for (int i = 0; i < BK * BN / 256; ++i) {
+      const int idx = tid + i * 256;
+      const int k = idx % BK, n = idx / BK;
+      const bool ok = (n0 + n < N) && (k0 + k < K);
+      cp(&Bs[st][k][n], ok ? B + (int64_t)(k0 + k) + (int64_t)(n0 + n) * ldb : B, ok);
+    }
+    cp_async_commit();
+  };
+  const int ktiles = (K + BK - 1) / BK;
+  if (ktiles > 0) load(0, 0);
+  for (int kt = 0; kt < ktiles; ++kt) {
+    if (kt + 1 < ktiles) {
+      load((kt + 1) & 1, (kt + 1) * BK);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const int st = kt & 1;
+#pragma unroll
+    for (int k = 0; k < BK; ++k) {
+      T a[TM], b[4];
+#pragma unroll
+      for (int i = 0; i < TM; ++i) a[i] = As[st][k][ty * TM + i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[st][k][tx + 32 * j];
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+  const T* D = tk.mode == kGemmFrom ? pc + tk.d : C;
+  const int ldD = tk.mode == kGemmFrom ? tk.ldd : ldc;
+  const bool ld = tk.mode == kGemmSub || tk.mode == kGemmFrom;
+  const T sgn = tk.mode == kGemmSet ? T(-1) : T(1);
+  T cv[TM][4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+      const int m = m0 + ty * TM + i, n = n0 + tx + 32 * j;
+      cv[i][j] = (ld && m < M && n < N) ? D[(int64_t)m + (int64_t)n * ldD] : T(0);
+    }
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+      const int m = m0 + ty * TM + i, n = n0 + tx + 32 * j;
+      if (m < M && n < N) C[(int64_t)m + (int64_t)n * ldc] = cv[i][j] - sgn * acc[i][j];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Split-K products for few right-hand sides (N <= NMAX): the solve products
 // g = y - U12 x_u have a handful of rows and thousands of K, which a 64 x 64

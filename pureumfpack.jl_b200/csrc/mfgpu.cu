@@ -119,6 +119,9 @@ struct SolveSchedule {
     int64_t sp_first = 0, sp_count = 0, sp_tiles = 0, sp_tiles_tc = 0;
     int32_t sp_max_k = 0;
     int64_t rd_first = 0, rd_count = 0, rd_elems = 0;
+    // GEMM steps whose tasks have few rows: the same tasks in BM x 128 tiles
+    int64_t sm_first = 0, sm_count = 0, sm_tiles = 0;
+    int32_t sm_bm = 0;
   };
   std::vector<Step> steps;
   std::vector<int32_t> ids;
@@ -133,10 +136,12 @@ struct SolveSchedule {
   std::vector<int2> asrc;
   std::vector<GemmTask> sgemms, sgemms_tc;
   std::vector<SplitRed> sreds;
+  std::vector<GemmTask> gemms_sm;
   int64_t split_scratch = 0;        // partial products, elements (after x in the solve arena)
   int elem = 0;                     // front element size the K chunks were chosen for
   bool thin = false;                // thin supernodes have their own steps (not in the persistent solve)
-  DevBuf d_ids, d_gemms, d_gemms_tc, d_phases, d_skinny, d_rows, d_aptr, d_asrc, d_sgemms, d_sgemms_tc, d_sreds;
+  DevBuf d_ids, d_gemms, d_gemms_tc, d_phases, d_skinny, d_rows, d_aptr, d_asrc, d_sgemms, d_sgemms_tc, d_sreds,
+      d_gemms_sm;
 };
 
 }  // namespace
@@ -1281,6 +1286,34 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R, int elem) {
       S.split_scratch = std::max(S.split_scratch, scratch);
     }
   }
+  // few-row products (M = a pivot count, low in the tree): BM x 128 tiles
+  // when they waste at most half the work of 64 x 64 tiles on idle rows
+  if (R > kSkinnyMaxN) {
+    for (auto& st : S.steps) {
+      if (st.kind != 3 || st.sp_count) continue;
+      int32_t maxm = 0;
+      for (int64_t i = st.first; i < st.first + st.count; ++i) maxm = std::max(maxm, S.gemms[i].m);
+      const int bm = maxm <= 16 ? 16 : 32;
+      double w64 = 0, wsm = 0;
+      for (int64_t i = st.first; i < st.first + st.count; ++i) {
+        const GemmTask& g = S.gemms[i];
+        w64 += (double)ceil_div(g.m, 64) * 64 * ceil_div(g.n, 64) * 64 * g.k;
+        wsm += (double)ceil_div(g.m, bm) * bm * ceil_div(g.n, kSkinnyMBN) * kSkinnyMBN * g.k;
+      }
+      if (!(wsm <= 0.5 * w64)) continue;
+      st.sm_bm = bm;
+      st.sm_first = (int64_t)S.gemms_sm.size();
+      for (int64_t i = st.first; i < st.first + st.count; ++i) {
+        GemmTask t = S.gemms[i];
+        t.tiles_m = (int)ceil_div(t.m, bm);
+        t.tiles_n = (int)ceil_div(t.n, kSkinnyMBN);
+        t.tile_base = st.sm_tiles;
+        st.sm_tiles += (int64_t)t.tiles_m * t.tiles_n;
+        S.gemms_sm.push_back(t);
+      }
+      st.sm_count = st.count;
+    }
+  }
   // the same steps as phases of the persistent kernel (kSolveThreads per CTA:
   // kSolveThreads / 32 right-hand sides per gather item)
   const int64_t ych = ceil_div(R, kSolveCols), wch = ceil_div(R, kSolveThreads / 32);
@@ -1308,6 +1341,7 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R, int elem) {
   upload(S.d_sgemms, S.sgemms, h->stream);
   upload(S.d_sgemms_tc, S.sgemms_tc, h->stream);
   upload(S.d_sreds, S.sreds, h->stream);
+  upload(S.d_gemms_sm, S.gemms_sm, h->stream);
 }
 
 // One solve A x = b for device b (ldb) into device x (ldx) (x overwritten, or
@@ -1450,6 +1484,14 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
             launch_tc(h, gtc, gcount, ttc, (const float*)pool, (const float*)fsol, (float*)fsol, st, gmaxk);
             fold();
           }, s.level, ttc);
+        else if (s.sm_count)
+          klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
+            const GemmTask* gs = S.d_gemms_sm.as<GemmTask>() + s.sm_first;
+            if (s.sm_bm == 16)
+              k_gemm_skinny_m<T, 16><<<(unsigned)s.sm_tiles, 256, 0, st>>>(gs, (int)s.sm_count, pool, fsol, fsol);
+            else
+              k_gemm_skinny_m<T, 32><<<(unsigned)s.sm_tiles, 256, 0, st>>>(gs, (int)s.sm_count, pool, fsol, fsol);
+          }, s.level, s.sm_tiles);
         else
           klaunch(h, KC_GEMM_SOLVE, s.flops, bytes, [&] {
             launch_gemm<T>(g64, gcount, t64, pool, fsol, fsol, st);
@@ -1539,7 +1581,7 @@ void solve_graph(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<
       (uintptr_t)S.d_ids.p, (uintptr_t)S.d_gemms.p, (uintptr_t)S.d_phases.p, (uintptr_t)h->b_prow.p,
       (uintptr_t)S.d_gemms_tc.p, (uintptr_t)S.d_skinny.p, (uintptr_t)h->b_skinny.p, (uintptr_t)h->use_tc,
       (uintptr_t)S.d_rows.p, (uintptr_t)S.d_aptr.p, (uintptr_t)S.d_asrc.p, (uintptr_t)S.d_sgemms.p,
-      (uintptr_t)S.d_sgemms_tc.p, (uintptr_t)S.d_sreds.p,
+      (uintptr_t)S.d_sgemms_tc.p, (uintptr_t)S.d_sreds.p, (uintptr_t)S.d_gemms_sm.p,
       (uintptr_t)h->tc_bf16x3, (uintptr_t)h->choice_version, (uintptr_t)h->wait_ns,
       (uintptr_t)h->persistent, (uintptr_t)h->b_bar.p,
       (uintptr_t)h->b_rowfac.p, (uintptr_t)h->stream};
@@ -1702,7 +1744,7 @@ void mfgpu_destroy(mfgpu_ctx* h) {
                     &h->b_ux, &h->b_fsol, &h->b_b, &h->b_x, &h->b_f32, &h->b_r, &h->b_d, &h->b_err, &h->b_norm,
                     &h->sched.d_ids, &h->sched.d_gemms, &h->sched.d_gemms_tc, &h->sched.d_phases,
                     &h->sched.d_rows, &h->sched.d_aptr, &h->sched.d_asrc, &h->sched.d_sgemms, &h->sched.d_sgemms_tc,
-                    &h->sched.d_sreds, &h->b_bar,
+                    &h->sched.d_sreds, &h->sched.d_gemms_sm, &h->b_bar,
                     &h->b_stamps};
   for (DevBuf* b : bufs) b->release();
   if (h->factor_exec) cudaGraphExecDestroy(h->factor_exec);
