@@ -256,6 +256,46 @@ __global__ void __launch_bounds__(32 * tiny_warps<T>()) k_bwd_tiny(DevPlan P, So
   }
 }
 
+// Leaf supernodes (no children, nf <= kLeafFront), the whole bottom tree
+// level, forward: one warp per (supernode, 32 right-hand sides), one lane
+// per right-hand side holding its column of the block in registers (every
+// register index is a compile-time constant: the loops run to kLeafFront
+// with warp-uniform guards), so there is no shared memory and no index
+// arithmetic per element.  Same operations, in the same order, as
+// k_fwd_tiny.  (The backward pass keeps k_bwd_tiny: its gathers of x over
+// the update rows coalesce across lanes along the rows, which a lane per
+// right-hand side would lose.)
+constexpr int kLeafFront = 16;
+constexpr int kLeafWarps = 4;
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kLeafWarps) k_fwd_leaf(DevPlan P, SolveArgs A, const int32_t* __restrict__ tasks,
+                                                              int ntasks, const T* __restrict__ pool, T* fsol) {
+  const int ti = blockIdx.x * kLeafWarps + warp_id();
+  if (ti >= ntasks) return;
+  const int64_t c = (int64_t)blockIdx.y * 32 + lane_id();
+  if (c >= A.nrhs) return;
+  const int s = tasks[ti];
+  const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
+  T f[kLeafFront];
+#pragma unroll
+  for (int i = 0; i < kLeafFront; ++i) f[i] = i < np ? rhs_value<T>(A, c1, i, c) : T(0);
+  const T* L = pool + P.lpan_off[s];
+#pragma unroll
+  for (int a = 0; a < kLeafFront; ++a) {
+    if (a < np) {
+      const T fa = f[a];
+#pragma unroll
+      for (int i = a + 1; i < kLeafFront; ++i)
+        if (i < nf) f[i] -= L[i + (int64_t)a * nf] * fa;
+    }
+  }
+  T* out = fsol + P.colbase[s] * A.nrhs + c * nf;
+#pragma unroll
+  for (int i = 0; i < kLeafFront; ++i)
+    if (i < nf) out[i] = f[i];
+}
+
 // Large supernodes: gather the rhs block, one warp per right-hand side;
 // item (bx, by) covers columns by * warps .. of supernode tasks[bx] (the
 // persistent solve's form; the step launches use k_fwd_assemble_rows).

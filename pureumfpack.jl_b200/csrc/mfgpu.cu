@@ -106,7 +106,8 @@ struct SolveSchedule {
   struct Step {
     int kind;        // 0 fwd_small, 1 fwd_assemble, 3 gemm (A: pool; B, C, D: solve arena), 4 bwd_small,
                      // 5 bwd_gather, 6 fwd_tiny, 7 bwd_tiny (nf <= kTinyFront, one warp per supernode),
-                     // 8 fwd_thin (thin large supernodes; step launches only)
+                     // 8 fwd_thin (thin large supernodes; step launches only),
+                     // 10 fwd_leaf (leaves with nf <= kLeafFront; step launches only)
     int64_t first, count, tiles;
     double flops = 0, elems = 0;
     int64_t tiles_tc = 0;   // GEMM steps: grid in 128 x 128 tensor-core tiles (gemms_tc)
@@ -1050,13 +1051,21 @@ void build_solve_schedule(mfgpu_ctx* h, int64_t R, int elem) {
   };
   // the small supernodes of slots [a, m): the tiny ones (one warp each) and
   // the rest (one CTA each), as two independent steps
+  // class of a small supernode: 0 leaf (forward only: no children, nf <=
+  // kLeafFront; step launches only), 1 tiny, 2 the rest
+  auto small_class = [&](int32_t s, bool fwd) {
+    if (fwd && thin && P.child_ptr[s + 1] == P.child_ptr[s] && P.nf[s] <= kLeafFront) return 0;
+    return P.nf[s] <= kTinyFront ? 1 : 2;
+  };
   auto small_steps = [&](int32_t a, int32_t m, int tiny_kind, int small_kind, int32_t level) {
-    for (int pass = 0; pass < 2; ++pass) {
-      SolveSchedule::Step st{pass == 0 ? tiny_kind : small_kind, (int64_t)S.ids.size(), 0, 0};
+    const bool fwd = tiny_kind == 6;
+    for (int pass = fwd ? 0 : 1; pass < 3; ++pass) {
+      const int kind = pass == 0 ? 10 : (pass == 1 ? tiny_kind : small_kind);
+      SolveSchedule::Step st{kind, (int64_t)S.ids.size(), 0, 0};
       st.level = level;
       for (int32_t i = a; i < m; ++i) {
         const int32_t s = P.slot_super[i];
-        if ((P.nf[s] <= kTinyFront) != (pass == 0)) continue;
+        if (small_class(s, fwd) != pass) continue;
         S.ids.push_back(s);
         small_work(st, s);
         ++st.count;
@@ -1425,7 +1434,7 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
   for (const auto& s : S.steps) {
     const double bytes = s.elems * sizeof(T);
     fork.at(s.level);
-    const bool side = s.kind == 0 || s.kind == 4 || s.kind == 6 || s.kind == 7;
+    const bool side = s.kind == 0 || s.kind == 4 || s.kind == 6 || s.kind == 7 || s.kind == 10;
     const cudaStream_t ss = side ? fork.side() : st;
     switch (s.kind) {
       case 0:
@@ -1505,6 +1514,12 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
         klaunch(h, KC_FWD_SMALL, s.flops, bytes, [&] {
           k_fwd_tiny<T><<<dim3((unsigned)((s.count + tiny_warps<T>() - 1) / tiny_warps<T>()), (unsigned)((R + 31) / 32)),
                           32 * tiny_warps<T>(), 0, ss>>>(h->dp, DS, A, ids + s.first, (int)s.count, pool, fsol);
+        }, s.level, s.count);
+        break;
+      case 10:
+        klaunch(h, KC_FWD_SMALL, s.flops, bytes, [&] {
+          k_fwd_leaf<T><<<dim3((unsigned)((s.count + kLeafWarps - 1) / kLeafWarps), (unsigned)((R + 31) / 32)),
+                          32 * kLeafWarps, 0, ss>>>(h->dp, A, ids + s.first, (int)s.count, pool, fsol);
         }, s.level, s.count);
         break;
       case 7:

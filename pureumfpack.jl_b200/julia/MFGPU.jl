@@ -184,6 +184,24 @@ function solve(h::Handle, B::AbstractVecOrMat{Float64}; refine::Integer = 0)
     return B isa AbstractVector ? vec(X) : X
 end
 
+# factor!(h, A, Rs, check) followed by solve(h, B; refine) in one call: the
+# right-hand sides cross the bus while the GPU factors.  Returns X.
+function factor_solve!(h::Handle, A::SparseMatrixCSC{Float64, <:Integer}, Rs, B::AbstractVecOrMat{Float64};
+                       refine::Integer = 0, check::Bool = true)
+    rs = Rs === nothing ? C_NULL : pointer(Rs)
+    Bc = Matrix{Float64}(reshape(B, size(B, 1), :))
+    X = similar(Bc)
+    n = size(Bc, 1)
+    rc = GC.@preserve Rs ccall((:mfgpu_factor_solve, libmfgpu), Cint,
+        (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int32, Int64, Ptr{Float64}, Int64, Ptr{Float64}, Int64, Int32),
+        h.ptr, nonzeros(A), rs, Int32(check), size(Bc, 2), Bc, n, X, n, Int32(refine))
+    st = _check(h, rc)
+    st > 0 && throw(Main.LinearAlgebra.SingularException(st))
+    h.f32 = false
+    h.c64 = false
+    return B isa AbstractVector ? vec(X) : X
+end
+
 # --- batched systems (many independent systems through one handle) -------
 # ordering: 0 = AMD (as splu(A; method=:multifrontal)), 1 = COLAMD.
 function batch_analyze!(h::Handle, As::AbstractVector{<:SparseMatrixCSC{Float64, <:Integer}}; ordering::Integer = 0)
