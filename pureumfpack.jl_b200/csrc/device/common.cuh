@@ -181,6 +181,19 @@ __device__ __forceinline__ T to_front(Wide<T> v) {
 }
 
 // 8-byte asynchronous global->shared copy with zero fill when !pred.
+// Exact e / d and e % d by one 64-bit multiply and shift, for e * d < 2^32
+// (m = ceil(2^32 / d): e m / 2^32 = e / d + e (m - 2^32 / d) / 2^32, whose
+// second term stays below 1 / d, so the floor is e / d's).  Built once per
+// divisor, it replaces the integer divisions of element loops that walk a
+// block of runtime height.
+struct FastDiv {
+  uint64_t m;
+  uint32_t d;
+  // floor((2^32 - 1) / d) + 1 == ceil(2^32 / d) for every d >= 1 (one 32-bit division)
+  __device__ __forceinline__ explicit FastDiv(uint32_t dd) : m((uint64_t)(0xFFFFFFFFu / dd) + 1), d(dd) {}
+  __device__ __forceinline__ uint32_t div(uint32_t e) const { return (uint32_t)(((uint64_t)e * m) >> 32); }
+};
+
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   const int bytes = pred ? 8 : 0;

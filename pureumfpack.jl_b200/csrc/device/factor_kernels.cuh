@@ -51,8 +51,10 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_fronts(DevPlan P, DevSt
     const int m = P.nu[k], nfk = P.nf[k], npk = P.np[k];
     const T* cb = pool + P.front_off[k] + npk + (int64_t)npk * nfk;
     const int32_t* rl = P.rel + P.upd_off[k];
+    if (m == 0) continue;
+    const FastDiv dm((uint32_t)m);
     for (int e = tid; e < m * m; e += nthr) {
-      const int r = e % m, t = e / m;
+      const int t = (int)dm.div(e), r = e - t * m;
       F[rl[r] + rl[t] * nf] += cb[r + (int64_t)t * nfk];
     }
     __syncthreads();
@@ -84,9 +86,12 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_fronts(DevPlan P, DevSt
       if (i >= seg || d != T(0)) F[i + k * nf] *= rcp;
     __syncthreads();
     const int rows = nf - k - 1;
-    for (int e = tid; e < rows * rows; e += nthr) {
-      const int i = k + 1 + e % rows, j = k + 1 + e / rows;
-      F[i + j * nf] -= F[i + k * nf] * F[k + j * nf];
+    if (rows > 0) {
+      const FastDiv drows((uint32_t)rows);
+      for (int e = tid; e < rows * rows; e += nthr) {
+        const int q = (int)drows.div(e), i = k + 1 + e - q * rows, j = k + 1 + q;
+        F[i + j * nf] -= F[i + k * nf] * F[k + j * nf];
+      }
     }
     __syncthreads();
   }
@@ -641,8 +646,9 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
       for (int i = 0; i < 8; ++i) A[(s8 + i) + c * kLdS] = o[i];
     }
     __syncthreads();
+    const FastDiv drest((uint32_t)(rest > 0 ? rest : 1));
     for (int e = t; e < rest * rest; e += kSpecThreads) {   // trailing update
-      const int r = s8 + 8 + e % rest, c = s8 + 8 + e / rest;
+      const int q = (int)drest.div(e), r = s8 + 8 + e - q * rest, c = s8 + 8 + q;
       T v = A[r + c * kLdS];
 #pragma unroll
       for (int k = 0; k < 8; ++k) v -= A[r + (s8 + k) * kLdS] * A[(s8 + k) + c * kLdS];
@@ -656,8 +662,9 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
   if (violated) bad = 1;
   __syncthreads();
   if (t == 0 && bad) atomicOr(S.flags, 1);
+  const FastDiv dkb((uint32_t)kb);
   for (int e = t; e < kb * kb; e += kSpecThreads) {
-    const int r = e % kb, c = e / kb;
+    const int c = (int)dkb.div(e), r = e - c * kb;
     F[(k0 + r) + (int64_t)(k0 + c) * nf] = A[r + c * kLdS];
   }
   T* dst = dinv + (P.dinv_off[s_] + k0 / kPanel) * (int64_t)kDinvElems;
@@ -831,8 +838,9 @@ __global__ void __launch_bounds__(kApplyThreads) k_panel_apply(DevPlan P, DevSta
     __syncthreads();
     mm64<T>(sP, sQ, sP, kLdP);
     bool violated = false;
+    const FastDiv drows((uint32_t)(rows > 0 ? rows : 1));
     for (int e = t; e < rows * kb; e += blockDim.x) {
-      const int r = e % rows, c = e / rows;
+      const int c = (int)drows.div(e), r = e - c * rows;
       const T v = sP[r + c * kLdP];
       if (tk.check && i0 + r < seg[c] && absd(v) > 1.0) violated = true;
       F[(i0 + r) + (int64_t)(k0 + c) * nf] = v;
@@ -849,8 +857,9 @@ __global__ void __launch_bounds__(kApplyThreads) k_panel_apply(DevPlan P, DevSta
     }
     __syncthreads();
     mm64<T>(sP, sQ, sQ, kLdQ);
+    const FastDiv dkb((uint32_t)kb);
     for (int e = t; e < kb * cols; e += blockDim.x) {
-      const int r = e % kb, c = e / kb;
+      const int c = (int)dkb.div(e), r = e - c * kb;
       F[(k0 + r) + (int64_t)(j0 + c) * nf] = sQ[r + c * kLdQ];
     }
   }

@@ -48,16 +48,25 @@ struct SolveArgs {
 // while its rows are read in factor order; the fronts then read their pivot
 // rows of c contiguously.  Each factor row is read by its own supernode only,
 // before that supernode writes the same rows of x, so c lives in x's storage.
+// The element kernels below run on a (row blocks, right-hand sides) grid:
+// row k = blockIdx.x * blockDim.x + threadIdx.x, columns blockIdx.y,
+// blockIdx.y + gridDim.y, ... (no 64-bit division per element).
+inline dim3 grid_rows_cols(int64_t n, int64_t nrhs, int threads = 256) {
+  return dim3((unsigned)((n + threads - 1) / threads), (unsigned)(nrhs < 65535 ? (nrhs > 0 ? nrhs : 1) : 65535));
+}
+
 template <typename T>
 __global__ void k_rhs_factor_order(int64_t n, int64_t nrhs, const Wide<T>* __restrict__ b, int64_t ldb,
                                    const double* __restrict__ rs, const int32_t* __restrict__ qf,
                                    const int32_t* __restrict__ prow, T* __restrict__ bfo, int64_t ldo) {
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n * nrhs) return;
-  const int64_t k = e % n, c = e / n;
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
   const int orow = qf[prow[k]];
-  const Wide<T> v = b[orow + c * ldb];
-  bfo[k + c * ldo] = (T)(rs ? Wide<T>(rs[orow]) * v : v);
+  const double r = rs ? rs[orow] : 1.0;
+  for (int64_t c = blockIdx.y; c < nrhs; c += gridDim.y) {
+    const Wide<T> v = b[orow + c * ldb];
+    bfo[k + c * ldo] = (T)(rs ? Wide<T>(r) * v : v);
+  }
 }
 
 // Element walk of a column-major rows x cols block by n threads with one
@@ -178,18 +187,21 @@ __global__ void __launch_bounds__(32 * tiny_warps<T>()) k_fwd_tiny(DevPlan P, De
   const int rc = min(32, (int)(A.nrhs - c0));
   const int np = P.np[s], nf = P.nf[s], c1 = P.c1[s];
   const int64_t R = A.nrhs;
+  const FastDiv dnf((uint32_t)nf);
   for (int e = lane; e < nf * rc; e += 32) {
-    const int r = e % nf, c = e / nf;
+    const int c = (int)dnf.div(e), r = e - c * nf;
     f[r * kTinyLd + c] = r < np ? rhs_value<T>(A, c1, r, c0 + c) : T(0);
   }
   __syncwarp();
   for (int ci = P.child_ptr[s + 1] - 1; ci >= P.child_ptr[s]; --ci) {
     const int k = P.child_idx[ci];
     const int m = P.nu[k], nfk = P.nf[k], npk = P.np[k];
+    if (m == 0) continue;
     const T* wv = fsol + P.colbase[k] * R + npk;
     const int32_t* rl = P.rel + P.upd_off[k];
+    const FastDiv dm((uint32_t)m);
     for (int e = lane; e < m * rc; e += 32) {
-      const int r = e % m, c = e / m;
+      const int c = (int)dm.div(e), r = e - c * m;
       f[front_pos(S, c1, np, rl[r]) * kTinyLd + c] += wv[r + (int64_t)(c0 + c) * nfk];
     }
     __syncwarp();
@@ -204,7 +216,7 @@ __global__ void __launch_bounds__(32 * tiny_warps<T>()) k_fwd_tiny(DevPlan P, De
   __syncwarp();
   T* out = fsol + P.colbase[s] * R;
   for (int e = lane; e < nf * rc; e += 32) {
-    const int r = e % nf, c = e / nf;
+    const int c = (int)dnf.div(e), r = e - c * nf;
     out[r + (int64_t)(c0 + c) * nf] = f[r * kTinyLd + c];
   }
 }
@@ -225,13 +237,17 @@ __global__ void __launch_bounds__(32 * tiny_warps<T>()) k_bwd_tiny(DevPlan P, So
   const int64_t R = A.nrhs;
   const T* fs = fsol + P.colbase[s] * R;
   const int32_t* us = P.upd + P.upd_off[s];
+  const FastDiv dnp((uint32_t)np);
   for (int e = lane; e < np * rc; e += 32) {
-    const int r = e % np, c = e / np;
+    const int c = (int)dnp.div(e), r = e - c * np;
     f[r * kTinyLd + c] = fs[r + (int64_t)(c0 + c) * nf];
   }
-  for (int e = lane; e < nu * rc; e += 32) {
-    const int t = e % nu, c = e / nu;
-    f[(np + t) * kTinyLd + c] = xw[us[t] + (int64_t)(c0 + c) * A.ldx];
+  if (nu > 0) {
+    const FastDiv dnu((uint32_t)nu);
+    for (int e = lane; e < nu * rc; e += 32) {
+      const int c = (int)dnu.div(e), t = e - c * nu;
+      f[(np + t) * kTinyLd + c] = xw[us[t] + (int64_t)(c0 + c) * A.ldx];
+    }
   }
   __syncwarp();
   if (lane < rc) {
@@ -251,7 +267,7 @@ __global__ void __launch_bounds__(32 * tiny_warps<T>()) k_bwd_tiny(DevPlan P, So
   }
   __syncwarp();
   for (int e = lane; e < np * rc; e += 32) {
-    const int r = e % np, c = e / np;
+    const int c = (int)dnp.div(e), r = e - c * np;
     xw[c1 + r + (int64_t)(c0 + c) * A.ldx] = f[r * kTinyLd + c];
   }
 }
@@ -587,12 +603,14 @@ __global__ void __launch_bounds__(256) k_split_reduce(const SplitRed* __restrict
 template <typename T>
 __global__ void k_solve_finish(int64_t n, int64_t nrhs, const int32_t* __restrict__ qf, const T* __restrict__ xw,
                                int64_t ldw, Wide<T>* __restrict__ x, int64_t ldx, int accumulate) {
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n * nrhs) return;
-  const int64_t k = e % n, c = e / n;
-  const Wide<T> v = (Wide<T>)xw[k + c * ldw];
-  Wide<T>* dst = x + qf[k] + c * ldx;
-  *dst = accumulate ? *dst + v : v;
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int q = qf[k];
+  for (int64_t c = blockIdx.y; c < nrhs; c += gridDim.y) {
+    const Wide<T> v = (Wide<T>)xw[k + c * ldw];
+    Wide<T>* dst = x + q + c * ldx;
+    *dst = accumulate ? *dst + v : v;
+  }
 }
 
 // r = b - A * x with the unscaled A in CSR (interface.jl:173), FP64.
@@ -600,24 +618,26 @@ __global__ void k_residual(int64_t n, int64_t nrhs, const int32_t* __restrict__ 
                            const int32_t* __restrict__ src, const double* __restrict__ ax,
                            const double* __restrict__ b, int64_t ldb, const double* __restrict__ x, int64_t ldx,
                            double* __restrict__ r, int64_t ldr) {
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n * nrhs) return;
-  const int64_t i = e % n, c = e / n;
-  double acc = 0.0;
-  for (int p = rp[i]; p < rp[i + 1]; ++p) acc += ax[src[p]] * x[ci[p] + c * ldx];
-  r[i + c * ldr] = b[i + c * ldb] - acc;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int64_t c = blockIdx.y; c < nrhs; c += gridDim.y) {
+    double acc = 0.0;
+    for (int p = rp[i]; p < rp[i + 1]; ++p) acc += ax[src[p]] * x[ci[p] + c * ldx];
+    r[i + c * ldr] = b[i + c * ldb] - acc;
+  }
 }
 
 // The same for ComplexF64 A (values interleaved re, im), b, x and r.
 __global__ void k_residual_z(int64_t n, int64_t nrhs, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                              const int32_t* __restrict__ src, const zc* __restrict__ ax, const zc* __restrict__ b,
                              int64_t ldb, const zc* __restrict__ x, int64_t ldx, zc* __restrict__ r, int64_t ldr) {
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n * nrhs) return;
-  const int64_t i = e % n, c = e / n;
-  zc acc(0.0);
-  for (int p = rp[i]; p < rp[i + 1]; ++p) acc += ax[src[p]] * x[ci[p] + c * ldx];
-  r[i + c * ldr] = b[i + c * ldb] - acc;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int64_t c = blockIdx.y; c < nrhs; c += gridDim.y) {
+    zc acc(0.0);
+    for (int p = rp[i]; p < rp[i + 1]; ++p) acc += ax[src[p]] * x[ci[p] + c * ldx];
+    r[i + c * ldr] = b[i + c * ldb] - acc;
+  }
 }
 
 // Per-column maxima of |r|, |x|, |b| for the normwise backward error: a

@@ -1394,7 +1394,7 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
   SolveArgs A{R, reinterpret_cast<const double*>(d_b), ldb, (use_rs && h->have_rs) ? h->b_rs.as<double>() : nullptr,
               P.n, xw};
   klaunch(h, KC_FWD_ASSEMBLE, 0, (double)P.n * R * (16.0 + sizeof(T)), [&] {
-    k_rhs_factor_order<T><<<grid1(P.n * R, 256), 256, 0, st>>>(P.n, R, d_b, ldb, A.rs, h->b_qf.as<int32_t>(),
+    k_rhs_factor_order<T><<<grid_rows_cols(P.n, R), 256, 0, st>>>(P.n, R, d_b, ldb, A.rs, h->b_qf.as<int32_t>(),
                                                               h->b_prow.as<int32_t>(), xw, P.n);
   });
   const unsigned ychunks = (unsigned)((R + solve_cols<T>() - 1) / solve_cols<T>());
@@ -1551,7 +1551,7 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
   fork.join();
   }
   klaunch(h, KC_SOLVE_FINISH, 0, (double)P.n * R * (sizeof(T) + sizeof(Wide<T>) * (1.0 + accumulate)), [&] {
-    k_solve_finish<T><<<grid1(P.n * R, 256), 256, 0, st>>>(P.n, R, h->b_qf.as<int32_t>(), xw, P.n, d_x, ldx,
+    k_solve_finish<T><<<grid_rows_cols(P.n, R), 256, 0, st>>>(P.n, R, h->b_qf.as<int32_t>(), xw, P.n, d_x, ldx,
                                                            accumulate);
   });
   CK(cudaGetLastError());
@@ -1571,11 +1571,11 @@ void solve_refine(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide
       klaunch(h, KC_RESIDUAL, 2.0 * P.nnz_a * R, (8.0 + sizeof(Wide<T>)) * P.nnz_a + 3.0 * sizeof(Wide<T>) * P.n * R,
               [&] {
         if constexpr (is_complex_v<T>)
-          k_residual_z<<<grid1(P.n * R, 256), 256, 0, st>>>(P.n, R, h->b_csr_ptr.as<int32_t>(),
+          k_residual_z<<<grid_rows_cols(P.n, R), 256, 0, st>>>(P.n, R, h->b_csr_ptr.as<int32_t>(),
                                                             h->b_csr_col.as<int32_t>(), h->b_csr_src.as<int32_t>(),
                                                             h->b_ax.as<zc>(), d_b, ldb, d_x, ldx, r, P.n);
         else
-          k_residual<<<grid1(P.n * R, 256), 256, 0, st>>>(P.n, R, h->b_csr_ptr.as<int32_t>(),
+          k_residual<<<grid_rows_cols(P.n, R), 256, 0, st>>>(P.n, R, h->b_csr_ptr.as<int32_t>(),
                                                           h->b_csr_col.as<int32_t>(), h->b_csr_src.as<int32_t>(),
                                                           h->b_ax.as<double>(), d_b, ldb, d_x, ldx, r, P.n);
       });
@@ -2188,7 +2188,7 @@ int mfgpu_backward_error_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, i
     h->b_norm.ensure(16);
     CK(cudaMemsetAsync(h->b_err.p, 0, nrhs * 3 * 8, st));
     CK(cudaMemsetAsync(h->b_norm.p, 0, 8, st));
-    k_residual<<<grid1(n * nrhs, 256), 256, 0, st>>>(n, nrhs, h->b_csr_ptr.as<int32_t>(), h->b_csr_col.as<int32_t>(),
+    k_residual<<<grid_rows_cols(n, nrhs), 256, 0, st>>>(n, nrhs, h->b_csr_ptr.as<int32_t>(), h->b_csr_col.as<int32_t>(),
                                                      h->b_csr_src.as<int32_t>(), h->b_ax.as<double>(), d_b, ldb, d_x,
                                                      ldx, h->b_r.as<double>(), n);
     k_bwd_error_parts<<<dim3((unsigned)((n + 255) / 256), (unsigned)std::min<int64_t>(nrhs, 65535)), 256, 0, st>>>(
