@@ -410,10 +410,9 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   return r;
 }
 
-// Split eight consecutive K values into three bf16 parts and store each part
-// as one 16-byte chunk at byte offset `off` of its part buffer.
-__device__ __forceinline__ void bx_put8(uint32_t p1, uint32_t p2, uint32_t p3, uint32_t off, const float* v) {
-  uint32_t w1[4], w2[4], w3[4];
+// Split eight consecutive K values into three bf16 parts (x = hi + mid + lo
+// exactly for FP32 x, each part rounded to nearest), packed two per word.
+__device__ __forceinline__ void bx_split8(const float* v, uint32_t (&w1)[4], uint32_t (&w2)[4], uint32_t (&w3)[4]) {
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const float x0 = v[2 * q], x1 = v[2 * q + 1];
@@ -424,6 +423,13 @@ __device__ __forceinline__ void bx_put8(uint32_t p1, uint32_t p2, uint32_t p3, u
     const float m0 = __uint_as_float(w2[q] << 16), m1 = __uint_as_float(w2[q] & 0xFFFF0000u);
     w3[q] = pack_bf16(r0 - m0, r1 - m1);
   }
+}
+
+// Split eight consecutive K values into three bf16 parts and store each part
+// as one 16-byte chunk at byte offset `off` of its part buffer.
+__device__ __forceinline__ void bx_put8(uint32_t p1, uint32_t p2, uint32_t p3, uint32_t off, const float* v) {
+  uint32_t w1[4], w2[4], w3[4];
+  bx_split8(v, w1, w2, w3);
   asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(p1 + off), "r"(w1[0]), "r"(w1[1]), "r"(w1[2]),
                "r"(w1[3]) : "memory");
   asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(p2 + off), "r"(w2[0]), "r"(w2[1]), "r"(w2[2]),
@@ -625,6 +631,241 @@ __global__ void __launch_bounds__(BxCfg<BN, STAGES, ACCS>::kThreads, STAGES == 1
     } else if (t == 0) {
       atomicOr(flags + 1, 1);
     }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::kTmemCols));
+}
+
+// ---------------------------------------------------------------------------
+// Pre-split operands for the deferred Schur updates F22 -= L21 * U12 of the
+// FP32 fronts.  Those products are the largest of the factorization, and in
+// k_gemm_bx3 every CTA of a tile row (column) splits the same A (B) tile into
+// its bf16 parts again.  Here each 128 x 64 operand tile is split once, by
+// k_split_planes, into three 16 KB parts laid out byte for byte as the MMA's
+// shared-memory tiles (K-major, 128-byte swizzle); k_gemm_bx3p then moves
+// each part into shared memory with one bulk copy (cp.async.bulk, completion
+// counted on the stage's mbarrier) and issues the same six products per
+// 16-wide K step into the same four round-robin accumulators, so C is
+// bitwise what k_gemm_bx3 writes.
+constexpr int kPlaneTile = (int)kPlaneTileBytes;   // bytes of one bf16 part of one 128 x 64 tile
+constexpr int kBxpThreads = 512;           // producer lane (warp 0), MMA lane (warp 1), then 16 epilogue warps
+
+// Split unit u of a launch's tasks: units unit_base .. of a task are its A
+// tiles (row tile i, K block kb: i * kt + kb), then its B tiles (column tile
+// j, K block kb).  Same split, tile mapping and zero fill as k_gemm_bx3's
+// staging warps.
+__global__ void __launch_bounds__(256) k_split_planes(const GemmTask* __restrict__ tasks,
+                                                      const PlaneTask* __restrict__ pt, int ntasks,
+                                                      const float* __restrict__ pool, uint8_t* __restrict__ planes) {
+  const int64_t u = blockIdx.x;
+  int lo = 0, hi = ntasks - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pt[mid].unit_base <= u) lo = mid;
+    else hi = mid - 1;
+  }
+  const GemmTask tk = tasks[lo];
+  const PlaneTask p = pt[lo];
+  const int64_t local = u - p.unit_base;
+  const int64_t na = (int64_t)tk.tiles_m * p.kt;
+  const int t = threadIdx.x;
+  uint32_t w1[4], w2[4], w3[4];
+  float v[8];
+  if (local < na) {
+    const int i = (int)(local / p.kt), kb = (int)(local % p.kt);
+    uint8_t* dst = planes + p.a_off + (int64_t)(i * p.kt + kb) * 3 * kPlaneTile;
+    const float* A = pool + tk.a;
+    const int r = t & 127, row = i * 128 + r;
+    for (int c = t >> 7; c < 8; c += 2) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int kk = kb * 64 + 8 * c + j;
+        v[j] = (row < tk.m && kk < tk.k) ? A[(int64_t)row + (int64_t)kk * tk.lda] : 0.0f;
+      }
+      bx_split8(v, w1, w2, w3);
+      const uint32_t off = sw128_offset_b16(r, 8 * c);
+      *reinterpret_cast<uint4*>(dst + off) = make_uint4(w1[0], w1[1], w1[2], w1[3]);
+      *reinterpret_cast<uint4*>(dst + kPlaneTile + off) = make_uint4(w2[0], w2[1], w2[2], w2[3]);
+      *reinterpret_cast<uint4*>(dst + 2 * kPlaneTile + off) = make_uint4(w3[0], w3[1], w3[2], w3[3]);
+    }
+  } else {
+    const int64_t lb = local - na;
+    const int j = (int)(lb / p.kt), kb = (int)(lb % p.kt);
+    uint8_t* dst = planes + p.b_off + (int64_t)(j * p.kt + kb) * 3 * kPlaneTile;
+    const float* B = pool + tk.b;
+    for (int q = 0; q < 4; ++q) {
+      const int idx = t + q * 256, n = idx >> 3, c = idx & 7, col = j * 128 + n;
+#pragma unroll
+      for (int jj = 0; jj < 8; ++jj) {
+        const int kk = kb * 64 + 8 * c + jj;
+        v[jj] = (col < tk.n && kk < tk.k) ? B[(int64_t)kk + (int64_t)col * tk.ldb] : 0.0f;
+      }
+      bx_split8(v, w1, w2, w3);
+      const uint32_t off = sw128_offset_b16(n, 8 * c);
+      *reinterpret_cast<uint4*>(dst + off) = make_uint4(w1[0], w1[1], w1[2], w1[3]);
+      *reinterpret_cast<uint4*>(dst + kPlaneTile + off) = make_uint4(w2[0], w2[1], w2[2], w2[3]);
+      *reinterpret_cast<uint4*>(dst + 2 * kPlaneTile + off) = make_uint4(w3[0], w3[1], w3[2], w3[3]);
+    }
+  }
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// Bulk copy (no tensor map, no multicast) of `bytes` from global memory to
+// this CTA's shared memory, counted on mbarrier `bar`.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(dst), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+
+template <int STAGES>
+__global__ void __launch_bounds__(kBxpThreads, 1)
+    k_gemm_bx3p(const GemmTask* __restrict__ tasks, const PlaneTask* __restrict__ pt, int ntasks,
+                const uint8_t* __restrict__ planes, float* pc, int* __restrict__ flags, uint64_t wait_ns) {
+  using Cfg = BxCfg<128, 2, 4>;   // tile shape, stage layout, instruction descriptor, accumulators
+  constexpr int BN = 128;
+  extern __shared__ __align__(16) uint8_t bxp_smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)bxp_smem_raw + 1023) & ~(uintptr_t)1023);
+  __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done, stall;
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int failed;
+
+  const int t = threadIdx.x, warp = warp_id(), lane = lane_id();
+  int lo = 0, hi = ntasks - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tasks[mid].tile_base <= (int64_t)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  const GemmTask tk = tasks[lo];
+  const PlaneTask pk = pt[lo];
+  const int64_t local = blockIdx.x - tk.tile_base;
+  const int ti = (int)(local % tk.tiles_m), tj = (int)(local / tk.tiles_m);
+  const int m0 = ti * Cfg::BM, n0 = tj * BN;
+  const int M = tk.m, N = tk.n;
+  const int nk = pk.kt;
+
+  if (t == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(&done, 1);
+    mbar_init(&stall, 1);   // nothing arrives on it (test hook, flags[2])
+    failed = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(Cfg::kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  const uint32_t sbase = smem_u32(smem);
+
+  if (warp == 0 && lane == 0) {
+    const uint8_t* a_src = planes + pk.a_off + (int64_t)ti * nk * 3 * kPlaneTile;
+    const uint8_t* b_src = planes + pk.b_off + (int64_t)tj * nk * 3 * kPlaneTile;
+    int issued = 0;
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % STAGES;
+      if (kb >= STAGES && !mbar_wait(&empty[s], (uint32_t)((kb / STAGES - 1) & 1), wait_ns)) {
+        failed = 1;
+        break;
+      }
+      if (failed) break;
+      const uint32_t st = sbase + s * Cfg::kStageBytes;
+      mbar_arrive_expect_tx(&full[s], 6 * kPlaneTile);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        bulk_g2s(st + q * Cfg::kABytes, a_src + (int64_t)(kb * 3 + q) * kPlaneTile, kPlaneTile, &full[s]);
+        bulk_g2s(st + 3 * Cfg::kABytes + q * Cfg::kBBytes, b_src + (int64_t)(kb * 3 + q) * kPlaneTile, kPlaneTile,
+                 &full[s]);
+      }
+      ++issued;
+    }
+    // copies in flight land before this CTA may end (a stage the MMA lane
+    // did not consume after a wait ran out)
+    for (int kb = issued > STAGES ? issued - STAGES : 0; kb < issued; ++kb)
+      mbar_wait(&full[kb % STAGES], (uint32_t)((kb / STAGES) & 1), kTcDrainNs);
+  } else if (warp == 1 && lane == 0) {
+    if (flags[2] && !mbar_wait(&stall, 0u, wait_ns)) failed = 1;   // test hook: a wait that runs out
+    for (int kb = 0; kb < nk && !failed; ++kb) {
+      const int s = kb % STAGES;
+      if (!mbar_wait(&full[s], (uint32_t)((kb / STAGES) & 1), wait_ns)) {
+        failed = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a1 = sbase + s * Cfg::kStageBytes, a2 = a1 + Cfg::kABytes, a3 = a2 + Cfg::kABytes;
+      const uint32_t b1 = a1 + 3 * Cfg::kABytes, b2 = b1 + Cfg::kBBytes, b3 = b2 + Cfg::kBBytes;
+#pragma unroll
+      for (int ks = 0; ks < Cfg::BK / 16; ++ks) {
+        const uint32_t ko = ks * 32;
+        const uint32_t acc = tmem + (uint32_t)((kb % Cfg::kAccs) * BN);
+        tc_mma_bf16(acc, umma_desc_sw128(a2 + ko), umma_desc_sw128(b2 + ko), Cfg::kIdesc,
+                    (kb >= Cfg::kAccs || ks > 0) ? 1u : 0u);
+        tc_mma_bf16(acc, umma_desc_sw128(a3 + ko), umma_desc_sw128(b1 + ko), Cfg::kIdesc, 1u);
+        tc_mma_bf16(acc, umma_desc_sw128(a1 + ko), umma_desc_sw128(b3 + ko), Cfg::kIdesc, 1u);
+        tc_mma_bf16(acc, umma_desc_sw128(a2 + ko), umma_desc_sw128(b1 + ko), Cfg::kIdesc, 1u);
+        tc_mma_bf16(acc, umma_desc_sw128(a1 + ko), umma_desc_sw128(b2 + ko), Cfg::kIdesc, 1u);
+        tc_mma_bf16(acc, umma_desc_sw128(a1 + ko), umma_desc_sw128(b1 + ko), Cfg::kIdesc, 1u);
+      }
+      tc_commit(&empty[s]);
+    }
+    tc_commit(&done);
+  }
+  __syncwarp();
+  tc_wait_done(&done, wait_ns, &failed);
+  __syncthreads();
+  const bool ok = !failed;
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) {
+    // warp w reads TMEM lanes 32 (w % 4) .. (rows) at columns 32 (w / 4) ..
+    float* C = pc + tk.c;
+    const int q = warp & 3, c0 = (warp >> 2) * 32;
+    const int row = m0 + q * 32 + lane;
+    const float* D = tk.mode == kGemmFrom ? pc + tk.d : C;
+    const int ldD = tk.mode == kGemmFrom ? tk.ldd : tk.ldc;
+    const bool ld = tk.mode == kGemmSub || tk.mode == kGemmFrom;
+    const float sgn = tk.mode == kGemmSet ? -1.0f : 1.0f;
+    const int nacc = nk < Cfg::kAccs ? nk : Cfg::kAccs;
+    {
+      uint32_t v[32];
+      float acc[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) acc[j] = 0.0f;
+      for (int b = 0; b < nacc; ++b) {
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + c0), v);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[j] += __uint_as_float(v[j]);
+      }
+      if (row < M) {
+#pragma unroll
+        for (int g = 0; g < 32; g += 8) {
+          float cv[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int col = n0 + c0 + g + j;
+            cv[j] = (ld && col < N) ? D[(int64_t)row + (int64_t)col * ldD] : 0.0f;
+          }
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int col = n0 + c0 + g + j;
+            if (col < N) C[(int64_t)row + (int64_t)col * tk.ldc] = cv[j] - sgn * acc[g + j];
+          }
+        }
+      }
+    }
+  } else if (t == 0) {
+    atomicOr(flags + 1, 1);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();

@@ -212,7 +212,8 @@ struct mfgpu_ctx {
   DevBuf b_c1, b_np, b_nu, b_nf, b_upd_off, b_front_off, b_colbase, b_child_ptr, b_child_idx, b_upd, b_rel, b_uoff,
       b_v_src, b_v_srow, b_v_frow, b_fc_super, b_fc_vbeg, b_fc_vend, b_fc_ch_ptr, b_fc_ch, b_lcolptr, b_ucolptr, b_qf,
       b_csr_ptr, b_csr_col, b_csr_src;
-  DevBuf b_small, b_panel, b_trsm, b_gemm, b_gemm_tc;
+  DevBuf b_small, b_panel, b_trsm, b_gemm, b_gemm_tc, b_plane_tasks;
+  DevBuf b_planes;   // bf16 parts of one level's Schur-update operand tiles (FP32 fronts)
   bool use_tc = true;      // FP32 fronts: GEMMs on tensor cores
   uint64_t wait_ns = kTcWaitNs;   // bound on every device-side wait (mbarriers, grid barriers)
   bool tc_bf16x3 = true;   // tensor-core split: BF16x3 (FP32 accuracy) or 3xTF32
@@ -429,6 +430,7 @@ void upload_launches(mfgpu_ctx* h) {
   upload(h->b_trsm, P.trsm_tasks, h->stream);
   upload(h->b_gemm, P.gemm_tasks, h->stream);
   upload(h->b_gemm_tc, P.gemm_tasks_tc, h->stream);
+  upload(h->b_plane_tasks, P.plane_tasks, h->stream);
 }
 
 DevState dev_state(mfgpu_ctx* h) {
@@ -553,6 +555,7 @@ void configure_kernels() {
                           (int)BxCfg<128, 2>::kSmem));
   CK(cudaFuncSetAttribute(k_gemm_bx3<128, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)BxCfg<128, 1, 1>::kSmem));
+  CK(cudaFuncSetAttribute(k_gemm_bx3p<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BxCfg<128, 2>::kSmem));
   CK(cudaFuncSetAttribute(k_solve_persistent<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)persistent_smem_bytes<T>()));
   done = true;
@@ -598,6 +601,15 @@ void launch_gemm<zc>(const GemmTask* tasks, int64_t count, int64_t tiles, const 
 // per SM.
 bool tc_worthwhile(double flops, int64_t tiles_tc) {
   return tiles_tc > 0 && flops >= 2.0 * kTcTile * kTcTile * 64.0 * (double)tiles_tc;
+}
+
+// The Schur updates take the split-once form when their tiles walk K of at
+// least kSplitPlanesMinK on average: a tile's epilogue and set-up are then
+// small beside its K loop, and the split is shared by the tiles of a row
+// (column).  Shorter K stays on k_gemm_bx3.
+constexpr double kSplitPlanesMinK = 192;
+bool split_worthwhile(const Launch& L) {
+  return L.tiles_tc > 0 && L.flops >= 2.0 * kTcTile * kTcTile * kSplitPlanesMinK * (double)L.tiles_tc;
 }
 
 // Kernel variant of tunable GEMM launch `id` with FP32 operands: the
@@ -723,7 +735,18 @@ void run_factor_launches(mfgpu_ctx* h) {
         break;
       case kLaunchGemm:
         h->cur_tune = (int32_t)tune_id;
-        if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, tc_worthwhile(L.flops, L.tiles_tc)))
+        if (sizeof(T) == 4 && L.schur && h->tc_bf16x3 && h->b_planes.p && split_worthwhile(L) &&
+            gemm_use_tc(h, tune_id, tc_worthwhile(L.flops, L.tiles_tc)))
+          // the Schur updates: operand tiles split once, then moved by bulk copies
+          klaunch(h, KC_GEMM_FACTOR, L.flops, bytes, [&] {
+            const GemmTask* tk = h->b_gemm_tc.as<GemmTask>() + L.first;
+            const PlaneTask* pk = h->b_plane_tasks.as<PlaneTask>() + L.first;
+            uint8_t* planes = h->b_planes.as<uint8_t>();
+            k_split_planes<<<(unsigned)L.split_units, 256, 0, st>>>(tk, pk, (int)L.count, (const float*)pool, planes);
+            k_gemm_bx3p<2><<<(unsigned)L.tiles_tc, kBxpThreads, BxCfg<128, 2>::kSmem, st>>>(
+                tk, pk, (int)L.count, planes, (float*)pool, h->b_flags.as<int>(), h->wait_ns);
+          }, L.level, L.tiles_tc);
+        else if (sizeof(T) == 4 && gemm_use_tc(h, tune_id, tc_worthwhile(L.flops, L.tiles_tc)))
           klaunch(h, KC_GEMM_FACTOR, L.flops, bytes, [&] {
             launch_tc(h, h->b_gemm_tc.as<GemmTask>() + L.first, L.count, L.tiles_tc, (const float*)pool,
                       (const float*)pool, (float*)pool, st, L.max_k);
@@ -880,13 +903,17 @@ int factor_impl(mfgpu_ctx* h, int32_t check) {
   }
   CK(cudaEventRecord(h->ev0, st));
   for (int attempt = 0; attempt < 2; ++attempt) {
+    // the planes buffer of the Schur updates' split operands (FP32 fronts;
+    // the pivoting launch list may need a different size)
+    if constexpr (std::is_same_v<T, float>)
+      if (P.planes_bytes > 0 && h->use_tc && h->tc_bf16x3) h->b_planes.ensure((size_t)P.planes_bytes);
     const std::vector<uintptr_t> key = {
         sizeof(T), (uintptr_t)h->launches_safe, (uintptr_t)h->have_rs, (uintptr_t)h->b_pool.p, (uintptr_t)h->b_vx.p,
         (uintptr_t)h->b_ax.p, (uintptr_t)h->b_rs.p, (uintptr_t)h->b_dinv.p, (uintptr_t)h->b_li.p,
         (uintptr_t)h->b_lx.p, (uintptr_t)h->b_ui.p, (uintptr_t)h->b_ux.p, (uintptr_t)h->b_small.p,
         (uintptr_t)h->b_panel.p, (uintptr_t)h->b_trsm.p, (uintptr_t)h->b_gemm.p, (uintptr_t)h->b_ipiv.p,
         (uintptr_t)h->b_gemm_tc.p, (uintptr_t)h->use_tc, (uintptr_t)h->tc_bf16x3, (uintptr_t)h->choice_version,
-        (uintptr_t)h->wait_ns,
+        (uintptr_t)h->wait_ns, (uintptr_t)h->b_planes.p, (uintptr_t)h->b_plane_tasks.p,
         (uintptr_t)h->b_info.p, (uintptr_t)h->b_flags.p, (uintptr_t)st};
     run_sequence(h, h->factor_key, h->factor_exec, h->factor_nodes, key, [&] { issue_factor<T>(h); });
     if (!P.has_speculative) break;
@@ -1750,7 +1777,7 @@ void mfgpu_destroy(mfgpu_ctx* h) {
                     &h->b_child_ptr, &h->b_child_idx, &h->b_upd, &h->b_rel, &h->b_uoff, &h->b_v_src, &h->b_v_srow,
                     &h->b_v_frow, &h->b_fc_super, &h->b_fc_vbeg, &h->b_fc_vend, &h->b_fc_ch_ptr, &h->b_fc_ch,
                     &h->b_lcolptr, &h->b_ucolptr, &h->b_qf, &h->b_csr_ptr, &h->b_csr_col, &h->b_csr_src,
-                    &h->b_small, &h->b_panel, &h->b_trsm, &h->b_gemm, &h->b_gemm_tc, &h->b_pool, &h->b_vx, &h->b_ax, &h->b_rs,
+                    &h->b_small, &h->b_panel, &h->b_trsm, &h->b_gemm, &h->b_gemm_tc, &h->b_plane_tasks, &h->b_planes, &h->b_pool, &h->b_vx, &h->b_ax, &h->b_rs,
                     &h->b_ipiv, &h->b_info, &h->b_prow, &h->b_rowfac, &h->b_flags, &h->b_dinv, &h->b_dinv_off,
                     &h->b_inv_off, &h->b_inv_blocks, &h->b_inv_tasks, &h->b_inv_tasks_tc, &h->b_lpan_off,
                     &h->b_u12_off, &h->b_skinny, &h->sched.d_skinny, &h->b_seg_end, &h->b_col_orig, &h->b_o_c1,

@@ -781,6 +781,8 @@ void build_launches_core(Plan& P, bool safe) {
   P.trsm_tasks.clear();
   P.gemm_tasks.clear();
   P.gemm_tasks_tc.clear();
+  P.plane_tasks.clear();
+  P.planes_bytes = 0;
   P.launches.clear();
   P.has_speculative = false;
   std::vector<int32_t> large;
@@ -924,8 +926,31 @@ void build_launches_core(Plan& P, bool safe) {
       lg.elems += 2.0 * nu * nu + 2.0 * nu * npv;
       push_gemm(P, lg, g);
     }
-    if (lg.count) P.launches.push_back(lg);
+    if (lg.count) {
+      // the operand tiles of these products, split into bf16 parts once
+      // (tensor-core form); the planes buffer is reused level by level
+      lg.schur = 1;
+      P.plane_tasks.resize(P.gemm_tasks_tc.size());
+      int64_t off = 0, units = 0;
+      for (int64_t i = lg.first; i < lg.first + lg.count; ++i) {
+        const GemmTask& g = P.gemm_tasks_tc[i];
+        PlaneTask pt{};
+        pt.kt = (int32_t)ceil_div(g.k, 64);
+        pt.a_off = off;
+        off += (int64_t)g.tiles_m * pt.kt * 3 * kPlaneTileBytes;
+        pt.b_off = off;
+        off += (int64_t)g.tiles_n * pt.kt * 3 * kPlaneTileBytes;
+        pt.unit_base = units;
+        units += (int64_t)(g.tiles_m + g.tiles_n) * pt.kt;
+        P.plane_tasks[i] = pt;
+      }
+      lg.split_units = units;
+      lg.planes_bytes = off;
+      P.planes_bytes = std::max(P.planes_bytes, off);
+      P.launches.push_back(lg);
+    }
   }
+  P.plane_tasks.resize(P.gemm_tasks_tc.size());
 }
 
 void add_copy_launches(Plan& P);
