@@ -639,8 +639,9 @@ __global__ void __launch_bounds__(BxCfg<BN, STAGES, ACCS>::kThreads, STAGES == 1
 }
 
 // ---------------------------------------------------------------------------
-// Pre-split operands for the deferred Schur updates F22 -= L21 * U12 of the
-// FP32 fronts.  Those products are the largest of the factorization, and in
+// Pre-split operands for the long-K updates of the FP32 fronts (the deferred
+// Schur updates F22 -= L21 * U12 and the K = 256 block updates of the pivot
+// blocks).  Those products are the largest of the factorization, and in
 // k_gemm_bx3 every CTA of a tile row (column) splits the same A (B) tile into
 // its bf16 parts again.  Here each 128 x 64 operand tile is split once, by
 // k_split_planes, into three 16 KB parts laid out byte for byte as the MMA's

@@ -603,10 +603,10 @@ bool tc_worthwhile(double flops, int64_t tiles_tc) {
   return tiles_tc > 0 && flops >= 2.0 * kTcTile * kTcTile * 64.0 * (double)tiles_tc;
 }
 
-// The Schur updates take the split-once form when their tiles walk K of at
-// least kSplitPlanesMinK on average: a tile's epilogue and set-up are then
-// small beside its K loop, and the split is shared by the tiles of a row
-// (column).  Shorter K stays on k_gemm_bx3.
+// A factor GEMM launch (FP32 fronts) takes the split-once form when its
+// tiles walk K of at least kSplitPlanesMinK on average: a tile's epilogue
+// and set-up are then small beside its K loop, and the split is shared by
+// the tiles of a row (column).  Shorter K stays on k_gemm_bx3.
 constexpr double kSplitPlanesMinK = 192;
 bool split_worthwhile(const Launch& L) {
   return L.tiles_tc > 0 && L.flops >= 2.0 * kTcTile * kTcTile * kSplitPlanesMinK * (double)L.tiles_tc;
@@ -735,9 +735,9 @@ void run_factor_launches(mfgpu_ctx* h) {
         break;
       case kLaunchGemm:
         h->cur_tune = (int32_t)tune_id;
-        if (sizeof(T) == 4 && L.schur && h->tc_bf16x3 && h->b_planes.p && split_worthwhile(L) &&
+        if (sizeof(T) == 4 && h->tc_bf16x3 && h->b_planes.p && split_worthwhile(L) &&
             gemm_use_tc(h, tune_id, tc_worthwhile(L.flops, L.tiles_tc)))
-          // the Schur updates: operand tiles split once, then moved by bulk copies
+          // long-K updates: operand tiles split once, then moved by bulk copies
           klaunch(h, KC_GEMM_FACTOR, L.flops, bytes, [&] {
             const GemmTask* tk = h->b_gemm_tc.as<GemmTask>() + L.first;
             const PlaneTask* pk = h->b_plane_tasks.as<PlaneTask>() + L.first;
@@ -903,7 +903,7 @@ int factor_impl(mfgpu_ctx* h, int32_t check) {
   }
   CK(cudaEventRecord(h->ev0, st));
   for (int attempt = 0; attempt < 2; ++attempt) {
-    // the planes buffer of the Schur updates' split operands (FP32 fronts;
+    // the planes buffer of the long-K updates' split operands (FP32 fronts;
     // the pivoting launch list may need a different size)
     if constexpr (std::is_same_v<T, float>)
       if (P.planes_bytes > 0 && h->use_tc && h->tc_bf16x3) h->b_planes.ensure((size_t)P.planes_bytes);

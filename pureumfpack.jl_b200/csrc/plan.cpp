@@ -926,31 +926,31 @@ void build_launches_core(Plan& P, bool safe) {
       lg.elems += 2.0 * nu * nu + 2.0 * nu * npv;
       push_gemm(P, lg, g);
     }
-    if (lg.count) {
-      // the operand tiles of these products, split into bf16 parts once
-      // (tensor-core form); the planes buffer is reused level by level
-      lg.schur = 1;
-      P.plane_tasks.resize(P.gemm_tasks_tc.size());
-      int64_t off = 0, units = 0;
-      for (int64_t i = lg.first; i < lg.first + lg.count; ++i) {
-        const GemmTask& g = P.gemm_tasks_tc[i];
-        PlaneTask pt{};
-        pt.kt = (int32_t)ceil_div(g.k, 64);
-        pt.a_off = off;
-        off += (int64_t)g.tiles_m * pt.kt * 3 * kPlaneTileBytes;
-        pt.b_off = off;
-        off += (int64_t)g.tiles_n * pt.kt * 3 * kPlaneTileBytes;
-        pt.unit_base = units;
-        units += (int64_t)(g.tiles_m + g.tiles_n) * pt.kt;
-        P.plane_tasks[i] = pt;
-      }
-      lg.split_units = units;
-      lg.planes_bytes = off;
-      P.planes_bytes = std::max(P.planes_bytes, off);
-      P.launches.push_back(lg);
-    }
+    if (lg.count) P.launches.push_back(lg);
   }
-  P.plane_tasks.resize(P.gemm_tasks_tc.size());
+  // every GEMM launch's operand tiles as bf16 parts (the tensor-core form
+  // that splits its operands once; the planes buffer is reused launch by
+  // launch, the launches run in order on one stream)
+  P.plane_tasks.assign(P.gemm_tasks_tc.size(), PlaneTask{});
+  for (Launch& L : P.launches) {
+    if (L.kind != kLaunchGemm) continue;
+    int64_t off = 0, units = 0;
+    for (int64_t i = L.first; i < L.first + L.count; ++i) {
+      const GemmTask& g = P.gemm_tasks_tc[i];
+      PlaneTask pt{};
+      pt.kt = (int32_t)ceil_div(g.k, 64);
+      pt.a_off = off;
+      off += (int64_t)g.tiles_m * pt.kt * 3 * kPlaneTileBytes;
+      pt.b_off = off;
+      off += (int64_t)g.tiles_n * pt.kt * 3 * kPlaneTileBytes;
+      pt.unit_base = units;
+      units += (int64_t)(g.tiles_m + g.tiles_n) * pt.kt;
+      P.plane_tasks[i] = pt;
+    }
+    L.split_units = units;
+    L.planes_bytes = off;
+    P.planes_bytes = std::max(P.planes_bytes, off);
+  }
 }
 
 void add_copy_launches(Plan& P);

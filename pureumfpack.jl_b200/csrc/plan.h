@@ -78,8 +78,8 @@ struct GemmTask {        // column-major, offsets in elements of the launch's ba
   int32_t ldd, pad;      // kGemmFrom: leading dimension of D
 };
 
-// A deferred Schur update F22 -= L21 * U12 (FP32 fronts on tensor cores)
-// with its operands split once into bf16 parts: byte offsets of the task's A
+// A factor GEMM task (FP32 fronts on tensor cores) with its operands split
+// once into bf16 parts: byte offsets of the task's A
 // and B part tiles in the planes buffer (tiles_m (tiles_n) x kt tiles of
 // three kPlaneTileBytes parts each), the prefix of the launch's split units
 // ((tiles_m + tiles_n) * kt per task), and its K blocks of 64.
@@ -118,8 +118,7 @@ struct Launch {
   double flops = 0;      // algorithmic flops of the launch
   double elems = 0;      // algorithmic element moves (x sizeof(front type) = bytes)
   double extra_bytes = 0;// index / FP64 input bytes
-  int32_t schur = 0;     // GEMM launches: the level's deferred Schur updates (plane_tasks set)
-  int64_t split_units = 0, planes_bytes = 0;   // their operand split: units, buffer bytes
+  int64_t split_units = 0, planes_bytes = 0;   // GEMM launches: the operand split (plane_tasks): units, bytes
 };
 
 struct Plan {
@@ -188,8 +187,8 @@ struct Plan {
   std::vector<TrsmTask> trsm_tasks;
   std::vector<GemmTask> gemm_tasks;
   std::vector<GemmTask> gemm_tasks_tc;   // the same updates tiled 128 x 128 (FP32 fronts, tensor cores)
-  std::vector<PlaneTask> plane_tasks;    // per gemm_tasks_tc entry; set for the Schur launches' tasks
-  int64_t planes_bytes = 0;              // largest planes buffer of one Schur launch
+  std::vector<PlaneTask> plane_tasks;    // per gemm_tasks_tc entry
+  int64_t planes_bytes = 0;              // largest planes buffer of one GEMM launch
   std::vector<Launch> launches;
   bool has_speculative = false;
   // Front merging (execution only).  Chains of supernodes (a child whose
