@@ -659,7 +659,8 @@ constexpr int kBxpThreads = 512;           // producer lane (warp 0), MMA lane (
 // staging warps.
 __global__ void __launch_bounds__(256) k_split_planes(const GemmTask* __restrict__ tasks,
                                                       const PlaneTask* __restrict__ pt, int ntasks,
-                                                      const float* __restrict__ pool, uint8_t* __restrict__ planes) {
+                                                      const float* __restrict__ pa, const float* __restrict__ pb,
+                                                      uint8_t* __restrict__ planes) {
   const int64_t u = blockIdx.x;
   int lo = 0, hi = ntasks - 1;
   while (lo < hi) {
@@ -677,7 +678,7 @@ __global__ void __launch_bounds__(256) k_split_planes(const GemmTask* __restrict
   if (local < na) {
     const int i = (int)(local / p.kt), kb = (int)(local % p.kt);
     uint8_t* dst = planes + p.a_off + (int64_t)(i * p.kt + kb) * 3 * kPlaneTile;
-    const float* A = pool + tk.a;
+    const float* A = pa + tk.a;
     const int r = t & 127, row = i * 128 + r;
     for (int c = t >> 7; c < 8; c += 2) {
 #pragma unroll
@@ -695,7 +696,7 @@ __global__ void __launch_bounds__(256) k_split_planes(const GemmTask* __restrict
     const int64_t lb = local - na;
     const int j = (int)(lb / p.kt), kb = (int)(lb % p.kt);
     uint8_t* dst = planes + p.b_off + (int64_t)(j * p.kt + kb) * 3 * kPlaneTile;
-    const float* B = pool + tk.b;
+    const float* B = pb + tk.b;
     for (int q = 0; q < 4; ++q) {
       const int idx = t + q * 256, n = idx >> 3, c = idx & 7, col = j * 128 + n;
 #pragma unroll

@@ -742,7 +742,8 @@ void run_factor_launches(mfgpu_ctx* h) {
             const GemmTask* tk = h->b_gemm_tc.as<GemmTask>() + L.first;
             const PlaneTask* pk = h->b_plane_tasks.as<PlaneTask>() + L.first;
             uint8_t* planes = h->b_planes.as<uint8_t>();
-            k_split_planes<<<(unsigned)L.split_units, 256, 0, st>>>(tk, pk, (int)L.count, (const float*)pool, planes);
+            k_split_planes<<<(unsigned)L.split_units, 256, 0, st>>>(tk, pk, (int)L.count, (const float*)pool,
+                                                                    (const float*)pool, planes);
             k_gemm_bx3p<2><<<(unsigned)L.tiles_tc, kBxpThreads, BxCfg<128, 2>::kSmem, st>>>(
                 tk, pk, (int)L.count, planes, (float*)pool, h->b_flags.as<int>(), h->wait_ns);
           }, L.level, L.tiles_tc);
