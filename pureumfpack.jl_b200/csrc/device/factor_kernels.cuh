@@ -508,6 +508,52 @@ __device__ __forceinline__ void spec_inverse_blocks(const T* A, T* Li, T* Ui, in
   }
 }
 
+// The triangles of factored diagonal block i inverted (into Li / Ui's
+// diagonal block i) by one warp: lanes 0-7 a column of inv(L_ii) each,
+// lanes 8-15 a column of inv(U_ii), the block and its pivots' reciprocals in
+// every lane's registers so the dependent chains read no shared memory.
+template <typename T>
+__device__ __forceinline__ void spec_diag_inverses(const T* A, T* Li, T* Ui, int i, int lane) {
+  const int s8 = 8 * i;
+  T blk[8][8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int q = 0; q < 8; ++q) blk[r][q] = A[(s8 + r) + (s8 + q) * kLdS];
+  T rd[8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) rd[r] = T(1) / blk[r][r];
+  if (lane < 8) {          // column `lane` of inv(L_ii)
+    const int c = lane;
+    T x[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) x[r] = (r == c) ? T(1) : T(0);
+#pragma unroll
+    for (int r = 1; r < 8; ++r) {
+      T v = x[r];
+#pragma unroll
+      for (int k = 0; k < r; ++k) v -= blk[r][k] * x[k];
+      x[r] = (r > c) ? v : x[r];
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r) Li[(s8 + r) + (s8 + c) * kLdS] = x[r];
+  } else if (lane < 16) {  // column `lane - 8` of inv(U_ii)
+    const int c = lane - 8;
+    T x[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) x[r] = T(0);
+#pragma unroll
+    for (int r = 7; r >= 0; --r) {
+      T v = (r == c) ? T(1) : T(0);
+#pragma unroll
+      for (int k = r + 1; k < 8; ++k) v -= blk[r][k] * x[k];
+      x[r] = (r <= c) ? v * rd[r] : T(0);
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r) Ui[(s8 + r) + (s8 + c) * kLdS] = x[r];
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState S, const PanelTask* __restrict__ tasks,
                                                              T* __restrict__ pool, T* __restrict__ dinv) {
@@ -517,6 +563,7 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
   T* Ui = Li + 64 * kLdS;                    // inv(U)
   __shared__ int bad;
   __shared__ int seg[64];                    // per block column: end of its pivot rows (block-relative)
+  __shared__ T rdiag[64];                    // reciprocals of U's diagonal
   const PanelTask tk = tasks[blockIdx.x];
   const int s_ = tk.s, k0 = tk.k0;
   const int np = P.np[s_], nf = P.nf[s_], c1 = P.c1[s_];
@@ -545,6 +592,11 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
   bool violated = false;
   for (int sb = 0; sb < 8; ++sb) {
     const int s8 = sb * 8;
+    // (A) warp 0 factors diagonal block sb; meanwhile warp 1 inverts the
+    // triangles of block sb - 1, and warps 2-7 form the off-diagonal
+    // inverse blocks of block row / column sb - 2 and apply step sb - 1's
+    // update to the blocks beyond sb (its block row and column sb were
+    // updated ahead, in (C) of step sb - 1).  All read final data only.
     if (warp == 0) {   // 8 x 8 diagonal block: lanes 0..7 hold its rows
       T a[8];
 #pragma unroll
@@ -567,96 +619,89 @@ __global__ void __launch_bounds__(kSpecThreads) k_panel_spec(DevPlan P, DevState
       if (lane < 8) {
 #pragma unroll
         for (int q = 0; q < 8; ++q) A[(s8 + lane) + (s8 + q) * kLdS] = a[q];
+        rdiag[s8 + lane] = T(1) / a[lane];   // the reciprocal of this row's pivot
       }
-      // the factored 8 x 8 block to every lane's registers (row i from lane
-      // i), and the reciprocals of its pivots, for the triangular inverses:
-      // no shared-memory loads or divisions inside their dependent chains
-      T blk[8][8];
+    } else if (warp == 1) {
+      if (sb >= 1) spec_diag_inverses<T>(A, Li, Ui, sb - 1, lane);
+    } else {
+      const int u = t - 64;
+      if (sb >= 2) spec_inverse_blocks<T>(A, Li, Ui, sb - 2, u);
+      if (sb >= 1) {   // step sb - 1 on the blocks beyond sb
+        const int p8 = s8 - 8, b0 = s8 + 8, nd = 64 - b0;
+        if (nd > 0) {
+          const FastDiv dnd((uint32_t)nd);
+          for (int e = u; e < nd * nd; e += kSpecThreads - 64) {
+            const int q = (int)dnd.div(e), r = b0 + e - q * nd, c = b0 + q;
+            T v = A[r + c * kLdS];
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int q = 0; q < 8; ++q) blk[i][q] = __shfl_sync(0xffffffffu, a[q], i);
-      T rd[8];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) rd[i] = T(1) / blk[i][i];
-      if (lane < 8) {          // column `lane` of inv(L_ss)
-        const int c = lane;
-        T x[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) x[i] = (i == c) ? T(1) : T(0);
-#pragma unroll
-        for (int i = 1; i < 8; ++i) {
-          T v = x[i];
-#pragma unroll
-          for (int k = 0; k < i; ++k) v -= blk[i][k] * x[k];
-          x[i] = (i > c) ? v : x[i];
+            for (int k = 0; k < 8; ++k) v -= A[r + (p8 + k) * kLdS] * A[(p8 + k) + c * kLdS];
+            A[r + c * kLdS] = v;
+          }
         }
-#pragma unroll
-        for (int i = 0; i < 8; ++i) Li[(s8 + i) + (s8 + c) * kLdS] = x[i];
-      } else if (lane < 16) {  // column `lane-8` of inv(U_ss)
-        const int c = lane - 8;
-        T x[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) x[i] = T(0);
-#pragma unroll
-        for (int i = 7; i >= 0; --i) {
-          T v = (i == c) ? T(1) : T(0);
-#pragma unroll
-          for (int k = i + 1; k < 8; ++k) v -= blk[i][k] * x[k];
-          x[i] = (i <= c) ? v * rd[i] : T(0);
-        }
-#pragma unroll
-        for (int i = 0; i < 8; ++i) Ui[(s8 + i) + (s8 + c) * kLdS] = x[i];
       }
-    } else if (sb >= 2) {
-      // meanwhile the other warps form the off-diagonal inverse blocks of
-      // block row / column sb - 1, whose inputs are all final
-      spec_inverse_blocks<T>(A, Li, Ui, sb - 1, t - 32);
     }
     __syncthreads();
+    // (B) block column sb of L (X U_ss = A_rs, back substitution with the
+    // pivots' reciprocals) and block row sb of U (L_ss Y = A_sc, forward
+    // substitution with the unit lower triangle)
     const int rest = 56 - s8;   // rows / columns after this block
-    if (t < rest) {             // L block column: row s8+8+t times inv(U_ss)
+    if (t < rest) {
       const int r = s8 + 8 + t;
-      T a[8], o[8];
-#pragma unroll
-      for (int k = 0; k < 8; ++k) a[k] = A[r + (s8 + k) * kLdS];
+      T x[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
-        T v = T(0);
+        T v = A[r + (s8 + q) * kLdS];
 #pragma unroll
-        for (int k = 0; k <= q; ++k) v += a[k] * Ui[(s8 + k) + (s8 + q) * kLdS];
-        o[q] = v;
-        if (r < seg[s8 + q] && absd(v) > 1.0) violated = true;
+        for (int k = 0; k < q; ++k) v -= x[k] * A[(s8 + k) + (s8 + q) * kLdS];
+        x[q] = v * rdiag[s8 + q];
+        if (r < seg[s8 + q] && absd(x[q]) > 1.0) violated = true;
       }
 #pragma unroll
-      for (int q = 0; q < 8; ++q) A[r + (s8 + q) * kLdS] = o[q];
-    } else if (t >= 64 && t < 64 + rest) {   // U block row: inv(L_ss) times column s8+8+(t-64)
+      for (int q = 0; q < 8; ++q) A[r + (s8 + q) * kLdS] = x[q];
+    } else if (t >= 64 && t < 64 + rest) {
       const int c = s8 + 8 + (t - 64);
-      T a[8], o[8];
-#pragma unroll
-      for (int k = 0; k < 8; ++k) a[k] = A[(s8 + k) + c * kLdS];
+      T y[8];
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
-        T v = a[i];
+        T v = A[(s8 + i) + c * kLdS];
 #pragma unroll
-        for (int k = 0; k < i; ++k) v += Li[(s8 + i) + (s8 + k) * kLdS] * a[k];
-        o[i] = v;
+        for (int k = 0; k < i; ++k) v -= A[(s8 + i) + (s8 + k) * kLdS] * y[k];
+        y[i] = v;
       }
 #pragma unroll
-      for (int i = 0; i < 8; ++i) A[(s8 + i) + c * kLdS] = o[i];
+      for (int i = 0; i < 8; ++i) A[(s8 + i) + c * kLdS] = y[i];
     }
     __syncthreads();
-    const FastDiv drest((uint32_t)(rest > 0 ? rest : 1));
-    for (int e = t; e < rest * rest; e += kSpecThreads) {   // trailing update
-      const int q = (int)drest.div(e), r = s8 + 8 + e - q * rest, c = s8 + 8 + q;
-      T v = A[r + c * kLdS];
+    // (C) this step's update of block column and block row sb + 1 only
+    // (what the next diagonal block and its L column / U row read); the
+    // rest of the update runs in (A) of the next step
+    if (rest > 0) {
+      const int b8 = s8 + 8, n1 = rest * 8, n2 = 8 * (rest - 8);
+      const FastDiv drest((uint32_t)rest);
+      for (int e = t; e < n1 + n2; e += kSpecThreads) {
+        int r, c;
+        if (e < n1) {
+          const int q = (int)drest.div(e);
+          r = b8 + e - q * rest;
+          c = b8 + q;
+        } else {
+          const int e2 = e - n1;
+          r = b8 + (e2 & 7);
+          c = b8 + 8 + (e2 >> 3);
+        }
+        T v = A[r + c * kLdS];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) v -= A[r + (s8 + k) * kLdS] * A[(s8 + k) + c * kLdS];
-      A[r + c * kLdS] = v;
+        for (int k = 0; k < 8; ++k) v -= A[r + (s8 + k) * kLdS] * A[(s8 + k) + c * kLdS];
+        A[r + c * kLdS] = v;
+      }
     }
     __syncthreads();
   }
-  // the last block row of inv(L) and block column of inv(U)
+  // the inverses' remaining blocks: diagonal block 7 and block row / column
+  // 6, then block row / column 7
+  if (warp == 1) spec_diag_inverses<T>(A, Li, Ui, 7, lane);
+  else if (warp >= 2) spec_inverse_blocks<T>(A, Li, Ui, 6, t - 64);
+  __syncthreads();
   spec_inverse_blocks<T>(A, Li, Ui, 7, t);
   __syncthreads();
   if (violated) bad = 1;
