@@ -614,16 +614,35 @@ __global__ void k_solve_finish(int64_t n, int64_t nrhs, const int32_t* __restric
 }
 
 // r = b - A * x with the unscaled A in CSR (interface.jl:173), FP64.
+constexpr int kResidualCols = 8;
+inline dim3 grid_residual(int64_t n, int64_t nrhs) {
+  return grid_rows_cols(n, (nrhs + kResidualCols - 1) / kResidualCols);
+}
 __global__ void k_residual(int64_t n, int64_t nrhs, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                            const int32_t* __restrict__ src, const double* __restrict__ ax,
                            const double* __restrict__ b, int64_t ldb, const double* __restrict__ x, int64_t ldx,
                            double* __restrict__ r, int64_t ldr) {
+  // kResidualCols right-hand sides per thread (blockIdx.y: groups of them):
+  // the row's entries are read once for all of them; each column's sum runs
+  // over the row in the same order
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  for (int64_t c = blockIdx.y; c < nrhs; c += gridDim.y) {
-    double acc = 0.0;
-    for (int p = rp[i]; p < rp[i + 1]; ++p) acc += ax[src[p]] * x[ci[p] + c * ldx];
-    r[i + c * ldr] = b[i + c * ldb] - acc;
+  const int p0 = rp[i], p1 = rp[i + 1];
+  for (int64_t c0 = (int64_t)blockIdx.y * kResidualCols; c0 < nrhs; c0 += (int64_t)gridDim.y * kResidualCols) {
+    const int cc = (int)(nrhs - c0 < kResidualCols ? nrhs - c0 : kResidualCols);
+    double acc[kResidualCols];
+#pragma unroll
+    for (int j = 0; j < kResidualCols; ++j) acc[j] = 0.0;
+    for (int p = p0; p < p1; ++p) {
+      const double a = ax[src[p]];
+      const double* xp = x + ci[p] + c0 * ldx;
+#pragma unroll
+      for (int j = 0; j < kResidualCols; ++j)
+        if (j < cc) acc[j] += a * xp[j * ldx];
+    }
+#pragma unroll
+    for (int j = 0; j < kResidualCols; ++j)
+      if (j < cc) r[i + (c0 + j) * ldr] = b[i + (c0 + j) * ldb] - acc[j];
   }
 }
 

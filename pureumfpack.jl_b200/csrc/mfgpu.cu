@@ -1603,7 +1603,7 @@ void solve_refine(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide
                                                             h->b_csr_col.as<int32_t>(), h->b_csr_src.as<int32_t>(),
                                                             h->b_ax.as<zc>(), d_b, ldb, d_x, ldx, r, P.n);
         else
-          k_residual<<<grid_rows_cols(P.n, R), 256, 0, st>>>(P.n, R, h->b_csr_ptr.as<int32_t>(),
+          k_residual<<<grid_residual(P.n, R), 256, 0, st>>>(P.n, R, h->b_csr_ptr.as<int32_t>(),
                                                           h->b_csr_col.as<int32_t>(), h->b_csr_src.as<int32_t>(),
                                                           h->b_ax.as<double>(), d_b, ldb, d_x, ldx, r, P.n);
       });
@@ -2216,7 +2216,7 @@ int mfgpu_backward_error_device(mfgpu_ctx* h, int64_t nrhs, const double* d_b, i
     h->b_norm.ensure(16);
     CK(cudaMemsetAsync(h->b_err.p, 0, nrhs * 3 * 8, st));
     CK(cudaMemsetAsync(h->b_norm.p, 0, 8, st));
-    k_residual<<<grid_rows_cols(n, nrhs), 256, 0, st>>>(n, nrhs, h->b_csr_ptr.as<int32_t>(), h->b_csr_col.as<int32_t>(),
+    k_residual<<<grid_residual(n, nrhs), 256, 0, st>>>(n, nrhs, h->b_csr_ptr.as<int32_t>(), h->b_csr_col.as<int32_t>(),
                                                      h->b_csr_src.as<int32_t>(), h->b_ax.as<double>(), d_b, ldb, d_x,
                                                      ldx, h->b_r.as<double>(), n);
     k_bwd_error_parts<<<dim3((unsigned)((n + 255) / 256), (unsigned)std::min<int64_t>(nrhs, 65535)), 256, 0, st>>>(
