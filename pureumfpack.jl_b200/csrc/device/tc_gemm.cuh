@@ -825,45 +825,42 @@ __global__ void __launch_bounds__(kBxpThreads, 1)
     tc_commit(&done);
   }
   __syncwarp();
+  // warp w owns TMEM lanes 32 (w % 4) .. (rows) at columns 32 (w / 4) ..;
+  // its C (or D) values are loaded while the MMAs still run: C is neither
+  // read nor written by this CTA's K loop
+  float* C = pc + tk.c;
+  const int q = warp & 3, c0 = (warp >> 2) * 32;
+  const int row = m0 + q * 32 + lane;
+  const float* D = tk.mode == kGemmFrom ? pc + tk.d : C;
+  const int ldD = tk.mode == kGemmFrom ? tk.ldd : tk.ldc;
+  const bool ld = tk.mode == kGemmSub || tk.mode == kGemmFrom;
+  const float sgn = tk.mode == kGemmSet ? -1.0f : 1.0f;
+  float cv[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const int col = n0 + c0 + j;
+    cv[j] = (ld && row < M && col < N) ? D[(int64_t)row + (int64_t)col * ldD] : 0.0f;
+  }
   tc_wait_done(&done, wait_ns, &failed);
   __syncthreads();
   const bool ok = !failed;
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (ok) {
-    // warp w reads TMEM lanes 32 (w % 4) .. (rows) at columns 32 (w / 4) ..
-    float* C = pc + tk.c;
-    const int q = warp & 3, c0 = (warp >> 2) * 32;
-    const int row = m0 + q * 32 + lane;
-    const float* D = tk.mode == kGemmFrom ? pc + tk.d : C;
-    const int ldD = tk.mode == kGemmFrom ? tk.ldd : tk.ldc;
-    const bool ld = tk.mode == kGemmSub || tk.mode == kGemmFrom;
-    const float sgn = tk.mode == kGemmSet ? -1.0f : 1.0f;
     const int nacc = nk < Cfg::kAccs ? nk : Cfg::kAccs;
-    {
-      uint32_t v[32];
-      float acc[32];
+    uint32_t v[32];
+    float acc[32];
 #pragma unroll
-      for (int j = 0; j < 32; ++j) acc[j] = 0.0f;
-      for (int b = 0; b < nacc; ++b) {
-        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + c0), v);
+    for (int j = 0; j < 32; ++j) acc[j] = 0.0f;
+    for (int b = 0; b < nacc; ++b) {
+      tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + c0), v);
 #pragma unroll
-        for (int j = 0; j < 32; ++j) acc[j] += __uint_as_float(v[j]);
-      }
-      if (row < M) {
+      for (int j = 0; j < 32; ++j) acc[j] += __uint_as_float(v[j]);
+    }
+    if (row < M) {
 #pragma unroll
-        for (int g = 0; g < 32; g += 8) {
-          float cv[8];
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const int col = n0 + c0 + g + j;
-            cv[j] = (ld && col < N) ? D[(int64_t)row + (int64_t)col * ldD] : 0.0f;
-          }
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const int col = n0 + c0 + g + j;
-            if (col < N) C[(int64_t)row + (int64_t)col * tk.ldc] = cv[j] - sgn * acc[g + j];
-          }
-        }
+      for (int j = 0; j < 32; ++j) {
+        const int col = n0 + c0 + j;
+        if (col < N) C[(int64_t)row + (int64_t)col * tk.ldc] = cv[j] - sgn * acc[j];
       }
     }
   } else if (t == 0) {
