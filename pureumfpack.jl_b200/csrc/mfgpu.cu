@@ -607,7 +607,7 @@ bool tc_worthwhile(double flops, int64_t tiles_tc) {
 // tiles walk K of at least kSplitPlanesMinK on average: a tile's epilogue
 // and set-up are then small beside its K loop, and the split is shared by
 // the tiles of a row (column).  Shorter K stays on k_gemm_bx3.
-constexpr double kSplitPlanesMinK = 192;
+constexpr double kSplitPlanesMinK = 128;
 bool split_worthwhile(const Launch& L) {
   return L.tiles_tc > 0 && L.flops >= 2.0 * kTcTile * kTcTile * kSplitPlanesMinK * (double)L.tiles_tc;
 }
