@@ -48,11 +48,17 @@ struct SolveArgs {
 // while its rows are read in factor order; the fronts then read their pivot
 // rows of c contiguously.  Each factor row is read by its own supernode only,
 // before that supernode writes the same rows of x, so c lives in x's storage.
-// The element kernels below run on a (row blocks, right-hand sides) grid:
-// row k = blockIdx.x * blockDim.x + threadIdx.x, columns blockIdx.y,
-// blockIdx.y + gridDim.y, ... (no 64-bit division per element).
+// The element kernels below run on a (row blocks, right-hand-side groups)
+// grid: row k = blockIdx.x * blockDim.x + threadIdx.x, column groups
+// blockIdx.y, blockIdx.y + gridDim.y, ... (no 64-bit division per element);
+// k_rhs_factor_order and k_solve_finish take kElemCols right-hand sides per
+// thread, so a row's permutation and scaling are read once for all of them.
 inline dim3 grid_rows_cols(int64_t n, int64_t nrhs, int threads = 256) {
   return dim3((unsigned)((n + threads - 1) / threads), (unsigned)(nrhs < 65535 ? (nrhs > 0 ? nrhs : 1) : 65535));
+}
+constexpr int kElemCols = 8;
+inline dim3 grid_rows_groups(int64_t n, int64_t nrhs) {
+  return grid_rows_cols(n, (nrhs + kElemCols - 1) / kElemCols);
 }
 
 template <typename T>
@@ -63,9 +69,15 @@ __global__ void k_rhs_factor_order(int64_t n, int64_t nrhs, const Wide<T>* __res
   if (k >= n) return;
   const int orow = qf[prow[k]];
   const double r = rs ? rs[orow] : 1.0;
-  for (int64_t c = blockIdx.y; c < nrhs; c += gridDim.y) {
-    const Wide<T> v = b[orow + c * ldb];
-    bfo[k + c * ldo] = (T)(rs ? Wide<T>(r) * v : v);
+  for (int64_t c0 = (int64_t)blockIdx.y * kElemCols; c0 < nrhs; c0 += (int64_t)gridDim.y * kElemCols) {
+    const int cc = (int)(nrhs - c0 < kElemCols ? nrhs - c0 : kElemCols);
+    Wide<T> v[kElemCols];
+#pragma unroll
+    for (int j = 0; j < kElemCols; ++j)
+      if (j < cc) v[j] = b[orow + (c0 + j) * ldb];
+#pragma unroll
+    for (int j = 0; j < kElemCols; ++j)
+      if (j < cc) bfo[k + (c0 + j) * ldo] = (T)(rs ? Wide<T>(r) * v[j] : v[j]);
   }
 }
 
@@ -606,10 +618,18 @@ __global__ void k_solve_finish(int64_t n, int64_t nrhs, const int32_t* __restric
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const int q = qf[k];
-  for (int64_t c = blockIdx.y; c < nrhs; c += gridDim.y) {
-    const Wide<T> v = (Wide<T>)xw[k + c * ldw];
-    Wide<T>* dst = x + q + c * ldx;
-    *dst = accumulate ? *dst + v : v;
+  for (int64_t c0 = (int64_t)blockIdx.y * kElemCols; c0 < nrhs; c0 += (int64_t)gridDim.y * kElemCols) {
+    const int cc = (int)(nrhs - c0 < kElemCols ? nrhs - c0 : kElemCols);
+    Wide<T> v[kElemCols], o[kElemCols];
+#pragma unroll
+    for (int j = 0; j < kElemCols; ++j)
+      if (j < cc) {
+        v[j] = (Wide<T>)xw[k + (c0 + j) * ldw];
+        o[j] = accumulate ? x[q + (c0 + j) * ldx] : Wide<T>(0.0);
+      }
+#pragma unroll
+    for (int j = 0; j < kElemCols; ++j)
+      if (j < cc) x[q + (c0 + j) * ldx] = accumulate ? o[j] + v[j] : v[j];
   }
 }
 

@@ -1422,7 +1422,7 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
   SolveArgs A{R, reinterpret_cast<const double*>(d_b), ldb, (use_rs && h->have_rs) ? h->b_rs.as<double>() : nullptr,
               P.n, xw};
   klaunch(h, KC_FWD_ASSEMBLE, 0, (double)P.n * R * (16.0 + sizeof(T)), [&] {
-    k_rhs_factor_order<T><<<grid_rows_cols(P.n, R), 256, 0, st>>>(P.n, R, d_b, ldb, A.rs, h->b_qf.as<int32_t>(),
+    k_rhs_factor_order<T><<<grid_rows_groups(P.n, R), 256, 0, st>>>(P.n, R, d_b, ldb, A.rs, h->b_qf.as<int32_t>(),
                                                               h->b_prow.as<int32_t>(), xw, P.n);
   });
   const unsigned ychunks = (unsigned)((R + solve_cols<T>() - 1) / solve_cols<T>());
@@ -1579,7 +1579,7 @@ void solve_once(mfgpu_ctx* h, int64_t R, const Wide<T>* d_b, int64_t ldb, Wide<T
   fork.join();
   }
   klaunch(h, KC_SOLVE_FINISH, 0, (double)P.n * R * (sizeof(T) + sizeof(Wide<T>) * (1.0 + accumulate)), [&] {
-    k_solve_finish<T><<<grid_rows_cols(P.n, R), 256, 0, st>>>(P.n, R, h->b_qf.as<int32_t>(), xw, P.n, d_x, ldx,
+    k_solve_finish<T><<<grid_rows_groups(P.n, R), 256, 0, st>>>(P.n, R, h->b_qf.as<int32_t>(), xw, P.n, d_x, ldx,
                                                            accumulate);
   });
   CK(cudaGetLastError());
