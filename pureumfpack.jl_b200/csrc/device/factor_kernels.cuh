@@ -912,21 +912,35 @@ __global__ void __launch_bounds__(kApplyThreads) k_panel_apply(DevPlan P, DevSta
 
 // _pivot_rows: prow[c1+a] = V-row at block position a after the block's
 // sequential interchanges; rowfac = inverse of prow.
+// One warp per supernode: the identity and the inverse in parallel; the
+// interchanges in their sequential order, visiting only the positions that
+// swap (found 32 at a time by ballot; none after speculative panels).
 __global__ void k_finalize_pivots(DevPlan P, DevState S) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= P.ns) return;
+  const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (s >= P.ns) return;   // warp-uniform
+  const int lane = lane_id();
   const int c1 = P.c1[s], np = P.np[s];
   int32_t* pr = S.prow + c1;
-  for (int a = 0; a < np; ++a) pr[a] = c1 + a;
-  for (int a = 0; a < np; ++a) {
-    const int p = S.ipiv[c1 + a];
-    if (p != a) {
-      const int32_t t = pr[a];
-      pr[a] = pr[p];
-      pr[p] = t;
+  for (int a = lane; a < np; a += 32) pr[a] = c1 + a;
+  __syncwarp();
+  for (int base = 0; base < np; base += 32) {
+    const int a = base + lane;
+    const int p = a < np ? S.ipiv[c1 + a] : a;
+    unsigned mask = __ballot_sync(0xffffffffu, a < np && p != a);
+    while (mask) {
+      const int j = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const int pj = __shfl_sync(0xffffffffu, p, j);
+      if (lane == 0) {
+        const int32_t t = pr[base + j];
+        pr[base + j] = pr[pj];
+        pr[pj] = t;
+      }
+      __syncwarp();
     }
   }
-  for (int a = 0; a < np; ++a) S.rowfac[pr[a]] = c1 + a;
+  __syncwarp();
+  for (int a = lane; a < np; a += 32) S.rowfac[pr[a]] = c1 + a;
 }
 
 // Direct CSC scatter; row indices are written 1-based (Julia's convention).

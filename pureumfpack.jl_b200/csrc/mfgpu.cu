@@ -857,7 +857,7 @@ void issue_factor(mfgpu_ctx* h) {
   run_factor_launches<T>(h);
   issue_inverses<T>(h);
   if (P.ns)
-    klaunch(h, KC_PIVOTS, 0, 16.0 * P.n, [&] { k_finalize_pivots<<<grid1(P.ns, 128), 128, 0, st>>>(h->dp, dev_state(h)); });
+    klaunch(h, KC_PIVOTS, 0, 16.0 * P.n, [&] { k_finalize_pivots<<<grid1(P.ns * 32, 128), 128, 0, st>>>(h->dp, dev_state(h)); });
   if (P.fc_total)
     klaunch(h, KC_SCATTER, 0, (double)(P.nnz_l + P.nnz_u) * (8.0 + sizeof(Wide<T>) + sizeof(T)), [&] {
       if (P.merged)
