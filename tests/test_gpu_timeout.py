@@ -1,8 +1,9 @@
 """Bounded device waits: a wait that runs out is a status, not a hang.
 
-The tensor-core GEMMs of the FP32 fronts synchronise their warps through
-mbarriers, and the persistent solve synchronises its CTAs through a grid
-barrier; every one of these waits is bounded by the handle's wait limit
+The tensor-core GEMMs of the FP32 fronts (register-staged and bulk-copy
+forms) synchronise their warps through mbarriers, and the persistent solve
+synchronises its CTAs through a grid barrier; every one of these waits is
+bounded by the handle's wait limit
 (mfgpu_set_wait_limit, 4 s by default).  The test hook mfgpu_test_stall makes
 a wait that can never complete -- the GEMMs' MMA issuer waits on an mbarrier
 that nothing arrives at, CTA 0 of the persistent solve never arrives at its
@@ -30,8 +31,12 @@ MFGPU_ERR_TIMEOUT = -5
 MFGPU_ERR_STATE = -4
 
 
-def test_tensor_core_wait_runs_out_and_the_handle_recovers():
-    A = M.poisson3d(20)
+@pytest.mark.parametrize("k", [20, 40], ids=["poisson3d-20", "poisson3d-40"])
+def test_tensor_core_wait_runs_out_and_the_handle_recovers(k):
+    # poisson3d-40 has long-K Schur updates, so the bulk-copy GEMM
+    # (k_gemm_bx3p) gives up its waits too: its producer lets the copies in
+    # flight land before the CTA ends
+    A = M.poisson3d(k)
     S = symbolic_mf(A)
     Rs = row_scaling(A, 1)
     b = M.rhs(A.n, seed=6)
