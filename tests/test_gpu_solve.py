@@ -11,7 +11,7 @@ import pytest
 
 from helpers import backward_error
 from oracle import oracle as O
-from pureumfpack import SCALE_MAX, SCALE_NONE, SCALE_SUM, multifrontal_lu, solve, splu
+from pureumfpack import PRECISION_FP64, PRECISION_MIXED, SCALE_MAX, SCALE_NONE, SCALE_SUM, multifrontal_lu, solve, splu
 from pureumfpack import matrices as M
 
 pytestmark = pytest.mark.gpu
@@ -69,6 +69,30 @@ def test_multiple_rhs_equal_per_column(nrhs):
         xc = solve(F, np.ascontiguousarray(B[:, c]), refine=1)
         assert np.linalg.norm(X[:, c] - xc) <= 1e-13 * np.linalg.norm(xc)
     assert backward_error(A, X, B) <= 1e-14
+
+
+@pytest.mark.parametrize("precision,refine", [(PRECISION_FP64, 0), (PRECISION_MIXED, 2)], ids=["fp64", "mixed"])
+def test_many_rhs_large_fronts_match_oracle(precision, refine):
+    # Many right-hand sides on fronts with hundreds of pivots: the solve runs
+    # its row-parallel pull assembly and gather, K-chunked top-level products
+    # with their fold, the thin-supernode and leaf kernels and the few-row
+    # product tiles, and the mixed form's factorization the bulk-copy GEMM;
+    # the solutions must agree with the oracle's solve(F, B; refine)
+    # (src/interface.jl:170-177) and reach the accuracy target.
+    from pureumfpack import GpuContext, row_scaling, symbolic_mf
+
+    A = M.poisson3d(28)
+    B = M.rhs(A.n, seed=9, nrhs=96)
+    S = symbolic_mf(A)
+    Rs = row_scaling(A, 1)
+    ctx = GpuContext(device=0, precision=precision)
+    ctx.analyze(A, S)
+    assert ctx.factor(A.nzval, Rs, True) == 0
+    X = ctx.solve(B, refine)
+    Xo = O.solve(O.splu(A), B, refine=max(refine, 1))
+    assert np.linalg.norm(X - Xo) <= 1e-10 * np.linalg.norm(Xo)
+    assert backward_error(A, X, B) <= 1e-14
+    np.testing.assert_array_equal(ctx.solve(B, refine), X)   # deterministic: the same bits again
 
 
 def test_refinement_does_not_degrade():
