@@ -9,6 +9,7 @@
 //   AMD / COLAMD ordering  src/amd.jl:13-539   (CSparse cs_amd, order=1)
 //   symbolic analysis      src/symbolic.jl:15-237
 //   numeric multifrontal   src/multifrontal.jl:45-375
+//   Gilbert-Peierls LU     src/gplu.jl:62-303 (the method splu uses by default)
 //   CSC triangular solves  src/solve.jl:10-39
 //   solve + refinement     src/interface.jl:123-177
 // The dense front kernels (getrf / trsm / gemm) are the same LAPACK/BLAS calls
@@ -966,6 +967,150 @@ void usolve(const FT& F, T* y) {
   }
 }
 
+// ---- Gilbert-Peierls left-looking LU (gplu.jl:62-303) ----------------------
+// Depth-first search from row j0 in the graph of the partial L (edge j -> i
+// when row j is a pivot, J = pinv[j], and row i is stored in L's column J);
+// finished rows go to xi[--top], so xi[top..n) is a topological order
+// (gplu.jl:70-102).
+i64 gp_dfs(i64 j0, const vector<i64>& Lp, const vector<i64>& Li, const vector<i64>& pinv, i64 top,
+           vector<i64>& xi, vector<i64>& stack, vector<i64>& pstack, vector<char>& marked) {
+  i64 head = 0;
+  stack[0] = j0;
+  while (head >= 0) {
+    i64 j = stack[head];
+    i64 J = pinv[j];
+    if (!marked[j]) {
+      marked[j] = 1;
+      pstack[head] = J >= 0 ? Lp[J] : 0;
+    }
+    bool done = true;
+    if (J >= 0) {
+      for (i64 p = pstack[head]; p < Lp[J + 1]; ++p) {
+        i64 i = Li[p];
+        if (!marked[i]) {
+          pstack[head] = p;
+          stack[++head] = i;
+          done = false;
+          break;
+        }
+      }
+    }
+    if (done) {
+      --head;
+      xi[--top] = j;
+    }
+  }
+  return top;
+}
+
+// The reach of A(:, col) in the graph of L, in the order of A's stored rows
+// (gplu.jl:106-122); leaves marked all clear.
+i64 gp_reach(const vector<i64>& Lp, const vector<i64>& Li, const i64* cp, const i64* ri, i64 col,
+             const vector<i64>& pinv, vector<i64>& xi, vector<i64>& stack, vector<i64>& pstack,
+             vector<char>& marked, i64 n) {
+  i64 top = n;
+  for (i64 p = cp[col]; p < cp[col + 1]; ++p)
+    if (!marked[ri[p]]) top = gp_dfs(ri[p], Lp, Li, pinv, top, xi, stack, pstack, marked);
+  for (i64 p = top; p < n; ++p) marked[xi[p]] = 0;
+  return top;
+}
+
+// Sort each column's (row, value) pairs by row (gplu.jl:383-415: the keys of a
+// column are distinct, so any sort gives this order).
+void gp_sortcols(i64 n, const vector<i64>& cp, vector<i64>& ri, vector<double>& x) {
+  vector<std::pair<i64, double>> tmp;
+  for (i64 j = 0; j < n; ++j) {
+    tmp.clear();
+    for (i64 p = cp[j]; p < cp[j + 1]; ++p) tmp.emplace_back(ri[p], x[p]);
+    std::sort(tmp.begin(), tmp.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    for (i64 p = cp[j]; p < cp[j + 1]; ++p) {
+      ri[p] = tmp[p - cp[j]].first;
+      x[p] = tmp[p - cp[j]].second;
+    }
+  }
+}
+
+// gplu(A; q, tol, check, sort_factors) (gplu.jl:173-303), 0-based.  Returns 0,
+// or -1 when the pivot rows do not form a permutation (a singular matrix
+// factored with check = false: the reference's invperm throws there);
+// F.status = k (1-based) when check is set and column k has no nonzero pivot.
+int gplu0(i64 n, const i64* cp, const i64* ri, const double* ax, const vector<i64>& q, double tol, bool check,
+          bool sort_factors, Factor& F) {
+  F = Factor();
+  F.n = n;
+  vector<double> x(n, 0.0);
+  vector<i64> xi(n), stack(n), pstack(n), pinv(n, -1);
+  vector<char> marked(n, 0);
+  F.Lp.assign(n + 1, 0);
+  F.Up.assign(n + 1, 0);
+  for (i64 k = 0; k < n; ++k) {
+    i64 col = q[k];
+    i64 top = gp_reach(F.Lp, F.Li, cp, ri, col, pinv, xi, stack, pstack, marked, n);
+    for (i64 p = top; p < n; ++p) x[xi[p]] = 0.0;
+    for (i64 p = cp[col]; p < cp[col + 1]; ++p) x[ri[p]] = ax[p];
+    for (i64 px = top; px < n; ++px) {   // L x = A(:, col), unit diagonal stored first
+      i64 j = xi[px], J = pinv[j];
+      if (J < 0) continue;
+      double xj = x[j];
+      for (i64 p = F.Lp[J] + 1; p < F.Lp[J + 1]; ++p) x[F.Li[p]] -= F.Lx[p] * xj;
+    }
+    i64 ipiv = -1;
+    double a = -1.0;
+    for (i64 px = top; px < n; ++px) {   // U entries in reach order; largest unpivoted row
+      i64 i = xi[px];
+      if (pinv[i] < 0) {
+        double t = std::fabs(x[i]);
+        if (t > a) {
+          a = t;
+          ipiv = i;
+        }
+      } else {
+        F.Ui.push_back(pinv[i]);
+        F.Ux.push_back(x[i]);
+      }
+    }
+    if (ipiv < 0 || a <= 0) {
+      if (check) {
+        F.status = k + 1;
+        return 0;
+      }
+      if (ipiv < 0) ipiv = col;
+    }
+    if (pinv[col] < 0 && std::fabs(x[col]) >= tol * a) ipiv = col;
+    double pivot = x[ipiv];
+    F.Ui.push_back(k);
+    F.Ux.push_back(pivot);
+    F.Up[k + 1] = (i64)F.Ui.size();
+    pinv[ipiv] = k;
+    F.Li.push_back(ipiv);
+    F.Lx.push_back(1.0);
+    for (i64 px = top; px < n; ++px) {
+      i64 i = xi[px];
+      if (pinv[i] < 0) {
+        F.Li.push_back(i);
+        F.Lx.push_back(x[i] / pivot);
+      }
+      x[i] = 0.0;
+    }
+    F.Lp[k + 1] = (i64)F.Li.size();
+  }
+  vector<char> seen(n, 0);
+  for (i64 i = 0; i < n; ++i) {
+    if (pinv[i] < 0 || seen[pinv[i]]) return -1;
+    seen[pinv[i]] = 1;
+  }
+  for (auto& r : F.Li) r = pinv[r];
+  if (sort_factors) {
+    gp_sortcols(n, F.Lp, F.Li, F.Lx);
+    gp_sortcols(n, F.Up, F.Ui, F.Ux);
+  }
+  F.q = q;
+  F.pinv = pinv;
+  F.p.assign(n, 0);
+  for (i64 i = 0; i < n; ++i) F.p[pinv[i]] = i;
+  return 0;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1115,6 +1260,22 @@ void* orc_numeric(void* sym, const double* nzval, const i64* colptr, const i64* 
   *status = rc < 0 ? rc : F->status;
   return F;
 }
+// gplu(A; q, tol, check, sort_factors) (gplu.jl:173-303): q1 1-based or NULL
+// for the natural order.  *status as orc_multifrontal_lu (k > 0: no nonzero
+// pivot at column k under check; -1: the pivot rows are not a permutation).
+void* orc_gplu(i64 n, const i64* colptr, const i64* rowval, const double* nzval, const i64* q1, double tol,
+               int check, int sort_factors, i64* status) {
+  vector<i64> cp, ri;
+  to0(n, colptr, rowval, cp, ri);
+  vector<i64> q(n);
+  for (i64 k = 0; k < n; ++k) q[k] = q1 ? q1[k] - 1 : k;
+  Factor* F = new Factor();
+  int rc = gplu0(n, cp.data(), ri.data(), nzval, q, tol, check != 0, sort_factors != 0, *F);
+  if (rc < 0) g_err = "gplu: the pivot rows are not a permutation (singular matrix, check = false)";
+  *status = rc < 0 ? rc : F->status;
+  return F;
+}
+
 void orc_factor_free(void* h) { delete (Factor*)h; }
 void orc_factor_sizes(void* h, i64* out) {
   Factor* F = (Factor*)h;

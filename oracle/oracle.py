@@ -13,6 +13,9 @@ its 1-based Int64 index convention:
 * ``symbolic_mf``        src/symbolic.jl:211-226
 * ``multifrontal_lu``    src/multifrontal.jl:146-358
 * ``solve``              src/interface.jl:170-177 (with ``_solve_factor`` :123-138)
+* ``gplu``, ``splu_gplu`` src/gplu.jl:173-303 and splu(A; method=:gplu,
+  ordering) (src/interface.jl:93-120): Gilbert-Peierls left-looking LU with
+  threshold partial pivoting
 * ``*_f32``              the same for the reference's generic Tv = Float32: row
   scaling, the numeric phase (sgetrf / strsm / sgemm fronts) and the solve
   with its refinement, all in Float32 arithmetic
@@ -79,6 +82,9 @@ def lib():
         L.orc_multifrontal_lu.restype = ctypes.c_void_p
         L.orc_multifrontal_lu.argtypes = [ctypes.c_int64, _i64p, _i64p, _f64p, _i64p, ctypes.c_int, _i64p]
         L.orc_numeric.restype = ctypes.c_void_p
+        L.orc_gplu.restype = ctypes.c_void_p
+        L.orc_gplu.argtypes = [ctypes.c_int64, _i64p, _i64p, _f64p, _i64p, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                               _i64p]
         L.orc_numeric.argtypes = [ctypes.c_void_p, _f64p, _i64p, _i64p, ctypes.c_int, _i64p]
         L.orc_factor_free.argtypes = [ctypes.c_void_p]
         L.orc_factor_sizes.argtypes = [ctypes.c_void_p, _i64p]
@@ -272,6 +278,35 @@ def multifrontal_lu(A, q=None, check: bool = True) -> Factor:
     return _extract(h)
 
 
+def gplu(A, q=None, tol: float = 0.1, check: bool = True, sort_factors: bool = True) -> Factor:
+    """gplu(A; q, tol, check, sort_factors) (gplu.jl:173-303), A as given."""
+    if A.m != A.n:
+        raise ValueError("DimensionMismatch: gplu requires a square matrix")
+    st = np.zeros(1, np.int64)
+    qa = _i(q) if q is not None else None
+    h = lib().orc_gplu(A.n, _p(_i(A.colptr)), _p(_i(A.rowval)), _p(_f(A.nzval), _f64p), _p(qa), float(tol),
+                       int(check), int(sort_factors), _p(st))
+    if st[0] < 0:
+        lib().orc_factor_free(ctypes.c_void_p(h))
+        raise RuntimeError("oracle: " + lib().orc_last_error().decode())
+    if st[0] > 0:
+        lib().orc_factor_free(ctypes.c_void_p(h))
+        raise SingularException(int(st[0]))
+    return _extract(h)
+
+
+def gplu_order(A, ordering: str) -> np.ndarray:
+    """The column order splu(A; method=:gplu, ordering) factors in
+    (interface.jl:108-116), 1-based."""
+    if ordering == "natural":
+        return np.arange(1, A.n + 1, dtype=np.int64)
+    if ordering == "amd":
+        return amd_order_sym(A)
+    if ordering == "colamd":
+        return colamd_order(A)
+    raise ValueError(f"ArgumentError: unknown ordering {ordering}")
+
+
 def numeric(S: Symbolic, A, check: bool = True) -> Factor:
     """Numeric phase only, on a precomputed symbolic object."""
     st = np.zeros(1, np.int64)
@@ -304,6 +339,16 @@ def splu(A, scale: int = SCALE_SUM, check: bool = True, q=None) -> PureLU:
     As = A if scale == SCALE_NONE else apply_row_scaling(A, Rs)
     F = multifrontal_lu(As, q=q, check=check)
     return PureLU(F, Rs, A)
+
+
+def splu_gplu(A, ordering: str = "amd", tol: float = 0.1, scale: int = SCALE_SUM, check: bool = True) -> PureLU:
+    """splu(A; method=:gplu, ordering, tol, scale, check) (interface.jl:93-120)."""
+    if A.m != A.n:
+        raise ValueError("DimensionMismatch: splu requires a square matrix")
+    Rs = row_scaling(A, scale)
+    As = A if scale == SCALE_NONE else apply_row_scaling(A, Rs)
+    q = gplu_order(A, ordering)
+    return PureLU(gplu(As, q=q, tol=tol, check=check), Rs, A)
 
 
 def solve(F: PureLU, b: np.ndarray, refine: int = 0) -> np.ndarray:
