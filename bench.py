@@ -77,6 +77,9 @@ def parse():
     ap.add_argument("--dtype", default="float64", choices=["float64", "float32"],
                     help="float32: the workload as a Float32 matrix through the Float32 C ABI (a side line, "
                          "not the headline metric)")
+    ap.add_argument("--method", default="multifrontal", choices=["multifrontal", "gplu"],
+                    help="gplu: splu(A; method=:gplu) (Gilbert-Peierls, one warp per system) on --workload "
+                         "poisson2d-100 (default for this method) or batch-N")
     ap.add_argument("--no-autotune", action="store_true",
                     help="mixed form: keep the built-in GEMM variant rule instead of the learned autotuner")
     return ap.parse_args()
@@ -583,8 +586,87 @@ def run_f32(args):
     return 0
 
 
+def run_gplu(args):
+    """splu(A; method=:gplu, ordering=:amd, tol=0.1, scale=SCALE_SUM) then
+    solve(F, b; refine=2) (src/interface.jl:93-120,170-177) on one system or
+    a batch of independent systems, with host buffers; beside it the oracle's
+    restatement of the same Gilbert-Peierls factorization and solve on the
+    host cores (one system per thread).  value = the device time of the
+    library's kernels (factor, finish, solve; CUDA events on its stream),
+    e2e = the API calls' wall time (ordering, scaling, copies included)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+
+    from oracle import oracle as O
+    from pureumfpack import SCALE_SUM, BatchGPLU
+    from pureumfpack import matrices as M
+
+    torch.cuda.set_device(0)
+    wl = args.workload if args.workload != "poisson3d-64" else "poisson2d-100"
+    if wl.startswith("batch-"):
+        sysl = M.batched_set(int(wl.split("-", 1)[1]), seed=0, nrhs=4)
+        desc = "2-D side U[16,64] / 3-D side U[8,20], shift U[0,1], 4 rhs each"
+    else:
+        A, B = make_workload(wl, 1)
+        sysl = [(A, np.asfortranarray(B.reshape(A.n, -1)))]
+        desc = f"n={A.n} nnz={A.nnz()} 1 rhs"
+    As, Bs = [a for a, _ in sysl], [b for _, b in sysl]
+    refine = 2
+    dev_ms, wall = [], []
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        F = BatchGPLU(As, ordering="amd", tol=0.1, scale=SCALE_SUM)
+        Xs = F.solve(Bs, refine=refine)
+        t1 = time.perf_counter()
+        if it >= args.warmup:
+            tm = F.ctx.timings()
+            dev_ms.append(tm["factor_ms"] + tm["finish_ms"] + tm["solve_ms"])
+            wall.append(t1 - t0)
+    tm = F.ctx.timings()
+    eta = max(_oracle_eta(A, X, B) for A, X, B in zip(As, Xs, Bs))
+    # parity: every system's factors and solution against the oracle (sampled for large batches)
+    idx = list(range(0, len(As), max(1, len(As) // 64)))
+    exact = True
+    for i in idx:
+        Fo = O.splu_gplu(As[i], ordering="amd", tol=0.1, scale=O.SCALE_SUM)
+        L, U, p, q, pinv = F.factors(i)
+        exact &= (np.array_equal(L.rowval, Fo.F.Lrowval) and np.array_equal(L.nzval, Fo.F.Lnzval)
+                  and np.array_equal(U.rowval, Fo.F.Urowval) and np.array_equal(U.nzval, Fo.F.Unzval)
+                  and np.array_equal(p, Fo.F.p) and np.array_equal(Xs[i], O.solve(Fo, Bs[i], refine=refine)))
+    cpu = None
+    if not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+
+        def one(i):
+            Fo = O.splu_gplu(As[i], ordering="amd", tol=0.1, scale=O.SCALE_SUM)
+            O.solve(Fo, Bs[i], refine=refine)
+
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=cores) as ex:
+            list(ex.map(one, range(len(As))))
+        cpu = {"value": time.perf_counter() - t0, "unit": "s", "cores": min(cores, len(As)), "kind": "port",
+               "sample": f"the oracle's splu(method=:gplu, AMD) + solve(refine={refine}) of every system, "
+                         f"one system per host thread"}
+    sec = float(np.median(dev_ms)) / 1e3
+    line = {"metric": f"{wl} splu(method=:gplu) factor+solve s", "value": sec, "unit": "s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": f"{wl}: {len(As)} system(s), {desc}, AMD, SCALE_SUM, "
+                                                        f"tol 0.1, refine {refine}"},
+            "e2e": {"value": float(np.median(wall)), "unit": "s",
+                    "h2d_bytes_per_step": int(sum(A.nnz() * 16 + A.n * 16 + B.nbytes for A, B in sysl)),
+                    "d2h_bytes_per_step": int(sum(B.nbytes for B in Bs))},
+            "kernels_ms": {"factor": tm["factor_ms"], "finish": tm["finish_ms"], "solve": tm["solve_ms"]},
+            "factor_launches": tm["factor_launches"], "reruns": tm["reruns"], "bwd_err": eta,
+            "parity": {"systems_checked": len(idx), "bitwise_equal": bool(exact)}, "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.method == "gplu":
+        return run_gplu(args)
     if args.dtype == "float32":
         return run_f32(args)
     if args.workload.startswith("batch-"):

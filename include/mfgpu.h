@@ -331,6 +331,50 @@ int mfgpu_batch_get_factors(mfgpu_ctx* h, int64_t sys, int64_t* lcolptr, int64_t
                             int64_t* pinv);
 
 /* ------------------------------------------------------------------------
+ * Gilbert-Peierls LU on the GPU: gplu(A; q, tol, check, sort_factors)
+ * (src/gplu.jl:173-303), the factorization splu(A; method=:gplu, ordering,
+ * tol, scale, check) runs by default (src/interface.jl:93-120), and the
+ * solves over its factors: F \ b (src/solve.jl:66-77) or, with row scaling
+ * and refinement, solve(F::PureLU, b; refine) (src/interface.jl:123-177).
+ * Factors, pivots and solutions are bit for bit the reference's.  One warp
+ * factors one system; a handle holds one or many independent systems.
+ * ---------------------------------------------------------------------- */
+typedef struct mfgpu_gplu mfgpu_gplu;
+int mfgpu_gplu_create(int32_t device, mfgpu_gplu** out);
+void mfgpu_gplu_destroy(mfgpu_gplu* g);
+const char* mfgpu_gplu_last_error(const mfgpu_gplu* g);
+/* Entries of L (and of U) each system gets on its first attempt; 0 (the
+ * default) sizes them from the symbolic fill of (A + A^T)[q, q].  A system
+ * that outgrows its room is factored again with three times as much. */
+int mfgpu_gplu_set_initial_capacity(mfgpu_gplu* g, int64_t entries);
+/* Factor nsys systems: system i is n[i] x n[i] (colptr[i], rowval[i],
+ * nzval[i]; rows ascending in each column) in the column order q[i]
+ * (1-based; q or q[i] NULL: natural), with its rows scaled by rs[i] (rs or
+ * rs[i] NULL: unscaled), i.e. gplu(rs[i] .* A_i; q = q[i], tol, check,
+ * sort_factors).  status[i] (may be NULL) receives 0 or, under check, the
+ * first column without a nonzero pivot (SingularException(k)).  Returns the
+ * number of singular systems when check != 0, else 0; MFGPU_ERR_ARGUMENT when
+ * a system's pivot rows are not a permutation (check = 0 on a singular
+ * matrix: the reference's invperm throws). */
+int mfgpu_gplu_factor(mfgpu_gplu* g, int64_t nsys, const int64_t* n, const int64_t* const* colptr,
+                      const int64_t* const* rowval, const double* const* nzval, const int64_t* const* q,
+                      const double* const* rs, double tol, int32_t check, int32_t sort_factors, int64_t* status);
+/* out3 = {n, nnz(L), nnz(U)} of system sys (0-based). */
+int mfgpu_gplu_sizes(mfgpu_gplu* g, int64_t sys, int64_t* out3);
+/* System sys's GPLUFactorization fields (gplu.jl:45-51), 1-based; any
+ * pointer may be NULL. */
+int mfgpu_gplu_get_factors(mfgpu_gplu* g, int64_t sys, int64_t* lcolptr, int64_t* lrowval, double* lnzval,
+                           int64_t* ucolptr, int64_t* urowval, double* unzval, int64_t* p, int64_t* q,
+                           int64_t* pinv);
+/* x[i] = solve for b[i] (n[i] x nrhs, column-major) of every system, with
+ * refine refinement steps against the unscaled A_i when the system was
+ * factored with a row scaling (PureLU), or the raw F \ b otherwise. */
+int mfgpu_gplu_solve(mfgpu_gplu* g, int64_t nrhs, const double* const* b, double* const* x, int32_t refine);
+/* {factor kernel ms (all attempts), finish kernel ms, last solve kernel ms,
+ * factor launches, systems factored again} of the last calls. */
+int mfgpu_gplu_timings(mfgpu_gplu* g, double* out5);
+
+/* ------------------------------------------------------------------------
  * Autotuner interface (no counterpart in the reference).  The batched GEMM
  * launches of the mixed form -- factor updates, pivot-block inversion, and
  * the solve products for nrhs right-hand sides, in issue order -- can each run

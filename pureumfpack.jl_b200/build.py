@@ -18,6 +18,7 @@ OUT = os.path.join(HERE, "pureumfpack", "libmfgpu.so")
 SOURCES = [
     "csrc/mfgpu.cu",
     "csrc/costmodel.cu",
+    "csrc/gplu.cu",
     "csrc/plan.cpp",
     "csrc/host/symbolic.cpp",
     "csrc/host/api_host.cpp",
@@ -31,6 +32,7 @@ DEPENDS = SOURCES + [
     "csrc/device/solve_kernels.cuh",
     "csrc/device/tc_gemm.cuh",
     "csrc/device/solve_persistent.cuh",
+    "csrc/device/gplu_kernels.cuh",
     "../include/mfgpu.h",
 ]
 NVCC_FLAGS = [

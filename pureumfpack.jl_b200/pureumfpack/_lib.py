@@ -74,6 +74,16 @@ SIGNATURES = [
     ("mfgpu_batch_solve", ctypes.c_int, [vp, i64, ctypes.POINTER(vp), ctypes.POINTER(vp), i32]),
     ("mfgpu_batch_factor_sizes", ctypes.c_int, [vp, i64, i64p]),
     ("mfgpu_batch_get_factors", ctypes.c_int, [vp, i64, i64p, i64p, f64p, i64p, i64p, f64p, i64p, i64p, i64p]),
+    ("mfgpu_gplu_create", ctypes.c_int, [i32, ctypes.POINTER(vp)]),
+    ("mfgpu_gplu_destroy", None, [vp]),
+    ("mfgpu_gplu_last_error", cp, [vp]),
+    ("mfgpu_gplu_set_initial_capacity", ctypes.c_int, [vp, i64]),
+    ("mfgpu_gplu_factor", ctypes.c_int, [vp, i64, i64p, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                         ctypes.POINTER(vp), ctypes.POINTER(vp), f64, i32, i32, i64p]),
+    ("mfgpu_gplu_sizes", ctypes.c_int, [vp, i64, i64p]),
+    ("mfgpu_gplu_get_factors", ctypes.c_int, [vp, i64, i64p, i64p, f64p, i64p, i64p, f64p, i64p, i64p, i64p]),
+    ("mfgpu_gplu_solve", ctypes.c_int, [vp, i64, ctypes.POINTER(vp), ctypes.POINTER(vp), i32]),
+    ("mfgpu_gplu_timings", ctypes.c_int, [vp, f64p]),
     ("mfgpu_tune_features", ctypes.c_int, [vp, i64, i64p, f32p, i64]),
     ("mfgpu_tune_set_choice", ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int8), i64]),
     ("mfgpu_mlp_create", ctypes.c_int, [i32, i32, i32, ctypes.c_uint64, ctypes.POINTER(vp)]),

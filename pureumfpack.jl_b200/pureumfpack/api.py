@@ -2,8 +2,10 @@
 
 Mirrors PureUMFPACK.jl (names, argument meaning, errors):
 
-* ``splu(A; method=:multifrontal, ordering, tol, scale, check)`` -> ``PureLU``
-  (src/interface.jl:93-120)
+* ``splu(A; method, ordering, tol, scale, check)`` -> ``PureLU``
+  (src/interface.jl:93-120), ``method=:multifrontal`` or ``:gplu``
+* ``gplu(A; q, tol, check, sort_factors)`` -> ``GPLUFactorization``
+  (src/gplu.jl:173-303), one warp per system on the GPU
 * ``multifrontal_lu(A; q, tol, check)`` -> ``GPLUFactorization``
   (src/multifrontal.jl:146-358)
 * ``solve(F, b; refine)`` (src/interface.jl:170-177), ``F \\ b`` as
@@ -560,10 +562,12 @@ def splu(A: SparseCSC, method: str = "gplu", ordering: str = "amd", tol: float =
          check: bool = True, device: int = 0, precision: int = PRECISION_FP64, relax: bool = False) -> PureLU:
     """splu(A; method, ordering, tol, scale, check) (src/interface.jl:93-120).
 
-    ``method="multifrontal"`` is the path this library implements; as in the
-    reference it ignores ``ordering`` and ``tol`` (AMD + postorder).  The
-    Gilbert-Peierls method (the reference's default ``method=:gplu``) is not
-    part of this library.
+    ``method="multifrontal"`` factors with the multifrontal kernels; as in
+    the reference it ignores ``ordering`` and ``tol`` (AMD + postorder).
+    ``method="gplu"`` (the reference's default) orders the columns by
+    ``ordering`` (``"amd"``, ``"colamd"`` or ``"natural"``) and runs the
+    Gilbert-Peierls factorization on the GPU with threshold ``tol``
+    (``gplu``); ``precision`` and ``relax`` apply to the multifrontal method.
     """
     method = method.lstrip(":") if isinstance(method, str) else method
     if A.m != A.n:
@@ -573,9 +577,22 @@ def splu(A: SparseCSC, method: str = "gplu", ordering: str = "amd", tol: float =
         Rs = row_scaling(A, scale)
         ctx, S = _factor(A, None, check, None if scale == SCALE_NONE else Rs, device, precision, relax)
         return PureLU(ctx, Rs, A, S)
-    if method == "gplu":
-        raise NotImplementedError("method=:gplu (Gilbert-Peierls) is outside libmfgpu; use method='multifrontal'")
-    raise ArgumentError(f"unknown method {method}")
+    if method != "gplu":
+        raise ArgumentError(f"unknown method {method}")
+    if ordering == "natural":
+        q = np.arange(1, A.n + 1, dtype=np.int64)
+    elif ordering == "amd":
+        q = amd_order_sym(A)
+    elif ordering == "colamd":
+        q = colamd_order(A)
+    else:
+        raise ArgumentError(f"unknown ordering {ordering}")
+    Rs = row_scaling(A, scale)
+    ctx = GpluContext(device)
+    st = ctx.factor([A], [q], None if scale == SCALE_NONE else [Rs], tol=tol, check=check)
+    if st[0] > 0:
+        raise SingularException(int(st[0]))
+    return PureLU(ctx, Rs, A)
 
 
 def splu_q(A: SparseCSC, q, scale=SCALE_SUM, check: bool = True, device: int = 0,
@@ -587,6 +604,154 @@ def splu_q(A: SparseCSC, q, scale=SCALE_SUM, check: bool = True, device: int = 0
     Rs = row_scaling(A, scale)
     ctx, S = _factor(A, q, check, None if scale == SCALE_NONE else Rs, device, precision)
     return PureLU(ctx, Rs, A, S)
+
+
+# ---------------------------------------------------------------------------
+# Gilbert-Peierls LU (src/gplu.jl)
+# ---------------------------------------------------------------------------
+class GpluContext:
+    """One libmfgpu Gilbert-Peierls handle: the factors of one or many
+    independent systems, resident on the GPU (one warp factors one system)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = L.lib()
+        h = ctypes.c_void_p()
+        rc = self._lib.mfgpu_gplu_create(int(device), ctypes.byref(h))
+        if rc != 0:
+            raise MfgpuError(rc, "mfgpu_gplu_create failed (needs a B200 / sm_100 device)")
+        self._h = h
+        self.n = 0
+        self.sizes = []
+
+    def _check(self, rc: int):
+        if rc < 0:
+            msg = self._lib.mfgpu_gplu_last_error(self._h).decode()
+            if rc == -1:
+                raise ArgumentError(msg)
+            if rc == -6:
+                raise DimensionMismatch(msg)
+            raise MfgpuError(rc, msg)
+        return rc
+
+    def set_initial_capacity(self, entries: int):
+        """Entries of L and of U each system gets before it first overflows
+        (0: sized from the symbolic fill)."""
+        self._check(self._lib.mfgpu_gplu_set_initial_capacity(self._h, int(entries)))
+
+    def factor(self, As, qs=None, Rs=None, tol: float = 0.1, check: bool = True,
+               sort_factors: bool = True) -> np.ndarray:
+        """gplu(Rs_i .* A_i; q = qs[i], tol, check, sort_factors) for every
+        system; returns the per-system status (0, or the singular column)."""
+        for A in As:
+            if A.m != A.n:
+                raise DimensionMismatch("gplu requires a square matrix")
+        cps = [_i(A.colptr) for A in As]
+        rvs = [_i(A.rowval) for A in As]
+        nzs = [_f(A.nzval) for A in As]
+        n = np.array([A.n for A in As], np.int64)
+        qa = None if qs is None else [_i(q) if q is not None else None for q in qs]
+        ra = None if Rs is None else [_f(r) if r is not None else None for r in Rs]
+
+        def parr(arrs):
+            if arrs is None:
+                return None
+            return (ctypes.c_void_p * len(arrs))(*[a.ctypes.data if a is not None else None for a in arrs])
+
+        status = np.zeros(len(As), np.int64)
+        self._check(self._lib.mfgpu_gplu_factor(self._h, len(As), L.ptr(n), parr(cps), parr(rvs), parr(nzs),
+                                                parr(qa), parr(ra), float(tol), int(bool(check)),
+                                                int(bool(sort_factors)), L.ptr(status)))
+        self.sizes = [A.n for A in As]
+        self.n = As[0].n if len(As) == 1 else 0
+        return status
+
+    def factors(self, sys: int = 0):
+        """(L, U, p, q, pinv) of system sys: A_i[p, q] == L * U."""
+        sz = np.empty(3, np.int64)
+        self._check(self._lib.mfgpu_gplu_sizes(self._h, int(sys), L.ptr(sz)))
+        n, nl, nu = (int(v) for v in sz)
+        Lp, Li, Lx = np.empty(n + 1, np.int64), np.empty(nl, np.int64), np.empty(nl)
+        Up, Ui, Ux = np.empty(n + 1, np.int64), np.empty(nu, np.int64), np.empty(nu)
+        p, q, pinv = np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.int64)
+        self._check(self._lib.mfgpu_gplu_get_factors(self._h, int(sys), L.ptr(Lp), L.ptr(Li), L.ptr(Lx, L.f64p),
+                                                     L.ptr(Up), L.ptr(Ui), L.ptr(Ux, L.f64p), L.ptr(p), L.ptr(q),
+                                                     L.ptr(pinv)))
+        return SparseCSC(n, n, Lp, Li, Lx), SparseCSC(n, n, Up, Ui, Ux), p, q, pinv
+
+    def solve_batch(self, Bs, refine: int = 0):
+        """x_i for every system's b_i (vectors, or n_i x k with one k)."""
+        Bs = [np.asfortranarray(b, dtype=np.float64) for b in Bs]
+        if len(Bs) != len(self.sizes):
+            raise DimensionMismatch("one right-hand side block per system")
+        k = 1 if Bs[0].ndim == 1 else Bs[0].shape[1]
+        for n, b in zip(self.sizes, Bs):
+            if b.shape[0] != n or (1 if b.ndim == 1 else b.shape[1]) != k:
+                raise DimensionMismatch("right-hand side block does not match its system")
+        Xs = [np.empty_like(b) for b in Bs]
+        self._check(self._lib.mfgpu_gplu_solve(self._h, k, L.ptr_array(Bs), L.ptr_array(Xs), int(refine)))
+        return Xs
+
+    def solve(self, b, refine: int = 0) -> np.ndarray:
+        """The single system's solve(F, b; refine); b a vector or n x k."""
+        return self.solve_batch([b], refine)[0]
+
+    def timings(self) -> dict:
+        out = np.zeros(5)
+        self._check(self._lib.mfgpu_gplu_timings(self._h, L.ptr(out, L.f64p)))
+        return {"factor_ms": out[0], "finish_ms": out[1], "solve_ms": out[2], "factor_launches": int(out[3]),
+                "reruns": int(out[4])}
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            try:
+                self._lib.mfgpu_gplu_destroy(self._h)
+            except Exception:
+                pass
+            self._h = None
+
+
+def gplu(A: SparseCSC, q=None, tol: float = 0.1, check: bool = True, sort_factors: bool = True,
+         device: int = 0) -> GPLUFactorization:
+    """gplu(A; q, tol, check, sort_factors) (src/gplu.jl:173-303) on the GPU:
+    A[p, q] == L * U with threshold partial pivoting; factors, pivots and
+    F \\ b are bit for bit the reference's."""
+    if A.m != A.n:
+        raise DimensionMismatch("gplu requires a square matrix")
+    ctx = GpluContext(device)
+    st = ctx.factor([A], None if q is None else [q], None, tol=tol, check=check, sort_factors=sort_factors)
+    if st[0] > 0:
+        raise SingularException(int(st[0]))
+    return GPLUFactorization(ctx)
+
+
+class BatchGPLU:
+    """splu(A_i; method=:gplu, ordering, tol, scale) of many independent
+    systems in one call: one warp per system, all systems side by side."""
+
+    def __init__(self, As, ordering: str = "amd", tol: float = 0.1, scale=SCALE_SUM, check: bool = True,
+                 device: int = 0, initial_capacity: int = 0):
+        self.As = list(As)
+        order = {"natural": lambda A: np.arange(1, A.n + 1, dtype=np.int64), "amd": amd_order_sym,
+                 "colamd": colamd_order}
+        if ordering not in order:
+            raise ArgumentError(f"unknown ordering {ordering}")
+        scale = ScaleKind(int(scale))
+        self.Rs = [row_scaling(A, scale) for A in self.As]
+        qs = [order[ordering](A) for A in self.As]
+        self.ctx = GpluContext(device)
+        if initial_capacity:
+            self.ctx.set_initial_capacity(initial_capacity)
+        self.status = self.ctx.factor(self.As, qs, None if scale == SCALE_NONE else self.Rs, tol=tol, check=check)
+
+    def __len__(self):
+        return len(self.As)
+
+    def solve(self, Bs, refine: int = 0):
+        return self.ctx.solve_batch(Bs, refine)
+
+    def factors(self, i: int):
+        """(L, U, p, q, pinv) of system i: (Rs_i .* A_i)[p, q] == L * U."""
+        return self.ctx.factors(i)
 
 
 # ---------------------------------------------------------------------------
