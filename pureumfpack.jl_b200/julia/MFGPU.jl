@@ -11,6 +11,7 @@
 module MFGPU
 
 using SparseArrays: SparseMatrixCSC, nonzeros, rowvals
+using LinearAlgebra: SingularException
 
 const libmfgpu = get(ENV, "PUREUMFPACK_MFGPU", joinpath(@__DIR__, "..", "pureumfpack", "libmfgpu.so"))
 
@@ -231,6 +232,83 @@ function batch_solve(h::Handle, Bs::Vector{Matrix{Float64}}; refine::Integer = 0
     GC.@preserve Bs Xs _check(h, ccall((:mfgpu_batch_solve, libmfgpu), Cint,
         (Ptr{Cvoid}, Int64, Ptr{Ptr{Float64}}, Ptr{Ptr{Float64}}, Int32),
         h.ptr, size(Bs[1], 2), Ptr{Float64}[pointer(B) for B in Bs], Ptr{Float64}[pointer(X) for X in Xs],
+        Int32(refine)))
+    return Xs
+end
+
+# --- Gilbert-Peierls LU (gplu, splu(A; method=:gplu)) on the GPU -----------
+# A separate handle type; one warp factors one system, factors and solutions
+# are bit for bit the reference's gplu / solve.  The reference's splu keeps
+# its own ordering (amd_order_sym / colamd_order) and row scaling and hands
+# q and Rs over, e.g. in src/interface.jl's :gplu branch:
+#     g = MFGPU.gplu_create(); MFGPU.gplu_factor!(g, [A], [q]; rs = [Rs], tol = tol, check = check)
+#     L, U, p, q, pinv = MFGPU.gplu_factors(g, 1)
+mutable struct GpluHandle
+    ptr::Ptr{Cvoid}
+    ns::Vector{Int}
+end
+
+function _gcheck(g::GpluHandle, rc::Cint)
+    rc >= 0 && return Int(rc)
+    msg = unsafe_string(ccall((:mfgpu_gplu_last_error, libmfgpu), Cstring, (Ptr{Cvoid},), g.ptr))
+    rc == -1 && throw(ArgumentError(msg))
+    rc == -6 && throw(DimensionMismatch(msg))
+    error("libmfgpu error $rc: $msg")
+end
+
+function gplu_create(; device::Integer = 0)
+    ptr = Ref{Ptr{Cvoid}}(C_NULL)
+    rc = ccall((:mfgpu_gplu_create, libmfgpu), Cint, (Int32, Ref{Ptr{Cvoid}}), Int32(device), ptr)
+    rc == 0 || error("mfgpu_gplu_create failed ($rc): needs a B200 / sm_100 device")
+    g = GpluHandle(ptr[], Int[])
+    finalizer(x -> ccall((:mfgpu_gplu_destroy, libmfgpu), Cvoid, (Ptr{Cvoid},), x.ptr), g)
+    return g
+end
+
+# gplu(rs[i] .* As[i]; q = qs[i], tol, check, sort_factors) for every system;
+# throws SingularException(k) for the first singular system under check.
+function gplu_factor!(g::GpluHandle, As::AbstractVector{<:SparseMatrixCSC{Float64, <:Integer}},
+                      qs::AbstractVector; rs = nothing, tol::Real = 0.1, check::Bool = true,
+                      sort_factors::Bool = true)
+    ns = Int64[size(A, 1) for A in As]
+    cols = [_i64(A.colptr) for A in As]
+    rows = [_i64(rowvals(A)) for A in As]
+    qv = [_i64(q) for q in qs]
+    status = zeros(Int64, length(As))
+    rsp = rs === nothing ? Ptr{Float64}[C_NULL for _ in As] : Ptr{Float64}[pointer(r) for r in rs]
+    GC.@preserve As cols rows qv rs _gcheck(g, ccall((:mfgpu_gplu_factor, libmfgpu), Cint,
+        (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Ptr{Int64}}, Ptr{Ptr{Int64}}, Ptr{Ptr{Float64}}, Ptr{Ptr{Int64}},
+         Ptr{Ptr{Float64}}, Float64, Int32, Int32, Ptr{Int64}),
+        g.ptr, length(As), ns, Ptr{Int64}[pointer(c) for c in cols], Ptr{Int64}[pointer(r) for r in rows],
+        Ptr{Float64}[pointer(nonzeros(A)) for A in As], Ptr{Int64}[pointer(q) for q in qv], rsp,
+        Float64(tol), Int32(check), Int32(sort_factors), status))
+    g.ns = Int.(ns)
+    k = findfirst(>(0), status)
+    k === nothing || throw(SingularException(Int(status[k])))
+    return g
+end
+
+# GPLUFactorization fields (src/gplu.jl:45-51) of system i (1-based).
+function gplu_factors(g::GpluHandle, i::Integer = 1)
+    sz = Vector{Int64}(undef, 3)
+    _gcheck(g, ccall((:mfgpu_gplu_sizes, libmfgpu), Cint, (Ptr{Cvoid}, Int64, Ptr{Int64}), g.ptr, i - 1, sz))
+    n, nl, nu = sz
+    Lp = Vector{Int64}(undef, n + 1); Li = Vector{Int64}(undef, nl); Lx = Vector{Float64}(undef, nl)
+    Up = Vector{Int64}(undef, n + 1); Ui = Vector{Int64}(undef, nu); Ux = Vector{Float64}(undef, nu)
+    p = Vector{Int64}(undef, n); q = Vector{Int64}(undef, n); pinv = Vector{Int64}(undef, n)
+    _gcheck(g, ccall((:mfgpu_gplu_get_factors, libmfgpu), Cint,
+        (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}, Ptr{Int64},
+         Ptr{Int64}, Ptr{Int64}), g.ptr, i - 1, Lp, Li, Lx, Up, Ui, Ux, p, q, pinv))
+    return SparseMatrixCSC(n, n, Lp, Li, Lx), SparseMatrixCSC(n, n, Up, Ui, Ux), p, q, pinv
+end
+
+# solve(F_i, b_i; refine) for every system (PureLU semantics when the
+# systems were factored with rs, the raw F \ b otherwise).
+function gplu_solve(g::GpluHandle, Bs::Vector{Matrix{Float64}}; refine::Integer = 0)
+    Xs = [similar(B) for B in Bs]
+    GC.@preserve Bs Xs _gcheck(g, ccall((:mfgpu_gplu_solve, libmfgpu), Cint,
+        (Ptr{Cvoid}, Int64, Ptr{Ptr{Float64}}, Ptr{Ptr{Float64}}, Int32),
+        g.ptr, size(Bs[1], 2), Ptr{Float64}[pointer(B) for B in Bs], Ptr{Float64}[pointer(X) for X in Xs],
         Int32(refine)))
     return Xs
 end
