@@ -75,40 +75,58 @@ struct GpFactors {
   int32_t* pinv;    // row -> pivot step, -1 before it is a pivot
 };
 
-// Depth-first search from row j0 (gplu.jl:70-102): returns the new top; the
-// rows it finishes go to xi[--top].  All lanes hold the same head, j, pp;
-// lane 0 writes the stack, the marks and xi; a __syncwarp ends every step.
-// A search that would leave its n-entry stack or reach arrays returns -1
-// instead (no row is pushed or finished twice, so this does not happen).
-__device__ __forceinline__ int64_t gp_dfs(int32_t j0, int32_t stamp, int64_t top, int64_t n, const int64_t* __restrict__ lp,
-                                          const int32_t* __restrict__ li, const int32_t* __restrict__ pinv,
-                                          int32_t* mark, int32_t* xi, int32_t* stack, int64_t* pstack, int lane) {
+// Depth-first search from the pivot row j0 (pinv[j0] = J0 >= 0;
+// gplu.jl:70-102): returns the new top; the rows it finishes go to
+// xi[--top].  All lanes hold the same head, j, J, pp; lane 0 writes the
+// stack and j's mark, a __syncwarp ends every step.  A row that is not yet a
+// pivot has no edges: pushing it finishes it on the next step, so the scan
+// finishes the unmarked ones it meets before the first unmarked pivot row at
+// once, in scan order (each lane writes its own row's mark and xi slot), and
+// pushes only pivot rows.  A search that would leave its n-entry stack or
+// reach arrays returns -1 instead (no row is pushed or finished twice, so
+// this does not happen).
+__device__ __forceinline__ int64_t gp_dfs(int32_t j0, int32_t J0, int32_t stamp, int64_t top, int64_t n,
+                                          const int64_t* __restrict__ lp, const int32_t* __restrict__ li,
+                                          const int32_t* __restrict__ pinv, int32_t* mark, int32_t* xi,
+                                          int32_t* stack, int64_t* pstack, int lane) {
   int64_t head = 0;
-  int32_t j = j0;
-  int64_t pp = 0;
-  bool fresh = true;   // j has just been pushed (its first visit)
-  if (lane == 0) stack[0] = j0;
+  int32_t j = j0, J = J0;
+  int64_t pp = lp[J0];
+  if (lane == 0) {
+    stack[0] = j0;
+    mark[j0] = stamp;
+  }
+  __syncwarp();
   while (head >= 0) {
-    const int32_t J = pinv[j];
-    if (fresh) {
-      pp = J >= 0 ? lp[J] : 0;
-      if (lane == 0) mark[j] = stamp;
-    }
-    const int64_t pend = J >= 0 ? lp[J + 1] : 0;
+    const int64_t pend = lp[J + 1];
     bool pushed = false;
-    int32_t inext = -1;
+    int32_t inext = -1, Jnext = -1;
     while (pp < pend) {
       const int64_t p = pp + lane;
       bool unmarked = false;
-      int32_t i = -1;
+      int32_t i = -1, Ji = -1;
       if (p < pend) {
         i = li[p];
         unmarked = i != j && mark[i] != stamp;   // j's own mark may still be in flight
+        if (unmarked) Ji = pinv[i];
       }
-      const unsigned bal = __ballot_sync(kGpFull, unmarked);
-      if (bal) {
-        const int f = __ffs(bal) - 1;
+      const unsigned bu = __ballot_sync(kGpFull, unmarked);
+      const unsigned bl = __ballot_sync(kGpFull, unmarked && Ji < 0);
+      const unsigned bp = bu & ~bl;
+      const int f = bp ? __ffs(bp) - 1 : 32;
+      const unsigned leaves = f == 32 ? bl : (bl & ((1u << f) - 1u));
+      if (leaves) {
+        const int c = __popc(leaves);
+        if (top < c) return -1;
+        if ((leaves >> lane) & 1u) {
+          xi[top - 1 - __popc(leaves & ((1u << lane) - 1u))] = i;
+          mark[i] = stamp;
+        }
+        top -= c;
+      }
+      if (bp) {
         inext = __shfl_sync(kGpFull, i, f);
+        Jnext = __shfl_sync(kGpFull, Ji, f);
         pp += f;
         pushed = true;
         break;
@@ -120,10 +138,12 @@ __device__ __forceinline__ int64_t gp_dfs(int32_t j0, int32_t stamp, int64_t top
       if (lane == 0) {
         pstack[head] = pp;
         stack[head + 1] = inext;
+        mark[inext] = stamp;
       }
       ++head;
       j = inext;
-      fresh = true;
+      J = Jnext;
+      pp = lp[J];
       __syncwarp();
     } else {
       if (top <= 0) return -1;
@@ -134,7 +154,7 @@ __device__ __forceinline__ int64_t gp_dfs(int32_t j0, int32_t stamp, int64_t top
       if (head >= 0) {
         j = stack[head];
         pp = pstack[head];
-        fresh = false;
+        J = pinv[j];
       }
     }
   }
@@ -194,7 +214,22 @@ __global__ void __launch_bounds__(32 * kGpWarps)
     int64_t top = n;
     for (int64_t pa = a0; pa < a1; ++pa) {
       const int32_t b = ri[pa];
-      if (mark[b] != stamp) top = gp_dfs(b, stamp, top, n, lp, li, pinv, mark, xi, stack, pstack, lane);
+      if (mark[b] == stamp) continue;
+      const int32_t Jb = pinv[b];
+      if (Jb < 0) {   // a row without edges finishes at once
+        if (top <= 0) {
+          top = -1;
+        } else {
+          --top;
+          if (lane == 0) {
+            mark[b] = stamp;
+            xi[top] = b;
+          }
+          __syncwarp();
+        }
+      } else {
+        top = gp_dfs(b, Jb, stamp, top, n, lp, li, pinv, mark, xi, stack, pstack, lane);
+      }
       if (top < 0) {
         if (lane == 0) status[s] = kGpInternal;
         return;
@@ -221,10 +256,9 @@ __global__ void __launch_bounds__(32 * kGpWarps)
       }
       const int cnt = (int)((n - base) < 32 ? (n - base) : 32);
       for (int t = 0; t < cnt; ++t) {
-        const int32_t J = __shfl_sync(kGpFull, Jl, t);
-        if (J < 0) continue;
-        const int32_t j = __shfl_sync(kGpFull, jl, t);
         const int64_t p0 = __shfl_sync(kGpFull, b0, t), p1 = __shfl_sync(kGpFull, b1, t);
+        if (p0 >= p1) continue;   // not a pivot row, or a column of L without entries below its diagonal
+        const int32_t j = __shfl_sync(kGpFull, jl, t);
         const double xj = x[j];
         for (int64_t p = p0 + lane; p < p1; p += 32) {
           const int32_t i = li[p];
