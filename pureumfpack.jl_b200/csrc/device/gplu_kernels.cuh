@@ -52,6 +52,7 @@ constexpr int64_t kGpInternal = -5;         // a depth-first search left its bou
 
 constexpr unsigned kGpFull = 0xffffffffu;
 constexpr int kGpWarps = 4;                  // warps (systems) per CTA of the factor kernel
+constexpr int kGpScan = 4;                   // 32-row chunks of a column of L loaded together
 
 // Workspace of the factor kernel, per column of every system.
 struct GpWork {
@@ -101,37 +102,48 @@ __device__ __forceinline__ int64_t gp_dfs(int32_t j0, int32_t J0, int32_t stamp,
     const int64_t pend = lp[J + 1];
     bool pushed = false;
     int32_t inext = -1, Jnext = -1;
-    while (pp < pend) {
-      const int64_t p = pp + lane;
-      bool unmarked = false;
-      int32_t i = -1, Ji = -1;
-      if (p < pend) {
-        i = li[p];
-        unmarked = i != j && mark[i] != stamp;   // j's own mark may still be in flight
-        if (unmarked) Ji = pinv[i];
+    // the column is read kGpScan chunks of 32 rows at a time (their rows,
+    // marks and pivot steps loaded together), then consumed chunk by chunk
+    // in order; a column's rows are distinct, so finishing rows in one chunk
+    // leaves the marks loaded for the next ones valid
+    while (pp < pend && !pushed) {
+      int32_t iv[kGpScan], jv[kGpScan];
+      bool uv[kGpScan];
+#pragma unroll
+      for (int c = 0; c < kGpScan; ++c) {
+        const int64_t p = pp + 32 * c + lane;
+        iv[c] = p < pend ? li[p] : -1;
       }
-      const unsigned bu = __ballot_sync(kGpFull, unmarked);
-      const unsigned bl = __ballot_sync(kGpFull, unmarked && Ji < 0);
-      const unsigned bp = bu & ~bl;
-      const int f = bp ? __ffs(bp) - 1 : 32;
-      const unsigned leaves = f == 32 ? bl : (bl & ((1u << f) - 1u));
-      if (leaves) {
-        const int c = __popc(leaves);
-        if (top < c) return -1;
-        if ((leaves >> lane) & 1u) {
-          xi[top - 1 - __popc(leaves & ((1u << lane) - 1u))] = i;
-          mark[i] = stamp;
+#pragma unroll
+      for (int c = 0; c < kGpScan; ++c)
+        uv[c] = iv[c] >= 0 && iv[c] != j && mark[iv[c]] != stamp;   // j's own mark may still be in flight
+#pragma unroll
+      for (int c = 0; c < kGpScan; ++c) jv[c] = uv[c] ? pinv[iv[c]] : -1;
+#pragma unroll
+      for (int c = 0; c < kGpScan; ++c) {
+        if (pushed) break;
+        const unsigned bu = __ballot_sync(kGpFull, uv[c]);
+        const unsigned bl = __ballot_sync(kGpFull, uv[c] && jv[c] < 0);
+        const unsigned bp = bu & ~bl;
+        const int f = bp ? __ffs(bp) - 1 : 32;
+        const unsigned leaves = f == 32 ? bl : (bl & ((1u << f) - 1u));
+        if (leaves) {
+          const int cnt = __popc(leaves);
+          if (top < cnt) return -1;
+          if ((leaves >> lane) & 1u) {
+            xi[top - 1 - __popc(leaves & ((1u << lane) - 1u))] = iv[c];
+            mark[iv[c]] = stamp;
+          }
+          top -= cnt;
         }
-        top -= c;
+        if (bp) {
+          inext = __shfl_sync(kGpFull, iv[c], f);
+          Jnext = __shfl_sync(kGpFull, jv[c], f);
+          pp += 32 * c + f;
+          pushed = true;
+        }
       }
-      if (bp) {
-        inext = __shfl_sync(kGpFull, i, f);
-        Jnext = __shfl_sync(kGpFull, Ji, f);
-        pp += f;
-        pushed = true;
-        break;
-      }
-      pp += 32;
+      if (!pushed) pp += 32 * kGpScan;
     }
     if (pushed) {
       if (head + 1 >= n) return -1;
@@ -166,7 +178,7 @@ __device__ __forceinline__ int64_t gp_dfs(int32_t j0, int32_t J0, int32_t stamp,
 // scaling) multiplies row i of A as Rs .* A does; q is the column order.
 // status[s] receives 0, k + 1 or a kGp* code.  Workspaces need no clearing:
 // each system clears its own at its start.
-__global__ void __launch_bounds__(32 * kGpWarps)
+__global__ void __launch_bounds__(32 * kGpWarps, 1)
     k_gplu_factor(const GpSys* __restrict__ sys, const int32_t* __restrict__ list, int64_t nlist,
                   const int64_t* __restrict__ acp, const int32_t* __restrict__ ari, const double* __restrict__ ax,
                   const double* __restrict__ rs, const int32_t* __restrict__ qord, double tol, int check,
@@ -260,7 +272,18 @@ __global__ void __launch_bounds__(32 * kGpWarps)
         if (p0 >= p1) continue;   // not a pivot row, or a column of L without entries below its diagonal
         const int32_t j = __shfl_sync(kGpFull, jl, t);
         const double xj = x[j];
-        for (int64_t p = p0 + lane; p < p1; p += 32) {
+        // four rows per lane in flight (the column's rows are distinct)
+        int64_t p = p0 + lane;
+        for (; p + 96 < p1; p += 128) {
+          const int32_t i0 = li[p], i1 = li[p + 32], i2 = li[p + 64], i3 = li[p + 96];
+          const double a0 = lx[p], a1 = lx[p + 32], a2 = lx[p + 64], a3 = lx[p + 96];
+          const double y0 = x[i0], y1 = x[i1], y2 = x[i2], y3 = x[i3];
+          x[i0] = __dsub_rn(y0, __dmul_rn(a0, xj));
+          x[i1] = __dsub_rn(y1, __dmul_rn(a1, xj));
+          x[i2] = __dsub_rn(y2, __dmul_rn(a2, xj));
+          x[i3] = __dsub_rn(y3, __dmul_rn(a3, xj));
+        }
+        for (; p < p1; p += 32) {
           const int32_t i = li[p];
           x[i] = __dsub_rn(x[i], __dmul_rn(lx[p], xj));
         }
@@ -509,7 +532,7 @@ __device__ __forceinline__ void gp_lu_solve(const GpSolveArgs& A, const GpSys& d
 // workspaces hold system s's nrhs columns at col0 * nrhs, column r at
 // + r * n.  The refinement residual r = b - A x is the column-oriented
 // product of the unscaled A, as SparseArrays forms it.
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 1)
     k_gplu_solve(GpSolveArgs A, int64_t nsys, int64_t nrhs, const double* __restrict__ B, double* __restrict__ X,
                  double* __restrict__ C, double* __restrict__ R, int refine) {
   const int lane = threadIdx.x & 31;
