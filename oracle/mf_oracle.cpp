@@ -9,7 +9,8 @@
 //   AMD / COLAMD ordering  src/amd.jl:13-539   (CSparse cs_amd, order=1)
 //   symbolic analysis      src/symbolic.jl:15-237
 //   numeric multifrontal   src/multifrontal.jl:45-375
-//   Gilbert-Peierls LU     src/gplu.jl:62-303 (the method splu uses by default)
+//   Gilbert-Peierls LU     src/gplu.jl:62-303 (the method splu uses by default),
+//                          Float64, Float32 and ComplexF64
 //   CSC triangular solves  src/solve.jl:10-39
 //   solve + refinement     src/interface.jl:123-177
 // The dense front kernels (getrf / trsm / gemm) are the same LAPACK/BLAS calls
@@ -1015,10 +1016,96 @@ i64 gp_reach(const vector<i64>& Lp, const vector<i64>& Li, const i64* cp, const 
   return top;
 }
 
-// Sort each column's (row, value) pairs by row (gplu.jl:383-415: the keys of a
-// column are distinct, so any sort gives this order).
-void gp_sortcols(i64 n, const vector<i64>& cp, vector<i64>& ri, vector<double>& x) {
-  vector<std::pair<i64, double>> tmp;
+// Scalar arithmetic of the Gilbert-Peierls restatement for each element type,
+// each operation rounded on its own as Julia evaluates it (no contraction:
+// the oracle is built for baseline x86-64, which has no fused multiply-add).
+// Complex values follow Julia Base: z * w = (re re - im im, re im + im re),
+// z / w by the robust Smith method of Baudin and Smith with its scaling, and
+// abs(z) = hypot(re, im) by Borges' fma-corrected algorithm.
+double jl_hypot(double x, double y) {
+  double ax = std::fabs(x), ay = std::fabs(y);
+  if (std::isinf(ax) || std::isinf(ay)) return INFINITY;
+  if (ay > ax) std::swap(ax, ay);
+  if (ay <= ax * std::sqrt(0x1p-53)) return ax;   // widely varying operands (and ay == 0)
+  double scale = 0x1p-563;                         // eps * sqrt(floatmin)
+  if (ax > std::sqrt(0x1.fffffffffffffp+1022)) {   // sqrt(floatmax / 2)
+    ax = ax * scale;
+    ay = ay * scale;
+    scale = 1.0 / scale;
+  } else if (ay < 0x1p-511) {                      // sqrt(floatmin)
+    ax = ax / scale;
+    ay = ay / scale;
+  } else {
+    scale = 1.0;
+  }
+  double h = std::sqrt(std::fma(ax, ax, ay * ay));
+  const double hsq = h * h, axsq = ax * ax;
+  h = h - (std::fma(-ay, ay, hsq - axsq) + std::fma(h, h, -hsq) - std::fma(ax, ax, -axsq)) / (2.0 * h);
+  return h * scale;
+}
+double jl_cdiv2(double a, double b, double c, double d, double r, double t) {
+  if (r != 0) {
+    const double br = b * r;
+    return br != 0 ? (a + br) * t : a * t + (b * t) * r;
+  }
+  return (a + d * (b / c)) * t;
+}
+void jl_cdiv1(double a, double b, double c, double d, double& p, double& q) {
+  const double r = d / c;
+  const double t = 1.0 / (c + d * r);
+  p = jl_cdiv2(a, b, c, d, r, t);
+  q = jl_cdiv2(b, -a, c, d, r, t);
+}
+cplx jl_cdiv(cplx z, cplx w) {
+  double a = z.real(), b = z.imag(), c = w.real(), d = w.imag();
+  const double ab = std::fabs(a) >= std::fabs(b) ? std::fabs(a) : std::fabs(b);
+  const double cd = std::fabs(c) >= std::fabs(d) ? std::fabs(c) : std::fabs(d);
+  const double halfov = 0.5 * 0x1.fffffffffffffp+1023;
+  const double twounf = 0x1p-1022 * 2.0 / 0x1p-52;
+  const double bs = 2.0 / (0x1p-52 * 0x1p-52);
+  double S = 1.0;
+  if (ab >= halfov) { a = 0.5 * a; b = 0.5 * b; S = 2.0 * S; }
+  if (cd >= halfov) { c = 0.5 * c; d = 0.5 * d; S = 0.5 * S; }
+  if (ab <= twounf) { a = a * bs; b = b * bs; S = S / bs; }
+  if (cd <= twounf) { c = c * bs; d = d * bs; S = S * bs; }
+  double p, q;
+  if (std::fabs(d) <= std::fabs(c)) {
+    jl_cdiv1(a, b, c, d, p, q);
+  } else {
+    jl_cdiv1(b, a, d, c, p, q);
+    q = -q;
+  }
+  return cplx(p * S, q * S);
+}
+
+template <typename T>
+struct GpOps {   // Float64 and Float32
+  using R = T;
+  static T scale(R r, T a) { return a * r; }
+  static T mul(T a, T b) { return a * b; }
+  static T add(T a, T b) { return a + b; }
+  static T sub(T a, T b) { return a - b; }
+  static T div(T a, T b) { return a / b; }
+  static R mag(T a) { return std::fabs(a); }
+};
+template <>
+struct GpOps<cplx> {
+  using R = double;
+  static cplx scale(R r, cplx a) { return cplx(a.real() * r, a.imag() * r); }
+  static cplx mul(cplx z, cplx w) {
+    return cplx(z.real() * w.real() - z.imag() * w.imag(), z.real() * w.imag() + z.imag() * w.real());
+  }
+  static cplx add(cplx a, cplx b) { return cplx(a.real() + b.real(), a.imag() + b.imag()); }
+  static cplx sub(cplx a, cplx b) { return cplx(a.real() - b.real(), a.imag() - b.imag()); }
+  static cplx div(cplx a, cplx b) { return jl_cdiv(a, b); }
+  static R mag(cplx a) { return jl_hypot(a.real(), a.imag()); }
+};
+
+// Each column's (row, value) pairs sorted by row (gplu.jl:383-415: the keys
+// of a column are distinct, so any sort gives this order).
+template <typename T>
+void gp_sortcols_t(i64 n, const vector<i64>& cp, vector<i64>& ri, vector<T>& x) {
+  vector<std::pair<i64, T>> tmp;
   for (i64 j = 0; j < n; ++j) {
     tmp.clear();
     for (i64 p = cp[j]; p < cp[j + 1]; ++p) tmp.emplace_back(ri[p], x[p]);
@@ -1030,15 +1117,20 @@ void gp_sortcols(i64 n, const vector<i64>& cp, vector<i64>& ri, vector<double>& 
   }
 }
 
-// gplu(A; q, tol, check, sort_factors) (gplu.jl:173-303), 0-based.  Returns 0,
-// or -1 when the pivot rows do not form a permutation (a singular matrix
-// factored with check = false: the reference's invperm throws there);
-// F.status = k (1-based) when check is set and column k has no nonzero pivot.
-int gplu0(i64 n, const i64* cp, const i64* ri, const double* ax, const vector<i64>& q, double tol, bool check,
-          bool sort_factors, Factor& F) {
-  F = Factor();
+// gplu(A; q, tol, check, sort_factors) (gplu.jl:173-303), 0-based, for
+// Tv = Float64, Float32 or ComplexF64 (tol converted to real(Tv), as
+// gplu.jl:213 does).  Returns 0, or -1 when the pivot rows do not form a
+// permutation (a singular matrix factored with check = false: the
+// reference's invperm throws there); F.status = k (1-based) when check is
+// set and column k has no nonzero pivot.
+template <typename T>
+int gplu0(i64 n, const i64* cp, const i64* ri, const T* ax, const vector<i64>& q, typename GpOps<T>::R tol,
+          bool check, bool sort_factors, FactorT<T>& F) {
+  using O = GpOps<T>;
+  using R = typename O::R;
+  F = FactorT<T>();
   F.n = n;
-  vector<double> x(n, 0.0);
+  vector<T> x(n, T(0));
   vector<i64> xi(n), stack(n), pstack(n), pinv(n, -1);
   vector<char> marked(n, 0);
   F.Lp.assign(n + 1, 0);
@@ -1046,20 +1138,20 @@ int gplu0(i64 n, const i64* cp, const i64* ri, const double* ax, const vector<i6
   for (i64 k = 0; k < n; ++k) {
     i64 col = q[k];
     i64 top = gp_reach(F.Lp, F.Li, cp, ri, col, pinv, xi, stack, pstack, marked, n);
-    for (i64 p = top; p < n; ++p) x[xi[p]] = 0.0;
+    for (i64 p = top; p < n; ++p) x[xi[p]] = T(0);
     for (i64 p = cp[col]; p < cp[col + 1]; ++p) x[ri[p]] = ax[p];
     for (i64 px = top; px < n; ++px) {   // L x = A(:, col), unit diagonal stored first
       i64 j = xi[px], J = pinv[j];
       if (J < 0) continue;
-      double xj = x[j];
-      for (i64 p = F.Lp[J] + 1; p < F.Lp[J + 1]; ++p) x[F.Li[p]] -= F.Lx[p] * xj;
+      T xj = x[j];
+      for (i64 p = F.Lp[J] + 1; p < F.Lp[J + 1]; ++p) x[F.Li[p]] = O::sub(x[F.Li[p]], O::mul(F.Lx[p], xj));
     }
     i64 ipiv = -1;
-    double a = -1.0;
+    R a = R(-1);
     for (i64 px = top; px < n; ++px) {   // U entries in reach order; largest unpivoted row
       i64 i = xi[px];
       if (pinv[i] < 0) {
-        double t = std::fabs(x[i]);
+        R t = O::mag(x[i]);
         if (t > a) {
           a = t;
           ipiv = i;
@@ -1076,21 +1168,21 @@ int gplu0(i64 n, const i64* cp, const i64* ri, const double* ax, const vector<i6
       }
       if (ipiv < 0) ipiv = col;
     }
-    if (pinv[col] < 0 && std::fabs(x[col]) >= tol * a) ipiv = col;
-    double pivot = x[ipiv];
+    if (pinv[col] < 0 && O::mag(x[col]) >= tol * a) ipiv = col;
+    T pivot = x[ipiv];
     F.Ui.push_back(k);
     F.Ux.push_back(pivot);
     F.Up[k + 1] = (i64)F.Ui.size();
     pinv[ipiv] = k;
     F.Li.push_back(ipiv);
-    F.Lx.push_back(1.0);
+    F.Lx.push_back(T(1));
     for (i64 px = top; px < n; ++px) {
       i64 i = xi[px];
       if (pinv[i] < 0) {
         F.Li.push_back(i);
-        F.Lx.push_back(x[i] / pivot);
+        F.Lx.push_back(O::div(x[i], pivot));
       }
-      x[i] = 0.0;
+      x[i] = T(0);
     }
     F.Lp[k + 1] = (i64)F.Li.size();
   }
@@ -1101,14 +1193,47 @@ int gplu0(i64 n, const i64* cp, const i64* ri, const double* ax, const vector<i6
   }
   for (auto& r : F.Li) r = pinv[r];
   if (sort_factors) {
-    gp_sortcols(n, F.Lp, F.Li, F.Lx);
-    gp_sortcols(n, F.Up, F.Ui, F.Ux);
+    gp_sortcols_t(n, F.Lp, F.Li, F.Lx);
+    gp_sortcols_t(n, F.Up, F.Ui, F.Ux);
   }
   F.q = q;
   F.pinv = pinv;
   F.p.assign(n, 0);
   for (i64 i = 0; i < n; ++i) F.p[pinv[i]] = i;
   return 0;
+}
+
+// solve(F::PureLU{ComplexF64}, b; refine) over Gilbert-Peierls factors
+// (interface.jl:123-177, solve.jl:10-39) in Julia's complex arithmetic.
+void gp_solve_c64(const FactorC& F, const double* Rs, i64 n, const i64* colptr, const i64* rowval,
+                  const double* nzval_ri, const cplx* b, cplx* x, int refine) {
+  using O = GpOps<cplx>;
+  vector<cplx> c(n), r(n), ax(n);
+  auto solve1 = [&](const cplx* bb, cplx* xx, bool accumulate) {
+    for (i64 k = 0; k < n; ++k) c[k] = Rs ? O::scale(Rs[F.p[k]], bb[F.p[k]]) : bb[F.p[k]];
+    for (i64 j = 0; j < n; ++j) {
+      const cplx yj = c[j];
+      for (i64 p = F.Lp[j] + 1; p < F.Lp[j + 1]; ++p) c[F.Li[p]] = O::sub(c[F.Li[p]], O::mul(F.Lx[p], yj));
+    }
+    for (i64 j = n - 1; j >= 0; --j) {
+      const i64 pd = F.Up[j + 1] - 1;
+      const cplx yj = O::div(c[j], F.Ux[pd]);
+      c[j] = yj;
+      for (i64 p = F.Up[j]; p < pd; ++p) c[F.Ui[p]] = O::sub(c[F.Ui[p]], O::mul(F.Ux[p], yj));
+    }
+    for (i64 k = 0; k < n; ++k) xx[F.q[k]] = accumulate ? O::add(xx[F.q[k]], c[k]) : c[k];
+  };
+  solve1(b, x, false);
+  for (int it = 0; it < refine; ++it) {
+    std::fill(ax.begin(), ax.end(), cplx(0.0, 0.0));
+    for (i64 j = 0; j < n; ++j) {
+      const cplx xj = x[j];
+      for (i64 p = colptr[j] - 1; p < colptr[j + 1] - 1; ++p)
+        ax[rowval[p] - 1] = O::add(ax[rowval[p] - 1], O::mul(cplx(nzval_ri[2 * p], nzval_ri[2 * p + 1]), xj));
+    }
+    for (i64 i = 0; i < n; ++i) r[i] = O::sub(b[i], ax[i]);
+    solve1(r.data(), x, true);
+  }
 }
 
 }  // namespace
@@ -1274,6 +1399,65 @@ void* orc_gplu(i64 n, const i64* colptr, const i64* rowval, const double* nzval,
   if (rc < 0) g_err = "gplu: the pivot rows are not a permutation (singular matrix, check = false)";
   *status = rc < 0 ? rc : F->status;
   return F;
+}
+
+// gplu of a Float32 matrix, all arithmetic in Float32; the factor's values
+// are returned widened to Float64 (exactly), as the other Float32 entry points.
+void* orc_gplu_f32(i64 n, const i64* colptr, const i64* rowval, const float* nzval, const i64* q1, double tol,
+                   int check, int sort_factors, i64* status) {
+  vector<i64> cp, ri;
+  to0(n, colptr, rowval, cp, ri);
+  vector<i64> q(n);
+  for (i64 k = 0; k < n; ++k) q[k] = q1 ? q1[k] - 1 : k;
+  FactorT<float> F32;
+  int rc = gplu0(n, cp.data(), ri.data(), nzval, q, (float)tol, check != 0, sort_factors != 0, F32);
+  Factor* F = new Factor();
+  F->n = F32.n;
+  F->Lp = F32.Lp;
+  F->Li = F32.Li;
+  F->Up = F32.Up;
+  F->Ui = F32.Ui;
+  F->Lx.assign(F32.Lx.begin(), F32.Lx.end());
+  F->Ux.assign(F32.Ux.begin(), F32.Ux.end());
+  F->p = F32.p;
+  F->q = F32.q;
+  F->pinv = F32.pinv;
+  F->status = F32.status;
+  if (rc < 0) g_err = "gplu: the pivot rows are not a permutation (singular matrix, check = false)";
+  *status = rc < 0 ? rc : F->status;
+  return F;
+}
+
+// gplu of a ComplexF64 matrix (values as interleaved re, im doubles).
+void* orc_gplu_c64(i64 n, const i64* colptr, const i64* rowval, const double* nzval_ri, const i64* q1, double tol,
+                   int check, int sort_factors, i64* status) {
+  vector<i64> cp, ri;
+  to0(n, colptr, rowval, cp, ri);
+  vector<i64> q(n);
+  for (i64 k = 0; k < n; ++k) q[k] = q1 ? q1[k] - 1 : k;
+  vector<cplx> xz(cp[n]);
+  for (i64 p = 0; p < cp[n]; ++p) xz[p] = cplx(nzval_ri[2 * p], nzval_ri[2 * p + 1]);
+  FactorC* F = new FactorC();
+  int rc = gplu0(n, cp.data(), ri.data(), xz.data(), q, tol, check != 0, sort_factors != 0, *F);
+  if (rc < 0) g_err = "gplu: the pivot rows are not a permutation (singular matrix, check = false)";
+  *status = rc < 0 ? rc : F->status;
+  return F;
+}
+
+// solve(F, b; refine) over complex Gilbert-Peierls factors (Rs NULL: the raw
+// F \ b, refine 0).  B, X: nrhs columns of n interleaved (re, im) doubles.
+void orc_gplu_solve_c64(void* h, const double* Rs, i64 n, const i64* colptr, const i64* rowval,
+                        const double* nzval_ri, i64 nrhs, const double* B, double* X, int refine) {
+  const FactorC* F = (const FactorC*)h;
+  vector<cplx> b(n), x(n);
+  for (i64 c = 0; c < nrhs; ++c) {
+    for (i64 i = 0; i < n; ++i) b[i] = cplx(B[2 * (c * n + i)], B[2 * (c * n + i) + 1]);
+    gp_solve_c64(*F, Rs, n, colptr, rowval, nzval_ri, b.data(), x.data(), refine);
+    for (i64 i = 0; i < n; ++i) {
+      X[2 * (c * n + i)] = x[i].real();
+      X[2 * (c * n + i) + 1] = x[i].imag();
+    }
+  }
 }
 
 void orc_factor_free(void* h) { delete (Factor*)h; }

@@ -85,6 +85,14 @@ def lib():
         L.orc_gplu.restype = ctypes.c_void_p
         L.orc_gplu.argtypes = [ctypes.c_int64, _i64p, _i64p, _f64p, _i64p, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                _i64p]
+        L.orc_gplu_f32.restype = ctypes.c_void_p
+        L.orc_gplu_f32.argtypes = [ctypes.c_int64, _i64p, _i64p, _f32p, _i64p, ctypes.c_double, ctypes.c_int,
+                                   ctypes.c_int, _i64p]
+        L.orc_gplu_c64.restype = ctypes.c_void_p
+        L.orc_gplu_c64.argtypes = [ctypes.c_int64, _i64p, _i64p, _f64p, _i64p, ctypes.c_double, ctypes.c_int,
+                                   ctypes.c_int, _i64p]
+        L.orc_gplu_solve_c64.argtypes = [ctypes.c_void_p, _f64p, ctypes.c_int64, _i64p, _i64p, _f64p, ctypes.c_int64,
+                                         _f64p, _f64p, ctypes.c_int]
         L.orc_numeric.argtypes = [ctypes.c_void_p, _f64p, _i64p, _i64p, ctypes.c_int, _i64p]
         L.orc_factor_free.argtypes = [ctypes.c_void_p]
         L.orc_factor_sizes.argtypes = [ctypes.c_void_p, _i64p]
@@ -278,21 +286,36 @@ def multifrontal_lu(A, q=None, check: bool = True) -> Factor:
     return _extract(h)
 
 
-def gplu(A, q=None, tol: float = 0.1, check: bool = True, sort_factors: bool = True) -> Factor:
-    """gplu(A; q, tol, check, sort_factors) (gplu.jl:173-303), A as given."""
+def gplu(A, q=None, tol: float = 0.1, check: bool = True, sort_factors: bool = True):
+    """gplu(A; q, tol, check, sort_factors) (gplu.jl:173-303), A as given:
+    Float64, Float32 (values returned widened to Float64, exactly) or
+    ComplexF64 (a ``ComplexCSC``; returns a ``FactorC``)."""
     if A.m != A.n:
         raise ValueError("DimensionMismatch: gplu requires a square matrix")
     st = np.zeros(1, np.int64)
     qa = _i(q) if q is not None else None
-    h = lib().orc_gplu(A.n, _p(_i(A.colptr)), _p(_i(A.rowval)), _p(_f(A.nzval), _f64p), _p(qa), float(tol),
-                       int(check), int(sort_factors), _p(st))
+    pat = (A.n, _p(_i(A.colptr)), _p(_i(A.rowval)))
+    cz = np.iscomplexobj(A.nzval)
+    if cz:
+        h = lib().orc_gplu_c64(*pat, _p(_ri(A.nzval), _f64p), _p(qa), float(tol), int(check), int(sort_factors),
+                               _p(st))
+    elif A.nzval.dtype == np.float32:
+        h = lib().orc_gplu_f32(*pat, _p(_f32(A.nzval), _f32p), _p(qa), float(tol), int(check), int(sort_factors),
+                               _p(st))
+    else:
+        h = lib().orc_gplu(*pat, _p(_f(A.nzval), _f64p), _p(qa), float(tol), int(check), int(sort_factors), _p(st))
+    free = lib().orc_factor_free_c64 if cz else lib().orc_factor_free
     if st[0] < 0:
-        lib().orc_factor_free(ctypes.c_void_p(h))
+        free(ctypes.c_void_p(h))
         raise RuntimeError("oracle: " + lib().orc_last_error().decode())
     if st[0] > 0:
-        lib().orc_factor_free(ctypes.c_void_p(h))
+        free(ctypes.c_void_p(h))
         raise SingularException(int(st[0]))
-    return _extract(h)
+    if cz:
+        return _extract_c64(h)
+    F = _extract(h)
+    F.f32 = A.nzval.dtype == np.float32
+    return F
 
 
 def gplu_order(A, ordering: str) -> np.ndarray:
@@ -342,13 +365,56 @@ def splu(A, scale: int = SCALE_SUM, check: bool = True, q=None) -> PureLU:
 
 
 def splu_gplu(A, ordering: str = "amd", tol: float = 0.1, scale: int = SCALE_SUM, check: bool = True) -> PureLU:
-    """splu(A; method=:gplu, ordering, tol, scale, check) (interface.jl:93-120)."""
+    """splu(A; method=:gplu, ordering, tol, scale, check) (interface.jl:93-120)
+    for Float64, Float32 and ComplexF64 values."""
     if A.m != A.n:
         raise ValueError("DimensionMismatch: splu requires a square matrix")
-    Rs = row_scaling(A, scale)
-    As = A if scale == SCALE_NONE else apply_row_scaling(A, Rs)
+    if np.iscomplexobj(A.nzval):
+        Rs = row_scaling_c64(A, scale)
+        As = A if scale == SCALE_NONE else apply_row_scaling_c64(A, Rs)
+    elif A.nzval.dtype == np.float32:
+        Rs = row_scaling_f32(A, scale)
+        As = A.copy()
+        if scale != SCALE_NONE:
+            As.nzval = (_f32(As.nzval) * Rs[As.rowval - 1]).astype(np.float32)
+    else:
+        Rs = row_scaling(A, scale)
+        As = A if scale == SCALE_NONE else apply_row_scaling(A, Rs)
     q = gplu_order(A, ordering)
     return PureLU(gplu(As, q=q, tol=tol, check=check), Rs, A)
+
+
+def solve_gplu(F, b, refine: int = 0):
+    """solve(F, b; refine) over Gilbert-Peierls factors in the factors' own
+    element type: F a PureLU (row scaling, refinement against F.A), or a raw
+    factor (F \\ b, refine 0)."""
+    if isinstance(F, PureLU):
+        Fo, Rs, A = F.F, F.Rs, F.A
+    else:
+        Fo, Rs, A = F, None, None
+        if refine:
+            raise ValueError("refinement needs a PureLU")
+    n = len(Fo.p)
+    cp = _i(A.colptr) if A is not None else np.ones(n + 1, np.int64)
+    rv = _i(A.rowval) if A is not None else np.zeros(0, np.int64)
+    if isinstance(Fo, FactorC):
+        B = np.asfortranarray(b, dtype=np.complex128)
+        nrhs = 1 if B.ndim == 1 else B.shape[1]
+        Bri = np.ascontiguousarray(B.ravel(order="F")).view(np.float64)
+        Xri = np.empty_like(Bri)
+        nz = _ri(A.nzval) if A is not None else np.zeros(0)
+        lib().orc_gplu_solve_c64(ctypes.c_void_p(Fo.handle), _p(_f(Rs), _f64p) if Rs is not None else None, n,
+                                 _p(cp), _p(rv), _p(nz, _f64p), nrhs, _p(Bri, _f64p), _p(Xri, _f64p), int(refine))
+        return Xri.view(np.complex128).reshape(B.shape, order="F")
+    if getattr(Fo, "f32", False):
+        B = np.asfortranarray(b, dtype=np.float32)
+        nrhs = 1 if B.ndim == 1 else B.shape[1]
+        X = np.empty_like(B)
+        nz = _f32(A.nzval) if A is not None else np.zeros(0, np.float32)
+        lib().orc_solve_f32(ctypes.c_void_p(Fo.handle), _p(_f32(Rs), _f32p) if Rs is not None else None, n, _p(cp),
+                            _p(rv), _p(nz, _f32p), nrhs, _p(B, _f32p), _p(X, _f32p), int(refine))
+        return X
+    return solve(F, b, refine=refine) if Rs is not None else solve_raw(Fo, b)
 
 
 def solve(F: PureLU, b: np.ndarray, refine: int = 0) -> np.ndarray:
@@ -488,6 +554,19 @@ def multifrontal_lu_c64(A: ComplexCSC, q=None, check: bool = True) -> FactorC:
         if st[0] > 0:
             raise SingularException(int(st[0]))
         raise RuntimeError("oracle: " + lib().orc_last_error().decode())
+    sz = np.empty(3, dtype=np.int64)
+    lib().orc_factor_sizes_c64(ctypes.c_void_p(h), _p(sz))
+    n, nl, nu = (int(v) for v in sz)
+    Lp, Up = np.empty(n + 1, np.int64), np.empty(n + 1, np.int64)
+    Li, Ui = np.empty(nl, np.int64), np.empty(nu, np.int64)
+    Lx, Ux = np.empty(nl, np.complex128), np.empty(nu, np.complex128)
+    p, qq, pinv = np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.int64)
+    lib().orc_factor_get_c64(ctypes.c_void_p(h), _p(Lp), _p(Li), _p(Lx.view(np.float64), _f64p), _p(Up), _p(Ui),
+                             _p(Ux.view(np.float64), _f64p), _p(p), _p(qq), _p(pinv))
+    return FactorC(Lp, Li, Lx, Up, Ui, Ux, p, qq, pinv, handle=h)
+
+
+def _extract_c64(h) -> FactorC:
     sz = np.empty(3, dtype=np.int64)
     lib().orc_factor_sizes_c64(ctypes.c_void_p(h), _p(sz))
     n, nl, nu = (int(v) for v in sz)

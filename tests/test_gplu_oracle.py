@@ -7,8 +7,10 @@ through the reference's fill identity predicted_fill(S) ==
 nnz(gplu(M; q = S.qf, tol = 0)) (test/multifrontal_test.jl:12-21, 43-51), the
 reconstruction, strict-pivoting, sort_factors, canonical-CSC and
 singularity tests of test/pureumfpack_test.jl:11-57 and
-test/robustness.jl:38-42, and splu(A; method = :gplu) end to end over the
-orderings and scalings (test/pureumfpack_test.jl:80-123).
+test/robustness.jl:38-42, splu(A; method = :gplu) end to end over the
+orderings and scalings (test/pureumfpack_test.jl:80-123), and the generic
+element types of test/robustness.jl:8-26 (ComplexF64 through every
+ordering, Float32 staying Float32).
 """
 
 import json
@@ -148,3 +150,58 @@ def test_splu_gplu_orderings_and_scalings(make):
             x = O.solve(F, b)
             assert np.linalg.norm(A.to_scipy() @ x - b) / np.linalg.norm(b) <= 1e-8
             assert np.linalg.norm(x - xref) / np.linalg.norm(xref) <= 1e-6
+
+
+def sprand_complex(n, density, shift, seed):
+    import scipy.sparse as sp
+
+    rng = np.random.default_rng(seed)
+    nnz = rng.binomial(n * n, density)
+    I, J = rng.integers(0, n, nnz), rng.integers(0, n, nnz)
+    V = rng.random(nnz) + 1j * rng.random(nnz)
+    return (sp.coo_matrix((V, (I, J)), shape=(n, n)).tocsc() + shift * sp.eye(n, format="csc")).tocsc()
+
+
+@pytest.mark.parametrize("ordering", ["amd", "colamd", "natural"])
+def test_gplu_complex_robustness(ordering):
+    """test/robustness.jl:8-17: splu(A::SparseMatrixCSC{ComplexF64}; ordering) \\ b
+    (the default method, :gplu) to residual 1e-10, and against a direct solve."""
+    import scipy.sparse.linalg as spla
+
+    S = sprand_complex(400, 8 / 400, 5.0, 7)
+    A = O.ComplexCSC.from_scipy(S)
+    rng = np.random.default_rng(8)
+    b = rng.standard_normal(400) + 1j * rng.standard_normal(400)
+    F = O.splu_gplu(A, ordering=ordering)
+    x = O.solve_gplu(F, b)
+    assert np.linalg.norm(S @ x - b) / np.linalg.norm(b) <= 1e-10
+    xr = spla.spsolve(S, b)
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) <= 1e-9
+    L = F.F
+    for cp, ri in ((L.Lcolptr, L.Lrowval), (L.Ucolptr, L.Urowval)):
+        assert all(np.all(np.diff(ri[cp[j] - 1:cp[j + 1] - 1]) > 0) for j in range(400))
+    # the raw factor solves A[p, q] x = b too
+    Fr = O.gplu(A, q=O.gplu_order(A, ordering))
+    xr2 = O.solve_gplu(Fr, b)
+    assert np.linalg.norm(S @ xr2 - b) / np.linalg.norm(b) <= 1e-10
+
+
+def test_gplu_float32_robustness():
+    """test/robustness.jl:18-26: a Float32 matrix stays Float32 end to end."""
+    n = 300
+    rng = np.random.default_rng(9)
+    nnz = rng.binomial(n * n, 8 / n)
+    I, J = rng.integers(1, n + 1, nnz), rng.integers(1, n + 1, nnz)
+    d = np.arange(1, n + 1)
+    A = SparseCSC.from_coo(np.concatenate([I, d]), np.concatenate([J, d]),
+                           np.concatenate([rng.random(nnz), np.full(n, 5.0)]), n, n)
+    A = SparseCSC(n, n, A.colptr, A.rowval, A.nzval.astype(np.float32))
+    b = rng.standard_normal(n).astype(np.float32)
+    F = O.splu_gplu(A, ordering="amd")
+    x = O.solve_gplu(F, b)
+    assert x.dtype == np.float32
+    assert np.linalg.norm(A.to_scipy().astype(np.float64) @ x - b) / np.linalg.norm(b) <= 1e-4
+    # the Float32 values are Float32 numbers (widened exactly) and differ from the Float64 factorization's
+    F64 = O.splu_gplu(SparseCSC(n, n, A.colptr, A.rowval, A.nzval.astype(np.float64)), ordering="amd")
+    assert np.array_equal(F.F.Lnzval.astype(np.float32).astype(np.float64), F.F.Lnzval)
+    assert not np.array_equal(F.F.Lnzval, F64.F.Lnzval)
