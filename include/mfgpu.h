@@ -370,6 +370,27 @@ int mfgpu_gplu_get_factors(mfgpu_gplu* g, int64_t sys, int64_t* lcolptr, int64_t
  * refine refinement steps against the unscaled A_i when the system was
  * factored with a row scaling (PureLU), or the raw F \ b otherwise. */
 int mfgpu_gplu_solve(mfgpu_gplu* g, int64_t nrhs, const double* const* b, double* const* x, int32_t refine);
+/* The same for the reference's other element types: Float32 values, Rs, b
+ * and x (tol rounded to Float32, all arithmetic in Float32), and ComplexF64
+ * values, b and x as interleaved (re, im) doubles with a real Float64 Rs
+ * (Julia's complex product, division and abs).  A handle's factor-fetch and
+ * solve calls must match the type it last factored (MFGPU_ERR_STATE). */
+int mfgpu_gplu_factor_f32(mfgpu_gplu* g, int64_t nsys, const int64_t* n, const int64_t* const* colptr,
+                          const int64_t* const* rowval, const float* const* nzval, const int64_t* const* q,
+                          const float* const* rs, double tol, int32_t check, int32_t sort_factors, int64_t* status);
+int mfgpu_gplu_get_factors_f32(mfgpu_gplu* g, int64_t sys, int64_t* lcolptr, int64_t* lrowval, float* lnzval,
+                               int64_t* ucolptr, int64_t* urowval, float* unzval, int64_t* p, int64_t* q,
+                               int64_t* pinv);
+int mfgpu_gplu_solve_f32(mfgpu_gplu* g, int64_t nrhs, const float* const* b, float* const* x, int32_t refine);
+int mfgpu_gplu_factor_c64(mfgpu_gplu* g, int64_t nsys, const int64_t* n, const int64_t* const* colptr,
+                          const int64_t* const* rowval, const double* const* nzval_ri, const int64_t* const* q,
+                          const double* const* rs, double tol, int32_t check, int32_t sort_factors,
+                          int64_t* status);
+int mfgpu_gplu_get_factors_c64(mfgpu_gplu* g, int64_t sys, int64_t* lcolptr, int64_t* lrowval, double* lnzval_ri,
+                               int64_t* ucolptr, int64_t* urowval, double* unzval_ri, int64_t* p, int64_t* q,
+                               int64_t* pinv);
+int mfgpu_gplu_solve_c64(mfgpu_gplu* g, int64_t nrhs, const double* const* b_ri, double* const* x_ri,
+                         int32_t refine);
 /* {factor kernel ms (all attempts), finish kernel ms, last solve kernel ms,
  * factor launches, systems factored again} of the last calls. */
 int mfgpu_gplu_timings(mfgpu_gplu* g, double* out5);

@@ -17,10 +17,12 @@
 //   * the pivot search is a warp reduction over the reach with the first
 //     position winning ties, as the reference's strict `>` scan;
 //   * U's and L's new entries are appended in reach order by ballot ranks.
-// Every product, difference and quotient is rounded on its own
-// (__dmul_rn / __dsub_rn / __dadd_rn / __ddiv_rn, never a fused multiply-add),
-// as the reference's scalar loops round them, so factors and solutions are
-// bit for bit the reference's.
+// The element type is Float64, Float32 or ComplexF64 (the reference's
+// generic Tv).  Every product, sum, difference and quotient is rounded on its
+// own (the *_rn intrinsics, never a contracted multiply-add), as the
+// reference's scalar loops round them; complex values follow Julia's own
+// multiplication, division and abs (GpArith), so factors and solutions are
+// bit for bit the reference's restatement's.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -54,9 +56,133 @@ constexpr unsigned kGpFull = 0xffffffffu;
 constexpr int kGpWarps = 4;                  // warps (systems) per CTA of the factor kernel
 constexpr int kGpScan = 4;                   // 32-row chunks of a column of L loaded together
 
+// ComplexF64 as Julia lays it out: (re, im) doubles.
+struct __align__(16) GpComplex {
+  double re, im;
+};
+
+// Julia's abs(::ComplexF64) = hypot(re, im): Borges' algorithm with the
+// fused-multiply-add correction, as Julia Base runs it on hardware with FMA.
+__device__ __forceinline__ double gp_hypot(double x, double y) {
+  double ax = fabs(x), ay = fabs(y);
+  if (isinf(ax) || isinf(ay)) return __longlong_as_double(0x7ff0000000000000LL);
+  if (ay > ax) {
+    const double t = ax;
+    ax = ay;
+    ay = t;
+  }
+  if (ay <= __dmul_rn(ax, __dsqrt_rn(0x1p-53))) return ax;   // widely varying operands (and ay == 0)
+  double scale = 0x1p-563;                                   // eps * sqrt(floatmin)
+  if (ax > __dsqrt_rn(0x1.fffffffffffffp+1022)) {           // sqrt(floatmax / 2)
+    ax = __dmul_rn(ax, scale);
+    ay = __dmul_rn(ay, scale);
+    scale = __ddiv_rn(1.0, scale);
+  } else if (ay < 0x1p-511) {                                // sqrt(floatmin)
+    ax = __ddiv_rn(ax, scale);
+    ay = __ddiv_rn(ay, scale);
+  } else {
+    scale = 1.0;
+  }
+  double h = __dsqrt_rn(__fma_rn(ax, ax, __dmul_rn(ay, ay)));
+  const double hsq = __dmul_rn(h, h), axsq = __dmul_rn(ax, ax);
+  const double num = __dsub_rn(__dadd_rn(__fma_rn(-ay, ay, __dsub_rn(hsq, axsq)), __fma_rn(h, h, -hsq)),
+                               __fma_rn(ax, ax, -axsq));
+  h = __dsub_rn(h, __ddiv_rn(num, __dmul_rn(2.0, h)));
+  return __dmul_rn(h, scale);
+}
+
+__device__ __forceinline__ double gp_cdiv2(double a, double b, double c, double d, double r, double t) {
+  if (r != 0) {
+    const double br = __dmul_rn(b, r);
+    return br != 0 ? __dmul_rn(__dadd_rn(a, br), t) : __dadd_rn(__dmul_rn(a, t), __dmul_rn(__dmul_rn(b, t), r));
+  }
+  return __dmul_rn(__dadd_rn(a, __dmul_rn(d, __ddiv_rn(b, c))), t);
+}
+
+// Julia's ComplexF64 division: Smith's method with the Baudin-Smith twist
+// and its overflow / underflow scaling.
+__device__ __forceinline__ GpComplex gp_cdiv(GpComplex z, GpComplex w) {
+  double a = z.re, b = z.im, c = w.re, d = w.im;
+  const double ab = fabs(a) >= fabs(b) ? fabs(a) : fabs(b);
+  const double cd = fabs(c) >= fabs(d) ? fabs(c) : fabs(d);
+  const double halfov = 0x1.fffffffffffffp+1022;   // floatmax / 2
+  const double twounf = 0x1p-969;                   // 2 floatmin / eps
+  const double bs = 0x1p+105;                       // 2 / eps^2
+  double S = 1.0;
+  if (ab >= halfov) { a = 0.5 * a; b = 0.5 * b; S = 2.0 * S; }
+  if (cd >= halfov) { c = 0.5 * c; d = 0.5 * d; S = 0.5 * S; }
+  if (ab <= twounf) { a = __dmul_rn(a, bs); b = __dmul_rn(b, bs); S = __ddiv_rn(S, bs); }
+  if (cd <= twounf) { c = __dmul_rn(c, bs); d = __dmul_rn(d, bs); S = __dmul_rn(S, bs); }
+  double p, q;
+  if (fabs(d) <= fabs(c)) {
+    const double r = __ddiv_rn(d, c), t = __ddiv_rn(1.0, __dadd_rn(c, __dmul_rn(d, r)));
+    p = gp_cdiv2(a, b, c, d, r, t);
+    q = gp_cdiv2(b, -a, c, d, r, t);
+  } else {
+    const double r = __ddiv_rn(c, d), t = __ddiv_rn(1.0, __dadd_rn(d, __dmul_rn(c, r)));
+    p = gp_cdiv2(b, a, d, c, r, t);
+    q = -gp_cdiv2(a, -b, d, c, r, t);
+  }
+  return GpComplex{__dmul_rn(p, S), __dmul_rn(q, S)};
+}
+
+// The scalar operations of one element type, each rounded on its own as
+// Julia rounds them (R: the real type of magnitudes, row scaling and tol).
+template <typename T>
+struct GpArith;
+template <>
+struct GpArith<double> {
+  using R = double;
+  static __device__ __forceinline__ double zero() { return 0.0; }
+  static __device__ __forceinline__ double one() { return 1.0; }
+  static __device__ __forceinline__ double scale(R r, double a) { return __dmul_rn(a, r); }
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+  static __device__ __forceinline__ R mag(double a) { return fabs(a); }
+  static __device__ __forceinline__ R rmul(R a, R b) { return __dmul_rn(a, b); }
+};
+template <>
+struct GpArith<float> {
+  using R = float;
+  static __device__ __forceinline__ float zero() { return 0.0f; }
+  static __device__ __forceinline__ float one() { return 1.0f; }
+  static __device__ __forceinline__ float scale(R r, float a) { return __fmul_rn(a, r); }
+  static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+  static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+  static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+  static __device__ __forceinline__ R mag(float a) { return fabsf(a); }
+  static __device__ __forceinline__ R rmul(R a, R b) { return __fmul_rn(a, b); }
+};
+template <>
+struct GpArith<GpComplex> {
+  using R = double;
+  static __device__ __forceinline__ GpComplex zero() { return GpComplex{0.0, 0.0}; }
+  static __device__ __forceinline__ GpComplex one() { return GpComplex{1.0, 0.0}; }
+  static __device__ __forceinline__ GpComplex scale(R r, GpComplex a) {
+    return GpComplex{__dmul_rn(a.re, r), __dmul_rn(a.im, r)};
+  }
+  static __device__ __forceinline__ GpComplex mul(GpComplex z, GpComplex w) {
+    return GpComplex{__dsub_rn(__dmul_rn(z.re, w.re), __dmul_rn(z.im, w.im)),
+                     __dadd_rn(__dmul_rn(z.re, w.im), __dmul_rn(z.im, w.re))};
+  }
+  static __device__ __forceinline__ GpComplex add(GpComplex a, GpComplex b) {
+    return GpComplex{__dadd_rn(a.re, b.re), __dadd_rn(a.im, b.im)};
+  }
+  static __device__ __forceinline__ GpComplex sub(GpComplex a, GpComplex b) {
+    return GpComplex{__dsub_rn(a.re, b.re), __dsub_rn(a.im, b.im)};
+  }
+  static __device__ __forceinline__ GpComplex div(GpComplex a, GpComplex b) { return gp_cdiv(a, b); }
+  static __device__ __forceinline__ R mag(GpComplex a) { return gp_hypot(a.re, a.im); }
+  static __device__ __forceinline__ R rmul(R a, R b) { return __dmul_rn(a, b); }
+};
+
 // Workspace of the factor kernel, per column of every system.
+template <typename T>
 struct GpWork {
-  double* x;        // dense column being solved (zero between steps)
+  T* x;             // dense column being solved (zero between steps)
   int32_t* xi;      // reach in topological order (xi[top..n))
   int32_t* stack;   // depth-first stack
   int64_t* pstack;  // resume position in L of each stack entry
@@ -66,13 +192,14 @@ struct GpWork {
 // Factors being built: L's rows are A's row numbers until the finish kernel
 // relabels them in pivot order; L's unit diagonal comes first in its column,
 // U's diagonal last.
+template <typename T>
 struct GpFactors {
   int64_t* lp;      // per system n + 1, relative to the system's l0
   int32_t* li;
-  double* lx;
+  T* lx;
   int64_t* up;
   int32_t* ui;
-  double* ux;
+  T* ux;
   int32_t* pinv;    // row -> pivot step, -1 before it is a pivot
 };
 
@@ -178,11 +305,14 @@ __device__ __forceinline__ int64_t gp_dfs(int32_t j0, int32_t J0, int32_t stamp,
 // scaling) multiplies row i of A as Rs .* A does; q is the column order.
 // status[s] receives 0, k + 1 or a kGp* code.  Workspaces need no clearing:
 // each system clears its own at its start.
+template <typename T>
 __global__ void __launch_bounds__(32 * kGpWarps, 1)
     k_gplu_factor(const GpSys* __restrict__ sys, const int32_t* __restrict__ list, int64_t nlist,
-                  const int64_t* __restrict__ acp, const int32_t* __restrict__ ari, const double* __restrict__ ax,
-                  const double* __restrict__ rs, const int32_t* __restrict__ qord, double tol, int check,
-                  GpFactors F, GpWork W, int64_t* __restrict__ status) {
+                  const int64_t* __restrict__ acp, const int32_t* __restrict__ ari, const T* __restrict__ ax,
+                  const typename GpArith<T>::R* __restrict__ rs, const int32_t* __restrict__ qord,
+                  typename GpArith<T>::R tol, int check, GpFactors<T> F, GpWork<T> W, int64_t* __restrict__ status) {
+  using O = GpArith<T>;
+  using R = typename O::R;
   const int lane = threadIdx.x & 31;
   const int64_t w = (int64_t)blockIdx.x * kGpWarps + (threadIdx.x >> 5);
   if (w >= nlist) return;
@@ -191,17 +321,17 @@ __global__ void __launch_bounds__(32 * kGpWarps, 1)
   const int64_t n = d.n;
   const int64_t* cp = acp + d.cp0;
   const int32_t* ri = ari + d.nz0;
-  const double* av = ax + d.nz0;
-  const double* r = rs ? rs + d.col0 : nullptr;
+  const T* av = ax + d.nz0;
+  const R* r = rs ? rs + d.col0 : nullptr;
   const int32_t* q = qord + d.col0;
   int64_t* lp = F.lp + d.cp0;
   int64_t* up = F.up + d.cp0;
   int32_t* li = F.li + d.l0;
-  double* lx = F.lx + d.l0;
+  T* lx = F.lx + d.l0;
   int32_t* ui = F.ui + d.u0;
-  double* ux = F.ux + d.u0;
+  T* ux = F.ux + d.u0;
   int32_t* pinv = F.pinv + d.col0;
-  double* x = W.x + d.col0;
+  T* x = W.x + d.col0;
   int32_t* xi = W.xi + d.col0;
   int32_t* stack = W.stack + d.col0;
   int64_t* pstack = W.pstack + d.col0;
@@ -210,7 +340,7 @@ __global__ void __launch_bounds__(32 * kGpWarps, 1)
   for (int64_t i = lane; i < n; i += 32) {
     pinv[i] = -1;
     mark[i] = 0;
-    x[i] = 0.0;
+    x[i] = O::zero();
   }
   if (lane == 0) {
     lp[0] = 0;
@@ -250,7 +380,7 @@ __global__ void __launch_bounds__(32 * kGpWarps, 1)
     // x = A(:, col), scaled (x is zero outside the previous reaches)
     for (int64_t pa = a0 + lane; pa < a1; pa += 32) {
       const int32_t i = ri[pa];
-      x[i] = r ? __dmul_rn(r[i], av[pa]) : av[pa];
+      x[i] = r ? O::scale(r[i], av[pa]) : av[pa];
     }
     __syncwarp();
     // L x = A(:, col) over the reach in topological order (gplu.jl:226-235)
@@ -271,41 +401,41 @@ __global__ void __launch_bounds__(32 * kGpWarps, 1)
         const int64_t p0 = __shfl_sync(kGpFull, b0, t), p1 = __shfl_sync(kGpFull, b1, t);
         if (p0 >= p1) continue;   // not a pivot row, or a column of L without entries below its diagonal
         const int32_t j = __shfl_sync(kGpFull, jl, t);
-        const double xj = x[j];
+        const T xj = x[j];
         // four rows per lane in flight (the column's rows are distinct)
         int64_t p = p0 + lane;
         for (; p + 96 < p1; p += 128) {
           const int32_t i0 = li[p], i1 = li[p + 32], i2 = li[p + 64], i3 = li[p + 96];
-          const double a0 = lx[p], a1 = lx[p + 32], a2 = lx[p + 64], a3 = lx[p + 96];
-          const double y0 = x[i0], y1 = x[i1], y2 = x[i2], y3 = x[i3];
-          x[i0] = __dsub_rn(y0, __dmul_rn(a0, xj));
-          x[i1] = __dsub_rn(y1, __dmul_rn(a1, xj));
-          x[i2] = __dsub_rn(y2, __dmul_rn(a2, xj));
-          x[i3] = __dsub_rn(y3, __dmul_rn(a3, xj));
+          const T a0 = lx[p], a1 = lx[p + 32], a2 = lx[p + 64], a3 = lx[p + 96];
+          const T y0 = x[i0], y1 = x[i1], y2 = x[i2], y3 = x[i3];
+          x[i0] = O::sub(y0, O::mul(a0, xj));
+          x[i1] = O::sub(y1, O::mul(a1, xj));
+          x[i2] = O::sub(y2, O::mul(a2, xj));
+          x[i3] = O::sub(y3, O::mul(a3, xj));
         }
         for (; p < p1; p += 32) {
           const int32_t i = li[p];
-          x[i] = __dsub_rn(x[i], __dmul_rn(lx[p], xj));
+          x[i] = O::sub(x[i], O::mul(lx[p], xj));
         }
         __syncwarp();
       }
     }
     // U entries in reach order; largest unpivoted magnitude, first on ties
     // (gplu.jl:238-254)
-    double best = -1.0;
+    R best = R(-1);
     int64_t bpos = INT64_MAX;
     for (int64_t base = top; base < n; base += 32) {
       const int64_t px = base + lane;
       bool piv = false;
       int32_t pi = -1;
-      double v = 0.0;
+      T v = O::zero();
       if (px < n) {
         const int32_t i = xi[px];
         pi = pinv[i];
         v = x[i];
         piv = pi >= 0;
         if (!piv) {
-          const double t = fabs(v);
+          const R t = O::mag(v);
           if (t > best) {
             best = t;
             bpos = px;
@@ -326,7 +456,7 @@ __global__ void __launch_bounds__(32 * kGpWarps, 1)
       unz += c;
     }
     for (int off = 16; off; off >>= 1) {
-      const double ob = __shfl_xor_sync(kGpFull, best, off);
+      const R ob = __shfl_xor_sync(kGpFull, best, off);
       const int64_t op = __shfl_xor_sync(kGpFull, bpos, off);
       if (ob > best || (ob == best && op < bpos)) {
         best = ob;
@@ -334,7 +464,7 @@ __global__ void __launch_bounds__(32 * kGpWarps, 1)
       }
     }
     int32_t ipiv = bpos == INT64_MAX ? -1 : xi[bpos];
-    if (ipiv < 0 || best <= 0.0) {   // gplu.jl:255-258
+    if (ipiv < 0 || best <= R(0)) {   // gplu.jl:255-258
       if (check) {
         if (lane == 0) status[s] = k + 1;
         return;
@@ -342,8 +472,8 @@ __global__ void __launch_bounds__(32 * kGpWarps, 1)
       if (ipiv < 0) ipiv = col;
     }
     // threshold partial pivoting: the diagonal row when it is large enough
-    if (pinv[col] < 0 && fabs(x[col]) >= __dmul_rn(tol, best)) ipiv = col;
-    const double pivot = x[ipiv];
+    if (pinv[col] < 0 && O::mag(x[col]) >= O::rmul(tol, best)) ipiv = col;
+    const T pivot = x[ipiv];
     if (lnz + 1 > d.lcap) {
       if (lane == 0) status[s] = kGpOverflowL;
       return;
@@ -354,7 +484,7 @@ __global__ void __launch_bounds__(32 * kGpWarps, 1)
       up[k + 1] = unz + 1;
       pinv[ipiv] = (int32_t)k;
       li[lnz] = ipiv;
-      lx[lnz] = 1.0;
+      lx[lnz] = O::one();
     }
     ++unz;
     ++lnz;
@@ -365,7 +495,7 @@ __global__ void __launch_bounds__(32 * kGpWarps, 1)
       const int64_t px = base + lane;
       bool keep = false;
       int32_t i = -1;
-      double v = 0.0;
+      T v = O::zero();
       if (px < n) {
         i = xi[px];
         keep = pinv[i] < 0;
@@ -380,10 +510,10 @@ __global__ void __launch_bounds__(32 * kGpWarps, 1)
       if (keep) {
         const int rk = __popc(bal & ((1u << lane) - 1u));
         li[lnz + rk] = i;
-        lx[lnz + rk] = __ddiv_rn(v, pivot);
+        lx[lnz + rk] = O::div(v, pivot);
       }
       lnz += c;
-      if (px < n) x[i] = 0.0;
+      if (px < n) x[i] = O::zero();
     }
     if (lane == 0) lp[k + 1] = lnz;
     __syncwarp();
@@ -397,12 +527,12 @@ __global__ void __launch_bounds__(32 * kGpWarps, 1)
 
 // Copy the factors of the finished systems list[0..nlist) from the old
 // segments to the new ones (a rerun grew other systems' room).
+template <typename T>
 __global__ void k_gplu_move(const GpSys* __restrict__ olds, const GpSys* __restrict__ news,
                             const int32_t* __restrict__ list, int64_t nlist, const int64_t* __restrict__ lp,
-                            const int64_t* __restrict__ up, const int32_t* __restrict__ oli,
-                            const double* __restrict__ olx, const int32_t* __restrict__ oui,
-                            const double* __restrict__ oux, int32_t* __restrict__ nli, double* __restrict__ nlx,
-                            int32_t* __restrict__ nui, double* __restrict__ nux) {
+                            const int64_t* __restrict__ up, const int32_t* __restrict__ oli, const T* __restrict__ olx,
+                            const int32_t* __restrict__ oui, const T* __restrict__ oux, int32_t* __restrict__ nli,
+                            T* __restrict__ nlx, int32_t* __restrict__ nui, T* __restrict__ nux) {
   const int64_t w = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (w >= nlist) return;
@@ -424,8 +554,9 @@ constexpr int kGpSortStage = 1024;   // keys of a column staged in shared memory
 // One column's (key, value) pairs from (ki, kx) to (oi, ox): keys relabelled
 // by map (NULL: as they are) and, when sorting, placed by rank (the keys of
 // a column are distinct, so the rank is the sorted position; gplu.jl:383-415).
-__device__ __forceinline__ void gp_column_out(int64_t len, const int32_t* ki, const double* kx, const int32_t* map,
-                                              bool sort, int32_t* oi, double* ox, int32_t* stage, int lane) {
+template <typename T>
+__device__ __forceinline__ void gp_column_out(int64_t len, const int32_t* ki, const T* kx, const int32_t* map,
+                                              bool sort, int32_t* oi, T* ox, int32_t* stage, int lane) {
   if (!sort || len <= 1) {
     for (int64_t e = lane; e < len; e += 32) {
       oi[e] = map ? map[ki[e]] : ki[e];
@@ -455,10 +586,11 @@ __device__ __forceinline__ void gp_column_out(int64_t len, const int32_t* ki, co
 // Finished factors (gplu.jl:292-302): L's rows in pivot order, both factors'
 // columns sorted when sort is set, p = invperm(pinv).  One warp per column of
 // every system whose status is 0.
+template <typename T>
 __global__ void __launch_bounds__(32 * kGpWarps)
     k_gplu_finish(const GpSys* __restrict__ sys, const int32_t* __restrict__ col_sys, int64_t ncols,
-                  const int64_t* __restrict__ status, GpFactors F, int sort, int32_t* __restrict__ lo_i,
-                  double* __restrict__ lo_x, int32_t* __restrict__ uo_i, double* __restrict__ uo_x,
+                  const int64_t* __restrict__ status, GpFactors<T> F, int sort, int32_t* __restrict__ lo_i,
+                  T* __restrict__ lo_x, int32_t* __restrict__ uo_i, T* __restrict__ uo_x,
                   int32_t* __restrict__ perm) {
   __shared__ int32_t stage[kGpWarps][kGpSortStage];
   const int lane = threadIdx.x & 31;
@@ -480,47 +612,50 @@ __global__ void __launch_bounds__(32 * kGpWarps)
 }
 
 // The finished factors of a batch, for the solves.
+template <typename T>
 struct GpSolveArgs {
   const GpSys* sys;
   const int64_t* lp;
   const int32_t* li;
-  const double* lx;
+  const T* lx;
   const int64_t* up;
   const int32_t* ui;
-  const double* ux;
-  const int32_t* perm;   // p (0-based)
+  const T* ux;
+  const int32_t* perm;                    // p (0-based)
   const int32_t* q;
-  const double* rs;      // NULL: the raw GPLUFactorization solve
-  const int64_t* acp;    // unscaled A for the refinement residual
+  const typename GpArith<T>::R* rs;       // NULL: the raw GPLUFactorization solve
+  const int64_t* acp;                     // unscaled A for the refinement residual
   const int32_t* ari;
-  const double* ax;
+  const T* ax;
 };
 
 // c = L \ c then U \ c in place (solve.jl:10-39), all lanes of the warp.
-__device__ __forceinline__ void gp_lu_solve(const GpSolveArgs& A, const GpSys& d, double* c, int lane) {
+template <typename T>
+__device__ __forceinline__ void gp_lu_solve(const GpSolveArgs<T>& A, const GpSys& d, T* c, int lane) {
+  using O = GpArith<T>;
   const int64_t n = d.n;
   const int64_t* lp = A.lp + d.cp0;
   const int32_t* li = A.li + d.l0;
-  const double* lx = A.lx + d.l0;
+  const T* lx = A.lx + d.l0;
   const int64_t* up = A.up + d.cp0;
   const int32_t* ui = A.ui + d.u0;
-  const double* ux = A.ux + d.u0;
+  const T* ux = A.ux + d.u0;
   for (int64_t j = 0; j < n; ++j) {
     const int64_t p0 = lp[j] + 1, p1 = lp[j + 1];
     if (p0 >= p1) continue;
-    const double yj = c[j];
+    const T yj = c[j];
     for (int64_t p = p0 + lane; p < p1; p += 32) {
       const int32_t i = li[p];
-      c[i] = __dsub_rn(c[i], __dmul_rn(lx[p], yj));
+      c[i] = O::sub(c[i], O::mul(lx[p], yj));
     }
     __syncwarp();
   }
   for (int64_t j = n - 1; j >= 0; --j) {
     const int64_t p0 = up[j], pd = up[j + 1] - 1;
-    const double yj = __ddiv_rn(c[j], ux[pd]);
+    const T yj = O::div(c[j], ux[pd]);
     for (int64_t p = p0 + lane; p < pd; p += 32) {
       const int32_t i = ui[p];
-      c[i] = __dsub_rn(c[i], __dmul_rn(ux[p], yj));
+      c[i] = O::sub(c[i], O::mul(ux[p], yj));
     }
     if (lane == 0) c[j] = yj;
     __syncwarp();
@@ -532,9 +667,11 @@ __device__ __forceinline__ void gp_lu_solve(const GpSolveArgs& A, const GpSys& d
 // workspaces hold system s's nrhs columns at col0 * nrhs, column r at
 // + r * n.  The refinement residual r = b - A x is the column-oriented
 // product of the unscaled A, as SparseArrays forms it.
+template <typename T>
 __global__ void __launch_bounds__(128, 1)
-    k_gplu_solve(GpSolveArgs A, int64_t nsys, int64_t nrhs, const double* __restrict__ B, double* __restrict__ X,
-                 double* __restrict__ C, double* __restrict__ R, int refine) {
+    k_gplu_solve(GpSolveArgs<T> A, int64_t nsys, int64_t nrhs, const T* __restrict__ B, T* __restrict__ X,
+                 T* __restrict__ C, T* __restrict__ R, int refine) {
+  using O = GpArith<T>;
   const int lane = threadIdx.x & 31;
   const int64_t w = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (w >= nsys * nrhs) return;
@@ -542,16 +679,16 @@ __global__ void __launch_bounds__(128, 1)
   const GpSys d = A.sys[s];
   const int64_t n = d.n;
   const int64_t off = d.col0 * nrhs + rr * n;
-  const double* b = B + off;
-  double* x = X + off;
-  double* c = C + off;
-  double* ax = R + off;
+  const T* b = B + off;
+  T* x = X + off;
+  T* c = C + off;
+  T* ax = R + off;
   const int32_t* p = A.perm + d.col0;
   const int32_t* q = A.q + d.col0;
-  const double* rs = A.rs ? A.rs + d.col0 : nullptr;
+  const auto* rs = A.rs ? A.rs + d.col0 : nullptr;
   for (int64_t k = lane; k < n; k += 32) {
     const int32_t i = p[k];
-    c[k] = rs ? __dmul_rn(rs[i], b[i]) : b[i];
+    c[k] = rs ? O::scale(rs[i], b[i]) : b[i];
   }
   __syncwarp();
   gp_lu_solve(A, d, c, lane);
@@ -559,27 +696,27 @@ __global__ void __launch_bounds__(128, 1)
   __syncwarp();
   const int64_t* cp = A.acp + d.cp0;
   const int32_t* ri = A.ari + d.nz0;
-  const double* av = A.ax + d.nz0;
+  const T* av = A.ax + d.nz0;
   for (int it = 0; it < refine; ++it) {
-    for (int64_t i = lane; i < n; i += 32) ax[i] = 0.0;
+    for (int64_t i = lane; i < n; i += 32) ax[i] = O::zero();
     __syncwarp();
     for (int64_t j = 0; j < n; ++j) {
-      const double xj = x[j];
+      const T xj = x[j];
       for (int64_t pa = cp[j] + lane; pa < cp[j + 1]; pa += 32) {
         const int32_t i = ri[pa];
-        ax[i] = __dadd_rn(ax[i], __dmul_rn(av[pa], xj));
+        ax[i] = O::add(ax[i], O::mul(av[pa], xj));
       }
       __syncwarp();
     }
-    for (int64_t i = lane; i < n; i += 32) ax[i] = __dsub_rn(b[i], ax[i]);   // r = b - A x
+    for (int64_t i = lane; i < n; i += 32) ax[i] = O::sub(b[i], ax[i]);   // r = b - A x
     __syncwarp();
     for (int64_t k = lane; k < n; k += 32) {
       const int32_t i = p[k];
-      c[k] = rs ? __dmul_rn(rs[i], ax[i]) : ax[i];
+      c[k] = rs ? O::scale(rs[i], ax[i]) : ax[i];
     }
     __syncwarp();
     gp_lu_solve(A, d, c, lane);
-    for (int64_t k = lane; k < n; k += 32) x[q[k]] = __dadd_rn(x[q[k]], c[k]);
+    for (int64_t k = lane; k < n; k += 32) x[q[k]] = O::add(x[q[k]], c[k]);
     __syncwarp();
   }
 }

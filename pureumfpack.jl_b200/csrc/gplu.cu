@@ -87,6 +87,15 @@ int64_t clamp_cap(int64_t e, int64_t n) {
 
 unsigned blocks_for(int64_t warps, int per_block) { return (unsigned)((warps + per_block - 1) / per_block); }
 
+// Element types of a handle's factors: the reference's Tv.
+enum GpType { kGpF64 = 0, kGpF32 = 1, kGpC64 = 2 };
+
+// Value e of a system's input as the device type (ComplexF64 as interleaved
+// re, im doubles).
+inline double load_val(const double* p, int64_t e, double*) { return p[e]; }
+inline float load_val(const float* p, int64_t e, float*) { return p[e]; }
+inline GpComplex load_val(const double* p, int64_t e, GpComplex*) { return GpComplex{p[2 * e], p[2 * e + 1]}; }
+
 }  // namespace
 
 struct mfgpu_gplu {
@@ -101,6 +110,8 @@ struct mfgpu_gplu {
   std::vector<int64_t> status;
   std::vector<int32_t> q;     // 0-based orders, every system
   bool factored = false, scaled = false;
+  int vt = kGpF64;            // element type of the factors
+  size_t esize = 8;           // bytes per value
   double t_factor_ms = 0, t_finish_ms = 0, t_solve_ms = 0;
   int64_t attempts = 0, reruns = 0;
   GBuf d_sys, d_sys_old, d_list, d_colsys, d_acp, d_ari, d_ax, d_rs, d_q, d_status;
@@ -182,16 +193,29 @@ void lay_out(std::vector<GpSys>& sys, const std::vector<int64_t>& cap_l, const s
   }
 }
 
-GpFactors working(mfgpu_gplu* g) {
-  return GpFactors{g->d_lp.as<int64_t>(), g->d_li.as<int32_t>(), g->d_lx.as<double>(), g->d_up.as<int64_t>(),
-                   g->d_ui.as<int32_t>(), g->d_ux.as<double>(), g->d_pinv.as<int32_t>()};
+template <typename T>
+GpFactors<T> working(mfgpu_gplu* g) {
+  return GpFactors<T>{g->d_lp.as<int64_t>(), g->d_li.as<int32_t>(), g->d_lx.as<T>(), g->d_up.as<int64_t>(),
+                      g->d_ui.as<int32_t>(), g->d_ux.as<T>(), g->d_pinv.as<int32_t>()};
 }
 
+template <typename T> constexpr int type_of();
+template <> constexpr int type_of<double>() { return kGpF64; }
+template <> constexpr int type_of<float>() { return kGpF32; }
+template <> constexpr int type_of<GpComplex>() { return kGpC64; }
+
+// T: the device value type; In: the caller's value array element (double
+// pairs for ComplexF64); R: the real type of Rs and tol.
+template <typename T, typename In>
 int factor_impl(mfgpu_gplu* g, int64_t nsys, const int64_t* n, const int64_t* const* colptr,
-                const int64_t* const* rowval, const double* const* nzval, const int64_t* const* qin,
-                const double* const* rs, double tol, int32_t check, int32_t sort_factors, int64_t* status_out) {
+                const int64_t* const* rowval, const In* const* nzval, const int64_t* const* qin,
+                const typename GpArith<T>::R* const* rs, typename GpArith<T>::R tol, int32_t check,
+                int32_t sort_factors, int64_t* status_out) {
+  using R = typename GpArith<T>::R;
   if (nsys < 0 || (nsys > 0 && (!n || !colptr))) return fail(g, MFGPU_ERR_ARGUMENT, "bad system arrays");
   g->factored = false;
+  g->vt = type_of<T>();
+  g->esize = sizeof(T);
   g->nsys = nsys;
   g->sys.assign(nsys, GpSys{});
   g->status.assign(nsys, kGpPending);
@@ -225,7 +249,8 @@ int factor_impl(mfgpu_gplu* g, int64_t nsys, const int64_t* n, const int64_t* co
   // host arrays: 0-based pattern, values, orders, scaling
   std::vector<int64_t> acp(ncp);
   std::vector<int32_t> ari(nnz_all), colsys(ncols);
-  std::vector<double> ax(nnz_all), rsv(any_rs ? ncols : 0, 1.0);
+  std::vector<T> ax(nnz_all);
+  std::vector<R> rsv(any_rs ? ncols : 0, R(1));
   g->q.assign(ncols, 0);
   for (int64_t s = 0; s < nsys; ++s) {
     const GpSys& d = g->sys[s];
@@ -233,7 +258,7 @@ int factor_impl(mfgpu_gplu* g, int64_t nsys, const int64_t* n, const int64_t* co
     for (int64_t j = 0; j <= ns; ++j) acp[d.cp0 + j] = colptr[s][j] - 1;
     for (int64_t e = 0; e < nnz; ++e) {
       ari[d.nz0 + e] = (int32_t)(rowval[s][e] - 1);
-      ax[d.nz0 + e] = nzval[s][e];
+      ax[d.nz0 + e] = load_val(nzval[s], e, (T*)nullptr);
     }
     std::vector<char> seen(ns, 0);
     for (int64_t k = 0; k < ns; ++k) {
@@ -265,10 +290,10 @@ int factor_impl(mfgpu_gplu* g, int64_t nsys, const int64_t* n, const int64_t* co
   g->d_pinv.ensure(ncols * 4);
   g->d_perm.ensure(ncols * 4);
   g->d_li.ensure(tot_l * 4);
-  g->d_lx.ensure(tot_l * 8);
+  g->d_lx.ensure(tot_l * sizeof(T));
   g->d_ui.ensure(tot_u * 4);
-  g->d_ux.ensure(tot_u * 8);
-  g->d_x.ensure(ncols * 8);
+  g->d_ux.ensure(tot_u * sizeof(T));
+  g->d_x.ensure(ncols * sizeof(T));
   g->d_xi.ensure(ncols * 4);
   g->d_stack.ensure(ncols * 4);
   g->d_pstack.ensure(ncols * 8);
@@ -277,15 +302,15 @@ int factor_impl(mfgpu_gplu* g, int64_t nsys, const int64_t* n, const int64_t* co
   for (int64_t s = 0; s < nsys; ++s) list[s] = (int32_t)s;
   g->attempts = g->reruns = 0;
   g->t_factor_ms = g->t_finish_ms = 0;
-  const GpWork W{g->d_x.as<double>(), g->d_xi.as<int32_t>(), g->d_stack.as<int32_t>(), g->d_pstack.as<int64_t>(),
-                 g->d_mark.as<int32_t>()};
+  const GpWork<T> W{g->d_x.as<T>(), g->d_xi.as<int32_t>(), g->d_stack.as<int32_t>(), g->d_pstack.as<int64_t>(),
+                    g->d_mark.as<int32_t>()};
   while (!list.empty()) {
     put(g->d_list, list, st);
     GP_CK(cudaEventRecord(g->ev[0], st));
-    k_gplu_factor<<<blocks_for((int64_t)list.size(), kGpWarps), 32 * kGpWarps, 0, st>>>(
+    k_gplu_factor<T><<<blocks_for((int64_t)list.size(), kGpWarps), 32 * kGpWarps, 0, st>>>(
         g->d_sys.as<GpSys>(), g->d_list.as<int32_t>(), (int64_t)list.size(), g->d_acp.as<int64_t>(),
-        g->d_ari.as<int32_t>(), g->d_ax.as<double>(), any_rs ? g->d_rs.as<double>() : nullptr, g->d_q.as<int32_t>(),
-        tol, check ? 1 : 0, working(g), W, g->d_status.as<int64_t>());
+        g->d_ari.as<int32_t>(), g->d_ax.as<T>(), any_rs ? g->d_rs.as<R>() : nullptr, g->d_q.as<int32_t>(), tol,
+        check ? 1 : 0, working<T>(g), W, g->d_status.as<int64_t>());
     GP_CK(cudaGetLastError());
     GP_CK(cudaEventRecord(g->ev[1], st));
     GP_CK(cudaMemcpyAsync(g->status.data(), g->d_status.p, nsys * 8, cudaMemcpyDeviceToHost, st));
@@ -315,18 +340,17 @@ int factor_impl(mfgpu_gplu* g, int64_t nsys, const int64_t* n, const int64_t* co
     lay_out(g->sys, cap_l, cap_u, tot_l, tot_u);
     GBuf nli, nlx, nui, nux;
     nli.ensure(tot_l * 4);
-    nlx.ensure(tot_l * 8);
+    nlx.ensure(tot_l * sizeof(T));
     nui.ensure(tot_u * 4);
-    nux.ensure(tot_u * 8);
+    nux.ensure(tot_u * sizeof(T));
     put(g->d_sys_old, old, st);
     put(g->d_sys, g->sys, st);
     if (!done.empty()) {
       put(g->d_list, done, st);
-      k_gplu_move<<<blocks_for((int64_t)done.size(), 4), 128, 0, st>>>(
+      k_gplu_move<T><<<blocks_for((int64_t)done.size(), 4), 128, 0, st>>>(
           g->d_sys_old.as<GpSys>(), g->d_sys.as<GpSys>(), g->d_list.as<int32_t>(), (int64_t)done.size(),
-          g->d_lp.as<int64_t>(), g->d_up.as<int64_t>(), g->d_li.as<int32_t>(), g->d_lx.as<double>(),
-          g->d_ui.as<int32_t>(), g->d_ux.as<double>(), nli.as<int32_t>(), nlx.as<double>(), nui.as<int32_t>(),
-          nux.as<double>());
+          g->d_lp.as<int64_t>(), g->d_up.as<int64_t>(), g->d_li.as<int32_t>(), g->d_lx.as<T>(),
+          g->d_ui.as<int32_t>(), g->d_ux.as<T>(), nli.as<int32_t>(), nlx.as<T>(), nui.as<int32_t>(), nux.as<T>());
       GP_CK(cudaGetLastError());
     }
     GP_CK(cudaStreamSynchronize(st));
@@ -338,15 +362,15 @@ int factor_impl(mfgpu_gplu* g, int64_t nsys, const int64_t* n, const int64_t* co
   }
   // relabel and sort (gplu.jl:292-302)
   g->d_lo_i.ensure(tot_l * 4);
-  g->d_lo_x.ensure(tot_l * 8);
+  g->d_lo_x.ensure(tot_l * sizeof(T));
   g->d_uo_i.ensure(tot_u * 4);
-  g->d_uo_x.ensure(tot_u * 8);
+  g->d_uo_x.ensure(tot_u * sizeof(T));
   GP_CK(cudaEventRecord(g->ev[2], st));
   if (ncols > 0) {
-    k_gplu_finish<<<blocks_for(ncols, kGpWarps), 32 * kGpWarps, 0, st>>>(
-        g->d_sys.as<GpSys>(), g->d_colsys.as<int32_t>(), ncols, g->d_status.as<int64_t>(), working(g),
-        sort_factors ? 1 : 0, g->d_lo_i.as<int32_t>(), g->d_lo_x.as<double>(), g->d_uo_i.as<int32_t>(),
-        g->d_uo_x.as<double>(), g->d_perm.as<int32_t>());
+    k_gplu_finish<T><<<blocks_for(ncols, kGpWarps), 32 * kGpWarps, 0, st>>>(
+        g->d_sys.as<GpSys>(), g->d_colsys.as<int32_t>(), ncols, g->d_status.as<int64_t>(), working<T>(g),
+        sort_factors ? 1 : 0, g->d_lo_i.as<int32_t>(), g->d_lo_x.as<T>(), g->d_uo_i.as<int32_t>(),
+        g->d_uo_x.as<T>(), g->d_perm.as<int32_t>());
     GP_CK(cudaGetLastError());
   }
   GP_CK(cudaEventRecord(g->ev[3], st));
@@ -421,8 +445,30 @@ int mfgpu_gplu_factor(mfgpu_gplu* g, int64_t nsys, const int64_t* n, const int64
                       const int64_t* const* rowval, const double* const* nzval, const int64_t* const* q,
                       const double* const* rs, double tol, int32_t check, int32_t sort_factors, int64_t* status) {
   if (!g) return MFGPU_ERR_ARGUMENT;
-  return guarded(g, [&] { return factor_impl(g, nsys, n, colptr, rowval, nzval, q, rs, tol, check, sort_factors,
-                                             status); });
+  return guarded(g, [&] {
+    return factor_impl<double, double>(g, nsys, n, colptr, rowval, nzval, q, rs, tol, check, sort_factors, status);
+  });
+}
+
+int mfgpu_gplu_factor_f32(mfgpu_gplu* g, int64_t nsys, const int64_t* n, const int64_t* const* colptr,
+                          const int64_t* const* rowval, const float* const* nzval, const int64_t* const* q,
+                          const float* const* rs, double tol, int32_t check, int32_t sort_factors, int64_t* status) {
+  if (!g) return MFGPU_ERR_ARGUMENT;
+  return guarded(g, [&] {
+    return factor_impl<float, float>(g, nsys, n, colptr, rowval, nzval, q, rs, (float)tol, check, sort_factors,
+                                     status);
+  });
+}
+
+int mfgpu_gplu_factor_c64(mfgpu_gplu* g, int64_t nsys, const int64_t* n, const int64_t* const* colptr,
+                          const int64_t* const* rowval, const double* const* nzval_ri, const int64_t* const* q,
+                          const double* const* rs, double tol, int32_t check, int32_t sort_factors,
+                          int64_t* status) {
+  if (!g) return MFGPU_ERR_ARGUMENT;
+  return guarded(g, [&] {
+    return factor_impl<GpComplex, double>(g, nsys, n, colptr, rowval, nzval_ri, q, rs, tol, check, sort_factors,
+                                          status);
+  });
 }
 
 int mfgpu_gplu_sizes(mfgpu_gplu* g, int64_t sys, int64_t* out3) {
@@ -441,15 +487,22 @@ int mfgpu_gplu_sizes(mfgpu_gplu* g, int64_t sys, int64_t* out3) {
   });
 }
 
-int mfgpu_gplu_get_factors(mfgpu_gplu* g, int64_t sys, int64_t* lcolptr, int64_t* lrowval, double* lnzval,
-                           int64_t* ucolptr, int64_t* urowval, double* unzval, int64_t* p, int64_t* q,
-                           int64_t* pinv) {
+}  // extern "C"
+
+namespace {
+
+// One system's factors (values of the handle's element type, copied as
+// bytes: ComplexF64 as interleaved re, im doubles).
+int get_factors_impl(mfgpu_gplu* g, int vt, int64_t sys, int64_t* lcolptr, int64_t* lrowval, void* lnzval,
+                     int64_t* ucolptr, int64_t* urowval, void* unzval, int64_t* p, int64_t* q, int64_t* pinv) {
   if (!g) return MFGPU_ERR_ARGUMENT;
   if (!g->factored) return fail(g, MFGPU_ERR_STATE, "no completed factorization");
+  if (g->vt != vt) return fail(g, MFGPU_ERR_STATE, "the factors hold another element type");
   if (sys < 0 || sys >= g->nsys) return fail(g, MFGPU_ERR_ARGUMENT, "system index out of range");
   return guarded(g, [&] {
     const GpSys& d = g->sys[sys];
     const int64_t n = d.n;
+    const size_t es = g->esize;
     std::vector<int64_t> lp(n + 1), up(n + 1);
     GP_CK(cudaMemcpy(lp.data(), g->d_lp.as<int64_t>() + d.cp0, (n + 1) * 8, cudaMemcpyDeviceToHost));
     GP_CK(cudaMemcpy(up.data(), g->d_up.as<int64_t>() + d.cp0, (n + 1) * 8, cudaMemcpyDeviceToHost));
@@ -459,8 +512,8 @@ int mfgpu_gplu_get_factors(mfgpu_gplu* g, int64_t sys, int64_t* lcolptr, int64_t
     GP_CK(cudaMemcpy(ui.data(), g->d_uo_i.as<int32_t>() + d.u0, nu * 4, cudaMemcpyDeviceToHost));
     GP_CK(cudaMemcpy(pm.data(), g->d_perm.as<int32_t>() + d.col0, n * 4, cudaMemcpyDeviceToHost));
     GP_CK(cudaMemcpy(pv.data(), g->d_pinv.as<int32_t>() + d.col0, n * 4, cudaMemcpyDeviceToHost));
-    if (lnzval) GP_CK(cudaMemcpy(lnzval, g->d_lo_x.as<double>() + d.l0, nl * 8, cudaMemcpyDeviceToHost));
-    if (unzval) GP_CK(cudaMemcpy(unzval, g->d_uo_x.as<double>() + d.u0, nu * 8, cudaMemcpyDeviceToHost));
+    if (lnzval) GP_CK(cudaMemcpy(lnzval, g->d_lo_x.as<char>() + d.l0 * es, nl * es, cudaMemcpyDeviceToHost));
+    if (unzval) GP_CK(cudaMemcpy(unzval, g->d_uo_x.as<char>() + d.u0 * es, nu * es, cudaMemcpyDeviceToHost));
     for (int64_t k = 0; k <= n; ++k) {
       if (lcolptr) lcolptr[k] = lp[k] + 1;
       if (ucolptr) ucolptr[k] = up[k] + 1;
@@ -478,14 +531,17 @@ int mfgpu_gplu_get_factors(mfgpu_gplu* g, int64_t sys, int64_t* lcolptr, int64_t
   });
 }
 
-int mfgpu_gplu_solve(mfgpu_gplu* g, int64_t nrhs, const double* const* b, double* const* x, int32_t refine) {
+template <typename T>
+int solve_impl(mfgpu_gplu* g, int64_t nrhs, const void* const* b, void* const* x, int32_t refine) {
+  using R = typename GpArith<T>::R;
   if (!g || nrhs < 0 || refine < 0) return MFGPU_ERR_ARGUMENT;
   if (!g->factored) return fail(g, MFGPU_ERR_STATE, "solve before a completed factorization");
+  if (g->vt != type_of<T>()) return fail(g, MFGPU_ERR_STATE, "the factors hold another element type");
   if (nrhs == 0 || g->ncols == 0) return MFGPU_OK;
   if (!b || !x) return fail(g, MFGPU_ERR_ARGUMENT, "missing right-hand sides");
   return guarded(g, [&] {
     cudaStream_t st = g->st;
-    const size_t bytes = (size_t)g->ncols * nrhs * 8;
+    const size_t bytes = (size_t)g->ncols * nrhs * sizeof(T);
     g->d_b.ensure(bytes);
     g->d_xs.ensure(bytes);
     g->d_c.ensure(bytes);
@@ -494,23 +550,24 @@ int mfgpu_gplu_solve(mfgpu_gplu* g, int64_t nrhs, const double* const* b, double
       const GpSys& d = g->sys[s];
       if (d.n == 0) continue;
       if (!b[s] || !x[s]) throw GpFail(MFGPU_ERR_ARGUMENT, "missing right-hand side of a system");
-      GP_CK(cudaMemcpyAsync(g->d_b.as<double>() + d.col0 * nrhs, b[s], d.n * nrhs * 8, cudaMemcpyHostToDevice, st));
+      GP_CK(cudaMemcpyAsync(g->d_b.as<T>() + d.col0 * nrhs, b[s], d.n * nrhs * sizeof(T), cudaMemcpyHostToDevice,
+                            st));
     }
-    const GpSolveArgs A{g->d_sys.as<GpSys>(),    g->d_lp.as<int64_t>(),  g->d_lo_i.as<int32_t>(),
-                        g->d_lo_x.as<double>(),  g->d_up.as<int64_t>(),  g->d_uo_i.as<int32_t>(),
-                        g->d_uo_x.as<double>(),  g->d_perm.as<int32_t>(), g->d_q.as<int32_t>(),
-                        g->scaled ? g->d_rs.as<double>() : nullptr, g->d_acp.as<int64_t>(), g->d_ari.as<int32_t>(),
-                        g->d_ax.as<double>()};
+    const GpSolveArgs<T> A{g->d_sys.as<GpSys>(), g->d_lp.as<int64_t>(),    g->d_lo_i.as<int32_t>(),
+                           g->d_lo_x.as<T>(),    g->d_up.as<int64_t>(),    g->d_uo_i.as<int32_t>(),
+                           g->d_uo_x.as<T>(),    g->d_perm.as<int32_t>(),  g->d_q.as<int32_t>(),
+                           g->scaled ? g->d_rs.as<R>() : nullptr,          g->d_acp.as<int64_t>(),
+                           g->d_ari.as<int32_t>(), g->d_ax.as<T>()};
     GP_CK(cudaEventRecord(g->ev[0], st));
-    k_gplu_solve<<<blocks_for(g->nsys * nrhs, 4), 128, 0, st>>>(A, g->nsys, nrhs, g->d_b.as<double>(),
-                                                                 g->d_xs.as<double>(), g->d_c.as<double>(),
-                                                                 g->d_r.as<double>(), refine);
+    k_gplu_solve<T><<<blocks_for(g->nsys * nrhs, 4), 128, 0, st>>>(A, g->nsys, nrhs, g->d_b.as<T>(), g->d_xs.as<T>(),
+                                                                    g->d_c.as<T>(), g->d_r.as<T>(), refine);
     GP_CK(cudaGetLastError());
     GP_CK(cudaEventRecord(g->ev[1], st));
     for (int64_t s = 0; s < g->nsys; ++s) {
       const GpSys& d = g->sys[s];
       if (d.n == 0) continue;
-      GP_CK(cudaMemcpyAsync(x[s], g->d_xs.as<double>() + d.col0 * nrhs, d.n * nrhs * 8, cudaMemcpyDeviceToHost, st));
+      GP_CK(cudaMemcpyAsync(x[s], g->d_xs.as<T>() + d.col0 * nrhs, d.n * nrhs * sizeof(T), cudaMemcpyDeviceToHost,
+                            st));
     }
     GP_CK(cudaStreamSynchronize(st));
     float ms = 0;
@@ -518,6 +575,41 @@ int mfgpu_gplu_solve(mfgpu_gplu* g, int64_t nrhs, const double* const* b, double
     g->t_solve_ms = ms;
     return MFGPU_OK;
   });
+}
+
+}  // namespace
+
+extern "C" {
+
+int mfgpu_gplu_get_factors(mfgpu_gplu* g, int64_t sys, int64_t* lcolptr, int64_t* lrowval, double* lnzval,
+                           int64_t* ucolptr, int64_t* urowval, double* unzval, int64_t* p, int64_t* q,
+                           int64_t* pinv) {
+  return get_factors_impl(g, kGpF64, sys, lcolptr, lrowval, lnzval, ucolptr, urowval, unzval, p, q, pinv);
+}
+
+int mfgpu_gplu_get_factors_f32(mfgpu_gplu* g, int64_t sys, int64_t* lcolptr, int64_t* lrowval, float* lnzval,
+                               int64_t* ucolptr, int64_t* urowval, float* unzval, int64_t* p, int64_t* q,
+                               int64_t* pinv) {
+  return get_factors_impl(g, kGpF32, sys, lcolptr, lrowval, lnzval, ucolptr, urowval, unzval, p, q, pinv);
+}
+
+int mfgpu_gplu_get_factors_c64(mfgpu_gplu* g, int64_t sys, int64_t* lcolptr, int64_t* lrowval, double* lnzval_ri,
+                               int64_t* ucolptr, int64_t* urowval, double* unzval_ri, int64_t* p, int64_t* q,
+                               int64_t* pinv) {
+  return get_factors_impl(g, kGpC64, sys, lcolptr, lrowval, lnzval_ri, ucolptr, urowval, unzval_ri, p, q, pinv);
+}
+
+int mfgpu_gplu_solve(mfgpu_gplu* g, int64_t nrhs, const double* const* b, double* const* x, int32_t refine) {
+  return solve_impl<double>(g, nrhs, (const void* const*)b, (void* const*)x, refine);
+}
+
+int mfgpu_gplu_solve_f32(mfgpu_gplu* g, int64_t nrhs, const float* const* b, float* const* x, int32_t refine) {
+  return solve_impl<float>(g, nrhs, (const void* const*)b, (void* const*)x, refine);
+}
+
+int mfgpu_gplu_solve_c64(mfgpu_gplu* g, int64_t nrhs, const double* const* b_ri, double* const* x_ri,
+                         int32_t refine) {
+  return solve_impl<GpComplex>(g, nrhs, (const void* const*)b_ri, (void* const*)x_ri, refine);
 }
 
 int mfgpu_gplu_timings(mfgpu_gplu* g, double* out5) {

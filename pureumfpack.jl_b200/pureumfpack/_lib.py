@@ -84,6 +84,16 @@ SIGNATURES = [
     ("mfgpu_gplu_get_factors", ctypes.c_int, [vp, i64, i64p, i64p, f64p, i64p, i64p, f64p, i64p, i64p, i64p]),
     ("mfgpu_gplu_solve", ctypes.c_int, [vp, i64, ctypes.POINTER(vp), ctypes.POINTER(vp), i32]),
     ("mfgpu_gplu_timings", ctypes.c_int, [vp, f64p]),
+    ("mfgpu_gplu_factor_f32", ctypes.c_int, [vp, i64, i64p, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                             ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp), f64, i32,
+                                             i32, i64p]),
+    ("mfgpu_gplu_get_factors_f32", ctypes.c_int, [vp, i64, i64p, i64p, f32p, i64p, i64p, f32p, i64p, i64p, i64p]),
+    ("mfgpu_gplu_solve_f32", ctypes.c_int, [vp, i64, ctypes.POINTER(vp), ctypes.POINTER(vp), i32]),
+    ("mfgpu_gplu_factor_c64", ctypes.c_int, [vp, i64, i64p, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                             ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp), f64, i32,
+                                             i32, i64p]),
+    ("mfgpu_gplu_get_factors_c64", ctypes.c_int, [vp, i64, i64p, i64p, f64p, i64p, i64p, f64p, i64p, i64p, i64p]),
+    ("mfgpu_gplu_solve_c64", ctypes.c_int, [vp, i64, ctypes.POINTER(vp), ctypes.POINTER(vp), i32]),
     ("mfgpu_tune_features", ctypes.c_int, [vp, i64, i64p, f32p, i64]),
     ("mfgpu_tune_set_choice", ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int8), i64]),
     ("mfgpu_mlp_create", ctypes.c_int, [i32, i32, i32, ctypes.c_uint64, ctypes.POINTER(vp)]),

@@ -641,46 +641,68 @@ class GpluContext:
     def factor(self, As, qs=None, Rs=None, tol: float = 0.1, check: bool = True,
                sort_factors: bool = True) -> np.ndarray:
         """gplu(Rs_i .* A_i; q = qs[i], tol, check, sort_factors) for every
-        system; returns the per-system status (0, or the singular column)."""
+        system; returns the per-system status (0, or the singular column).
+        The values' type (Float64, Float32 or ComplexF64, the same for every
+        system) is the arithmetic's, as the reference's generic Tv."""
         for A in As:
             if A.m != A.n:
                 raise DimensionMismatch("gplu requires a square matrix")
+        kind = ("c64" if np.iscomplexobj(As[0].nzval) else "f32" if As[0].nzval.dtype == np.float32 else "f64") \
+            if As else "f64"
+        for A in As:
+            k = "c64" if np.iscomplexobj(A.nzval) else "f32" if A.nzval.dtype == np.float32 else "f64"
+            if k != kind:
+                raise ArgumentError("every system of a batch needs the same element type")
+        vt = {"f64": np.float64, "f32": np.float32, "c64": np.complex128}[kind]
+        rt = np.float32 if kind == "f32" else np.float64
         cps = [_i(A.colptr) for A in As]
         rvs = [_i(A.rowval) for A in As]
-        nzs = [_f(A.nzval) for A in As]
+        nzs = [np.ascontiguousarray(A.nzval, dtype=vt) for A in As]
         n = np.array([A.n for A in As], np.int64)
         qa = None if qs is None else [_i(q) if q is not None else None for q in qs]
-        ra = None if Rs is None else [_f(r) if r is not None else None for r in Rs]
+        ra = None if Rs is None else [np.ascontiguousarray(r, dtype=rt) if r is not None else None for r in Rs]
 
         def parr(arrs):
             if arrs is None:
                 return None
             return (ctypes.c_void_p * len(arrs))(*[a.ctypes.data if a is not None else None for a in arrs])
 
+        fn = {"f64": self._lib.mfgpu_gplu_factor, "f32": self._lib.mfgpu_gplu_factor_f32,
+              "c64": self._lib.mfgpu_gplu_factor_c64}[kind]
         status = np.zeros(len(As), np.int64)
-        self._check(self._lib.mfgpu_gplu_factor(self._h, len(As), L.ptr(n), parr(cps), parr(rvs), parr(nzs),
-                                                parr(qa), parr(ra), float(tol), int(bool(check)),
-                                                int(bool(sort_factors)), L.ptr(status)))
+        self._check(fn(self._h, len(As), L.ptr(n), parr(cps), parr(rvs), parr(nzs), parr(qa), parr(ra), float(tol),
+                       int(bool(check)), int(bool(sort_factors)), L.ptr(status)))
+        self.kind = kind
         self.sizes = [A.n for A in As]
         self.n = As[0].n if len(As) == 1 else 0
         return status
 
     def factors(self, sys: int = 0):
-        """(L, U, p, q, pinv) of system sys: A_i[p, q] == L * U."""
+        """(L, U, p, q, pinv) of system sys: A_i[p, q] == L * U, values in
+        the factored element type."""
         sz = np.empty(3, np.int64)
         self._check(self._lib.mfgpu_gplu_sizes(self._h, int(sys), L.ptr(sz)))
         n, nl, nu = (int(v) for v in sz)
-        Lp, Li, Lx = np.empty(n + 1, np.int64), np.empty(nl, np.int64), np.empty(nl)
-        Up, Ui, Ux = np.empty(n + 1, np.int64), np.empty(nu, np.int64), np.empty(nu)
+        kind = getattr(self, "kind", "f64")
+        vt = {"f64": np.float64, "f32": np.float32, "c64": np.complex128}[kind]
+        Lp, Li, Lx = np.empty(n + 1, np.int64), np.empty(nl, np.int64), np.empty(nl, vt)
+        Up, Ui, Ux = np.empty(n + 1, np.int64), np.empty(nu, np.int64), np.empty(nu, vt)
         p, q, pinv = np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.int64)
-        self._check(self._lib.mfgpu_gplu_get_factors(self._h, int(sys), L.ptr(Lp), L.ptr(Li), L.ptr(Lx, L.f64p),
-                                                     L.ptr(Up), L.ptr(Ui), L.ptr(Ux, L.f64p), L.ptr(p), L.ptr(q),
-                                                     L.ptr(pinv)))
+        fn, vp = {"f64": (self._lib.mfgpu_gplu_get_factors, L.f64p),
+                  "f32": (self._lib.mfgpu_gplu_get_factors_f32, L.f32p),
+                  "c64": (self._lib.mfgpu_gplu_get_factors_c64, L.f64p)}[kind]
+        lx = Lx.view(np.float64) if kind == "c64" else Lx
+        ux = Ux.view(np.float64) if kind == "c64" else Ux
+        self._check(fn(self._h, int(sys), L.ptr(Lp), L.ptr(Li), L.ptr(lx, vp), L.ptr(Up), L.ptr(Ui), L.ptr(ux, vp),
+                       L.ptr(p), L.ptr(q), L.ptr(pinv)))
         return SparseCSC(n, n, Lp, Li, Lx), SparseCSC(n, n, Up, Ui, Ux), p, q, pinv
 
     def solve_batch(self, Bs, refine: int = 0):
-        """x_i for every system's b_i (vectors, or n_i x k with one k)."""
-        Bs = [np.asfortranarray(b, dtype=np.float64) for b in Bs]
+        """x_i for every system's b_i (vectors, or n_i x k with one k), in
+        the factored element type."""
+        kind = getattr(self, "kind", "f64")
+        vt = {"f64": np.float64, "f32": np.float32, "c64": np.complex128}[kind]
+        Bs = [np.asfortranarray(b, dtype=vt) for b in Bs]
         if len(Bs) != len(self.sizes):
             raise DimensionMismatch("one right-hand side block per system")
         k = 1 if Bs[0].ndim == 1 else Bs[0].shape[1]
@@ -688,7 +710,9 @@ class GpluContext:
             if b.shape[0] != n or (1 if b.ndim == 1 else b.shape[1]) != k:
                 raise DimensionMismatch("right-hand side block does not match its system")
         Xs = [np.empty_like(b) for b in Bs]
-        self._check(self._lib.mfgpu_gplu_solve(self._h, k, L.ptr_array(Bs), L.ptr_array(Xs), int(refine)))
+        fn = {"f64": self._lib.mfgpu_gplu_solve, "f32": self._lib.mfgpu_gplu_solve_f32,
+              "c64": self._lib.mfgpu_gplu_solve_c64}[kind]
+        self._check(fn(self._h, k, L.ptr_array(Bs), L.ptr_array(Xs), int(refine)))
         return Xs
 
     def solve(self, b, refine: int = 0) -> np.ndarray:

@@ -10,9 +10,13 @@ reference's GP-LU tests (test/pureumfpack_test.jl:11-123,
 test/multifrontal_test.jl:12-21, test/robustness.jl:38-42,
 test/interfaces.jl): the orderings and scalings of splu(A; method=:gplu),
 tol 0 / 0.1 / 1 (threshold and strict partial pivoting), sort_factors off,
-singular matrices, a batch of independent systems, and factors that outgrow
-their first segment.
+singular matrices, a batch of independent systems, factors that outgrow
+their first segment, and the reference's generic element types
+(test/robustness.jl:8-26): ComplexF64 in Julia's complex arithmetic and
+Float32 end to end.
 """
+
+import ctypes
 
 import numpy as np
 import pytest
@@ -184,3 +188,108 @@ def test_context_reuse_and_state():
     with pytest.raises(ArgumentError):
         bad = SparseCSC(2, 2, np.array([1, 3, 4]), np.array([2, 1, 2]), np.ones(3))   # rows not ascending
         ctx.factor([bad])
+
+
+# -- the reference's generic Tv: ComplexF64 and Float32 (test/robustness.jl) --
+def sprand_c(n, density, shift, seed):
+    import scipy.sparse as sp
+
+    rng = np.random.default_rng(seed)
+    nnz = rng.binomial(n * n, density)
+    I, J = rng.integers(0, n, nnz), rng.integers(0, n, nnz)
+    V = rng.random(nnz) + 1j * rng.random(nnz)
+    return (sp.coo_matrix((V, (I, J)), shape=(n, n)).tocsc() + shift * sp.eye(n, format="csc")).tocsc()
+
+
+def grid_c(k, seed):
+    """Complex values on the 3-D grid pattern with a weak diagonal: row
+    interchanges under tol = 1."""
+    import scipy.sparse as sp
+
+    S = M.poisson3d(k).to_scipy().tocoo()
+    rng = np.random.default_rng(seed)
+    v = rng.standard_normal(S.nnz) + 1j * rng.standard_normal(S.nnz)
+    return sp.csc_matrix((v, (S.row, S.col)), shape=S.shape)
+
+
+def crandn(n, seed, k=None):
+    rng = np.random.default_rng(seed)
+    shape = (n,) if k is None else (n, k)
+    return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+
+@pytest.mark.parametrize("ordering", ["amd", "colamd", "natural"])
+def test_complex_splu_matches_oracle_bitwise(ordering):
+    """test/robustness.jl:8-17 (splu's default method on ComplexF64)."""
+    S = sprand_c(400, 8 / 400, 5.0, 7)
+    A, Ao = SparseCSC.from_scipy(S), O.ComplexCSC.from_scipy(S)
+    Fo = O.splu_gplu(Ao, ordering=ordering)
+    F = splu(A, ordering=ordering)
+    np.testing.assert_array_equal(F.Rs, Fo.Rs)
+    assert_bitwise(Fo.F, *F.ctx.factors())
+    b = crandn(400, 8)
+    for refine in (0, 1):
+        x = solve(F, b, refine=refine)
+        np.testing.assert_array_equal(x, O.solve_gplu(Fo, b, refine=refine))
+        assert np.linalg.norm(S @ x - b) / np.linalg.norm(b) <= 1e-10
+
+
+@pytest.mark.parametrize("tol", [0.1, 1.0])
+def test_complex_grid_with_interchanges(tol):
+    S = grid_c(7, 3)
+    A, Ao = SparseCSC.from_scipy(S), O.ComplexCSC.from_scipy(S)
+    q = O.amd_order_sym(Ao)
+    Fo = O.gplu(Ao, q=q, tol=tol)
+    F = gplu(A, q=q, tol=tol)
+    assert not np.array_equal(Fo.p, Fo.q)   # rows were interchanged
+    assert_bitwise(Fo, F.L, F.U, F.p, F.q, F.pinv)
+    B = crandn(A.n, 4, 3)
+    np.testing.assert_array_equal(F.ldiv(B), O.solve_gplu(Fo, B))
+
+
+def test_float32_splu_matches_oracle_bitwise():
+    """test/robustness.jl:18-26: a Float32 matrix is factored and solved in
+    Float32 (x is Float32, residual <= 1e-4)."""
+    n = 300
+    rng = np.random.default_rng(9)
+    nnz = rng.binomial(n * n, 8 / n)
+    I, J = rng.integers(1, n + 1, nnz), rng.integers(1, n + 1, nnz)
+    d = np.arange(1, n + 1)
+    A = SparseCSC.from_coo(np.concatenate([I, d]), np.concatenate([J, d]),
+                           np.concatenate([rng.random(nnz), np.full(n, 5.0)]), n, n).astype(np.float32)
+    b = rng.standard_normal(n).astype(np.float32)
+    Fo = O.splu_gplu(A, ordering="amd")
+    F = splu(A, ordering="amd")
+    assert F.Rs.dtype == np.float32
+    L, U, p, q, pinv = F.ctx.factors()
+    assert L.nzval.dtype == np.float32
+    assert_bitwise(Fo.F, SparseCSC(n, n, L.colptr, L.rowval, L.nzval.astype(np.float64)),
+                   SparseCSC(n, n, U.colptr, U.rowval, U.nzval.astype(np.float64)), p, q, pinv)
+    for refine in (0, 2):
+        x = solve(F, b, refine=refine)
+        assert x.dtype == np.float32
+        np.testing.assert_array_equal(x, O.solve_gplu(Fo, b, refine=refine))
+    x = F.ldiv(b)
+    assert np.linalg.norm(A.to_scipy().astype(np.float64) @ x - b) / np.linalg.norm(b) <= 1e-4
+
+
+def test_complex_batch_and_type_checks():
+    """A batch of complex systems, each as splu(A_i) alone; the handle's
+    real-valued calls refuse its complex factors."""
+    Ss = [sprand_c(60 + 13 * i, 6 / (60 + 13 * i), 4.0, 20 + i) for i in range(6)] + [grid_c(5, 9)]
+    As = [SparseCSC.from_scipy(S) for S in Ss]
+    Fb = BatchGPLU(As, ordering="colamd", tol=0.1, scale=SCALE_MAX)
+    Bs = [crandn(A.n, 30 + i, 2) for i, A in enumerate(As)]
+    Xs = Fb.solve(Bs, refine=1)
+    for i, S in enumerate(Ss):
+        Fo = O.splu_gplu(O.ComplexCSC.from_scipy(S), ordering="colamd", tol=0.1, scale=O.SCALE_MAX)
+        assert_bitwise(Fo.F, *Fb.factors(i))
+        np.testing.assert_array_equal(Xs[i], O.solve_gplu(Fo, Bs[i], refine=1))
+    ctx = Fb.ctx
+    n = As[0].n
+    out = np.empty(n + 1, np.int64)
+    rc = ctx._lib.mfgpu_gplu_get_factors(ctx._h, 0, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), None, None,
+                                         None, None, None, None, None, None)
+    assert rc == -4   # MFGPU_ERR_STATE: complex factors, real fetch
+    with pytest.raises(ArgumentError):   # one element type per batch
+        ctx.factor([As[0], SparseCSC.from_scipy(Ss[1].real)])
