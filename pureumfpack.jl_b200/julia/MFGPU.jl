@@ -12,6 +12,7 @@ module MFGPU
 
 using SparseArrays: SparseMatrixCSC, nonzeros, rowvals
 using LinearAlgebra: SingularException
+using Libdl
 
 const libmfgpu = get(ENV, "PUREUMFPACK_MFGPU", joinpath(@__DIR__, "..", "pureumfpack", "libmfgpu.so"))
 
@@ -246,6 +247,7 @@ end
 mutable struct GpluHandle
     ptr::Ptr{Cvoid}
     ns::Vector{Int}
+    T::DataType    # element type of the last factorization
 end
 
 function _gcheck(g::GpluHandle, rc::Cint)
@@ -260,29 +262,40 @@ function gplu_create(; device::Integer = 0)
     ptr = Ref{Ptr{Cvoid}}(C_NULL)
     rc = ccall((:mfgpu_gplu_create, libmfgpu), Cint, (Int32, Ref{Ptr{Cvoid}}), Int32(device), ptr)
     rc == 0 || error("mfgpu_gplu_create failed ($rc): needs a B200 / sm_100 device")
-    g = GpluHandle(ptr[], Int[])
+    g = GpluHandle(ptr[], Int[], Float64)
     finalizer(x -> ccall((:mfgpu_gplu_destroy, libmfgpu), Cvoid, (Ptr{Cvoid},), x.ptr), g)
     return g
 end
 
-# gplu(rs[i] .* As[i]; q = qs[i], tol, check, sort_factors) for every system;
+# The C entry points of each element type (the reference's generic Tv):
+# values, Rs (real(Tv)) and the suffix of the factor / get / solve symbols.
+_gsuffix(::Type{Float64}) = ""
+_gsuffix(::Type{Float32}) = "_f32"
+_gsuffix(::Type{ComplexF64}) = "_c64"
+_gsym(base::String, T::DataType) = Symbol(base * _gsuffix(T))
+
+# gplu(rs[i] .* As[i]; q = qs[i], tol, check, sort_factors) for every
+# system, all of one element type Tv (Float64, Float32 or ComplexF64);
 # throws SingularException(k) for the first singular system under check.
-function gplu_factor!(g::GpluHandle, As::AbstractVector{<:SparseMatrixCSC{Float64, <:Integer}},
+function gplu_factor!(g::GpluHandle, As::AbstractVector{<:SparseMatrixCSC{Tv, <:Integer}},
                       qs::AbstractVector; rs = nothing, tol::Real = 0.1, check::Bool = true,
-                      sort_factors::Bool = true)
+                      sort_factors::Bool = true) where {Tv <: Union{Float64, Float32, ComplexF64}}
     ns = Int64[size(A, 1) for A in As]
     cols = [_i64(A.colptr) for A in As]
     rows = [_i64(rowvals(A)) for A in As]
     qv = [_i64(q) for q in qs]
     status = zeros(Int64, length(As))
-    rsp = rs === nothing ? Ptr{Float64}[C_NULL for _ in As] : Ptr{Float64}[pointer(r) for r in rs]
-    GC.@preserve As cols rows qv rs _gcheck(g, ccall((:mfgpu_gplu_factor, libmfgpu), Cint,
-        (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Ptr{Int64}}, Ptr{Ptr{Int64}}, Ptr{Ptr{Float64}}, Ptr{Ptr{Int64}},
-         Ptr{Ptr{Float64}}, Float64, Int32, Int32, Ptr{Int64}),
+    R = real(Tv)
+    rsp = rs === nothing ? Ptr{R}[C_NULL for _ in As] : Ptr{R}[pointer(r) for r in rs]
+    fn = _gsym("mfgpu_gplu_factor", Tv)
+    GC.@preserve As cols rows qv rs _gcheck(g, ccall(Libdl.dlsym(_libhandle(), fn), Cint,
+        (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Ptr{Int64}}, Ptr{Ptr{Int64}}, Ptr{Ptr{Tv}}, Ptr{Ptr{Int64}},
+         Ptr{Ptr{R}}, Float64, Int32, Int32, Ptr{Int64}),
         g.ptr, length(As), ns, Ptr{Int64}[pointer(c) for c in cols], Ptr{Int64}[pointer(r) for r in rows],
-        Ptr{Float64}[pointer(nonzeros(A)) for A in As], Ptr{Int64}[pointer(q) for q in qv], rsp,
+        Ptr{Tv}[pointer(nonzeros(A)) for A in As], Ptr{Int64}[pointer(q) for q in qv], rsp,
         Float64(tol), Int32(check), Int32(sort_factors), status))
     g.ns = Int.(ns)
+    g.T = Tv
     k = findfirst(>(0), status)
     k === nothing || throw(SingularException(Int(status[k])))
     return g
@@ -290,27 +303,36 @@ end
 
 # GPLUFactorization fields (src/gplu.jl:45-51) of system i (1-based).
 function gplu_factors(g::GpluHandle, i::Integer = 1)
+    T = g.T
     sz = Vector{Int64}(undef, 3)
     _gcheck(g, ccall((:mfgpu_gplu_sizes, libmfgpu), Cint, (Ptr{Cvoid}, Int64, Ptr{Int64}), g.ptr, i - 1, sz))
     n, nl, nu = sz
-    Lp = Vector{Int64}(undef, n + 1); Li = Vector{Int64}(undef, nl); Lx = Vector{Float64}(undef, nl)
-    Up = Vector{Int64}(undef, n + 1); Ui = Vector{Int64}(undef, nu); Ux = Vector{Float64}(undef, nu)
+    Lp = Vector{Int64}(undef, n + 1); Li = Vector{Int64}(undef, nl); Lx = Vector{T}(undef, nl)
+    Up = Vector{Int64}(undef, n + 1); Ui = Vector{Int64}(undef, nu); Ux = Vector{T}(undef, nu)
     p = Vector{Int64}(undef, n); q = Vector{Int64}(undef, n); pinv = Vector{Int64}(undef, n)
-    _gcheck(g, ccall((:mfgpu_gplu_get_factors, libmfgpu), Cint,
-        (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}, Ptr{Int64},
+    _gcheck(g, ccall(Libdl.dlsym(_libhandle(), _gsym("mfgpu_gplu_get_factors", T)), Cint,
+        (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{T}, Ptr{Int64}, Ptr{Int64}, Ptr{T}, Ptr{Int64},
          Ptr{Int64}, Ptr{Int64}), g.ptr, i - 1, Lp, Li, Lx, Up, Ui, Ux, p, q, pinv))
     return SparseMatrixCSC(n, n, Lp, Li, Lx), SparseMatrixCSC(n, n, Up, Ui, Ux), p, q, pinv
 end
 
 # solve(F_i, b_i; refine) for every system (PureLU semantics when the
-# systems were factored with rs, the raw F \ b otherwise).
-function gplu_solve(g::GpluHandle, Bs::Vector{Matrix{Float64}}; refine::Integer = 0)
-    Xs = [similar(B) for B in Bs]
-    GC.@preserve Bs Xs _gcheck(g, ccall((:mfgpu_gplu_solve, libmfgpu), Cint,
-        (Ptr{Cvoid}, Int64, Ptr{Ptr{Float64}}, Ptr{Ptr{Float64}}, Int32),
-        g.ptr, size(Bs[1], 2), Ptr{Float64}[pointer(B) for B in Bs], Ptr{Float64}[pointer(X) for X in Xs],
-        Int32(refine)))
+# systems were factored with rs, the raw F \ b otherwise), in the factors'
+# element type.
+function gplu_solve(g::GpluHandle, Bs::Vector{<:Matrix}; refine::Integer = 0)
+    T = g.T
+    Bt = [Matrix{T}(B) for B in Bs]
+    Xs = [similar(B) for B in Bt]
+    GC.@preserve Bt Xs _gcheck(g, ccall(Libdl.dlsym(_libhandle(), _gsym("mfgpu_gplu_solve", T)), Cint,
+        (Ptr{Cvoid}, Int64, Ptr{Ptr{T}}, Ptr{Ptr{T}}, Int32),
+        g.ptr, size(Bt[1], 2), Ptr{T}[pointer(B) for B in Bt], Ptr{T}[pointer(X) for X in Xs], Int32(refine)))
     return Xs
+end
+
+const _LIBHANDLE = Ref{Ptr{Cvoid}}(C_NULL)
+function _libhandle()
+    _LIBHANDLE[] == C_NULL && (_LIBHANDLE[] = Libdl.dlopen(libmfgpu))
+    return _LIBHANDLE[]
 end
 
 end # module
