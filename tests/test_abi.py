@@ -45,3 +45,24 @@ def test_gpu_entry_points_fail_cleanly_without_device(has_gpu):
     assert rc == -8 and not h.value
     assert L.mfgpu_factor(None, None, None, 1) == -1
     assert L.mfgpu_solve(None, 1, None, 1, None, 1, 0) == -1
+
+
+def test_gplu_entry_points_fail_cleanly_without_device(has_gpu):
+    """The Gilbert-Peierls handle needs a B200; without one it is refused and
+    the Python entry points raise instead of computing anywhere else."""
+    if has_gpu:
+        pytest.skip("a GPU is present")
+    from pureumfpack import MfgpuError, SparseCSC, _lib, gplu, splu
+
+    L = _lib.lib()
+    g = ctypes.c_void_p()
+    assert L.mfgpu_gplu_create(0, ctypes.byref(g)) == -8 and not g.value
+    assert L.mfgpu_gplu_create(0, None) == -1
+    assert L.mfgpu_gplu_factor(None, 0, None, None, None, None, None, None, 0.1, 1, 1, None) == -1
+    assert L.mfgpu_gplu_solve(None, 1, None, None, 0) == -1
+    assert L.mfgpu_gplu_solve_c64(None, 1, None, None, 0) == -1
+    A = SparseCSC.from_coo([1, 2], [1, 2], [2.0, 3.0], 2, 2)
+    with pytest.raises(MfgpuError):
+        gplu(A)
+    with pytest.raises(MfgpuError):
+        splu(A)   # the default method is :gplu
