@@ -28,6 +28,12 @@ batched handle per GPU; one step = factor + solve(refine) of every system to
 backward error <= 1e-14 per system.  With N > 1 the systems are split across
 ranks by predicted flops (no collective); value = the max over ranks of the
 step time (strong scaling: the batch is fixed).
+
+`--method gplu` measures splu's default method instead, the Gilbert-Peierls
+factorization (one warp per system) with solve(refine=2), on poisson2d-100
+or a batch-N workload, beside the oracle's restatement on the host cores;
+a single-GPU default run also reports it for poisson2d-100 under `gplu`
+(`--no-gplu` skips it).
 """
 
 from __future__ import annotations
@@ -80,6 +86,8 @@ def parse():
     ap.add_argument("--method", default="multifrontal", choices=["multifrontal", "gplu"],
                     help="gplu: splu(A; method=:gplu) (Gilbert-Peierls, one warp per system) on --workload "
                          "poisson2d-100 (default for this method) or batch-N")
+    ap.add_argument("--no-gplu", action="store_true",
+                    help="skip the side measurement of splu's default Gilbert-Peierls method on poisson2d-100")
     ap.add_argument("--no-autotune", action="store_true",
                     help="mixed form: keep the built-in GEMM variant rule instead of the learned autotuner")
     return ap.parse_args()
@@ -586,24 +594,21 @@ def run_f32(args):
     return 0
 
 
-def run_gplu(args):
+def gplu_measure(wl: str, steps: int, warmup: int, cpu: bool = True) -> dict:
     """splu(A; method=:gplu, ordering=:amd, tol=0.1, scale=SCALE_SUM) then
     solve(F, b; refine=2) (src/interface.jl:93-120,170-177) on one system or
-    a batch of independent systems, with host buffers; beside it the oracle's
-    restatement of the same Gilbert-Peierls factorization and solve on the
-    host cores (one system per thread).  value = the device time of the
-    library's kernels (factor, finish, solve; CUDA events on its stream),
-    e2e = the API calls' wall time (ordering, scaling, copies included)."""
+    a batch of independent systems (`batch-N`), with host buffers; beside it
+    the oracle's restatement of the same Gilbert-Peierls factorization and
+    solve on the host cores (one system per thread).  s = the device time of
+    the library's kernels (factor, finish, solve; CUDA events on its stream,
+    median over the timed steps), e2e_s = the API calls' wall time
+    (ordering, scaling, copies included)."""
     from concurrent.futures import ThreadPoolExecutor
-
-    import torch
 
     from oracle import oracle as O
     from pureumfpack import SCALE_SUM, BatchGPLU
     from pureumfpack import matrices as M
 
-    torch.cuda.set_device(0)
-    wl = args.workload if args.workload != "poisson3d-64" else "poisson2d-100"
     if wl.startswith("batch-"):
         sysl = M.batched_set(int(wl.split("-", 1)[1]), seed=0, nrhs=4)
         desc = "2-D side U[16,64] / 3-D side U[8,20], shift U[0,1], 4 rhs each"
@@ -614,12 +619,12 @@ def run_gplu(args):
     As, Bs = [a for a, _ in sysl], [b for _, b in sysl]
     refine = 2
     dev_ms, wall = [], []
-    for it in range(args.warmup + args.steps):
+    for it in range(warmup + steps):
         t0 = time.perf_counter()
         F = BatchGPLU(As, ordering="amd", tol=0.1, scale=SCALE_SUM)
         Xs = F.solve(Bs, refine=refine)
         t1 = time.perf_counter()
-        if it >= args.warmup:
+        if it >= warmup:
             tm = F.ctx.timings()
             dev_ms.append(tm["factor_ms"] + tm["finish_ms"] + tm["solve_ms"])
             wall.append(t1 - t0)
@@ -634,8 +639,8 @@ def run_gplu(args):
         exact &= (np.array_equal(L.rowval, Fo.F.Lrowval) and np.array_equal(L.nzval, Fo.F.Lnzval)
                   and np.array_equal(U.rowval, Fo.F.Urowval) and np.array_equal(U.nzval, Fo.F.Unzval)
                   and np.array_equal(p, Fo.F.p) and np.array_equal(Xs[i], O.solve(Fo, Bs[i], refine=refine)))
-    cpu = None
-    if not args.no_cpu_baseline:
+    cpu_line = None
+    if cpu:
         cores = os.cpu_count() or 1
 
         def one(i):
@@ -645,20 +650,34 @@ def run_gplu(args):
         t0 = time.perf_counter()
         with ThreadPoolExecutor(max_workers=cores) as ex:
             list(ex.map(one, range(len(As))))
-        cpu = {"value": time.perf_counter() - t0, "unit": "s", "cores": min(cores, len(As)), "kind": "port",
-               "sample": f"the oracle's splu(method=:gplu, AMD) + solve(refine={refine}) of every system, "
-                         f"one system per host thread"}
-    sec = float(np.median(dev_ms)) / 1e3
-    line = {"metric": f"{wl} splu(method=:gplu) factor+solve s", "value": sec, "unit": "s", "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": f"{wl}: {len(As)} system(s), {desc}, AMD, SCALE_SUM, "
-                                                        f"tol 0.1, refine {refine}"},
-            "e2e": {"value": float(np.median(wall)), "unit": "s",
-                    "h2d_bytes_per_step": int(sum(A.nnz() * 16 + A.n * 16 + B.nbytes for A, B in sysl)),
-                    "d2h_bytes_per_step": int(sum(B.nbytes for B in Bs))},
+        cpu_line = {"value": time.perf_counter() - t0, "unit": "s", "cores": min(cores, len(As)), "kind": "port",
+                    "sample": f"the oracle's splu(method=:gplu, AMD) + solve(refine={refine}) of every system, "
+                              f"one system per host thread"}
+    return {"workload": f"{wl}: {len(As)} system(s), {desc}, AMD, SCALE_SUM, tol 0.1, refine {refine}",
+            "s": float(np.median(dev_ms)) / 1e3, "e2e_s": float(np.median(wall)),
+            "h2d_bytes": int(sum(A.nnz() * 16 + A.n * 16 + B.nbytes for A, B in sysl)),
+            "d2h_bytes": int(sum(B.nbytes for B in Bs)),
             "kernels_ms": {"factor": tm["factor_ms"], "finish": tm["finish_ms"], "solve": tm["solve_ms"]},
             "factor_launches": tm["factor_launches"], "reruns": tm["reruns"], "bwd_err": eta,
-            "parity": {"systems_checked": len(idx), "bitwise_equal": bool(exact)}, "cpu_baseline": cpu}
+            "parity": {"systems_checked": len(idx), "bitwise_equal": bool(exact)}, "cpu_baseline": cpu_line}
+
+
+def run_gplu(args):
+    """`--method gplu`: the Gilbert-Peierls path (gplu_measure) as its own
+    JSON line; `--workload` poisson2d-100 (the default for this method) or
+    batch-N.  One GPU."""
+    import torch
+
+    torch.cuda.set_device(0)
+    wl = args.workload if args.workload != "poisson3d-64" else "poisson2d-100"
+    g = gplu_measure(wl, args.steps, args.warmup, cpu=not args.no_cpu_baseline)
+    line = {"metric": f"{wl} splu(method=:gplu) factor+solve s", "value": g["s"], "unit": "s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": g["workload"]},
+            "e2e": {"value": g["e2e_s"], "unit": "s", "h2d_bytes_per_step": g["h2d_bytes"],
+                    "d2h_bytes_per_step": g["d2h_bytes"]},
+            "kernels_ms": g["kernels_ms"], "factor_launches": g["factor_launches"], "reruns": g["reruns"],
+            "bwd_err": g["bwd_err"], "parity": g["parity"], "cpu_baseline": g["cpu_baseline"]}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -887,6 +906,13 @@ def main():
                                                  "front_elems", "front_elems_full", "pool_elems", "lean",
                                                  "flops_inverse", "fronts", "merged", "flops_exec")},
     }
+    if world == 1 and not args.no_gplu:
+        # splu's default method (Gilbert-Peierls) on the 2-D Poisson matrix of
+        # the reference's CPU-runnable configuration, beside the headline
+        try:
+            line["gplu"] = gplu_measure("poisson2d-100", 3, 3, cpu=not args.no_cpu_baseline)
+        except Exception as e:  # a side measurement must not kill the headline
+            line["gplu"] = {"error": str(e)}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
