@@ -24,6 +24,8 @@ from __future__ import annotations
 
 import ctypes
 import json
+import os
+from concurrent.futures import ThreadPoolExecutor
 from enum import IntEnum
 
 import numpy as np
@@ -760,8 +762,11 @@ class BatchGPLU:
         if ordering not in order:
             raise ArgumentError(f"unknown ordering {ordering}")
         scale = ScaleKind(int(scale))
-        self.Rs = [row_scaling(A, scale) for A in self.As]
-        qs = [order[ordering](A) for A in self.As]
+        # the host orderings and scalings of the systems, side by side (the
+        # library's host code releases the interpreter and keeps no shared state)
+        with ThreadPoolExecutor(max_workers=max(1, min(len(self.As), os.cpu_count() or 1))) as ex:
+            qs = list(ex.map(order[ordering], self.As))
+            self.Rs = list(ex.map(lambda A: row_scaling(A, scale), self.As))
         self.ctx = GpluContext(device)
         if initial_capacity:
             self.ctx.set_initial_capacity(initial_capacity)
