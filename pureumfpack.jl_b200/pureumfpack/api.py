@@ -649,6 +649,14 @@ class GpluContext:
         for A in As:
             if A.m != A.n:
                 raise DimensionMismatch("gplu requires a square matrix")
+        for arrs, what in ((qs, "q"), (Rs, "Rs")):
+            if arrs is None:
+                continue
+            if len(arrs) != len(As):
+                raise DimensionMismatch(f"one {what} per system")
+            for A, a in zip(As, arrs):
+                if a is not None and len(a) != A.n:
+                    raise DimensionMismatch(f"length({what}) must equal size(A, 1)")
         kind = ("c64" if np.iscomplexobj(As[0].nzval) else "f32" if As[0].nzval.dtype == np.float32 else "f64") \
             if As else "f64"
         for A in As:

@@ -66,3 +66,21 @@ def test_gplu_entry_points_fail_cleanly_without_device(has_gpu):
         gplu(A)
     with pytest.raises(MfgpuError):
         splu(A)   # the default method is :gplu
+
+
+def test_gplu_wrapper_checks_lengths_before_the_library():
+    """q and Rs reach the C ABI as bare pointers, so the Python wrapper
+    checks their lengths first (DimensionMismatch, no library call)."""
+    import numpy as np
+
+    from pureumfpack import DimensionMismatch, SparseCSC
+    from pureumfpack.api import GpluContext
+
+    A = SparseCSC.from_coo([1, 2, 3], [1, 2, 3], [1.0, 2.0, 3.0], 3, 3)
+    ctx = GpluContext.__new__(GpluContext)   # no device needed: the checks come first
+    with pytest.raises(DimensionMismatch):
+        ctx.factor([A], [np.array([1, 2])])
+    with pytest.raises(DimensionMismatch):
+        ctx.factor([A], None, [np.ones(2)])
+    with pytest.raises(DimensionMismatch):
+        ctx.factor([A, A], [np.array([1, 2, 3])])
