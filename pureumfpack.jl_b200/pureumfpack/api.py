@@ -210,6 +210,8 @@ def symbolic_mf(A: SparseCSC, q=None, relax: bool = False) -> SymbolicMF:
     lib = L.lib()
     h = ctypes.c_void_p()
     qa = _i(q) if q is not None else None
+    if qa is not None and len(qa) != A.n:   # q reaches the C ABI as a bare pointer
+        raise DimensionMismatch("length(q) must equal size(A, 2)")
     _check_host(lib.mfgpu_symbolic_create(A.n, L.ptr(_i(A.colptr)), L.ptr(_i(A.rowval)), L.ptr(qa), ctypes.byref(h)))
     if relax:
         _check_host(lib.mfgpu_symbolic_relax(h))

@@ -61,3 +61,13 @@ def test_fill_kat_64():
     assert predicted_fill(S) == 3749118
     assert S.nsuper == 9348
     assert np.array_equal(np.sort(S.qf), np.arange(1, A.n + 1))
+
+
+def test_short_order_is_rejected_before_the_library():
+    """A caller's q reaches the C ABI as a bare pointer: a short one is a
+    DimensionMismatch on the host, never a read past its end."""
+    from pureumfpack import DimensionMismatch, SparseCSC, symbolic_mf
+
+    A = SparseCSC.from_coo([1, 2, 3], [1, 2, 3], [1.0, 2.0, 3.0], 3, 3)
+    with pytest.raises(DimensionMismatch):
+        symbolic_mf(A, q=[1, 2])
