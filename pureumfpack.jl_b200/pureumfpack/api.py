@@ -318,6 +318,15 @@ class GpuContext:
     def analyze(self, A: SparseCSC, S: SymbolicMF):
         self._check(self._lib.mfgpu_analyze_symbolic(self._h, A.n, L.ptr(_i(A.colptr)), L.ptr(_i(A.rowval)), S._h))
         self.n = A.n
+        self.nnz = A.nnz()
+
+    def _values(self, nzval, Rs):
+        """The factor calls copy nnz values and n row factors from bare
+        pointers: check the lengths against the analyzed pattern first."""
+        if getattr(self, "nnz", None) is not None and len(nzval) != self.nnz:
+            raise DimensionMismatch("nzval must hold one value per entry of the analyzed pattern")
+        if Rs is not None and len(Rs) != self.n:
+            raise DimensionMismatch("length(Rs) must equal size(A, 1)")
 
     def analyze_arrays(self, A: SparseCSC, qf, parent, sstart, upd_ptr, upd_idx):
         """mfgpu_analyze with the reference's own symbolic arrays (1-based)."""
@@ -329,14 +338,17 @@ class GpuContext:
                                             L.ptr(_i(parent)), ns, L.ptr(_i(sstart)), L.ptr(_i(upd_ptr)),
                                             L.ptr(_i(upd_idx))))
         self.n = A.n
+        self.nnz = A.nnz()
 
     def factor(self, nzval, Rs=None, check: bool = True) -> int:
+        self._values(nzval, Rs)
         rs = _f(Rs) if Rs is not None else None
         self.f32 = self.c64 = False
         return self._check(self._lib.mfgpu_factor(self._h, L.ptr(_f(nzval), L.f64p), L.ptr(rs, L.f64p), int(check)))
 
     def factor_f32(self, nzval, Rs=None, check: bool = True) -> int:
         """Factorization of a Float32 matrix: Float32 fronts, Float32 factors."""
+        self._values(nzval, Rs)
         v = np.ascontiguousarray(nzval, dtype=np.float32)
         rs = np.ascontiguousarray(Rs, dtype=np.float32) if Rs is not None else None
         self.f32, self.c64 = True, False
@@ -344,6 +356,7 @@ class GpuContext:
 
     def factor_c64(self, nzval, Rs=None, check: bool = True) -> int:
         """Factorization of a ComplexF64 matrix: complex fronts, complex factors."""
+        self._values(nzval, Rs)
         rs = _f(Rs) if Rs is not None else None
         self.f32, self.c64 = False, True
         return self._check(self._lib.mfgpu_factor_c64(self._h, L.ptr(_z(nzval), L.f64p), L.ptr(rs, L.f64p),
@@ -352,6 +365,7 @@ class GpuContext:
     def factor_scaled(self, nzval, scale, check: bool = True) -> int:
         """Row scaling of kind ``scale`` computed on the device, then the
         factorization of Diagonal(Rs) * A."""
+        self._values(nzval, None)
         return self._check(self._lib.mfgpu_factor_scaled(self._h, L.ptr(_f(nzval), L.f64p), int(scale), int(check)))
 
     def row_scaling(self) -> np.ndarray:
@@ -425,6 +439,7 @@ class GpuContext:
         """factor(nzval, Rs) then solve(b, refine) in one call, the
         right-hand sides' copy overlapped with the factorization.  Returns
         (status, x); x is None when the factorization found a singular column."""
+        self._values(nzval, Rs)
         rs = _f(Rs) if Rs is not None else None
         B = np.asfortranarray(b, dtype=np.float64)
         nrhs = 1 if B.ndim == 1 else B.shape[1]

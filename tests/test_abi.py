@@ -84,3 +84,22 @@ def test_gplu_wrapper_checks_lengths_before_the_library():
         ctx.factor([A], None, [np.ones(2)])
     with pytest.raises(DimensionMismatch):
         ctx.factor([A, A], [np.array([1, 2, 3])])
+
+
+def test_factor_wrapper_checks_value_lengths():
+    """The factor calls copy nnz values and n row factors from bare
+    pointers; the Python wrapper checks both against the analyzed pattern."""
+    import numpy as np
+
+    from pureumfpack import DimensionMismatch, GpuContext
+
+    ctx = GpuContext.__new__(GpuContext)   # no device needed: the checks come first
+    ctx.n, ctx.nnz = 3, 7
+    ctx._values(np.ones(7), np.ones(3))
+    with pytest.raises(DimensionMismatch):
+        ctx._values(np.ones(6), None)
+    with pytest.raises(DimensionMismatch):
+        ctx._values(np.ones(7), np.ones(2))
+    for call in (ctx.factor, ctx.factor_f32, ctx.factor_c64):
+        with pytest.raises(DimensionMismatch):
+            call(np.ones(5), None)
