@@ -243,7 +243,7 @@ end
 # its own ordering (amd_order_sym / colamd_order) and row scaling and hands
 # q and Rs over, e.g. in src/interface.jl's :gplu branch:
 #     g = MFGPU.gplu_create(); MFGPU.gplu_factor!(g, [A], [q]; rs = [Rs], tol = tol, check = check)
-#     L, U, p, q, pinv = MFGPU.gplu_factors(g, 1)
+#     L, U, p, q, pinv = MFGPU.gplu_factors(g, 1; indextype = Ti)
 mutable struct GpluHandle
     ptr::Ptr{Cvoid}
     ns::Vector{Int}
@@ -301,8 +301,10 @@ function gplu_factor!(g::GpluHandle, As::AbstractVector{<:SparseMatrixCSC{Tv, <:
     return g
 end
 
-# GPLUFactorization fields (src/gplu.jl:45-51) of system i (1-based).
-function gplu_factors(g::GpluHandle, i::Integer = 1)
+# GPLUFactorization fields (src/gplu.jl:45-51) of system i (1-based), with
+# index type Ti (that of the factored matrix: an Int32 matrix gets Int32
+# factors and permutations, test/robustness.jl:27-36).
+function gplu_factors(g::GpluHandle, i::Integer = 1; indextype::Type{<:Integer} = Int64)
     T = g.T
     sz = Vector{Int64}(undef, 3)
     _gcheck(g, ccall((:mfgpu_gplu_sizes, libmfgpu), Cint, (Ptr{Cvoid}, Int64, Ptr{Int64}), g.ptr, i - 1, sz))
@@ -313,7 +315,9 @@ function gplu_factors(g::GpluHandle, i::Integer = 1)
     _gcheck(g, ccall(Libdl.dlsym(_libhandle(), _gsym("mfgpu_gplu_get_factors", T)), Cint,
         (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{T}, Ptr{Int64}, Ptr{Int64}, Ptr{T}, Ptr{Int64},
          Ptr{Int64}, Ptr{Int64}), g.ptr, i - 1, Lp, Li, Lx, Up, Ui, Ux, p, q, pinv))
-    return SparseMatrixCSC(n, n, Lp, Li, Lx), SparseMatrixCSC(n, n, Up, Ui, Ux), p, q, pinv
+    Ti = indextype
+    return SparseMatrixCSC(n, n, _ti(Ti, Lp), _ti(Ti, Li), Lx), SparseMatrixCSC(n, n, _ti(Ti, Up), _ti(Ti, Ui), Ux),
+           _ti(Ti, p), _ti(Ti, q), _ti(Ti, pinv)
 end
 
 # solve(F_i, b_i; refine) for every system (PureLU semantics when the
