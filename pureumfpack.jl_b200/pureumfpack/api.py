@@ -586,7 +586,9 @@ def splu(A: SparseCSC, method: str = "gplu", ordering: str = "amd", tol: float =
     ``method="gplu"`` (the reference's default) orders the columns by
     ``ordering`` (``"amd"``, ``"colamd"`` or ``"natural"``) and runs the
     Gilbert-Peierls factorization on the GPU with threshold ``tol``
-    (``gplu``); ``precision`` and ``relax`` apply to the multifrontal method.
+    (``gplu``): the reference's exact results, but a chain of column steps
+    that one warp runs, far slower than ``method="multifrontal"`` on large
+    systems.  ``precision`` and ``relax`` apply to the multifrontal method.
     """
     method = method.lstrip(":") if isinstance(method, str) else method
     if A.m != A.n:
